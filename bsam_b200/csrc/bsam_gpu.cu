@@ -1,0 +1,635 @@
+// bsam_gpu.cu -- C ABI of the B200 FAS V-cycle (include/bsam_gpu.h).
+//
+// Host orchestration of the reference's MultigridIterations / AFASVcycle
+// (lib/afasroutines.f90:38-106, 488-547) over the device patch table.  All
+// field storage lives in one device arena per handle and stays resident
+// across time steps; host arrays cross the bus only in put/get calls.
+//
+// Device layout of a field (one component of one patch): element (i,j,k),
+// i in [0, mx1+1] etc., lives at base + i + j*sy + k*sz.  The allocation
+// starts `lead` elements before element (0,0,0) so that every interior row
+// (i = 1) begins on a 128-byte boundary; sy is a multiple of 128 bytes.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/bsam_gpu.h"
+#include "bsam_types.h"
+#include "kernels.cuh"
+
+using namespace bsam;
+
+namespace {
+
+struct LevelPlan {
+  int level = 0;
+  std::vector<int> patches;  // ApplyOnLevel order
+  Item* d_fine = nullptr;    // tiles over each patch's interior
+  int nfine = 0;
+  Item* d_coarse = nullptr;  // tiles over each patch's footprint in its parent
+  int ncoarse = 0;
+};
+
+}  // namespace
+
+struct bsam_gpu {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bsam_run_params rp{};
+  bool have_hierarchy = false;
+  int minlevel = 0, finestlevel = 0;
+  std::vector<bsam_patch_desc> desc;
+  std::vector<DevPatch> hp;
+  std::vector<int64_t> field_elems;  // elements per field allocation, per patch
+  DevPatch* d_patches = nullptr;
+  char* d_arena = nullptr;
+  size_t arena_bytes = 0;
+  std::vector<LevelPlan> levels;  // index level - minlevel
+  Item* d_items = nullptr;
+  double* d_partials = nullptr;
+  int max_items = 0;
+  DevStatus* d_status = nullptr;
+  DevStatus* h_status = nullptr;  // pinned
+  std::vector<double> trace;
+  std::string err;
+  // instrumentation
+  bool profiling = false;
+  bsam_gpu_stats stats{};
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pool;
+  size_t ev_used = 0;
+  int64_t ev_cells = 0;  // cells of the finest level
+};
+
+namespace {
+
+int fail(bsam_gpu* h, int code, const std::string& msg) {
+  if (h) h->err = msg;
+  return code;
+}
+
+#define CU(call)                                                                  \
+  do {                                                                            \
+    cudaError_t e_ = (call);                                                      \
+    if (e_ != cudaSuccess)                                                        \
+      return fail(h, BSAM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+int64_t roundup(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
+
+LevelPlan& plan(bsam_gpu* h, int level) { return h->levels[level - h->minlevel]; }
+
+void tiles_for(int patch, const int* n, int ndims, std::vector<Item>& out) {
+  const int tx = (n[0] + TILE_X - 1) / TILE_X;
+  const int ty = (n[1] + TILE_Y - 1) / TILE_Y;
+  const int tz = ndims == 3 ? n[2] : 1;
+  for (int z = 0; z < tz; ++z)
+    for (int y = 0; y < ty; ++y)
+      for (int x = 0; x < tx; ++x) out.push_back(Item{patch, x, y, z});
+}
+
+dim3 block_dim() { return dim3(32, TILE_Y, 1); }
+
+// Timed finest-level smoothing stages: events are pooled and read back at
+// the next host synchronisation (drain_events).
+void stage_begin(bsam_gpu* h, int level) {
+  if (!h->profiling || level != h->finestlevel) return;
+  if (h->ev_used == h->ev_pool.size()) {
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    h->ev_pool.push_back({a, b});
+  }
+  cudaEventRecord(h->ev_pool[h->ev_used].first, h->stream);
+}
+
+void stage_end(bsam_gpu* h, int level) {
+  if (!h->profiling || level != h->finestlevel) return;
+  cudaEventRecord(h->ev_pool[h->ev_used].second, h->stream);
+  ++h->ev_used;
+}
+
+void drain_events(bsam_gpu* h) {
+  for (size_t e = 0; e < h->ev_used; ++e) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, h->ev_pool[e].first, h->ev_pool[e].second) == cudaSuccess) {
+      h->stats.smooth_ms += ms;
+      h->stats.smooth_stages += 1;
+      h->stats.smooth_cells += h->ev_cells;
+      h->stats.smooth_bytes += 6.0 * sizeof(double) * (double)h->ev_cells;
+    }
+  }
+  h->ev_used = 0;
+}
+
+// Launch helpers dispatching on dimension (FP64 path).
+template <int D>
+void launch_relax(bsam_gpu* h, const LevelPlan& L, int color) {
+  k_relax<double, D><<<L.nfine, block_dim(), 0, h->stream>>>(h->d_patches, L.d_fine, color);
+}
+
+int ghost_level(bsam_gpu* h, int level);
+
+void relax_level(bsam_gpu* h, int level) {
+  const LevelPlan& L = plan(h, level);
+  stage_begin(h, level);
+  for (int pass = 0; pass < h->rp.nsmoothingpasses; ++pass)
+    for (int color = 0; color < 2; ++color) {
+      if (h->rp.ndims == 2) launch_relax<2>(h, L, color);
+      else launch_relax<3>(h, L, color);
+      ++h->stats.launches;
+    }
+  stage_end(h, level);
+}
+
+void vcycle(bsam_gpu* h, int level) {
+  relax_level(h, level);  // LevelRelax (afas:499)
+  if (level > h->minlevel) {
+    const LevelPlan& L = plan(h, level);
+    const dim3 b = block_dim();
+    if (h->rp.ndims == 2) {
+      k_restrict<double, 2><<<L.ncoarse, b, 0, h->stream>>>(h->d_patches, L.d_coarse);
+      k_coarse_load<double, 2><<<L.ncoarse, b, 0, h->stream>>>(h->d_patches, L.d_coarse);
+    } else {
+      k_restrict<double, 3><<<L.ncoarse, b, 0, h->stream>>>(h->d_patches, L.d_coarse);
+      k_coarse_load<double, 3><<<L.ncoarse, b, 0, h->stream>>>(h->d_patches, L.d_coarse);
+    }
+    h->stats.launches += 2;
+    vcycle(h, level - 1);  // afas:511
+    if (h->rp.ndims == 2)
+      k_correct<double, 2><<<L.nfine, b, 0, h->stream>>>(h->d_patches, L.d_fine);
+    else
+      k_correct<double, 3><<<L.nfine, b, 0, h->stream>>>(h->d_patches, L.d_fine);
+    ++h->stats.launches;
+    relax_level(h, level);  // afas:517
+  }
+}
+
+int ghost_level(bsam_gpu* h, int level) {
+  const LevelPlan& L = plan(h, level);
+  for (int p : L.patches) {
+    const DevPatch& P = h->hp[p];
+    int64_t total = (int64_t)(P.n[0] + 2) * (P.n[1] + 2) * (h->rp.ndims == 3 ? P.n[2] + 2 : 1);
+    int nb = (int)((total + 255) / 256);
+    if (h->rp.ndims == 2) k_setbc<double, 2><<<nb, 256, 0, h->stream>>>(h->d_patches, p, total);
+    else k_setbc<double, 3><<<nb, 256, 0, h->stream>>>(h->d_patches, p, total);
+    ++h->stats.launches;
+  }
+  return BSAM_OK;
+}
+
+int face_rule(int ndims, int face, int code, int* rule) {
+  if (code == 1) {
+    *rule = BC_COPY;
+  } else if (code >= 10 && code <= 99) {
+    // UserBC2D: faces 1,2 -> 2 - q (all vars); faces 3,4 -> copy of vars 1,2.
+    // UserBC3D: every face -> 2 - q (problem.f90:646-756).
+    *rule = (ndims == 2 && face >= 2) ? BC_COPY : BC_REFLECT;
+  } else if (code == 999) {
+    *rule = BC_NONE;
+  } else {
+    return -1;  // periodic (2) is not supported by this build
+  }
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* bsam_gpu_strerror(int code) {
+  switch (code) {
+    case BSAM_OK: return "ok";
+    case BSAM_ERR_ARG: return "invalid argument";
+    case BSAM_ERR_CUDA: return "CUDA runtime error";
+    case BSAM_ERR_NOMEM: return "device memory allocation failed";
+    case BSAM_ERR_STATE: return "call out of order";
+    case BSAM_ERR_UNSUPPORTED: return "configuration not supported";
+    case BSAM_ERR_NODEVICE: return "no usable CUDA device";
+    case BSAM_ERR_DIVERGED: return "non-finite residual";
+    default: return "unknown status";
+  }
+}
+
+const char* bsam_gpu_last_error(bsam_gpu* h) { return h ? h->err.c_str() : "null handle"; }
+
+int bsam_gpu_create(bsam_gpu** out, int device, const bsam_run_params* p) {
+  bsam_gpu* h = nullptr;
+  if (!out || !p) return BSAM_ERR_ARG;
+  *out = nullptr;
+  if (p->ndims < 2 || p->ndims > 3 || p->nrvars != 2 || p->mbc != 1 || p->maux != 0 ||
+      p->errortype != 1 || p->nsmoothingpasses < 1 || p->maxvcycles < 1)
+    return BSAM_ERR_UNSUPPORTED;
+  if (p->precision != BSAM_PREC_FP64) return BSAM_ERR_UNSUPPORTED;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= device || device < 0)
+    return BSAM_ERR_NODEVICE;
+  h = new bsam_gpu();
+  h->device = device;
+  h->rp = *p;
+  if (cudaSetDevice(device) != cudaSuccess) {
+    delete h;
+    return BSAM_ERR_NODEVICE;
+  }
+  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMalloc(&h->d_status, sizeof(DevStatus)) != cudaSuccess ||
+      cudaMallocHost(&h->h_status, sizeof(DevStatus)) != cudaSuccess) {
+    delete h;
+    return BSAM_ERR_CUDA;
+  }
+  cudaMemset(h->d_status, 0, sizeof(DevStatus));
+  *out = h;
+  return BSAM_OK;
+}
+
+static void free_hierarchy(bsam_gpu* h) {
+  for (auto& L : h->levels) {
+    L.d_fine = nullptr;
+    L.d_coarse = nullptr;
+  }
+  if (h->d_items) cudaFree(h->d_items);
+  if (h->d_arena) cudaFree(h->d_arena);
+  if (h->d_patches) cudaFree(h->d_patches);
+  if (h->d_partials) cudaFree(h->d_partials);
+  h->d_items = nullptr;
+  h->d_arena = nullptr;
+  h->d_patches = nullptr;
+  h->d_partials = nullptr;
+  h->levels.clear();
+  h->hp.clear();
+  h->desc.clear();
+  h->field_elems.clear();
+  h->have_hierarchy = false;
+}
+
+int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patches,
+                           int finestlevel) {
+  if (!h || npatch <= 0 || !patches) return BSAM_ERR_ARG;
+  CU(cudaSetDevice(h->device));
+  free_hierarchy(h);
+  const int nd = h->rp.ndims;
+  int minlevel = patches[0].level;
+  for (int p = 0; p < npatch; ++p) minlevel = std::min(minlevel, patches[p].level);
+  if (finestlevel < 0 || minlevel > 0) return fail(h, BSAM_ERR_ARG, "levels out of range");
+  if (finestlevel > 0)
+    return fail(h, BSAM_ERR_UNSUPPORTED, "levels above the root (AMR) need coarse-fine ghosts");
+  h->minlevel = minlevel;
+  h->finestlevel = finestlevel;
+  h->levels.assign(finestlevel - minlevel + 1, LevelPlan{});
+  for (int l = minlevel; l <= finestlevel; ++l) plan(h, l).level = l;
+  h->desc.assign(patches, patches + npatch);
+  h->hp.assign(npatch, DevPatch{});
+  h->field_elems.assign(npatch, 0);
+
+  const double eps2 = h->rp.eps * h->rp.eps;
+  size_t total = 0;
+  std::vector<size_t> offs(npatch);
+  for (int p = 0; p < npatch; ++p) {
+    const bsam_patch_desc& d = patches[p];
+    if (d.level < minlevel || d.level > finestlevel)
+      return fail(h, BSAM_ERR_ARG, "patch level out of range");
+    DevPatch& P = h->hp[p];
+    P.ndims = nd;
+    for (int n = 0; n < 3; ++n) {
+      P.n[n] = n < nd ? d.mx[n] : 1;
+      if (P.n[n] <= 0) return fail(h, BSAM_ERR_ARG, "mx must be positive");
+    }
+    P.parent = d.parent;
+    P.level = d.level;
+    P.prec = PREC_F64;
+    P.problem = 0;
+    if (d.parent >= 0) {
+      if (d.parent >= npatch || patches[d.parent].level != d.level - 1)
+        return fail(h, BSAM_ERR_ARG, "parent must be a patch on the next coarser level");
+      for (int n = 0; n < nd; ++n) {
+        if (P.n[n] % 2) return fail(h, BSAM_ERR_ARG, "a patch with a parent needs even mx");
+        P.cn[n] = P.n[n] / 2;
+        P.off[n] = d.mbounds[n][0] - 1;
+        if (d.mbounds[n][1] - d.mbounds[n][0] + 1 != P.cn[n] || P.off[n] < 0 ||
+            d.mbounds[n][1] > patches[d.parent].mx[n])
+          return fail(h, BSAM_ERR_ARG, "mbounds inconsistent with mx / parent");
+      }
+    } else if (d.level != minlevel) {
+      return fail(h, BSAM_ERR_ARG, "only the coarsest level may lack a parent");
+    }
+    for (int n = nd; n < 3; ++n) {
+      P.cn[n] = 1;
+      P.off[n] = 0;
+    }
+    P.wt = 1;
+    for (int f = 0; f < 6; ++f) {
+      if (f >= 2 * nd) {
+        P.bc[f] = BC_NONE;
+        continue;
+      }
+      int rule;
+      if (face_rule(nd, f, d.mthbc[f], &rule))
+        return fail(h, BSAM_ERR_UNSUPPORTED, "boundary code not supported");
+      P.bc[f] = rule;
+      if (rule == BC_NONE) P.wt = 0;
+    }
+    if (!P.wt) return fail(h, BSAM_ERR_UNSUPPORTED, "internal faces need AMR support");
+    // Layout (FP64): rows aligned to 128 bytes.
+    const int64_t A = 128 / sizeof(double), lead = A - 1;
+    P.sy = roundup(lead + P.n[0] + 2, A);
+    P.sz = nd == 3 ? P.sy * (P.n[1] + 2) : 0;
+    const int64_t vol = nd == 3 ? P.sz * (P.n[2] + 2) : P.sy * (P.n[1] + 2);
+    h->field_elems[p] = roundup(lead + vol, 32);
+    offs[p] = total;
+    const bool parent_of_any = [&] {
+      for (int c = 0; c < npatch; ++c)
+        if (patches[c].parent == p) return true;
+      return false;
+    }();
+    const int nfields = 2 /*q*/ + 2 /*f*/ + 2 /*qold*/ + (parent_of_any ? 2 : 0);
+    total += (size_t)h->field_elems[p] * nfields * sizeof(double);
+    // Problem constants (problem.f90:183-187): h2 = h*h; dt/h2; eps2/h2; 2d*eps2/h2.
+    P.h = d.dx;
+    const double h2 = d.dx * d.dx;
+    P.dt = h->rp.dt;
+    P.eps2 = eps2;
+    P.alpha = h->rp.alpha;
+    P.tmp1 = h->rp.dt / h2;
+    P.tmp2 = eps2 / h2;
+    P.tmp3 = (2.0 * nd) * eps2 / h2;
+    plan(h, d.level).patches.push_back(p);
+  }
+  if (cudaMalloc(&h->d_arena, total) != cudaSuccess)
+    return fail(h, BSAM_ERR_NOMEM, "arena allocation failed");
+  h->arena_bytes = total;
+  CU(cudaMemsetAsync(h->d_arena, 0, total, h->stream));
+  for (int p = 0; p < npatch; ++p) {
+    DevPatch& P = h->hp[p];
+    double* base = reinterpret_cast<double*>(h->d_arena + offs[p]);
+    const int64_t fe = h->field_elems[p], lead = 128 / sizeof(double) - 1;
+    int slot = 0;
+    auto next = [&]() { return (void*)(base + fe * (slot++) + lead); };
+    P.q[0] = next();
+    P.q[1] = next();
+    P.f[0] = next();
+    P.f[1] = next();
+    P.qo[0] = next();
+    P.qo[1] = next();
+    bool parent_of_any = false;
+    for (int c = 0; c < npatch; ++c) parent_of_any |= patches[c].parent == p;
+    if (parent_of_any) {
+      P.qs[0] = next();
+      P.qs[1] = next();
+    }
+  }
+  // Work lists.
+  std::vector<Item> all;
+  std::vector<std::pair<int, int>> spans_fine(h->levels.size()), spans_coarse(h->levels.size());
+  for (size_t li = 0; li < h->levels.size(); ++li) {
+    LevelPlan& L = h->levels[li];
+    int s = (int)all.size();
+    for (int p : L.patches) tiles_for(p, h->hp[p].n, nd, all);
+    spans_fine[li] = {s, (int)all.size() - s};
+    s = (int)all.size();
+    for (int p : L.patches)
+      if (h->hp[p].parent >= 0) tiles_for(p, h->hp[p].cn, nd, all);
+    spans_coarse[li] = {s, (int)all.size() - s};
+  }
+  CU(cudaMalloc(&h->d_items, all.size() * sizeof(Item)));
+  CU(cudaMemcpyAsync(h->d_items, all.data(), all.size() * sizeof(Item), cudaMemcpyHostToDevice,
+                     h->stream));
+  h->max_items = 1;
+  for (size_t li = 0; li < h->levels.size(); ++li) {
+    LevelPlan& L = h->levels[li];
+    L.d_fine = h->d_items + spans_fine[li].first;
+    L.nfine = spans_fine[li].second;
+    L.d_coarse = h->d_items + spans_coarse[li].first;
+    L.ncoarse = spans_coarse[li].second;
+    h->max_items = std::max(h->max_items, L.nfine);
+  }
+  CU(cudaMalloc(&h->d_partials, sizeof(double) * h->max_items));
+  CU(cudaMalloc(&h->d_patches, sizeof(DevPatch) * npatch));
+  CU(cudaMemcpyAsync(h->d_patches, h->hp.data(), sizeof(DevPatch) * npatch,
+                     cudaMemcpyHostToDevice, h->stream));
+  CU(cudaMemsetAsync(h->d_status, 0, sizeof(DevStatus), h->stream));
+  CU(cudaStreamSynchronize(h->stream));
+  h->have_hierarchy = true;
+  return BSAM_OK;
+}
+
+static int field_ptr(bsam_gpu* h, int patch, int field, int comp, double** ptr, bool* interior) {
+  const DevPatch& P = h->hp[patch];
+  void* p = nullptr;
+  *interior = false;
+  switch (field) {
+    case BSAM_FIELD_Q: p = P.q[comp]; break;
+    case BSAM_FIELD_QOLD: p = P.qo[comp]; break;
+    case BSAM_FIELD_F: p = P.f[comp]; *interior = true; break;
+    default: return BSAM_ERR_ARG;
+  }
+  *ptr = static_cast<double*>(p);
+  return BSAM_OK;
+}
+
+// Copy between a Fortran array and the pitched device field; dir 0 = H2D.
+static int copy_field(bsam_gpu* h, int patch, int field, double* host, int dir) {
+  if (!h || !h->have_hierarchy) return BSAM_ERR_STATE;
+  if (patch < 0 || patch >= (int)h->hp.size() || !host) return BSAM_ERR_ARG;
+  CU(cudaSetDevice(h->device));
+  const DevPatch& P = h->hp[patch];
+  const int nd = h->rp.ndims;
+  for (int comp = 0; comp < 2; ++comp) {
+    double* dev;
+    bool interior;
+    if (field_ptr(h, patch, field, comp, &dev, &interior)) return BSAM_ERR_ARG;
+    const int g = interior ? 0 : 1;  // ghost layers present in the host array
+    const int e0 = P.n[0] + 2 * g, e1 = P.n[1] + 2 * g, e2 = nd == 3 ? P.n[2] + 2 * g : 1;
+    const size_t hcomp = (size_t)e0 * e1 * e2;
+    double* hbase = host + comp * hcomp;
+    for (int kz = 0; kz < e2; ++kz) {
+      const int k = nd == 3 ? kz + (1 - g) : 0;
+      double* d = dev + (int64_t)(1 - g) + (int64_t)(1 - g) * P.sy + (int64_t)k * P.sz;
+      double* hs = hbase + (size_t)kz * e0 * e1;
+      if (dir == 0)
+        CU(cudaMemcpy2DAsync(d, P.sy * sizeof(double), hs, e0 * sizeof(double),
+                             e0 * sizeof(double), e1, cudaMemcpyHostToDevice, h->stream));
+      else
+        CU(cudaMemcpy2DAsync(hs, e0 * sizeof(double), d, P.sy * sizeof(double),
+                             e0 * sizeof(double), e1, cudaMemcpyDeviceToHost, h->stream));
+    }
+  }
+  CU(cudaStreamSynchronize(h->stream));
+  return BSAM_OK;
+}
+
+int bsam_gpu_put_field(bsam_gpu* h, int patch, int field, const double* a) {
+  return copy_field(h, patch, field, const_cast<double*>(a), 0);
+}
+
+int bsam_gpu_get_field(bsam_gpu* h, int patch, int field, double* out) {
+  return copy_field(h, patch, field, out, 1);
+}
+
+int bsam_gpu_set_ghost(bsam_gpu* h) {
+  if (!h || !h->have_hierarchy) return BSAM_ERR_STATE;
+  CU(cudaSetDevice(h->device));
+  for (int l = h->finestlevel; l >= h->minlevel; --l) ghost_level(h, l);
+  CU(cudaGetLastError());
+  CU(cudaStreamSynchronize(h->stream));
+  return BSAM_OK;
+}
+
+int bsam_gpu_copy_q_to_qold(bsam_gpu* h) {
+  if (!h || !h->have_hierarchy) return BSAM_ERR_STATE;
+  CU(cudaSetDevice(h->device));
+  const int64_t lead = 128 / sizeof(double) - 1;
+  for (size_t p = 0; p < h->hp.size(); ++p) {
+    const DevPatch& P = h->hp[p];
+    for (int c = 0; c < 2; ++c)
+      CU(cudaMemcpyAsync(static_cast<double*>(P.qo[c]) - lead, static_cast<double*>(P.q[c]) - lead,
+                         h->field_elems[p] * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  }
+  return BSAM_OK;
+}
+
+int bsam_gpu_multigrid_iterations(bsam_gpu* h, int* nvcycles, double* residual, int* converged) {
+  if (!h || !h->have_hierarchy) return BSAM_ERR_STATE;
+  CU(cudaSetDevice(h->device));
+  const int nd = h->rp.ndims;
+  const dim3 b = block_dim();
+  // GetSourceFunction + UpdateSourceFunction on levels finest..root
+  // (afas:57-64).  FillDown(source) and FillDown(solution) (afas:47, 66, 73,
+  // 90) only write regions that RestrictSolution / CoarseLoadingFunction
+  // overwrite before any read when the levels are nested uniform grids, so
+  // they are not issued.
+  for (int l = h->finestlevel; l >= 0; --l) {
+    const LevelPlan& L = plan(h, l);
+    if (nd == 2) k_source<double, 2><<<L.nfine, b, 0, h->stream>>>(h->d_patches, L.d_fine);
+    else k_source<double, 3><<<L.nfine, b, 0, h->stream>>>(h->d_patches, L.d_fine);
+    ++h->stats.launches;
+  }
+  const LevelPlan& F = plan(h, h->finestlevel);
+  int64_t ncells = 0;
+  for (int p : F.patches) {
+    int64_t c = 1;
+    for (int n = 0; n < nd; ++n) c *= h->hp[p].n[n];
+    ncells += c;
+  }
+  const double denom = (double)(h->rp.nrvars * ncells);
+  h->trace.clear();
+  int it = 0, conv = 0;
+  double res = 0.0;
+  for (it = 1; it <= h->rp.maxvcycles; ++it) {
+    vcycle(h, h->finestlevel);
+    if (nd == 2)
+      k_resid_norm<double, 2><<<F.nfine, b, 0, h->stream>>>(h->d_patches, F.d_fine, h->d_partials,
+                                                           h->d_status, F.nfine, denom,
+                                                           h->rp.qerrortol);
+    else
+      k_resid_norm<double, 3><<<F.nfine, b, 0, h->stream>>>(h->d_patches, F.d_fine, h->d_partials,
+                                                           h->d_status, F.nfine, denom,
+                                                           h->rp.qerrortol);
+    ++h->stats.launches;
+    CU(cudaGetLastError());
+    CU(cudaMemcpyAsync(h->h_status, h->d_status, sizeof(DevStatus), cudaMemcpyDeviceToHost,
+                       h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    drain_events(h);
+    res = h->h_status->residual;
+    h->trace.push_back(res);
+    if (!std::isfinite(res)) {
+      if (nvcycles) *nvcycles = it;
+      if (residual) *residual = res;
+      if (converged) *converged = 0;
+      return fail(h, BSAM_ERR_DIVERGED, "residual is not finite");
+    }
+    if (res < h->rp.qerrortol) {
+      conv = 1;
+      break;
+    }
+  }
+  if (it > h->rp.maxvcycles) it = h->rp.maxvcycles;
+  if (nvcycles) *nvcycles = it;
+  if (residual) *residual = res;
+  if (converged) *converged = conv;
+  return BSAM_OK;
+}
+
+int bsam_gpu_residual_trace(bsam_gpu* h, double* out, int maxn) {
+  if (!h) return BSAM_ERR_ARG;
+  const int n = std::min<int>(maxn, (int)h->trace.size());
+  for (int i = 0; i < n; ++i) out[i] = h->trace[i];
+  return (int)h->trace.size();
+}
+
+int bsam_gpu_mass(bsam_gpu* h, double* mass) {
+  if (!h || !h->have_hierarchy || !mass) return BSAM_ERR_STATE;
+  CU(cudaSetDevice(h->device));
+  const LevelPlan& R = plan(h, 0);
+  const double hh = h->hp[R.patches[0]].h;
+  const double hd = h->rp.ndims == 2 ? hh * hh : hh * hh * hh;
+  if (h->rp.ndims == 2)
+    k_mass<double, 2><<<R.nfine, block_dim(), 0, h->stream>>>(h->d_patches, R.d_fine,
+                                                             h->d_partials, h->d_status, R.nfine, hd);
+  else
+    k_mass<double, 3><<<R.nfine, block_dim(), 0, h->stream>>>(h->d_patches, R.d_fine,
+                                                             h->d_partials, h->d_status, R.nfine, hd);
+  ++h->stats.launches;
+  CU(cudaGetLastError());
+  CU(cudaMemcpyAsync(h->h_status, h->d_status, sizeof(DevStatus), cudaMemcpyDeviceToHost,
+                     h->stream));
+  CU(cudaStreamSynchronize(h->stream));
+  *mass = h->h_status->mass;
+  return BSAM_OK;
+}
+
+int bsam_gpu_get_stream(bsam_gpu* h, void** stream) {
+  if (!h || !stream) return BSAM_ERR_ARG;
+  *stream = (void*)h->stream;
+  return BSAM_OK;
+}
+
+int bsam_gpu_profile(bsam_gpu* h, int enable) {
+  if (!h) return BSAM_ERR_ARG;
+  if (enable) {
+    h->stats = bsam_gpu_stats{};
+    h->ev_used = 0;
+    if (h->have_hierarchy) {
+      h->ev_cells = 0;
+      for (int p : plan(h, h->finestlevel).patches) {
+        int64_t c = 1;
+        for (int n = 0; n < h->rp.ndims; ++n) c *= h->hp[p].n[n];
+        h->ev_cells += c;
+      }
+    }
+  }
+  h->profiling = enable != 0;
+  return BSAM_OK;
+}
+
+int bsam_gpu_get_stats(bsam_gpu* h, bsam_gpu_stats* out) {
+  if (!h || !out) return BSAM_ERR_ARG;
+  if (h->ev_used) {
+    cudaStreamSynchronize(h->stream);
+    drain_events(h);
+  }
+  *out = h->stats;
+  return BSAM_OK;
+}
+
+int bsam_gpu_destroy(bsam_gpu* h) {
+  if (!h) return BSAM_ERR_ARG;
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  for (auto& e : h->ev_pool) {
+    cudaEventDestroy(e.first);
+    cudaEventDestroy(e.second);
+  }
+  free_hierarchy(h);
+  if (h->d_status) cudaFree(h->d_status);
+  if (h->h_status) cudaFreeHost(h->h_status);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return BSAM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,67 @@
+// bsam_types.h -- device-resident patch table shared by host and kernels.
+//
+// Every grid of the hierarchy (root, below-root multigrid levels, AMR
+// patches, and the patches of many independent problems in a batch) is one
+// DevPatch.  Kernels never loop over levels or problems on the host side of
+// the launch: they take a work list of Items (patch, tile) so that one launch
+// covers every patch of a level -- or of a V-cycle stage across a batch.
+#pragma once
+#include <stdint.h>
+
+namespace bsam {
+
+// Tile of cells one CTA handles: 32 threads x 2 cells in x, TILE_Y rows,
+// one z plane.  Blocks are (32, TILE_Y).
+constexpr int TILE_X = 64;
+constexpr int TILE_Y = 4;
+constexpr int BLOCK_THREADS = 32 * TILE_Y;
+
+// Per-face ghost rule applied by SetBC (boundary.f90:643-891):
+//   BC_NONE    ghost not written by SetBC (internal 999 / periodic 2 faces)
+//   BC_COPY    q(ghost) = q(mirror)            (mthbc 1; UserBC2D faces 3,4)
+//   BC_REFLECT q(ghost) = 2 - q(mirror)        (UserBC2D faces 1,2; UserBC3D)
+enum : int32_t { BC_NONE = 0, BC_COPY = 1, BC_REFLECT = 2 };
+
+enum : int32_t { PREC_F64 = 0, PREC_F32 = 1 };
+
+struct DevPatch {
+  int32_t ndims;
+  int32_t n[3];       // interior cells per dimension (n[2] = 1 in 2D)
+  int32_t cn[3];      // this patch's footprint in its parent: n / 2
+  int32_t off[3];     // mbounds(:,1) - 1: origin of the footprint in the parent
+  int32_t bc[6];      // BC_* per face (x-lo, x-hi, y-lo, y-hi, z-lo, z-hi)
+  int32_t parent;     // patch index of the parent, -1 on the coarsest level
+  int32_t level;
+  int32_t wt;         // 1: every face physical -> kernels write ghosts through
+  int32_t prec;       // PREC_*
+  int32_t problem;    // problem (batch slot) this patch belongs to
+  int32_t pad_;
+  int64_t sy, sz;     // element strides of j and k
+  // Base pointers of element (0,0,0), the low ghost corner, per component.
+  void* q[2];         // solution (phi, mu), with ghost ring
+  void* f[2];         // right-hand side (source / FAS load), interior used
+  void* qs[2];        // snapshot of q after restriction (the children's qc)
+  void* qo[2];        // qold
+  // Problem constants, all computed on the host in FP64 exactly as the
+  // reference does (problem.f90:183-187, 246-248, 472-476).
+  double h, dt, eps2, alpha;
+  double tmp1;        // dt / h^2
+  double tmp2;        // eps2 / h^2
+  double tmp3;        // 2d * eps2 / h^2
+};
+
+struct Item {
+  int32_t patch;
+  int32_t tx, ty, tz;  // tile coordinates
+};
+
+// Device-side status of a solve (one per problem slot).
+struct DevStatus {
+  double sumsq;        // last residual sum of squares
+  double residual;     // sqrt(sumsq / (nrvars * ncells))
+  double mass;
+  uint32_t ticket;     // last-block-done counter of the reductions
+  int32_t converged;
+};
+
+}  // namespace bsam

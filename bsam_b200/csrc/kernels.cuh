@@ -1,0 +1,480 @@
+// kernels.cuh -- FAS V-cycle kernels over the device patch table.
+//
+// One kernel per reference routine on the hot path.  Each launch takes a
+// work list of Items (patch, tile) so that a single launch covers every patch
+// of a level.  A CTA is 32 x TILE_Y threads; every thread owns a pair of
+// adjacent cells in x (one red, one black), which keeps warps on 64
+// contiguous cells of a row (coalesced 8-byte loads).
+//
+// Ghost cells: for patches whose faces are all physical (DevPatch::wt), the
+// kernel that changes a boundary cell also writes the ghost cells SetBC would
+// derive from it (write-through).  This reproduces SetGhost's result exactly:
+// SetBC2D/3D (boundary.f90:661-885) processes the faces in order and copies
+// whole rows including the ghost rows, so a ghost outside in the set S of
+// dimensions ends up as the map of each face in S (ascending dimension) applied
+// to the interior cell reflected across all of S.
+#pragma once
+#include "bsam_types.h"
+#include "problem_ch.cuh"
+
+namespace bsam {
+
+template <class T> __device__ __forceinline__ T* fld(void* p) { return static_cast<T*>(p); }
+
+__device__ __forceinline__ int64_t cidx(const DevPatch& P, int i, int j, int k) {
+  return (int64_t)i + (int64_t)j * P.sy + (int64_t)k * P.sz;
+}
+
+template <class T> __device__ __forceinline__ T bc_map(int code, T v) {
+  return code == BC_REFLECT ? T(2) - v : v;
+}
+
+// Ghost write-through for the cell (i,j,k) of patch P whose new values are
+// (v0, v1).  Only called when the cell may touch the boundary.
+template <class T, int D>
+__device__ void write_through(const DevPatch& P, T* q0, T* q1, int i, int j, int k, T v0,
+                              T v1) {
+  const int co[3] = {i, j, k};
+  int opt[3][3];   // per dimension: own coordinate, lo ghost, hi ghost (-1 absent)
+  int code[3][3];
+  bool any = false;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    opt[d][0] = co[d];
+    opt[d][1] = -1;
+    opt[d][2] = -1;
+    code[d][0] = BC_NONE;
+    code[d][1] = BC_NONE;
+    code[d][2] = BC_NONE;
+    if (d < D) {
+      if (co[d] == 1 && P.bc[2 * d] != BC_NONE) {
+        opt[d][1] = 0;
+        code[d][1] = P.bc[2 * d];
+        any = true;
+      }
+      if (co[d] == P.n[d] && P.bc[2 * d + 1] != BC_NONE) {
+        opt[d][2] = P.n[d] + 1;
+        code[d][2] = P.bc[2 * d + 1];
+        any = true;
+      }
+    }
+  }
+  if (!any) return;
+  const int ncombo = (D == 2) ? 9 : 27;
+  for (int cmb = 1; cmb < ncombo; ++cmb) {
+    int sel[3] = {cmb % 3, (cmb / 3) % 3, (cmb / 9) % 3};
+    bool ok = true;
+    int g[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      g[d] = opt[d][sel[d]];
+      if (g[d] < 0) ok = false;
+    }
+    if (!ok) continue;
+    T a = v0, b = v1;
+#pragma unroll
+    for (int d = 0; d < D; ++d)
+      if (sel[d] != 0) {
+        a = bc_map<T>(code[d][sel[d]], a);
+        b = bc_map<T>(code[d][sel[d]], b);
+      }
+    const int64_t c = cidx(P, g[0], g[1], D == 3 ? g[2] : 0);
+    q0[c] = a;
+    q1[c] = b;
+  }
+}
+
+template <class T, int D>
+__device__ __forceinline__ void load_stencil(const DevPatch& P, const T* __restrict__ q0,
+                                             const T* __restrict__ q1, int64_t c,
+                                             problem::Stencil<T, D>& s) {
+  const int64_t st[3] = {1, P.sy, P.sz};
+  s.pc = q0[c];
+  s.mc = q1[c];
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    s.pm[d] = q0[c - st[d]];
+    s.pp[d] = q0[c + st[d]];
+    s.mm[d] = q1[c - st[d]];
+    s.mp[d] = q1[c + st[d]];
+  }
+}
+
+__device__ __forceinline__ bool near_boundary(const DevPatch& P, int i, int j, int k, int D) {
+  bool b = (i == 1) | (i == P.n[0]) | (j == 1) | (j == P.n[1]);
+  if (D == 3) b = b | (k == 1) | (k == P.n[2]);
+  return b;
+}
+
+// ---------------------------------------------------------------------------
+// RelaxGrid (one colour pass) + SetGhost(level, ipass) for physical faces.
+// color 0 = ipass 1 = cells with even i+j(+k); color 1 = ipass 2.
+template <class T, int D>
+__global__ void __launch_bounds__(BLOCK_THREADS)
+    k_relax(const DevPatch* __restrict__ PT, const Item* __restrict__ items, int color) {
+  const Item it = items[blockIdx.x];
+  const DevPatch& P = PT[it.patch];
+  const int j = it.ty * TILE_Y + threadIdx.y + 1;
+  const int k = (D == 3) ? it.tz + 1 : 0;
+  if (j > P.n[1]) return;
+  const int i0 = (it.tx * 32 + threadIdx.x) * 2 + 1;
+  const int i = i0 + ((i0 + j + k + color) & 1);
+  if (i > P.n[0]) return;
+  T* q0 = fld<T>(P.q[0]);
+  T* q1 = fld<T>(P.q[1]);
+  const T* f0 = fld<T>(P.f[0]);
+  const T* f1 = fld<T>(P.f[1]);
+  const int64_t c = cidx(P, i, j, k);
+  problem::Stencil<T, D> s;
+  load_stencil<T, D>(P, q0, q1, c, s);
+  T phi, mu;
+  problem::RelaxCell<T, D>(s, f0[c], f1[c], T(P.tmp1), T(P.tmp2), T(P.tmp3), T(P.alpha), phi,
+                           mu);
+  q0[c] = phi;
+  q1[c] = mu;
+  if (P.wt && near_boundary(P, i, j, k, D)) write_through<T, D>(P, q0, q1, i, j, k, phi, mu);
+}
+
+// Residual rf = f - Operator(q) at one cell (afas:799-840).
+template <class T, int D>
+__device__ __forceinline__ void residual_cell(const DevPatch& P, const T* q0, const T* q1,
+                                              const T* f0, const T* f1, int64_t c, T& r0,
+                                              T& r1) {
+  problem::Stencil<T, D> s;
+  load_stencil<T, D>(P, q0, q1, c, s);
+  T o0, o1;
+  problem::OperatorCell<T, D>(s, T(P.tmp1), T(P.tmp2), T(P.alpha), o0, o1);
+  r0 = f0[c] - o0;
+  r1 = f1[c] - o1;
+}
+
+// Deterministic block sum of a double (fixed shuffle tree + fixed smem order).
+__device__ __forceinline__ double block_sum(double v) {
+  __shared__ double red[BLOCK_THREADS / 32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x, warp = threadIdx.y;
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  double s = 0.0;
+  if (warp == 0 && lane == 0) {
+    for (int w = 0; w < BLOCK_THREADS / 32; ++w) s += red[w];
+  }
+  __syncthreads();
+  return s;  // valid in thread (0,0)
+}
+
+// Second stage of a two-stage reduction: the last CTA to finish sums the
+// per-CTA partials in index order.  Returns true in thread (0,0) of that CTA
+// with the total in `total`.
+__device__ __forceinline__ bool last_block_total(double mine, double* partials,
+                                                 uint32_t* ticket, int nblocks,
+                                                 double& total) {
+  __shared__ bool is_last;
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    partials[blockIdx.x] = mine;
+    __threadfence();
+    const uint32_t t = atomicAdd(ticket, 1u);
+    is_last = (t == (uint32_t)nblocks - 1u);
+  }
+  __syncthreads();
+  if (!is_last) return false;
+  __threadfence();
+  const int tid = threadIdx.y * 32 + threadIdx.x;
+  double s = 0.0;
+  for (int b = tid; b < nblocks; b += BLOCK_THREADS) s += ((volatile double*)partials)[b];
+  const double tot = block_sum(s);
+  if (tid == 0) {
+    total = tot;
+    *ticket = 0u;
+    return true;
+  }
+  return false;
+}
+
+// ErrorAFAS / L2Error / SquareSum (afas:108-221), errortype 1:
+// residual = sqrt(sum rf^2 / (nrvars * ncells)) over the finest level.
+template <class T, int D>
+__global__ void __launch_bounds__(BLOCK_THREADS)
+    k_resid_norm(const DevPatch* __restrict__ PT, const Item* __restrict__ items,
+                 double* __restrict__ partials, DevStatus* __restrict__ st, int nitems,
+                 double denom, double tol) {
+  const Item it = items[blockIdx.x];
+  const DevPatch& P = PT[it.patch];
+  const int j = it.ty * TILE_Y + threadIdx.y + 1;
+  const int k = (D == 3) ? it.tz + 1 : 0;
+  const int i0 = (it.tx * 32 + threadIdx.x) * 2 + 1;
+  const T* q0 = fld<T>(P.q[0]);
+  const T* q1 = fld<T>(P.q[1]);
+  const T* f0 = fld<T>(P.f[0]);
+  const T* f1 = fld<T>(P.f[1]);
+  double acc = 0.0;
+  if (j <= P.n[1]) {
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+      const int i = i0 + t;
+      if (i <= P.n[0]) {
+        T r0, r1;
+        residual_cell<T, D>(P, q0, q1, f0, f1, cidx(P, i, j, k), r0, r1);
+        acc += (double)r0 * (double)r0 + (double)r1 * (double)r1;
+      }
+    }
+  }
+  const double bs = block_sum(acc);
+  double total;
+  if (last_block_total(bs, partials, &st->ticket, nitems, total)) {
+    const double r = sqrt(total / denom);
+    st->sumsq = total;
+    st->residual = r;
+    st->converged = (r < tol) ? 1 : 0;
+  }
+}
+
+// RestrictSolution (afas:600-644) + the parent's SetGhost(level-1, 0) for
+// physical faces + GetCoarseGhostPoints (boundary.f90:1203-1269): the parent
+// solution and its snapshot qs (the children's qc) are both written.
+template <class T, int D>
+__global__ void __launch_bounds__(BLOCK_THREADS)
+    k_restrict(const DevPatch* __restrict__ PT, const Item* __restrict__ items) {
+  const Item it = items[blockIdx.x];
+  const DevPatch& C = PT[it.patch];
+  const DevPatch& P = PT[C.parent];
+  const int jc = it.ty * TILE_Y + threadIdx.y + 1;
+  const int kc = (D == 3) ? it.tz + 1 : 0;
+  if (jc > C.cn[1]) return;
+  const int ic0 = (it.tx * 32 + threadIdx.x) * 2 + 1;
+#pragma unroll
+  for (int t = 0; t < 2; ++t) {
+    const int ic = ic0 + t;
+    if (ic > C.cn[0]) break;
+    const int i = 2 * ic, j = 2 * jc, k = 2 * kc;
+    T val[2];
+#pragma unroll
+    for (int v = 0; v < 2; ++v) {
+      const T* a = fld<T>(C.q[v]);
+      if (D == 2) {
+        val[v] = T(0.25) * (a[cidx(C, i, j, 0)] + a[cidx(C, i - 1, j, 0)] +
+                            a[cidx(C, i, j - 1, 0)] + a[cidx(C, i - 1, j - 1, 0)]);
+      } else {
+        val[v] = T(0.125) * (a[cidx(C, i, j, k)] + a[cidx(C, i - 1, j, k)] +
+                             a[cidx(C, i, j - 1, k)] + a[cidx(C, i - 1, j - 1, k)] +
+                             a[cidx(C, i, j, k - 1)] + a[cidx(C, i - 1, j, k - 1)] +
+                             a[cidx(C, i, j - 1, k - 1)] + a[cidx(C, i - 1, j - 1, k - 1)]);
+      }
+    }
+    const int pi = C.off[0] + ic, pj = C.off[1] + jc, pk = (D == 3) ? C.off[2] + kc : 0;
+    const int64_t pc = cidx(P, pi, pj, pk);
+    T* pq0 = fld<T>(P.q[0]);
+    T* pq1 = fld<T>(P.q[1]);
+    T* ps0 = fld<T>(P.qs[0]);
+    T* ps1 = fld<T>(P.qs[1]);
+    pq0[pc] = val[0];
+    pq1[pc] = val[1];
+    ps0[pc] = val[0];
+    ps1[pc] = val[1];
+    if (P.wt && near_boundary(P, pi, pj, pk, D)) {
+      write_through<T, D>(P, pq0, pq1, pi, pj, pk, val[0], val[1]);
+      write_through<T, D>(P, ps0, ps1, pi, pj, pk, val[0], val[1]);
+    }
+  }
+}
+
+// CoarseLoadingFunction (afas:646-714):
+//   parent%f(mb) = Restriction(f - Operator(q)) + Operator(qc, h = parent%dx)
+template <class T, int D>
+__global__ void __launch_bounds__(BLOCK_THREADS)
+    k_coarse_load(const DevPatch* __restrict__ PT, const Item* __restrict__ items) {
+  const Item it = items[blockIdx.x];
+  const DevPatch& C = PT[it.patch];
+  const DevPatch& P = PT[C.parent];
+  const int jc = it.ty * TILE_Y + threadIdx.y + 1;
+  const int kc = (D == 3) ? it.tz + 1 : 0;
+  if (jc > C.cn[1]) return;
+  const int ic0 = (it.tx * 32 + threadIdx.x) * 2 + 1;
+  const T* q0 = fld<T>(C.q[0]);
+  const T* q1 = fld<T>(C.q[1]);
+  const T* f0 = fld<T>(C.f[0]);
+  const T* f1 = fld<T>(C.f[1]);
+#pragma unroll
+  for (int t = 0; t < 2; ++t) {
+    const int ic = ic0 + t;
+    if (ic > C.cn[0]) break;
+    const int i = 2 * ic, j = 2 * jc, k = 2 * kc;
+    // Restriction of rf: children in the reference's summation order.
+    const int nch = (D == 2) ? 4 : 8;
+    T s0 = T(0), s1 = T(0);
+#pragma unroll
+    for (int ch = 0; ch < nch; ++ch) {
+      const int ii = i - (ch & 1), jj = j - ((ch >> 1) & 1), kk = (D == 3) ? k - (ch >> 2) : 0;
+      T r0, r1;
+      residual_cell<T, D>(C, q0, q1, f0, f1, cidx(C, ii, jj, kk), r0, r1);
+      if (ch == 0) {
+        s0 = r0;
+        s1 = r1;
+      } else {
+        s0 = s0 + r0;
+        s1 = s1 + r1;
+      }
+    }
+    const T w = (D == 2) ? T(0.25) : T(0.125);
+    const T R0 = w * s0, R1 = w * s1;
+    const int pi = C.off[0] + ic, pj = C.off[1] + jc, pk = (D == 3) ? C.off[2] + kc : 0;
+    const int64_t pc = cidx(P, pi, pj, pk);
+    problem::Stencil<T, D> s;
+    load_stencil<T, D>(P, fld<T>(P.qs[0]), fld<T>(P.qs[1]), pc, s);
+    T o0, o1;
+    problem::OperatorCell<T, D>(s, T(P.tmp1), T(P.tmp2), T(P.alpha), o0, o1);
+    fld<T>(P.f[0])[pc] = R0 + o0;
+    fld<T>(P.f[1])[pc] = R1 + o1;
+  }
+}
+
+// CorrectFine with BiLin/TriLinProlongationP1 (afas:842-963,
+// gridutilities.f90:137-175, 474-529): q += P(parent%q - qc) on the
+// interior; the ghost ring is refreshed by write-through (the reference's
+// SetGhost(level, 0) overwrites the prolongated ring, afas:515).
+template <class T>
+__device__ __forceinline__ T lin_x(bool even, T a, T b) {
+  return even ? T(3) * a + b : a + T(3) * b;
+}
+
+template <class T, int D>
+__global__ void __launch_bounds__(BLOCK_THREADS)
+    k_correct(const DevPatch* __restrict__ PT, const Item* __restrict__ items) {
+  const Item it = items[blockIdx.x];
+  const DevPatch& C = PT[it.patch];
+  const DevPatch& P = PT[C.parent];
+  const int J = it.ty * TILE_Y + threadIdx.y + 1;
+  const int K = (D == 3) ? it.tz + 1 : 0;
+  if (J > C.n[1]) return;
+  const int I0 = (it.tx * 32 + threadIdx.x) * 2 + 1;
+  const T* pq0 = fld<T>(P.q[0]);
+  const T* pq1 = fld<T>(P.q[1]);
+  const T* ps0 = fld<T>(P.qs[0]);
+  const T* ps1 = fld<T>(P.qs[1]);
+  T* q0 = fld<T>(C.q[0]);
+  T* q1 = fld<T>(C.q[1]);
+#pragma unroll
+  for (int t = 0; t < 2; ++t) {
+    const int I = I0 + t;
+    if (I > C.n[0]) break;
+    const int m = I >> 1, n = J >> 1, p = K >> 1;
+    const bool ex = (I & 1) == 0, ey = (J & 1) == 0, ez = (K & 1) == 0;
+    T corr[2];
+#pragma unroll
+    for (int v = 0; v < 2; ++v) {
+      const T* pq = v ? pq1 : pq0;
+      const T* ps = v ? ps1 : ps0;
+      auto e = [&](int a, int b, int c) -> T {
+        const int64_t x = cidx(P, C.off[0] + a, C.off[1] + b, D == 3 ? C.off[2] + c : 0);
+        return pq[x] - ps[x];
+      };
+      if (D == 2) {
+        const T b0 = lin_x<T>(ex, e(m, n, 0), e(m + 1, n, 0));
+        const T b1 = lin_x<T>(ex, e(m, n + 1, 0), e(m + 1, n + 1, 0));
+        corr[v] = lin_x<T>(ey, b0, b1) / T(16);
+      } else {
+        const T b00 = lin_x<T>(ex, e(m, n, p), e(m + 1, n, p));
+        const T b10 = lin_x<T>(ex, e(m, n + 1, p), e(m + 1, n + 1, p));
+        const T b01 = lin_x<T>(ex, e(m, n, p + 1), e(m + 1, n, p + 1));
+        const T b11 = lin_x<T>(ex, e(m, n + 1, p + 1), e(m + 1, n + 1, p + 1));
+        const T c0 = lin_x<T>(ey, b00, b10);
+        const T c1 = lin_x<T>(ey, b01, b11);
+        corr[v] = lin_x<T>(ez, c0, c1) / T(64);
+      }
+    }
+    const int64_t c = cidx(C, I, J, K);
+    const T a0 = q0[c] + corr[0];
+    const T a1 = q1[c] + corr[1];
+    q0[c] = a0;
+    q1[c] = a1;
+    if (C.wt && near_boundary(C, I, J, K, D)) write_through<T, D>(C, q0, q1, I, J, K, a0, a1);
+  }
+}
+
+// GetSourceFunction + UpdateSourceFunction on one level (afas:312-367,
+// 427-486): f = Source(qold) + 0.
+template <class T, int D>
+__global__ void __launch_bounds__(BLOCK_THREADS)
+    k_source(const DevPatch* __restrict__ PT, const Item* __restrict__ items) {
+  const Item it = items[blockIdx.x];
+  const DevPatch& P = PT[it.patch];
+  const int j = it.ty * TILE_Y + threadIdx.y + 1;
+  const int k = (D == 3) ? it.tz + 1 : 0;
+  if (j > P.n[1]) return;
+  const int i0 = (it.tx * 32 + threadIdx.x) * 2 + 1;
+  const T* qo = fld<T>(P.qo[0]);
+  T* f0 = fld<T>(P.f[0]);
+  T* f1 = fld<T>(P.f[1]);
+#pragma unroll
+  for (int t = 0; t < 2; ++t) {
+    const int i = i0 + t;
+    if (i > P.n[0]) break;
+    const int64_t c = cidx(P, i, j, k);
+    T a, b;
+    problem::SourceCell<T>(qo[c], T(P.alpha), a, b);
+    f0[c] = a;
+    f1[c] = b;
+  }
+}
+
+// SetBC (boundary.f90:598-891) for one patch, all ghost cells, any face
+// codes: a ghost is written when at least one of the dimensions it lies
+// outside of has a physical face; its value is the face maps of those
+// dimensions (ascending) applied to the cell reflected across them.
+template <class T, int D>
+__global__ void k_setbc(const DevPatch* __restrict__ PT, int patch, int64_t ntotal) {
+  const DevPatch& P = PT[patch];
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= ntotal) return;
+  const int e0 = P.n[0] + 2, e1 = P.n[1] + 2;
+  int co[3] = {(int)(g % e0), (int)((g / e0) % e1), D == 3 ? (int)(g / ((int64_t)e0 * e1)) : 0};
+  int src[3] = {co[0], co[1], co[2]};
+  int codes[3] = {BC_NONE, BC_NONE, BC_NONE};
+  bool write = false;
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    if (co[d] == 0 && P.bc[2 * d] != BC_NONE) {
+      src[d] = 1;
+      codes[d] = P.bc[2 * d];
+      write = true;
+    } else if (co[d] == P.n[d] + 1 && P.bc[2 * d + 1] != BC_NONE) {
+      src[d] = P.n[d];
+      codes[d] = P.bc[2 * d + 1];
+      write = true;
+    }
+  }
+  if (!write) return;
+#pragma unroll
+  for (int v = 0; v < 2; ++v) {
+    T* q = fld<T>(P.q[v]);
+    T val = q[cidx(P, src[0], src[1], src[2])];
+#pragma unroll
+    for (int d = 0; d < D; ++d)
+      if (codes[d] != BC_NONE) val = bc_map<T>(codes[d], val);
+    q[cidx(P, co[0], co[1], co[2])] = val;
+  }
+}
+
+// h^d * sum(phi) over a patch interior (AfterStep2D/3D integral(1)).
+template <class T, int D>
+__global__ void __launch_bounds__(BLOCK_THREADS)
+    k_mass(const DevPatch* __restrict__ PT, const Item* __restrict__ items,
+           double* __restrict__ partials, DevStatus* __restrict__ st, int nitems, double hd) {
+  const Item it = items[blockIdx.x];
+  const DevPatch& P = PT[it.patch];
+  const int j = it.ty * TILE_Y + threadIdx.y + 1;
+  const int k = (D == 3) ? it.tz + 1 : 0;
+  const int i0 = (it.tx * 32 + threadIdx.x) * 2 + 1;
+  const T* q0 = fld<T>(P.q[0]);
+  double acc = 0.0;
+  if (j <= P.n[1]) {
+    if (i0 <= P.n[0]) acc += (double)q0[cidx(P, i0, j, k)];
+    if (i0 + 1 <= P.n[0]) acc += (double)q0[cidx(P, i0 + 1, j, k)];
+  }
+  const double bs = block_sum(acc);
+  double total;
+  if (last_block_total(bs, partials, &st->ticket, nitems, total)) st->mass = hd * total;
+}
+
+}  // namespace bsam

@@ -1,0 +1,112 @@
+// problem_ch.cuh -- device twins of the simple_cahn-hilliard problem module.
+//
+// The reference's plugin API is the Fortran module `Problem`
+// (problems/simple_cahn-hilliard/problem.f90), whose routines the multigrid
+// library calls by fixed names (lib/afasroutines.f90:318,434,556,653,801;
+// lib/boundary.f90:645,748).  This header holds __device__ functions with the
+// same names and formulas, evaluated per cell from its stencil neighbourhood.
+// Operation order follows the Fortran expressions left to right so that FP64
+// results match the reference arithmetic bit for bit (the library is built
+// with --fmad=false, so no multiply-add is contracted).
+#pragma once
+
+namespace bsam {
+namespace problem {
+
+// Mob, Dfe, Dfc, D2fc (problem.f90:760-813).
+template <class T> __device__ __forceinline__ T Mob(T) { return T(1); }
+template <class T> __device__ __forceinline__ T Dfe(T c, T alpha) {
+  return (c - T(0.5)) * alpha / T(4);
+}
+template <class T> __device__ __forceinline__ T Dfc(T c, T alpha) {
+  T cmh = c - T(0.5);
+  return cmh * cmh * cmh * alpha;
+}
+template <class T> __device__ __forceinline__ T D2fc(T c, T alpha) {
+  T cmh = c - T(0.5);
+  return T(3) * cmh * cmh * alpha;
+}
+
+// Neighbourhood of one cell: centre values and the -/+ neighbours per
+// dimension, for both components (phi = q(:,:,1), mu = q(:,:,2)).
+template <class T, int D> struct Stencil {
+  T pc, mc;        // phi, mu at the cell
+  T pm[D], pp[D];  // phi at i-1 / i+1 (per dimension)
+  T mm[D], mp[D];  // mu  at i-1 / i+1
+};
+
+// One cell of RelaxGrid2D / RelaxGrid3D (problem.f90:192-213, 485-516): the
+// per-cell 2x2 Newton update of (phi, mu) solved by Cramer's rule.
+// tmp1 = dt/h^2, tmp2 = eps2/h^2, tmp3 = 2d*eps2/h^2.
+template <class T, int D>
+__device__ __forceinline__ void RelaxCell(const Stencil<T, D>& s, T f0, T f1, T tmp1, T tmp2,
+                                          T tmp3, T alpha, T& phi, T& mu) {
+  T m[2 * D];
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    m[2 * d] = Mob(T(0.5) * (s.pm[d] + s.pc));
+    m[2 * d + 1] = Mob(T(0.5) * (s.pp[d] + s.pc));
+  }
+  T msum = m[0];
+#pragma unroll
+  for (int t = 1; t < 2 * D; ++t) msum = msum + m[t];
+  const T a12 = tmp1 * msum;
+  const T a21 = -D2fc(s.pc, alpha) - tmp3;
+  // b(1): f + tmp1*(m1*mu(i-1) + m2*mu(i+1) + m3*mu(j-1) + m4*mu(j+1) ...)
+  T smu = m[0] * s.mm[0] + m[1] * s.mp[0];
+#pragma unroll
+  for (int d = 1; d < D; ++d) {
+    smu = smu + m[2 * d] * s.mm[d];
+    smu = smu + m[2 * d + 1] * s.mp[d];
+  }
+  const T b1 = f0 + tmp1 * smu;
+  // b(2): f + Dfc - D2fc*phi - tmp2*(phi(i+1) + phi(i-1) + phi(j+1) + ...)
+  T sph = s.pp[0] + s.pm[0];
+#pragma unroll
+  for (int d = 1; d < D; ++d) {
+    sph = sph + s.pp[d];
+    sph = sph + s.pm[d];
+  }
+  const T b2 = f1 + Dfc(s.pc, alpha) - D2fc(s.pc, alpha) * s.pc - tmp2 * sph;
+  const T det = T(1) - a12 * a21;
+  phi = (b1 - a12 * b2) / det;
+  mu = (b2 - a21 * b1) / det;
+}
+
+// One cell of Operator2D / Operator3D (problem.f90:250-256, 554-560) with
+// ULapMob (304-329, 607-642), UDiv and ULap (gridutilities.f90:42-87,
+// 345-404):
+//   res1 = phi - tmp1 * UDiv(Mob * grad mu)
+//   res2 = mu - Dfc(phi) + tmp2 * ULap(phi)
+template <class T, int D>
+__device__ __forceinline__ void OperatorCell(const Stencil<T, D>& s, T tmp1, T tmp2, T alpha,
+                                             T& r0, T& r1) {
+  T udiv = Mob(T(0.5) * (s.pp[0] + s.pc)) * (s.mp[0] - s.mc) -
+           Mob(T(0.5) * (s.pc + s.pm[0])) * (s.mc - s.mm[0]);
+#pragma unroll
+  for (int d = 1; d < D; ++d) {
+    udiv = udiv + Mob(T(0.5) * (s.pp[d] + s.pc)) * (s.mp[d] - s.mc);
+    udiv = udiv - Mob(T(0.5) * (s.pc + s.pm[d])) * (s.mc - s.mm[d]);
+  }
+  r0 = s.pc - tmp1 * udiv;
+  T lap = s.pp[0] + s.pm[0];
+#pragma unroll
+  for (int d = 1; d < D; ++d) {
+    lap = lap + s.pp[d];
+    lap = lap + s.pm[d];
+  }
+  lap = lap - T(2 * D) * s.pc;
+  r1 = s.mc - Dfc(s.pc, alpha) + tmp2 * lap;
+}
+
+// Source2D/3D followed by UpdateSourceFunction (problem.f90:278-279,
+// 281-303; lib/afasroutines.f90:467-472): f = Source(qold) + SourceUpdate,
+// with SourceUpdate = 0 for this problem.
+template <class T>
+__device__ __forceinline__ void SourceCell(T qold_phi, T alpha, T& f0, T& f1) {
+  f0 = qold_phi + T(0);
+  f1 = -Dfe(qold_phi, alpha) + T(0);
+}
+
+}  // namespace problem
+}  // namespace bsam

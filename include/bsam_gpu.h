@@ -1,0 +1,144 @@
+/*
+ * bsam_gpu.h -- C ABI of the B200-native FAS multigrid V-cycle for the BSAM
+ * simple_cahn-hilliard problem module.
+ *
+ * Plain C types only (no CUDA or torch types), callable from Fortran through
+ * iso_c_binding (bind(C)) or from C/C++/Python ctypes.  Every call returns an
+ * int status: 0 = BSAM_OK (matches err_OK = 0, lib/treeops.f90:66), negative
+ * values are errors; bsam_gpu_strerror() names them.  The library never exits
+ * or stops the process.
+ *
+ * Array arguments use the reference's Fortran layout: column-major, i fastest,
+ * with the patch's ghost ring for q/qold, q(0:mx1+1, 0:mx2+1[, 0:mx3+1], 1:2)
+ * (lib/bsamstorage.f90:74-102), and interior-only f(1:mx1, 1:mx2[, 1:mx3], 1:2).
+ * Arrays are copied during the call and never retained.
+ */
+#ifndef BSAM_GPU_H
+#define BSAM_GPU_H
+#include <stddef.h>
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  BSAM_OK = 0,
+  BSAM_ERR_ARG = -1,        /* invalid argument or parameter */
+  BSAM_ERR_CUDA = -2,       /* a CUDA runtime call failed */
+  BSAM_ERR_NOMEM = -3,      /* device allocation failed */
+  BSAM_ERR_STATE = -4,      /* call out of order (e.g. no hierarchy yet) */
+  BSAM_ERR_UNSUPPORTED = -5,/* configuration not supported by this build */
+  BSAM_ERR_NODEVICE = -6,   /* no CUDA device / kernels unavailable */
+  BSAM_ERR_DIVERGED = -7    /* non-finite residual detected */
+};
+
+/* Field selectors for put/get (the nodeinfo components of
+ * lib/nodeinfodef.f90:204-215 that the hot path reads or writes). */
+enum { BSAM_FIELD_Q = 0, BSAM_FIELD_QOLD = 1, BSAM_FIELD_F = 2 };
+
+/* Precision of the solve. */
+enum { BSAM_PREC_FP64 = 0, BSAM_PREC_MIXED = 1 };
+
+typedef struct bsam_gpu bsam_gpu; /* opaque handle: one per host thread */
+
+/* Run parameters: the &rundata / &problemdata values the hot path reads
+ * (lib/bsamroutines.f90:68-100; problems/simple_cahn-hilliard/problem.f90:17,
+ * problemdef.f90:4).  nrvars must be 2, mbc 1, maux 0, errortype 1. */
+typedef struct {
+  int32_t ndims, nrvars, mbc, maux;
+  int32_t nsmoothingpasses, maxvcycles, errortype, precision;
+  double dt, qerrortol, alpha, eps;
+} bsam_run_params;
+
+/* One patch of the hierarchy: the nodeinfo geometry (lib/nodeinfodef.f90:
+ * 172-207).  Indices follow the Fortran conventions (1-based boxes).
+ * parent: index of the parent in the patch array, -1 for the coarsest level.
+ * mbounds: this patch's index box in its parent (lib/treeops via
+ * InitSeed/MakeNewGrid).  mthbc per face: 1 Neumann reflection, 10-99 the
+ * problem's UserBC, 999 internal (coarse-fine).  dx is the grid spacing. */
+typedef struct {
+  int32_t level, parent;
+  int32_t mx[3];
+  int32_t mbounds[3][2];
+  int32_t mglobal[3][2];
+  int32_t mthbc[6];
+  double dx;
+  double xlower[3];
+} bsam_patch_desc;
+
+/* Replaces nothing in the reference: creates the device context on CUDA
+ * device `device` (one stream per handle). */
+int bsam_gpu_create(bsam_gpu** h, int device, const bsam_run_params* p);
+
+/* Replaces the tree set-up that makes the hierarchy reachable to
+ * MultigridIterations: RootInit/InitSeed/AllocFields
+ * (lib/bsamroutines.f90:205-494, lib/bsamstorage.f90:46-123).  patches[] is in
+ * ApplyOnLevel order within each level (lib/treeops.f90:536-572).  Device
+ * fields are allocated and zeroed (AllocFields sets q = qold = 0). */
+int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patches,
+                           int finestlevel);
+
+/* Copy a host field of one patch to the device (BSAM_FIELD_Q/QOLD: array with
+ * ghost ring; BSAM_FIELD_F: interior only). */
+int bsam_gpu_put_field(bsam_gpu* h, int patch, int field, const double* a);
+
+/* Copy a device field of one patch back to the host, same layouts. */
+int bsam_gpu_get_field(bsam_gpu* h, int patch, int field, double* out);
+
+/* SetGhost(level, 0) (lib/boundary.f90:58-89) on every level, as BSAMSolver
+ * does after QInit (lib/bsamroutines.f90:144). */
+int bsam_gpu_set_ghost(bsam_gpu* h);
+
+/* CopyQToQold on all levels (lib/bsamroutines.f90:568-580, 659-661). */
+int bsam_gpu_copy_q_to_qold(bsam_gpu* h);
+
+/* Replaces MultigridIterations (lib/afasroutines.f90:38-106): source set-up
+ * followed by up to maxvcycles FAS V(nu,nu) cycles until the finest-level
+ * residual (ErrorAFAS, errortype 1) drops below qerrortol.
+ *   nvcycles  V-cycles performed
+ *   residual  last residual
+ *   converged 1 if residual < qerrortol (reference: lconverged), else 0
+ * Non-convergence is not an error, as in the reference. */
+int bsam_gpu_multigrid_iterations(bsam_gpu* h, int* nvcycles, double* residual,
+                                  int* converged);
+
+/* Residuals of each V-cycle of the last multigrid_iterations call (the
+ * reference prints them, lib/afasroutines.f90:95).  Returns the count. */
+int bsam_gpu_residual_trace(bsam_gpu* h, double* out, int maxn);
+
+/* FP64 mass h^d * sum(phi) over the root level: AfterStep2D/3D integral(1)
+ * (problems/simple_cahn-hilliard/problem.f90:121-122, 416-418). */
+int bsam_gpu_mass(bsam_gpu* h, double* mass);
+
+/* The CUDA stream (cudaStream_t) every kernel of this handle runs on, for
+ * callers that order their own work or record events against it. */
+int bsam_gpu_get_stream(bsam_gpu* h, void** stream);
+
+/* Instrumentation counters since the last bsam_gpu_profile(h, 1) call. */
+typedef struct {
+  int64_t launches;       /* kernels launched by the library */
+  int64_t smooth_stages;  /* timed finest-level smoothing stages (nu sweeps) */
+  int64_t smooth_cells;   /* cells per timed stage, summed over stages */
+  double smooth_ms;       /* CUDA-event time of those stages */
+  double smooth_bytes;    /* algorithmic bytes: 6 * sizeof(value) per cell */
+} bsam_gpu_stats;
+
+/* enable = 1: reset the counters and time every finest-level smoothing stage
+ * with CUDA events on the handle's stream; 0: stop timing (counters kept). */
+int bsam_gpu_profile(bsam_gpu* h, int enable);
+int bsam_gpu_get_stats(bsam_gpu* h, bsam_gpu_stats* out);
+
+/* Release the handle and its device memory. */
+int bsam_gpu_destroy(bsam_gpu* h);
+
+/* Name of a status code (static string). */
+const char* bsam_gpu_strerror(int code);
+
+/* Detail message of the last failing call on this handle (valid until the
+ * next call on the handle). */
+const char* bsam_gpu_last_error(bsam_gpu* h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

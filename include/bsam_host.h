@@ -1,0 +1,49 @@
+/*
+ * bsam_host.h -- host driver above the C ABI (bsam_gpu.h).
+ *
+ * Restates, in C++, the part of the reference's Fortran driver that sets up a
+ * uniform root grid with its below-root multigrid levels and advances it in
+ * time, calling the C ABI where the Fortran calls MultigridIterations.  A
+ * Fortran host would make the same calls through iso_c_binding.
+ */
+#ifndef BSAM_HOST_H
+#define BSAM_HOST_H
+#include <stdint.h>
+#include "bsam_gpu.h"
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* The &griddata values of a single uniform root grid
+ * (lib/bsamroutines.f90:219-244; maxlevel = 0). */
+typedef struct {
+  int32_t ndims;
+  int32_t mx[3];
+  int32_t mthbc[6];
+  int32_t minlevel;  /* <= 0, or 1 for the automatic choice */
+  int32_t pad_;
+  double xlower[3], xupper[3];
+} bsam_host_grid;
+
+/* Number of levels (root + below-root) the grid gets. */
+int bsam_host_levels(const bsam_host_grid* g);
+
+/* Replaces RootInit + CreateBelowSeedLevels + InitSeed
+ * (lib/bsamroutines.f90:205-494, lib/treeops.f90:193-289): fills out[0] with
+ * the root and out[l] with level -l, ready for bsam_gpu_set_hierarchy. */
+int bsam_host_build_uniform(const bsam_host_grid* g, bsam_patch_desc* out, int maxn,
+                            int* npatch);
+
+/* Replaces the time-step loop of TakeTimeSteps for maxlevel = 0, eqfn = 1
+ * (lib/bsamroutines.f90:632-762): per step SetGhost(root,0), CopyQToQold,
+ * MultigridIterations.  Optional outputs per step (NULL to skip): root q with
+ * ghost ring at q_steps + step*q_stride, V-cycle count, final residual,
+ * convergence flag, FP64 mass. */
+int bsam_host_take_time_steps(bsam_gpu* h, int nsteps, int root_patch, double* q_steps,
+                              int64_t q_stride, int* nvcycles, double* residuals,
+                              int* converged, double* mass);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

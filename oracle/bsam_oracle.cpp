@@ -1,0 +1,925 @@
+// bsam_oracle.cpp -- CPU oracle for the BSAM FAS V-cycle (TEST INFRASTRUCTURE).
+//
+// A plain C++ restatement of the reference Fortran hot path for the
+// simple_cahn-hilliard problem module.  Only tests/, __graft_entry__.smoke()
+// and bench.py's cpu_baseline leg load this file's library; the product path
+// (bsam_b200/, include/) never does.
+//
+// Parity pinning: UNPINNED against reference outputs.  The reference is
+// Fortran 90 with no compiler in this image and ships no tests or golden
+// vectors; the restatement is checked by known-answer tests and invariants
+// derived from the reference's formulas (tests/test_oracle.py).
+//
+// Faithfulness rules followed throughout:
+//  * every array statement evaluates its whole right-hand side before the
+//    assignment (Fortran array semantics);
+//  * expressions are evaluated left to right exactly as written in the
+//    reference (no reassociation; build with -ffp-contract=off);
+//  * reductions (sum) run sequentially in column-major order;
+//  * statement order of the reference routines is kept, including the
+//    numerically dead FillDown / UpdateSourceFunction passes.
+#include "bsam_oracle.h"
+
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+namespace {
+
+// Fortran-style array with arbitrary lower bounds, up to 4 dimensions,
+// column-major (first index fastest).
+struct FArr {
+  int lo[4] = {0, 0, 0, 0};
+  int n[4] = {0, 0, 0, 0};
+  long st[4] = {0, 0, 0, 0};
+  std::vector<double> d;
+  void alloc(int l0, int h0, int l1, int h1, int l2, int h2, int l3, int h3,
+             double v = 0.0) {
+    int l[4] = {l0, l1, l2, l3}, h[4] = {h0, h1, h2, h3};
+    long s = 1;
+    for (int a = 0; a < 4; ++a) {
+      lo[a] = l[a];
+      n[a] = h[a] - l[a] + 1;
+      if (n[a] < 0) n[a] = 0;
+      st[a] = s;
+      s *= n[a];
+    }
+    d.assign((size_t)s, v);
+  }
+  inline long idx(int i, int j, int k, int v) const {
+    return (long)(i - lo[0]) + st[1] * (j - lo[1]) + st[2] * (k - lo[2]) +
+           st[3] * (v - lo[3]);
+  }
+  inline double& operator()(int i, int j, int k, int v) { return d[idx(i, j, k, v)]; }
+  inline double operator()(int i, int j, int k, int v) const { return d[idx(i, j, k, v)]; }
+  int hi(int a) const { return lo[a] + n[a] - 1; }
+};
+
+// The nodeinfo patch record (lib/nodeinfodef.f90:124-219), reduced to the
+// components the hot path touches.
+struct Patch {
+  int level = 0, nrvars = 2, mbc = 1, maux = 0;
+  int mx[3] = {1, 1, 1};
+  int mbounds[3][2] = {{1, 1}, {1, 1}, {1, 1}};
+  int mglobal[3][2] = {{1, 1}, {1, 1}, {1, 1}};
+  int mthbc[6] = {1, 1, 1, 1, 1, 1};
+  double dx[3] = {0, 0, 0}, xlower[3] = {0, 0, 0};
+  bool tobedeleted = false;
+  Patch* parent = nullptr;
+  FArr q, qold, qc, f, rf, ftmp;
+};
+
+// Module state of NodeInfoDef / ProblemDef used on the hot path.
+struct Ctx {
+  int ndims = 2;
+  double dt = 0, qerrortol = 1e-6, alpha = 1, eps = 0, eps2 = 0;
+  int maxvcycles = 20, nsmoothingpasses = 2, errortype = 1;
+  int minlevel = 0, finestlevel = 0;
+  static const int rootlevel = 0;
+  std::vector<std::unique_ptr<Patch>> store;
+  // levels[level - minlevel] in ApplyOnLevel order (youngest first).
+  std::vector<std::vector<Patch*>> levels;
+  std::vector<Patch*>& on(int level) { return levels[level - minlevel]; }
+};
+
+// ---------------------------------------------------------------------------
+// Problem module elemental functions (problem.f90:760-813).
+inline double Mob(const Ctx&, double) { return 1.0; }
+inline double Ff(const Ctx& c, double x) {
+  double cm1 = x - 1.0;
+  return x * x * cm1 * cm1 * c.alpha / 4.0;
+}
+inline double Dfe(const Ctx& c, double x) { return (x - 0.5) * c.alpha / 4.0; }
+inline double Dfc(const Ctx& c, double x) {
+  double cmh = x - 0.5;
+  return cmh * cmh * cmh * c.alpha;
+}
+inline double D2fc(const Ctx& c, double x) {
+  double cmh = x - 0.5;
+  return 3.0 * cmh * cmh * c.alpha;
+}
+
+// AllocFields (lib/bsamstorage.f90:46-123).
+void AllocFields(const Ctx& c, Patch& p) {
+  int mx[3] = {1, 1, 1}, cmx[3] = {1, 1, 1};
+  for (int n = 0; n < c.ndims; ++n) {
+    mx[n] = p.mx[n];
+    cmx[n] = (mx[n] % 2 == 1) ? 1 : mx[n] / 2;
+  }
+  int m = p.mbc, nv = p.nrvars;
+  if (c.ndims == 2) {
+    p.q.alloc(1 - m, mx[0] + m, 1 - m, mx[1] + m, 1, 1, 1, nv);
+    p.qold.alloc(1 - m, mx[0] + m, 1 - m, mx[1] + m, 1, 1, 1, nv);
+    p.qc.alloc(1 - m, cmx[0] + m, 1 - m, cmx[1] + m, 1, 1, 1, nv);
+    p.f.alloc(1, mx[0], 1, mx[1], 1, 1, 1, nv);
+    p.rf.alloc(1, mx[0], 1, mx[1], 1, 1, 1, nv);
+    p.ftmp.alloc(1, mx[0], 1, mx[1], 1, 1, 1, nv);
+  } else {
+    p.q.alloc(1 - m, mx[0] + m, 1 - m, mx[1] + m, 1 - m, mx[2] + m, 1, nv);
+    p.qold.alloc(1 - m, mx[0] + m, 1 - m, mx[1] + m, 1 - m, mx[2] + m, 1, nv);
+    p.qc.alloc(1 - m, cmx[0] + m, 1 - m, cmx[1] + m, 1 - m, cmx[2] + m, 1, nv);
+    p.f.alloc(1, mx[0], 1, mx[1], 1, mx[2], 1, nv);
+    p.rf.alloc(1, mx[0], 1, mx[1], 1, mx[2], 1, nv);
+    p.ftmp.alloc(1, mx[0], 1, mx[1], 1, mx[2], 1, nv);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// RelaxGrid2D (problem.f90:164-215).  q has bounds (0:mx+1), f (1:mx).
+void RelaxGrid2D(const Ctx& c, FArr& q, const FArr& f, const int* mx, double h,
+                 int ipass) {
+  double h2 = h * h;
+  double tmp1 = c.dt / h2;
+  double tmp2 = c.eps2 / h2;
+  double tmp3 = 4.0 * c.eps2 / h2;
+  for (int j = 1; j <= mx[1]; ++j) {
+    for (int i = 1 + (j + ipass) % 2; i <= mx[0]; i += 2) {
+      double m1 = Mob(c, 0.5 * (q(i - 1, j, 1, 1) + q(i, j, 1, 1)));
+      double m2 = Mob(c, 0.5 * (q(i + 1, j, 1, 1) + q(i, j, 1, 1)));
+      double m3 = Mob(c, 0.5 * (q(i, j - 1, 1, 1) + q(i, j, 1, 1)));
+      double m4 = Mob(c, 0.5 * (q(i, j + 1, 1, 1) + q(i, j, 1, 1)));
+      double a12 = tmp1 * (m1 + m2 + m3 + m4);
+      double a21 = -D2fc(c, q(i, j, 1, 1)) - tmp3;
+      double b1 = f(i, j, 1, 1) + tmp1 * (m1 * q(i - 1, j, 1, 2) + m2 * q(i + 1, j, 1, 2) +
+                                          m3 * q(i, j - 1, 1, 2) + m4 * q(i, j + 1, 1, 2));
+      double b2 = f(i, j, 1, 2) + Dfc(c, q(i, j, 1, 1)) - D2fc(c, q(i, j, 1, 1)) * q(i, j, 1, 1) -
+                  tmp2 * (q(i + 1, j, 1, 1) + q(i - 1, j, 1, 1) + q(i, j + 1, 1, 1) +
+                          q(i, j - 1, 1, 1));
+      double det = 1.0 - a12 * a21;
+      q(i, j, 1, 1) = (b1 - a12 * b2) / det;
+      q(i, j, 1, 2) = (b2 - a21 * b1) / det;
+    }
+  }
+}
+
+// RelaxGrid3D (problem.f90:453-518).
+void RelaxGrid3D(const Ctx& c, FArr& q, const FArr& f, const int* mx, double h,
+                 int ipass) {
+  double h2 = h * h;
+  double tmp1 = c.dt / h2;
+  double tmp2 = c.eps2 / h2;
+  double tmp3 = 6.0 * c.eps2 / h2;
+  for (int k = 1; k <= mx[2]; ++k) {
+    for (int j = 1; j <= mx[1]; ++j) {
+      for (int i = 1 + (k + j + ipass) % 2; i <= mx[0]; i += 2) {
+        double m1 = Mob(c, 0.5 * (q(i - 1, j, k, 1) + q(i, j, k, 1)));
+        double m2 = Mob(c, 0.5 * (q(i + 1, j, k, 1) + q(i, j, k, 1)));
+        double m3 = Mob(c, 0.5 * (q(i, j - 1, k, 1) + q(i, j, k, 1)));
+        double m4 = Mob(c, 0.5 * (q(i, j + 1, k, 1) + q(i, j, k, 1)));
+        double m5 = Mob(c, 0.5 * (q(i, j, k - 1, 1) + q(i, j, k, 1)));
+        double m6 = Mob(c, 0.5 * (q(i, j, k + 1, 1) + q(i, j, k, 1)));
+        double a12 = tmp1 * (m1 + m2 + m3 + m4 + m5 + m6);
+        double a21 = -D2fc(c, q(i, j, k, 1)) - tmp3;
+        double b1 = f(i, j, k, 1) + tmp1 * (m1 * q(i - 1, j, k, 2) + m2 * q(i + 1, j, k, 2) +
+                                            m3 * q(i, j - 1, k, 2) + m4 * q(i, j + 1, k, 2) +
+                                            m5 * q(i, j, k - 1, 2) + m6 * q(i, j, k + 1, 2));
+        double b2 = f(i, j, k, 2) + Dfc(c, q(i, j, k, 1)) -
+                    D2fc(c, q(i, j, k, 1)) * q(i, j, k, 1) -
+                    tmp2 * (q(i + 1, j, k, 1) + q(i - 1, j, k, 1) + q(i, j + 1, k, 1) +
+                            q(i, j - 1, k, 1) + q(i, j, k + 1, 1) + q(i, j, k - 1, 1));
+        double det = 1.0 - a12 * a21;
+        q(i, j, k, 1) = (b1 - a12 * b2) / det;
+        q(i, j, k, 2) = (b2 - a21 * b1) / det;
+      }
+    }
+  }
+}
+
+// Operator2D (problem.f90:231-257) with ULapMob2D (304-329), UDiv2D and
+// ULap2D (gridutilities.f90:42-87).  q carries the ring (0:mx+1); res is
+// returned with bounds (1:mx).
+void Operator2D(const Ctx& c, const FArr& q, const int* mx, double h, FArr& res) {
+  double h2 = h * h;
+  double tmp1 = c.dt / h2;
+  double tmp2 = c.eps2 / h2;
+  int n1 = mx[0], n2 = mx[1];
+  res.alloc(1, n1, 1, n2, 1, 1, 1, 2);
+  // ULapMob2D flux arrays f1(0:mx1,1:mx2), f2(1:mx1,0:mx2).
+  FArr f1, f2;
+  f1.alloc(0, n1, 1, n2, 1, 1, 1, 1);
+  f2.alloc(1, n1, 0, n2, 1, 1, 1, 1);
+  for (int j = 1; j <= n2; ++j)
+    for (int i = 0; i <= n1; ++i)
+      f1(i, j, 1, 1) = Mob(c, 0.5 * (q(i + 1, j, 1, 1) + q(i, j, 1, 1))) *
+                       (q(i + 1, j, 1, 2) - q(i, j, 1, 2));
+  for (int j = 0; j <= n2; ++j)
+    for (int i = 1; i <= n1; ++i)
+      f2(i, j, 1, 1) = Mob(c, 0.5 * (q(i, j + 1, 1, 1) + q(i, j, 1, 1))) *
+                       (q(i, j + 1, 1, 2) - q(i, j, 1, 2));
+  for (int j = 1; j <= n2; ++j)
+    for (int i = 1; i <= n1; ++i) {
+      double udiv = f1(i, j, 1, 1) - f1(i - 1, j, 1, 1) + f2(i, j, 1, 1) - f2(i, j - 1, 1, 1);
+      res(i, j, 1, 1) = q(i, j, 1, 1) - tmp1 * udiv;
+    }
+  for (int j = 1; j <= n2; ++j)
+    for (int i = 1; i <= n1; ++i) {
+      double ulap = q(i + 1, j, 1, 1) + q(i - 1, j, 1, 1) + q(i, j + 1, 1, 1) +
+                    q(i, j - 1, 1, 1) - 4.0 * q(i, j, 1, 1);
+      res(i, j, 1, 2) = q(i, j, 1, 2) - Dfc(c, q(i, j, 1, 1)) + tmp2 * ulap;
+    }
+}
+
+// Operator3D (problem.f90:534-561) with ULapMob3D (607-642), UDiv3D and
+// ULap3D (gridutilities.f90:345-404).
+void Operator3D(const Ctx& c, const FArr& q, const int* mx, double h, FArr& res) {
+  double h2 = h * h;
+  double tmp1 = c.dt / h2;
+  double tmp2 = c.eps2 / h2;
+  int n1 = mx[0], n2 = mx[1], n3 = mx[2];
+  res.alloc(1, n1, 1, n2, 1, n3, 1, 2);
+  FArr f1, f2, f3;
+  f1.alloc(0, n1, 1, n2, 1, n3, 1, 1);
+  f2.alloc(1, n1, 0, n2, 1, n3, 1, 1);
+  f3.alloc(1, n1, 1, n2, 0, n3, 1, 1);
+  for (int k = 1; k <= n3; ++k)
+    for (int j = 1; j <= n2; ++j)
+      for (int i = 0; i <= n1; ++i)
+        f1(i, j, k, 1) = Mob(c, 0.5 * (q(i + 1, j, k, 1) + q(i, j, k, 1))) *
+                         (q(i + 1, j, k, 2) - q(i, j, k, 2));
+  for (int k = 1; k <= n3; ++k)
+    for (int j = 0; j <= n2; ++j)
+      for (int i = 1; i <= n1; ++i)
+        f2(i, j, k, 1) = Mob(c, 0.5 * (q(i, j + 1, k, 1) + q(i, j, k, 1))) *
+                         (q(i, j + 1, k, 2) - q(i, j, k, 2));
+  for (int k = 0; k <= n3; ++k)
+    for (int j = 1; j <= n2; ++j)
+      for (int i = 1; i <= n1; ++i)
+        f3(i, j, k, 1) = Mob(c, 0.5 * (q(i, j, k + 1, 1) + q(i, j, k, 1))) *
+                         (q(i, j, k + 1, 2) - q(i, j, k, 2));
+  for (int k = 1; k <= n3; ++k)
+    for (int j = 1; j <= n2; ++j)
+      for (int i = 1; i <= n1; ++i) {
+        double udiv = f1(i, j, k, 1) - f1(i - 1, j, k, 1) + f2(i, j, k, 1) - f2(i, j - 1, k, 1) +
+                      f3(i, j, k, 1) - f3(i, j, k - 1, 1);
+        res(i, j, k, 1) = q(i, j, k, 1) - tmp1 * udiv;
+      }
+  for (int k = 1; k <= n3; ++k)
+    for (int j = 1; j <= n2; ++j)
+      for (int i = 1; i <= n1; ++i) {
+        double ulap = q(i + 1, j, k, 1) + q(i - 1, j, k, 1) + q(i, j + 1, k, 1) +
+                      q(i, j - 1, k, 1) + q(i, j, k + 1, 1) + q(i, j, k - 1, 1) -
+                      6.0 * q(i, j, k, 1);
+        res(i, j, k, 2) = q(i, j, k, 2) - Dfc(c, q(i, j, k, 1)) + tmp2 * ulap;
+      }
+}
+
+void Operator(const Ctx& c, const FArr& q, const int* mx, double h, FArr& res) {
+  if (c.ndims == 2) Operator2D(c, q, mx, h, res);
+  else Operator3D(c, q, mx, h, res);
+}
+
+// Restriction2D/3D (gridutilities.f90:89-110, 406-433).  `a` is addressed
+// with its own indices starting at 1 (the reference passes a(1:mx) sections).
+void Restriction(const Ctx& c, const FArr& a, const int* mx, int nv, FArr& out) {
+  int cm[3] = {mx[0] / 2, mx[1] / 2, c.ndims == 3 ? mx[2] / 2 : 1};
+  out.alloc(1, cm[0], 1, cm[1], 1, cm[2], 1, nv);
+  if (c.ndims == 2) {
+    for (int v = 1; v <= nv; ++v)
+      for (int jc = 1; jc <= cm[1]; ++jc)
+        for (int ic = 1; ic <= cm[0]; ++ic) {
+          int i = 2 * ic, j = 2 * jc;
+          out(ic, jc, 1, v) = 0.25 * (a(i, j, 1, v) + a(i - 1, j, 1, v) + a(i, j - 1, 1, v) +
+                                      a(i - 1, j - 1, 1, v));
+        }
+  } else {
+    for (int v = 1; v <= nv; ++v)
+      for (int kc = 1; kc <= cm[2]; ++kc)
+        for (int jc = 1; jc <= cm[1]; ++jc)
+          for (int ic = 1; ic <= cm[0]; ++ic) {
+            int i = 2 * ic, j = 2 * jc, k = 2 * kc;
+            out(ic, jc, kc, v) =
+                0.125 * (a(i, j, k, v) + a(i - 1, j, k, v) + a(i, j - 1, k, v) +
+                         a(i - 1, j - 1, k, v) + a(i, j, k - 1, v) + a(i - 1, j, k - 1, v) +
+                         a(i, j - 1, k - 1, v) + a(i - 1, j - 1, k - 1, v));
+          }
+  }
+}
+
+// BiLinProlongationP1 / TriLinProlongationP1 (gridutilities.f90:137-175,
+// 474-529).  a has bounds (0:cmx+1); out gets (0:mx+1) with mx = 2*cmx.
+void ProlongationP1(const Ctx& c, const FArr& a, const int* cmx, int nv, FArr& out) {
+  int mx0 = 2 * cmx[0], mx1 = 2 * cmx[1];
+  if (c.ndims == 2) {
+    FArr b;
+    b.alloc(0, mx0 + 1, 0, cmx[1] + 1, 1, 1, 1, nv);
+    for (int v = 1; v <= nv; ++v)
+      for (int n = 0; n <= cmx[1] + 1; ++n)
+        for (int m = 0; m <= cmx[0]; ++m) {
+          b(2 * m, n, 1, v) = 3.0 * a(m, n, 1, v) + a(m + 1, n, 1, v);
+          b(2 * m + 1, n, 1, v) = a(m, n, 1, v) + 3.0 * a(m + 1, n, 1, v);
+        }
+    out.alloc(0, mx0 + 1, 0, mx1 + 1, 1, 1, 1, nv);
+    for (int v = 1; v <= nv; ++v)
+      for (int n = 0; n <= cmx[1]; ++n)
+        for (int i = 0; i <= mx0 + 1; ++i) {
+          out(i, 2 * n, 1, v) = (3.0 * b(i, n, 1, v) + b(i, n + 1, 1, v)) / 16.0;
+          out(i, 2 * n + 1, 1, v) = (b(i, n, 1, v) + 3.0 * b(i, n + 1, 1, v)) / 16.0;
+        }
+  } else {
+    int mx2 = 2 * cmx[2];
+    FArr b, cc;
+    b.alloc(0, mx0 + 1, 0, cmx[1] + 1, 0, cmx[2] + 1, 1, nv);
+    for (int v = 1; v <= nv; ++v)
+      for (int p = 0; p <= cmx[2] + 1; ++p)
+        for (int n = 0; n <= cmx[1] + 1; ++n)
+          for (int m = 0; m <= cmx[0]; ++m) {
+            b(2 * m, n, p, v) = 3.0 * a(m, n, p, v) + a(m + 1, n, p, v);
+            b(2 * m + 1, n, p, v) = a(m, n, p, v) + 3.0 * a(m + 1, n, p, v);
+          }
+    cc.alloc(0, mx0 + 1, 0, mx1 + 1, 0, cmx[2] + 1, 1, nv);
+    for (int v = 1; v <= nv; ++v)
+      for (int p = 0; p <= cmx[2] + 1; ++p)
+        for (int n = 0; n <= cmx[1]; ++n)
+          for (int i = 0; i <= mx0 + 1; ++i) {
+            cc(i, 2 * n, p, v) = 3.0 * b(i, n, p, v) + b(i, n + 1, p, v);
+            cc(i, 2 * n + 1, p, v) = b(i, n, p, v) + 3.0 * b(i, n + 1, p, v);
+          }
+    out.alloc(0, mx0 + 1, 0, mx1 + 1, 0, mx2 + 1, 1, nv);
+    for (int v = 1; v <= nv; ++v)
+      for (int p = 0; p <= cmx[2]; ++p)
+        for (int j = 0; j <= mx1 + 1; ++j)
+          for (int i = 0; i <= mx0 + 1; ++i) {
+            out(i, j, 2 * p, v) = (3.0 * cc(i, j, p, v) + cc(i, j, p + 1, v)) / 64.0;
+            out(i, j, 2 * p + 1, v) = (cc(i, j, p, v) + 3.0 * cc(i, j, p + 1, v)) / 64.0;
+          }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Physical boundary conditions: SetBC2D/SetBC3D (boundary.f90:643-891) with
+// the problem module's UserBC2D/UserBC3D (problem.f90:646-756), mbc = 1.
+// Returns nonzero for a code the reference stops on.
+int SetBC2D(FArr& q, const int* mx, int nv, const int* mthbc) {
+  const int ll = 0, ul1 = mx[0] + 1, ul2 = mx[1] + 1;
+  for (int face = 1; face <= 4; ++face) {
+    int code = mthbc[face - 1];
+    if (code == 2 || code == 999) continue;
+    if (code == 1) {
+      for (int v = 1; v <= nv; ++v) {
+        if (face == 1) for (int j = ll; j <= ul2; ++j) q(0, j, 1, v) = q(1, j, 1, v);
+        if (face == 2) for (int j = ll; j <= ul2; ++j) q(mx[0] + 1, j, 1, v) = q(mx[0], j, 1, v);
+        if (face == 3) for (int i = ll; i <= ul1; ++i) q(i, 0, 1, v) = q(i, 1, 1, v);
+        if (face == 4) for (int i = ll; i <= ul1; ++i) q(i, mx[1] + 1, 1, v) = q(i, mx[1], 1, v);
+      }
+    } else if (code >= 10 && code <= 99) {
+      // UserBC2D(q, ..., bcnow = face).
+      if (face == 1)
+        for (int v = 1; v <= nv; ++v)
+          for (int j = ll; j <= ul2; ++j) q(0, j, 1, v) = 2.0 - q(1, j, 1, v);
+      if (face == 2)
+        for (int v = 1; v <= nv; ++v)
+          for (int j = ll; j <= ul2; ++j) q(mx[0] + 1, j, 1, v) = 2.0 - q(mx[0], j, 1, v);
+      if (face == 3)
+        for (int v = 1; v <= 2; ++v)
+          for (int i = ll; i <= ul1; ++i) q(i, 0, 1, v) = q(i, 1, 1, v);
+      if (face == 4)
+        for (int v = 1; v <= 2; ++v)
+          for (int i = ll; i <= ul1; ++i) q(i, mx[1] + 1, 1, v) = q(i, mx[1], 1, v);
+    } else {
+      return -1;
+    }
+  }
+  return 0;
+}
+
+int SetBC3D(FArr& q, const int* mx, int nv, const int* mthbc) {
+  const int ll = 0, ul[3] = {mx[0] + 1, mx[1] + 1, mx[2] + 1};
+  for (int face = 1; face <= 6; ++face) {
+    int code = mthbc[face - 1];
+    if (code == 2 || code == 999) continue;
+    bool user = (code >= 10 && code <= 99);
+    if (code != 1 && !user) return -1;
+    int dim = (face - 1) / 2;
+    bool hi = (face % 2) == 0;
+    int g = hi ? mx[dim] + 1 : 0;   // ghost index along dim
+    int s = hi ? mx[dim] : 1;       // source index along dim
+    for (int v = 1; v <= nv; ++v)
+      for (int k = ll; k <= ul[2]; ++k)
+        for (int j = ll; j <= ul[1]; ++j)
+          for (int i = ll; i <= ul[0]; ++i) {
+            int idx[3] = {i, j, k};
+            if (idx[dim] != g) continue;
+            int src[3] = {i, j, k};
+            src[dim] = s;
+            double val = q(src[0], src[1], src[2], v);
+            q(i, j, k, v) = user ? 2.0 - val : val;
+          }
+  }
+  return 0;
+}
+
+int SetBC(const Ctx& c, Patch& p) {
+  if (p.tobedeleted) return 0;
+  if (c.ndims == 2) return SetBC2D(p.q, p.mx, p.nrvars, p.mthbc);
+  return SetBC3D(p.q, p.mx, p.nrvars, p.mthbc);
+}
+
+// SetGhost (boundary.f90:58-89).  Only root and below-root levels exist in
+// the uniform configuration, so the coarse-fine interpolation and sibling
+// exchange branches (level > rootlevel) are not reached.
+int SetGhost(Ctx& c, int level, int /*ipass*/) {
+  int err = 0;
+  for (Patch* p : c.on(level)) err |= SetBC(c, *p);
+  return err;
+}
+
+// GetCoarseGhostPoints (boundary.f90:1203-1269).
+void GetCoarseGhostPoints(const Ctx& c, Patch& p) {
+  if (p.tobedeleted) return;
+  Patch& par = *p.parent;
+  int nv = p.nrvars;
+  int cmx[3] = {1, 1, 1}, il[3] = {1, 1, 1}, ih[3] = {1, 1, 1}, jl[3] = {1, 1, 1},
+      jh[3] = {1, 1, 1}, mb[3][2] = {{1, 1}, {1, 1}, {1, 1}};
+  for (int n = 0; n < c.ndims; ++n) {
+    cmx[n] = p.mx[n] / 2;
+    il[n] = 0;
+    ih[n] = cmx[n] + 1;
+    mb[n][0] = p.mbounds[n][0];
+    mb[n][1] = p.mbounds[n][1];
+    jl[n] = mb[n][0] - 1;
+    jh[n] = mb[n][1] + 1;
+  }
+  for (int v = 1; v <= nv; ++v) {
+    // Faces 1 and 2.
+    for (int k = il[2], pk = jl[2]; k <= ih[2]; ++k, ++pk)
+      for (int j = il[1], pj = jl[1]; j <= ih[1]; ++j, ++pj) {
+        p.qc(il[0], j, k, v) = par.q(jl[0], pj, pk, v);
+        p.qc(ih[0], j, k, v) = par.q(jh[0], pj, pk, v);
+      }
+    // Faces 3 and 4.
+    for (int k = il[2], pk = jl[2]; k <= ih[2]; ++k, ++pk)
+      for (int i = 1, pi = mb[0][0]; i <= cmx[0]; ++i, ++pi) {
+        p.qc(i, il[1], k, v) = par.q(pi, jl[1], pk, v);
+        p.qc(i, ih[1], k, v) = par.q(pi, jh[1], pk, v);
+      }
+    if (c.ndims == 3) {
+      for (int j = 1, pj = mb[1][0]; j <= cmx[1]; ++j, ++pj)
+        for (int i = 1, pi = mb[0][0]; i <= cmx[0]; ++i, ++pi) {
+          p.qc(i, j, il[2], v) = par.q(pi, pj, jl[2], v);
+          p.qc(i, j, ih[2], v) = par.q(pi, pj, jh[2], v);
+        }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// AFAS routines (lib/afasroutines.f90).
+inline int cmx_of(const Ctx& c, const Patch& p, int n) {
+  return n < c.ndims ? p.mx[n] / 2 : 1;
+}
+
+// Residual (afas:799-840): rf = f - Operator(q).
+void Residual(const Ctx& c, Patch& p) {
+  FArr res;
+  Operator(c, p.q, p.mx, p.dx[0], res);
+  int n3 = c.ndims == 3 ? p.mx[2] : 1;
+  for (int v = 1; v <= p.nrvars; ++v)
+    for (int k = 1; k <= n3; ++k)
+      for (int j = 1; j <= p.mx[1]; ++j)
+        for (int i = 1; i <= p.mx[0]; ++i) p.rf(i, j, k, v) = p.f(i, j, k, v) - res(i, j, k, v);
+}
+
+// SquareSum (afas:210-221): sum(rf*rf), sequential, column-major.
+double SquareSum(const Ctx& c, const Patch& p) {
+  double s = 0.0;
+  int n3 = c.ndims == 3 ? p.mx[2] : 1;
+  for (int v = 1; v <= p.nrvars; ++v)
+    for (int k = 1; k <= n3; ++k)
+      for (int j = 1; j <= p.mx[1]; ++j)
+        for (int i = 1; i <= p.mx[0]; ++i) {
+          double r = p.rf(i, j, k, v);
+          s = s + r * r;
+        }
+  return s;
+}
+
+// ErrorAFAS with errortype 1 + L2Error (afas:108-179).
+double ErrorAFAS(Ctx& c, int level) {
+  double ir1 = 0.0, ir2 = 0.0;
+  for (Patch* p : c.on(level)) {
+    Residual(c, *p);
+    ir1 = SquareSum(c, *p) + ir1;
+    long ncell = 1;
+    for (int n = 0; n < c.ndims; ++n) ncell *= p->mx[n];
+    ir2 = (double)(p->nrvars * ncell) + ir2;
+  }
+  return std::sqrt(ir1 / ir2);
+}
+
+// Copy a (1:cmx) restriction result into parent(mb) -- shared by
+// FillDownLevel and RestrictSolution.
+void StoreIntoParent(const Ctx& c, const FArr& src, FArr& dst, const Patch& p, int nv) {
+  int cm[3] = {cmx_of(c, p, 0), cmx_of(c, p, 1), cmx_of(c, p, 2)};
+  int mb0[3] = {p.mbounds[0][0], p.mbounds[1][0], c.ndims == 3 ? p.mbounds[2][0] : 1};
+  for (int v = 1; v <= nv; ++v)
+    for (int k = 1; k <= cm[2]; ++k)
+      for (int j = 1; j <= cm[1]; ++j)
+        for (int i = 1; i <= cm[0]; ++i)
+          dst(mb0[0] + i - 1, mb0[1] + j - 1, mb0[2] + k - 1, v) = src(i, j, k, v);
+}
+
+// FillDownLevel (afas:241-310).
+void FillDownLevel(Ctx& c, Patch& p, bool source) {
+  if (p.tobedeleted) return;
+  FArr r;
+  if (source) {
+    Restriction(c, p.f, p.mx, p.nrvars, r);
+    StoreIntoParent(c, r, p.parent->f, p, p.nrvars);
+  } else {
+    Restriction(c, p.q, p.mx, p.nrvars, r);
+    StoreIntoParent(c, r, p.parent->q, p, p.nrvars);
+  }
+}
+
+// FillDown (afas:223-239).
+void FillDown(Ctx& c, bool source) {
+  for (int level = c.finestlevel; level >= c.minlevel + 1; --level) {
+    for (Patch* p : c.on(level)) FillDownLevel(c, *p, source);
+    if (!source) SetGhost(c, level - 1, 0);
+  }
+}
+
+// GetSourceFunction (afas:312-367): ftmp = Source(q, qold).
+void GetSourceFunction(Ctx& c, Patch& p) {
+  if (p.tobedeleted) return;
+  int n3 = c.ndims == 3 ? p.mx[2] : 1;
+  for (int k = 1; k <= n3; ++k)
+    for (int j = 1; j <= p.mx[1]; ++j)
+      for (int i = 1; i <= p.mx[0]; ++i) p.ftmp(i, j, k, 1) = p.qold(i, j, k, 1);
+  for (int k = 1; k <= n3; ++k)
+    for (int j = 1; j <= p.mx[1]; ++j)
+      for (int i = 1; i <= p.mx[0]; ++i) p.ftmp(i, j, k, 2) = -Dfe(c, p.qold(i, j, k, 1));
+}
+
+// UpdateSourceFunction (afas:427-486): f = ftmp + SourceUpdate (= 0).
+void UpdateSourceFunction(Ctx& c, Patch& p) {
+  if (p.tobedeleted) return;
+  int n3 = c.ndims == 3 ? p.mx[2] : 1;
+  for (int v = 1; v <= p.nrvars; ++v)
+    for (int k = 1; k <= n3; ++k)
+      for (int j = 1; j <= p.mx[1]; ++j)
+        for (int i = 1; i <= p.mx[0]; ++i) p.f(i, j, k, v) = p.ftmp(i, j, k, v) + 0.0;
+}
+
+// RelaxPatch (afas:549-598).
+void RelaxPatch(Ctx& c, Patch& p, int ipass) {
+  if (p.tobedeleted) return;
+  if (c.ndims == 2) RelaxGrid2D(c, p.q, p.f, p.mx, p.dx[0], ipass);
+  else RelaxGrid3D(c, p.q, p.f, p.mx, p.dx[0], ipass);
+}
+
+// LevelRelax (afas:523-547).
+void LevelRelax(Ctx& c, int level) {
+  for (int pass = 1; pass <= c.nsmoothingpasses; ++pass)
+    for (int rb = 1; rb <= 2; ++rb) {
+      for (Patch* p : c.on(level)) RelaxPatch(c, *p, rb);
+      SetGhost(c, level, rb);
+    }
+}
+
+// RestrictSolution (afas:600-644).
+void RestrictSolution(Ctx& c, Patch& p) {
+  if (p.tobedeleted) return;
+  FArr r;
+  Restriction(c, p.q, p.mx, p.nrvars, r);
+  int cm[3] = {cmx_of(c, p, 0), cmx_of(c, p, 1), cmx_of(c, p, 2)};
+  for (int v = 1; v <= p.nrvars; ++v)
+    for (int k = 1; k <= cm[2]; ++k)
+      for (int j = 1; j <= cm[1]; ++j)
+        for (int i = 1; i <= cm[0]; ++i) p.qc(i, j, k, v) = r(i, j, k, v);
+  StoreIntoParent(c, p.qc, p.parent->q, p, p.nrvars);
+}
+
+// CoarseLoadingFunction (afas:646-714):
+//   parent%f(mb) = Restriction(rf) + Operator(qc incl. ring, h = parent%dx).
+void CoarseLoadingFunction(Ctx& c, Patch& p) {
+  if (p.tobedeleted) return;
+  Patch& par = *p.parent;
+  Residual(c, p);
+  FArr r, op;
+  Restriction(c, p.rf, p.mx, p.nrvars, r);
+  int cm[3] = {cmx_of(c, p, 0), cmx_of(c, p, 1), cmx_of(c, p, 2)};
+  Operator(c, p.qc, cm, par.dx[0], op);
+  FArr sum;
+  sum.alloc(1, cm[0], 1, cm[1], 1, cm[2], 1, p.nrvars);
+  for (int v = 1; v <= p.nrvars; ++v)
+    for (int k = 1; k <= cm[2]; ++k)
+      for (int j = 1; j <= cm[1]; ++j)
+        for (int i = 1; i <= cm[0]; ++i) sum(i, j, k, v) = r(i, j, k, v) + op(i, j, k, v);
+  StoreIntoParent(c, sum, par.f, p, p.nrvars);
+}
+
+// CorrectFine with mbc = 1 (afas:842-963).
+void CorrectFine(Ctx& c, Patch& p) {
+  if (p.tobedeleted) return;
+  Patch& par = *p.parent;
+  int cm[3] = {cmx_of(c, p, 0), cmx_of(c, p, 1), cmx_of(c, p, 2)};
+  int nv = p.nrvars;
+  int lo3 = c.ndims == 3 ? 0 : 1, hi3 = c.ndims == 3 ? cm[2] + 1 : 1;
+  int off[3] = {p.mbounds[0][0] - 1, p.mbounds[1][0] - 1,
+                c.ndims == 3 ? p.mbounds[2][0] - 1 : 0};
+  // qc(0:cmx+1) = parent%q(mb-1:mb+1) - qc(0:cmx+1)
+  for (int v = 1; v <= nv; ++v)
+    for (int k = lo3; k <= hi3; ++k)
+      for (int j = 0; j <= cm[1] + 1; ++j)
+        for (int i = 0; i <= cm[0] + 1; ++i)
+          p.qc(i, j, k, v) = par.q(off[0] + i, off[1] + j, c.ndims == 3 ? off[2] + k : 1, v) -
+                             p.qc(i, j, k, v);
+  FArr pr;
+  ProlongationP1(c, p.qc, cm, nv, pr);
+  int mlo3 = c.ndims == 3 ? 0 : 1, mhi3 = c.ndims == 3 ? p.mx[2] + 1 : 1;
+  for (int v = 1; v <= nv; ++v)
+    for (int k = mlo3; k <= mhi3; ++k)
+      for (int j = 0; j <= p.mx[1] + 1; ++j)
+        for (int i = 0; i <= p.mx[0] + 1; ++i) p.q(i, j, k, v) = p.q(i, j, k, v) + pr(i, j, k, v);
+}
+
+// AFASVcycle (afas:488-521).
+void AFASVcycle(Ctx& c, int level) {
+  LevelRelax(c, level);
+  if (level > c.minlevel) {
+    for (Patch* p : c.on(level)) RestrictSolution(c, *p);
+    SetGhost(c, level - 1, 0);
+    for (Patch* p : c.on(level)) GetCoarseGhostPoints(c, *p);
+    for (Patch* p : c.on(level)) CoarseLoadingFunction(c, *p);
+    AFASVcycle(c, level - 1);
+    for (Patch* p : c.on(level)) CorrectFine(c, *p);
+    SetGhost(c, level, 0);
+    LevelRelax(c, level);
+  }
+}
+
+// MultigridIterations (afas:38-106).  Returns the V-cycle count; the
+// residual trace goes to `trace` (maxvcycles entries) when non-null.
+int MultigridIterations(Ctx& c, double* last_residual, double* trace) {
+  FillDown(c, false);
+  for (int level = c.finestlevel; level >= Ctx::rootlevel; --level)
+    for (Patch* p : c.on(level)) GetSourceFunction(c, *p);
+  for (int level = c.finestlevel; level >= Ctx::rootlevel; --level)
+    for (Patch* p : c.on(level)) UpdateSourceFunction(c, *p);
+  FillDown(c, true);
+  int itmg;
+  double residual = 0.0;
+  for (itmg = 1; itmg <= c.maxvcycles; ++itmg) {
+    AFASVcycle(c, c.finestlevel);
+    FillDown(c, false);
+    for (int level = c.finestlevel; level >= Ctx::rootlevel; --level)
+      for (Patch* p : c.on(level)) UpdateSourceFunction(c, *p);
+    FillDown(c, true);
+    residual = ErrorAFAS(c, c.finestlevel);
+    if (trace) trace[itmg - 1] = residual;
+    if (residual < c.qerrortol) break;
+    // MultiGridUserBreak is .false. for this problem (problem.f90:814-821).
+  }
+  if (last_residual) *last_residual = residual;
+  return itmg > c.maxvcycles ? c.maxvcycles : itmg;
+}
+
+void CopyQToQold(Patch& p) {
+  if (p.tobedeleted) return;
+  p.qold.d = p.q.d;
+}
+
+int resolve_minlevel(const orc_params* p) {
+  if (p->minlevel != 1) return p->minlevel;
+  int ml = 0, mxt[3] = {p->mx[0], p->mx[1], p->mx[2]};
+  for (;;) {
+    bool even = true;
+    for (int n = 0; n < p->ndims; ++n) even = even && (mxt[n] % 2 == 0);
+    if (!even) break;
+    if (ml == 10) break;
+    ++ml;
+    for (int n = 0; n < p->ndims; ++n) mxt[n] /= 2;
+  }
+  return -ml;
+}
+
+// RootInit + CreateBelowSeedLevels + InitSeed (lib/bsamroutines.f90:205-494,
+// lib/treeops.f90:193-289) for a single root grid with maxlevel = 0.
+int BuildUniform(Ctx& c, const orc_params* p) {
+  if (p->ndims < 2 || p->ndims > 3) return -1;
+  if (p->errortype != 1) return -2;
+  for (int n = 0; n < p->ndims; ++n) {
+    if (p->mx[n] <= 0 || p->mx[n] % 2 != 0) return -3;
+    if (p->xupper[n] <= p->xlower[n]) return -4;
+  }
+  for (int f = 0; f < 2 * p->ndims; ++f) {
+    int code = p->mthbc[f];
+    if (!(code == 1 || (code >= 10 && code <= 99))) return -5;  // no periodic
+  }
+  c.ndims = p->ndims;
+  c.dt = p->dt;
+  c.qerrortol = p->qerrortol;
+  c.alpha = p->alpha;
+  c.eps = p->eps;
+  c.eps2 = p->eps * p->eps;
+  c.maxvcycles = p->maxvcycles;
+  c.nsmoothingpasses = p->nsmoothingpasses;
+  c.errortype = p->errortype;
+  c.minlevel = resolve_minlevel(p);
+  if (c.minlevel > 0 || c.minlevel < -10) return -6;
+  c.finestlevel = 0;
+  c.levels.assign(1 - c.minlevel, {});
+
+  auto root = std::make_unique<Patch>();
+  root->level = 0;
+  for (int n = 0; n < c.ndims; ++n) {
+    root->mx[n] = p->mx[n];
+    root->mglobal[n][0] = 1;
+    root->mglobal[n][1] = p->mx[n];
+    root->mbounds[n][0] = 1;
+    root->mbounds[n][1] = p->mx[n];
+    root->xlower[n] = p->xlower[n];
+    root->dx[n] = (p->xupper[n] - p->xlower[n]) / (double)p->mx[n];
+  }
+  for (int f = 0; f < 6; ++f) root->mthbc[f] = f < 2 * c.ndims ? p->mthbc[f] : 1;
+  for (int n = 1; n < c.ndims; ++n)
+    if (std::fabs(root->dx[0] - root->dx[n]) > 1.0e-10) return -7;
+  AllocFields(c, *root);
+  Patch* child = root.get();
+  c.on(0).push_back(child);
+  c.store.push_back(std::move(root));
+  for (int level = -1; level >= c.minlevel; --level) {
+    for (int n = 0; n < c.ndims; ++n)
+      if (child->mx[n] % 2 != 0) return -8;
+    auto seed = std::make_unique<Patch>();
+    seed->level = level;
+    for (int n = 0; n < c.ndims; ++n) {
+      seed->mx[n] = child->mx[n] / 2;
+      seed->dx[n] = child->dx[n] * 2.0;
+      seed->mglobal[n][0] = 1;
+      seed->mglobal[n][1] = child->mglobal[n][1] / 2;
+      child->mbounds[n][0] = 1;
+      child->mbounds[n][1] = seed->mx[n];
+      seed->mbounds[n][0] = 1;
+      seed->mbounds[n][1] = seed->mx[n];
+      seed->xlower[n] = child->xlower[n];
+    }
+    for (int f = 0; f < 6; ++f) seed->mthbc[f] = child->mthbc[f];
+    AllocFields(c, *seed);
+    child->parent = seed.get();
+    child = seed.get();
+    c.on(level).push_back(child);
+    c.store.push_back(std::move(seed));
+  }
+  return 0;
+}
+
+// Wrap a flat Fortran-ordered array into an FArr with the given bounds.
+FArr wrap(int ndims, const int* lo, const int* hi, int nv, const double* src) {
+  FArr a;
+  a.alloc(lo[0], hi[0], lo[1], hi[1], ndims == 3 ? lo[2] : 1, ndims == 3 ? hi[2] : 1, 1, nv);
+  if (src) std::memcpy(a.d.data(), src, a.d.size() * sizeof(double));
+  return a;
+}
+
+Ctx leaf_ctx(int ndims, double dt, double alpha, double eps) {
+  Ctx c;
+  c.ndims = ndims;
+  c.dt = dt;
+  c.alpha = alpha;
+  c.eps = eps;
+  c.eps2 = eps * eps;
+  return c;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int orc_minlevel(const orc_params* p) { return resolve_minlevel(p); }
+
+int orc_run_uniform(const orc_params* p, const double* q0, int nsteps, double* q_steps,
+                    int* nvcycles, double* resid_final, double* resid_trace, double* mass) {
+  Ctx c;
+  int err = BuildUniform(c, p);
+  if (err) return err;
+  Patch& root = *c.on(0)[0];
+  std::memcpy(root.q.d.data(), q0, root.q.d.size() * sizeof(double));
+  // BSAMSolver: SetGhost(rootlevel,0); CopyQToQold (bsamroutines.f90:144-147).
+  if (SetGhost(c, 0, 0)) return -9;
+  CopyQToQold(root);
+  bool firstamr = true;
+  double h = root.dx[0];
+  for (int step = 0; step < nsteps; ++step) {
+    c.finestlevel = 0;
+    SetGhost(c, 0, 0);  // AMR(rootlevel) with maxlevel = 0
+    if (firstamr) {
+      FillDown(c, false);
+      firstamr = false;
+    }
+    for (int level = c.minlevel; level <= c.finestlevel; ++level)
+      for (Patch* pp : c.on(level)) CopyQToQold(*pp);
+    double* tr = resid_trace ? resid_trace + (long)step * c.maxvcycles : nullptr;
+    if (tr)
+      for (int i = 0; i < c.maxvcycles; ++i) tr[i] = -1.0;
+    double last = 0.0;
+    int nv = MultigridIterations(c, &last, tr);
+    if (nvcycles) nvcycles[step] = nv;
+    if (resid_final) resid_final[step] = last;
+    if (q_steps)
+      std::memcpy(q_steps + (long)step * root.q.d.size(), root.q.d.data(),
+                  root.q.d.size() * sizeof(double));
+    if (mass) {
+      // AfterStep2D/3D, level 0 (problem.f90:121-122, 416-418).
+      double s = 0.0;
+      int n3 = c.ndims == 3 ? root.mx[2] : 1;
+      for (int k = 1; k <= n3; ++k)
+        for (int j = 1; j <= root.mx[1]; ++j)
+          for (int i = 1; i <= root.mx[0]; ++i) s = s + root.q(i, j, k, 1);
+      double hd = c.ndims == 2 ? h * h : h * h * h;
+      mass[step] = hd * s;
+    }
+  }
+  return 0;
+}
+
+void orc_relax_grid(int ndims, const int* mx, double h, double dt, double alpha, double eps,
+                    int ipass, double* q, const double* f) {
+  Ctx c = leaf_ctx(ndims, dt, alpha, eps);
+  int lo[3] = {0, 0, 0}, hi[3] = {mx[0] + 1, mx[1] + 1, ndims == 3 ? mx[2] + 1 : 1};
+  int flo[3] = {1, 1, 1}, fhi[3] = {mx[0], mx[1], ndims == 3 ? mx[2] : 1};
+  FArr Q = wrap(ndims, lo, hi, 2, q), F = wrap(ndims, flo, fhi, 2, f);
+  if (ndims == 2) RelaxGrid2D(c, Q, F, mx, h, ipass);
+  else RelaxGrid3D(c, Q, F, mx, h, ipass);
+  std::memcpy(q, Q.d.data(), Q.d.size() * sizeof(double));
+}
+
+void orc_operator(int ndims, const int* mx, double h, double dt, double alpha, double eps,
+                  const double* q, double* res) {
+  Ctx c = leaf_ctx(ndims, dt, alpha, eps);
+  int lo[3] = {0, 0, 0}, hi[3] = {mx[0] + 1, mx[1] + 1, ndims == 3 ? mx[2] + 1 : 1};
+  FArr Q = wrap(ndims, lo, hi, 2, q), R;
+  Operator(c, Q, mx, h, R);
+  std::memcpy(res, R.d.data(), R.d.size() * sizeof(double));
+}
+
+void orc_restriction(int ndims, const int* mx, int nv, const double* a, double* out) {
+  Ctx c = leaf_ctx(ndims, 0, 1, 0);
+  int lo[3] = {1, 1, 1}, hi[3] = {mx[0], mx[1], ndims == 3 ? mx[2] : 1};
+  FArr A = wrap(ndims, lo, hi, nv, a), O;
+  Restriction(c, A, mx, nv, O);
+  std::memcpy(out, O.d.data(), O.d.size() * sizeof(double));
+}
+
+void orc_prolongation_p1(int ndims, const int* cmx, int nv, const double* a, double* out) {
+  Ctx c = leaf_ctx(ndims, 0, 1, 0);
+  int lo[3] = {0, 0, 0}, hi[3] = {cmx[0] + 1, cmx[1] + 1, ndims == 3 ? cmx[2] + 1 : 1};
+  FArr A = wrap(ndims, lo, hi, nv, a), O;
+  ProlongationP1(c, A, cmx, nv, O);
+  std::memcpy(out, O.d.data(), O.d.size() * sizeof(double));
+}
+
+int orc_setbc(int ndims, const int* mx, int nv, const int* mthbc, double* q) {
+  int lo[3] = {0, 0, 0}, hi[3] = {mx[0] + 1, mx[1] + 1, ndims == 3 ? mx[2] + 1 : 1};
+  FArr Q = wrap(ndims, lo, hi, nv, q);
+  int err = ndims == 2 ? SetBC2D(Q, mx, nv, mthbc) : SetBC3D(Q, mx, nv, mthbc);
+  std::memcpy(q, Q.d.data(), Q.d.size() * sizeof(double));
+  return err;
+}
+
+void orc_source(int ndims, const int* mx, double alpha, const double* qold, double* f) {
+  Ctx c = leaf_ctx(ndims, 0, alpha, 0);
+  Patch p;
+  p.mx[0] = mx[0];
+  p.mx[1] = mx[1];
+  p.mx[2] = ndims == 3 ? mx[2] : 1;
+  AllocFields(c, p);
+  std::memcpy(p.qold.d.data(), qold, p.qold.d.size() * sizeof(double));
+  GetSourceFunction(c, p);
+  std::memcpy(f, p.ftmp.d.data(), p.ftmp.d.size() * sizeof(double));
+}
+
+double orc_energy2d(const int* mx, double h, double alpha, double eps, const double* cin) {
+  // Energy2D (problem.f90:330-361).
+  Ctx c = leaf_ctx(2, 0, alpha, eps);
+  int lo[3] = {0, 0, 1}, hi[3] = {mx[0] + 1, mx[1] + 1, 1};
+  FArr C = wrap(2, lo, hi, 1, cin);
+  int n1 = mx[0], n2 = mx[1];
+  double h2 = h * h;
+  FArr f1, f2;
+  f1.alloc(0, n1, 1, n2, 1, 1, 1, 1);
+  f2.alloc(1, n1, 0, n2, 1, 1, 1, 1);
+  for (int j = 1; j <= n2; ++j)
+    for (int i = 0; i <= n1; ++i) {
+      double d = C(i + 1, j, 1, 1) - C(i, j, 1, 1);
+      f1(i, j, 1, 1) = d * d;
+    }
+  for (int j = 0; j <= n2; ++j)
+    for (int i = 1; i <= n1; ++i) {
+      double d = C(i, j + 1, 1, 1) - C(i, j, 1, 1);
+      f2(i, j, 1, 1) = d * d;
+    }
+  double tmp = c.eps2 / h2 / 4.0;
+  double sF = 0.0, sG = 0.0;
+  for (int j = 1; j <= n2; ++j)
+    for (int i = 1; i <= n1; ++i) sF = sF + Ff(c, C(i, j, 1, 1));
+  for (int j = 1; j <= n2; ++j)
+    for (int i = 1; i <= n1; ++i)
+      sG = sG + (f1(i, j, 1, 1) + f1(i - 1, j, 1, 1) + f2(i, j, 1, 1) + f2(i, j - 1, 1, 1));
+  return h2 * (sF + tmp * sG);
+}
+
+}  // extern "C"

@@ -1,0 +1,86 @@
+/*
+ * bsam_oracle.h -- C API of the CPU oracle (TEST INFRASTRUCTURE ONLY).
+ *
+ * The oracle is a plain C++ restatement of the BSAM Fortran FAS multigrid
+ * hot path for the simple_cahn-hilliard problem module.  It exists so that
+ * tests, __graft_entry__.smoke() and bench.py's cpu_baseline leg can check
+ * the CUDA path; the product never links, loads or calls it.
+ *
+ * Parity pinning: the reference is Fortran 90, no Fortran compiler exists in
+ * this image, and the reference ships no tests or golden outputs.  Parity is
+ * UNPINNED against reference outputs; the restatement is checked by
+ * known-answer tests and invariants derived from the reference's formulas.
+ *
+ * Array layout (every array argument): Fortran column-major, i fastest, with
+ * the reference's bounds -- q(0:mx1+1, 0:mx2+1[, 0:mx3+1], 1:2) with the ghost
+ * ring, f(1:mx1, 1:mx2[, 1:mx3], 1:2) without it (lib/bsamstorage.f90:74-102).
+ */
+#ifndef BSAM_ORACLE_H
+#define BSAM_ORACLE_H
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+  int32_t ndims;            /* 2 or 3 */
+  int32_t mx[3];            /* root-level interior cells per dimension */
+  int32_t mthbc[6];         /* boundary code per face (1 Neumann, 10-99 user) */
+  int32_t minlevel;         /* <= 0, or 1 for the automatic choice */
+  int32_t nsmoothingpasses; /* nu of V(nu,nu) */
+  int32_t maxvcycles;
+  int32_t errortype;        /* only 1 is supported */
+  int32_t pad_;
+  double xlower[3], xupper[3];
+  double dt, qerrortol, alpha, eps;
+} orc_params;
+
+/* Uniform-grid time stepping (maxlevel = 0): restates BSAMSolver ->
+ * TakeTimeSteps -> MultigridIterations (lib/bsamroutines.f90:51-176,
+ * 582-789; lib/afasroutines.f90:38-106) for nsteps steps with eqfn = 1.
+ * q0: root q with ghost ring (the ring is recomputed by SetGhost).
+ * Outputs (any may be NULL):
+ *   q_steps       nsteps x size(q) -- root q (with ring) after each step
+ *   nvcycles      nsteps           -- V-cycles performed per step
+ *   resid_final   nsteps           -- last residual of each step
+ *   resid_trace   nsteps x maxvcycles (unused entries set to -1)
+ *   mass          nsteps           -- h^d * sum(phi) after each step
+ * Returns 0, or a negative code for invalid parameters.               */
+int orc_run_uniform(const orc_params* p, const double* q0, int nsteps,
+                    double* q_steps, int* nvcycles, double* resid_final,
+                    double* resid_trace, double* mass);
+
+/* Resolved minimum level for the parameters (lib/bsamroutines.f90:287-301). */
+int orc_minlevel(const orc_params* p);
+
+/* ---- leaf routines, for known-answer and fixture tests ---------------- */
+/* RelaxGrid2D/3D (problem.f90:164-215, 453-518): one colour pass in place.
+ * q: (0:mx+1)^d x 2, f: (1:mx)^d x 2.                                   */
+void orc_relax_grid(int ndims, const int* mx, double h, double dt,
+                    double alpha, double eps, int ipass, double* q,
+                    const double* f);
+/* Operator2D/3D (problem.f90:231-257, 534-561): res (1:mx)^d x 2.       */
+void orc_operator(int ndims, const int* mx, double h, double dt,
+                  double alpha, double eps, const double* q, double* res);
+/* Restriction2D/3D (gridutilities.f90:89-110, 406-433) of a (1:mx)^d x nv
+ * array into (1:mx/2)^d x nv.                                           */
+void orc_restriction(int ndims, const int* mx, int nv, const double* a,
+                     double* out);
+/* BiLin/TriLinProlongationP1 (gridutilities.f90:137-175, 474-529):
+ * a (0:cmx+1)^d x nv -> out (0:2cmx+1)^d x nv.                          */
+void orc_prolongation_p1(int ndims, const int* cmx, int nv, const double* a,
+                         double* out);
+/* SetBC2D/3D (boundary.f90:643-891) with the problem's UserBC2D/3D
+ * (problem.f90:646-756) on q (0:mx+1)^d x nv, in place.                 */
+int orc_setbc(int ndims, const int* mx, int nv, const int* mthbc, double* q);
+/* Source2D/3D (problem.f90:258-280, 562-585): f from qold.               */
+void orc_source(int ndims, const int* mx, double alpha, const double* qold,
+                double* f);
+/* Energy2D (problem.f90:330-361) of c (0:mx+1)^2.                        */
+double orc_energy2d(const int* mx, double h, double alpha, double eps,
+                    const double* c);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

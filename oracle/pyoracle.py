@@ -1,0 +1,180 @@
+"""ctypes bindings of the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg import
+this module.  See bsam_oracle.h for what the oracle restates and how far its
+parity is pinned.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = os.path.join(_HERE, "libbsam_oracle.so")
+
+
+class OrcParams(ctypes.Structure):
+    _fields_ = [
+        ("ndims", ctypes.c_int32), ("mx", ctypes.c_int32 * 3), ("mthbc", ctypes.c_int32 * 6),
+        ("minlevel", ctypes.c_int32), ("nsmoothingpasses", ctypes.c_int32),
+        ("maxvcycles", ctypes.c_int32), ("errortype", ctypes.c_int32), ("pad_", ctypes.c_int32),
+        ("xlower", ctypes.c_double * 3), ("xupper", ctypes.c_double * 3),
+        ("dt", ctypes.c_double), ("qerrortol", ctypes.c_double),
+        ("alpha", ctypes.c_double), ("eps", ctypes.c_double),
+    ]
+
+
+def build() -> str:
+    """Compile the oracle with its Makefile (no-op when up to date)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB):
+            build()
+        L = ctypes.CDLL(_LIB)
+        dp = ctypes.POINTER(ctypes.c_double)
+        ip = ctypes.POINTER(ctypes.c_int)
+        L.orc_run_uniform.argtypes = [ctypes.POINTER(OrcParams), dp, ctypes.c_int, dp, ip, dp, dp, dp]
+        L.orc_run_uniform.restype = ctypes.c_int
+        L.orc_minlevel.argtypes = [ctypes.POINTER(OrcParams)]
+        L.orc_relax_grid.argtypes = [ctypes.c_int, ip, ctypes.c_double, ctypes.c_double,
+                                     ctypes.c_double, ctypes.c_double, ctypes.c_int, dp, dp]
+        L.orc_operator.argtypes = [ctypes.c_int, ip, ctypes.c_double, ctypes.c_double,
+                                   ctypes.c_double, ctypes.c_double, dp, dp]
+        L.orc_restriction.argtypes = [ctypes.c_int, ip, ctypes.c_int, dp, dp]
+        L.orc_prolongation_p1.argtypes = [ctypes.c_int, ip, ctypes.c_int, dp, dp]
+        L.orc_setbc.argtypes = [ctypes.c_int, ip, ctypes.c_int, ip, dp]
+        L.orc_setbc.restype = ctypes.c_int
+        L.orc_source.argtypes = [ctypes.c_int, ip, ctypes.c_double, dp, dp]
+        L.orc_energy2d.argtypes = [ip, ctypes.c_double, ctypes.c_double, ctypes.c_double, dp]
+        L.orc_energy2d.restype = ctypes.c_double
+        _lib = L
+    return _lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _ip(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+
+
+def params_of(prob) -> OrcParams:
+    p = OrcParams()
+    p.ndims = prob.ndims
+    for n in range(3):
+        p.mx[n] = prob.mx[n] if n < prob.ndims else 1
+        p.xlower[n] = 0.0
+        p.xupper[n] = 1.0
+    for f in range(6):
+        p.mthbc[f] = prob.mthbc[f]
+    p.minlevel = prob.minlevel
+    p.nsmoothingpasses = prob.nsmoothingpasses
+    p.maxvcycles = prob.maxvcycles
+    p.errortype = 1
+    p.dt = prob.dt
+    p.qerrortol = prob.qerrortol
+    p.alpha = prob.alpha
+    p.eps = prob.eps
+    return p
+
+
+def run_uniform(prob, nsteps=None, keep_steps=True, q0=None):
+    """Run the oracle time loop.  Returns a dict with q per step (Fortran
+    layout with ring), V-cycle counts, final residuals, traces and mass."""
+    L = lib()
+    nsteps = prob.nsteps if nsteps is None else nsteps
+    p = params_of(prob)
+    q0 = prob.q0() if q0 is None else q0
+    q0 = np.asfortranarray(q0, dtype=np.float64)
+    qsize = q0.size
+    q_steps = np.zeros((nsteps,) + q0.shape, dtype=np.float64) if keep_steps else None
+    buf = np.zeros(nsteps * qsize) if keep_steps else None
+    nvc = np.zeros(nsteps, dtype=np.int32)
+    rfin = np.zeros(nsteps)
+    tr = np.zeros(nsteps * prob.maxvcycles)
+    mass = np.zeros(nsteps)
+    rc = L.orc_run_uniform(ctypes.byref(p), _dp(q0.ravel(order="F")), nsteps,
+                           _dp(buf) if keep_steps else None, _ip(nvc), _dp(rfin), _dp(tr), _dp(mass))
+    if rc != 0:
+        raise RuntimeError(f"orc_run_uniform failed: {rc}")
+    if keep_steps:
+        for s in range(nsteps):
+            q_steps[s] = buf[s * qsize:(s + 1) * qsize].reshape(q0.shape, order="F")
+    return {"q": q_steps, "nvcycles": nvc, "residual": rfin,
+            "trace": tr.reshape(nsteps, prob.maxvcycles), "mass": mass}
+
+
+def relax_grid(ndims, mx, h, dt, alpha, eps, ipass, q, f):
+    q = np.array(q, dtype=np.float64, order="F", copy=True)
+    f = np.asfortranarray(f, dtype=np.float64)
+    mxa = np.array(list(mx) + [1] * (3 - len(mx)), dtype=np.int32)
+    lib().orc_relax_grid(ndims, _ip(mxa), h, dt, alpha, eps, ipass,
+                         q.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), _dp(f))
+    return q
+
+
+def operator(ndims, mx, h, dt, alpha, eps, q):
+    q = np.asfortranarray(q, dtype=np.float64)
+    mxa = np.array(list(mx) + [1] * (3 - len(mx)), dtype=np.int32)
+    res = np.zeros(tuple(mx[:ndims]) + (2,), order="F")
+    lib().orc_operator(ndims, _ip(mxa), h, dt, alpha, eps, _dp(q), _dp(res))
+    return res
+
+
+def restriction(ndims, a):
+    a = np.asfortranarray(a, dtype=np.float64)
+    mx = a.shape[:ndims]
+    nv = a.shape[ndims]
+    mxa = np.array(list(mx) + [1] * (3 - ndims), dtype=np.int32)
+    out = np.zeros(tuple(m // 2 for m in mx) + (nv,), order="F")
+    lib().orc_restriction(ndims, _ip(mxa), nv, _dp(a), _dp(out))
+    return out
+
+
+def prolongation_p1(ndims, a):
+    a = np.asfortranarray(a, dtype=np.float64)
+    cmx = [s - 2 for s in a.shape[:ndims]]
+    nv = a.shape[ndims]
+    ca = np.array(cmx + [1] * (3 - ndims), dtype=np.int32)
+    out = np.zeros(tuple(2 * c + 2 for c in cmx) + (nv,), order="F")
+    lib().orc_prolongation_p1(ndims, _ip(ca), nv, _dp(a), _dp(out))
+    return out
+
+
+def setbc(ndims, q, mthbc):
+    q = np.array(q, dtype=np.float64, order="F", copy=True)
+    mx = [s - 2 for s in q.shape[:ndims]]
+    nv = q.shape[ndims]
+    mxa = np.array(mx + [1] * (3 - ndims), dtype=np.int32)
+    bc = np.array(list(mthbc) + [1] * (6 - len(mthbc)), dtype=np.int32)
+    rc = lib().orc_setbc(ndims, _ip(mxa), nv, _ip(bc), _dp(q))
+    if rc:
+        raise ValueError("unsupported boundary code")
+    return q
+
+
+def source(ndims, alpha, qold):
+    qold = np.asfortranarray(qold, dtype=np.float64)
+    mx = [s - 2 for s in qold.shape[:ndims]]
+    mxa = np.array(mx + [1] * (3 - ndims), dtype=np.int32)
+    f = np.zeros(tuple(mx) + (2,), order="F")
+    lib().orc_source(ndims, _ip(mxa), alpha, _dp(qold), _dp(f))
+    return f
+
+
+def energy2d(h, alpha, eps, c):
+    c = np.asfortranarray(c, dtype=np.float64)
+    mxa = np.array([c.shape[0] - 2, c.shape[1] - 2, 1], dtype=np.int32)
+    return lib().orc_energy2d(_ip(mxa), h, alpha, eps, _dp(c))

@@ -1,0 +1,98 @@
+"""FP64 parity of the CUDA path (through the C ABI) with the CPU oracle.
+
+Bar (FP64 form): per time step, phi and mu within 1e-11 relative (max norm)
+of the oracle, the same V-cycle count, and residuals within 1e-9 relative
+(the norm's summation order differs: the GPU reduces in a fixed tree).
+"""
+import numpy as np
+import pytest
+
+import bsam_b200 as B
+from bsam_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-11
+
+
+def relerr(a, b):
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def compare(oracle, prob, nsteps):
+    ref = oracle.run_uniform(prob, nsteps=nsteps)
+    with B.Solver(prob) as s:
+        got = s.run(nsteps)
+    inner = tuple(slice(1, m + 1) for m in prob.mx[:prob.ndims])
+    for st in range(nsteps):
+        for v in range(2):
+            e = relerr(got["q"][st][inner + (v,)], ref["q"][st][inner + (v,)])
+            assert e <= RTOL, (st, v, e)
+        # the ghost ring too (SetGhost semantics incl. edges and corners)
+        e = relerr(got["q"][st], ref["q"][st])
+        assert e <= RTOL, (st, "ring", e)
+    assert np.array_equal(got["nvcycles"], ref["nvcycles"]), (got["nvcycles"], ref["nvcycles"])
+    np.testing.assert_allclose(got["residual"], ref["residual"], rtol=1e-9)
+    np.testing.assert_allclose(got["mass"], ref["mass"], rtol=1e-13)
+    return got, ref
+
+
+def test_config1_small(gpu_lib, oracle):
+    got, ref = compare(oracle, W.config1(nsteps=4, n=32), 4)
+    # same arithmetic in the same order: expect bit-identical fields
+    assert np.array_equal(got["q"], ref["q"])
+
+
+def test_config1_full(gpu_lib, oracle):
+    compare(oracle, W.config1(nsteps=20), 20)
+
+
+def test_odd_coarsest_96(gpu_lib, oracle):
+    compare(oracle, W.config1(nsteps=3, n=96), 3)
+
+
+def test_3d_small(gpu_lib, oracle):
+    got, ref = compare(oracle, W.config3(nsteps=2, n=32), 2)
+    assert np.array_equal(got["q"], ref["q"])
+
+
+def test_3d_64(gpu_lib, oracle):
+    compare(oracle, W.config3(nsteps=2, n=64), 2)
+
+
+def test_user_bc_2d(gpu_lib, oracle):
+    prob = W.config1(nsteps=3, n=64)
+    prob.mthbc = (10, 10, 12, 11, 1, 1)
+    compare(oracle, prob, 3)
+
+
+def test_user_bc_3d(gpu_lib, oracle):
+    prob = W.config3(nsteps=2, n=16)
+    prob.mthbc = (10, 1, 1, 10, 10, 1)
+    compare(oracle, prob, 2)
+
+
+def test_rectangular_2d(gpu_lib, oracle):
+    # 128 x 64 root (the shipped example's shape), explicit minlevel = -5.
+    prob = W.config1(nsteps=2, n=64)
+    prob.mx = (128, 64, 1)
+    prob.c0 = 0.5 + 0.025 * W.uniform(11, 128 * 64, -1.0, 1.0)
+    prob.minlevel = -5
+    compare(oracle, prob, 2)
+
+
+def test_residual_trace_matches(gpu_lib, oracle):
+    prob = W.config1(nsteps=1, n=64)
+    ref = oracle.run_uniform(prob, nsteps=1)
+    with B.Solver(prob) as s:
+        s.step()
+        tr = s.trace()
+    want = ref["trace"][0][: len(tr)]
+    np.testing.assert_allclose(tr, want, rtol=1e-9)
+
+
+def test_put_get_roundtrip(gpu_lib):
+    prob = W.config3(nsteps=1, n=8)
+    q = prob.q0()
+    with B.Solver(prob) as s:
+        assert np.array_equal(s.get_q(), q)

@@ -54,10 +54,11 @@ class Problem:
     minlevel: int = 1          # 1 = automatic (lib/bsamroutines.f90:287-301)
     mthbc: tuple = (1, 1, 1, 1, 1, 1)
     c0: np.ndarray | None = None   # interior composition, Fortran order
+    xupper: tuple = (1.0, 1.0, 1.0)  # domain [0, xupper]; dx must be equal in all dims
 
     @property
     def h(self) -> float:
-        return 1.0 / self.mx[0]
+        return self.xupper[0] / self.mx[0]
 
     def q0(self) -> np.ndarray:
         """Root q with ghost ring, Fortran layout (0:mx+1)^d x 2."""
@@ -100,6 +101,15 @@ def initial_q(ndims, mx, c0, h, eps, alpha) -> np.ndarray:
         lap = lap + c[tuple(p)] + c[tuple(m)]
     mu = np.zeros(shape, order="F")
     mu[inner] = _dfc(c[inner], alpha) - _dfe(c[inner], alpha) - (eps * eps / (h * h)) * lap
+    for d in range(ndims):
+        lo = [slice(None)] * ndims
+        hi = [slice(None)] * ndims
+        lo[d], hi[d] = 0, shape[d] - 1
+        s_lo = [slice(None)] * ndims
+        s_hi = [slice(None)] * ndims
+        s_lo[d], s_hi[d] = 1, shape[d] - 2
+        mu[tuple(lo)] = mu[tuple(s_lo)]
+        mu[tuple(hi)] = mu[tuple(s_hi)]
     q = np.zeros(shape + (2,), order="F")
     q[..., 0] = c
     q[..., 1] = mu

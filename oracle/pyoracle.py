@@ -76,7 +76,7 @@ def params_of(prob) -> OrcParams:
     for n in range(3):
         p.mx[n] = prob.mx[n] if n < prob.ndims else 1
         p.xlower[n] = 0.0
-        p.xupper[n] = 1.0
+        p.xupper[n] = prob.xupper[n]
     for f in range(6):
         p.mthbc[f] = prob.mthbc[f]
     p.minlevel = prob.minlevel

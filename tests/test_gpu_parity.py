@@ -76,6 +76,7 @@ def test_rectangular_2d(gpu_lib, oracle):
     # 128 x 64 root (the shipped example's shape), explicit minlevel = -5.
     prob = W.config1(nsteps=2, n=64)
     prob.mx = (128, 64, 1)
+    prob.xupper = (1.0, 0.5, 1.0)
     prob.c0 = 0.5 + 0.025 * W.uniform(11, 128 * 64, -1.0, 1.0)
     prob.minlevel = -5
     compare(oracle, prob, 2)
@@ -91,8 +92,11 @@ def test_residual_trace_matches(gpu_lib, oracle):
     np.testing.assert_allclose(tr, want, rtol=1e-9)
 
 
-def test_put_get_roundtrip(gpu_lib):
-    prob = W.config3(nsteps=1, n=8)
-    q = prob.q0()
+@pytest.mark.parametrize("nd", [2, 3])
+def test_put_get_roundtrip(gpu_lib, nd):
+    prob = W.config3(nsteps=1, n=8) if nd == 3 else W.config1(nsteps=1, n=12)
+    rng = np.random.default_rng(nd)
     with B.Solver(prob) as s:
+        q = np.asfortranarray(rng.standard_normal(s.qshape))
+        s.put_q(q)
         assert np.array_equal(s.get_q(), q)

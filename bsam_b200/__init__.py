@@ -127,7 +127,7 @@ def host_grid(prob) -> HostGrid:
     for n in range(3):
         g.mx[n] = prob.mx[n] if n < prob.ndims else 1
         g.xlower[n] = 0.0
-        g.xupper[n] = 1.0
+        g.xupper[n] = prob.xupper[n]
     for f in range(6):
         g.mthbc[f] = prob.mthbc[f]
     g.minlevel = prob.minlevel

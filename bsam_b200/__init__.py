@@ -62,6 +62,7 @@ ABI_SYMBOLS = (
     "bsam_gpu_residual_trace", "bsam_gpu_mass", "bsam_gpu_destroy", "bsam_gpu_strerror",
     "bsam_gpu_last_error", "bsam_gpu_get_stream", "bsam_gpu_profile", "bsam_gpu_get_stats",
     "bsam_host_levels", "bsam_host_build_uniform", "bsam_host_take_time_steps",
+    "bsam_gpu_resid_norm_noalloc",
 )
 
 
@@ -97,6 +98,9 @@ def lib():
     L.bsam_gpu_get_stream.argtypes = [vp, ctypes.POINTER(vp)]
     L.bsam_gpu_profile.argtypes = [vp, ctypes.c_int]
     L.bsam_gpu_get_stats.argtypes = [vp, ctypes.POINTER(Stats)]
+    L.bsam_gpu_resid_norm_noalloc.argtypes = [
+        ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int32), ctypes.c_double,
+        ctypes.c_double, ctypes.c_double, ctypes.c_double, vp, vp, vp, vp]
     L.bsam_host_levels.argtypes = [ctypes.POINTER(HostGrid)]
     L.bsam_host_build_uniform.argtypes = [ctypes.POINTER(HostGrid), ctypes.POINTER(PatchDesc),
                                           ctypes.c_int, ip]

@@ -14,7 +14,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libbsam_gpu.so")
-SOURCES = ["bsam_gpu.cu", "bsam_host.cpp"]
+SOURCES = ["bsam_gpu.cu", "bsam_host.cpp", "bsam_noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

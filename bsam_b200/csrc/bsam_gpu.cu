@@ -211,6 +211,7 @@ const char* bsam_gpu_strerror(int code) {
     case BSAM_ERR_UNSUPPORTED: return "configuration not supported";
     case BSAM_ERR_NODEVICE: return "no usable CUDA device";
     case BSAM_ERR_DIVERGED: return "non-finite residual";
+    case BSAM_ERR_TOO_LARGE: return "patch exceeds the static scratch limit of the no-alloc entry point";
     default: return "unknown status";
   }
 }

@@ -29,7 +29,8 @@ enum {
   BSAM_ERR_STATE = -4,      /* call out of order (e.g. no hierarchy yet) */
   BSAM_ERR_UNSUPPORTED = -5,/* configuration not supported by this build */
   BSAM_ERR_NODEVICE = -6,   /* no CUDA device / kernels unavailable */
-  BSAM_ERR_DIVERGED = -7    /* non-finite residual detected */
+  BSAM_ERR_DIVERGED = -7,   /* non-finite residual detected */
+  BSAM_ERR_TOO_LARGE = -8   /* patch exceeds the static scratch of *_noalloc */
 };
 
 /* Field selectors for put/get (the nodeinfo components of
@@ -137,6 +138,33 @@ const char* bsam_gpu_strerror(int code);
 /* Detail message of the last failing call on this handle (valid until the
  * next call on the handle). */
 const char* bsam_gpu_last_error(bsam_gpu* h);
+
+/* Residual norm of one uniform patch, allocating no device memory.
+ *
+ * No counterpart in the reference.  It is for callers that cannot allocate
+ * device memory at the point where they need the norm: a host that has given
+ * all device memory to its own pool (a Fortran code's preallocated arena,
+ * PyTorch's caching allocator) or a step loop that must not pay the implicit
+ * device synchronisation of cudaMalloc/cudaFree.  It returns the same number
+ * as the final residual of bsam_gpu_multigrid_iterations (ErrorAFAS with
+ * errortype 1, lib/afasroutines.f90:108-221) for fields held by the caller:
+ *   q    device pointer, q(0:mx1+1, 0:mx2+1[, 0:mx3+1], 1:2), ghost ring set
+ *   f    device pointer, f(1:mx1, 1:mx2[, 1:mx3], 1:2)
+ *   out  device pointer to 2 doubles: out[0] = residual, out[1] = sum of rf^2,
+ *        written by a kernel on `stream` (NULL = legacy default stream);
+ *        synchronise the stream before reading them.
+ * Reductions go through one fixed scratch array compiled into the library
+ * (about 512 KiB held on every GPU that loads it until the process exits),
+ * so the patch may span at most BSAM_NOALLOC_MAX_TILES tiles of 64 x 4 x 1
+ * cells (16,777,216 cells when mx1 is a multiple of 64 and mx2 of 4); larger
+ * patches return BSAM_ERR_TOO_LARGE.  The first call on a device looks up the
+ * scratch array's device address with cudaGetSymbolAddress, so make that
+ * first call before capturing any stream.  All calls share the scratch: calls
+ * whose kernels overlap on the GPU race and give wrong results. */
+#define BSAM_NOALLOC_MAX_TILES 65536
+int bsam_gpu_resid_norm_noalloc(int device, int ndims, const int32_t* mx, double dx, double dt,
+                                double eps, double alpha, const double* q, const double* f,
+                                double* out, void* stream);
 
 #ifdef __cplusplus
 }

@@ -62,8 +62,14 @@ ABI_SYMBOLS = (
     "bsam_gpu_residual_trace", "bsam_gpu_mass", "bsam_gpu_destroy", "bsam_gpu_strerror",
     "bsam_gpu_last_error", "bsam_gpu_get_stream", "bsam_gpu_profile", "bsam_gpu_get_stats",
     "bsam_host_levels", "bsam_host_build_uniform", "bsam_host_take_time_steps",
-    "bsam_gpu_resid_norm_noalloc",
+    "bsam_gpu_resid_norm_noalloc", "bsam_gpu_set_tuning",
 )
+
+
+class Tuning(ctypes.Structure):
+    _fields_ = [("fuse_smoother", ctypes.c_int32), ("fuse_min_n", ctypes.c_int32),
+                ("chunk", ctypes.c_int32), ("bottom_cells", ctypes.c_int32),
+                ("reserved", ctypes.c_int32 * 4)]
 
 
 class Stats(ctypes.Structure):
@@ -101,6 +107,7 @@ def lib():
     L.bsam_gpu_resid_norm_noalloc.argtypes = [
         ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int32), ctypes.c_double,
         ctypes.c_double, ctypes.c_double, ctypes.c_double, vp, vp, vp, vp]
+    L.bsam_gpu_set_tuning.argtypes = [vp, ctypes.POINTER(Tuning)]
     L.bsam_host_levels.argtypes = [ctypes.POINTER(HostGrid)]
     L.bsam_host_build_uniform.argtypes = [ctypes.POINTER(HostGrid), ctypes.POINTER(PatchDesc),
                                           ctypes.c_int, ip]
@@ -160,7 +167,8 @@ class Solver:
     one TakeTimeSteps iteration (CopyQToQold + MultigridIterations).
     """
 
-    def __init__(self, prob, device: int = 0, precision: int = PREC_FP64, q0=None):
+    def __init__(self, prob, device: int = 0, precision: int = PREC_FP64, q0=None,
+                 fuse: int = 0, fuse_min_n: int = 64, chunk: int = 0, bottom_cells: int = 0):
         L = lib()
         self.prob = prob
         rp = RunParams(ndims=prob.ndims, nrvars=2, mbc=1, maux=0,
@@ -171,6 +179,9 @@ class Solver:
         _check(L.bsam_gpu_create(ctypes.byref(h), device, ctypes.byref(rp)), what="bsam_gpu_create")
         self.h = h
         try:
+            t = Tuning(fuse_smoother=fuse, fuse_min_n=fuse_min_n, chunk=chunk,
+                       bottom_cells=bottom_cells)
+            _check(L.bsam_gpu_set_tuning(h, ctypes.byref(t)), h, "bsam_gpu_set_tuning")
             self.patches, self.npatch = build_uniform(prob)
             _check(L.bsam_gpu_set_hierarchy(h, self.npatch, self.patches, 0), h,
                    "bsam_gpu_set_hierarchy")

@@ -21,6 +21,8 @@
 #include "../../include/bsam_gpu.h"
 #include "bsam_types.h"
 #include "kernels.cuh"
+#include "smooth_fused.cuh"
+#include "bottom.cuh"
 
 using namespace bsam;
 
@@ -33,6 +35,9 @@ struct LevelPlan {
   int nfine = 0;
   Item* d_coarse = nullptr;  // tiles over each patch's footprint in its parent
   int ncoarse = 0;
+  Item* d_fused = nullptr;   // fused-stage tiles (tile x, tile y, z chunk)
+  int nfused = 0;
+  bool fused = false;
 };
 
 }  // namespace
@@ -53,6 +58,13 @@ struct bsam_gpu {
   Item* d_items = nullptr;
   double* d_partials = nullptr;
   int max_items = 0;
+  int* d_err = nullptr;  // kernel error flag (bounded waits that gave up)
+  // Fused stages off by default: at L2-resident sizes the per-pass kernels
+  // are faster (see the profiles); tests and tuning switch them on.
+  bsam_tuning tuning{0, 64, 0, 0, {0, 0, 0, 0}};
+  int bottom_level = -1000;  // levels <= this run inside k_bottom
+  int* d_tops = nullptr;     // top patch of each k_bottom chain
+  int ntops = 0;
   DevStatus* d_status = nullptr;
   DevStatus* h_status = nullptr;  // pinned
   std::vector<double> trace;
@@ -134,20 +146,39 @@ void launch_relax(bsam_gpu* h, const LevelPlan& L, int color) {
 
 int ghost_level(bsam_gpu* h, int level);
 
-void relax_level(bsam_gpu* h, int level) {
+// LevelRelax (afas:523-547).  dir selects the buffers of a fused level:
+// 0 = pre-smoothing (q -> qb), 1 = post-smoothing (qb -> q).
+void relax_level(bsam_gpu* h, int level, int dir) {
   const LevelPlan& L = plan(h, level);
   stage_begin(h, level);
-  for (int pass = 0; pass < h->rp.nsmoothingpasses; ++pass)
-    for (int color = 0; color < 2; ++color) {
-      if (h->rp.ndims == 2) launch_relax<2>(h, L, color);
-      else launch_relax<3>(h, L, color);
-      ++h->stats.launches;
-    }
+  if (L.fused) {
+    k_smooth3_fused<double><<<L.nfused, Fused3<double>::THREADS, Fused3<double>::SMEM,
+                              h->stream>>>(h->d_patches, L.d_fused, dir, 0, h->d_err);
+    ++h->stats.launches;
+  } else {
+    for (int pass = 0; pass < h->rp.nsmoothingpasses; ++pass)
+      for (int color = 0; color < 2; ++color) {
+        if (h->rp.ndims == 2) launch_relax<2>(h, L, color);
+        else launch_relax<3>(h, L, color);
+        ++h->stats.launches;
+      }
+  }
   stage_end(h, level);
 }
 
 void vcycle(bsam_gpu* h, int level) {
-  relax_level(h, level);  // LevelRelax (afas:499)
+  if (level == h->bottom_level) {
+    // AFASVcycle(level) down to the coarsest level in one launch (bottom.cuh).
+    if (h->rp.ndims == 2)
+      k_bottom<double, 2><<<h->ntops, BOTTOM_THREADS, 0, h->stream>>>(h->d_patches, h->d_tops,
+                                                                      h->rp.nsmoothingpasses);
+    else
+      k_bottom<double, 3><<<h->ntops, BOTTOM_THREADS, 0, h->stream>>>(h->d_patches, h->d_tops,
+                                                                      h->rp.nsmoothingpasses);
+    ++h->stats.launches;
+    return;
+  }
+  relax_level(h, level, 0);  // LevelRelax (afas:499)
   if (level > h->minlevel) {
     const LevelPlan& L = plan(h, level);
     const dim3 b = block_dim();
@@ -165,7 +196,7 @@ void vcycle(bsam_gpu* h, int level) {
     else
       k_correct<double, 3><<<L.nfine, b, 0, h->stream>>>(h->d_patches, L.d_fine);
     ++h->stats.launches;
-    relax_level(h, level);  // afas:517
+    relax_level(h, level, 1);  // afas:517
   }
 }
 
@@ -243,6 +274,7 @@ int bsam_gpu_create(bsam_gpu** out, int device, const bsam_run_params* p) {
     return BSAM_ERR_CUDA;
   }
   cudaMemset(h->d_status, 0, sizeof(DevStatus));
+  h->d_err = &h->d_status->kerr;
   *out = h;
   return BSAM_OK;
 }
@@ -253,6 +285,9 @@ static void free_hierarchy(bsam_gpu* h) {
     L.d_coarse = nullptr;
   }
   if (h->d_items) cudaFree(h->d_items);
+  if (h->d_tops) cudaFree(h->d_tops);
+  h->d_tops = nullptr;
+  h->ntops = 0;
   if (h->d_arena) cudaFree(h->d_arena);
   if (h->d_patches) cudaFree(h->d_patches);
   if (h->d_partials) cudaFree(h->d_partials);
@@ -281,6 +316,26 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
   h->minlevel = minlevel;
   h->finestlevel = finestlevel;
   h->levels.assign(finestlevel - minlevel + 1, LevelPlan{});
+  // Bottom level: the finest level such that it and every coarser level hold
+  // at most bottom_cells cells per patch (uniform hierarchies only).
+  h->bottom_level = -1000;
+  {
+    const int bmax = h->tuning.bottom_cells == 0 ? BOTTOM_MAX_CELLS : h->tuning.bottom_cells;
+    if (bmax > 0 && finestlevel == 0) {
+      for (int l = minlevel; l <= finestlevel; ++l) {
+        bool small = true;
+        for (int p = 0; p < npatch; ++p)
+          if (patches[p].level == l) {
+            int64_t c = 1;
+            for (int n = 0; n < nd; ++n) c *= patches[p].mx[n];
+            small = small && c <= bmax;
+          }
+        if (!small) break;
+        h->bottom_level = l;
+      }
+      if (h->bottom_level - minlevel + 1 > BOTTOM_MAX_DEPTH) h->bottom_level = -1000;
+    }
+  }
   for (int l = minlevel; l <= finestlevel; ++l) plan(h, l).level = l;
   h->desc.assign(patches, patches + npatch);
   h->hp.assign(npatch, DevPatch{});
@@ -334,19 +389,40 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
       if (rule == BC_NONE) P.wt = 0;
     }
     if (!P.wt) return fail(h, BSAM_ERR_UNSUPPORTED, "internal faces need AMR support");
-    // Layout (FP64): rows aligned to 128 bytes.
+    // Fused stages: 3D levels with a parent (the coarsest level relaxes once
+    // per V-cycle and keeps the in-place path), all faces physical.
+    const int fmin = std::max(8, h->tuning.fuse_min_n);
+    P.fused = (h->tuning.fuse_smoother != 0 && nd == 3 && d.parent >= 0 && P.wt &&
+               d.level > h->bottom_level &&
+               P.n[0] >= fmin && P.n[1] >= fmin && P.n[2] >= fmin)
+                  ? 1
+                  : 0;
+    if (P.fused) {
+      const int tiles = ((P.n[0] + Fused3<double>::TX - 1) / Fused3<double>::TX) *
+                        ((P.n[1] + Fused3<double>::TY - 1) / Fused3<double>::TY);
+      int chunk = h->tuning.chunk;
+      if (chunk <= 0) {
+        // About one CTA per SM, chunks of at least 16 planes.
+        const int nchunk = std::max(1, std::min(148 / std::max(tiles, 1), P.n[2] / 16));
+        chunk = (P.n[2] + nchunk - 1) / nchunk;
+      }
+      P.zchunk = std::max(1, std::min(chunk, P.n[2]));
+    }
+    // Layout (FP64): rows aligned to 128 bytes.  The slack after the last row
+    // keeps the fused kernel's halo'd row copies inside the allocation.
     const int64_t A = 128 / sizeof(double), lead = A - 1;
     P.sy = roundup(lead + P.n[0] + 2, A);
     P.sz = nd == 3 ? P.sy * (P.n[1] + 2) : 0;
     const int64_t vol = nd == 3 ? P.sz * (P.n[2] + 2) : P.sy * (P.n[1] + 2);
-    h->field_elems[p] = roundup(lead + vol, 32);
+    h->field_elems[p] = roundup(lead + vol + 64, 32);
     offs[p] = total;
     const bool parent_of_any = [&] {
       for (int c = 0; c < npatch; ++c)
         if (patches[c].parent == p) return true;
       return false;
     }();
-    const int nfields = 2 /*q*/ + 2 /*f*/ + 2 /*qold*/ + (parent_of_any ? 2 : 0);
+    const int nfields = 2 /*q*/ + 2 /*f*/ + 2 /*qold*/ + (parent_of_any ? 2 : 0) +
+                        (P.fused ? 2 : 0);
     total += (size_t)h->field_elems[p] * nfields * sizeof(double);
     // Problem constants (problem.f90:183-187): h2 = h*h; dt/h2; eps2/h2; 2d*eps2/h2.
     P.h = d.dx;
@@ -381,10 +457,15 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
       P.qs[0] = next();
       P.qs[1] = next();
     }
+    if (P.fused) {
+      P.qb[0] = next();
+      P.qb[1] = next();
+    }
   }
   // Work lists.
   std::vector<Item> all;
-  std::vector<std::pair<int, int>> spans_fine(h->levels.size()), spans_coarse(h->levels.size());
+  std::vector<std::pair<int, int>> spans_fine(h->levels.size()), spans_coarse(h->levels.size()),
+      spans_fused(h->levels.size());
   for (size_t li = 0; li < h->levels.size(); ++li) {
     LevelPlan& L = h->levels[li];
     int s = (int)all.size();
@@ -394,6 +475,23 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
     for (int p : L.patches)
       if (h->hp[p].parent >= 0) tiles_for(p, h->hp[p].cn, nd, all);
     spans_coarse[li] = {s, (int)all.size() - s};
+    // A level runs fused stages only when every patch on it does.
+    L.fused = !L.patches.empty();
+    for (int p : L.patches) L.fused = L.fused && h->hp[p].fused;
+    if (!L.fused)
+      for (int p : L.patches) h->hp[p].fused = 0;
+    s = (int)all.size();
+    if (L.fused)
+      for (int p : L.patches) {
+        const DevPatch& P = h->hp[p];
+        const int tx = (P.n[0] + Fused3<double>::TX - 1) / Fused3<double>::TX;
+        const int ty = (P.n[1] + Fused3<double>::TY - 1) / Fused3<double>::TY;
+        const int tz = (P.n[2] + P.zchunk - 1) / P.zchunk;
+        for (int z = 0; z < tz; ++z)
+          for (int y = 0; y < ty; ++y)
+            for (int x = 0; x < tx; ++x) all.push_back(Item{p, x, y, z});
+      }
+    spans_fused[li] = {s, (int)all.size() - s};
   }
   CU(cudaMalloc(&h->d_items, all.size() * sizeof(Item)));
   CU(cudaMemcpyAsync(h->d_items, all.data(), all.size() * sizeof(Item), cudaMemcpyHostToDevice,
@@ -405,9 +503,21 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
     L.nfine = spans_fine[li].second;
     L.d_coarse = h->d_items + spans_coarse[li].first;
     L.ncoarse = spans_coarse[li].second;
+    L.d_fused = h->d_items + spans_fused[li].first;
+    L.nfused = spans_fused[li].second;
     h->max_items = std::max(h->max_items, L.nfine);
   }
+  CU(cudaFuncSetAttribute(k_smooth3_fused<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)Fused3<double>::SMEM));
   CU(cudaMalloc(&h->d_partials, sizeof(double) * h->max_items));
+  if (h->bottom_level >= minlevel) {
+    std::vector<int> tops = plan(h, h->bottom_level).patches;
+    h->ntops = (int)tops.size();
+    CU(cudaMalloc(&h->d_tops, sizeof(int) * tops.size()));
+    CU(cudaMemcpyAsync(h->d_tops, tops.data(), sizeof(int) * tops.size(),
+                       cudaMemcpyHostToDevice, h->stream));
+  }
+  CU(cudaMemsetAsync(h->d_err, 0, sizeof(int), h->stream));
   CU(cudaMalloc(&h->d_patches, sizeof(DevPatch) * npatch));
   CU(cudaMemcpyAsync(h->d_patches, h->hp.data(), sizeof(DevPatch) * npatch,
                      cudaMemcpyHostToDevice, h->stream));
@@ -536,6 +646,12 @@ int bsam_gpu_multigrid_iterations(bsam_gpu* h, int* nvcycles, double* residual, 
     CU(cudaStreamSynchronize(h->stream));
     drain_events(h);
     res = h->h_status->residual;
+    if (h->h_status->kerr) {
+      if (nvcycles) *nvcycles = it;
+      if (residual) *residual = res;
+      if (converged) *converged = 0;
+      return fail(h, BSAM_ERR_CUDA, "a fused smoothing stage timed out waiting for its copies");
+    }
     h->trace.push_back(res);
     if (!std::isfinite(res)) {
       if (nvcycles) *nvcycles = it;
@@ -580,6 +696,13 @@ int bsam_gpu_mass(bsam_gpu* h, double* mass) {
                      h->stream));
   CU(cudaStreamSynchronize(h->stream));
   *mass = h->h_status->mass;
+  return BSAM_OK;
+}
+
+int bsam_gpu_set_tuning(bsam_gpu* h, const bsam_tuning* t) {
+  if (!h || !t) return BSAM_ERR_ARG;
+  if (t->fuse_smoother < -1 || t->fuse_smoother > 1 || t->chunk < 0) return BSAM_ERR_ARG;
+  h->tuning = *t;
   return BSAM_OK;
 }
 

@@ -35,10 +35,13 @@ struct DevPatch {
   int32_t wt;         // 1: every face physical -> kernels write ghosts through
   int32_t prec;       // PREC_*
   int32_t problem;    // problem (batch slot) this patch belongs to
+  int32_t fused;      // 1: smoothing stages run the fused kernel (q -> qb -> q)
+  int32_t zchunk;     // fused kernel: planes (3D) / rows (2D) per streaming chunk
   int32_t pad_;
   int64_t sy, sz;     // element strides of j and k
   // Base pointers of element (0,0,0), the low ghost corner, per component.
-  void* q[2];         // solution (phi, mu), with ghost ring
+  void* q[2];         // solution (phi, mu), with ghost ring: the state between stages
+  void* qb[2];        // second buffer of fused levels: the pre-smoothed state
   void* f[2];         // right-hand side (source / FAS load), interior used
   void* qs[2];        // snapshot of q after restriction (the children's qc)
   void* qo[2];        // qold
@@ -62,6 +65,8 @@ struct DevStatus {
   double mass;
   uint32_t ticket;     // last-block-done counter of the reductions
   int32_t converged;
+  int32_t kerr;        // nonzero: a kernel's bounded wait gave up (see smooth_fused.cuh)
+  int32_t pad_;
 };
 
 }  // namespace bsam

@@ -1,18 +1,20 @@
 // kernels.cuh -- FAS V-cycle kernels over the device patch table.
 //
-// One kernel per reference routine on the hot path.  Each launch takes a
-// work list of Items (patch, tile) so that a single launch covers every patch
-// of a level.  A CTA is 32 x TILE_Y threads; every thread owns a pair of
-// adjacent cells in x (one red, one black), which keeps warps on 64
-// contiguous cells of a row (coalesced 8-byte loads).
+// One per-cell device function per reference routine on the hot path, and
+// two ways of mapping cells to threads:
+//  * grid kernels (k_*) take a work list of Items (patch, tile) so that one
+//    launch covers every patch of a level.  A CTA is 32 x TILE_Y threads;
+//    every thread owns a pair of adjacent cells in x (one red, one black),
+//    which keeps warps on 64 contiguous cells of a row;
+//  * block loops (bottom.cuh) walk all cells of a small patch with one CTA.
 //
 // Ghost cells: for patches whose faces are all physical (DevPatch::wt), the
-// kernel that changes a boundary cell also writes the ghost cells SetBC would
+// code that changes a boundary cell also writes the ghost cells SetBC would
 // derive from it (write-through).  This reproduces SetGhost's result exactly:
 // SetBC2D/3D (boundary.f90:661-885) processes the faces in order and copies
 // whole rows including the ghost rows, so a ghost outside in the set S of
-// dimensions ends up as the map of each face in S (ascending dimension) applied
-// to the interior cell reflected across all of S.
+// dimensions ends up as the map of each face in S (ascending dimension)
+// applied to the interior cell reflected across all of S.
 #pragma once
 #include "bsam_types.h"
 #include "problem_ch.cuh"
@@ -20,6 +22,12 @@
 namespace bsam {
 
 template <class T> __device__ __forceinline__ T* fld(void* p) { return static_cast<T*>(p); }
+
+// The pre-smoothed state of a level: the second buffer when the level's
+// stages run the fused kernel (q -> qb -> q), else q itself.
+__device__ __forceinline__ void* const* mid_state(const DevPatch& P) {
+  return P.fused ? P.qb : P.q;
+}
 
 __device__ __forceinline__ int64_t cidx(const DevPatch& P, int i, int j, int k) {
   return (int64_t)i + (int64_t)j * P.sy + (int64_t)k * P.sz;
@@ -29,58 +37,63 @@ template <class T> __device__ __forceinline__ T bc_map(int code, T v) {
   return code == BC_REFLECT ? T(2) - v : v;
 }
 
-// Ghost write-through for the cell (i,j,k) of patch P whose new values are
-// (v0, v1).  Only called when the cell may touch the boundary.
-template <class T, int D>
-__device__ void write_through(const DevPatch& P, T* q0, T* q1, int i, int j, int k, T v0,
-                              T v1) {
-  const int co[3] = {i, j, k};
-  int opt[3][3];   // per dimension: own coordinate, lo ghost, hi ghost (-1 absent)
-  int code[3][3];
-  bool any = false;
-#pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    opt[d][0] = co[d];
-    opt[d][1] = -1;
-    opt[d][2] = -1;
-    code[d][0] = BC_NONE;
-    code[d][1] = BC_NONE;
-    code[d][2] = BC_NONE;
-    if (d < D) {
-      if (co[d] == 1 && P.bc[2 * d] != BC_NONE) {
-        opt[d][1] = 0;
-        code[d][1] = P.bc[2 * d];
-        any = true;
-      }
-      if (co[d] == P.n[d] && P.bc[2 * d + 1] != BC_NONE) {
-        opt[d][2] = P.n[d] + 1;
-        code[d][2] = P.bc[2 * d + 1];
-        any = true;
-      }
-    }
+// Choice s of one dimension for a ghost combination: 0 = the cell's own
+// coordinate, 1 = the low ghost (coordinate 1 on a physical low face),
+// 2 = the high ghost (coordinate n on a physical high face).
+__device__ __forceinline__ bool ghost_choice(int s, int co, int n, int lo_code, int hi_code,
+                                             int& g, int& code) {
+  if (s == 0) {
+    g = co;
+    code = BC_NONE;
+    return true;
   }
-  if (!any) return;
-  const int ncombo = (D == 2) ? 9 : 27;
-  for (int cmb = 1; cmb < ncombo; ++cmb) {
-    int sel[3] = {cmb % 3, (cmb / 3) % 3, (cmb / 9) % 3};
-    bool ok = true;
-    int g[3];
+  if (s == 1) {
+    g = 0;
+    code = lo_code;
+    return co == 1 && lo_code != BC_NONE;
+  }
+  g = n + 1;
+  code = hi_code;
+  return co == n && hi_code != BC_NONE;
+}
+
+// Ghost write-through for the cell (i,j,k) of patch P whose new values are
+// (v0, v1).
+template <class T, int D>
+__device__ __forceinline__ void write_through(const DevPatch& P, T* q0, T* q1, int i, int j,
+                                              int k, T v0, T v1) {
 #pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      g[d] = opt[d][sel[d]];
-      if (g[d] < 0) ok = false;
-    }
-    if (!ok) continue;
-    T a = v0, b = v1;
+  for (int sz = 0; sz < (D == 3 ? 3 : 1); ++sz) {
+    int gz = k, cz = BC_NONE;
+    if (D == 3 && !ghost_choice(sz, k, P.n[2], P.bc[4], P.bc[5], gz, cz)) continue;
 #pragma unroll
-    for (int d = 0; d < D; ++d)
-      if (sel[d] != 0) {
-        a = bc_map<T>(code[d][sel[d]], a);
-        b = bc_map<T>(code[d][sel[d]], b);
+    for (int sy = 0; sy < 3; ++sy) {
+      int gy, cy;
+      if (!ghost_choice(sy, j, P.n[1], P.bc[2], P.bc[3], gy, cy)) continue;
+#pragma unroll
+      for (int sx = 0; sx < 3; ++sx) {
+        if (sx == 0 && sy == 0 && sz == 0) continue;
+        int gx, cx;
+        if (!ghost_choice(sx, i, P.n[0], P.bc[0], P.bc[1], gx, cx)) continue;
+        // Face maps applied in ascending dimension (SetBC's face order).
+        T a = v0, b = v1;
+        if (sx) {
+          a = bc_map<T>(cx, a);
+          b = bc_map<T>(cx, b);
+        }
+        if (sy) {
+          a = bc_map<T>(cy, a);
+          b = bc_map<T>(cy, b);
+        }
+        if (sz) {
+          a = bc_map<T>(cz, a);
+          b = bc_map<T>(cz, b);
+        }
+        const int64_t c = cidx(P, gx, gy, D == 3 ? gz : 0);
+        q0[c] = a;
+        q1[c] = b;
       }
-    const int64_t c = cidx(P, g[0], g[1], D == 3 ? g[2] : 0);
-    q0[c] = a;
-    q1[c] = b;
+    }
   }
 }
 
@@ -106,20 +119,12 @@ __device__ __forceinline__ bool near_boundary(const DevPatch& P, int i, int j, i
   return b;
 }
 
-// ---------------------------------------------------------------------------
-// RelaxGrid (one colour pass) + SetGhost(level, ipass) for physical faces.
-// color 0 = ipass 1 = cells with even i+j(+k); color 1 = ipass 2.
+// ---- per-cell bodies ---------------------------------------------------------
+
+// One cell of RelaxGrid (problem.f90:192-213 / 485-516), in place on q, with
+// SetGhost(level, ipass) for physical faces.
 template <class T, int D>
-__global__ void __launch_bounds__(BLOCK_THREADS)
-    k_relax(const DevPatch* __restrict__ PT, const Item* __restrict__ items, int color) {
-  const Item it = items[blockIdx.x];
-  const DevPatch& P = PT[it.patch];
-  const int j = it.ty * TILE_Y + threadIdx.y + 1;
-  const int k = (D == 3) ? it.tz + 1 : 0;
-  if (j > P.n[1]) return;
-  const int i0 = (it.tx * 32 + threadIdx.x) * 2 + 1;
-  const int i = i0 + ((i0 + j + k + color) & 1);
-  if (i > P.n[0]) return;
+__device__ __forceinline__ void relax_cell(const DevPatch& P, int i, int j, int k) {
   T* q0 = fld<T>(P.q[0]);
   T* q1 = fld<T>(P.q[1]);
   const T* f0 = fld<T>(P.f[0]);
@@ -148,30 +153,164 @@ __device__ __forceinline__ void residual_cell(const DevPatch& P, const T* q0, co
   r1 = f1[c] - o1;
 }
 
-// Deterministic block sum of a double (fixed shuffle tree + fixed smem order).
+// RestrictSolution (afas:600-644) of the coarse cell (ic,jc,kc) of child C
+// into parent P, + the parent's SetGhost(level-1, 0) for physical faces +
+// GetCoarseGhostPoints (boundary.f90:1203-1269): the parent solution and its
+// snapshot qs (the children's qc) are both written.
+template <class T, int D>
+__device__ __forceinline__ void restrict_cell(const DevPatch& C, const DevPatch& P, int ic, int jc,
+                                              int kc) {
+  const int i = 2 * ic, j = 2 * jc, k = 2 * kc;
+  T val[2];
+#pragma unroll
+  for (int v = 0; v < 2; ++v) {
+    const T* a = fld<T>(mid_state(C)[v]);
+    if (D == 2) {
+      val[v] = T(0.25) * (a[cidx(C, i, j, 0)] + a[cidx(C, i - 1, j, 0)] +
+                          a[cidx(C, i, j - 1, 0)] + a[cidx(C, i - 1, j - 1, 0)]);
+    } else {
+      val[v] = T(0.125) * (a[cidx(C, i, j, k)] + a[cidx(C, i - 1, j, k)] +
+                           a[cidx(C, i, j - 1, k)] + a[cidx(C, i - 1, j - 1, k)] +
+                           a[cidx(C, i, j, k - 1)] + a[cidx(C, i - 1, j, k - 1)] +
+                           a[cidx(C, i, j - 1, k - 1)] + a[cidx(C, i - 1, j - 1, k - 1)]);
+    }
+  }
+  const int pi = C.off[0] + ic, pj = C.off[1] + jc, pk = (D == 3) ? C.off[2] + kc : 0;
+  const int64_t pc = cidx(P, pi, pj, pk);
+  T* pq0 = fld<T>(P.q[0]);
+  T* pq1 = fld<T>(P.q[1]);
+  T* ps0 = fld<T>(P.qs[0]);
+  T* ps1 = fld<T>(P.qs[1]);
+  pq0[pc] = val[0];
+  pq1[pc] = val[1];
+  ps0[pc] = val[0];
+  ps1[pc] = val[1];
+  if (P.wt && near_boundary(P, pi, pj, pk, D)) {
+    write_through<T, D>(P, pq0, pq1, pi, pj, pk, val[0], val[1]);
+    write_through<T, D>(P, ps0, ps1, pi, pj, pk, val[0], val[1]);
+  }
+}
+
+// CoarseLoadingFunction (afas:646-714) at one coarse cell:
+//   parent%f(mb) = Restriction(f - Operator(q)) + Operator(qc, h = parent%dx)
+template <class T, int D>
+__device__ __forceinline__ void coarse_load_cell(const DevPatch& C, const DevPatch& P, int ic,
+                                                 int jc, int kc) {
+  const T* q0 = fld<T>(mid_state(C)[0]);
+  const T* q1 = fld<T>(mid_state(C)[1]);
+  const T* f0 = fld<T>(C.f[0]);
+  const T* f1 = fld<T>(C.f[1]);
+  const int i = 2 * ic, j = 2 * jc, k = 2 * kc;
+  // Restriction of rf: children in the reference's summation order.
+  const int nch = (D == 2) ? 4 : 8;
+  T s0 = T(0), s1 = T(0);
+#pragma unroll
+  for (int ch = 0; ch < nch; ++ch) {
+    const int ii = i - (ch & 1), jj = j - ((ch >> 1) & 1), kk = (D == 3) ? k - (ch >> 2) : 0;
+    T r0, r1;
+    residual_cell<T, D>(C, q0, q1, f0, f1, cidx(C, ii, jj, kk), r0, r1);
+    if (ch == 0) {
+      s0 = r0;
+      s1 = r1;
+    } else {
+      s0 = s0 + r0;
+      s1 = s1 + r1;
+    }
+  }
+  const T w = (D == 2) ? T(0.25) : T(0.125);
+  const T R0 = w * s0, R1 = w * s1;
+  const int pi = C.off[0] + ic, pj = C.off[1] + jc, pk = (D == 3) ? C.off[2] + kc : 0;
+  const int64_t pc = cidx(P, pi, pj, pk);
+  problem::Stencil<T, D> s;
+  load_stencil<T, D>(P, fld<T>(P.qs[0]), fld<T>(P.qs[1]), pc, s);
+  T o0, o1;
+  problem::OperatorCell<T, D>(s, T(P.tmp1), T(P.tmp2), T(P.alpha), o0, o1);
+  fld<T>(P.f[0])[pc] = R0 + o0;
+  fld<T>(P.f[1])[pc] = R1 + o1;
+}
+
+template <class T>
+__device__ __forceinline__ T lin_x(bool even, T a, T b) {
+  return even ? T(3) * a + b : a + T(3) * b;
+}
+
+// CorrectFine with BiLin/TriLinProlongationP1 (afas:842-963,
+// gridutilities.f90:137-175, 474-529) at the fine cell (I,J,K):
+// q += P(parent%q - qc); the ghost ring is refreshed by write-through (the
+// reference's SetGhost(level, 0) overwrites the prolongated ring, afas:515).
+template <class T, int D>
+__device__ __forceinline__ void correct_cell(const DevPatch& C, const DevPatch& P, int I, int J,
+                                             int K) {
+  const T* pq0 = fld<T>(P.q[0]);
+  const T* pq1 = fld<T>(P.q[1]);
+  const T* ps0 = fld<T>(P.qs[0]);
+  const T* ps1 = fld<T>(P.qs[1]);
+  T* q0 = fld<T>(mid_state(C)[0]);
+  T* q1 = fld<T>(mid_state(C)[1]);
+  const int m = I >> 1, n = J >> 1, p = K >> 1;
+  const bool ex = (I & 1) == 0, ey = (J & 1) == 0, ez = (K & 1) == 0;
+  T corr[2];
+#pragma unroll
+  for (int v = 0; v < 2; ++v) {
+    const T* pq = v ? pq1 : pq0;
+    const T* ps = v ? ps1 : ps0;
+    auto e = [&](int a, int b, int c) -> T {
+      const int64_t x = cidx(P, C.off[0] + a, C.off[1] + b, D == 3 ? C.off[2] + c : 0);
+      return pq[x] - ps[x];
+    };
+    if (D == 2) {
+      const T b0 = lin_x<T>(ex, e(m, n, 0), e(m + 1, n, 0));
+      const T b1 = lin_x<T>(ex, e(m, n + 1, 0), e(m + 1, n + 1, 0));
+      corr[v] = lin_x<T>(ey, b0, b1) / T(16);
+    } else {
+      const T b00 = lin_x<T>(ex, e(m, n, p), e(m + 1, n, p));
+      const T b10 = lin_x<T>(ex, e(m, n + 1, p), e(m + 1, n + 1, p));
+      const T b01 = lin_x<T>(ex, e(m, n, p + 1), e(m + 1, n, p + 1));
+      const T b11 = lin_x<T>(ex, e(m, n + 1, p + 1), e(m + 1, n + 1, p + 1));
+      const T c0 = lin_x<T>(ey, b00, b10);
+      const T c1 = lin_x<T>(ey, b01, b11);
+      corr[v] = lin_x<T>(ez, c0, c1) / T(64);
+    }
+  }
+  const int64_t c = cidx(C, I, J, K);
+  const T a0 = q0[c] + corr[0];
+  const T a1 = q1[c] + corr[1];
+  q0[c] = a0;
+  q1[c] = a1;
+  if (C.wt && near_boundary(C, I, J, K, D)) write_through<T, D>(C, q0, q1, I, J, K, a0, a1);
+}
+
+// ---- reductions --------------------------------------------------------------
+
+// Deterministic block sum of a double (fixed shuffle tree + fixed smem
+// order).  Any block shape whose size is a multiple of 32 and at most 1024.
 __device__ __forceinline__ double block_sum(double v) {
-  __shared__ double red[BLOCK_THREADS / 32];
+  __shared__ double red[32];
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  const int lane = threadIdx.x, warp = threadIdx.y;
+  const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+  const int nthreads = blockDim.x * blockDim.y * blockDim.z;
+  const int lane = tid & 31, warp = tid >> 5;
   if (lane == 0) red[warp] = v;
   __syncthreads();
   double s = 0.0;
-  if (warp == 0 && lane == 0) {
-    for (int w = 0; w < BLOCK_THREADS / 32; ++w) s += red[w];
+  if (tid == 0) {
+    for (int w = 0; w < nthreads / 32; ++w) s += red[w];
   }
   __syncthreads();
-  return s;  // valid in thread (0,0)
+  return s;  // valid in thread 0
 }
 
 // Second stage of a two-stage reduction: the last CTA to finish sums the
-// per-CTA partials in index order.  Returns true in thread (0,0) of that CTA
+// per-CTA partials in index order.  Returns true in thread 0 of that CTA
 // with the total in `total`.
 __device__ __forceinline__ bool last_block_total(double mine, double* partials,
                                                  uint32_t* ticket, int nblocks,
                                                  double& total) {
   __shared__ bool is_last;
-  if (threadIdx.x == 0 && threadIdx.y == 0) {
+  const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+  const int nthreads = blockDim.x * blockDim.y * blockDim.z;
+  if (tid == 0) {
     partials[blockIdx.x] = mine;
     __threadfence();
     const uint32_t t = atomicAdd(ticket, 1u);
@@ -180,9 +319,8 @@ __device__ __forceinline__ bool last_block_total(double mine, double* partials,
   __syncthreads();
   if (!is_last) return false;
   __threadfence();
-  const int tid = threadIdx.y * 32 + threadIdx.x;
   double s = 0.0;
-  for (int b = tid; b < nblocks; b += BLOCK_THREADS) s += ((volatile double*)partials)[b];
+  for (int b = tid; b < nblocks; b += nthreads) s += ((volatile double*)partials)[b];
   const double tot = block_sum(s);
   if (tid == 0) {
     total = tot;
@@ -190,6 +328,24 @@ __device__ __forceinline__ bool last_block_total(double mine, double* partials,
     return true;
   }
   return false;
+}
+
+// ---- grid kernels --------------------------------------------------------------
+
+// RelaxGrid (one colour pass) + SetGhost(level, ipass) for physical faces.
+// color 0 = ipass 1 = cells with even i+j(+k); color 1 = ipass 2.
+template <class T, int D>
+__global__ void __launch_bounds__(BLOCK_THREADS)
+    k_relax(const DevPatch* __restrict__ PT, const Item* __restrict__ items, int color) {
+  const Item it = items[blockIdx.x];
+  const DevPatch P = PT[it.patch];  // by value: fields stay in registers
+  const int j = it.ty * TILE_Y + threadIdx.y + 1;
+  const int k = (D == 3) ? it.tz + 1 : 0;
+  if (j > P.n[1]) return;
+  const int i0 = (it.tx * 32 + threadIdx.x) * 2 + 1;
+  const int i = i0 + ((i0 + j + k + color) & 1);
+  if (i > P.n[0]) return;
+  relax_cell<T, D>(P, i, j, k);
 }
 
 // ErrorAFAS / L2Error / SquareSum (afas:108-221), errortype 1:
@@ -200,7 +356,7 @@ __global__ void __launch_bounds__(BLOCK_THREADS)
                  double* __restrict__ partials, DevStatus* __restrict__ st, int nitems,
                  double denom, double tol) {
   const Item it = items[blockIdx.x];
-  const DevPatch& P = PT[it.patch];
+  const DevPatch P = PT[it.patch];
   const int j = it.ty * TILE_Y + threadIdx.y + 1;
   const int k = (D == 3) ? it.tz + 1 : 0;
   const int i0 = (it.tx * 32 + threadIdx.x) * 2 + 1;
@@ -230,15 +386,12 @@ __global__ void __launch_bounds__(BLOCK_THREADS)
   }
 }
 
-// RestrictSolution (afas:600-644) + the parent's SetGhost(level-1, 0) for
-// physical faces + GetCoarseGhostPoints (boundary.f90:1203-1269): the parent
-// solution and its snapshot qs (the children's qc) are both written.
 template <class T, int D>
 __global__ void __launch_bounds__(BLOCK_THREADS)
     k_restrict(const DevPatch* __restrict__ PT, const Item* __restrict__ items) {
   const Item it = items[blockIdx.x];
-  const DevPatch& C = PT[it.patch];
-  const DevPatch& P = PT[C.parent];
+  const DevPatch C = PT[it.patch];
+  const DevPatch P = PT[C.parent];
   const int jc = it.ty * TILE_Y + threadIdx.y + 1;
   const int kc = (D == 3) ? it.tz + 1 : 0;
   if (jc > C.cn[1]) return;
@@ -247,148 +400,43 @@ __global__ void __launch_bounds__(BLOCK_THREADS)
   for (int t = 0; t < 2; ++t) {
     const int ic = ic0 + t;
     if (ic > C.cn[0]) break;
-    const int i = 2 * ic, j = 2 * jc, k = 2 * kc;
-    T val[2];
-#pragma unroll
-    for (int v = 0; v < 2; ++v) {
-      const T* a = fld<T>(C.q[v]);
-      if (D == 2) {
-        val[v] = T(0.25) * (a[cidx(C, i, j, 0)] + a[cidx(C, i - 1, j, 0)] +
-                            a[cidx(C, i, j - 1, 0)] + a[cidx(C, i - 1, j - 1, 0)]);
-      } else {
-        val[v] = T(0.125) * (a[cidx(C, i, j, k)] + a[cidx(C, i - 1, j, k)] +
-                             a[cidx(C, i, j - 1, k)] + a[cidx(C, i - 1, j - 1, k)] +
-                             a[cidx(C, i, j, k - 1)] + a[cidx(C, i - 1, j, k - 1)] +
-                             a[cidx(C, i, j - 1, k - 1)] + a[cidx(C, i - 1, j - 1, k - 1)]);
-      }
-    }
-    const int pi = C.off[0] + ic, pj = C.off[1] + jc, pk = (D == 3) ? C.off[2] + kc : 0;
-    const int64_t pc = cidx(P, pi, pj, pk);
-    T* pq0 = fld<T>(P.q[0]);
-    T* pq1 = fld<T>(P.q[1]);
-    T* ps0 = fld<T>(P.qs[0]);
-    T* ps1 = fld<T>(P.qs[1]);
-    pq0[pc] = val[0];
-    pq1[pc] = val[1];
-    ps0[pc] = val[0];
-    ps1[pc] = val[1];
-    if (P.wt && near_boundary(P, pi, pj, pk, D)) {
-      write_through<T, D>(P, pq0, pq1, pi, pj, pk, val[0], val[1]);
-      write_through<T, D>(P, ps0, ps1, pi, pj, pk, val[0], val[1]);
-    }
+    restrict_cell<T, D>(C, P, ic, jc, kc);
   }
 }
 
-// CoarseLoadingFunction (afas:646-714):
-//   parent%f(mb) = Restriction(f - Operator(q)) + Operator(qc, h = parent%dx)
 template <class T, int D>
 __global__ void __launch_bounds__(BLOCK_THREADS)
     k_coarse_load(const DevPatch* __restrict__ PT, const Item* __restrict__ items) {
   const Item it = items[blockIdx.x];
-  const DevPatch& C = PT[it.patch];
-  const DevPatch& P = PT[C.parent];
+  const DevPatch C = PT[it.patch];
+  const DevPatch P = PT[C.parent];
   const int jc = it.ty * TILE_Y + threadIdx.y + 1;
   const int kc = (D == 3) ? it.tz + 1 : 0;
   if (jc > C.cn[1]) return;
   const int ic0 = (it.tx * 32 + threadIdx.x) * 2 + 1;
-  const T* q0 = fld<T>(C.q[0]);
-  const T* q1 = fld<T>(C.q[1]);
-  const T* f0 = fld<T>(C.f[0]);
-  const T* f1 = fld<T>(C.f[1]);
 #pragma unroll
   for (int t = 0; t < 2; ++t) {
     const int ic = ic0 + t;
     if (ic > C.cn[0]) break;
-    const int i = 2 * ic, j = 2 * jc, k = 2 * kc;
-    // Restriction of rf: children in the reference's summation order.
-    const int nch = (D == 2) ? 4 : 8;
-    T s0 = T(0), s1 = T(0);
-#pragma unroll
-    for (int ch = 0; ch < nch; ++ch) {
-      const int ii = i - (ch & 1), jj = j - ((ch >> 1) & 1), kk = (D == 3) ? k - (ch >> 2) : 0;
-      T r0, r1;
-      residual_cell<T, D>(C, q0, q1, f0, f1, cidx(C, ii, jj, kk), r0, r1);
-      if (ch == 0) {
-        s0 = r0;
-        s1 = r1;
-      } else {
-        s0 = s0 + r0;
-        s1 = s1 + r1;
-      }
-    }
-    const T w = (D == 2) ? T(0.25) : T(0.125);
-    const T R0 = w * s0, R1 = w * s1;
-    const int pi = C.off[0] + ic, pj = C.off[1] + jc, pk = (D == 3) ? C.off[2] + kc : 0;
-    const int64_t pc = cidx(P, pi, pj, pk);
-    problem::Stencil<T, D> s;
-    load_stencil<T, D>(P, fld<T>(P.qs[0]), fld<T>(P.qs[1]), pc, s);
-    T o0, o1;
-    problem::OperatorCell<T, D>(s, T(P.tmp1), T(P.tmp2), T(P.alpha), o0, o1);
-    fld<T>(P.f[0])[pc] = R0 + o0;
-    fld<T>(P.f[1])[pc] = R1 + o1;
+    coarse_load_cell<T, D>(C, P, ic, jc, kc);
   }
-}
-
-// CorrectFine with BiLin/TriLinProlongationP1 (afas:842-963,
-// gridutilities.f90:137-175, 474-529): q += P(parent%q - qc) on the
-// interior; the ghost ring is refreshed by write-through (the reference's
-// SetGhost(level, 0) overwrites the prolongated ring, afas:515).
-template <class T>
-__device__ __forceinline__ T lin_x(bool even, T a, T b) {
-  return even ? T(3) * a + b : a + T(3) * b;
 }
 
 template <class T, int D>
 __global__ void __launch_bounds__(BLOCK_THREADS)
     k_correct(const DevPatch* __restrict__ PT, const Item* __restrict__ items) {
   const Item it = items[blockIdx.x];
-  const DevPatch& C = PT[it.patch];
-  const DevPatch& P = PT[C.parent];
+  const DevPatch C = PT[it.patch];
+  const DevPatch P = PT[C.parent];
   const int J = it.ty * TILE_Y + threadIdx.y + 1;
   const int K = (D == 3) ? it.tz + 1 : 0;
   if (J > C.n[1]) return;
   const int I0 = (it.tx * 32 + threadIdx.x) * 2 + 1;
-  const T* pq0 = fld<T>(P.q[0]);
-  const T* pq1 = fld<T>(P.q[1]);
-  const T* ps0 = fld<T>(P.qs[0]);
-  const T* ps1 = fld<T>(P.qs[1]);
-  T* q0 = fld<T>(C.q[0]);
-  T* q1 = fld<T>(C.q[1]);
 #pragma unroll
   for (int t = 0; t < 2; ++t) {
     const int I = I0 + t;
     if (I > C.n[0]) break;
-    const int m = I >> 1, n = J >> 1, p = K >> 1;
-    const bool ex = (I & 1) == 0, ey = (J & 1) == 0, ez = (K & 1) == 0;
-    T corr[2];
-#pragma unroll
-    for (int v = 0; v < 2; ++v) {
-      const T* pq = v ? pq1 : pq0;
-      const T* ps = v ? ps1 : ps0;
-      auto e = [&](int a, int b, int c) -> T {
-        const int64_t x = cidx(P, C.off[0] + a, C.off[1] + b, D == 3 ? C.off[2] + c : 0);
-        return pq[x] - ps[x];
-      };
-      if (D == 2) {
-        const T b0 = lin_x<T>(ex, e(m, n, 0), e(m + 1, n, 0));
-        const T b1 = lin_x<T>(ex, e(m, n + 1, 0), e(m + 1, n + 1, 0));
-        corr[v] = lin_x<T>(ey, b0, b1) / T(16);
-      } else {
-        const T b00 = lin_x<T>(ex, e(m, n, p), e(m + 1, n, p));
-        const T b10 = lin_x<T>(ex, e(m, n + 1, p), e(m + 1, n + 1, p));
-        const T b01 = lin_x<T>(ex, e(m, n, p + 1), e(m + 1, n, p + 1));
-        const T b11 = lin_x<T>(ex, e(m, n + 1, p + 1), e(m + 1, n + 1, p + 1));
-        const T c0 = lin_x<T>(ey, b00, b10);
-        const T c1 = lin_x<T>(ey, b01, b11);
-        corr[v] = lin_x<T>(ez, c0, c1) / T(64);
-      }
-    }
-    const int64_t c = cidx(C, I, J, K);
-    const T a0 = q0[c] + corr[0];
-    const T a1 = q1[c] + corr[1];
-    q0[c] = a0;
-    q1[c] = a1;
-    if (C.wt && near_boundary(C, I, J, K, D)) write_through<T, D>(C, q0, q1, I, J, K, a0, a1);
+    correct_cell<T, D>(C, P, I, J, K);
   }
 }
 
@@ -398,7 +446,7 @@ template <class T, int D>
 __global__ void __launch_bounds__(BLOCK_THREADS)
     k_source(const DevPatch* __restrict__ PT, const Item* __restrict__ items) {
   const Item it = items[blockIdx.x];
-  const DevPatch& P = PT[it.patch];
+  const DevPatch P = PT[it.patch];
   const int j = it.ty * TILE_Y + threadIdx.y + 1;
   const int k = (D == 3) ? it.tz + 1 : 0;
   if (j > P.n[1]) return;
@@ -424,7 +472,7 @@ __global__ void __launch_bounds__(BLOCK_THREADS)
 // dimensions (ascending) applied to the cell reflected across them.
 template <class T, int D>
 __global__ void k_setbc(const DevPatch* __restrict__ PT, int patch, int64_t ntotal) {
-  const DevPatch& P = PT[patch];
+  const DevPatch P = PT[patch];
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= ntotal) return;
   const int e0 = P.n[0] + 2, e1 = P.n[1] + 2;
@@ -462,7 +510,7 @@ __global__ void __launch_bounds__(BLOCK_THREADS)
     k_mass(const DevPatch* __restrict__ PT, const Item* __restrict__ items,
            double* __restrict__ partials, DevStatus* __restrict__ st, int nitems, double hd) {
   const Item it = items[blockIdx.x];
-  const DevPatch& P = PT[it.patch];
+  const DevPatch P = PT[it.patch];
   const int j = it.ty * TILE_Y + threadIdx.y + 1;
   const int k = (D == 3) ? it.tz + 1 : 0;
   const int i0 = (it.tx * 32 + threadIdx.x) * 2 + 1;

@@ -71,6 +71,26 @@ typedef struct {
  * device `device` (one stream per handle). */
 int bsam_gpu_create(bsam_gpu** h, int device, const bsam_run_params* p);
 
+/* Kernel-shape choices (no reference counterpart).  Results do not depend on
+ * them: every choice computes the same arithmetic in the same order.
+ *   fuse_smoother  -1 automatic, 0 one launch per colour pass, 1 fused stage
+ *                  (all 2*nu passes of LevelRelax in one launch) where the
+ *                  level allows it
+ *   fuse_min_n     smallest extent per dimension of a fused level
+ *   chunk          planes (3D) / rows (2D) per streaming chunk, 0 = automatic
+ *   bottom_cells   levels of at most this many cells run their whole part of
+ *                  the V-cycle in one single-CTA launch; 0 = default (4096),
+ *                  -1 = never
+ * Call before bsam_gpu_set_hierarchy. */
+typedef struct {
+  int32_t fuse_smoother;
+  int32_t fuse_min_n;
+  int32_t chunk;
+  int32_t bottom_cells;
+  int32_t reserved[4];
+} bsam_tuning;
+int bsam_gpu_set_tuning(bsam_gpu* h, const bsam_tuning* t);
+
 /* Replaces the tree set-up that makes the hierarchy reachable to
  * MultigridIterations: RootInit/InitSeed/AllocFields
  * (lib/bsamroutines.f90:205-494, lib/bsamstorage.f90:46-123).  patches[] is in

@@ -100,3 +100,56 @@ def test_put_get_roundtrip(gpu_lib, nd):
         q = np.asfortranarray(rng.standard_normal(s.qshape))
         s.put_q(q)
         assert np.array_equal(s.get_q(), q)
+
+
+# ---- fused smoothing stages (one launch per LevelRelax) ---------------------
+
+def compare_tuned(oracle, prob, nsteps, **tuning):
+    ref = oracle.run_uniform(prob, nsteps=nsteps)
+    with B.Solver(prob, **tuning) as s:
+        got = s.run(nsteps)
+    assert np.array_equal(got["nvcycles"], ref["nvcycles"])
+    for st in range(nsteps):
+        e = relerr(got["q"][st], ref["q"][st])
+        assert e <= RTOL, (st, e)
+    return got, ref
+
+
+@pytest.mark.parametrize("chunk", [0, 5, 64])
+def test_fused_3d_bit_identical(gpu_lib, oracle, chunk):
+    # 48^3: levels 48, 24, 12 fused (several tiles, partial tiles, chunks with
+    # a remainder), 6 and 3 on the per-pass path.
+    prob = W.config3(nsteps=2, n=48)
+    got, ref = compare_tuned(oracle, prob, 2, fuse=1, fuse_min_n=8, chunk=chunk)
+    assert np.array_equal(got["q"], ref["q"])
+
+
+def test_fused_3d_rectangular_userbc(gpu_lib, oracle):
+    prob = W.config3(nsteps=2, n=32)
+    prob.mx = (64, 32, 48)
+    prob.xupper = (1.0, 0.5, 0.75)
+    prob.c0 = 0.55 + 0.025 * W.uniform(31, 64 * 32 * 48, -1.0, 1.0)
+    prob.mthbc = (10, 1, 1, 10, 1, 10)
+    got, ref = compare_tuned(oracle, prob, 2, fuse=1, fuse_min_n=8, chunk=7)
+    assert np.array_equal(got["q"], ref["q"])
+
+
+def test_fused_matches_unfused_128(gpu_lib):
+    prob = W.config3(nsteps=1, n=128)
+    with B.Solver(prob, fuse=0) as a:
+        ra = a.run(1)
+    with B.Solver(prob, fuse=1) as b:
+        rb = b.run(1)
+    assert np.array_equal(ra["q"], rb["q"]) and np.array_equal(ra["nvcycles"], rb["nvcycles"])
+
+
+@pytest.mark.parametrize("nd,n", [(2, 128), (2, 96), (3, 32)])
+def test_bottom_kernel_matches_per_level_launches(gpu_lib, nd, n):
+    # The single-CTA bottom of the V-cycle (levels <= 4096 cells) against one
+    # launch per phase: the same arithmetic, so bit-identical fields.
+    prob = W.config1(nsteps=2, n=n) if nd == 2 else W.config3(nsteps=2, n=n)
+    with B.Solver(prob, bottom_cells=-1) as a:
+        ra = a.run(2)
+    with B.Solver(prob) as b:
+        rb = b.run(2)
+    assert np.array_equal(ra["q"], rb["q"]) and np.array_equal(ra["nvcycles"], rb["nvcycles"])

@@ -41,28 +41,30 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks and throttle reasons, sampled every 20 ms with
+    timestamps while the benchmark runs; summary() keeps the samples inside a
+    wall-clock window (the timed region)."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, index: int):
         self.index = index
         self.proc = None
+        self.lines = []
 
-    def __enter__(self):
+    def start(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "20"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            time.sleep(1.0)  # let the sampler start producing before timing
         except Exception:
             self.proc = None
-        return self
 
-    def __exit__(self, *a):
-        self.lines = []
+    def stop(self):
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -72,19 +74,24 @@ class ClockSampler:
                 out = ""
             self.lines = [l for l in out.splitlines() if l.strip()]
 
-    def summary(self):
+    def summary(self, t0: float, t1: float):
+        import datetime
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for l in getattr(self, "lines", []):
+        for l in self.lines:
             parts = [p.strip() for p in l.split(",")]
-            if len(parts) < 9:
+            if len(parts) < 10:
                 continue
             try:
-                sm.append(float(parts[1]))
-                smax = float(parts[2])
+                ts = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                mhz, mx = float(parts[2]), float(parts[3])
             except ValueError:
                 continue
-            for n, v in zip(names, parts[5:9]):
+            if not (t0 <= ts <= t1):
+                continue
+            sm.append(mhz)
+            smax = mx
+            for n, v in zip(names, parts[6:10]):
                 if v.lower() == "active":
                     reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
@@ -196,29 +203,54 @@ def run_ours(args, world, rank, local):
             flush.fill_(1.0)
 
     # ---- device-resident timed region ----
-    solver.profile(True)
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
            for _ in range(args.steps)]
     nvc = []
+    launches0 = solver.stats()["launches"]
+    clk = ClockSampler(local)
+    clk.start()
     barrier(world)
     torch.cuda.synchronize()
     t_wall0 = time.perf_counter()
-    with ClockSampler(local) as clk:
-        for s in range(args.steps):
-            flush_l2()
-            evs[s][0].record(stream)
-            nv, res, conv = solver.step()
-            evs[s][1].record(stream)
-            nvc.append(nv)
-        torch.cuda.synchronize()
+    t_ep0 = time.time()
+    for s in range(args.steps):
+        flush_l2()
+        evs[s][0].record(stream)
+        nv, res, conv = solver.step()
+        evs[s][1].record(stream)
+        nvc.append(nv)
+    torch.cuda.synchronize()
+    t_ep1 = time.time()
     barrier(world)
     t_wall = time.perf_counter() - t_wall0
+    # Keep the GPU busy with further steps (untimed) until the sampler has seen
+    # at least half a second of load; used only if the timed region is too
+    # short to hold a 20 ms sample.
+    while time.time() - t_ep0 < 0.5:
+        solver.step()
+    torch.cuda.synchronize()
+    t_ep2 = time.time()
+    clk.stop()
+    clocks = clk.summary(t_ep0, t_ep1)
+    clocks["window"] = "timed region"
+    if clocks["samples"] == 0:
+        clocks = clk.summary(t_ep0, t_ep2)
+        clocks["window"] = "timed region + continued steps of the same workload"
     step_ms = [a.elapsed_time(b) for a, b in evs]
     dev_s = sum(step_ms) / 1e3
     dev_s_max = allmax(world, dev_s)
+    launches = solver.stats()["launches"] - launches0
+    value = world * args.steps / dev_s_max
+
+    # ---- smoother stage timing (roofline): CUDA events around every
+    # finest-level smoothing stage, on a separate pass of the same steps ----
+    solver.profile(True)
+    for s in range(min(args.steps, 3)):
+        flush_l2()
+        solver.step()
+    torch.cuda.synchronize()
     st = solver.stats()
     solver.profile(False)
-    value = world * args.steps / dev_s_max
 
     # ---- end-to-end through the C ABI with pinned host buffers ----
     qhost = torch.empty(int(np.prod(solver.qshape)), dtype=torch.float64, pin_memory=True)
@@ -269,8 +301,8 @@ def run_ours(args, world, rank, local):
                      "stage_ms": per_stage_ms},
         "e2e": {"value": world * args.steps / e2e_s, "unit": UNIT,
                 "h2d_bytes_per_step": qbytes, "d2h_bytes_per_step": qbytes},
-        "gpu_launches": int(st["launches"]),
-        "clocks": clk.summary(),
+        "gpu_launches": int(launches),
+        "clocks": clocks,
     }
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()

@@ -69,7 +69,7 @@ ABI_SYMBOLS = (
 class Tuning(ctypes.Structure):
     _fields_ = [("fuse_smoother", ctypes.c_int32), ("fuse_min_n", ctypes.c_int32),
                 ("chunk", ctypes.c_int32), ("bottom_cells", ctypes.c_int32),
-                ("reserved", ctypes.c_int32 * 4)]
+                ("graph", ctypes.c_int32), ("reserved", ctypes.c_int32 * 3)]
 
 
 class Stats(ctypes.Structure):
@@ -168,7 +168,8 @@ class Solver:
     """
 
     def __init__(self, prob, device: int = 0, precision: int = PREC_FP64, q0=None,
-                 fuse: int = 0, fuse_min_n: int = 64, chunk: int = 0, bottom_cells: int = 0):
+                 fuse: int = 0, fuse_min_n: int = 64, chunk: int = 0, bottom_cells: int = 0,
+                 graph: int = 0):
         L = lib()
         self.prob = prob
         rp = RunParams(ndims=prob.ndims, nrvars=2, mbc=1, maux=0,
@@ -180,7 +181,7 @@ class Solver:
         self.h = h
         try:
             t = Tuning(fuse_smoother=fuse, fuse_min_n=fuse_min_n, chunk=chunk,
-                       bottom_cells=bottom_cells)
+                       bottom_cells=bottom_cells, graph=graph)
             _check(L.bsam_gpu_set_tuning(h, ctypes.byref(t)), h, "bsam_gpu_set_tuning")
             self.patches, self.npatch = build_uniform(prob)
             _check(L.bsam_gpu_set_hierarchy(h, self.npatch, self.patches, 0), h,

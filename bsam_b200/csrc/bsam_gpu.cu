@@ -61,10 +61,15 @@ struct bsam_gpu {
   int* d_err = nullptr;  // kernel error flag (bounded waits that gave up)
   // Fused stages off by default: at L2-resident sizes the per-pass kernels
   // are faster (see the profiles); tests and tuning switch them on.
-  bsam_tuning tuning{0, 64, 0, 0, {0, 0, 0, 0}};
+  bsam_tuning tuning{0, 64, 0, 0, 0, {0, 0, 0}};
   int bottom_level = -1000;  // levels <= this run inside k_bottom
   int* d_tops = nullptr;     // top patch of each k_bottom chain
   int ntops = 0;
+  double denom = 1.0;        // nrvars * cells of the finest level (ErrorAFAS)
+  cudaGraphExec_t step_exec = nullptr;  // V-cycle loop graph (built lazily)
+  int graph_kernels_per_vcycle = 0;
+  double* d_trace = nullptr;  // per-V-cycle residuals of the graph path
+  double* h_trace = nullptr;  // pinned
   DevStatus* d_status = nullptr;
   DevStatus* h_status = nullptr;  // pinned
   std::vector<double> trace;
@@ -200,6 +205,62 @@ void vcycle(bsam_gpu* h, int level) {
   }
 }
 
+// ErrorAFAS on the finest level (afas:94, 108-221) into d_status.
+void launch_resid(bsam_gpu* h) {
+  const LevelPlan& F = plan(h, h->finestlevel);
+  if (h->rp.ndims == 2)
+    k_resid_norm<double, 2><<<F.nfine, block_dim(), 0, h->stream>>>(
+        h->d_patches, F.d_fine, h->d_partials, h->d_status, F.nfine, h->denom, h->rp.qerrortol);
+  else
+    k_resid_norm<double, 3><<<F.nfine, block_dim(), 0, h->stream>>>(
+        h->d_patches, F.d_fine, h->d_partials, h->d_status, F.nfine, h->denom, h->rp.qerrortol);
+  ++h->stats.launches;
+}
+
+// Captures the V-cycle loop of MultigridIterations (afas:69-104) as a graph
+// with one conditional WHILE node whose body is V-cycle + ErrorAFAS +
+// k_mg_loop; k_mg_loop sets the condition.  The default value 1 makes the
+// body run at least once per launch, as the reference's loop does.
+int build_step_graph(bsam_gpu* h) {
+  cudaGraph_t g = nullptr;
+  CU(cudaGraphCreate(&g, 0));
+  cudaGraphConditionalHandle handle;
+  cudaError_t e = cudaGraphConditionalHandleCreate(&handle, g, 1, cudaGraphCondAssignDefault);
+  cudaGraphNodeParams np{};
+  cudaGraphNode_t node;
+  if (e == cudaSuccess) {
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = handle;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    e = cudaGraphAddNode(&node, g, nullptr, 0, &np);
+  }
+  if (e == cudaSuccess) {
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    e = cudaStreamBeginCaptureToGraph(h->stream, body, nullptr, nullptr, 0,
+                                      cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      const int64_t before = h->stats.launches;
+      vcycle(h, h->finestlevel);
+      launch_resid(h);
+      k_mg_loop<<<1, 1, 0, h->stream>>>(h->d_status, h->d_trace, h->rp.maxvcycles,
+                                         h->rp.qerrortol, handle);
+      h->graph_kernels_per_vcycle = (int)(h->stats.launches - before) + 1;
+      h->stats.launches = before;
+      cudaGraph_t captured = nullptr;
+      e = cudaStreamEndCapture(h->stream, &captured);
+    }
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&h->step_exec, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    h->step_exec = nullptr;
+    cudaGetLastError();
+    return fail(h, BSAM_ERR_CUDA, std::string("step graph: ") + cudaGetErrorString(e));
+  }
+  return BSAM_OK;
+}
+
 int ghost_level(bsam_gpu* h, int level) {
   const LevelPlan& L = plan(h, level);
   for (int p : L.patches) {
@@ -288,6 +349,12 @@ static void free_hierarchy(bsam_gpu* h) {
   if (h->d_tops) cudaFree(h->d_tops);
   h->d_tops = nullptr;
   h->ntops = 0;
+  if (h->step_exec) cudaGraphExecDestroy(h->step_exec);
+  h->step_exec = nullptr;
+  if (h->d_trace) cudaFree(h->d_trace);
+  if (h->h_trace) cudaFreeHost(h->h_trace);
+  h->d_trace = nullptr;
+  h->h_trace = nullptr;
   if (h->d_arena) cudaFree(h->d_arena);
   if (h->d_patches) cudaFree(h->d_patches);
   if (h->d_partials) cudaFree(h->d_partials);
@@ -510,6 +577,17 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
   CU(cudaFuncSetAttribute(k_smooth3_fused<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)Fused3<double>::SMEM));
   CU(cudaMalloc(&h->d_partials, sizeof(double) * h->max_items));
+  CU(cudaMalloc(&h->d_trace, sizeof(double) * h->rp.maxvcycles));
+  CU(cudaMallocHost(&h->h_trace, sizeof(double) * h->rp.maxvcycles));
+  {
+    int64_t ncells = 0;
+    for (int p : plan(h, finestlevel).patches) {
+      int64_t c = 1;
+      for (int n = 0; n < nd; ++n) c *= h->hp[p].n[n];
+      ncells += c;
+    }
+    h->denom = (double)(h->rp.nrvars * ncells);  // L2Error's integralresult(2)
+  }
   if (h->bottom_level >= minlevel) {
     std::vector<int> tops = plan(h, h->bottom_level).patches;
     h->ntops = (int)tops.size();
@@ -556,6 +634,19 @@ static int copy_field(bsam_gpu* h, int patch, int field, double* host, int dir) 
     const int e0 = P.n[0] + 2 * g, e1 = P.n[1] + 2 * g, e2 = nd == 3 ? P.n[2] + 2 * g : 1;
     const size_t hcomp = (size_t)e0 * e1 * e2;
     double* hbase = host + comp * hcomp;
+    if (g == 1) {
+      // With the ghost ring every row of every plane sits at stride sy on the
+      // device (sz = sy * (n1 + 2)): one pitched copy per component.
+      if (dir == 0)
+        CU(cudaMemcpy2DAsync(dev, P.sy * sizeof(double), hbase, e0 * sizeof(double),
+                             e0 * sizeof(double), (size_t)e1 * e2, cudaMemcpyHostToDevice,
+                             h->stream));
+      else
+        CU(cudaMemcpy2DAsync(hbase, e0 * sizeof(double), dev, P.sy * sizeof(double),
+                             e0 * sizeof(double), (size_t)e1 * e2, cudaMemcpyDeviceToHost,
+                             h->stream));
+      continue;
+    }
     for (int kz = 0; kz < e2; ++kz) {
       const int k = nd == 3 ? kz + (1 - g) : 0;
       double* d = dev + (int64_t)(1 - g) + (int64_t)(1 - g) * P.sy + (int64_t)k * P.sz;
@@ -618,28 +709,39 @@ int bsam_gpu_multigrid_iterations(bsam_gpu* h, int* nvcycles, double* residual, 
     else k_source<double, 3><<<L.nfine, b, 0, h->stream>>>(h->d_patches, L.d_fine);
     ++h->stats.launches;
   }
-  const LevelPlan& F = plan(h, h->finestlevel);
-  int64_t ncells = 0;
-  for (int p : F.patches) {
-    int64_t c = 1;
-    for (int n = 0; n < nd; ++n) c *= h->hp[p].n[n];
-    ncells += c;
-  }
-  const double denom = (double)(h->rp.nrvars * ncells);
   h->trace.clear();
   int it = 0, conv = 0;
   double res = 0.0;
+  if (h->tuning.graph == 0 && !h->profiling) {
+    // The whole V-cycle loop as one graph launch (device-side WHILE node).
+    if (!h->step_exec) {
+      const int rc = build_step_graph(h);
+      if (rc) return rc;
+    }
+    k_mg_begin<<<1, 1, 0, h->stream>>>(h->d_status);
+    CU(cudaGetLastError());
+    CU(cudaGraphLaunch(h->step_exec, h->stream));
+    CU(cudaMemcpyAsync(h->h_status, h->d_status, sizeof(DevStatus), cudaMemcpyDeviceToHost,
+                       h->stream));
+    CU(cudaMemcpyAsync(h->h_trace, h->d_trace, sizeof(double) * h->rp.maxvcycles,
+                       cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    it = std::max(1, std::min(h->h_status->iters, h->rp.maxvcycles));
+    h->stats.launches += 1 + (int64_t)h->graph_kernels_per_vcycle * h->h_status->iters;
+    res = h->h_status->residual;
+    h->trace.assign(h->h_trace, h->h_trace + it);
+    if (nvcycles) *nvcycles = it;
+    if (residual) *residual = res;
+    if (converged) *converged = 0;
+    if (h->h_status->kerr)
+      return fail(h, BSAM_ERR_CUDA, "a fused smoothing stage timed out waiting for its copies");
+    if (!std::isfinite(res)) return fail(h, BSAM_ERR_DIVERGED, "residual is not finite");
+    if (converged) *converged = h->h_status->converged;
+    return BSAM_OK;
+  }
   for (it = 1; it <= h->rp.maxvcycles; ++it) {
     vcycle(h, h->finestlevel);
-    if (nd == 2)
-      k_resid_norm<double, 2><<<F.nfine, b, 0, h->stream>>>(h->d_patches, F.d_fine, h->d_partials,
-                                                           h->d_status, F.nfine, denom,
-                                                           h->rp.qerrortol);
-    else
-      k_resid_norm<double, 3><<<F.nfine, b, 0, h->stream>>>(h->d_patches, F.d_fine, h->d_partials,
-                                                           h->d_status, F.nfine, denom,
-                                                           h->rp.qerrortol);
-    ++h->stats.launches;
+    launch_resid(h);
     CU(cudaGetLastError());
     CU(cudaMemcpyAsync(h->h_status, h->d_status, sizeof(DevStatus), cudaMemcpyDeviceToHost,
                        h->stream));
@@ -701,8 +803,14 @@ int bsam_gpu_mass(bsam_gpu* h, double* mass) {
 
 int bsam_gpu_set_tuning(bsam_gpu* h, const bsam_tuning* t) {
   if (!h || !t) return BSAM_ERR_ARG;
-  if (t->fuse_smoother < -1 || t->fuse_smoother > 1 || t->chunk < 0) return BSAM_ERR_ARG;
+  if (t->fuse_smoother < -1 || t->fuse_smoother > 1 || t->chunk < 0 || t->graph < -1 ||
+      t->graph > 0)
+    return BSAM_ERR_ARG;
   h->tuning = *t;
+  if (h->step_exec) {
+    cudaGraphExecDestroy(h->step_exec);
+    h->step_exec = nullptr;
+  }
   return BSAM_OK;
 }
 

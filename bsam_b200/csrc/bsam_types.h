@@ -66,7 +66,7 @@ struct DevStatus {
   uint32_t ticket;     // last-block-done counter of the reductions
   int32_t converged;
   int32_t kerr;        // nonzero: a kernel's bounded wait gave up (see smooth_fused.cuh)
-  int32_t pad_;
+  int32_t iters;       // V-cycles done in the current MultigridIterations call
 };
 
 }  // namespace bsam

@@ -504,6 +504,30 @@ __global__ void k_setbc(const DevPatch* __restrict__ PT, int patch, int64_t ntot
   }
 }
 
+// ---- device-side V-cycle loop (MultigridIterations, afas:69-104) -----------
+
+// Start of a MultigridIterations call: no V-cycle done yet.
+static __global__ void k_mg_begin(DevStatus* __restrict__ st) {
+  st->iters = 0;
+  st->converged = 0;
+}
+
+// End of one V-cycle: record the residual and decide whether the conditional
+// WHILE node of the step graph runs another V-cycle.  Stops at convergence
+// (residual < qerrortol), after maxvcycles, on a non-finite residual (the
+// host reports it) or when a kernel recorded an error.
+static __global__ void k_mg_loop(DevStatus* __restrict__ st, double* __restrict__ trace, int maxv,
+                          double tol, cudaGraphConditionalHandle handle) {
+  const int it = st->iters + 1;
+  st->iters = it;
+  const double r = st->residual;
+  if (it <= maxv) trace[it - 1] = r;
+  const bool conv = r < tol;
+  st->converged = conv ? 1 : 0;
+  const bool again = !conv && it < maxv && isfinite(r) && st->kerr == 0;
+  cudaGraphSetConditional(handle, again ? 1u : 0u);
+}
+
 // h^d * sum(phi) over a patch interior (AfterStep2D/3D integral(1)).
 template <class T, int D>
 __global__ void __launch_bounds__(BLOCK_THREADS)

@@ -81,13 +81,18 @@ int bsam_gpu_create(bsam_gpu** h, int device, const bsam_run_params* p);
  *   bottom_cells   levels of at most this many cells run their whole part of
  *                  the V-cycle in one single-CTA launch; 0 = default (4096),
  *                  -1 = never
+ *   graph          0 = run the V-cycle loop of MultigridIterations as one
+ *                  captured CUDA graph with a device-side WHILE node (one
+ *                  launch per call); -1 = host loop (one launch per kernel,
+ *                  one host synchronisation per V-cycle)
  * Call before bsam_gpu_set_hierarchy. */
 typedef struct {
   int32_t fuse_smoother;
   int32_t fuse_min_n;
   int32_t chunk;
   int32_t bottom_cells;
-  int32_t reserved[4];
+  int32_t graph;
+  int32_t reserved[3];
 } bsam_tuning;
 int bsam_gpu_set_tuning(bsam_gpu* h, const bsam_tuning* t);
 

@@ -153,3 +153,19 @@ def test_bottom_kernel_matches_per_level_launches(gpu_lib, nd, n):
     with B.Solver(prob) as b:
         rb = b.run(2)
     assert np.array_equal(ra["q"], rb["q"]) and np.array_equal(ra["nvcycles"], rb["nvcycles"])
+
+
+@pytest.mark.parametrize("nd,n", [(2, 256), (3, 64)])
+def test_graph_loop_matches_host_loop(gpu_lib, nd, n):
+    # The device-side WHILE loop of the step graph stops after the same
+    # V-cycle as the host loop and leaves identical fields and residuals.
+    prob = W.config1(nsteps=3, n=n) if nd == 2 else W.config3(nsteps=2, n=n)
+    with B.Solver(prob, graph=-1) as a:
+        ra = a.run(prob.nsteps)
+        ta = a.trace()
+    with B.Solver(prob) as b:
+        rb = b.run(prob.nsteps)
+        tb = b.trace()
+    assert np.array_equal(ra["q"], rb["q"])
+    assert np.array_equal(ra["nvcycles"], rb["nvcycles"])
+    assert np.array_equal(ra["residual"], rb["residual"]) and np.array_equal(ta, tb)

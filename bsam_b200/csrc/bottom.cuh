@@ -43,14 +43,14 @@ __device__ __forceinline__ void block_restrict_load(const DevPatch& C, const Dev
     const int ic = idx % C.cn[0] + 1, rest = idx / C.cn[0];
     const int jc = rest % C.cn[1] + 1;
     const int kc = (D == 3) ? rest / C.cn[1] + 1 : 0;
-    restrict_cell<T, D>(C, P, ic, jc, kc);
+    restrict_cell<T, T, D>(C, P, ic, jc, kc);
   }
   __syncthreads();
   for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
     const int ic = idx % C.cn[0] + 1, rest = idx / C.cn[0];
     const int jc = rest % C.cn[1] + 1;
     const int kc = (D == 3) ? rest / C.cn[1] + 1 : 0;
-    coarse_load_cell<T, D>(C, P, ic, jc, kc);
+    coarse_load_cell<T, T, D>(C, P, ic, jc, kc);
   }
   __syncthreads();
 }
@@ -62,7 +62,7 @@ __device__ __forceinline__ void block_correct(const DevPatch& C, const DevPatch&
     const int I = idx % C.n[0] + 1, rest = idx / C.n[0];
     const int J = rest % C.n[1] + 1;
     const int K = (D == 3) ? rest / C.n[1] + 1 : 0;
-    correct_cell<T, D>(C, P, I, J, K);
+    correct_cell<T, T, D>(C, P, I, J, K);
   }
   __syncthreads();
 }

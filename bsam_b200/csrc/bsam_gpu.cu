@@ -9,6 +9,12 @@
 // i in [0, mx1+1] etc., lives at base + i + j*sy + k*sz.  The allocation
 // starts `lead` elements before element (0,0,0) so that every interior row
 // (i = 1) begins on a 128-byte boundary; sy is a multiple of 128 bytes.
+//
+// Patch records: the caller's patches keep their indices.  The FP64 form
+// runs the V-cycle on them directly.  The mixed form (mixed.cuh) appends one
+// working "twin" per finest-level patch: the caller's finest patch stays the
+// FP64 master state (put/get/mass/source/residual), the twin carries the
+// FP32 V-cycle; levels above 4096 cells are FP32, smaller ones FP64.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -23,14 +29,18 @@
 #include "kernels.cuh"
 #include "smooth_fused.cuh"
 #include "bottom.cuh"
+#include "mixed.cuh"
 
 using namespace bsam;
 
 namespace {
 
+// Levels with at most this many cells per patch stay FP64 in the mixed form.
+constexpr int64_t MIXED_FP64_CELLS = 4096;
+
 struct LevelPlan {
   int level = 0;
-  std::vector<int> patches;  // ApplyOnLevel order
+  std::vector<int> patches;  // records the V-cycle runs on (ApplyOnLevel order)
   Item* d_fine = nullptr;    // tiles over each patch's interior
   int nfine = 0;
   Item* d_coarse = nullptr;  // tiles over each patch's footprint in its parent
@@ -38,6 +48,7 @@ struct LevelPlan {
   Item* d_fused = nullptr;   // fused-stage tiles (tile x, tile y, z chunk)
   int nfused = 0;
   bool fused = false;
+  int prec = PREC_F64;
 };
 
 }  // namespace
@@ -47,20 +58,25 @@ struct bsam_gpu {
   cudaStream_t stream = nullptr;
   bsam_run_params rp{};
   bool have_hierarchy = false;
+  bool mixed = false;
   int minlevel = 0, finestlevel = 0;
+  int nuser = 0;                     // caller's patches: records [0, nuser)
   std::vector<bsam_patch_desc> desc;
   std::vector<DevPatch> hp;
-  std::vector<int64_t> field_elems;  // elements per field allocation, per patch
+  std::vector<int64_t> field_elems;  // elements per field allocation, per record
   DevPatch* d_patches = nullptr;
   char* d_arena = nullptr;
   size_t arena_bytes = 0;
-  std::vector<LevelPlan> levels;  // index level - minlevel
+  std::vector<LevelPlan> levels;     // index level - minlevel
+  std::vector<int> masters;          // finest-level state patches
+  Item* d_master = nullptr;          // tiles over the masters
+  int nmaster = 0;
   Item* d_items = nullptr;
   double* d_partials = nullptr;
   int max_items = 0;
   int* d_err = nullptr;  // kernel error flag (bounded waits that gave up)
   // Fused stages off by default: at L2-resident sizes the per-pass kernels
-  // are faster (see the profiles); tests and tuning switch them on.
+  // are faster; tests and tuning switch them on.
   bsam_tuning tuning{0, 64, 0, 0, 0, {0, 0, 0}};
   int bottom_level = -1000;  // levels <= this run inside k_bottom
   int* d_tops = nullptr;     // top patch of each k_bottom chain
@@ -79,7 +95,8 @@ struct bsam_gpu {
   bsam_gpu_stats stats{};
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pool;
   size_t ev_used = 0;
-  int64_t ev_cells = 0;  // cells of the finest level
+  int64_t ev_cells = 0;   // cells of the finest V-cycle level
+  int ev_bytes = 8;       // bytes per value on that level
 };
 
 namespace {
@@ -111,6 +128,8 @@ void tiles_for(int patch, const int* n, int ndims, std::vector<Item>& out) {
 
 dim3 block_dim() { return dim3(32, TILE_Y, 1); }
 
+int elem_bytes(int prec) { return prec == PREC_F32 ? 4 : 8; }
+
 // Timed finest-level smoothing stages: events are pooled and read back at
 // the next host synchronisation (drain_events).
 void stage_begin(bsam_gpu* h, int level) {
@@ -137,19 +156,35 @@ void drain_events(bsam_gpu* h) {
       h->stats.smooth_ms += ms;
       h->stats.smooth_stages += 1;
       h->stats.smooth_cells += h->ev_cells;
-      h->stats.smooth_bytes += 6.0 * sizeof(double) * (double)h->ev_cells;
+      h->stats.smooth_bytes += 6.0 * h->ev_bytes * (double)h->ev_cells;
     }
   }
   h->ev_used = 0;
 }
 
-// Launch helpers dispatching on dimension (FP64 path).
-template <int D>
-void launch_relax(bsam_gpu* h, const LevelPlan& L, int color) {
-  k_relax<double, D><<<L.nfine, block_dim(), 0, h->stream>>>(h->d_patches, L.d_fine, color);
+// ---- typed launches -----------------------------------------------------------
+
+template <class T, int D>
+void launch_relax_t(bsam_gpu* h, const LevelPlan& L, int color) {
+  k_relax<T, D><<<L.nfine, block_dim(), 0, h->stream>>>(h->d_patches, L.d_fine, color);
 }
 
-int ghost_level(bsam_gpu* h, int level);
+template <class TC, class TP, int D>
+void launch_transfer_t(bsam_gpu* h, const LevelPlan& L, int what) {
+  if (what == 0) {
+    k_restrict<TC, TP, D><<<L.ncoarse, block_dim(), 0, h->stream>>>(h->d_patches, L.d_coarse);
+    k_coarse_load<TC, TP, D><<<L.ncoarse, block_dim(), 0, h->stream>>>(h->d_patches, L.d_coarse);
+  } else {
+    k_correct<TC, TP, D><<<L.nfine, block_dim(), 0, h->stream>>>(h->d_patches, L.d_fine);
+  }
+}
+
+template <int D>
+void launch_transfer_d(bsam_gpu* h, const LevelPlan& L, int pc, int pp, int what) {
+  if (pc == PREC_F32 && pp == PREC_F32) launch_transfer_t<float, float, D>(h, L, what);
+  else if (pc == PREC_F32) launch_transfer_t<float, double, D>(h, L, what);
+  else launch_transfer_t<double, double, D>(h, L, what);
+}
 
 // LevelRelax (afas:523-547).  dir selects the buffers of a fused level:
 // 0 = pre-smoothing (q -> qb), 1 = post-smoothing (qb -> q).
@@ -157,23 +192,42 @@ void relax_level(bsam_gpu* h, int level, int dir) {
   const LevelPlan& L = plan(h, level);
   stage_begin(h, level);
   if (L.fused) {
-    k_smooth3_fused<double><<<L.nfused, Fused3<double>::THREADS, Fused3<double>::SMEM,
-                              h->stream>>>(h->d_patches, L.d_fused, dir, 0, h->d_err);
+    if (L.prec == PREC_F32)
+      k_smooth3_fused<float><<<L.nfused, Fused3<float>::THREADS, Fused3<float>::SMEM, h->stream>>>(
+          h->d_patches, L.d_fused, dir, 0, h->d_err);
+    else
+      k_smooth3_fused<double><<<L.nfused, Fused3<double>::THREADS, Fused3<double>::SMEM,
+                                h->stream>>>(h->d_patches, L.d_fused, dir, 0, h->d_err);
     ++h->stats.launches;
   } else {
     for (int pass = 0; pass < h->rp.nsmoothingpasses; ++pass)
       for (int color = 0; color < 2; ++color) {
-        if (h->rp.ndims == 2) launch_relax<2>(h, L, color);
-        else launch_relax<3>(h, L, color);
+        if (h->rp.ndims == 2) {
+          if (L.prec == PREC_F32) launch_relax_t<float, 2>(h, L, color);
+          else launch_relax_t<double, 2>(h, L, color);
+        } else {
+          if (L.prec == PREC_F32) launch_relax_t<float, 3>(h, L, color);
+          else launch_relax_t<double, 3>(h, L, color);
+        }
         ++h->stats.launches;
       }
   }
   stage_end(h, level);
 }
 
+void transfer(bsam_gpu* h, int level, int what) {
+  const LevelPlan& L = plan(h, level);
+  const int pp = plan(h, level - 1).prec;
+  if (h->rp.ndims == 2) launch_transfer_d<2>(h, L, L.prec, pp, what);
+  else launch_transfer_d<3>(h, L, L.prec, pp, what);
+  h->stats.launches += what == 0 ? 2 : 1;
+}
+
+// AFASVcycle (afas:488-521).
 void vcycle(bsam_gpu* h, int level) {
   if (level == h->bottom_level) {
-    // AFASVcycle(level) down to the coarsest level in one launch (bottom.cuh).
+    // AFASVcycle(level) down to the coarsest level in one launch (bottom.cuh);
+    // bottom levels are FP64 in both forms.
     if (h->rp.ndims == 2)
       k_bottom<double, 2><<<h->ntops, BOTTOM_THREADS, 0, h->stream>>>(h->d_patches, h->d_tops,
                                                                       h->rp.nsmoothingpasses);
@@ -185,42 +239,72 @@ void vcycle(bsam_gpu* h, int level) {
   }
   relax_level(h, level, 0);  // LevelRelax (afas:499)
   if (level > h->minlevel) {
-    const LevelPlan& L = plan(h, level);
-    const dim3 b = block_dim();
-    if (h->rp.ndims == 2) {
-      k_restrict<double, 2><<<L.ncoarse, b, 0, h->stream>>>(h->d_patches, L.d_coarse);
-      k_coarse_load<double, 2><<<L.ncoarse, b, 0, h->stream>>>(h->d_patches, L.d_coarse);
-    } else {
-      k_restrict<double, 3><<<L.ncoarse, b, 0, h->stream>>>(h->d_patches, L.d_coarse);
-      k_coarse_load<double, 3><<<L.ncoarse, b, 0, h->stream>>>(h->d_patches, L.d_coarse);
-    }
-    h->stats.launches += 2;
-    vcycle(h, level - 1);  // afas:511
-    if (h->rp.ndims == 2)
-      k_correct<double, 2><<<L.nfine, b, 0, h->stream>>>(h->d_patches, L.d_fine);
-    else
-      k_correct<double, 3><<<L.nfine, b, 0, h->stream>>>(h->d_patches, L.d_fine);
-    ++h->stats.launches;
+    transfer(h, level, 0);   // RestrictSolution + CoarseLoadingFunction (afas:503-509)
+    vcycle(h, level - 1);    // afas:511
+    transfer(h, level, 1);   // CorrectFine (afas:513)
     relax_level(h, level, 1);  // afas:517
   }
 }
 
-// ErrorAFAS on the finest level (afas:94, 108-221) into d_status.
+// ErrorAFAS on the finest level (afas:94, 108-221) into d_status.  In the
+// mixed form the same FP64 norm is taken by k_defect, which also prepares
+// the twins for the next FP32 V-cycle.
 void launch_resid(bsam_gpu* h) {
-  const LevelPlan& F = plan(h, h->finestlevel);
-  if (h->rp.ndims == 2)
-    k_resid_norm<double, 2><<<F.nfine, block_dim(), 0, h->stream>>>(
-        h->d_patches, F.d_fine, h->d_partials, h->d_status, F.nfine, h->denom, h->rp.qerrortol);
-  else
-    k_resid_norm<double, 3><<<F.nfine, block_dim(), 0, h->stream>>>(
-        h->d_patches, F.d_fine, h->d_partials, h->d_status, F.nfine, h->denom, h->rp.qerrortol);
+  const int nd = h->rp.ndims;
+  const dim3 b = block_dim();
+  if (!h->mixed) {
+    if (nd == 2)
+      k_resid_norm<double, 2><<<h->nmaster, b, 0, h->stream>>>(
+          h->d_patches, h->d_master, h->d_partials, h->d_status, h->nmaster, h->denom,
+          h->rp.qerrortol);
+    else
+      k_resid_norm<double, 3><<<h->nmaster, b, 0, h->stream>>>(
+          h->d_patches, h->d_master, h->d_partials, h->d_status, h->nmaster, h->denom,
+          h->rp.qerrortol);
+  } else {
+    const bool f32 = plan(h, h->finestlevel).prec == PREC_F32;
+#define DEFECT(TW, D)                                                                        \
+  k_defect<TW, D><<<h->nmaster, b, 0, h->stream>>>(h->d_patches, h->d_master, h->d_partials, \
+                                                   h->d_status, h->nmaster, h->denom,        \
+                                                   h->rp.qerrortol)
+    if (nd == 2) {
+      if (f32) DEFECT(float, 2);
+      else DEFECT(double, 2);
+    } else {
+      if (f32) DEFECT(float, 3);
+      else DEFECT(double, 3);
+    }
+#undef DEFECT
+  }
   ++h->stats.launches;
 }
 
+// Mixed form: q64 += q32 - fl32(q64) after the FP32 V-cycle.
+void launch_update(bsam_gpu* h) {
+  const int nd = h->rp.ndims;
+  const bool f32 = plan(h, h->finestlevel).prec == PREC_F32;
+  const dim3 b = block_dim();
+  if (nd == 2) {
+    if (f32) k_update<float, 2><<<h->nmaster, b, 0, h->stream>>>(h->d_patches, h->d_master);
+    else k_update<double, 2><<<h->nmaster, b, 0, h->stream>>>(h->d_patches, h->d_master);
+  } else {
+    if (f32) k_update<float, 3><<<h->nmaster, b, 0, h->stream>>>(h->d_patches, h->d_master);
+    else k_update<double, 3><<<h->nmaster, b, 0, h->stream>>>(h->d_patches, h->d_master);
+  }
+  ++h->stats.launches;
+}
+
+// One outer iteration of MultigridIterations: V-cycle, then ErrorAFAS.
+void iteration(bsam_gpu* h) {
+  vcycle(h, h->finestlevel);
+  if (h->mixed) launch_update(h);
+  launch_resid(h);
+}
+
 // Captures the V-cycle loop of MultigridIterations (afas:69-104) as a graph
-// with one conditional WHILE node whose body is V-cycle + ErrorAFAS +
-// k_mg_loop; k_mg_loop sets the condition.  The default value 1 makes the
-// body run at least once per launch, as the reference's loop does.
+// with one conditional WHILE node whose body is one iteration + k_mg_loop;
+// k_mg_loop sets the condition.  The default value 1 makes the body run at
+// least once per launch, as the reference's loop does.
 int build_step_graph(bsam_gpu* h) {
   cudaGraph_t g = nullptr;
   CU(cudaGraphCreate(&g, 0));
@@ -241,8 +325,7 @@ int build_step_graph(bsam_gpu* h) {
                                       cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
       const int64_t before = h->stats.launches;
-      vcycle(h, h->finestlevel);
-      launch_resid(h);
+      iteration(h);
       k_mg_loop<<<1, 1, 0, h->stream>>>(h->d_status, h->d_trace, h->rp.maxvcycles,
                                          h->rp.qerrortol, handle);
       h->graph_kernels_per_vcycle = (int)(h->stats.launches - before) + 1;
@@ -261,10 +344,11 @@ int build_step_graph(bsam_gpu* h) {
   return BSAM_OK;
 }
 
+// SetBC on the FP64 state patches of one level.
 int ghost_level(bsam_gpu* h, int level) {
-  const LevelPlan& L = plan(h, level);
-  for (int p : L.patches) {
+  for (int p = 0; p < h->nuser; ++p) {
     const DevPatch& P = h->hp[p];
+    if (P.level != level || P.prec != PREC_F64 || P.delta) continue;
     int64_t total = (int64_t)(P.n[0] + 2) * (P.n[1] + 2) * (h->rp.ndims == 3 ? P.n[2] + 2 : 1);
     int nb = (int)((total + 255) / 256);
     if (h->rp.ndims == 2) k_setbc<double, 2><<<nb, 256, 0, h->stream>>>(h->d_patches, p, total);
@@ -287,6 +371,12 @@ int face_rule(int ndims, int face, int code, int* rule) {
     return -1;  // periodic (2) is not supported by this build
   }
   return 0;
+}
+
+int64_t cells_of(const int* mx, int nd) {
+  int64_t c = 1;
+  for (int n = 0; n < nd; ++n) c *= mx[n];
+  return c;
 }
 
 }  // namespace
@@ -317,13 +407,15 @@ int bsam_gpu_create(bsam_gpu** out, int device, const bsam_run_params* p) {
   if (p->ndims < 2 || p->ndims > 3 || p->nrvars != 2 || p->mbc != 1 || p->maux != 0 ||
       p->errortype != 1 || p->nsmoothingpasses < 1 || p->maxvcycles < 1)
     return BSAM_ERR_UNSUPPORTED;
-  if (p->precision != BSAM_PREC_FP64) return BSAM_ERR_UNSUPPORTED;
+  if (p->precision != BSAM_PREC_FP64 && p->precision != BSAM_PREC_MIXED)
+    return BSAM_ERR_UNSUPPORTED;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= device || device < 0)
     return BSAM_ERR_NODEVICE;
   h = new bsam_gpu();
   h->device = device;
   h->rp = *p;
+  h->mixed = p->precision == BSAM_PREC_MIXED;
   if (cudaSetDevice(device) != cudaSuccess) {
     delete h;
     return BSAM_ERR_NODEVICE;
@@ -341,28 +433,27 @@ int bsam_gpu_create(bsam_gpu** out, int device, const bsam_run_params* p) {
 }
 
 static void free_hierarchy(bsam_gpu* h) {
-  for (auto& L : h->levels) {
-    L.d_fine = nullptr;
-    L.d_coarse = nullptr;
-  }
   if (h->d_items) cudaFree(h->d_items);
   if (h->d_tops) cudaFree(h->d_tops);
-  h->d_tops = nullptr;
-  h->ntops = 0;
   if (h->step_exec) cudaGraphExecDestroy(h->step_exec);
-  h->step_exec = nullptr;
   if (h->d_trace) cudaFree(h->d_trace);
   if (h->h_trace) cudaFreeHost(h->h_trace);
-  h->d_trace = nullptr;
-  h->h_trace = nullptr;
   if (h->d_arena) cudaFree(h->d_arena);
   if (h->d_patches) cudaFree(h->d_patches);
   if (h->d_partials) cudaFree(h->d_partials);
   h->d_items = nullptr;
+  h->d_tops = nullptr;
+  h->ntops = 0;
+  h->step_exec = nullptr;
+  h->d_trace = nullptr;
+  h->h_trace = nullptr;
   h->d_arena = nullptr;
   h->d_patches = nullptr;
   h->d_partials = nullptr;
+  h->d_master = nullptr;
+  h->nmaster = 0;
   h->levels.clear();
+  h->masters.clear();
   h->hp.clear();
   h->desc.clear();
   h->field_elems.clear();
@@ -382,40 +473,59 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
     return fail(h, BSAM_ERR_UNSUPPORTED, "levels above the root (AMR) need coarse-fine ghosts");
   h->minlevel = minlevel;
   h->finestlevel = finestlevel;
+  h->nuser = npatch;
   h->levels.assign(finestlevel - minlevel + 1, LevelPlan{});
+  for (int l = minlevel; l <= finestlevel; ++l) plan(h, l).level = l;
+  h->desc.assign(patches, patches + npatch);
+
   // Bottom level: the finest level such that it and every coarser level hold
   // at most bottom_cells cells per patch (uniform hierarchies only).
   h->bottom_level = -1000;
-  {
-    const int bmax = h->tuning.bottom_cells == 0 ? BOTTOM_MAX_CELLS : h->tuning.bottom_cells;
-    if (bmax > 0 && finestlevel == 0) {
-      for (int l = minlevel; l <= finestlevel; ++l) {
-        bool small = true;
-        for (int p = 0; p < npatch; ++p)
-          if (patches[p].level == l) {
-            int64_t c = 1;
-            for (int n = 0; n < nd; ++n) c *= patches[p].mx[n];
-            small = small && c <= bmax;
-          }
-        if (!small) break;
-        h->bottom_level = l;
-      }
-      if (h->bottom_level - minlevel + 1 > BOTTOM_MAX_DEPTH) h->bottom_level = -1000;
+  const int bmax = h->tuning.bottom_cells == 0 ? BOTTOM_MAX_CELLS : h->tuning.bottom_cells;
+  if (bmax > 0 && finestlevel == 0) {
+    for (int l = minlevel; l <= finestlevel; ++l) {
+      bool small = true;
+      for (int p = 0; p < npatch; ++p)
+        if (patches[p].level == l) small = small && cells_of(patches[p].mx, nd) <= bmax;
+      if (!small) break;
+      h->bottom_level = l;
     }
+    if (h->bottom_level - minlevel + 1 > BOTTOM_MAX_DEPTH) h->bottom_level = -1000;
   }
-  for (int l = minlevel; l <= finestlevel; ++l) plan(h, l).level = l;
-  h->desc.assign(patches, patches + npatch);
-  h->hp.assign(npatch, DevPatch{});
-  h->field_elems.assign(npatch, 0);
+  // Mixed form: levels at or below this size stay FP64 (the bottom of the
+  // V-cycle, including the coarsest level).
+  const int64_t fp64_cells = std::max<int64_t>(MIXED_FP64_CELLS, std::max(bmax, 0));
+
+  // Records: the caller's patches, then one twin per finest-level patch in
+  // the mixed form.
+  std::vector<int> twin_of(npatch, -1);
+  int nrec = npatch;
+  for (int p = 0; p < npatch; ++p)
+    if (patches[p].level == finestlevel) {
+      h->masters.push_back(p);
+      if (h->mixed) twin_of[p] = nrec++;
+    }
+  h->hp.assign(nrec, DevPatch{});
+  h->field_elems.assign(nrec, 0);
+  // rec_src[r]: the caller's patch whose geometry record r has.
+  std::vector<int> rec_src(nrec);
+  for (int p = 0; p < npatch; ++p) {
+    rec_src[p] = p;
+    if (twin_of[p] >= 0) rec_src[twin_of[p]] = p;
+  }
 
   const double eps2 = h->rp.eps * h->rp.eps;
   size_t total = 0;
-  std::vector<size_t> offs(npatch);
-  for (int p = 0; p < npatch; ++p) {
+  std::vector<size_t> offs(nrec);
+  std::vector<int> nfields(nrec, 0);
+  std::vector<char> want_qold(nrec, 0), want_qs(nrec, 0);
+  for (int r = 0; r < nrec; ++r) {
+    const int p = rec_src[r];
+    const bool is_twin = r >= npatch;
     const bsam_patch_desc& d = patches[p];
     if (d.level < minlevel || d.level > finestlevel)
       return fail(h, BSAM_ERR_ARG, "patch level out of range");
-    DevPatch& P = h->hp[p];
+    DevPatch& P = h->hp[r];
     P.ndims = nd;
     for (int n = 0; n < 3; ++n) {
       P.n[n] = n < nd ? d.mx[n] : 1;
@@ -423,8 +533,14 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
     }
     P.parent = d.parent;
     P.level = d.level;
-    P.prec = PREC_F64;
     P.problem = 0;
+    P.twin = is_twin ? -1 : twin_of[p];
+    // Precision of the record.
+    const int64_t ncell = cells_of(P.n, nd);
+    if (!h->mixed || (!is_twin && d.level == finestlevel) || ncell <= fp64_cells)
+      P.prec = PREC_F64;
+    else
+      P.prec = PREC_F32;
     if (d.parent >= 0) {
       if (d.parent >= npatch || patches[d.parent].level != d.level - 1)
         return fail(h, BSAM_ERR_ARG, "parent must be a patch on the next coarser level");
@@ -456,12 +572,19 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
       if (rule == BC_NONE) P.wt = 0;
     }
     if (!P.wt) return fail(h, BSAM_ERR_UNSUPPORTED, "internal faces need AMR support");
-    // Fused stages: 3D levels with a parent (the coarsest level relaxes once
-    // per V-cycle and keeps the in-place path), all faces physical.
+    // Does the V-cycle run on this record?  (Not on the masters of the mixed form.)
+    const bool in_vcycle = !(h->mixed && !is_twin && d.level == finestlevel);
+    // Mixed form: the V-cycle levels carry a correction of the master state
+    // (mixed.cuh); a reflecting face maps a correction to its negative.
+    P.delta = (h->mixed && in_vcycle) ? 1 : 0;
+    if (P.delta)
+      for (int f = 0; f < 2 * nd; ++f)
+        if (P.bc[f] == BC_REFLECT) P.bc[f] = BC_NEGATE;
+    // Fused stages: 3D V-cycle levels with a parent above the bottom, all
+    // faces physical.
     const int fmin = std::max(8, h->tuning.fuse_min_n);
-    P.fused = (h->tuning.fuse_smoother != 0 && nd == 3 && d.parent >= 0 && P.wt &&
-               d.level > h->bottom_level &&
-               P.n[0] >= fmin && P.n[1] >= fmin && P.n[2] >= fmin)
+    P.fused = (h->tuning.fuse_smoother != 0 && nd == 3 && in_vcycle && d.parent >= 0 &&
+               d.level > h->bottom_level && P.n[0] >= fmin && P.n[1] >= fmin && P.n[2] >= fmin)
                   ? 1
                   : 0;
     if (P.fused) {
@@ -475,22 +598,23 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
       }
       P.zchunk = std::max(1, std::min(chunk, P.n[2]));
     }
-    // Layout (FP64): rows aligned to 128 bytes.  The slack after the last row
-    // keeps the fused kernel's halo'd row copies inside the allocation.
-    const int64_t A = 128 / sizeof(double), lead = A - 1;
+    // Layout: rows aligned to 128 bytes; the slack after the last row keeps
+    // the fused kernel's halo'd row copies inside the allocation.
+    const int es = elem_bytes(P.prec);
+    const int64_t A = 128 / es, lead = A - 1;
     P.sy = roundup(lead + P.n[0] + 2, A);
     P.sz = nd == 3 ? P.sy * (P.n[1] + 2) : 0;
     const int64_t vol = nd == 3 ? P.sz * (P.n[2] + 2) : P.sy * (P.n[1] + 2);
-    h->field_elems[p] = roundup(lead + vol + 64, 32);
-    offs[p] = total;
-    const bool parent_of_any = [&] {
-      for (int c = 0; c < npatch; ++c)
-        if (patches[c].parent == p) return true;
-      return false;
-    }();
-    const int nfields = 2 /*q*/ + 2 /*f*/ + 2 /*qold*/ + (parent_of_any ? 2 : 0) +
-                        (P.fused ? 2 : 0);
-    total += (size_t)h->field_elems[p] * nfields * sizeof(double);
+    h->field_elems[r] = roundup(lead + vol + 64, 256 / es);
+    offs[r] = total;
+    bool parent_of_any = false;
+    if (in_vcycle)
+      for (int c = 0; c < npatch; ++c) parent_of_any |= patches[c].parent == p;
+    const bool has_qold = !is_twin && d.level >= 0 && P.prec == PREC_F64 &&
+                          (!h->mixed || d.level == finestlevel);
+    nfields[r] = 2 /*q*/ + 2 /*f*/ + (has_qold ? 2 : 0) + (parent_of_any ? 2 : 0) +
+                 (P.fused ? 2 : 0) + (P.delta ? 1 : 0);
+    total += (size_t)h->field_elems[r] * nfields[r] * es;
     // Problem constants (problem.f90:183-187): h2 = h*h; dt/h2; eps2/h2; 2d*eps2/h2.
     P.h = d.dx;
     const double h2 = d.dx * d.dx;
@@ -500,27 +624,33 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
     P.tmp1 = h->rp.dt / h2;
     P.tmp2 = eps2 / h2;
     P.tmp3 = (2.0 * nd) * eps2 / h2;
-    plan(h, d.level).patches.push_back(p);
+    if (in_vcycle) plan(h, d.level).patches.push_back(r);
+    want_qold[r] = has_qold;
+    want_qs[r] = parent_of_any;
   }
   if (cudaMalloc(&h->d_arena, total) != cudaSuccess)
     return fail(h, BSAM_ERR_NOMEM, "arena allocation failed");
   h->arena_bytes = total;
   CU(cudaMemsetAsync(h->d_arena, 0, total, h->stream));
-  for (int p = 0; p < npatch; ++p) {
-    DevPatch& P = h->hp[p];
-    double* base = reinterpret_cast<double*>(h->d_arena + offs[p]);
-    const int64_t fe = h->field_elems[p], lead = 128 / sizeof(double) - 1;
+  for (int r = 0; r < nrec; ++r) {
+    DevPatch& P = h->hp[r];
+    const int es = elem_bytes(P.prec);
+    char* base = h->d_arena + offs[r];
+    const int64_t fe = h->field_elems[r], lead = 128 / es - 1;
     int slot = 0;
-    auto next = [&]() { return (void*)(base + fe * (slot++) + lead); };
+    auto next = [&]() { return (void*)(base + (fe * (slot++) + lead) * es); };
+    const bool has_qold = want_qold[r], has_qs = want_qs[r];
     P.q[0] = next();
     P.q[1] = next();
     P.f[0] = next();
     P.f[1] = next();
-    P.qo[0] = next();
-    P.qo[1] = next();
-    bool parent_of_any = false;
-    for (int c = 0; c < npatch; ++c) parent_of_any |= patches[c].parent == p;
-    if (parent_of_any) {
+    P.qo[0] = P.qo[1] = nullptr;
+    P.qs[0] = P.qs[1] = nullptr;
+    if (has_qold) {
+      P.qo[0] = next();
+      P.qo[1] = next();
+    }
+    if (has_qs) {
       P.qs[0] = next();
       P.qs[1] = next();
     }
@@ -528,13 +658,21 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
       P.qb[0] = next();
       P.qb[1] = next();
     }
+    P.bs = P.delta ? next() : nullptr;
   }
-  // Work lists.
+  // Parents of the twins are the masters' parents.
+  for (int r = npatch; r < nrec; ++r) h->hp[r].parent = h->hp[rec_src[r]].parent;
+
+  // Level precisions and work lists.
   std::vector<Item> all;
-  std::vector<std::pair<int, int>> spans_fine(h->levels.size()), spans_coarse(h->levels.size()),
-      spans_fused(h->levels.size());
-  for (size_t li = 0; li < h->levels.size(); ++li) {
+  const size_t nl = h->levels.size();
+  std::vector<std::pair<int, int>> spans_fine(nl), spans_coarse(nl), spans_fused(nl);
+  for (size_t li = 0; li < nl; ++li) {
     LevelPlan& L = h->levels[li];
+    if (L.patches.empty()) return fail(h, BSAM_ERR_ARG, "a level between minlevel and finest is empty");
+    L.prec = h->hp[L.patches[0]].prec;
+    for (int p : L.patches)
+      if (h->hp[p].prec != L.prec) return fail(h, BSAM_ERR_ARG, "mixed precisions on one level");
     int s = (int)all.size();
     for (int p : L.patches) tiles_for(p, h->hp[p].n, nd, all);
     spans_fine[li] = {s, (int)all.size() - s};
@@ -543,7 +681,7 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
       if (h->hp[p].parent >= 0) tiles_for(p, h->hp[p].cn, nd, all);
     spans_coarse[li] = {s, (int)all.size() - s};
     // A level runs fused stages only when every patch on it does.
-    L.fused = !L.patches.empty();
+    L.fused = true;
     for (int p : L.patches) L.fused = L.fused && h->hp[p].fused;
     if (!L.fused)
       for (int p : L.patches) h->hp[p].fused = 0;
@@ -560,11 +698,15 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
       }
     spans_fused[li] = {s, (int)all.size() - s};
   }
+  const int s_master = (int)all.size();
+  for (int p : h->masters) tiles_for(p, h->hp[p].n, nd, all);
+  h->nmaster = (int)all.size() - s_master;
+
   CU(cudaMalloc(&h->d_items, all.size() * sizeof(Item)));
   CU(cudaMemcpyAsync(h->d_items, all.data(), all.size() * sizeof(Item), cudaMemcpyHostToDevice,
                      h->stream));
-  h->max_items = 1;
-  for (size_t li = 0; li < h->levels.size(); ++li) {
+  h->max_items = std::max(1, h->nmaster);
+  for (size_t li = 0; li < nl; ++li) {
     LevelPlan& L = h->levels[li];
     L.d_fine = h->d_items + spans_fine[li].first;
     L.nfine = spans_fine[li].second;
@@ -574,30 +716,30 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
     L.nfused = spans_fused[li].second;
     h->max_items = std::max(h->max_items, L.nfine);
   }
+  h->d_master = h->d_items + s_master;
   CU(cudaFuncSetAttribute(k_smooth3_fused<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)Fused3<double>::SMEM));
+  CU(cudaFuncSetAttribute(k_smooth3_fused<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)Fused3<float>::SMEM));
   CU(cudaMalloc(&h->d_partials, sizeof(double) * h->max_items));
   CU(cudaMalloc(&h->d_trace, sizeof(double) * h->rp.maxvcycles));
   CU(cudaMallocHost(&h->h_trace, sizeof(double) * h->rp.maxvcycles));
   {
     int64_t ncells = 0;
-    for (int p : plan(h, finestlevel).patches) {
-      int64_t c = 1;
-      for (int n = 0; n < nd; ++n) c *= h->hp[p].n[n];
-      ncells += c;
-    }
+    for (int p : h->masters) ncells += cells_of(h->hp[p].n, nd);
     h->denom = (double)(h->rp.nrvars * ncells);  // L2Error's integralresult(2)
   }
   if (h->bottom_level >= minlevel) {
     std::vector<int> tops = plan(h, h->bottom_level).patches;
+    for (int p : tops)
+      if (h->hp[p].prec != PREC_F64) return fail(h, BSAM_ERR_ARG, "bottom levels must be FP64");
     h->ntops = (int)tops.size();
     CU(cudaMalloc(&h->d_tops, sizeof(int) * tops.size()));
     CU(cudaMemcpyAsync(h->d_tops, tops.data(), sizeof(int) * tops.size(),
                        cudaMemcpyHostToDevice, h->stream));
   }
-  CU(cudaMemsetAsync(h->d_err, 0, sizeof(int), h->stream));
-  CU(cudaMalloc(&h->d_patches, sizeof(DevPatch) * npatch));
-  CU(cudaMemcpyAsync(h->d_patches, h->hp.data(), sizeof(DevPatch) * npatch,
+  CU(cudaMalloc(&h->d_patches, sizeof(DevPatch) * nrec));
+  CU(cudaMemcpyAsync(h->d_patches, h->hp.data(), sizeof(DevPatch) * nrec,
                      cudaMemcpyHostToDevice, h->stream));
   CU(cudaMemsetAsync(h->d_status, 0, sizeof(DevStatus), h->stream));
   CU(cudaStreamSynchronize(h->stream));
@@ -615,6 +757,7 @@ static int field_ptr(bsam_gpu* h, int patch, int field, int comp, double** ptr, 
     case BSAM_FIELD_F: p = P.f[comp]; *interior = true; break;
     default: return BSAM_ERR_ARG;
   }
+  if (!p) return BSAM_ERR_UNSUPPORTED;
   *ptr = static_cast<double*>(p);
   return BSAM_OK;
 }
@@ -622,14 +765,17 @@ static int field_ptr(bsam_gpu* h, int patch, int field, int comp, double** ptr, 
 // Copy between a Fortran array and the pitched device field; dir 0 = H2D.
 static int copy_field(bsam_gpu* h, int patch, int field, double* host, int dir) {
   if (!h || !h->have_hierarchy) return BSAM_ERR_STATE;
-  if (patch < 0 || patch >= (int)h->hp.size() || !host) return BSAM_ERR_ARG;
+  if (patch < 0 || patch >= h->nuser || !host) return BSAM_ERR_ARG;
   CU(cudaSetDevice(h->device));
   const DevPatch& P = h->hp[patch];
+  if (P.prec != PREC_F64 || P.delta)
+    return fail(h, BSAM_ERR_UNSUPPORTED, "the fields of mixed-precision working levels are internal");
   const int nd = h->rp.ndims;
   for (int comp = 0; comp < 2; ++comp) {
     double* dev;
     bool interior;
-    if (field_ptr(h, patch, field, comp, &dev, &interior)) return BSAM_ERR_ARG;
+    const int rc = field_ptr(h, patch, field, comp, &dev, &interior);
+    if (rc) return fail(h, rc, "field not held for this patch");
     const int g = interior ? 0 : 1;  // ghost layers present in the host array
     const int e0 = P.n[0] + 2 * g, e1 = P.n[1] + 2 * g, e2 = nd == 3 ? P.n[2] + 2 * g : 1;
     const size_t hcomp = (size_t)e0 * e1 * e2;
@@ -648,8 +794,8 @@ static int copy_field(bsam_gpu* h, int patch, int field, double* host, int dir) 
       continue;
     }
     for (int kz = 0; kz < e2; ++kz) {
-      const int k = nd == 3 ? kz + (1 - g) : 0;
-      double* d = dev + (int64_t)(1 - g) + (int64_t)(1 - g) * P.sy + (int64_t)k * P.sz;
+      const int k = nd == 3 ? kz + 1 : 0;
+      double* d = dev + 1 + P.sy + (int64_t)k * P.sz;
       double* hs = hbase + (size_t)kz * e0 * e1;
       if (dir == 0)
         CU(cudaMemcpy2DAsync(d, P.sy * sizeof(double), hs, e0 * sizeof(double),
@@ -683,9 +829,10 @@ int bsam_gpu_set_ghost(bsam_gpu* h) {
 int bsam_gpu_copy_q_to_qold(bsam_gpu* h) {
   if (!h || !h->have_hierarchy) return BSAM_ERR_STATE;
   CU(cudaSetDevice(h->device));
-  const int64_t lead = 128 / sizeof(double) - 1;
-  for (size_t p = 0; p < h->hp.size(); ++p) {
+  for (int p = 0; p < h->nuser; ++p) {
     const DevPatch& P = h->hp[p];
+    if (!P.qo[0]) continue;  // qold is read only on levels >= root (Source)
+    const int64_t lead = 128 / sizeof(double) - 1;
     for (int c = 0; c < 2; ++c)
       CU(cudaMemcpyAsync(static_cast<double*>(P.qo[c]) - lead, static_cast<double*>(P.q[c]) - lead,
                          h->field_elems[p] * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
@@ -698,17 +845,17 @@ int bsam_gpu_multigrid_iterations(bsam_gpu* h, int* nvcycles, double* residual, 
   CU(cudaSetDevice(h->device));
   const int nd = h->rp.ndims;
   const dim3 b = block_dim();
-  // GetSourceFunction + UpdateSourceFunction on levels finest..root
-  // (afas:57-64).  FillDown(source) and FillDown(solution) (afas:47, 66, 73,
-  // 90) only write regions that RestrictSolution / CoarseLoadingFunction
-  // overwrite before any read when the levels are nested uniform grids, so
-  // they are not issued.
-  for (int l = h->finestlevel; l >= 0; --l) {
-    const LevelPlan& L = plan(h, l);
-    if (nd == 2) k_source<double, 2><<<L.nfine, b, 0, h->stream>>>(h->d_patches, L.d_fine);
-    else k_source<double, 3><<<L.nfine, b, 0, h->stream>>>(h->d_patches, L.d_fine);
-    ++h->stats.launches;
-  }
+  // GetSourceFunction + UpdateSourceFunction on the state patches of levels
+  // >= root (afas:57-64).  FillDown(source) and FillDown(solution) (afas:47,
+  // 66, 73, 90) only write regions that RestrictSolution /
+  // CoarseLoadingFunction overwrite before any read when the levels are
+  // nested uniform grids, so they are not issued.
+  if (nd == 2) k_source<double, 2><<<h->nmaster, b, 0, h->stream>>>(h->d_patches, h->d_master);
+  else k_source<double, 3><<<h->nmaster, b, 0, h->stream>>>(h->d_patches, h->d_master);
+  ++h->stats.launches;
+  // Mixed form: the FP32 working copy and its right-hand side for the first
+  // V-cycle (the norm computed here is not a convergence test).
+  if (h->mixed) launch_resid(h);
   h->trace.clear();
   int it = 0, conv = 0;
   double res = 0.0;
@@ -740,8 +887,7 @@ int bsam_gpu_multigrid_iterations(bsam_gpu* h, int* nvcycles, double* residual, 
     return BSAM_OK;
   }
   for (it = 1; it <= h->rp.maxvcycles; ++it) {
-    vcycle(h, h->finestlevel);
-    launch_resid(h);
+    iteration(h);
     CU(cudaGetLastError());
     CU(cudaMemcpyAsync(h->h_status, h->d_status, sizeof(DevStatus), cudaMemcpyDeviceToHost,
                        h->stream));
@@ -782,16 +928,16 @@ int bsam_gpu_residual_trace(bsam_gpu* h, double* out, int maxn) {
 
 int bsam_gpu_mass(bsam_gpu* h, double* mass) {
   if (!h || !h->have_hierarchy || !mass) return BSAM_ERR_STATE;
+  if (h->finestlevel != 0) return fail(h, BSAM_ERR_UNSUPPORTED, "mass needs a uniform hierarchy");
   CU(cudaSetDevice(h->device));
-  const LevelPlan& R = plan(h, 0);
-  const double hh = h->hp[R.patches[0]].h;
+  const double hh = h->hp[h->masters[0]].h;
   const double hd = h->rp.ndims == 2 ? hh * hh : hh * hh * hh;
   if (h->rp.ndims == 2)
-    k_mass<double, 2><<<R.nfine, block_dim(), 0, h->stream>>>(h->d_patches, R.d_fine,
-                                                             h->d_partials, h->d_status, R.nfine, hd);
+    k_mass<double, 2><<<h->nmaster, block_dim(), 0, h->stream>>>(
+        h->d_patches, h->d_master, h->d_partials, h->d_status, h->nmaster, hd);
   else
-    k_mass<double, 3><<<R.nfine, block_dim(), 0, h->stream>>>(h->d_patches, R.d_fine,
-                                                             h->d_partials, h->d_status, R.nfine, hd);
+    k_mass<double, 3><<<h->nmaster, block_dim(), 0, h->stream>>>(
+        h->d_patches, h->d_master, h->d_partials, h->d_status, h->nmaster, hd);
   ++h->stats.launches;
   CU(cudaGetLastError());
   CU(cudaMemcpyAsync(h->h_status, h->d_status, sizeof(DevStatus), cudaMemcpyDeviceToHost,
@@ -827,11 +973,9 @@ int bsam_gpu_profile(bsam_gpu* h, int enable) {
     h->ev_used = 0;
     if (h->have_hierarchy) {
       h->ev_cells = 0;
-      for (int p : plan(h, h->finestlevel).patches) {
-        int64_t c = 1;
-        for (int n = 0; n < h->rp.ndims; ++n) c *= h->hp[p].n[n];
-        h->ev_cells += c;
-      }
+      const LevelPlan& F = plan(h, h->finestlevel);
+      for (int p : F.patches) h->ev_cells += cells_of(h->hp[p].n, h->rp.ndims);
+      h->ev_bytes = elem_bytes(F.prec);
     }
   }
   h->profiling = enable != 0;

@@ -20,7 +20,10 @@ constexpr int BLOCK_THREADS = 32 * TILE_Y;
 //   BC_NONE    ghost not written by SetBC (internal 999 / periodic 2 faces)
 //   BC_COPY    q(ghost) = q(mirror)            (mthbc 1; UserBC2D faces 3,4)
 //   BC_REFLECT q(ghost) = 2 - q(mirror)        (UserBC2D faces 1,2; UserBC3D)
-enum : int32_t { BC_NONE = 0, BC_COPY = 1, BC_REFLECT = 2 };
+//   BC_NEGATE  e(ghost) = -e(mirror): BC_REFLECT seen by a correction e of a
+//              state q (q = base + e and both obey 2 - q), used by the
+//              correction-form levels of the mixed precision cycle
+enum : int32_t { BC_NONE = 0, BC_COPY = 1, BC_REFLECT = 2, BC_NEGATE = 3 };
 
 enum : int32_t { PREC_F64 = 0, PREC_F32 = 1 };
 
@@ -37,6 +40,8 @@ struct DevPatch {
   int32_t problem;    // problem (batch slot) this patch belongs to
   int32_t fused;      // 1: smoothing stages run the fused kernel (q -> qb -> q)
   int32_t zchunk;     // fused kernel: planes (3D) / rows (2D) per streaming chunk
+  int32_t twin;       // mixed form: the working patch of this FP64 master, else -1
+  int32_t delta;      // 1: q holds a correction e of the base state bs (mixed.cuh)
   int32_t pad_;
   int64_t sy, sz;     // element strides of j and k
   // Base pointers of element (0,0,0), the low ghost corner, per component.
@@ -45,6 +50,7 @@ struct DevPatch {
   void* f[2];         // right-hand side (source / FAS load), interior used
   void* qs[2];        // snapshot of q after restriction (the children's qc)
   void* qo[2];        // qold
+  void* bs;           // correction-form levels: phi of the base state
   // Problem constants, all computed on the host in FP64 exactly as the
   // reference does (problem.f90:183-187, 246-248, 472-476).
   double h, dt, eps2, alpha;

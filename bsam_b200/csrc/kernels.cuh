@@ -34,7 +34,7 @@ __device__ __forceinline__ int64_t cidx(const DevPatch& P, int i, int j, int k) 
 }
 
 template <class T> __device__ __forceinline__ T bc_map(int code, T v) {
-  return code == BC_REFLECT ? T(2) - v : v;
+  return code == BC_REFLECT ? T(2) - v : (code == BC_NEGATE ? -v : v);
 }
 
 // Choice s of one dimension for a ghost combination: 0 = the cell's own
@@ -133,11 +133,26 @@ __device__ __forceinline__ void relax_cell(const DevPatch& P, int i, int j, int 
   problem::Stencil<T, D> s;
   load_stencil<T, D>(P, q0, q1, c, s);
   T phi, mu;
-  problem::RelaxCell<T, D>(s, f0[c], f1[c], T(P.tmp1), T(P.tmp2), T(P.tmp3), T(P.alpha), phi,
-                           mu);
+  if (P.delta)
+    problem::RelaxCell<T, D, true>(s, f0[c], f1[c], T(P.tmp1), T(P.tmp2), T(P.tmp3), T(P.alpha),
+                                   phi, mu, fld<T>(P.bs)[c]);
+  else
+    problem::RelaxCell<T, D>(s, f0[c], f1[c], T(P.tmp1), T(P.tmp2), T(P.tmp3), T(P.alpha), phi,
+                             mu);
   q0[c] = phi;
   q1[c] = mu;
   if (P.wt && near_boundary(P, i, j, k, D)) write_through<T, D>(P, q0, q1, i, j, k, phi, mu);
+}
+
+// Operator at one cell from its stencil, in the patch's form.
+template <class T, int D>
+__device__ __forceinline__ void operator_at(const DevPatch& P, const problem::Stencil<T, D>& s,
+                                            int64_t c, T& o0, T& o1) {
+  if (P.delta)
+    problem::OperatorCell<T, D, true>(s, T(P.tmp1), T(P.tmp2), T(P.alpha), o0, o1,
+                                      fld<T>(P.bs)[c]);
+  else
+    problem::OperatorCell<T, D>(s, T(P.tmp1), T(P.tmp2), T(P.alpha), o0, o1);
 }
 
 // Residual rf = f - Operator(q) at one cell (afas:799-840).
@@ -148,7 +163,7 @@ __device__ __forceinline__ void residual_cell(const DevPatch& P, const T* q0, co
   problem::Stencil<T, D> s;
   load_stencil<T, D>(P, q0, q1, c, s);
   T o0, o1;
-  problem::OperatorCell<T, D>(s, T(P.tmp1), T(P.tmp2), T(P.alpha), o0, o1);
+  operator_at<T, D>(P, s, c, o0, o1);
   r0 = f0[c] - o0;
   r1 = f1[c] - o1;
 }
@@ -157,58 +172,74 @@ __device__ __forceinline__ void residual_cell(const DevPatch& P, const T* q0, co
 // into parent P, + the parent's SetGhost(level-1, 0) for physical faces +
 // GetCoarseGhostPoints (boundary.f90:1203-1269): the parent solution and its
 // snapshot qs (the children's qc) are both written.
-template <class T, int D>
+// TC / TP: value types of the child and the parent (equal in the FP64 path;
+// in the mixed path the child may be FP32 over an FP64 parent).  Restriction
+// runs in the child's precision; the stored value converts exactly upward.
+template <class TC, class TP, int D>
 __device__ __forceinline__ void restrict_cell(const DevPatch& C, const DevPatch& P, int ic, int jc,
                                               int kc) {
   const int i = 2 * ic, j = 2 * jc, k = 2 * kc;
-  T val[2];
+  TP val[2];
 #pragma unroll
   for (int v = 0; v < 2; ++v) {
-    const T* a = fld<T>(mid_state(C)[v]);
+    const TC* a = fld<TC>(mid_state(C)[v]);
     if (D == 2) {
-      val[v] = T(0.25) * (a[cidx(C, i, j, 0)] + a[cidx(C, i - 1, j, 0)] +
-                          a[cidx(C, i, j - 1, 0)] + a[cidx(C, i - 1, j - 1, 0)]);
+      val[v] = TP(TC(0.25) * (a[cidx(C, i, j, 0)] + a[cidx(C, i - 1, j, 0)] +
+                              a[cidx(C, i, j - 1, 0)] + a[cidx(C, i - 1, j - 1, 0)]));
     } else {
-      val[v] = T(0.125) * (a[cidx(C, i, j, k)] + a[cidx(C, i - 1, j, k)] +
-                           a[cidx(C, i, j - 1, k)] + a[cidx(C, i - 1, j - 1, k)] +
-                           a[cidx(C, i, j, k - 1)] + a[cidx(C, i - 1, j, k - 1)] +
-                           a[cidx(C, i, j - 1, k - 1)] + a[cidx(C, i - 1, j - 1, k - 1)]);
+      val[v] = TP(TC(0.125) * (a[cidx(C, i, j, k)] + a[cidx(C, i - 1, j, k)] +
+                               a[cidx(C, i, j - 1, k)] + a[cidx(C, i - 1, j - 1, k)] +
+                               a[cidx(C, i, j, k - 1)] + a[cidx(C, i - 1, j, k - 1)] +
+                               a[cidx(C, i, j - 1, k - 1)] + a[cidx(C, i - 1, j - 1, k - 1)]));
     }
   }
   const int pi = C.off[0] + ic, pj = C.off[1] + jc, pk = (D == 3) ? C.off[2] + kc : 0;
   const int64_t pc = cidx(P, pi, pj, pk);
-  T* pq0 = fld<T>(P.q[0]);
-  T* pq1 = fld<T>(P.q[1]);
-  T* ps0 = fld<T>(P.qs[0]);
-  T* ps1 = fld<T>(P.qs[1]);
+  TP* pq0 = fld<TP>(P.q[0]);
+  TP* pq1 = fld<TP>(P.q[1]);
+  TP* ps0 = fld<TP>(P.qs[0]);
+  TP* ps1 = fld<TP>(P.qs[1]);
   pq0[pc] = val[0];
   pq1[pc] = val[1];
   ps0[pc] = val[0];
   ps1[pc] = val[1];
   if (P.wt && near_boundary(P, pi, pj, pk, D)) {
-    write_through<T, D>(P, pq0, pq1, pi, pj, pk, val[0], val[1]);
-    write_through<T, D>(P, ps0, ps1, pi, pj, pk, val[0], val[1]);
+    write_through<TP, D>(P, pq0, pq1, pi, pj, pk, val[0], val[1]);
+    write_through<TP, D>(P, ps0, ps1, pi, pj, pk, val[0], val[1]);
+  }
+  if (P.delta) {
+    // Correction form: the coarse base is the restriction of the fine base.
+    const TC* b = fld<TC>(C.bs);
+    if (D == 2)
+      fld<TP>(P.bs)[pc] = TP(TC(0.25) * (b[cidx(C, i, j, 0)] + b[cidx(C, i - 1, j, 0)] +
+                                         b[cidx(C, i, j - 1, 0)] + b[cidx(C, i - 1, j - 1, 0)]));
+    else
+      fld<TP>(P.bs)[pc] =
+          TP(TC(0.125) * (b[cidx(C, i, j, k)] + b[cidx(C, i - 1, j, k)] + b[cidx(C, i, j - 1, k)] +
+                          b[cidx(C, i - 1, j - 1, k)] + b[cidx(C, i, j, k - 1)] +
+                          b[cidx(C, i - 1, j, k - 1)] + b[cidx(C, i, j - 1, k - 1)] +
+                          b[cidx(C, i - 1, j - 1, k - 1)]));
   }
 }
 
 // CoarseLoadingFunction (afas:646-714) at one coarse cell:
 //   parent%f(mb) = Restriction(f - Operator(q)) + Operator(qc, h = parent%dx)
-template <class T, int D>
+template <class TC, class TP, int D>
 __device__ __forceinline__ void coarse_load_cell(const DevPatch& C, const DevPatch& P, int ic,
                                                  int jc, int kc) {
-  const T* q0 = fld<T>(mid_state(C)[0]);
-  const T* q1 = fld<T>(mid_state(C)[1]);
-  const T* f0 = fld<T>(C.f[0]);
-  const T* f1 = fld<T>(C.f[1]);
+  const TC* q0 = fld<TC>(mid_state(C)[0]);
+  const TC* q1 = fld<TC>(mid_state(C)[1]);
+  const TC* f0 = fld<TC>(C.f[0]);
+  const TC* f1 = fld<TC>(C.f[1]);
   const int i = 2 * ic, j = 2 * jc, k = 2 * kc;
   // Restriction of rf: children in the reference's summation order.
   const int nch = (D == 2) ? 4 : 8;
-  T s0 = T(0), s1 = T(0);
+  TC s0 = TC(0), s1 = TC(0);
 #pragma unroll
   for (int ch = 0; ch < nch; ++ch) {
     const int ii = i - (ch & 1), jj = j - ((ch >> 1) & 1), kk = (D == 3) ? k - (ch >> 2) : 0;
-    T r0, r1;
-    residual_cell<T, D>(C, q0, q1, f0, f1, cidx(C, ii, jj, kk), r0, r1);
+    TC r0, r1;
+    residual_cell<TC, D>(C, q0, q1, f0, f1, cidx(C, ii, jj, kk), r0, r1);
     if (ch == 0) {
       s0 = r0;
       s1 = r1;
@@ -217,16 +248,16 @@ __device__ __forceinline__ void coarse_load_cell(const DevPatch& C, const DevPat
       s1 = s1 + r1;
     }
   }
-  const T w = (D == 2) ? T(0.25) : T(0.125);
-  const T R0 = w * s0, R1 = w * s1;
+  const TC w = (D == 2) ? TC(0.25) : TC(0.125);
+  const TP R0 = TP(w * s0), R1 = TP(w * s1);
   const int pi = C.off[0] + ic, pj = C.off[1] + jc, pk = (D == 3) ? C.off[2] + kc : 0;
   const int64_t pc = cidx(P, pi, pj, pk);
-  problem::Stencil<T, D> s;
-  load_stencil<T, D>(P, fld<T>(P.qs[0]), fld<T>(P.qs[1]), pc, s);
-  T o0, o1;
-  problem::OperatorCell<T, D>(s, T(P.tmp1), T(P.tmp2), T(P.alpha), o0, o1);
-  fld<T>(P.f[0])[pc] = R0 + o0;
-  fld<T>(P.f[1])[pc] = R1 + o1;
+  problem::Stencil<TP, D> s;
+  load_stencil<TP, D>(P, fld<TP>(P.qs[0]), fld<TP>(P.qs[1]), pc, s);
+  TP o0, o1;
+  operator_at<TP, D>(P, s, pc, o0, o1);
+  fld<TP>(P.f[0])[pc] = R0 + o0;
+  fld<TP>(P.f[1])[pc] = R1 + o1;
 }
 
 template <class T>
@@ -238,46 +269,48 @@ __device__ __forceinline__ T lin_x(bool even, T a, T b) {
 // gridutilities.f90:137-175, 474-529) at the fine cell (I,J,K):
 // q += P(parent%q - qc); the ghost ring is refreshed by write-through (the
 // reference's SetGhost(level, 0) overwrites the prolongated ring, afas:515).
-template <class T, int D>
+// The correction e = parent%q - qc is formed and prolongated in the parent's
+// precision and added in the child's.
+template <class TC, class TP, int D>
 __device__ __forceinline__ void correct_cell(const DevPatch& C, const DevPatch& P, int I, int J,
                                              int K) {
-  const T* pq0 = fld<T>(P.q[0]);
-  const T* pq1 = fld<T>(P.q[1]);
-  const T* ps0 = fld<T>(P.qs[0]);
-  const T* ps1 = fld<T>(P.qs[1]);
-  T* q0 = fld<T>(mid_state(C)[0]);
-  T* q1 = fld<T>(mid_state(C)[1]);
+  const TP* pq0 = fld<TP>(P.q[0]);
+  const TP* pq1 = fld<TP>(P.q[1]);
+  const TP* ps0 = fld<TP>(P.qs[0]);
+  const TP* ps1 = fld<TP>(P.qs[1]);
+  TC* q0 = fld<TC>(mid_state(C)[0]);
+  TC* q1 = fld<TC>(mid_state(C)[1]);
   const int m = I >> 1, n = J >> 1, p = K >> 1;
   const bool ex = (I & 1) == 0, ey = (J & 1) == 0, ez = (K & 1) == 0;
-  T corr[2];
+  TP corr[2];
 #pragma unroll
   for (int v = 0; v < 2; ++v) {
-    const T* pq = v ? pq1 : pq0;
-    const T* ps = v ? ps1 : ps0;
-    auto e = [&](int a, int b, int c) -> T {
+    const TP* pq = v ? pq1 : pq0;
+    const TP* ps = v ? ps1 : ps0;
+    auto e = [&](int a, int b, int c) -> TP {
       const int64_t x = cidx(P, C.off[0] + a, C.off[1] + b, D == 3 ? C.off[2] + c : 0);
       return pq[x] - ps[x];
     };
     if (D == 2) {
-      const T b0 = lin_x<T>(ex, e(m, n, 0), e(m + 1, n, 0));
-      const T b1 = lin_x<T>(ex, e(m, n + 1, 0), e(m + 1, n + 1, 0));
-      corr[v] = lin_x<T>(ey, b0, b1) / T(16);
+      const TP b0 = lin_x<TP>(ex, e(m, n, 0), e(m + 1, n, 0));
+      const TP b1 = lin_x<TP>(ex, e(m, n + 1, 0), e(m + 1, n + 1, 0));
+      corr[v] = lin_x<TP>(ey, b0, b1) / TP(16);
     } else {
-      const T b00 = lin_x<T>(ex, e(m, n, p), e(m + 1, n, p));
-      const T b10 = lin_x<T>(ex, e(m, n + 1, p), e(m + 1, n + 1, p));
-      const T b01 = lin_x<T>(ex, e(m, n, p + 1), e(m + 1, n, p + 1));
-      const T b11 = lin_x<T>(ex, e(m, n + 1, p + 1), e(m + 1, n + 1, p + 1));
-      const T c0 = lin_x<T>(ey, b00, b10);
-      const T c1 = lin_x<T>(ey, b01, b11);
-      corr[v] = lin_x<T>(ez, c0, c1) / T(64);
+      const TP b00 = lin_x<TP>(ex, e(m, n, p), e(m + 1, n, p));
+      const TP b10 = lin_x<TP>(ex, e(m, n + 1, p), e(m + 1, n + 1, p));
+      const TP b01 = lin_x<TP>(ex, e(m, n, p + 1), e(m + 1, n, p + 1));
+      const TP b11 = lin_x<TP>(ex, e(m, n + 1, p + 1), e(m + 1, n + 1, p + 1));
+      const TP c0 = lin_x<TP>(ey, b00, b10);
+      const TP c1 = lin_x<TP>(ey, b01, b11);
+      corr[v] = lin_x<TP>(ez, c0, c1) / TP(64);
     }
   }
   const int64_t c = cidx(C, I, J, K);
-  const T a0 = q0[c] + corr[0];
-  const T a1 = q1[c] + corr[1];
+  const TC a0 = q0[c] + TC(corr[0]);
+  const TC a1 = q1[c] + TC(corr[1]);
   q0[c] = a0;
   q1[c] = a1;
-  if (C.wt && near_boundary(C, I, J, K, D)) write_through<T, D>(C, q0, q1, I, J, K, a0, a1);
+  if (C.wt && near_boundary(C, I, J, K, D)) write_through<TC, D>(C, q0, q1, I, J, K, a0, a1);
 }
 
 // ---- reductions --------------------------------------------------------------
@@ -386,7 +419,7 @@ __global__ void __launch_bounds__(BLOCK_THREADS)
   }
 }
 
-template <class T, int D>
+template <class TC, class TP, int D>
 __global__ void __launch_bounds__(BLOCK_THREADS)
     k_restrict(const DevPatch* __restrict__ PT, const Item* __restrict__ items) {
   const Item it = items[blockIdx.x];
@@ -400,11 +433,11 @@ __global__ void __launch_bounds__(BLOCK_THREADS)
   for (int t = 0; t < 2; ++t) {
     const int ic = ic0 + t;
     if (ic > C.cn[0]) break;
-    restrict_cell<T, D>(C, P, ic, jc, kc);
+    restrict_cell<TC, TP, D>(C, P, ic, jc, kc);
   }
 }
 
-template <class T, int D>
+template <class TC, class TP, int D>
 __global__ void __launch_bounds__(BLOCK_THREADS)
     k_coarse_load(const DevPatch* __restrict__ PT, const Item* __restrict__ items) {
   const Item it = items[blockIdx.x];
@@ -418,11 +451,11 @@ __global__ void __launch_bounds__(BLOCK_THREADS)
   for (int t = 0; t < 2; ++t) {
     const int ic = ic0 + t;
     if (ic > C.cn[0]) break;
-    coarse_load_cell<T, D>(C, P, ic, jc, kc);
+    coarse_load_cell<TC, TP, D>(C, P, ic, jc, kc);
   }
 }
 
-template <class T, int D>
+template <class TC, class TP, int D>
 __global__ void __launch_bounds__(BLOCK_THREADS)
     k_correct(const DevPatch* __restrict__ PT, const Item* __restrict__ items) {
   const Item it = items[blockIdx.x];
@@ -436,7 +469,7 @@ __global__ void __launch_bounds__(BLOCK_THREADS)
   for (int t = 0; t < 2; ++t) {
     const int I = I0 + t;
     if (I > C.n[0]) break;
-    correct_cell<T, D>(C, P, I, J, K);
+    correct_cell<TC, TP, D>(C, P, I, J, K);
   }
 }
 

@@ -27,6 +27,14 @@ template <class T> __device__ __forceinline__ T D2fc(T c, T alpha) {
   return T(3) * cmh * cmh * alpha;
 }
 
+// Dfc(b + e) - Dfc(b) = alpha e (3 c^2 + 3 c e + e^2), c = b - 1/2: the
+// change of the convex part over a correction e, formed so that rounding
+// scales with e (the correction form of the mixed-precision inner cycle).
+template <class T> __device__ __forceinline__ T DfcDelta(T b, T e, T alpha) {
+  const T c = b - T(0.5);
+  return alpha * e * (T(3) * c * c + T(3) * c * e + e * e);
+}
+
 // Neighbourhood of one cell: centre values and the -/+ neighbours per
 // dimension, for both components (phi = q(:,:,1), mu = q(:,:,2)).
 template <class T, int D> struct Stencil {
@@ -38,9 +46,14 @@ template <class T, int D> struct Stencil {
 // One cell of RelaxGrid2D / RelaxGrid3D (problem.f90:192-213, 485-516): the
 // per-cell 2x2 Newton update of (phi, mu) solved by Cramer's rule.
 // tmp1 = dt/h^2, tmp2 = eps2/h^2, tmp3 = 2d*eps2/h^2.
-template <class T, int D>
+// DELTA = true: the stencil holds a correction e of the base state whose phi
+// at the cell is `base`; the same Newton step is taken on
+// L(base + e) - L(base) = f, with Dfc replaced by DfcDelta and D2fc taken at
+// base + e.  DELTA = false is the reference's update, operation for
+// operation.
+template <class T, int D, bool DELTA = false>
 __device__ __forceinline__ void RelaxCell(const Stencil<T, D>& s, T f0, T f1, T tmp1, T tmp2,
-                                          T tmp3, T alpha, T& phi, T& mu) {
+                                          T tmp3, T alpha, T& phi, T& mu, T base = T(0)) {
   T m[2 * D];
 #pragma unroll
   for (int d = 0; d < D; ++d) {
@@ -51,7 +64,8 @@ __device__ __forceinline__ void RelaxCell(const Stencil<T, D>& s, T f0, T f1, T 
 #pragma unroll
   for (int t = 1; t < 2 * D; ++t) msum = msum + m[t];
   const T a12 = tmp1 * msum;
-  const T a21 = -D2fc(s.pc, alpha) - tmp3;
+  const T cfull = DELTA ? base + s.pc : s.pc;
+  const T a21 = -D2fc(cfull, alpha) - tmp3;
   // b(1): f + tmp1*(m1*mu(i-1) + m2*mu(i+1) + m3*mu(j-1) + m4*mu(j+1) ...)
   T smu = m[0] * s.mm[0] + m[1] * s.mp[0];
 #pragma unroll
@@ -67,7 +81,8 @@ __device__ __forceinline__ void RelaxCell(const Stencil<T, D>& s, T f0, T f1, T 
     sph = sph + s.pp[d];
     sph = sph + s.pm[d];
   }
-  const T b2 = f1 + Dfc(s.pc, alpha) - D2fc(s.pc, alpha) * s.pc - tmp2 * sph;
+  const T nl = DELTA ? DfcDelta(base, s.pc, alpha) : Dfc(s.pc, alpha);
+  const T b2 = f1 + nl - D2fc(cfull, alpha) * s.pc - tmp2 * sph;
   const T det = T(1) - a12 * a21;
   phi = (b1 - a12 * b2) / det;
   mu = (b2 - a21 * b1) / det;
@@ -78,9 +93,10 @@ __device__ __forceinline__ void RelaxCell(const Stencil<T, D>& s, T f0, T f1, T 
 // 345-404):
 //   res1 = phi - tmp1 * UDiv(Mob * grad mu)
 //   res2 = mu - Dfc(phi) + tmp2 * ULap(phi)
-template <class T, int D>
+// DELTA = true: L(base + e) - L(base) for a correction e (see RelaxCell).
+template <class T, int D, bool DELTA = false>
 __device__ __forceinline__ void OperatorCell(const Stencil<T, D>& s, T tmp1, T tmp2, T alpha,
-                                             T& r0, T& r1) {
+                                             T& r0, T& r1, T base = T(0)) {
   T udiv = Mob(T(0.5) * (s.pp[0] + s.pc)) * (s.mp[0] - s.mc) -
            Mob(T(0.5) * (s.pc + s.pm[0])) * (s.mc - s.mm[0]);
 #pragma unroll
@@ -96,7 +112,8 @@ __device__ __forceinline__ void OperatorCell(const Stencil<T, D>& s, T tmp1, T t
     lap = lap + s.pm[d];
   }
   lap = lap - T(2 * D) * s.pc;
-  r1 = s.mc - Dfc(s.pc, alpha) + tmp2 * lap;
+  const T nl = DELTA ? DfcDelta(base, s.pc, alpha) : Dfc(s.pc, alpha);
+  r1 = s.mc - nl + tmp2 * lap;
 }
 
 // Source2D/3D followed by UpdateSourceFunction (problem.f90:278-279,

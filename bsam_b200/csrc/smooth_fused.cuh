@@ -153,7 +153,11 @@ __device__ __forceinline__ void fused3_cell(const DevPatch& P, T* sphi, T* smu,
     s.mp[2] = nb_or_face(zh, P.bc[5], s.mc, mu_, sop);
   }
   T phi, mu;
-  problem::RelaxCell<T, 3>(s, f0, f1, T(P.tmp1), T(P.tmp2), T(P.tmp3), T(P.alpha), phi, mu);
+  if (P.delta)
+    problem::RelaxCell<T, 3, true>(s, f0, f1, T(P.tmp1), T(P.tmp2), T(P.tmp3), T(P.alpha), phi,
+                                   mu, __ldg(static_cast<const T*>(P.bs) + gc));
+  else
+    problem::RelaxCell<T, 3>(s, f0, f1, T(P.tmp1), T(P.tmp2), T(P.tmp3), T(P.alpha), phi, mu);
   sphi[so + lc] = phi;
   smu[so + lc] = mu;
 }

@@ -15,6 +15,8 @@
 // working "twin" per finest-level patch: the caller's finest patch stays the
 // FP64 master state (put/get/mass/source/residual), the twin carries the
 // FP32 V-cycle; levels above 4096 cells are FP32, smaller ones FP64.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -72,6 +74,7 @@ struct bsam_gpu {
   Item* d_master = nullptr;          // tiles over the masters
   int nmaster = 0;
   Item* d_items = nullptr;
+  CUtensorMap* d_tmaps = nullptr;    // TMA maps of the fused levels' fields
   double* d_partials = nullptr;
   int max_items = 0;
   int* d_err = nullptr;  // kernel error flag (bounded waits that gave up)
@@ -379,6 +382,43 @@ int64_t cells_of(const int* mx, int nd) {
   return c;
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// dependency on libcuda).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+// 3D map of one field of patch P: the array from its allocation start
+// (`lead` elements before element (0,0,0)), dims (sy, n1+2, n2+2), box
+// (hx, hy, 1).  Returns false if the driver rejects it.
+bool encode_field_map(CUtensorMap* m, const DevPatch& P, const void* field, int hx, int hy) {
+  auto enc = tensor_map_encoder();
+  if (!enc) return false;
+  const int es = elem_bytes(P.prec);
+  const int64_t lead = 128 / es - 1;
+  void* base = (char*)field - lead * es;
+  const cuuint64_t dims[3] = {(cuuint64_t)P.sy, (cuuint64_t)(P.n[1] + 2),
+                              (cuuint64_t)(P.n[2] + 2)};
+  const cuuint64_t strides[2] = {(cuuint64_t)(P.sy * es), (cuuint64_t)(P.sz * es)};
+  const cuuint32_t box[3] = {(cuuint32_t)hx, (cuuint32_t)hy, 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const CUresult r =
+      enc(m, P.prec == PREC_F32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
+          3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
 }  // namespace
 
 extern "C" {
@@ -434,6 +474,8 @@ int bsam_gpu_create(bsam_gpu** out, int device, const bsam_run_params* p) {
 
 static void free_hierarchy(bsam_gpu* h) {
   if (h->d_items) cudaFree(h->d_items);
+  if (h->d_tmaps) cudaFree(h->d_tmaps);
+  h->d_tmaps = nullptr;
   if (h->d_tops) cudaFree(h->d_tops);
   if (h->step_exec) cudaGraphExecDestroy(h->step_exec);
   if (h->d_trace) cudaFree(h->d_trace);
@@ -584,12 +626,14 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
     // faces physical.
     const int fmin = std::max(8, h->tuning.fuse_min_n);
     P.fused = (h->tuning.fuse_smoother != 0 && nd == 3 && in_vcycle && d.parent >= 0 &&
-               d.level > h->bottom_level && P.n[0] >= fmin && P.n[1] >= fmin && P.n[2] >= fmin)
+               d.level > h->bottom_level && !(P.delta && P.prec == PREC_F64) &&
+               P.n[0] >= fmin && P.n[1] >= fmin && P.n[2] >= fmin)
                   ? 1
                   : 0;
     if (P.fused) {
-      const int tiles = ((P.n[0] + Fused3<double>::TX - 1) / Fused3<double>::TX) *
-                        ((P.n[1] + Fused3<double>::TY - 1) / Fused3<double>::TY);
+      const int ftx = P.prec == PREC_F32 ? Fused3<float>::TX : Fused3<double>::TX;
+      const int fty = P.prec == PREC_F32 ? Fused3<float>::TY : Fused3<double>::TY;
+      const int tiles = ((P.n[0] + ftx - 1) / ftx) * ((P.n[1] + fty - 1) / fty);
       int chunk = h->tuning.chunk;
       if (chunk <= 0) {
         // About one CTA per SM, chunks of at least 16 planes.
@@ -662,6 +706,29 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
   }
   // Parents of the twins are the masters' parents.
   for (int r = npatch; r < nrec; ++r) h->hp[r].parent = h->hp[rec_src[r]].parent;
+  // TMA tensor maps of the fused records (q0, q1, qb0, qb1, f0, f1, bs).
+  {
+    std::vector<int> fused_recs;
+    for (int r = 0; r < nrec; ++r)
+      if (h->hp[r].fused) fused_recs.push_back(r);
+    if (!fused_recs.empty()) {
+      std::vector<CUtensorMap> maps(7 * fused_recs.size());
+      for (size_t k = 0; k < fused_recs.size(); ++k) {
+        const DevPatch& P = h->hp[fused_recs[k]];
+        const int hx = P.prec == PREC_F32 ? Fused3<float>::HX : Fused3<double>::HX;
+        const int hy = P.prec == PREC_F32 ? Fused3<float>::HY : Fused3<double>::HY;
+        const void* fields[7] = {P.q[0], P.q[1], P.qb[0], P.qb[1],
+                                 P.f[0], P.f[1], P.bs ? P.bs : P.q[0]};
+        for (int m = 0; m < 7; ++m)
+          if (!encode_field_map(&maps[7 * k + m], P, fields[m], hx, hy))
+            return fail(h, BSAM_ERR_CUDA, "cuTensorMapEncodeTiled rejected a field map");
+      }
+      CU(cudaMalloc(&h->d_tmaps, sizeof(CUtensorMap) * maps.size()));
+      CU(cudaMemcpyAsync(h->d_tmaps, maps.data(), sizeof(CUtensorMap) * maps.size(),
+                         cudaMemcpyHostToDevice, h->stream));
+      for (size_t k = 0; k < fused_recs.size(); ++k) h->hp[fused_recs[k]].tmaps = h->d_tmaps + 7 * k;
+    }
+  }
 
   // Level precisions and work lists.
   std::vector<Item> all;
@@ -689,8 +756,10 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
     if (L.fused)
       for (int p : L.patches) {
         const DevPatch& P = h->hp[p];
-        const int tx = (P.n[0] + Fused3<double>::TX - 1) / Fused3<double>::TX;
-        const int ty = (P.n[1] + Fused3<double>::TY - 1) / Fused3<double>::TY;
+        const int ftx = P.prec == PREC_F32 ? Fused3<float>::TX : Fused3<double>::TX;
+        const int fty = P.prec == PREC_F32 ? Fused3<float>::TY : Fused3<double>::TY;
+        const int tx = (P.n[0] + ftx - 1) / ftx;
+        const int ty = (P.n[1] + fty - 1) / fty;
         const int tz = (P.n[2] + P.zchunk - 1) / P.zchunk;
         for (int z = 0; z < tz; ++z)
           for (int y = 0; y < ty; ++y)

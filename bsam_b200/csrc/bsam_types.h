@@ -51,6 +51,7 @@ struct DevPatch {
   void* qs[2];        // snapshot of q after restriction (the children's qc)
   void* qo[2];        // qold
   void* bs;           // correction-form levels: phi of the base state
+  const void* tmaps;  // fused levels: TMA tensor maps of q0, q1, qb0, qb1, f0, f1, bs
   // Problem constants, all computed on the host in FP64 exactly as the
   // reference does (problem.f90:183-187, 246-248, 472-476).
   double h, dt, eps2, alpha;

@@ -71,6 +71,18 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
       : "memory");
 }
 
+// Tiled 3D tensor copy global -> shared on the TMA engine (no multicast).
+// The x coordinate times the element size is a multiple of 16 bytes at every
+// call site (tile origins are multiples of 32 cells, see k_smooth3_fused).
+__device__ __forceinline__ void tma_load_3d(void* dst, const void* tmap, int x, int y, int z,
+                                            uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, "
+      "{%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
+      "l"(tmap), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+
 // Bounded wait on an mbarrier phase.  Returns false after `limit` polls; the
 // caller records the failure and leaves without touching the stage's data.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* b, uint32_t parity, uint32_t limit) {
@@ -80,6 +92,12 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* b, uint32_t parity, 
   }
   return false;
 }
+
+// Device-side view of a CUtensorMap (128 bytes, 64-byte aligned), built on
+// the host with cuTensorMapEncodeTiled.
+struct alignas(64) CUtensorMapOpaque {
+  unsigned long long v[16];
+};
 
 constexpr uint32_t kWaitPolls = 1u << 22;   // about 0.3 s of polling
 constexpr int kErrTmaTimeout = 1;
@@ -93,15 +111,19 @@ constexpr int kErrTmaTimeout = 1;
 // steps.  So the four passes of a step run concurrently between two barriers.
 template <class T>
 struct Fused3 {
-  static constexpr int TX = 32, TY = 16, H = 4;
+  // Staged fields: phi, mu, f1, f2 and, for FP32 correction-form levels, the
+  // base phi.  FP64 tiles are half as tall so that the ring fits in 227 KB.
+  static constexpr int NFIELD = sizeof(T) == 4 ? 5 : 4;
+  static constexpr int TX = 32, TY = sizeof(T) == 4 ? 16 : 8, H = 4;
   static constexpr int HX = TX + 2 * H, HY = TY + 2 * H;
-  static constexpr int LAG = 2;                 // planes between consecutive passes
-  static constexpr int PREFETCH = 2;            // planes loaded ahead of use
-  static constexpr int NS = 2 * 4 + 1 + PREFETCH;  // planes t-8 .. t+PREFETCH
+  static constexpr int LAG = 2;                             // planes between passes
+  static constexpr int PREFETCH = sizeof(T) == 4 ? 2 : 1;   // planes loaded ahead
+  static constexpr int NS = 2 * 4 + 1 + PREFETCH;           // planes t-8 .. t+PREFETCH
   static constexpr int THREADS = 512;
   static constexpr int PLANE = HX * HY;
-  static constexpr size_t SMEM = 2ull * NS * PLANE * sizeof(T) + NS * sizeof(uint64_t);
+  static constexpr size_t SMEM = (size_t)NFIELD * NS * PLANE * sizeof(T) + NS * sizeof(uint64_t);
   static_assert((HX * sizeof(T)) % 16 == 0, "bulk rows must be multiples of 16 bytes");
+  static_assert(SMEM <= 227 * 1024, "the stage ring must fit in one CTA's shared memory");
 };
 
 template <class T>
@@ -113,13 +135,12 @@ __device__ __forceinline__ T nb_or_face(bool at_face, int code, T self, const T*
 // (problem.f90:489-513), neighbours across physical faces by the SetBC rule.
 // so/som/sop: slot offsets of planes z, z-1, z+1; zl/zh: z on a z face.
 template <class T>
-__device__ __forceinline__ void fused3_cell(const DevPatch& P, T* sphi, T* smu,
-                                            const T* __restrict__ gf0,
-                                            const T* __restrict__ gf1, int lc, int64_t gc,
-                                            int so, int som, int sop, bool xl, bool xh,
-                                            bool yl, bool yh, bool zl, bool zh) {
+__device__ __forceinline__ void fused3_cell(const DevPatch& P, T* sphi, T* smu, const T* sf0,
+                                            const T* sf1, const T* sbs, int lc, int so, int som,
+                                            int sop, bool xl, bool xh, bool yl, bool yh, bool zl,
+                                            bool zh) {
   using C = Fused3<T>;
-  const T f0 = __ldg(gf0 + gc), f1 = __ldg(gf1 + gc);
+  const T f0 = sf0[so + lc], f1 = sf1[so + lc];
   const T* ph = sphi + lc;
   const T* mu_ = smu + lc;
   problem::Stencil<T, 3> s;
@@ -153,9 +174,9 @@ __device__ __forceinline__ void fused3_cell(const DevPatch& P, T* sphi, T* smu,
     s.mp[2] = nb_or_face(zh, P.bc[5], s.mc, mu_, sop);
   }
   T phi, mu;
-  if (P.delta)
+  if (C::NFIELD == 5 && P.delta)
     problem::RelaxCell<T, 3, true>(s, f0, f1, T(P.tmp1), T(P.tmp2), T(P.tmp3), T(P.alpha), phi,
-                                   mu, __ldg(static_cast<const T*>(P.bs) + gc));
+                                   mu, sbs[so + lc]);
   else
     problem::RelaxCell<T, 3>(s, f0, f1, T(P.tmp1), T(P.tmp2), T(P.tmp3), T(P.alpha), phi, mu);
   sphi[so + lc] = phi;
@@ -169,10 +190,13 @@ __global__ void __launch_bounds__(Fused3<T>::THREADS, 1)
     k_smooth3_fused(const DevPatch* __restrict__ PT, const Item* __restrict__ items, int dir,
                     int color0, int* __restrict__ err) {
   using C = Fused3<T>;
-  extern __shared__ __align__(128) unsigned char smem_raw[];
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
   T* sphi = reinterpret_cast<T*>(smem_raw);
   T* smu = sphi + C::NS * C::PLANE;
-  uint64_t* bar = reinterpret_cast<uint64_t*>(smu + C::NS * C::PLANE);
+  T* sf0 = smu + C::NS * C::PLANE;
+  T* sf1 = sf0 + C::NS * C::PLANE;
+  T* sbs = sf1 + C::NS * C::PLANE;  // only when NFIELD == 5
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sphi + C::NFIELD * C::NS * C::PLANE);
 
   const Item it = items[blockIdx.x];
   const DevPatch P = PT[it.patch];  // by value: fields stay in registers
@@ -180,41 +204,36 @@ __global__ void __launch_bounds__(Fused3<T>::THREADS, 1)
   const int x0 = it.tx * C::TX, y0 = it.ty * C::TY;
   const int zc0 = it.tz * P.zchunk + 1;
   const int zc1 = min(zc0 + P.zchunk, n2 + 1);
-  const T* in0 = fld<T>(dir ? P.qb[0] : P.q[0]);
-  const T* in1 = fld<T>(dir ? P.qb[1] : P.q[1]);
   T* out0 = fld<T>(dir ? P.q[0] : P.qb[0]);
   T* out1 = fld<T>(dir ? P.q[1] : P.qb[1]);
-  const T* gf0 = fld<T>(P.f[0]);
-  const T* gf1 = fld<T>(P.f[1]);
 
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x < C::NS) mbar_init(&bar[threadIdx.x], 1);
   fence_mbar_init();
   __syncthreads();
 
-  // Interior rows of the halo'd tile: only interior cells are ever read (a
-  // neighbour across a physical face comes from the SetBC rule instead).
-  const int jlo = max(1, y0 - 3), jhi = min(n1, y0 + C::TY + 4);
-  const int nrows = jhi - jlo + 1;
-  const uint32_t slot_bytes = (uint32_t)(nrows * 2 * C::HX * sizeof(T));
+  // Only interior cells of the staged boxes are ever read (a neighbour across
+  // a physical face comes from the SetBC rule instead).
+  const int nfield = (C::NFIELD == 5 && P.delta) ? 5 : 4;
+  const uint32_t box_bytes = (uint32_t)(nfield * C::PLANE * sizeof(T));
+  const int lead = 128 / (int)sizeof(T) - 1;
 
   // Issues the bulk copies of plane z (same decision in every thread; warp 0
   // issues).  Returns true when a copy was issued.
+  // One tiled TMA box (HX x HY x 1) per field per plane.  The maps address
+  // each field from its allocation start, whose first element sits `lead`
+  // elements before element (0,0,0); boxes reaching outside the array are
+  // zero-filled by the TMA unit (those cells are never read).
   auto issue = [&](int z) -> bool {
     if (z < 1 || z > n2) return false;
-    if (warp == 0) {
+    if (threadIdx.x == 0) {
       const int s = z % C::NS;
-      if (lane == 0) {
-        fence_proxy_async_smem();
-        mbar_arrive_expect_tx(&bar[s], slot_bytes);
-      }
-      __syncwarp();
-      for (int r = lane; r < 2 * nrows; r += 32) {
-        const int fidx = r >= nrows, j = jlo + (r - fidx * nrows);
-        const T* src = (fidx ? in1 : in0) + (int64_t)(x0 - 3) + (int64_t)j * P.sy +
-                       (int64_t)z * P.sz;
-        T* dst = (fidx ? smu : sphi) + s * C::PLANE + (j - (y0 - 3)) * C::HX;
-        bulk_g2s(dst, src, C::HX * sizeof(T), &bar[s]);
+      fence_proxy_async_smem();
+      mbar_arrive_expect_tx(&bar[s], box_bytes);
+      const CUtensorMapOpaque* maps = static_cast<const CUtensorMapOpaque*>(P.tmaps);
+      const int x = x0 - 3 + lead;
+      for (int fidx = 0; fidx < nfield; ++fidx) {
+        const int m = fidx < 2 ? fidx + 2 * dir : fidx + 2;  // q0 q1 | qb0 qb1 | f0 f1 bs
+        tma_load_3d(sphi + (fidx * C::NS + s) * C::PLANE, &maps[m], x, y0 - 3, z, &bar[s]);
       }
     }
     return true;
@@ -281,8 +300,7 @@ __global__ void __launch_bounds__(Fused3<T>::THREADS, 1)
         const int som = ((z + C::NS - 1) % C::NS) * C::PLANE;
         const int sop = ((z + 1) % C::NS) * C::PLANE;
         const int lc = (j - (y0 - 3)) * C::HX + (i - (x0 - 3));
-        const int64_t gc = (int64_t)z * P.sz + (int64_t)j * P.sy + i;
-        fused3_cell<T>(P, sphi, smu, gf0, gf1, lc, gc, so, som, sop, i == 1, i == n0, j == 1,
+        fused3_cell<T>(P, sphi, smu, sf0, sf1, sbs, lc, so, som, sop, i == 1, i == n0, j == 1,
                        j == n1, z == 1, z == n2);
       }
     }

@@ -63,6 +63,10 @@ ABI_SYMBOLS = (
     "bsam_gpu_last_error", "bsam_gpu_get_stream", "bsam_gpu_profile", "bsam_gpu_get_stats",
     "bsam_host_levels", "bsam_host_build_uniform", "bsam_host_take_time_steps",
     "bsam_gpu_resid_norm_noalloc", "bsam_gpu_set_tuning",
+    "bsam_batch_create", "bsam_batch_destroy", "bsam_batch_set_tuning", "bsam_batch_footprint",
+    "bsam_batch_submit", "bsam_batch_advance", "bsam_batch_sync", "bsam_batch_run",
+    "bsam_batch_poll", "bsam_batch_slot_phase", "bsam_batch_collect", "bsam_batch_get_stream",
+    "bsam_batch_get_stats", "bsam_batch_last_error",
 )
 
 
@@ -113,6 +117,8 @@ def lib():
                                           ctypes.c_int, ip]
     L.bsam_host_take_time_steps.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp, ctypes.c_int64,
                                             ip, dp, ip, dp]
+    from . import batch as _batch
+    _batch.bind(L)
     _lib = L
     return L
 

@@ -1,0 +1,255 @@
+"""Batched and continuously batched Cahn-Hilliard solves (include/bsam_batch.h).
+
+A Batch keeps many independent problems resident on one GPU and advances
+them together, one V-cycle of every running problem per device "tick"; each
+problem converges, steps and finishes on its own schedule.  Problems may be
+submitted while others run (continuous batching); a submission is admitted
+when a slot and the problem's device footprint fit in the batch's pool.
+
+There is no CPU path: every call goes to libbsam_gpu.so.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+PREC_FP64, PREC_MIXED = 0, 1
+SLOT_IDLE, SLOT_RUNNING, SLOT_DONE, SLOT_FAILED = 0, 1, 2, 3
+MAX_STEPS = 256
+ERR_NOMEM = -3
+
+
+class BatchParams(ctypes.Structure):
+    _fields_ = [("ndims", ctypes.c_int32), ("precision", ctypes.c_int32),
+                ("nsmoothingpasses", ctypes.c_int32), ("maxvcycles", ctypes.c_int32),
+                ("max_slots", ctypes.c_int32), ("pad_", ctypes.c_int32),
+                ("pool_bytes", ctypes.c_int64), ("qerrortol", ctypes.c_double)]
+
+
+def _host_grid_type():
+    from . import HostGrid
+    return HostGrid
+
+
+class BatchProblem(ctypes.Structure):
+    pass
+
+
+class StepResult(ctypes.Structure):
+    _fields_ = [("nvcycles", ctypes.c_int32), ("converged", ctypes.c_int32),
+                ("residual", ctypes.c_double)]
+
+
+class BatchTuning(ctypes.Structure):
+    _fields_ = [("grid_ctas", ctypes.c_int32), ("reserved", ctypes.c_int32 * 7)]
+
+
+class BatchStats(ctypes.Structure):
+    _fields_ = [("ticks", ctypes.c_int64), ("launches", ctypes.c_int64),
+                ("kernels_per_tick", ctypes.c_int64), ("captures", ctypes.c_int64),
+                ("pool_used", ctypes.c_int64), ("pool_bytes", ctypes.c_int64),
+                ("resident", ctypes.c_int32), ("running", ctypes.c_int32)]
+
+
+def bind(L):
+    """Declares the batch entry points' signatures on the loaded library."""
+    HostGrid = _host_grid_type()
+    if "_fields_" not in BatchProblem.__dict__:
+        BatchProblem._fields_ = [("grid", HostGrid), ("nsteps", ctypes.c_int32),
+                                 ("pad_", ctypes.c_int32), ("dt", ctypes.c_double),
+                                 ("eps", ctypes.c_double), ("alpha", ctypes.c_double)]
+    vp, ip = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)
+    dp = ctypes.POINTER(ctypes.c_double)
+    L.bsam_batch_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.POINTER(BatchParams)]
+    L.bsam_batch_destroy.argtypes = [vp]
+    L.bsam_batch_set_tuning.argtypes = [vp, ctypes.POINTER(BatchTuning)]
+    L.bsam_batch_footprint.argtypes = [vp, ctypes.POINTER(BatchProblem),
+                                       ctypes.POINTER(ctypes.c_int64)]
+    L.bsam_batch_submit.argtypes = [vp, ctypes.POINTER(BatchProblem), dp, ip]
+    L.bsam_batch_advance.argtypes = [vp, ctypes.c_int]
+    L.bsam_batch_sync.argtypes = [vp]
+    L.bsam_batch_run.argtypes = [vp]
+    L.bsam_batch_poll.argtypes = [vp, ip, ctypes.c_int]
+    L.bsam_batch_slot_phase.argtypes = [vp, ctypes.c_int, ip, ip]
+    L.bsam_batch_collect.argtypes = [vp, ctypes.c_int, dp, ctypes.POINTER(StepResult), dp]
+    L.bsam_batch_get_stream.argtypes = [vp, ctypes.POINTER(vp)]
+    L.bsam_batch_get_stats.argtypes = [vp, ctypes.POINTER(BatchStats)]
+    L.bsam_batch_last_error.argtypes = [vp]
+    L.bsam_batch_last_error.restype = ctypes.c_char_p
+
+
+def _lib():
+    from . import lib
+    return lib()
+
+
+def _check(rc, h, what):
+    if rc != 0:
+        from . import BsamError
+        L = _lib()
+        msg = L.bsam_gpu_strerror(rc).decode()
+        if h is not None and h.value:
+            detail = L.bsam_batch_last_error(h)
+            if detail:
+                msg += ": " + detail.decode()
+        raise BsamError(f"{what} failed ({rc}): {msg}")
+
+
+def problem_struct(prob) -> BatchProblem:
+    """The C descriptor of a workloads.Problem."""
+    from . import host_grid
+    _lib()  # binds BatchProblem's layout
+    return BatchProblem(grid=host_grid(prob), nsteps=prob.nsteps, pad_=0, dt=prob.dt,
+                        eps=prob.eps, alpha=prob.alpha)
+
+
+class Batch:
+    """Many problems of one dimensionality resident on one GPU.
+
+    submit() admits a problem (returns its slot, or None when the pool or the
+    slots are full); advance()/run() issue V-cycle ticks; poll() lists the
+    finished slots; collect() reads one back and frees its slot.
+    """
+
+    def __init__(self, ndims: int, precision: int = PREC_MIXED, max_slots: int = 64,
+                 pool_bytes: int = 0, qerrortol: float = 1e-8, maxvcycles: int = 20,
+                 nsmoothingpasses: int = 2, device: int = 0, grid_ctas: int = 0):
+        L = _lib()
+        bp = BatchParams(ndims=ndims, precision=precision, nsmoothingpasses=nsmoothingpasses,
+                         maxvcycles=maxvcycles, max_slots=max_slots, pad_=0,
+                         pool_bytes=pool_bytes, qerrortol=qerrortol)
+        h = ctypes.c_void_p()
+        _check(L.bsam_batch_create(ctypes.byref(h), device, ctypes.byref(bp)), None,
+               "bsam_batch_create")
+        self.h = h
+        self.ndims = ndims
+        self.max_slots = max_slots
+        self.probs = {}
+        if grid_ctas:
+            self.set_tuning(grid_ctas=grid_ctas)
+
+    def set_tuning(self, grid_ctas: int = 0):
+        t = BatchTuning(grid_ctas=grid_ctas)
+        _check(_lib().bsam_batch_set_tuning(self.h, ctypes.byref(t)), self.h, "set_tuning")
+
+    def footprint(self, prob) -> int:
+        n = ctypes.c_int64(0)
+        ps = problem_struct(prob)
+        _check(_lib().bsam_batch_footprint(self.h, ctypes.byref(ps), ctypes.byref(n)), self.h,
+               "footprint")
+        return n.value
+
+    def submit(self, prob, q0=None):
+        """Admits prob with initial state q0 (default prob.q0()); returns the
+        slot, or None when it does not fit now."""
+        q0 = prob.q0() if q0 is None else q0
+        q0 = np.asfortranarray(q0, dtype=np.float64)
+        ps = problem_struct(prob)
+        slot = ctypes.c_int(-1)
+        rc = _lib().bsam_batch_submit(self.h, ctypes.byref(ps),
+                                      q0.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                      ctypes.byref(slot))
+        if rc == ERR_NOMEM:
+            return None
+        _check(rc, self.h, "submit")
+        self.probs[slot.value] = prob
+        return slot.value
+
+    def advance(self, max_ticks: int = 1):
+        _check(_lib().bsam_batch_advance(self.h, max_ticks), self.h, "advance")
+
+    def sync(self):
+        _check(_lib().bsam_batch_sync(self.h), self.h, "sync")
+
+    def run(self):
+        _check(_lib().bsam_batch_run(self.h), self.h, "run")
+
+    def poll(self) -> list:
+        buf = (ctypes.c_int * self.max_slots)()
+        n = _lib().bsam_batch_poll(self.h, buf, self.max_slots)
+        if n < 0:
+            _check(n, self.h, "poll")
+        return [buf[i] for i in range(min(n, self.max_slots))]
+
+    def phase(self, slot: int):
+        ph, st = ctypes.c_int(0), ctypes.c_int(0)
+        _check(_lib().bsam_batch_slot_phase(self.h, slot, ctypes.byref(ph), ctypes.byref(st)),
+               self.h, "slot_phase")
+        return ph.value, st.value
+
+    def collect(self, slot: int, want_q: bool = True):
+        """Final root q (with ghosts), per-step results and FP64 mass of slot."""
+        prob = self.probs.pop(slot)
+        shape = tuple(m + 2 for m in prob.mx[:prob.ndims]) + (2,)
+        q = np.zeros(shape, order="F") if want_q else None
+        steps = (StepResult * prob.nsteps)()
+        mass = ctypes.c_double(0.0)
+        rc = _lib().bsam_batch_collect(
+            self.h, slot, q.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if want_q else None,
+            steps, ctypes.byref(mass))
+        _check(rc, self.h, "collect")
+        return {"q": q,
+                "nvcycles": np.array([s.nvcycles for s in steps], dtype=np.int32),
+                "converged": np.array([s.converged for s in steps], dtype=np.int32),
+                "residual": np.array([s.residual for s in steps]),
+                "mass": mass.value}
+
+    def stream(self) -> int:
+        p = ctypes.c_void_p()
+        _check(_lib().bsam_batch_get_stream(self.h, ctypes.byref(p)), self.h, "get_stream")
+        return p.value or 0
+
+    def stats(self) -> dict:
+        st = BatchStats()
+        _check(_lib().bsam_batch_get_stats(self.h, ctypes.byref(st)), self.h, "get_stats")
+        return {k: getattr(st, k) for k, _ in BatchStats._fields_}
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            _lib().bsam_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+def solve_all(problems, precision: int = PREC_MIXED, max_slots: int | None = None,
+              pool_bytes: int = 0, device: int = 0, grid_ctas: int = 0):
+    """Solves every problem (one dimensionality) in one batch; admits more as
+    slots free up.  Returns the collect() results in input order."""
+    if not problems:
+        return []
+    nd = problems[0].ndims
+    ms = max_slots or len(problems)
+    tol = problems[0].qerrortol
+    with Batch(nd, precision=precision, max_slots=ms, pool_bytes=pool_bytes, qerrortol=tol,
+               maxvcycles=problems[0].maxvcycles, device=device, grid_ctas=grid_ctas) as b:
+        out = [None] * len(problems)
+        pending = list(range(len(problems)))
+        slot_of = {}
+        while pending or slot_of:
+            while pending:
+                s = b.submit(problems[pending[0]])
+                if s is None:
+                    break
+                slot_of[s] = pending.pop(0)
+            if not slot_of:
+                raise RuntimeError("a problem does not fit in an empty batch")
+            if pending:
+                b.advance(4)  # then admit into the slots that freed up
+            else:
+                b.advance(1 << 20)
+            b.sync()
+            for s in b.poll():
+                out[slot_of.pop(s)] = b.collect(s)
+        return out

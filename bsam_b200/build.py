@@ -14,7 +14,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libbsam_gpu.so")
-SOURCES = ["bsam_gpu.cu", "bsam_host.cpp", "bsam_noalloc.cu"]
+SOURCES = ["bsam_gpu.cu", "bsam_host.cpp", "bsam_noalloc.cu", "bsam_batch.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -30,7 +30,8 @@ def _stale() -> bool:
         return True
     t = os.path.getmtime(LIB)
     deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)]
-    deps.append(os.path.join(HERE, "..", "include", "bsam_gpu.h"))
+    inc = os.path.join(HERE, "..", "include")
+    deps += [os.path.join(inc, f) for f in os.listdir(inc)]
     deps.append(os.path.abspath(__file__))
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 

@@ -1,0 +1,243 @@
+// batch.cuh -- kernels of the batched engine (bsam_batch.cu).
+//
+// Every V-cycle stage of a tick is one launch over a device-resident work
+// list that covers that stage for all resident problems; the list's length
+// is read on the device, so problems can be added between ticks without
+// re-capturing the tick graph.  CTAs walk the list in a grid-stride loop and
+// run the same tile bodies as the single-problem kernels (kernels.cuh,
+// mixed.cuh, bottom.cuh); tiles of finished problems are skipped.
+//
+// Per-problem control (k_batch_control) replaces the host loop of
+// MultigridIterations (afas:69-104) and of TakeTimeSteps
+// (lib/bsamroutines.f90:632-762) for each slot: it sums the slot's own
+// residual partials in the same order as last_block_total, so every
+// decision matches the single-problem engine bit for bit.
+#pragma once
+#include "bottom.cuh"
+#include "kernels.cuh"
+#include "mixed.cuh"
+
+namespace bsam {
+
+enum : int32_t { SLOT_IDLE = 0, SLOT_RUNNING = 1, SLOT_DONE = 2, SLOT_FAILED = 3 };
+
+// Host-owned per-slot configuration (rewritten whenever lists are rebuilt).
+struct SlotCfg {
+  int32_t ib, ie;     // the slot's tiles in the master list (its residual partials)
+  int32_t rec0, nrec; // its patch records
+  int32_t master;     // record holding the FP64 state
+  int32_t nsteps, maxv, pad_;
+  double denom;       // nrvars * cells (L2Error's integralresult(2))
+  double tol;
+};
+
+// Device-owned per-slot state (the host writes it only at admission).
+struct SlotState {
+  int32_t phase, step, iters, vcycles;
+};
+
+struct StepLog {
+  int32_t nv, conv;
+  double res;
+};
+
+// Mirror in mapped host memory: what the host polls.
+struct SlotOut {
+  int32_t phase, step, vcycles, pad_;
+};
+
+struct BatchCtl {
+  int32_t ticks_left;  // ticks this graph launch may still run
+  int32_t running;     // slots still running after this tick's control pass
+  int64_t ticks;       // ticks executed since creation
+};
+
+template <class T, int D>
+__global__ void __launch_bounds__(BLOCK_THREADS)
+    kb_relax(const DevPatch* __restrict__ PT, const Item* __restrict__ items,
+             const int* __restrict__ count, int color) {
+  const int n = *count;
+  for (int b = blockIdx.x; b < n; b += gridDim.x) relax_item<T, D>(PT, items[b], color);
+}
+
+// Transfers between a depth-d record (value type TC) and its parent, whose
+// type is the record's pprec.
+template <class TC, int D>
+__global__ void __launch_bounds__(BLOCK_THREADS)
+    kb_restrict(const DevPatch* __restrict__ PT, const Item* __restrict__ items,
+                const int* __restrict__ count) {
+  const int n = *count;
+  for (int b = blockIdx.x; b < n; b += gridDim.x) {
+    const Item it = items[b];
+    if (PT[it.patch].pprec == PREC_F32) restrict_item<TC, float, D>(PT, it);
+    else restrict_item<TC, double, D>(PT, it);
+  }
+}
+
+template <class TC, int D>
+__global__ void __launch_bounds__(BLOCK_THREADS)
+    kb_coarse_load(const DevPatch* __restrict__ PT, const Item* __restrict__ items,
+                   const int* __restrict__ count) {
+  const int n = *count;
+  for (int b = blockIdx.x; b < n; b += gridDim.x) {
+    const Item it = items[b];
+    if (PT[it.patch].pprec == PREC_F32) coarse_load_item<TC, float, D>(PT, it);
+    else coarse_load_item<TC, double, D>(PT, it);
+  }
+}
+
+template <class TC, int D>
+__global__ void __launch_bounds__(BLOCK_THREADS)
+    kb_correct(const DevPatch* __restrict__ PT, const Item* __restrict__ items,
+               const int* __restrict__ count) {
+  const int n = *count;
+  for (int b = blockIdx.x; b < n; b += gridDim.x) {
+    const Item it = items[b];
+    if (PT[it.patch].pprec == PREC_F32) correct_item<TC, float, D>(PT, it);
+    else correct_item<TC, double, D>(PT, it);
+  }
+}
+
+// Bottom chains (FP64 in both forms), one CTA per chain at a time.
+template <int D>
+__global__ void __launch_bounds__(BOTTOM_THREADS)
+    kb_bottom(const DevPatch* __restrict__ PT, const Item* __restrict__ tops,
+              const int* __restrict__ count, int nu) {
+  __shared__ int chain[BOTTOM_MAX_DEPTH];
+  __shared__ int depth;
+  const int n = *count;
+  for (int b = blockIdx.x; b < n; b += gridDim.x) {
+    const int top = tops[b].patch;
+    if (!PT[top].active) continue;  // uniform per CTA
+    bottom_chain<double, D>(PT, top, nu, chain, depth);
+  }
+}
+
+// Source of the masters whose new time step starts in this tick.
+template <int D>
+__global__ void __launch_bounds__(BLOCK_THREADS)
+    kb_source(const DevPatch* __restrict__ PT, const Item* __restrict__ items,
+              const int* __restrict__ count) {
+  const int n = *count;
+  for (int b = blockIdx.x; b < n; b += gridDim.x) source_item<double, D>(PT, items[b], 1);
+}
+
+// FP64 form: residual partial of every master tile.
+template <int D>
+__global__ void __launch_bounds__(BLOCK_THREADS)
+    kb_resid(const DevPatch* __restrict__ PT, const Item* __restrict__ items,
+             const int* __restrict__ count, double* __restrict__ partials) {
+  const int n = *count;
+  for (int b = blockIdx.x; b < n; b += gridDim.x) {
+    const Item it = items[b];
+    const DevPatch P = PT[it.patch];
+    if (!P.active) continue;  // uniform per CTA
+    const double s = block_sum(resid_item<double, D>(P, it));
+    if (threadIdx.x == 0 && threadIdx.y == 0) partials[b] = s;
+  }
+}
+
+// Mixed form: defect of every master tile (newstep_only = 0, with partials)
+// or of the masters starting a time step (newstep_only = 1: twin set-up only).
+template <int D>
+__global__ void __launch_bounds__(BLOCK_THREADS)
+    kb_defect(const DevPatch* __restrict__ PT, const Item* __restrict__ items,
+              const int* __restrict__ count, double* __restrict__ partials, int newstep_only) {
+  const int n = *count;
+  for (int b = blockIdx.x; b < n; b += gridDim.x) {
+    const Item it = items[b];
+    const DevPatch M = PT[it.patch];
+    if (!M.active || (newstep_only && !M.newstep)) continue;  // uniform per CTA
+    const bool w32 = PT[M.twin].prec == PREC_F32;
+    const double acc = w32 ? defect_item<float, D>(PT, it, newstep_only)
+                           : defect_item<double, D>(PT, it, newstep_only);
+    const double s = block_sum(acc);
+    if (!newstep_only && threadIdx.x == 0 && threadIdx.y == 0) partials[b] = s;
+  }
+}
+
+template <int D>
+__global__ void __launch_bounds__(BLOCK_THREADS)
+    kb_update(const DevPatch* __restrict__ PT, const Item* __restrict__ items,
+              const int* __restrict__ count) {
+  const int n = *count;
+  for (int b = blockIdx.x; b < n; b += gridDim.x) {
+    const Item it = items[b];
+    const DevPatch M = PT[it.patch];
+    if (!M.active) continue;
+    if (PT[M.twin].prec == PREC_F32) update_item<float, D>(PT, it);
+    else update_item<double, D>(PT, it);
+  }
+}
+
+// End of a tick, one CTA per slot: ErrorAFAS of the slot from its partials,
+// then MultigridIterations' exit test and TakeTimeSteps' step advance.
+// Block of BLOCK_THREADS threads: the partial sums are added in the order of
+// last_block_total over the slot's own tiles.
+__global__ void __launch_bounds__(BLOCK_THREADS)
+    k_batch_control(DevPatch* __restrict__ PT, const SlotCfg* __restrict__ cfg,
+                    SlotState* __restrict__ state, StepLog* __restrict__ log, int max_steps,
+                    SlotOut* __restrict__ out, const double* __restrict__ partials,
+                    BatchCtl* __restrict__ ctl, int nslots) {
+  const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+  const int nthreads = blockDim.x * blockDim.y;
+  for (int s = blockIdx.x; s < nslots; s += gridDim.x) {
+    if (state[s].phase != SLOT_RUNNING) continue;  // uniform per CTA
+    const SlotCfg C = cfg[s];
+    double acc = 0.0;
+    for (int b = tid; b < C.ie - C.ib; b += nthreads) acc += partials[C.ib + b];
+    const double total = block_sum(acc);
+    if (tid == 0) {
+      SlotState S = state[s];
+      const double r = sqrt(total / C.denom);
+      S.iters += 1;
+      S.vcycles += 1;
+      const bool conv = r < C.tol;
+      const bool finite = isfinite(r);
+      PT[C.master].newstep = 0;
+      if (conv || S.iters >= C.maxv || !finite) {
+        if (S.step < max_steps) {
+          StepLog L;
+          L.nv = S.iters;
+          L.conv = conv ? 1 : 0;
+          L.res = r;
+          log[(int64_t)s * max_steps + S.step] = L;
+        }
+        S.step += 1;
+        S.iters = 0;
+        if (!finite || S.step >= C.nsteps) {
+          S.phase = finite ? SLOT_DONE : SLOT_FAILED;
+          for (int r2 = C.rec0; r2 < C.rec0 + C.nrec; ++r2) PT[r2].active = 0;
+        } else {
+          PT[C.master].newstep = 1;  // CopyQToQold + source at the next tick
+        }
+      }
+      state[s] = S;
+      if (S.phase == SLOT_RUNNING) atomicAdd(&ctl->running, 1);
+      // Mapped host mirror: counters first, the phase last.
+      volatile SlotOut* vo = out + s;
+      vo->vcycles = S.vcycles;
+      vo->step = S.step;
+      __threadfence_system();
+      vo->phase = S.phase;
+    }
+  }
+}
+
+// WHILE condition of the tick graph: another tick while some slot runs and
+// the launch's tick budget lasts.
+__global__ void k_batch_cond(BatchCtl* __restrict__ ctl, cudaGraphConditionalHandle handle) {
+  ctl->ticks += 1;
+  const int left = ctl->ticks_left - 1;
+  ctl->ticks_left = left;
+  const bool again = ctl->running > 0 && left > 0;
+  ctl->running = 0;
+  cudaGraphSetConditional(handle, again ? 1u : 0u);
+}
+
+__global__ void k_batch_budget(BatchCtl* __restrict__ ctl, int ticks) {
+  ctl->ticks_left = ticks;
+  ctl->running = 0;
+}
+
+}  // namespace bsam

@@ -67,16 +67,15 @@ __device__ __forceinline__ void block_correct(const DevPatch& C, const DevPatch&
   __syncthreads();
 }
 
-// tops[b]: the top patch of chain b; the chain follows parent links down to
-// the coarsest level.  nu = nsmoothingpasses.
+// AFASVcycle from `top` down its parent links to the coarsest level and back,
+// by the whole CTA.  chain / depth: the caller's shared scratch.
 template <class T, int D>
-__global__ void __launch_bounds__(BOTTOM_THREADS)
-    k_bottom(const DevPatch* __restrict__ PT, const int* __restrict__ tops, int nu) {
-  __shared__ int chain[BOTTOM_MAX_DEPTH];
-  __shared__ int depth;
+__device__ __forceinline__ void bottom_chain(const DevPatch* __restrict__ PT, int top, int nu,
+                                             int* chain, int& depth) {
+  __syncthreads();  // chain[] of a previous call is no longer read
   if (threadIdx.x == 0) {
     int d = 0;
-    for (int p = tops[blockIdx.x]; p >= 0 && d < BOTTOM_MAX_DEPTH; p = PT[p].parent) chain[d++] = p;
+    for (int p = top; p >= 0 && d < BOTTOM_MAX_DEPTH; p = PT[p].parent) chain[d++] = p;
     depth = d;
   }
   __syncthreads();
@@ -97,6 +96,19 @@ __global__ void __launch_bounds__(BOTTOM_THREADS)
     block_correct<T, D>(P, Q);
     block_relax<T, D>(P, nu);
   }
+}
+
+// tops[b]: the top patch of chain b; the chain follows parent links down to
+// the coarsest level.  nu = nsmoothingpasses.  Chains whose top is inactive
+// (finished batch slots) are skipped.
+template <class T, int D>
+__global__ void __launch_bounds__(BOTTOM_THREADS)
+    k_bottom(const DevPatch* __restrict__ PT, const int* __restrict__ tops, int nu) {
+  __shared__ int chain[BOTTOM_MAX_DEPTH];
+  __shared__ int depth;
+  const int top = tops[blockIdx.x];
+  if (!PT[top].active) return;
+  bottom_chain<T, D>(PT, top, nu, chain, depth);
 }
 
 }  // namespace bsam

@@ -1,0 +1,946 @@
+// bsam_batch.cu -- C ABI of the batched / continuously batched engine
+// (include/bsam_batch.h).
+//
+// Device state of a batch:
+//  * one memory pool; each resident problem ("slot") holds one contiguous
+//    region of it with all its fields, laid out exactly as bsam_gpu.cu lays
+//    out a single problem (pitched SoA, 128-byte aligned interior rows);
+//  * one patch table with a fixed block of RMAX records per slot;
+//  * work lists (Items) per V-cycle stage and depth, shared by all slots and
+//    appended to on admission; their lengths live on the device;
+//  * per-slot configuration / state / step log, and a mapped host mirror of
+//    each slot's phase that the host polls without synchronising.
+// A tick (one V-cycle of every running problem + its control) is captured
+// once into a graph whose WHILE node repeats ticks on the device; the graph
+// is captured again only when a list outgrows its capacity or a problem with
+// more grid-kernel depths arrives.
+//
+// Records of one slot (local index): FP64 form 0 = root (level 0), l =
+// level -l; mixed form 0 = FP64 master, 1 = working twin of the root,
+// l + 1 = level -l.  Depth d of the V-cycle is level -d.  Depths whose
+// levels have more than BOTTOM_MAX_CELLS cells run grid kernels ("top"
+// depths); the rest run inside k_bottom's chain, as in the single-problem
+// engine, and are FP64 in both forms.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/bsam_batch.h"
+#include "batch.cuh"
+#include "bsam_types.h"
+
+using namespace bsam;
+
+namespace {
+
+constexpr int RMAX = 16;  // records per slot
+constexpr int MAXD = 8;   // top depths
+// Mixed form: levels at or below this size stay FP64 (as in bsam_gpu.cu).
+constexpr int64_t FP64_CELLS = 4096;
+enum { L_MASTER = 0, L_TOPS = 1, L_FINE = 2, L_COARSE = 2 + MAXD, NLIST = 2 + 2 * MAXD };
+
+struct List {
+  Item* d = nullptr;
+  int cap = 0;            // device capacity in items
+  std::vector<Item> h;
+  int uploaded = 0;       // h[0, uploaded) are on the device
+};
+
+struct SlotPlan {
+  bool used = false;
+  bool stale = false;     // retired, and its tiles are still in the lists
+  size_t off = 0, bytes = 0;
+  int nrec = 0, ntop = 0, master = 0, top = 0;
+  int64_t cells = 0;
+  bsam_batch_problem prob{};
+  std::vector<DevPatch> recs;  // absolute record indices
+};
+
+struct StageChunk {
+  size_t a, b;
+  cudaEvent_t ev;
+};
+
+int64_t roundup(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
+
+int64_t cells_of(const int* n, int nd) {
+  int64_t c = 1;
+  for (int d = 0; d < nd; ++d) c *= n[d];
+  return c;
+}
+
+void tiles_for(int patch, const int* n, int nd, std::vector<Item>& out) {
+  const int tx = (n[0] + TILE_X - 1) / TILE_X;
+  const int ty = (n[1] + TILE_Y - 1) / TILE_Y;
+  const int tz = nd == 3 ? n[2] : 1;
+  for (int z = 0; z < tz; ++z)
+    for (int y = 0; y < ty; ++y)
+      for (int x = 0; x < tx; ++x) out.push_back(Item{patch, x, y, z});
+}
+
+}  // namespace
+
+struct bsam_batch {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bsam_batch_params bp{};
+  bool mixed = false;
+  int nsm = 148;
+  bsam_batch_tuning tuning{};
+  // pool
+  char* d_pool = nullptr;
+  size_t pool_bytes = 0, pool_used = 0;
+  std::map<size_t, size_t> free_;  // offset -> size, coalesced
+  // records, slots
+  DevPatch* d_pt = nullptr;
+  std::vector<SlotPlan> slots;
+  SlotCfg* d_cfg = nullptr;
+  std::vector<SlotCfg> h_cfg;
+  bool cfg_dirty = false;
+  SlotState* d_state = nullptr;
+  StepLog* d_log = nullptr;
+  SlotOut* h_out = nullptr;  // mapped
+  SlotOut* d_out = nullptr;
+  BatchCtl* d_ctl = nullptr;
+  DevStatus* d_status = nullptr;
+  DevStatus* h_status = nullptr;
+  double* d_partials = nullptr;
+  int partials_cap = 0;
+  List lists[NLIST];
+  int* d_counts = nullptr;
+  std::vector<int> counts_dev;  // counts last uploaded
+  // graph
+  cudaGraphExec_t exec = nullptr;
+  int cap_depth = 0;
+  bool need_capture = true;
+  int64_t kernels_per_tick = 0;
+  bsam_batch_stats st{};
+  // pinned staging ring for host -> device copies
+  char* stage = nullptr;
+  size_t stage_bytes = 0, stage_head = 0;
+  std::deque<StageChunk> chunks;
+  std::vector<size_t> pending;  // chunk indices (into `chunks`) awaiting an event
+  std::vector<cudaEvent_t> free_events;
+  std::string err;
+};
+
+namespace {
+
+int fail(bsam_batch* b, int code, const std::string& msg) {
+  if (b) b->err = msg;
+  return code;
+}
+
+#define CU(call)                                                                  \
+  do {                                                                            \
+    cudaError_t e_ = (call);                                                      \
+    if (e_ != cudaSuccess)                                                        \
+      return fail(b, BSAM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+// ---- pool ----------------------------------------------------------------------
+
+bool pool_alloc(bsam_batch* b, size_t bytes, size_t* off) {
+  for (auto it = b->free_.begin(); it != b->free_.end(); ++it) {
+    if (it->second < bytes) continue;
+    *off = it->first;
+    const size_t rest = it->second - bytes, at = it->first + bytes;
+    b->free_.erase(it);
+    if (rest) b->free_[at] = rest;
+    b->pool_used += bytes;
+    return true;
+  }
+  return false;
+}
+
+void pool_free(bsam_batch* b, size_t off, size_t bytes) {
+  auto it = b->free_.emplace(off, bytes).first;
+  auto nx = std::next(it);
+  if (nx != b->free_.end() && it->first + it->second == nx->first) {
+    it->second += nx->second;
+    b->free_.erase(nx);
+  }
+  if (it != b->free_.begin()) {
+    auto pv = std::prev(it);
+    if (pv->first + pv->second == it->first) {
+      pv->second += it->second;
+      b->free_.erase(it);
+    }
+  }
+  b->pool_used -= bytes;
+}
+
+// ---- staging ring ------------------------------------------------------------
+
+cudaEvent_t take_event(bsam_batch* b) {
+  if (!b->free_events.empty()) {
+    cudaEvent_t e = b->free_events.back();
+    b->free_events.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+  return e;
+}
+
+// Marks every chunk staged since the last call as done once the copies
+// queued so far have executed.
+void stage_commit(bsam_batch* b) {
+  if (b->pending.empty()) return;
+  cudaEvent_t e = take_event(b);
+  cudaEventRecord(e, b->stream);
+  for (size_t i : b->pending) b->chunks[i].ev = e;
+  b->pending.clear();
+}
+
+// Pinned host memory for n bytes, valid until the copies queued from it have
+// executed (stage_commit).
+char* stage_alloc(bsam_batch* b, size_t n) {
+  n = (size_t)roundup((int64_t)std::max<size_t>(n, 1), 256);
+  if (n > b->stage_bytes) {
+    // Grow: wait for everything staged so far, then replace the ring.
+    cudaStreamSynchronize(b->stream);
+    for (auto& c : b->chunks)
+      if (c.ev && std::find(b->free_events.begin(), b->free_events.end(), c.ev) ==
+                      b->free_events.end())
+        b->free_events.push_back(c.ev);
+    b->chunks.clear();
+    b->pending.clear();
+    if (b->stage) cudaFreeHost(b->stage);
+    b->stage_bytes = std::max({n, 2 * b->stage_bytes, (size_t)64 << 20});
+    if (cudaMallocHost(&b->stage, b->stage_bytes) != cudaSuccess) {
+      b->stage = nullptr;
+      b->stage_bytes = 0;
+      return nullptr;
+    }
+    b->stage_head = 0;
+  }
+  if (b->stage_head + n > b->stage_bytes) b->stage_head = 0;
+  const size_t a = b->stage_head, e = a + n;
+  // Chunks are in allocation order; the ones this range overlaps are at the
+  // front (the previous lap of the ring).
+  while (!b->chunks.empty()) {
+    StageChunk& c = b->chunks.front();
+    if (c.b <= a || c.a >= e) break;
+    if (!c.ev) stage_commit(b);  // staged in this call sequence: fence it now
+    cudaEventSynchronize(c.ev);
+    // The event may be shared with later chunks: recycle it with the last.
+    const cudaEvent_t ev = c.ev;
+    b->chunks.pop_front();
+    for (size_t& i : b->pending) --i;
+    bool shared = false;
+    for (auto& o : b->chunks) shared |= o.ev == ev;
+    if (!shared) b->free_events.push_back(ev);
+  }
+  b->chunks.push_back(StageChunk{a, e, nullptr});
+  b->pending.push_back(b->chunks.size() - 1);
+  b->stage_head = e;
+  return b->stage + a;
+}
+
+// Queues a host -> device copy of n bytes through the staging ring.
+int stage_copy(bsam_batch* b, void* dst, const void* src, size_t n) {
+  char* s = stage_alloc(b, n);
+  if (!s) return fail(b, BSAM_ERR_NOMEM, "pinned staging allocation failed");
+  std::memcpy(s, src, n);
+  CU(cudaMemcpyAsync(dst, s, n, cudaMemcpyHostToDevice, b->stream));
+  return BSAM_OK;
+}
+
+// ---- problem plan ----------------------------------------------------------------
+
+int face_rule(int nd, int face, int code, int* rule) {
+  if (code == 1) *rule = BC_COPY;
+  else if (code >= 10 && code <= 99) *rule = (nd == 2 && face >= 2) ? BC_COPY : BC_REFLECT;
+  else return -1;  // internal faces and periodic faces have no batch form
+  return 0;
+}
+
+// Builds the slot's records (absolute indices from rec0; field pointers
+// relative to a pool region starting at `base`).  base == nullptr: size only.
+int plan_slot(bsam_batch* b, const bsam_batch_problem* pr, int rec0, char* base, SlotPlan& S) {
+  const int nd = b->bp.ndims;
+  if (pr->grid.ndims != nd) return fail(b, BSAM_ERR_ARG, "problem ndims differs from the batch");
+  if (pr->nsteps < 1 || pr->nsteps > BSAM_BATCH_MAX_STEPS)
+    return fail(b, BSAM_ERR_ARG, "nsteps out of range");
+  if (!(pr->dt > 0) || !(pr->eps > 0)) return fail(b, BSAM_ERR_ARG, "dt and eps must be positive");
+  bsam_patch_desc desc[RMAX];
+  int np = 0;
+  int rc = bsam_host_build_uniform(&pr->grid, desc, RMAX - 1, &np);
+  if (rc) return fail(b, rc, "grid rejected (see bsam_host_build_uniform)");
+  const bool mixed = b->mixed;
+  const int nrec = np + (mixed ? 1 : 0);
+  // Depth of the first bottom level.
+  int ntop = np;
+  for (int l = 0; l < np; ++l)
+    if (cells_of(desc[l].mx, nd) <= BOTTOM_MAX_CELLS) {
+      ntop = l;
+      break;
+    }
+  if (ntop >= np)
+    return fail(b, BSAM_ERR_UNSUPPORTED, "the coarsest level exceeds the bottom kernel's size");
+  if (ntop > MAXD) return fail(b, BSAM_ERR_UNSUPPORTED, "too many levels above the bottom");
+  if (np - ntop > BOTTOM_MAX_DEPTH) return fail(b, BSAM_ERR_UNSUPPORTED, "bottom chain too deep");
+  auto rec_of = [&](int l) { return mixed ? (l == 0 ? 1 : l + 1) : l; };  // V-cycle record
+  S.recs.assign(nrec, DevPatch{});
+  S.nrec = nrec;
+  S.ntop = ntop;
+  S.master = 0;
+  S.top = rec0 + rec_of(ntop);
+  S.cells = cells_of(desc[0].mx, nd);
+  const double eps2 = pr->eps * pr->eps;
+  size_t total = 0;
+  for (int r = 0; r < nrec; ++r) {
+    const bool is_master_only = mixed && r == 0;
+    const int l = mixed ? (r == 0 ? 0 : r - 1) : r;  // level index (desc)
+    const bsam_patch_desc& d = desc[l];
+    DevPatch& P = S.recs[r];
+    P.ndims = nd;
+    for (int n = 0; n < 3; ++n) P.n[n] = n < nd ? d.mx[n] : 1;
+    P.parent = d.parent >= 0 ? rec0 + rec_of(d.parent) : -1;
+    P.level = d.level;
+    P.problem = rec0 / RMAX;
+    P.active = 1;
+    P.newstep = (r == 0) ? 1 : 0;
+    P.twin = is_master_only ? rec0 + 1 : -1;
+    const int64_t ncell = cells_of(P.n, nd);
+    P.prec = (!mixed || is_master_only || ncell <= FP64_CELLS) ? PREC_F64 : PREC_F32;
+    for (int n = 0; n < 3; ++n) {
+      P.cn[n] = 1;
+      P.off[n] = 0;
+    }
+    if (d.parent >= 0)
+      for (int n = 0; n < nd; ++n) {
+        P.cn[n] = P.n[n] / 2;
+        P.off[n] = d.mbounds[n][0] - 1;
+      }
+    P.wt = 1;
+    for (int f = 0; f < 6; ++f) {
+      if (f >= 2 * nd) {
+        P.bc[f] = BC_NONE;
+        continue;
+      }
+      int rule;
+      if (face_rule(nd, f, d.mthbc[f], &rule))
+        return fail(b, BSAM_ERR_UNSUPPORTED, "batch problems need physical faces (codes 1, 10-99)");
+      P.bc[f] = rule;
+    }
+    P.delta = (mixed && !is_master_only) ? 1 : 0;
+    if (P.delta)
+      for (int f = 0; f < 2 * nd; ++f)
+        if (P.bc[f] == BC_REFLECT) P.bc[f] = BC_NEGATE;
+    P.fused = 0;
+    P.zchunk = 1;
+    const int es = P.prec == PREC_F32 ? 4 : 8;
+    const int64_t A = 128 / es, lead = A - 1;
+    P.sy = roundup(lead + P.n[0] + 2, A);
+    P.sz = nd == 3 ? P.sy * (P.n[1] + 2) : 0;
+    const int64_t vol = nd == 3 ? P.sz * (P.n[2] + 2) : P.sy * (P.n[1] + 2);
+    const int64_t fe = roundup(lead + vol + 64, 256 / es);
+    // Every V-cycle record below the root is the parent of the next finer
+    // one and keeps the snapshot qs of its restricted state.
+    const bool is_parent = !is_master_only && l >= 1;
+    const int nfield = 4 + (is_parent ? 2 : 0) + (P.delta ? 1 : 0);
+    if (base) {
+      char* rb = base + total;
+      int slotn = 0;
+      auto next = [&]() { return (void*)(rb + (fe * (slotn++) + lead) * es); };
+      P.q[0] = next();
+      P.q[1] = next();
+      P.f[0] = next();
+      P.f[1] = next();
+      P.qo[0] = P.qo[1] = nullptr;  // the source reads q at the start of a step
+      P.qs[0] = P.qs[1] = nullptr;
+      if (is_parent) {
+        P.qs[0] = next();
+        P.qs[1] = next();
+      }
+      P.qb[0] = P.qb[1] = nullptr;
+      P.bs = P.delta ? next() : nullptr;
+      P.tmaps = nullptr;
+    }
+    total += (size_t)fe * nfield * es;
+    P.h = d.dx;
+    const double h2 = d.dx * d.dx;
+    P.dt = pr->dt;
+    P.eps2 = eps2;
+    P.alpha = pr->alpha;
+    P.tmp1 = pr->dt / h2;
+    P.tmp2 = eps2 / h2;
+    P.tmp3 = (2.0 * nd) * eps2 / h2;
+  }
+  for (int r = 0; r < nrec; ++r) {
+    DevPatch& P = S.recs[r];
+    P.pprec = P.parent >= 0 ? S.recs[P.parent - rec0].prec : P.prec;
+  }
+  S.bytes = (size_t)roundup((int64_t)total, 4096);
+  S.prob = *pr;
+  return BSAM_OK;
+}
+
+// Appends a slot's tiles to the lists and records its master range.
+void append_items(bsam_batch* b, int s) {
+  SlotPlan& S = b->slots[s];
+  const int nd = b->bp.ndims;
+  const int rec0 = s * RMAX;
+  SlotCfg& C = b->h_cfg[s];
+  C.ib = (int)b->lists[L_MASTER].h.size();
+  tiles_for(rec0 + S.master, S.recs[S.master].n, nd, b->lists[L_MASTER].h);
+  C.ie = (int)b->lists[L_MASTER].h.size();
+  b->lists[L_TOPS].h.push_back(Item{S.top, 0, 0, 0});
+  const int first = b->mixed ? 1 : 0;  // record of depth 0
+  for (int d = 0; d < S.ntop; ++d) {
+    const int r = first + d;
+    tiles_for(rec0 + r, S.recs[r].n, nd, b->lists[L_FINE + d].h);
+    tiles_for(rec0 + r, S.recs[r].cn, nd, b->lists[L_COARSE + d].h);
+  }
+  b->cfg_dirty = true;
+}
+
+// Rebuilds every list from the resident slots (drops retired slots' tiles).
+void compact(bsam_batch* b) {
+  for (auto& L : b->lists) {
+    L.h.clear();
+    L.uploaded = 0;
+  }
+  for (size_t s = 0; s < b->slots.size(); ++s) {
+    b->slots[s].stale = false;
+    if (b->slots[s].used) append_items(b, (int)s);
+  }
+  b->cfg_dirty = true;
+}
+
+// ---- tick -------------------------------------------------------------------
+
+int grid_for(bsam_batch* b, int l) {
+  const int cap = std::max(1, b->lists[l].cap);
+  const int lim = b->tuning.grid_ctas > 0 ? b->tuning.grid_ctas : 16 * b->nsm;
+  return std::max(1, std::min(cap, lim));
+}
+
+template <int D>
+void tick_t(bsam_batch* b, cudaGraphConditionalHandle handle) {
+  const dim3 blk(32, TILE_Y, 1);
+  cudaStream_t s = b->stream;
+  const int nu = b->bp.nsmoothingpasses;
+  DevPatch* pt = b->d_pt;
+  const int* cnt = b->d_counts;
+  const List* L = b->lists;
+  int64_t n = 0;
+  auto relax = [&](int d) {
+    for (int pass = 0; pass < nu; ++pass)
+      for (int color = 0; color < 2; ++color) {
+        if (b->mixed)
+          kb_relax<float, D><<<grid_for(b, L_FINE + d), blk, 0, s>>>(pt, L[L_FINE + d].d,
+                                                                    cnt + L_FINE + d, color);
+        else
+          kb_relax<double, D><<<grid_for(b, L_FINE + d), blk, 0, s>>>(pt, L[L_FINE + d].d,
+                                                                     cnt + L_FINE + d, color);
+        ++n;
+      }
+  };
+  const int gm = grid_for(b, L_MASTER);
+  kb_source<D><<<gm, blk, 0, s>>>(pt, L[L_MASTER].d, cnt + L_MASTER);
+  ++n;
+  if (b->mixed) {
+    kb_defect<D><<<gm, blk, 0, s>>>(pt, L[L_MASTER].d, cnt + L_MASTER, b->d_partials, 1);
+    ++n;
+  }
+  for (int d = 0; d < b->cap_depth; ++d) {
+    relax(d);
+    const int gc = grid_for(b, L_COARSE + d);
+    if (b->mixed) {
+      kb_restrict<float, D><<<gc, blk, 0, s>>>(pt, L[L_COARSE + d].d, cnt + L_COARSE + d);
+      kb_coarse_load<float, D><<<gc, blk, 0, s>>>(pt, L[L_COARSE + d].d, cnt + L_COARSE + d);
+    } else {
+      kb_restrict<double, D><<<gc, blk, 0, s>>>(pt, L[L_COARSE + d].d, cnt + L_COARSE + d);
+      kb_coarse_load<double, D><<<gc, blk, 0, s>>>(pt, L[L_COARSE + d].d, cnt + L_COARSE + d);
+    }
+    n += 2;
+  }
+  {
+    const int cap = std::max(1, L[L_TOPS].cap);
+    const int gb = std::max(1, std::min(cap, 4 * b->nsm));
+    kb_bottom<D><<<gb, BOTTOM_THREADS, 0, s>>>(pt, L[L_TOPS].d, cnt + L_TOPS, nu);
+    ++n;
+  }
+  for (int d = b->cap_depth - 1; d >= 0; --d) {
+    const int gf = grid_for(b, L_FINE + d);
+    if (b->mixed) kb_correct<float, D><<<gf, blk, 0, s>>>(pt, L[L_FINE + d].d, cnt + L_FINE + d);
+    else kb_correct<double, D><<<gf, blk, 0, s>>>(pt, L[L_FINE + d].d, cnt + L_FINE + d);
+    ++n;
+    relax(d);
+  }
+  if (b->mixed) {
+    kb_update<D><<<gm, blk, 0, s>>>(pt, L[L_MASTER].d, cnt + L_MASTER);
+    kb_defect<D><<<gm, blk, 0, s>>>(pt, L[L_MASTER].d, cnt + L_MASTER, b->d_partials, 0);
+    n += 2;
+  } else {
+    kb_resid<D><<<gm, blk, 0, s>>>(pt, L[L_MASTER].d, cnt + L_MASTER, b->d_partials);
+    ++n;
+  }
+  const int gctl = std::max(1, std::min(b->bp.max_slots, 2 * b->nsm));
+  k_batch_control<<<gctl, BLOCK_THREADS, 0, s>>>(pt, b->d_cfg, b->d_state, b->d_log,
+                                                 BSAM_BATCH_MAX_STEPS, b->d_out, b->d_partials,
+                                                 b->d_ctl, b->bp.max_slots);
+  k_batch_cond<<<1, 1, 0, s>>>(b->d_ctl, handle);
+  n += 2;
+  b->kernels_per_tick = n;
+}
+
+int capture(bsam_batch* b) {
+  CU(cudaStreamSynchronize(b->stream));
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  b->exec = nullptr;
+  cudaGraph_t g = nullptr;
+  CU(cudaGraphCreate(&g, 0));
+  cudaGraphConditionalHandle handle;
+  cudaError_t e = cudaGraphConditionalHandleCreate(&handle, g, 1, cudaGraphCondAssignDefault);
+  cudaGraphNodeParams np{};
+  cudaGraphNode_t node;
+  if (e == cudaSuccess) {
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = handle;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    e = cudaGraphAddNode(&node, g, nullptr, 0, &np);
+  }
+  if (e == cudaSuccess) {
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    e = cudaStreamBeginCaptureToGraph(b->stream, body, nullptr, nullptr, 0,
+                                      cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      if (b->bp.ndims == 2) tick_t<2>(b, handle);
+      else tick_t<3>(b, handle);
+      cudaGraph_t captured = nullptr;
+      e = cudaStreamEndCapture(b->stream, &captured);
+    }
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    b->exec = nullptr;
+    cudaGetLastError();
+    return fail(b, BSAM_ERR_CUDA, std::string("tick graph: ") + cudaGetErrorString(e));
+  }
+  b->need_capture = false;
+  ++b->st.captures;
+  return BSAM_OK;
+}
+
+// Uploads list growth, counts and slot configuration; re-captures the tick
+// graph when capacities or depths changed.
+int flush(bsam_batch* b) {
+  for (int l = 0; l < NLIST; ++l) {
+    List& L = b->lists[l];
+    const int n = (int)L.h.size();
+    if (n > L.cap) {
+      CU(cudaStreamSynchronize(b->stream));
+      if (L.d) cudaFree(L.d);
+      L.d = nullptr;
+      int cap = std::max(256, L.cap);
+      while (cap < n) cap *= 2;
+      if (cudaMalloc(&L.d, sizeof(Item) * cap) != cudaSuccess) {
+        L.cap = 0;
+        return fail(b, BSAM_ERR_NOMEM, "work list allocation failed");
+      }
+      L.cap = cap;
+      L.uploaded = 0;
+      b->need_capture = true;
+      if (l == L_MASTER && cap > b->partials_cap) {
+        if (b->d_partials) cudaFree(b->d_partials);
+        b->d_partials = nullptr;
+        if (cudaMalloc(&b->d_partials, sizeof(double) * cap) != cudaSuccess)
+          return fail(b, BSAM_ERR_NOMEM, "partials allocation failed");
+        b->partials_cap = cap;
+      }
+    }
+    if (L.uploaded < n) {
+      const int rc = stage_copy(b, L.d + L.uploaded, L.h.data() + L.uploaded,
+                                sizeof(Item) * (n - L.uploaded));
+      if (rc) return rc;
+      L.uploaded = n;
+    }
+  }
+  std::vector<int> counts(NLIST);
+  for (int l = 0; l < NLIST; ++l) counts[l] = (int)b->lists[l].h.size();
+  if (counts != b->counts_dev) {
+    const int rc = stage_copy(b, b->d_counts, counts.data(), sizeof(int) * NLIST);
+    if (rc) return rc;
+    b->counts_dev = counts;
+  }
+  if (b->cfg_dirty) {
+    const int rc = stage_copy(b, b->d_cfg, b->h_cfg.data(), sizeof(SlotCfg) * b->h_cfg.size());
+    if (rc) return rc;
+    b->cfg_dirty = false;
+  }
+  int depth = 1;
+  for (auto& S : b->slots)
+    if (S.used) depth = std::max(depth, S.ntop);
+  if (depth > b->cap_depth) {
+    b->cap_depth = depth;
+    b->need_capture = true;
+  }
+  stage_commit(b);
+  if (b->need_capture) return capture(b);
+  return BSAM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* bsam_batch_last_error(bsam_batch* b) { return b ? b->err.c_str() : "null handle"; }
+
+int bsam_batch_create(bsam_batch** out, int device, const bsam_batch_params* p) {
+  if (!out || !p) return BSAM_ERR_ARG;
+  *out = nullptr;
+  if (p->ndims < 2 || p->ndims > 3 || p->nsmoothingpasses < 1 || p->maxvcycles < 1 ||
+      p->max_slots < 1 || p->max_slots > (1 << 20) / RMAX || p->pool_bytes < 0)
+    return BSAM_ERR_ARG;
+  if (p->precision != BSAM_PREC_FP64 && p->precision != BSAM_PREC_MIXED)
+    return BSAM_ERR_UNSUPPORTED;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)
+    return BSAM_ERR_NODEVICE;
+  if (cudaSetDevice(device) != cudaSuccess) return BSAM_ERR_NODEVICE;
+  bsam_batch* b = new bsam_batch();
+  b->device = device;
+  b->bp = *p;
+  b->mixed = p->precision == BSAM_PREC_MIXED;
+  cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, device);
+  const int ns = p->max_slots;
+  size_t pool = (size_t)p->pool_bytes;
+  if (pool == 0) {
+    size_t fr = 0, tot = 0;
+    cudaMemGetInfo(&fr, &tot);
+    pool = fr / 2;
+  }
+  pool = (size_t)roundup((int64_t)pool, 4096);
+  bool ok = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaMalloc(&b->d_pool, pool) == cudaSuccess &&
+            cudaMalloc(&b->d_pt, sizeof(DevPatch) * ns * RMAX) == cudaSuccess &&
+            cudaMalloc(&b->d_cfg, sizeof(SlotCfg) * ns) == cudaSuccess &&
+            cudaMalloc(&b->d_state, sizeof(SlotState) * ns) == cudaSuccess &&
+            cudaMalloc(&b->d_log, sizeof(StepLog) * ns * BSAM_BATCH_MAX_STEPS) == cudaSuccess &&
+            cudaHostAlloc(&b->h_out, sizeof(SlotOut) * ns, cudaHostAllocMapped) == cudaSuccess &&
+            cudaMalloc(&b->d_ctl, sizeof(BatchCtl)) == cudaSuccess &&
+            cudaMalloc(&b->d_status, sizeof(DevStatus)) == cudaSuccess &&
+            cudaMallocHost(&b->h_status, sizeof(DevStatus)) == cudaSuccess &&
+            cudaMalloc(&b->d_counts, sizeof(int) * NLIST) == cudaSuccess;
+  if (ok) ok = cudaHostGetDevicePointer((void**)&b->d_out, b->h_out, 0) == cudaSuccess;
+  if (!ok) {
+    cudaGetLastError();
+    bsam_batch_destroy(b);
+    return BSAM_ERR_NOMEM;
+  }
+  b->pool_bytes = pool;
+  b->free_[0] = pool;
+  b->slots.assign(ns, SlotPlan{});
+  b->h_cfg.assign(ns, SlotCfg{});
+  std::memset(b->h_out, 0, sizeof(SlotOut) * ns);
+  cudaMemsetAsync(b->d_pt, 0, sizeof(DevPatch) * ns * RMAX, b->stream);  // active = 0
+  cudaMemsetAsync(b->d_cfg, 0, sizeof(SlotCfg) * ns, b->stream);
+  cudaMemsetAsync(b->d_state, 0, sizeof(SlotState) * ns, b->stream);  // SLOT_IDLE
+  cudaMemsetAsync(b->d_ctl, 0, sizeof(BatchCtl), b->stream);
+  cudaMemsetAsync(b->d_counts, 0, sizeof(int) * NLIST, b->stream);
+  cudaMemsetAsync(b->d_status, 0, sizeof(DevStatus), b->stream);
+  b->counts_dev.assign(NLIST, 0);
+  if (cudaStreamSynchronize(b->stream) != cudaSuccess) {
+    bsam_batch_destroy(b);
+    return BSAM_ERR_CUDA;
+  }
+  *out = b;
+  return BSAM_OK;
+}
+
+int bsam_batch_destroy(bsam_batch* b) {
+  if (!b) return BSAM_ERR_ARG;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  for (auto& L : b->lists)
+    if (L.d) cudaFree(L.d);
+  for (auto& c : b->chunks)
+    if (c.ev) b->free_events.push_back(c.ev);
+  std::sort(b->free_events.begin(), b->free_events.end());
+  b->free_events.erase(std::unique(b->free_events.begin(), b->free_events.end()),
+                       b->free_events.end());
+  for (auto e : b->free_events) cudaEventDestroy(e);
+  if (b->stage) cudaFreeHost(b->stage);
+  if (b->d_partials) cudaFree(b->d_partials);
+  if (b->d_counts) cudaFree(b->d_counts);
+  if (b->h_status) cudaFreeHost(b->h_status);
+  if (b->d_status) cudaFree(b->d_status);
+  if (b->d_ctl) cudaFree(b->d_ctl);
+  if (b->h_out) cudaFreeHost(b->h_out);
+  if (b->d_log) cudaFree(b->d_log);
+  if (b->d_state) cudaFree(b->d_state);
+  if (b->d_cfg) cudaFree(b->d_cfg);
+  if (b->d_pt) cudaFree(b->d_pt);
+  if (b->d_pool) cudaFree(b->d_pool);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+  return BSAM_OK;
+}
+
+int bsam_batch_set_tuning(bsam_batch* b, const bsam_batch_tuning* t) {
+  if (!b || !t || t->grid_ctas < 0) return BSAM_ERR_ARG;
+  b->tuning = *t;
+  b->need_capture = true;
+  return BSAM_OK;
+}
+
+int bsam_batch_footprint(bsam_batch* b, const bsam_batch_problem* prob, int64_t* bytes) {
+  if (!b || !prob || !bytes) return BSAM_ERR_ARG;
+  SlotPlan S;
+  const int rc = plan_slot(b, prob, 0, nullptr, S);
+  if (rc) return rc;
+  *bytes = (int64_t)S.bytes;
+  return BSAM_OK;
+}
+
+int bsam_batch_submit(bsam_batch* b, const bsam_batch_problem* prob, const double* q0,
+                      int* slot) {
+  if (!b || !prob || !q0 || !slot) return BSAM_ERR_ARG;
+  CU(cudaSetDevice(b->device));
+  SlotPlan probe;
+  int rc = plan_slot(b, prob, 0, nullptr, probe);
+  if (rc) return rc;
+  // A free slot whose old tiles are gone from the lists; compact if only
+  // retired ones are left.
+  int s = -1;
+  bool any_stale = false;
+  for (size_t i = 0; i < b->slots.size(); ++i) {
+    if (b->slots[i].used) continue;
+    if (!b->slots[i].stale) {
+      s = (int)i;
+      break;
+    }
+    any_stale = true;
+  }
+  if (s < 0 && !any_stale) return fail(b, BSAM_ERR_NOMEM, "no free slot");
+  size_t off = 0;
+  if (!pool_alloc(b, probe.bytes, &off)) return fail(b, BSAM_ERR_NOMEM, "pool is full");
+  if (s < 0) {
+    compact(b);
+    for (size_t i = 0; i < b->slots.size(); ++i)
+      if (!b->slots[i].used) {
+        s = (int)i;
+        break;
+      }
+  }
+  SlotPlan& S = b->slots[s];
+  const int rec0 = s * RMAX;
+  rc = plan_slot(b, prob, rec0, b->d_pool + off, S);
+  if (rc) {
+    pool_free(b, off, probe.bytes);
+    return rc;
+  }
+  S.used = true;
+  S.stale = false;
+  S.off = off;
+  const int nd = b->bp.ndims;
+  // Fresh fields, records, the initial state and its ghosts.
+  CU(cudaMemsetAsync(b->d_pool + off, 0, S.bytes, b->stream));
+  rc = stage_copy(b, b->d_pt + rec0, S.recs.data(), sizeof(DevPatch) * S.nrec);
+  if (rc) return rc;
+  const DevPatch& M = S.recs[S.master];
+  const int e0 = M.n[0] + 2, e1 = M.n[1] + 2, e2 = nd == 3 ? M.n[2] + 2 : 1;
+  const size_t hcomp = (size_t)e0 * e1 * e2;
+  char* st = stage_alloc(b, sizeof(double) * 2 * hcomp);
+  if (!st) return fail(b, BSAM_ERR_NOMEM, "pinned staging allocation failed");
+  std::memcpy(st, q0, sizeof(double) * 2 * hcomp);
+  for (int c = 0; c < 2; ++c)
+    CU(cudaMemcpy2DAsync(M.q[c], M.sy * sizeof(double), st + c * hcomp * sizeof(double),
+                         e0 * sizeof(double), e0 * sizeof(double), (size_t)e1 * e2,
+                         cudaMemcpyHostToDevice, b->stream));
+  const int64_t total = (int64_t)hcomp;
+  const int nb = (int)((total + 255) / 256);
+  if (nd == 2) k_setbc<double, 2><<<nb, 256, 0, b->stream>>>(b->d_pt, rec0 + S.master, total);
+  else k_setbc<double, 3><<<nb, 256, 0, b->stream>>>(b->d_pt, rec0 + S.master, total);
+  CU(cudaGetLastError());
+  SlotState z{SLOT_RUNNING, 0, 0, 0};
+  rc = stage_copy(b, b->d_state + s, &z, sizeof(SlotState));
+  if (rc) return rc;
+  SlotCfg& C = b->h_cfg[s];
+  C.rec0 = rec0;
+  C.nrec = S.nrec;
+  C.master = rec0 + S.master;
+  C.nsteps = prob->nsteps;
+  C.maxv = b->bp.maxvcycles;
+  C.denom = 2.0 * (double)S.cells;
+  C.tol = b->bp.qerrortol;
+  append_items(b, s);
+  volatile SlotOut* o = b->h_out + s;
+  o->step = 0;
+  o->vcycles = 0;
+  o->phase = SLOT_RUNNING;
+  stage_commit(b);
+  *slot = s;
+  return BSAM_OK;
+}
+
+int bsam_batch_advance(bsam_batch* b, int max_ticks) {
+  if (!b || max_ticks < 1) return BSAM_ERR_ARG;
+  CU(cudaSetDevice(b->device));
+  int rc = flush(b);
+  if (rc) return rc;
+  k_batch_budget<<<1, 1, 0, b->stream>>>(b->d_ctl, max_ticks);
+  CU(cudaGetLastError());
+  CU(cudaGraphLaunch(b->exec, b->stream));
+  b->st.launches += 1;
+  return BSAM_OK;
+}
+
+int bsam_batch_sync(bsam_batch* b) {
+  if (!b) return BSAM_ERR_ARG;
+  CU(cudaSetDevice(b->device));
+  CU(cudaStreamSynchronize(b->stream));
+  return BSAM_OK;
+}
+
+static int running_slots(bsam_batch* b) {
+  int n = 0;
+  for (size_t s = 0; s < b->slots.size(); ++s)
+    if (b->slots[s].used && ((volatile SlotOut*)b->h_out)[s].phase == SLOT_RUNNING) ++n;
+  return n;
+}
+
+int bsam_batch_run(bsam_batch* b) {
+  if (!b) return BSAM_ERR_ARG;
+  for (int guard = 0; guard < 1000000; ++guard) {
+    int rc = bsam_batch_advance(b, 1 << 20);
+    if (rc) return rc;
+    rc = bsam_batch_sync(b);
+    if (rc) return rc;
+    if (running_slots(b) == 0) return BSAM_OK;
+  }
+  return fail(b, BSAM_ERR_STATE, "batch did not finish");
+}
+
+int bsam_batch_poll(bsam_batch* b, int* slots, int maxn) {
+  if (!b) return BSAM_ERR_ARG;
+  int n = 0;
+  for (size_t s = 0; s < b->slots.size(); ++s) {
+    if (!b->slots[s].used) continue;
+    const int ph = ((volatile SlotOut*)b->h_out)[s].phase;
+    if (ph == SLOT_DONE || ph == SLOT_FAILED) {
+      if (slots && n < maxn) slots[n] = (int)s;
+      ++n;
+    }
+  }
+  return n;
+}
+
+int bsam_batch_slot_phase(bsam_batch* b, int slot, int* phase, int* steps_done) {
+  if (!b || slot < 0 || slot >= (int)b->slots.size()) return BSAM_ERR_ARG;
+  volatile SlotOut* o = b->h_out + slot;
+  if (phase) *phase = b->slots[slot].used ? o->phase : SLOT_IDLE;
+  if (steps_done) *steps_done = b->slots[slot].used ? o->step : 0;
+  return BSAM_OK;
+}
+
+int bsam_batch_collect(bsam_batch* b, int slot, double* q, bsam_step_result* steps,
+                       double* mass) {
+  if (!b || slot < 0 || slot >= (int)b->slots.size() || !b->slots[slot].used)
+    return BSAM_ERR_ARG;
+  CU(cudaSetDevice(b->device));
+  CU(cudaStreamSynchronize(b->stream));
+  SlotPlan& S = b->slots[slot];
+  const int ph = ((volatile SlotOut*)b->h_out)[slot].phase;
+  if (ph != SLOT_DONE && ph != SLOT_FAILED) return fail(b, BSAM_ERR_STATE, "problem not finished");
+  const int nd = b->bp.ndims;
+  const DevPatch& M = S.recs[S.master];
+  const int rec_master = slot * RMAX + S.master;
+  const SlotCfg& C = b->h_cfg[slot];
+  if (q) {
+    const int e0 = M.n[0] + 2, e1 = M.n[1] + 2, e2 = nd == 3 ? M.n[2] + 2 : 1;
+    const size_t hcomp = (size_t)e0 * e1 * e2;
+    for (int c = 0; c < 2; ++c)
+      CU(cudaMemcpy2DAsync(q + c * hcomp, e0 * sizeof(double), M.q[c], M.sy * sizeof(double),
+                           e0 * sizeof(double), (size_t)e1 * e2, cudaMemcpyDeviceToHost,
+                           b->stream));
+  }
+  std::vector<StepLog> lg(S.prob.nsteps);
+  CU(cudaMemcpyAsync(lg.data(), b->d_log + (int64_t)slot * BSAM_BATCH_MAX_STEPS,
+                     sizeof(StepLog) * lg.size(), cudaMemcpyDeviceToHost, b->stream));
+  if (mass) {
+    const double hh = M.h;
+    const double hd = nd == 2 ? hh * hh : hh * hh * hh;
+    const int ni = C.ie - C.ib;
+    const Item* items = b->lists[L_MASTER].d + C.ib;
+    (void)rec_master;
+    if (nd == 2)
+      k_mass<double, 2><<<ni, dim3(32, TILE_Y), 0, b->stream>>>(b->d_pt, items, b->d_partials,
+                                                                 b->d_status, ni, hd);
+    else
+      k_mass<double, 3><<<ni, dim3(32, TILE_Y), 0, b->stream>>>(b->d_pt, items, b->d_partials,
+                                                                 b->d_status, ni, hd);
+    CU(cudaGetLastError());
+    CU(cudaMemcpyAsync(b->h_status, b->d_status, sizeof(DevStatus), cudaMemcpyDeviceToHost,
+                       b->stream));
+  }
+  CU(cudaStreamSynchronize(b->stream));
+  const int done = ((volatile SlotOut*)b->h_out)[slot].step;
+  if (steps)
+    for (int i = 0; i < S.prob.nsteps; ++i) {
+      if (i < done) {
+        steps[i].nvcycles = lg[i].nv;
+        steps[i].converged = lg[i].conv;
+        steps[i].residual = lg[i].res;
+      } else {
+        steps[i].nvcycles = 0;
+        steps[i].converged = 0;
+        steps[i].residual = NAN;
+      }
+    }
+  if (mass) *mass = b->h_status->mass;
+  // Release: memory now, the slot once its tiles leave the lists.
+  pool_free(b, S.off, S.bytes);
+  S.used = false;
+  S.stale = true;
+  volatile SlotOut* o = b->h_out + slot;
+  o->phase = SLOT_IDLE;
+  int live = 0, dead = 0;
+  for (auto& x : b->slots) {
+    if (x.used) ++live;
+    else if (x.stale) ++dead;
+  }
+  // Drop retired tiles once they outnumber the resident problems.
+  if (dead > std::max(8, live)) compact(b);
+  return ph == SLOT_FAILED ? fail(b, BSAM_ERR_DIVERGED, "residual is not finite") : BSAM_OK;
+}
+
+int bsam_batch_get_stream(bsam_batch* b, void** stream) {
+  if (!b || !stream) return BSAM_ERR_ARG;
+  *stream = (void*)b->stream;
+  return BSAM_OK;
+}
+
+int bsam_batch_get_stats(bsam_batch* b, bsam_batch_stats* s) {
+  if (!b || !s) return BSAM_ERR_ARG;
+  cudaSetDevice(b->device);
+  BatchCtl c{};
+  if (cudaMemcpy(&c, b->d_ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return fail(b, BSAM_ERR_CUDA, "stats read failed");
+  bsam_batch_stats o = b->st;
+  o.ticks = c.ticks;
+  o.kernels_per_tick = b->kernels_per_tick;
+  o.launches = c.ticks * b->kernels_per_tick;
+  o.pool_used = (int64_t)b->pool_used;
+  o.pool_bytes = (int64_t)b->pool_bytes;
+  o.resident = 0;
+  for (auto& x : b->slots) o.resident += x.used ? 1 : 0;
+  o.running = running_slots(b);
+  *s = o;
+  return BSAM_OK;
+}
+
+}  // extern "C"

@@ -576,6 +576,8 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
     P.parent = d.parent;
     P.level = d.level;
     P.problem = 0;
+    P.active = 1;
+    P.newstep = 0;
     P.twin = is_twin ? -1 : twin_of[p];
     // Precision of the record.
     const int64_t ncell = cells_of(P.n, nd);
@@ -706,6 +708,8 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
   }
   // Parents of the twins are the masters' parents.
   for (int r = npatch; r < nrec; ++r) h->hp[r].parent = h->hp[rec_src[r]].parent;
+  for (int r = 0; r < nrec; ++r)
+    h->hp[r].pprec = h->hp[r].parent >= 0 ? h->hp[h->hp[r].parent].prec : h->hp[r].prec;
   // TMA tensor maps of the fused records (q0, q1, qb0, qb1, f0, f1, bs).
   {
     std::vector<int> fused_recs;

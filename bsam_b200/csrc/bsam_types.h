@@ -42,7 +42,9 @@ struct DevPatch {
   int32_t zchunk;     // fused kernel: planes (3D) / rows (2D) per streaming chunk
   int32_t twin;       // mixed form: the working patch of this FP64 master, else -1
   int32_t delta;      // 1: q holds a correction e of the base state bs (mixed.cuh)
-  int32_t pad_;
+  int32_t active;     // 0: every kernel skips this patch (finished or idle batch slot)
+  int32_t newstep;    // batch masters: a new time step starts this iteration
+  int32_t pprec;      // PREC_* of the parent (transfer kernels pick their types by it)
   int64_t sy, sz;     // element strides of j and k
   // Base pointers of element (0,0,0), the low ghost corner, per component.
   void* q[2];         // solution (phi, mu), with ghost ring: the state between stages

@@ -363,15 +363,21 @@ __device__ __forceinline__ bool last_block_total(double mine, double* partials,
   return false;
 }
 
-// ---- grid kernels --------------------------------------------------------------
+// ---- tile bodies ---------------------------------------------------------------
+//
+// One function per kernel that processes one Item (tile) of its work list.
+// The grid kernels below run one tile per CTA; the batch kernels (batch.cuh)
+// run the same bodies in a grid-stride loop over a device-resident list.
+// Inactive patches (finished or idle batch slots) are skipped whole, which is
+// uniform per CTA.
 
 // RelaxGrid (one colour pass) + SetGhost(level, ipass) for physical faces.
 // color 0 = ipass 1 = cells with even i+j(+k); color 1 = ipass 2.
 template <class T, int D>
-__global__ void __launch_bounds__(BLOCK_THREADS)
-    k_relax(const DevPatch* __restrict__ PT, const Item* __restrict__ items, int color) {
-  const Item it = items[blockIdx.x];
+__device__ __forceinline__ void relax_item(const DevPatch* __restrict__ PT, const Item it,
+                                           int color) {
   const DevPatch P = PT[it.patch];  // by value: fields stay in registers
+  if (!P.active) return;
   const int j = it.ty * TILE_Y + threadIdx.y + 1;
   const int k = (D == 3) ? it.tz + 1 : 0;
   if (j > P.n[1]) return;
@@ -381,15 +387,9 @@ __global__ void __launch_bounds__(BLOCK_THREADS)
   relax_cell<T, D>(P, i, j, k);
 }
 
-// ErrorAFAS / L2Error / SquareSum (afas:108-221), errortype 1:
-// residual = sqrt(sum rf^2 / (nrvars * ncells)) over the finest level.
+// Sum of rf^2 over this thread's cells of a tile (ErrorAFAS's SquareSum).
 template <class T, int D>
-__global__ void __launch_bounds__(BLOCK_THREADS)
-    k_resid_norm(const DevPatch* __restrict__ PT, const Item* __restrict__ items,
-                 double* __restrict__ partials, DevStatus* __restrict__ st, int nitems,
-                 double denom, double tol) {
-  const Item it = items[blockIdx.x];
-  const DevPatch P = PT[it.patch];
+__device__ __forceinline__ double resid_item(const DevPatch& P, const Item it) {
   const int j = it.ty * TILE_Y + threadIdx.y + 1;
   const int k = (D == 3) ? it.tz + 1 : 0;
   const int i0 = (it.tx * 32 + threadIdx.x) * 2 + 1;
@@ -409,21 +409,13 @@ __global__ void __launch_bounds__(BLOCK_THREADS)
       }
     }
   }
-  const double bs = block_sum(acc);
-  double total;
-  if (last_block_total(bs, partials, &st->ticket, nitems, total)) {
-    const double r = sqrt(total / denom);
-    st->sumsq = total;
-    st->residual = r;
-    st->converged = (r < tol) ? 1 : 0;
-  }
+  return acc;
 }
 
 template <class TC, class TP, int D>
-__global__ void __launch_bounds__(BLOCK_THREADS)
-    k_restrict(const DevPatch* __restrict__ PT, const Item* __restrict__ items) {
-  const Item it = items[blockIdx.x];
+__device__ __forceinline__ void restrict_item(const DevPatch* __restrict__ PT, const Item it) {
   const DevPatch C = PT[it.patch];
+  if (!C.active) return;
   const DevPatch P = PT[C.parent];
   const int jc = it.ty * TILE_Y + threadIdx.y + 1;
   const int kc = (D == 3) ? it.tz + 1 : 0;
@@ -438,10 +430,9 @@ __global__ void __launch_bounds__(BLOCK_THREADS)
 }
 
 template <class TC, class TP, int D>
-__global__ void __launch_bounds__(BLOCK_THREADS)
-    k_coarse_load(const DevPatch* __restrict__ PT, const Item* __restrict__ items) {
-  const Item it = items[blockIdx.x];
+__device__ __forceinline__ void coarse_load_item(const DevPatch* __restrict__ PT, const Item it) {
   const DevPatch C = PT[it.patch];
+  if (!C.active) return;
   const DevPatch P = PT[C.parent];
   const int jc = it.ty * TILE_Y + threadIdx.y + 1;
   const int kc = (D == 3) ? it.tz + 1 : 0;
@@ -456,10 +447,9 @@ __global__ void __launch_bounds__(BLOCK_THREADS)
 }
 
 template <class TC, class TP, int D>
-__global__ void __launch_bounds__(BLOCK_THREADS)
-    k_correct(const DevPatch* __restrict__ PT, const Item* __restrict__ items) {
-  const Item it = items[blockIdx.x];
+__device__ __forceinline__ void correct_item(const DevPatch* __restrict__ PT, const Item it) {
   const DevPatch C = PT[it.patch];
+  if (!C.active) return;
   const DevPatch P = PT[C.parent];
   const int J = it.ty * TILE_Y + threadIdx.y + 1;
   const int K = (D == 3) ? it.tz + 1 : 0;
@@ -474,17 +464,19 @@ __global__ void __launch_bounds__(BLOCK_THREADS)
 }
 
 // GetSourceFunction + UpdateSourceFunction on one level (afas:312-367,
-// 427-486): f = Source(qold) + 0.
+// 427-486): f = Source(qold) + 0.  newstep_only (batches): only masters
+// whose new time step starts now; they keep no qold, so qold = q (the
+// reference's CopyQToQold just before, lib/bsamroutines.f90:659-661).
 template <class T, int D>
-__global__ void __launch_bounds__(BLOCK_THREADS)
-    k_source(const DevPatch* __restrict__ PT, const Item* __restrict__ items) {
-  const Item it = items[blockIdx.x];
+__device__ __forceinline__ void source_item(const DevPatch* __restrict__ PT, const Item it,
+                                            int newstep_only) {
   const DevPatch P = PT[it.patch];
+  if (!P.active || (newstep_only && !P.newstep)) return;
   const int j = it.ty * TILE_Y + threadIdx.y + 1;
   const int k = (D == 3) ? it.tz + 1 : 0;
   if (j > P.n[1]) return;
   const int i0 = (it.tx * 32 + threadIdx.x) * 2 + 1;
-  const T* qo = fld<T>(P.qo[0]);
+  const T* qo = fld<T>(P.qo[0] ? P.qo[0] : P.q[0]);
   T* f0 = fld<T>(P.f[0]);
   T* f1 = fld<T>(P.f[1]);
 #pragma unroll
@@ -497,6 +489,56 @@ __global__ void __launch_bounds__(BLOCK_THREADS)
     f0[c] = a;
     f1[c] = b;
   }
+}
+
+// ---- grid kernels (one tile per CTA) --------------------------------------------
+
+template <class T, int D>
+__global__ void __launch_bounds__(BLOCK_THREADS)
+    k_relax(const DevPatch* __restrict__ PT, const Item* __restrict__ items, int color) {
+  relax_item<T, D>(PT, items[blockIdx.x], color);
+}
+
+// ErrorAFAS / L2Error / SquareSum (afas:108-221), errortype 1:
+// residual = sqrt(sum rf^2 / (nrvars * ncells)) over the finest level.
+template <class T, int D>
+__global__ void __launch_bounds__(BLOCK_THREADS)
+    k_resid_norm(const DevPatch* __restrict__ PT, const Item* __restrict__ items,
+                 double* __restrict__ partials, DevStatus* __restrict__ st, int nitems,
+                 double denom, double tol) {
+  const Item it = items[blockIdx.x];
+  const double bs = block_sum(resid_item<T, D>(PT[it.patch], it));
+  double total;
+  if (last_block_total(bs, partials, &st->ticket, nitems, total)) {
+    const double r = sqrt(total / denom);
+    st->sumsq = total;
+    st->residual = r;
+    st->converged = (r < tol) ? 1 : 0;
+  }
+}
+
+template <class TC, class TP, int D>
+__global__ void __launch_bounds__(BLOCK_THREADS)
+    k_restrict(const DevPatch* __restrict__ PT, const Item* __restrict__ items) {
+  restrict_item<TC, TP, D>(PT, items[blockIdx.x]);
+}
+
+template <class TC, class TP, int D>
+__global__ void __launch_bounds__(BLOCK_THREADS)
+    k_coarse_load(const DevPatch* __restrict__ PT, const Item* __restrict__ items) {
+  coarse_load_item<TC, TP, D>(PT, items[blockIdx.x]);
+}
+
+template <class TC, class TP, int D>
+__global__ void __launch_bounds__(BLOCK_THREADS)
+    k_correct(const DevPatch* __restrict__ PT, const Item* __restrict__ items) {
+  correct_item<TC, TP, D>(PT, items[blockIdx.x]);
+}
+
+template <class T, int D>
+__global__ void __launch_bounds__(BLOCK_THREADS)
+    k_source(const DevPatch* __restrict__ PT, const Item* __restrict__ items) {
+  source_item<T, D>(PT, items[blockIdx.x], 0);
 }
 
 // SetBC (boundary.f90:598-891) for one patch, all ghost cells, any face

@@ -22,15 +22,15 @@
 
 namespace bsam {
 
-// Defect kernel over the masters' tiles: ErrorAFAS of q64 (the same norm as
-// k_resid_norm) plus the twins' start (e = 0), base and right-hand side.
+// Defect of one master tile: ErrorAFAS of q64 (the same norm as
+// k_resid_norm) plus the twin's start (e = 0), base and right-hand side.
+// Returns this thread's sum of squares.  newstep_only (batches): only masters
+// whose time step starts in this iteration.
 template <class TW, int D>
-__global__ void __launch_bounds__(BLOCK_THREADS)
-    k_defect(const DevPatch* __restrict__ PT, const Item* __restrict__ items,
-             double* __restrict__ partials, DevStatus* __restrict__ st, int nitems,
-             double denom, double tol) {
-  const Item it = items[blockIdx.x];
+__device__ __forceinline__ double defect_item(const DevPatch* __restrict__ PT, const Item it,
+                                              int newstep_only) {
   const DevPatch M = PT[it.patch];
+  if (!M.active || (newstep_only && !M.newstep)) return 0.0;
   const DevPatch W = PT[M.twin];
   const int j = it.ty * TILE_Y + threadIdx.y + 1;
   const int k = (D == 3) ? it.tz + 1 : 0;
@@ -61,22 +61,14 @@ __global__ void __launch_bounds__(BLOCK_THREADS)
         write_through<TW, D>(W, e0, e1, i, j, k, TW(0), TW(0));
     }
   }
-  const double bs = block_sum(acc);
-  double total;
-  if (last_block_total(bs, partials, &st->ticket, nitems, total)) {
-    const double r = sqrt(total / denom);
-    st->sumsq = total;
-    st->residual = r;
-    st->converged = (r < tol) ? 1 : 0;
-  }
+  return acc;
 }
 
-// q64 += e on the interior; ghosts by write-through.
+// q64 += e on the interior of one master tile; ghosts by write-through.
 template <class TW, int D>
-__global__ void __launch_bounds__(BLOCK_THREADS)
-    k_update(const DevPatch* __restrict__ PT, const Item* __restrict__ items) {
-  const Item it = items[blockIdx.x];
+__device__ __forceinline__ void update_item(const DevPatch* __restrict__ PT, const Item it) {
   const DevPatch M = PT[it.patch];
+  if (!M.active) return;
   const DevPatch W = PT[M.twin];
   const int j = it.ty * TILE_Y + threadIdx.y + 1;
   const int k = (D == 3) ? it.tz + 1 : 0;
@@ -97,6 +89,28 @@ __global__ void __launch_bounds__(BLOCK_THREADS)
     q1[c] = nb;
     if (M.wt && near_boundary(M, i, j, k, D)) write_through<double, D>(M, q0, q1, i, j, k, na, nb);
   }
+}
+
+// Defect kernel over the masters' tiles, with the FP64 norm in d_status.
+template <class TW, int D>
+__global__ void __launch_bounds__(BLOCK_THREADS)
+    k_defect(const DevPatch* __restrict__ PT, const Item* __restrict__ items,
+             double* __restrict__ partials, DevStatus* __restrict__ st, int nitems,
+             double denom, double tol) {
+  const double bs = block_sum(defect_item<TW, D>(PT, items[blockIdx.x], 0));
+  double total;
+  if (last_block_total(bs, partials, &st->ticket, nitems, total)) {
+    const double r = sqrt(total / denom);
+    st->sumsq = total;
+    st->residual = r;
+    st->converged = (r < tol) ? 1 : 0;
+  }
+}
+
+template <class TW, int D>
+__global__ void __launch_bounds__(BLOCK_THREADS)
+    k_update(const DevPatch* __restrict__ PT, const Item* __restrict__ items) {
+  update_item<TW, D>(PT, items[blockIdx.x]);
 }
 
 }  // namespace bsam

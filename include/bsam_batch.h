@@ -1,0 +1,141 @@
+/*
+ * bsam_batch.h -- many independent Cahn-Hilliard solves on one GPU.
+ *
+ * The reference advances one problem per process (TakeTimeSteps ->
+ * MultigridIterations, lib/bsamroutines.f90:632-762, lib/afasroutines.f90:
+ * 38-106).  A batch holds many such problems ("slots") resident in device
+ * memory at once and advances all of them together: one "tick" is one FAS
+ * V-cycle (AFASVcycle, afas:488-521) of every running problem, issued as one
+ * launch per V-cycle stage across the whole batch, followed by each
+ * problem's own convergence test (ErrorAFAS, afas:94-101) and, when it
+ * converges or reaches maxvcycles, the start of its next time step
+ * (CopyQToQold + GetSourceFunction) -- all decided on the device.  Ticks run
+ * inside one CUDA graph with a device-side WHILE loop.
+ *
+ * Per problem the arithmetic is exactly the single-problem library's
+ * (bsam_gpu.h) in the same precision form, so a problem's result does not
+ * depend on what else is in the batch: results are bitwise identical alone
+ * and in any mix, and bitwise identical to bsam_gpu_multigrid_iterations.
+ *
+ * Continuous batching: problems may be submitted at any time, also while
+ * others are being advanced; a submission is admitted when a slot and its
+ * device footprint (bsam_batch_footprint) are free in the batch's memory pool
+ * and refused with BSAM_ERR_NOMEM otherwise.  Finished problems are read back
+ * and their memory released with bsam_batch_collect.
+ *
+ * No reference counterpart: the reference has no batched or served form.
+ */
+#ifndef BSAM_BATCH_H
+#define BSAM_BATCH_H
+#include <stdint.h>
+#include "bsam_gpu.h"
+#include "bsam_host.h"
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct bsam_batch bsam_batch;
+
+/* Longest time-step record kept per problem. */
+#define BSAM_BATCH_MAX_STEPS 256
+
+/* Slot phases (bsam_batch_poll). */
+#define BSAM_SLOT_IDLE 0
+#define BSAM_SLOT_RUNNING 1
+#define BSAM_SLOT_DONE 2
+#define BSAM_SLOT_FAILED 3 /* non-finite residual */
+
+typedef struct {
+  int32_t ndims;            /* 2 or 3: every problem of the batch */
+  int32_t precision;        /* BSAM_PREC_FP64 or BSAM_PREC_MIXED */
+  int32_t nsmoothingpasses; /* rundata nsmoothingpasses (2) */
+  int32_t maxvcycles;       /* per time step */
+  int32_t max_slots;        /* problems resident at once */
+  int32_t pad_;
+  int64_t pool_bytes;       /* device memory for problem state; 0 = half of free */
+  double qerrortol;
+} bsam_batch_params;
+
+/* One problem: a uniform root grid with its below-root levels (the same
+ * &griddata subset bsam_host_build_uniform takes) and its own constants. */
+typedef struct {
+  bsam_host_grid grid;
+  int32_t nsteps; /* time steps to take, 1..BSAM_BATCH_MAX_STEPS */
+  int32_t pad_;
+  double dt, eps, alpha;
+} bsam_batch_problem;
+
+/* Per time step of a problem, as MultigridIterations reports it. */
+typedef struct {
+  int32_t nvcycles;
+  int32_t converged;
+  double residual;
+} bsam_step_result;
+
+/* Execution choices that leave every result bit unchanged (the autotuner's
+ * knobs): grid_ctas caps the CTAs of each stage launch (0 = 16 per SM). */
+typedef struct {
+  int32_t grid_ctas;
+  int32_t reserved[7];
+} bsam_batch_tuning;
+
+typedef struct {
+  int64_t ticks;          /* V-cycle ticks executed */
+  int64_t launches;       /* kernel launches issued for those ticks */
+  int64_t kernels_per_tick;
+  int64_t captures;       /* tick graph (re)captures */
+  int64_t pool_used;      /* bytes of the pool held by resident problems */
+  int64_t pool_bytes;
+  int32_t resident;       /* slots holding a problem */
+  int32_t running;
+} bsam_batch_stats;
+
+int bsam_batch_create(bsam_batch** b, int device, const bsam_batch_params* p);
+int bsam_batch_destroy(bsam_batch* b);
+int bsam_batch_set_tuning(bsam_batch* b, const bsam_batch_tuning* t);
+
+/* Device bytes the problem occupies while resident (its admission size). */
+int bsam_batch_footprint(bsam_batch* b, const bsam_batch_problem* prob, int64_t* bytes);
+
+/* Admits a problem with initial root state q0 (Fortran layout
+ * q(0:mx+1, 0:my+1[, 0:mz+1], 2), ghost values are replaced by SetBC).  The
+ * copy is queued behind the work already issued; q0 may be reused on return.
+ * *slot receives the problem's slot.  BSAM_ERR_NOMEM: no free slot or not
+ * enough pool memory now (retry after a collect). */
+int bsam_batch_submit(bsam_batch* b, const bsam_batch_problem* prob, const double* q0,
+                      int* slot);
+
+/* Queues up to max_ticks V-cycle ticks (fewer if every problem finishes);
+ * returns without waiting. */
+int bsam_batch_advance(bsam_batch* b, int max_ticks);
+
+/* Waits for all queued work. */
+int bsam_batch_sync(bsam_batch* b);
+
+/* Advances until no problem is running (waits). */
+int bsam_batch_run(bsam_batch* b);
+
+/* Slots whose problems have finished (DONE or FAILED) and are not yet
+ * collected, as seen by the work completed so far (does not wait).  Returns
+ * their number; up to maxn are written to slots. */
+int bsam_batch_poll(bsam_batch* b, int* slots, int maxn);
+
+/* Phase of a slot as seen by the work completed so far (BSAM_SLOT_*), and
+ * the number of time steps it has completed. */
+int bsam_batch_slot_phase(bsam_batch* b, int slot, int* phase, int* steps_done);
+
+/* Reads back a finished problem and releases its slot and memory (waits for
+ * queued work).  Optional outputs (NULL to skip): root q with ghost ring,
+ * one bsam_step_result per time step (nsteps entries), FP64 mass of phi
+ * (AfterStep's integral(1)). */
+int bsam_batch_collect(bsam_batch* b, int slot, double* q, bsam_step_result* steps,
+                       double* mass);
+
+int bsam_batch_get_stream(bsam_batch* b, void** stream);
+int bsam_batch_get_stats(bsam_batch* b, bsam_batch_stats* s);
+const char* bsam_batch_last_error(bsam_batch* b);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -42,14 +42,18 @@ class StepResult(ctypes.Structure):
 
 
 class BatchTuning(ctypes.Structure):
-    _fields_ = [("grid_ctas", ctypes.c_int32), ("reserved", ctypes.c_int32 * 7)]
+    _fields_ = [("grid_ctas", ctypes.c_int32), ("eager", ctypes.c_int32),
+                ("per_pass", ctypes.c_int32), ("fused_ctas", ctypes.c_int32),
+                ("reserved", ctypes.c_int32 * 4)]
 
 
 class BatchStats(ctypes.Structure):
     _fields_ = [("ticks", ctypes.c_int64), ("launches", ctypes.c_int64),
                 ("kernels_per_tick", ctypes.c_int64), ("captures", ctypes.c_int64),
                 ("pool_used", ctypes.c_int64), ("pool_bytes", ctypes.c_int64),
-                ("resident", ctypes.c_int32), ("running", ctypes.c_int32)]
+                ("resident", ctypes.c_int32), ("running", ctypes.c_int32),
+                ("smooth_stages", ctypes.c_int64), ("smooth_ms", ctypes.c_double),
+                ("smooth_bytes", ctypes.c_double)]
 
 
 def bind(L):
@@ -73,6 +77,7 @@ def bind(L):
     L.bsam_batch_poll.argtypes = [vp, ip, ctypes.c_int]
     L.bsam_batch_slot_phase.argtypes = [vp, ctypes.c_int, ip, ip]
     L.bsam_batch_collect.argtypes = [vp, ctypes.c_int, dp, ctypes.POINTER(StepResult), dp]
+    L.bsam_batch_profile.argtypes = [vp, ctypes.c_int]
     L.bsam_batch_get_stream.argtypes = [vp, ctypes.POINTER(vp)]
     L.bsam_batch_get_stats.argtypes = [vp, ctypes.POINTER(BatchStats)]
     L.bsam_batch_last_error.argtypes = [vp]
@@ -129,9 +134,14 @@ class Batch:
         if grid_ctas:
             self.set_tuning(grid_ctas=grid_ctas)
 
-    def set_tuning(self, grid_ctas: int = 0):
-        t = BatchTuning(grid_ctas=grid_ctas)
+    def set_tuning(self, grid_ctas: int = 0, eager: int = 0, per_pass: int = 0,
+                   fused_ctas: int = 0):
+        t = BatchTuning(grid_ctas=grid_ctas, eager=eager, per_pass=per_pass,
+                        fused_ctas=fused_ctas)
         _check(_lib().bsam_batch_set_tuning(self.h, ctypes.byref(t)), self.h, "set_tuning")
+
+    def profile(self, enable: bool = True):
+        _check(_lib().bsam_batch_profile(self.h, int(enable)), self.h, "profile")
 
     def footprint(self, prob) -> int:
         n = ctypes.c_int64(0)
@@ -224,7 +234,8 @@ class Batch:
 
 
 def solve_all(problems, precision: int = PREC_MIXED, max_slots: int | None = None,
-              pool_bytes: int = 0, device: int = 0, grid_ctas: int = 0):
+              pool_bytes: int = 0, device: int = 0, grid_ctas: int = 0, eager: int = 0,
+              per_pass: int = 0, fused_ctas: int = 0):
     """Solves every problem (one dimensionality) in one batch; admits more as
     slots free up.  Returns the collect() results in input order."""
     if not problems:
@@ -233,7 +244,10 @@ def solve_all(problems, precision: int = PREC_MIXED, max_slots: int | None = Non
     ms = max_slots or len(problems)
     tol = problems[0].qerrortol
     with Batch(nd, precision=precision, max_slots=ms, pool_bytes=pool_bytes, qerrortol=tol,
-               maxvcycles=problems[0].maxvcycles, device=device, grid_ctas=grid_ctas) as b:
+               maxvcycles=problems[0].maxvcycles, device=device) as b:
+        if grid_ctas or eager or per_pass or fused_ctas:
+            b.set_tuning(grid_ctas=grid_ctas, eager=eager, per_pass=per_pass,
+                         fused_ctas=fused_ctas)
         out = [None] * len(problems)
         pending = list(range(len(problems)))
         slot_of = {}

@@ -49,6 +49,8 @@ struct SlotOut {
 struct BatchCtl {
   int32_t ticks_left;  // ticks this graph launch may still run
   int32_t running;     // slots still running after this tick's control pass
+  int32_t kerr;        // nonzero: a fused stage's copy wait gave up (fused2.cuh)
+  int32_t pad_;
   int64_t ticks;       // ticks executed since creation
 };
 
@@ -225,14 +227,15 @@ __global__ void __launch_bounds__(BLOCK_THREADS)
 }
 
 // WHILE condition of the tick graph: another tick while some slot runs and
-// the launch's tick budget lasts.
-__global__ void k_batch_cond(BatchCtl* __restrict__ ctl, cudaGraphConditionalHandle handle) {
+// the launch's tick budget lasts.  in_graph = 0: eager ticks (counters only).
+__global__ void k_batch_cond(BatchCtl* __restrict__ ctl, cudaGraphConditionalHandle handle,
+                             int in_graph) {
   ctl->ticks += 1;
   const int left = ctl->ticks_left - 1;
   ctl->ticks_left = left;
-  const bool again = ctl->running > 0 && left > 0;
+  const bool again = ctl->running > 0 && left > 0 && ctl->kerr == 0;
   ctl->running = 0;
-  cudaGraphSetConditional(handle, again ? 1u : 0u);
+  if (in_graph) cudaGraphSetConditional(handle, again ? 1u : 0u);
 }
 
 __global__ void k_batch_budget(BatchCtl* __restrict__ ctl, int ticks) {

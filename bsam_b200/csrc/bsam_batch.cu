@@ -21,6 +21,8 @@
 // levels have more than BOTTOM_MAX_CELLS cells run grid kernels ("top"
 // depths); the rest run inside k_bottom's chain, as in the single-problem
 // engine, and are FP64 in both forms.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -34,16 +36,29 @@
 #include "../../include/bsam_batch.h"
 #include "batch.cuh"
 #include "bsam_types.h"
+#include "fused2.cuh"
 
 using namespace bsam;
 
 namespace {
 
 constexpr int RMAX = 16;  // records per slot
+constexpr int NMAPS = 7;  // TMA maps per fused record
 constexpr int MAXD = 8;   // top depths
 // Mixed form: levels at or below this size stay FP64 (as in bsam_gpu.cu).
 constexpr int64_t FP64_CELLS = 4096;
-enum { L_MASTER = 0, L_TOPS = 1, L_FINE = 2, L_COARSE = 2 + MAXD, NLIST = 2 + 2 * MAXD };
+// Lists: master tiles; bottom-chain tops; per top depth d: tiles of every
+// record (correction), footprint tiles (restriction / coarse load), tiles of
+// records smoothed per colour pass, fused-stage tiles.
+enum {
+  L_MASTER = 0,
+  L_TOPS = 1,
+  L_FINE = 2,
+  L_COARSE = 2 + MAXD,
+  L_RELAX = 2 + 2 * MAXD,
+  L_FUSED = 2 + 3 * MAXD,
+  NLIST = 2 + 4 * MAXD
+};
 
 struct List {
   Item* d = nullptr;
@@ -60,6 +75,7 @@ struct SlotPlan {
   int64_t cells = 0;
   bsam_batch_problem prob{};
   std::vector<DevPatch> recs;  // absolute record indices
+  std::vector<CUtensorMap> maps;  // NMAPS per record (fused records only encoded)
 };
 
 struct StageChunk {
@@ -99,6 +115,7 @@ struct bsam_batch {
   std::map<size_t, size_t> free_;  // offset -> size, coalesced
   // records, slots
   DevPatch* d_pt = nullptr;
+  CUtensorMap* d_tmaps = nullptr;  // NMAPS per record: fused stages' TMA maps
   std::vector<SlotPlan> slots;
   SlotCfg* d_cfg = nullptr;
   std::vector<SlotCfg> h_cfg;
@@ -121,6 +138,10 @@ struct bsam_batch {
   bool need_capture = true;
   int64_t kernels_per_tick = 0;
   bsam_batch_stats st{};
+  // profiling (eager ticks): events around the finest-depth smoothing stages
+  bool profiling = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pool;
+  size_t ev_used = 0;
   // pinned staging ring for host -> device copies
   char* stage = nullptr;
   size_t stage_bytes = 0, stage_head = 0;
@@ -262,6 +283,41 @@ int face_rule(int nd, int face, int code, int* rule) {
   return 0;
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// dependency on libcuda).
+PFN_cuTensorMapEncodeTiled_v12000 map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+// 2D map of one field of a 2D record: rows of sy elements from the
+// allocation start (lead elements before element (0,0)), n1 + 2 rows, box of
+// the fused stage's shared tile (RX x RY).
+bool encode_map2d(CUtensorMap* m, const DevPatch& P, const void* field) {
+  auto enc = map_encoder();
+  if (!enc) return false;
+  const bool f32 = P.prec == PREC_F32;
+  const int es = f32 ? 4 : 8;
+  const int64_t lead = 128 / es - 1;
+  void* base = (char*)field - lead * es;
+  const cuuint64_t dims[2] = {(cuuint64_t)P.sy, (cuuint64_t)(P.n[1] + 2)};
+  const cuuint64_t strides[1] = {(cuuint64_t)(P.sy * es)};
+  const cuuint32_t box[2] = {(cuuint32_t)(f32 ? Fused2<float>::RX : Fused2<double>::RX),
+                             (cuuint32_t)(f32 ? Fused2<float>::RY : Fused2<double>::RY)};
+  const cuuint32_t estr[2] = {1, 1};
+  return enc(m, f32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, base,
+             dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 // Builds the slot's records (absolute indices from rec0; field pointers
 // relative to a pool region starting at `base`).  base == nullptr: size only.
 int plan_slot(bsam_batch* b, const bsam_batch_problem* pr, int rec0, char* base, SlotPlan& S) {
@@ -289,6 +345,7 @@ int plan_slot(bsam_batch* b, const bsam_batch_problem* pr, int rec0, char* base,
   if (np - ntop > BOTTOM_MAX_DEPTH) return fail(b, BSAM_ERR_UNSUPPORTED, "bottom chain too deep");
   auto rec_of = [&](int l) { return mixed ? (l == 0 ? 1 : l + 1) : l; };  // V-cycle record
   S.recs.assign(nrec, DevPatch{});
+  S.maps.clear();
   S.nrec = nrec;
   S.ntop = ntop;
   S.master = 0;
@@ -335,7 +392,12 @@ int plan_slot(bsam_batch* b, const bsam_batch_problem* pr, int rec0, char* base,
     if (P.delta)
       for (int f = 0; f < 2 * nd; ++f)
         if (P.bc[f] == BC_REFLECT) P.bc[f] = BC_NEGATE;
-    P.fused = 0;
+    // Fused shared-memory stages: 2D levels above the bottom, 2*nu <= 4.
+    const int depth = mixed ? r - 1 : r;
+    P.fused = (!b->tuning.per_pass && nd == 2 && !is_master_only && depth < ntop &&
+               b->bp.nsmoothingpasses <= 2)
+                  ? 1
+                  : 0;
     P.zchunk = 1;
     const int es = P.prec == PREC_F32 ? 4 : 8;
     const int64_t A = 128 / es, lead = A - 1;
@@ -346,7 +408,7 @@ int plan_slot(bsam_batch* b, const bsam_batch_problem* pr, int rec0, char* base,
     // Every V-cycle record below the root is the parent of the next finer
     // one and keeps the snapshot qs of its restricted state.
     const bool is_parent = !is_master_only && l >= 1;
-    const int nfield = 4 + (is_parent ? 2 : 0) + (P.delta ? 1 : 0);
+    const int nfield = 4 + (is_parent ? 2 : 0) + (P.delta ? 1 : 0) + (P.fused ? 2 : 0);
     if (base) {
       char* rb = base + total;
       int slotn = 0;
@@ -363,7 +425,21 @@ int plan_slot(bsam_batch* b, const bsam_batch_problem* pr, int rec0, char* base,
       }
       P.qb[0] = P.qb[1] = nullptr;
       P.bs = P.delta ? next() : nullptr;
+      if (P.fused) {
+        P.qb[0] = next();
+        P.qb[1] = next();
+      }
       P.tmaps = nullptr;
+      if (P.fused) {
+        // TMA maps of q0, q1, qb0, qb1, f0, f1, bs for the fused stage.
+        if (S.maps.size() < (size_t)nrec * NMAPS) S.maps.assign((size_t)nrec * NMAPS, CUtensorMap{});
+        const void* fields[NMAPS] = {P.q[0], P.q[1], P.qb[0], P.qb[1],
+                                     P.f[0], P.f[1], P.bs ? P.bs : P.q[0]};
+        for (int m = 0; m < NMAPS; ++m)
+          if (!encode_map2d(&S.maps[(size_t)r * NMAPS + m], P, fields[m]))
+            return fail(b, BSAM_ERR_CUDA, "cuTensorMapEncodeTiled rejected a field map");
+        P.tmaps = b->d_tmaps + (size_t)(rec0 + r) * NMAPS;
+      }
     }
     total += (size_t)fe * nfield * es;
     P.h = d.dx;
@@ -397,8 +473,18 @@ void append_items(bsam_batch* b, int s) {
   const int first = b->mixed ? 1 : 0;  // record of depth 0
   for (int d = 0; d < S.ntop; ++d) {
     const int r = first + d;
-    tiles_for(rec0 + r, S.recs[r].n, nd, b->lists[L_FINE + d].h);
-    tiles_for(rec0 + r, S.recs[r].cn, nd, b->lists[L_COARSE + d].h);
+    const DevPatch& P = S.recs[r];
+    tiles_for(rec0 + r, P.n, nd, b->lists[L_FINE + d].h);
+    tiles_for(rec0 + r, P.cn, nd, b->lists[L_COARSE + d].h);
+    if (!P.fused) {
+      tiles_for(rec0 + r, P.n, nd, b->lists[L_RELAX + d].h);
+    } else {
+      const int tx = P.prec == PREC_F32 ? Fused2<float>::TX : Fused2<double>::TX;
+      const int ty = P.prec == PREC_F32 ? Fused2<float>::TY : Fused2<double>::TY;
+      for (int y = 0; y < (P.n[1] + ty - 1) / ty; ++y)
+        for (int x = 0; x < (P.n[0] + tx - 1) / tx; ++x)
+          b->lists[L_FUSED + d].h.push_back(Item{rec0 + r, x, y, 0});
+    }
   }
   b->cfg_dirty = true;
 }
@@ -424,8 +510,25 @@ int grid_for(bsam_batch* b, int l) {
   return std::max(1, std::min(cap, lim));
 }
 
+void stage_mark(bsam_batch* b, int d, bool begin) {
+  if (!b->profiling || d != 0) return;
+  if (begin) {
+    if (b->ev_used == b->ev_pool.size()) {
+      cudaEvent_t x, y;
+      cudaEventCreate(&x);
+      cudaEventCreate(&y);
+      b->ev_pool.push_back({x, y});
+    }
+    cudaEventRecord(b->ev_pool[b->ev_used].first, b->stream);
+  } else {
+    cudaEventRecord(b->ev_pool[b->ev_used].second, b->stream);
+    ++b->ev_used;
+  }
+}
+
+// Issues one tick.  in_graph: captured into the WHILE body (handle valid).
 template <int D>
-void tick_t(bsam_batch* b, cudaGraphConditionalHandle handle) {
+void tick_t(bsam_batch* b, cudaGraphConditionalHandle handle, int in_graph) {
   const dim3 blk(32, TILE_Y, 1);
   cudaStream_t s = b->stream;
   const int nu = b->bp.nsmoothingpasses;
@@ -433,17 +536,32 @@ void tick_t(bsam_batch* b, cudaGraphConditionalHandle handle) {
   const int* cnt = b->d_counts;
   const List* L = b->lists;
   int64_t n = 0;
-  auto relax = [&](int d) {
-    for (int pass = 0; pass < nu; ++pass)
-      for (int color = 0; color < 2; ++color) {
-        if (b->mixed)
-          kb_relax<float, D><<<grid_for(b, L_FINE + d), blk, 0, s>>>(pt, L[L_FINE + d].d,
-                                                                    cnt + L_FINE + d, color);
-        else
-          kb_relax<double, D><<<grid_for(b, L_FINE + d), blk, 0, s>>>(pt, L[L_FINE + d].d,
-                                                                     cnt + L_FINE + d, color);
-        ++n;
-      }
+  // LevelRelax of depth d for every running problem; dir selects the fused
+  // stage's buffers (0: q -> qb before the correction, 1: qb -> q after).
+  auto relax = [&](int d, int dir) {
+    stage_mark(b, d, true);
+    if (L[L_RELAX + d].cap > 0)
+      for (int pass = 0; pass < nu; ++pass)
+        for (int color = 0; color < 2; ++color) {
+          const int g = grid_for(b, L_RELAX + d);
+          if (b->mixed)
+            kb_relax<float, D><<<g, blk, 0, s>>>(pt, L[L_RELAX + d].d, cnt + L_RELAX + d, color);
+          else
+            kb_relax<double, D><<<g, blk, 0, s>>>(pt, L[L_RELAX + d].d, cnt + L_RELAX + d, color);
+          ++n;
+        }
+    if (D == 2 && L[L_FUSED + d].cap > 0) {
+      const int lim = b->tuning.fused_ctas > 0 ? b->tuning.fused_ctas : 4 * b->nsm;
+      const int g = std::max(1, std::min(L[L_FUSED + d].cap, lim));
+      if (b->mixed)
+        kb_smooth2<float><<<g, Fused2<float>::THREADS, Fused2<float>::SMEM, s>>>(
+            pt, L[L_FUSED + d].d, cnt + L_FUSED + d, dir, nu, &b->d_ctl->kerr);
+      else
+        kb_smooth2<double><<<g, Fused2<double>::THREADS, Fused2<double>::SMEM, s>>>(
+            pt, L[L_FUSED + d].d, cnt + L_FUSED + d, dir, nu, &b->d_ctl->kerr);
+      ++n;
+    }
+    stage_mark(b, d, false);
   };
   const int gm = grid_for(b, L_MASTER);
   kb_source<D><<<gm, blk, 0, s>>>(pt, L[L_MASTER].d, cnt + L_MASTER);
@@ -453,7 +571,7 @@ void tick_t(bsam_batch* b, cudaGraphConditionalHandle handle) {
     ++n;
   }
   for (int d = 0; d < b->cap_depth; ++d) {
-    relax(d);
+    relax(d, 0);
     const int gc = grid_for(b, L_COARSE + d);
     if (b->mixed) {
       kb_restrict<float, D><<<gc, blk, 0, s>>>(pt, L[L_COARSE + d].d, cnt + L_COARSE + d);
@@ -475,7 +593,7 @@ void tick_t(bsam_batch* b, cudaGraphConditionalHandle handle) {
     if (b->mixed) kb_correct<float, D><<<gf, blk, 0, s>>>(pt, L[L_FINE + d].d, cnt + L_FINE + d);
     else kb_correct<double, D><<<gf, blk, 0, s>>>(pt, L[L_FINE + d].d, cnt + L_FINE + d);
     ++n;
-    relax(d);
+    relax(d, 1);
   }
   if (b->mixed) {
     kb_update<D><<<gm, blk, 0, s>>>(pt, L[L_MASTER].d, cnt + L_MASTER);
@@ -489,7 +607,7 @@ void tick_t(bsam_batch* b, cudaGraphConditionalHandle handle) {
   k_batch_control<<<gctl, BLOCK_THREADS, 0, s>>>(pt, b->d_cfg, b->d_state, b->d_log,
                                                  BSAM_BATCH_MAX_STEPS, b->d_out, b->d_partials,
                                                  b->d_ctl, b->bp.max_slots);
-  k_batch_cond<<<1, 1, 0, s>>>(b->d_ctl, handle);
+  k_batch_cond<<<1, 1, 0, s>>>(b->d_ctl, handle, in_graph);
   n += 2;
   b->kernels_per_tick = n;
 }
@@ -516,8 +634,11 @@ int capture(bsam_batch* b) {
     e = cudaStreamBeginCaptureToGraph(b->stream, body, nullptr, nullptr, 0,
                                       cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
-      if (b->bp.ndims == 2) tick_t<2>(b, handle);
-      else tick_t<3>(b, handle);
+      const bool prof = b->profiling;
+      b->profiling = false;  // no events inside the graph
+      if (b->bp.ndims == 2) tick_t<2>(b, handle, 1);
+      else tick_t<3>(b, handle, 1);
+      b->profiling = prof;
       cudaGraph_t captured = nullptr;
       e = cudaStreamEndCapture(b->stream, &captured);
     }
@@ -626,6 +747,7 @@ int bsam_batch_create(bsam_batch** out, int device, const bsam_batch_params* p) 
   bool ok = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) == cudaSuccess &&
             cudaMalloc(&b->d_pool, pool) == cudaSuccess &&
             cudaMalloc(&b->d_pt, sizeof(DevPatch) * ns * RMAX) == cudaSuccess &&
+            cudaMalloc(&b->d_tmaps, sizeof(CUtensorMap) * NMAPS * ns * RMAX) == cudaSuccess &&
             cudaMalloc(&b->d_cfg, sizeof(SlotCfg) * ns) == cudaSuccess &&
             cudaMalloc(&b->d_state, sizeof(SlotState) * ns) == cudaSuccess &&
             cudaMalloc(&b->d_log, sizeof(StepLog) * ns * BSAM_BATCH_MAX_STEPS) == cudaSuccess &&
@@ -635,6 +757,11 @@ int bsam_batch_create(bsam_batch** out, int device, const bsam_batch_params* p) 
             cudaMallocHost(&b->h_status, sizeof(DevStatus)) == cudaSuccess &&
             cudaMalloc(&b->d_counts, sizeof(int) * NLIST) == cudaSuccess;
   if (ok) ok = cudaHostGetDevicePointer((void**)&b->d_out, b->h_out, 0) == cudaSuccess;
+  if (ok)
+    ok = cudaFuncSetAttribute(kb_smooth2<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)Fused2<float>::SMEM) == cudaSuccess &&
+         cudaFuncSetAttribute(kb_smooth2<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)Fused2<double>::SMEM) == cudaSuccess;
   if (!ok) {
     cudaGetLastError();
     bsam_batch_destroy(b);
@@ -665,6 +792,10 @@ int bsam_batch_destroy(bsam_batch* b) {
   cudaSetDevice(b->device);
   if (b->stream) cudaStreamSynchronize(b->stream);
   if (b->exec) cudaGraphExecDestroy(b->exec);
+  for (auto& e : b->ev_pool) {
+    cudaEventDestroy(e.first);
+    cudaEventDestroy(e.second);
+  }
   for (auto& L : b->lists)
     if (L.d) cudaFree(L.d);
   for (auto& c : b->chunks)
@@ -684,6 +815,7 @@ int bsam_batch_destroy(bsam_batch* b) {
   if (b->d_state) cudaFree(b->d_state);
   if (b->d_cfg) cudaFree(b->d_cfg);
   if (b->d_pt) cudaFree(b->d_pt);
+  if (b->d_tmaps) cudaFree(b->d_tmaps);
   if (b->d_pool) cudaFree(b->d_pool);
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
@@ -691,7 +823,9 @@ int bsam_batch_destroy(bsam_batch* b) {
 }
 
 int bsam_batch_set_tuning(bsam_batch* b, const bsam_batch_tuning* t) {
-  if (!b || !t || t->grid_ctas < 0) return BSAM_ERR_ARG;
+  if (!b || !t || t->grid_ctas < 0 || t->eager < 0 || t->eager > 1 || t->per_pass < 0 ||
+      t->per_pass > 1 || t->fused_ctas < 0)
+    return BSAM_ERR_ARG;
   b->tuning = *t;
   b->need_capture = true;
   return BSAM_OK;
@@ -751,6 +885,12 @@ int bsam_batch_submit(bsam_batch* b, const bsam_batch_problem* prob, const doubl
   CU(cudaMemsetAsync(b->d_pool + off, 0, S.bytes, b->stream));
   rc = stage_copy(b, b->d_pt + rec0, S.recs.data(), sizeof(DevPatch) * S.nrec);
   if (rc) return rc;
+  for (int r = 0; r < S.nrec; ++r)
+    if (S.recs[r].fused) {
+      rc = stage_copy(b, b->d_tmaps + (size_t)(rec0 + r) * NMAPS, &S.maps[(size_t)r * NMAPS],
+                      sizeof(CUtensorMap) * NMAPS);
+      if (rc) return rc;
+    }
   const DevPatch& M = S.recs[S.master];
   const int e0 = M.n[0] + 2, e1 = M.n[1] + 2, e2 = nd == 3 ? M.n[2] + 2 : 1;
   const size_t hcomp = (size_t)e0 * e1 * e2;
@@ -794,8 +934,51 @@ int bsam_batch_advance(bsam_batch* b, int max_ticks) {
   if (rc) return rc;
   k_batch_budget<<<1, 1, 0, b->stream>>>(b->d_ctl, max_ticks);
   CU(cudaGetLastError());
-  CU(cudaGraphLaunch(b->exec, b->stream));
-  b->st.launches += 1;
+  if (!b->tuning.eager && !b->profiling) {
+    CU(cudaGraphLaunch(b->exec, b->stream));
+    return BSAM_OK;
+  }
+  // Eager ticks: exactly max_ticks; with profiling, one tick at a time so
+  // that each timed stage is attributed to the problems running in it.
+  const cudaGraphConditionalHandle none = 0;
+  for (int t = 0; t < max_ticks; ++t) {
+    int64_t cells0 = 0;
+    int es = b->mixed ? 4 : 8;
+    if (b->profiling) {
+      CU(cudaStreamSynchronize(b->stream));
+      for (size_t s = 0; s < b->slots.size(); ++s)
+        if (b->slots[s].used && ((volatile SlotOut*)b->h_out)[s].phase == SLOT_RUNNING &&
+            b->slots[s].ntop > 0)
+          cells0 += b->slots[s].cells;
+    }
+    b->ev_used = 0;
+    if (b->bp.ndims == 2) tick_t<2>(b, none, 0);
+    else tick_t<3>(b, none, 0);
+    CU(cudaGetLastError());
+    if (b->profiling) {
+      CU(cudaStreamSynchronize(b->stream));
+      for (size_t e = 0; e < b->ev_used; ++e) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, b->ev_pool[e].first, b->ev_pool[e].second) == cudaSuccess) {
+          b->st.smooth_ms += ms;
+          b->st.smooth_stages += 1;
+          b->st.smooth_bytes += 6.0 * es * (double)cells0;
+        }
+      }
+      b->ev_used = 0;
+    }
+  }
+  return BSAM_OK;
+}
+
+int bsam_batch_profile(bsam_batch* b, int enable) {
+  if (!b) return BSAM_ERR_ARG;
+  if (enable) {
+    b->st.smooth_ms = 0.0;
+    b->st.smooth_stages = 0;
+    b->st.smooth_bytes = 0.0;
+  }
+  b->profiling = enable != 0;
   return BSAM_OK;
 }
 
@@ -803,6 +986,9 @@ int bsam_batch_sync(bsam_batch* b) {
   if (!b) return BSAM_ERR_ARG;
   CU(cudaSetDevice(b->device));
   CU(cudaStreamSynchronize(b->stream));
+  int32_t kerr = 0;
+  CU(cudaMemcpy(&kerr, &b->d_ctl->kerr, sizeof(kerr), cudaMemcpyDeviceToHost));
+  if (kerr) return fail(b, BSAM_ERR_CUDA, "a fused smoothing stage timed out waiting for its copies");
   return BSAM_OK;
 }
 

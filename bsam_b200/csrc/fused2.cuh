@@ -1,0 +1,194 @@
+// fused2.cuh -- a whole 2D smoothing stage per shared-memory tile.
+//
+// LevelRelax (afas:523-547) makes 2*nu colour passes over a level, each
+// followed by SetGhost.  Done as one launch per pass, every pass streams the
+// level's q, f (and the correction form's base) through HBM again.  Here one
+// CTA brings a TX x TY tile of the level with a halo of H = 4 cells into
+// shared memory (one TMA tensor copy per field), runs all 2*nu <= 4 passes
+// there -- pass p on the tile grown by 2*nu-1-p cells, so that every cell it
+// reads from pass p-1 is exact -- and writes the tile's interior back once:
+// HBM traffic per stage is about one read of (phi, mu, f1, f2[, base]) and
+// one write of (phi, mu), plus the halo.
+//
+// Every cell update is the same per-cell code in the same order of passes as
+// RelaxGrid2D; cells in a tile's halo are recomputed redundantly from the
+// same inputs, so the result is bit-identical to the per-pass kernels.
+// Physical ghosts inside the tile are refreshed after each update exactly as
+// the per-pass write-through does (in a 5-point pass a face ghost is read only
+// by its own mirror cell, the one that writes it).  The stage reads one state
+// buffer and writes the other (q -> qb before the coarse-grid correction,
+// qb -> q after it), so no tile reads a neighbour's already-smoothed cells.
+//
+// Thread layout: warp w takes rows w, w + 8, ...; lane l the cell pair
+// (2l, 2l+1) of a row, of which it updates the one of the pass's colour.
+// TX = 56 keeps the widest pass (TX + 6 cells) within 31 pairs.
+#pragma once
+#include "kernels.cuh"
+#include "smooth_fused.cuh"
+
+namespace bsam {
+
+template <class T>
+struct Fused2 {
+  static constexpr int TX = 56;
+  static constexpr int TY = sizeof(T) == 4 ? 32 : 16;
+  static constexpr int H = 4;  // halo: supports 2*nu <= 4 passes
+  static constexpr int RX = TX + 2 * H;  // 64: 256 / 512-byte shared rows
+  static constexpr int RY = TY + 2 * H;
+  static constexpr int PLANE = RX * RY;
+  static constexpr int NF = 5;  // phi, mu, f1, f2, base
+  static constexpr int THREADS = 256;
+  static constexpr int WARPS = THREADS / 32;
+  static constexpr size_t SMEM = sizeof(T) * NF * PLANE;
+  static_assert((sizeof(T) * PLANE) % 128 == 0, "field planes stay 128-byte aligned");
+};
+
+// Tiled 2D tensor copy global -> shared (no multicast).  x * sizeof(T) is a
+// multiple of 16 bytes at every call site: x = tile origin (a multiple of 56
+// cells) - 3 + lead, with lead = 31 (FP32) or 15 (FP64).
+__device__ __forceinline__ void tma_load_2d(void* dst, const void* tmap, int x, int y,
+                                            uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, "
+      "{%2, %3}], [%4];" ::"r"(smem_u32(dst)),
+      "l"(tmap), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// Ghost images of the updated cell (i,j) inside the shared tile: the face
+// maps of SetBC2D (boundary.f90:661-738), as write_through applies them.
+template <class T>
+__device__ __forceinline__ void smem_ghosts2(const DevPatch& P, T* s0, T* s1, int si, int i,
+                                             int j, T v0, T v1) {
+  constexpr int RX = Fused2<T>::RX;
+  if (i == 1 && P.bc[0] != BC_NONE) {
+    s0[si - 1] = bc_map<T>(P.bc[0], v0);
+    s1[si - 1] = bc_map<T>(P.bc[0], v1);
+  }
+  if (i == P.n[0] && P.bc[1] != BC_NONE) {
+    s0[si + 1] = bc_map<T>(P.bc[1], v0);
+    s1[si + 1] = bc_map<T>(P.bc[1], v1);
+  }
+  if (j == 1 && P.bc[2] != BC_NONE) {
+    s0[si - RX] = bc_map<T>(P.bc[2], v0);
+    s1[si - RX] = bc_map<T>(P.bc[2], v1);
+  }
+  if (j == P.n[1] && P.bc[3] != BC_NONE) {
+    s0[si + RX] = bc_map<T>(P.bc[3], v0);
+    s1[si + RX] = bc_map<T>(P.bc[3], v1);
+  }
+}
+
+// dir 0: q -> qb (pre-smoothing); dir 1: qb -> q (post-smoothing).
+// P.tmaps: 2D maps of q0, q1, qb0, qb1, f0, f1, bs (box RX x RY).
+// A copy that has not landed after kWaitPolls polls sets *err and ends the
+// launch for this CTA.
+template <class T>
+__global__ void __launch_bounds__(Fused2<T>::THREADS)
+    kb_smooth2(const DevPatch* __restrict__ PT, const Item* __restrict__ items,
+               const int* __restrict__ count, int dir, int nu, int* __restrict__ err) {
+  using F = Fused2<T>;
+  extern __shared__ __align__(1024) unsigned char smem2_raw[];
+  __shared__ __align__(8) uint64_t bar;
+  T* s0 = reinterpret_cast<T*>(smem2_raw);
+  T* s1 = s0 + F::PLANE;
+  T* sf0 = s1 + F::PLANE;
+  T* sf1 = sf0 + F::PLANE;
+  T* sbs = sf1 + F::PLANE;
+  const int n = *count;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int npass = 2 * nu;
+  if (tid == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  uint32_t phase = 0;
+  for (int b = blockIdx.x; b < n; b += gridDim.x) {
+    const Item it = items[b];
+    const DevPatch P = PT[it.patch];
+    if (!P.active) continue;  // uniform per CTA
+    const int gx0 = it.tx * F::TX + 1 - F::H;  // global i of shared column 0
+    const int gy0 = it.ty * F::TY + 1 - F::H;  // global j of shared row 0
+    const int lead = 128 / (int)sizeof(T) - 1;
+    if (tid == 0) {
+      const CUtensorMapOpaque* maps = static_cast<const CUtensorMapOpaque*>(P.tmaps);
+      const int m0 = dir == 0 ? 0 : 2;
+      const uint32_t plane = (uint32_t)(sizeof(T) * F::PLANE);
+      fence_proxy_async_smem();  // earlier generic accesses to the tile come first
+      mbar_arrive_expect_tx(&bar, plane * (P.delta ? 5u : 4u));
+      const int x = gx0 + lead;  // column of element (gx0, *) from the allocation start
+      tma_load_2d(s0, &maps[m0], x, gy0, &bar);
+      tma_load_2d(s1, &maps[m0 + 1], x, gy0, &bar);
+      tma_load_2d(sf0, &maps[4], x, gy0, &bar);
+      tma_load_2d(sf1, &maps[5], x, gy0, &bar);
+      if (P.delta) tma_load_2d(sbs, &maps[6], x, gy0, &bar);
+    }
+    const bool ok = __syncthreads_and(mbar_wait_bounded(&bar, phase, kWaitPolls));
+    phase ^= 1u;
+    if (!ok) {
+      if (tid == 0) atomicExch(err, kErrTmaTimeout);
+      break;
+    }
+    T* o0 = fld<T>(dir == 0 ? P.qb[0] : P.q[0]);
+    T* o1 = fld<T>(dir == 0 ? P.qb[1] : P.q[1]);
+    const int n0 = P.n[0], n1 = P.n[1];
+    const T tmp1 = T(P.tmp1), tmp2 = T(P.tmp2), tmp3 = T(P.tmp3), alpha = T(P.alpha);
+    for (int p = 0; p < npass; ++p) {
+      const int color = p & 1;
+      const int grow = npass - 1 - p;
+      // Region of this pass in shared coordinates, clipped to the interior.
+      const int xa = max(F::H - grow, 1 - gx0), xb = min(F::H + F::TX + grow, n0 + 1 - gx0);
+      const int ya = max(F::H - grow, 1 - gy0), yb = min(F::H + F::TY + grow, n1 + 1 - gy0);
+      for (int sy = ya + warp; sy < yb; sy += F::WARPS) {
+        const int j = gy0 + sy;
+        int sx = xa + 2 * lane;
+        int i = gx0 + sx;
+        if ((i + j + color) & 1) {
+          ++sx;
+          ++i;
+        }
+        if (sx >= xb) continue;
+        const int si = sy * F::RX + sx;
+        problem::Stencil<T, 2> st;
+        st.pc = s0[si];
+        st.mc = s1[si];
+        st.pm[0] = s0[si - 1];
+        st.pp[0] = s0[si + 1];
+        st.mm[0] = s1[si - 1];
+        st.mp[0] = s1[si + 1];
+        st.pm[1] = s0[si - F::RX];
+        st.pp[1] = s0[si + F::RX];
+        st.mm[1] = s1[si - F::RX];
+        st.mp[1] = s1[si + F::RX];
+        T phi, mu;
+        if (P.delta)
+          problem::RelaxCell<T, 2, true>(st, sf0[si], sf1[si], tmp1, tmp2, tmp3, alpha, phi, mu,
+                                         sbs[si]);
+        else
+          problem::RelaxCell<T, 2>(st, sf0[si], sf1[si], tmp1, tmp2, tmp3, alpha, phi, mu);
+        s0[si] = phi;
+        s1[si] = mu;
+        if (P.wt && (i == 1 || i == n0 || j == 1 || j == n1))
+          smem_ghosts2<T>(P, s0, s1, si, i, j, phi, mu);
+      }
+      __syncthreads();
+    }
+    // Write back the tile's interior cells, ghosts by write-through.
+    for (int e = tid; e < F::TX * F::TY; e += F::THREADS) {
+      const int ly = e / F::TX, lx = e - ly * F::TX;
+      const int sx = F::H + lx, sy = F::H + ly;
+      const int i = gx0 + sx, j = gy0 + sy;
+      if (i > n0 || j > n1) continue;
+      const int si = sy * F::RX + sx;
+      const T v0 = s0[si], v1 = s1[si];
+      const int64_t c = cidx(P, i, j, 0);
+      o0[c] = v0;
+      o1[c] = v1;
+      if (P.wt && near_boundary(P, i, j, 0, 2)) write_through<T, 2>(P, o0, o1, i, j, 0, v0, v1);
+    }
+    __syncthreads();  // the shared tile is refilled for the next item
+  }
+}
+
+}  // namespace bsam

@@ -73,10 +73,18 @@ typedef struct {
 } bsam_step_result;
 
 /* Execution choices that leave every result bit unchanged (the autotuner's
- * knobs): grid_ctas caps the CTAs of each stage launch (0 = 16 per SM). */
+ * knobs): grid_ctas caps the CTAs of each stage launch (0 = 16 per SM);
+ * eager = 1 issues every tick's kernels from the host instead of the
+ * graph's device-side loop (then advance runs exactly max_ticks ticks);
+ * per_pass = 1 makes problems admitted afterwards smooth with one launch per
+ * colour pass instead of the fused shared-memory stage of 2D levels;
+ * fused_ctas caps the CTAs of a fused stage launch (0 = 4 per SM). */
 typedef struct {
   int32_t grid_ctas;
-  int32_t reserved[7];
+  int32_t eager;
+  int32_t per_pass;
+  int32_t fused_ctas;
+  int32_t reserved[4];
 } bsam_batch_tuning;
 
 typedef struct {
@@ -88,6 +96,10 @@ typedef struct {
   int64_t pool_bytes;
   int32_t resident;       /* slots holding a problem */
   int32_t running;
+  /* bsam_batch_profile: finest-depth smoothing stages timed with events */
+  int64_t smooth_stages;
+  double smooth_ms;
+  double smooth_bytes;    /* algorithmic: 6 * value bytes * cells per stage */
 } bsam_batch_stats;
 
 int bsam_batch_create(bsam_batch** b, int device, const bsam_batch_params* p);
@@ -130,6 +142,11 @@ int bsam_batch_slot_phase(bsam_batch* b, int slot, int* phase, int* steps_done);
  * (AfterStep's integral(1)). */
 int bsam_batch_collect(bsam_batch* b, int slot, double* q, bsam_step_result* steps,
                        double* mass);
+
+/* enable != 0: ticks run eagerly, one at a time, and each finest-depth
+ * smoothing stage (2 x nsmoothingpasses colour passes over every running
+ * problem's root level) is timed with CUDA events into the stats; 0 stops. */
+int bsam_batch_profile(bsam_batch* b, int enable);
 
 int bsam_batch_get_stream(bsam_batch* b, void** stream);
 int bsam_batch_get_stats(bsam_batch* b, bsam_batch_stats* s);

@@ -137,6 +137,38 @@ def test_batch_tuning_leaves_results_unchanged(gpu_lib):
     probs = [make(n, 90 + i) for i, n in enumerate([128, 96, 64])]
     a = BB.solve_all(probs, precision=BB.PREC_MIXED)
     b = BB.solve_all(probs, precision=BB.PREC_MIXED, grid_ctas=7)
-    for x, y in zip(a, b):
+    c = BB.solve_all(probs, precision=BB.PREC_MIXED, eager=1)
+    d = BB.solve_all(probs, precision=BB.PREC_MIXED, per_pass=1)  # no fused stages
+    e = BB.solve_all(probs, precision=BB.PREC_MIXED, fused_ctas=5)
+    for x, *others in zip(a, b, c, d, e):
+        for k in ("q", "nvcycles", "residual"):
+            for y in others:
+                assert np.array_equal(x[k], y[k]), k
+
+
+def test_batch_fused_fp64_stage_bit_identical(gpu_lib):
+    # FP64 form with the fused shared-memory stage (default) vs per-pass.
+    # 160 and 72 leave partial fused tiles (64 x 16 for FP64) at the far edges.
+    probs = [make(n, 110 + i, nsteps=2) for i, n in enumerate([192, 160, 72])]
+    a = BB.solve_all(probs, precision=BB.PREC_FP64)
+    b = BB.solve_all(probs, precision=BB.PREC_FP64, per_pass=1)
+    for p, x, y in zip(probs, a, b):
         for k in ("q", "nvcycles", "residual"):
             assert np.array_equal(x[k], y[k]), k
+        same(x, single(p, BB.PREC_FP64))
+
+
+def test_batch_profile_counts_finest_stages(gpu_lib):
+    probs = [make(n, 95 + i) for i, n in enumerate([128, 96])]
+    with BB.Batch(2, precision=BB.PREC_MIXED, max_slots=2) as bt:
+        for p in probs:
+            bt.submit(p)
+        bt.profile(True)
+        bt.advance(2)
+        bt.sync()
+        st = bt.stats()
+        bt.profile(False)
+    # two finest-depth stages (pre and post) per tick
+    assert st["smooth_stages"] == 4 and st["smooth_ms"] > 0
+    cells = sum(n * n for n in (128, 96))
+    assert st["smooth_bytes"] == 4 * 6 * 4 * cells

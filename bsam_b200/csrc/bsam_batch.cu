@@ -553,12 +553,15 @@ void tick_t(bsam_batch* b, cudaGraphConditionalHandle handle, int in_graph) {
     if (D == 2 && L[L_FUSED + d].cap > 0) {
       const int lim = b->tuning.fused_ctas > 0 ? b->tuning.fused_ctas : 4 * b->nsm;
       const int g = std::max(1, std::min(L[L_FUSED + d].cap, lim));
+      // Every fused record of a mixed batch is a correction-form FP32 level;
+      // of an FP64 batch, a plain FP64 level.
       if (b->mixed)
-        kb_smooth2<float><<<g, Fused2<float>::THREADS, Fused2<float>::SMEM, s>>>(
+        kb_smooth2<float, true><<<g, Fused2<float>::THREADS, Fused2<float>::smem(true), s>>>(
             pt, L[L_FUSED + d].d, cnt + L_FUSED + d, dir, nu, &b->d_ctl->kerr);
       else
-        kb_smooth2<double><<<g, Fused2<double>::THREADS, Fused2<double>::SMEM, s>>>(
-            pt, L[L_FUSED + d].d, cnt + L_FUSED + d, dir, nu, &b->d_ctl->kerr);
+        kb_smooth2<double, false>
+            <<<g, Fused2<double>::THREADS, Fused2<double>::smem(false), s>>>(
+                pt, L[L_FUSED + d].d, cnt + L_FUSED + d, dir, nu, &b->d_ctl->kerr);
       ++n;
     }
     stage_mark(b, d, false);
@@ -758,9 +761,11 @@ int bsam_batch_create(bsam_batch** out, int device, const bsam_batch_params* p) 
             cudaMalloc(&b->d_counts, sizeof(int) * NLIST) == cudaSuccess;
   if (ok) ok = cudaHostGetDevicePointer((void**)&b->d_out, b->h_out, 0) == cudaSuccess;
   if (ok)
-    ok = cudaFuncSetAttribute(kb_smooth2<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    ok = cudaFuncSetAttribute(kb_smooth2<float, true>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)Fused2<float>::SMEM) == cudaSuccess &&
-         cudaFuncSetAttribute(kb_smooth2<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+         cudaFuncSetAttribute(kb_smooth2<double, false>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)Fused2<double>::SMEM) == cudaSuccess;
   if (!ok) {
     cudaGetLastError();

@@ -40,6 +40,8 @@ struct Fused2 {
   static constexpr int THREADS = 256;
   static constexpr int WARPS = THREADS / 32;
   static constexpr size_t SMEM = sizeof(T) * NF * PLANE;
+  // Shared bytes of a launch: the base plane only for correction-form levels.
+  static constexpr size_t smem(bool delta) { return sizeof(T) * (delta ? NF : NF - 1) * PLANE; }
   static_assert((sizeof(T) * PLANE) % 128 == 0, "field planes stay 128-byte aligned");
 };
 
@@ -53,6 +55,18 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const void* tmap, int x, 
       "{%2, %3}], [%4];" ::"r"(smem_u32(dst)),
       "l"(tmap), "r"(x), "r"(y), "r"(smem_u32(bar))
       : "memory");
+}
+
+// Bounded wait on an mbarrier phase by one thread, sleeping between polls
+// (32 ns doubling to 512 ns).  Returns false after `limit` polls.
+__device__ __forceinline__ bool mbar_wait_backoff(uint64_t* b, uint32_t parity, uint32_t limit) {
+  uint32_t ns = 32;
+  for (uint32_t it = 0; it < limit; ++it) {
+    if (mbar_try_wait(b, parity)) return true;
+    __nanosleep(ns);
+    if (ns < 512) ns <<= 1;
+  }
+  return false;
 }
 
 // Ghost images of the updated cell (i,j) inside the shared tile: the face
@@ -82,8 +96,9 @@ __device__ __forceinline__ void smem_ghosts2(const DevPatch& P, T* s0, T* s1, in
 // dir 0: q -> qb (pre-smoothing); dir 1: qb -> q (post-smoothing).
 // P.tmaps: 2D maps of q0, q1, qb0, qb1, f0, f1, bs (box RX x RY).
 // A copy that has not landed after kWaitPolls polls sets *err and ends the
-// launch for this CTA.
-template <class T>
+// launch for this CTA.  DELTA: every record of the list is a correction-form
+// level (the mixed form's working levels), with a base field.
+template <class T, bool DELTA>
 __global__ void __launch_bounds__(Fused2<T>::THREADS)
     kb_smooth2(const DevPatch* __restrict__ PT, const Item* __restrict__ items,
                const int* __restrict__ count, int dir, int nu, int* __restrict__ err) {
@@ -116,15 +131,21 @@ __global__ void __launch_bounds__(Fused2<T>::THREADS)
       const int m0 = dir == 0 ? 0 : 2;
       const uint32_t plane = (uint32_t)(sizeof(T) * F::PLANE);
       fence_proxy_async_smem();  // earlier generic accesses to the tile come first
-      mbar_arrive_expect_tx(&bar, plane * (P.delta ? 5u : 4u));
+      mbar_arrive_expect_tx(&bar, plane * (DELTA ? 5u : 4u));
       const int x = gx0 + lead;  // column of element (gx0, *) from the allocation start
       tma_load_2d(s0, &maps[m0], x, gy0, &bar);
       tma_load_2d(s1, &maps[m0 + 1], x, gy0, &bar);
       tma_load_2d(sf0, &maps[4], x, gy0, &bar);
       tma_load_2d(sf1, &maps[5], x, gy0, &bar);
-      if (P.delta) tma_load_2d(sbs, &maps[6], x, gy0, &bar);
+      if (DELTA) tma_load_2d(sbs, &maps[6], x, gy0, &bar);
     }
-    const bool ok = __syncthreads_and(mbar_wait_bounded(&bar, phase, kWaitPolls));
+    // One thread polls (with back-off, so that the waiting CTA takes no issue
+    // slots from the CTAs computing beside it); after the barrier every
+    // thread observes the completed phase itself.
+    bool ok = true;
+    if (tid == 0) ok = mbar_wait_backoff(&bar, phase, kWaitPolls);
+    ok = __syncthreads_and(ok);
+    if (ok && tid != 0) (void)mbar_try_wait(&bar, phase);
     phase ^= 1u;
     if (!ok) {
       if (tid == 0) atomicExch(err, kErrTmaTimeout);
@@ -140,52 +161,60 @@ __global__ void __launch_bounds__(Fused2<T>::THREADS)
       // Region of this pass in shared coordinates, clipped to the interior.
       const int xa = max(F::H - grow, 1 - gx0), xb = min(F::H + F::TX + grow, n0 + 1 - gx0);
       const int ya = max(F::H - grow, 1 - gy0), yb = min(F::H + F::TY + grow, n1 + 1 - gy0);
-      for (int sy = ya + warp; sy < yb; sy += F::WARPS) {
-        const int j = gy0 + sy;
-        int sx = xa + 2 * lane;
-        int i = gx0 + sx;
-        if ((i + j + color) & 1) {
-          ++sx;
-          ++i;
+      // A warp's rows step by WARPS (even), so the column of the pass's
+      // colour in the lane's pair is the same on all of them.
+      const int sy0 = ya + warp;
+      int sx = xa + 2 * lane;
+      if ((gx0 + sx + gy0 + sy0 + color) & 1) ++sx;
+      if (sx < xb) {
+        const int i = gx0 + sx;
+        const bool edge_i = P.wt && (i == 1 || i == n0);
+        int si = sy0 * F::RX + sx;
+        for (int sy = sy0; sy < yb; sy += F::WARPS, si += F::WARPS * F::RX) {
+          problem::Stencil<T, 2> st;
+          st.pc = s0[si];
+          st.mc = s1[si];
+          st.pm[0] = s0[si - 1];
+          st.pp[0] = s0[si + 1];
+          st.mm[0] = s1[si - 1];
+          st.mp[0] = s1[si + 1];
+          st.pm[1] = s0[si - F::RX];
+          st.pp[1] = s0[si + F::RX];
+          st.mm[1] = s1[si - F::RX];
+          st.mp[1] = s1[si + F::RX];
+          T phi, mu;
+          if constexpr (DELTA)
+            problem::RelaxCell<T, 2, true>(st, sf0[si], sf1[si], tmp1, tmp2, tmp3, alpha, phi,
+                                           mu, sbs[si]);
+          else
+            problem::RelaxCell<T, 2>(st, sf0[si], sf1[si], tmp1, tmp2, tmp3, alpha, phi, mu);
+          s0[si] = phi;
+          s1[si] = mu;
+          const int j = gy0 + sy;
+          if (edge_i || (P.wt && (j == 1 || j == n1)))
+            smem_ghosts2<T>(P, s0, s1, si, i, j, phi, mu);
         }
-        if (sx >= xb) continue;
-        const int si = sy * F::RX + sx;
-        problem::Stencil<T, 2> st;
-        st.pc = s0[si];
-        st.mc = s1[si];
-        st.pm[0] = s0[si - 1];
-        st.pp[0] = s0[si + 1];
-        st.mm[0] = s1[si - 1];
-        st.mp[0] = s1[si + 1];
-        st.pm[1] = s0[si - F::RX];
-        st.pp[1] = s0[si + F::RX];
-        st.mm[1] = s1[si - F::RX];
-        st.mp[1] = s1[si + F::RX];
-        T phi, mu;
-        if (P.delta)
-          problem::RelaxCell<T, 2, true>(st, sf0[si], sf1[si], tmp1, tmp2, tmp3, alpha, phi, mu,
-                                         sbs[si]);
-        else
-          problem::RelaxCell<T, 2>(st, sf0[si], sf1[si], tmp1, tmp2, tmp3, alpha, phi, mu);
-        s0[si] = phi;
-        s1[si] = mu;
-        if (P.wt && (i == 1 || i == n0 || j == 1 || j == n1))
-          smem_ghosts2<T>(P, s0, s1, si, i, j, phi, mu);
       }
       __syncthreads();
     }
-    // Write back the tile's interior cells, ghosts by write-through.
-    for (int e = tid; e < F::TX * F::TY; e += F::THREADS) {
-      const int ly = e / F::TX, lx = e - ly * F::TX;
-      const int sx = F::H + lx, sy = F::H + ly;
-      const int i = gx0 + sx, j = gy0 + sy;
-      if (i > n0 || j > n1) continue;
-      const int si = sy * F::RX + sx;
-      const T v0 = s0[si], v1 = s1[si];
-      const int64_t c = cidx(P, i, j, 0);
-      o0[c] = v0;
-      o1[c] = v1;
-      if (P.wt && near_boundary(P, i, j, 0, 2)) write_through<T, 2>(P, o0, o1, i, j, 0, v0, v1);
+    // Write back the tile's interior cells (warps over rows, lanes along
+    // them), ghosts by write-through.
+    for (int ly = warp; ly < F::TY; ly += F::WARPS) {
+      const int j = gy0 + F::H + ly;
+      if (j > n1) break;
+      const int srow = (F::H + ly) * F::RX + F::H;
+      T* r0 = o0 + (int64_t)j * P.sy;
+      T* r1 = o1 + (int64_t)j * P.sy;
+      const bool edge_j = P.wt && (j == 1 || j == n1);
+      for (int lx = lane; lx < F::TX; lx += 32) {
+        const int i = gx0 + F::H + lx;
+        if (i > n0) break;
+        const T v0 = s0[srow + lx], v1 = s1[srow + lx];
+        r0[i] = v0;
+        r1[i] = v1;
+        if (edge_j || (P.wt && (i == 1 || i == n0)))
+          write_through<T, 2>(P, o0, o1, i, j, 0, v0, v1);
+      }
     }
     __syncthreads();  // the shared tile is refilled for the next item
   }

@@ -65,6 +65,35 @@ __device__ __forceinline__ void RelaxCell(const Stencil<T, D>& s, T f0, T f1, T 
   for (int t = 1; t < 2 * D; ++t) msum = msum + m[t];
   const T a12 = tmp1 * msum;
   const T cfull = DELTA ? base + s.pc : s.pc;
+  if constexpr (sizeof(T) == 4) {
+    // FP32 working levels of the mixed form: the same Newton step with
+    // contracted products and one approximate reciprocal (__fdividef,
+    // 2 ulp), since these levels only smooth a correction whose FP64 defect
+    // is recomputed exactly; the FP64 path below keeps the reference's
+    // operation order.
+    const T d2 = D2fc(cfull, alpha);
+    const T a21f = -d2 - tmp3;
+    T smuf = m[0] * s.mm[0] + m[1] * s.mp[0];
+#pragma unroll
+    for (int d = 1; d < D; ++d) {
+      smuf = smuf + m[2 * d] * s.mm[d];
+      smuf = smuf + m[2 * d + 1] * s.mp[d];
+    }
+    T sphf = s.pp[0] + s.pm[0];
+#pragma unroll
+    for (int d = 1; d < D; ++d) {
+      sphf = sphf + s.pp[d];
+      sphf = sphf + s.pm[d];
+    }
+    const T nlf = DELTA ? DfcDelta(base, s.pc, alpha) : Dfc(s.pc, alpha);
+    const T b1f = __fmaf_rn(tmp1, smuf, f0);
+    const T b2f = __fmaf_rn(-tmp2, sphf, __fmaf_rn(-d2, s.pc, f1 + nlf));
+    const T detf = __fmaf_rn(-a12, a21f, T(1));
+    const T r = __fdividef(T(1), detf);
+    phi = __fmaf_rn(-a12, b2f, b1f) * r;
+    mu = __fmaf_rn(-a21f, b1f, b2f) * r;
+    return;
+  }
   const T a21 = -D2fc(cfull, alpha) - tmp3;
   // b(1): f + tmp1*(m1*mu(i-1) + m2*mu(i+1) + m3*mu(j-1) + m4*mu(j+1) ...)
   T smu = m[0] * s.mm[0] + m[1] * s.mp[0];

@@ -78,6 +78,9 @@ def bind(L):
     L.bsam_batch_slot_phase.argtypes = [vp, ctypes.c_int, ip, ip]
     L.bsam_batch_collect.argtypes = [vp, ctypes.c_int, dp, ctypes.POINTER(StepResult), dp]
     L.bsam_batch_profile.argtypes = [vp, ctypes.c_int]
+    L.bsam_batch_submit_seeded.argtypes = [vp, ctypes.POINTER(BatchProblem), ctypes.c_uint64,
+                                           ctypes.c_double, ctypes.c_double, ip]
+    L.bsam_batch_busy.argtypes = [vp]
     L.bsam_batch_get_stream.argtypes = [vp, ctypes.POINTER(vp)]
     L.bsam_batch_get_stats.argtypes = [vp, ctypes.POINTER(BatchStats)]
     L.bsam_batch_last_error.argtypes = [vp]
@@ -165,6 +168,25 @@ class Batch:
         _check(rc, self.h, "submit")
         self.probs[slot.value] = prob
         return slot.value
+
+    def submit_seeded(self, prob):
+        """Admits prob with its initial state drawn on the device from
+        (prob.seed, prob.cbar, prob.amp) -- the same bits as prob.q0()."""
+        ps = problem_struct(prob)
+        slot = ctypes.c_int(-1)
+        rc = _lib().bsam_batch_submit_seeded(self.h, ctypes.byref(ps), prob.seed, prob.cbar,
+                                             prob.amp, ctypes.byref(slot))
+        if rc == ERR_NOMEM:
+            return None
+        _check(rc, self.h, "submit_seeded")
+        self.probs[slot.value] = prob
+        return slot.value
+
+    def busy(self) -> bool:
+        rc = _lib().bsam_batch_busy(self.h)
+        if rc < 0:
+            _check(rc, self.h, "busy")
+        return rc == 1
 
     def advance(self, max_ticks: int = 1):
         _check(_lib().bsam_batch_advance(self.h, max_ticks), self.h, "advance")

@@ -238,6 +238,69 @@ __global__ void k_batch_cond(BatchCtl* __restrict__ ctl, cudaGraphConditionalHan
   if (in_graph) cudaGraphSetConditional(handle, again ? 1u : 0u);
 }
 
+// ---- seeded initial state on the device ---------------------------------------
+//
+// QInit replacement for generated workloads (the reference's QInit2D/3D,
+// problem.f90:58-101, 362-397, fills q on the host; here the state of a
+// submitted problem can instead be drawn where it lives):
+//   c(i,j[,k]) = cbar + amp * U(-1, 1), U from SplitMix64 stream `seed` in
+//   column-major interior order, U(a,b) = a + (b - a) * ((x >> 11) * 2^-53);
+//   mu = Dfc(c) - Dfe(c) - eps^2/h^2 * ULap(c) with Neumann (copy) ghosts.
+// The same arithmetic in the same order as the host generator
+// (bsam_b200/workloads.py: uniform, initial_q), so both give identical bits.
+
+__device__ __forceinline__ double seeded_u(uint64_t seed, int64_t idx) {
+  uint64_t z = seed + (uint64_t)(idx + 1) * 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  z = z ^ (z >> 31);
+  const double u = (double)(z >> 11) * 0x1.0p-53;
+  return -1.0 + 2.0 * u;
+}
+
+// c at interior-or-ghost cell (i,j,k) under Neumann copy ghosts.
+template <int D>
+__device__ __forceinline__ double seeded_c(const DevPatch& P, uint64_t seed, double cbar,
+                                           double amp, int i, int j, int k) {
+  i = i < 1 ? 1 : (i > P.n[0] ? P.n[0] : i);
+  j = j < 1 ? 1 : (j > P.n[1] ? P.n[1] : j);
+  if (D == 3) k = k < 1 ? 1 : (k > P.n[2] ? P.n[2] : k);
+  const int64_t idx = (int64_t)(i - 1) + (int64_t)P.n[0] * ((j - 1) + (int64_t)P.n[1] * (D == 3 ? k - 1 : 0));
+  return cbar + amp * seeded_u(seed, idx);
+}
+
+// Interior of the state record `rec`: c and mu (ghosts by a k_setbc launch).
+template <int D>
+__global__ void k_init_seeded(const DevPatch* __restrict__ PT, int rec, uint64_t seed,
+                              double cbar, double amp, double k2) {
+  const DevPatch P = PT[rec];
+  const int64_t n = (int64_t)P.n[0] * P.n[1] * (D == 3 ? P.n[2] : 1);
+  for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n;
+       g += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(g % P.n[0]) + 1;
+    const int64_t r = g / P.n[0];
+    const int j = (int)(r % P.n[1]) + 1;
+    const int k = D == 3 ? (int)(r / P.n[1]) + 1 : 0;
+    const double c = seeded_c<D>(P, seed, cbar, amp, i, j, k);
+    // lap = -2d c + (c(i+1) + c(i-1)) + (c(j+1) + c(j-1)) [+ ...], summed
+    // left to right per dimension as the host generator does.
+    double lap = -2.0 * D * c;
+    lap = lap + seeded_c<D>(P, seed, cbar, amp, i + 1, j, k);
+    lap = lap + seeded_c<D>(P, seed, cbar, amp, i - 1, j, k);
+    lap = lap + seeded_c<D>(P, seed, cbar, amp, i, j + 1, k);
+    lap = lap + seeded_c<D>(P, seed, cbar, amp, i, j - 1, k);
+    if (D == 3) {
+      lap = lap + seeded_c<D>(P, seed, cbar, amp, i, j, k + 1);
+      lap = lap + seeded_c<D>(P, seed, cbar, amp, i, j, k - 1);
+    }
+    const double alpha = P.alpha;
+    const double mu = problem::Dfc(c, alpha) - problem::Dfe(c, alpha) - k2 * lap;
+    const int64_t ci = cidx(P, i, j, k);
+    fld<double>(P.q[0])[ci] = c;
+    fld<double>(P.q[1])[ci] = mu;
+  }
+}
+
 __global__ void k_batch_budget(BatchCtl* __restrict__ ctl, int ticks) {
   ctl->ticks_left = ticks;
   ctl->running = 0;

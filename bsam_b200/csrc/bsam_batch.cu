@@ -845,9 +845,16 @@ int bsam_batch_footprint(bsam_batch* b, const bsam_batch_problem* prob, int64_t*
   return BSAM_OK;
 }
 
-int bsam_batch_submit(bsam_batch* b, const bsam_batch_problem* prob, const double* q0,
-                      int* slot) {
-  if (!b || !prob || !q0 || !slot) return BSAM_ERR_ARG;
+// Admission of one problem; its initial state is either copied from the host
+// (q0) or drawn on the device (init).
+struct SeedInit {
+  uint64_t seed;
+  double cbar, amp;
+};
+
+static int admit(bsam_batch* b, const bsam_batch_problem* prob, const double* q0,
+                 const SeedInit* init, int* slot) {
+  if (!b || !prob || (!q0 && !init) || !slot) return BSAM_ERR_ARG;
   CU(cudaSetDevice(b->device));
   SlotPlan probe;
   int rc = plan_slot(b, prob, 0, nullptr, probe);
@@ -899,13 +906,26 @@ int bsam_batch_submit(bsam_batch* b, const bsam_batch_problem* prob, const doubl
   const DevPatch& M = S.recs[S.master];
   const int e0 = M.n[0] + 2, e1 = M.n[1] + 2, e2 = nd == 3 ? M.n[2] + 2 : 1;
   const size_t hcomp = (size_t)e0 * e1 * e2;
-  char* st = stage_alloc(b, sizeof(double) * 2 * hcomp);
-  if (!st) return fail(b, BSAM_ERR_NOMEM, "pinned staging allocation failed");
-  std::memcpy(st, q0, sizeof(double) * 2 * hcomp);
-  for (int c = 0; c < 2; ++c)
-    CU(cudaMemcpy2DAsync(M.q[c], M.sy * sizeof(double), st + c * hcomp * sizeof(double),
-                         e0 * sizeof(double), e0 * sizeof(double), (size_t)e1 * e2,
-                         cudaMemcpyHostToDevice, b->stream));
+  if (q0) {
+    char* st = stage_alloc(b, sizeof(double) * 2 * hcomp);
+    if (!st) return fail(b, BSAM_ERR_NOMEM, "pinned staging allocation failed");
+    std::memcpy(st, q0, sizeof(double) * 2 * hcomp);
+    for (int c = 0; c < 2; ++c)
+      CU(cudaMemcpy2DAsync(M.q[c], M.sy * sizeof(double), st + c * hcomp * sizeof(double),
+                           e0 * sizeof(double), e0 * sizeof(double), (size_t)e1 * e2,
+                           cudaMemcpyHostToDevice, b->stream));
+  } else {
+    const double h = M.h;
+    const double k2 = (prob->eps * prob->eps) / (h * h);
+    const int64_t ncell = S.cells;
+    const int gi = (int)std::min<int64_t>((ncell + 255) / 256, 16 * b->nsm);
+    if (nd == 2)
+      k_init_seeded<2><<<gi, 256, 0, b->stream>>>(b->d_pt, rec0 + S.master, init->seed,
+                                                   init->cbar, init->amp, k2);
+    else
+      k_init_seeded<3><<<gi, 256, 0, b->stream>>>(b->d_pt, rec0 + S.master, init->seed,
+                                                   init->cbar, init->amp, k2);
+  }
   const int64_t total = (int64_t)hcomp;
   const int nb = (int)((total + 255) / 256);
   if (nd == 2) k_setbc<double, 2><<<nb, 256, 0, b->stream>>>(b->d_pt, rec0 + S.master, total);
@@ -930,6 +950,27 @@ int bsam_batch_submit(bsam_batch* b, const bsam_batch_problem* prob, const doubl
   stage_commit(b);
   *slot = s;
   return BSAM_OK;
+}
+
+int bsam_batch_submit(bsam_batch* b, const bsam_batch_problem* prob, const double* q0,
+                      int* slot) {
+  if (!q0) return BSAM_ERR_ARG;
+  return admit(b, prob, q0, nullptr, slot);
+}
+
+int bsam_batch_submit_seeded(bsam_batch* b, const bsam_batch_problem* prob, uint64_t seed,
+                             double cbar, double amp, int* slot) {
+  const SeedInit init{seed, cbar, amp};
+  return admit(b, prob, nullptr, &init, slot);
+}
+
+int bsam_batch_busy(bsam_batch* b) {
+  if (!b) return BSAM_ERR_ARG;
+  cudaSetDevice(b->device);
+  const cudaError_t e = cudaStreamQuery(b->stream);
+  if (e == cudaSuccess) return 0;
+  if (e == cudaErrorNotReady) return 1;
+  return fail(b, BSAM_ERR_CUDA, std::string("stream query: ") + cudaGetErrorString(e));
 }
 
 int bsam_batch_advance(bsam_batch* b, int max_ticks) {

@@ -1,0 +1,151 @@
+"""Served form: continuous batching of Cahn-Hilliard solve requests on one GPU.
+
+Requests arrive over time (a Poisson stream in the benchmark).  The server
+keeps one batch engine per dimensionality (include/bsam_batch.h), each on its
+own CUDA stream, so 2D and 3D work overlaps on the device.  A request is
+admitted as soon as its engine has a free slot and room for the request's
+device footprint in its memory pool; otherwise it waits in FIFO order.
+Admitted problems stay resident on the device for all their time steps and
+are advanced together, a few V-cycle ticks per engine launch; every loop the
+server collects what has finished and admits what now fits, so requests that
+arrive while others are on the GPU join the running batch.
+
+A result depends only on its own request: the batch engine computes every
+problem exactly as it would alone (tests/test_gpu_serve.py checks it).
+"""
+from __future__ import annotations
+
+import dataclasses
+import time
+from collections import deque
+
+import numpy as np
+
+from . import batch as BB
+
+
+@dataclasses.dataclass
+class Request:
+    rid: int
+    arrival: float           # seconds after the stream starts
+    prob: object             # workloads.Problem (seeded form)
+    admitted: float | None = None
+    finished: float | None = None
+    result: dict | None = None
+
+    @property
+    def latency(self) -> float:
+        return self.finished - self.arrival
+
+
+class Server:
+    """Continuous-batching server over one batch engine per dimensionality.
+
+    pool_bytes: device memory for resident problem state, split between the
+    2D and 3D engines by `share_2d`.  ticks: V-cycle ticks per engine launch
+    (the admission / completion granularity).
+    """
+
+    def __init__(self, pool_bytes: int, precision: int = BB.PREC_MIXED, max_slots: int = 256,
+                 share_2d: float = 0.5, ticks: int = 4, qerrortol: float = 1e-8,
+                 maxvcycles: int = 20, device: int = 0, keep_q: bool = False):
+        p2 = int(pool_bytes * share_2d)
+        self.engines = {
+            2: BB.Batch(2, precision=precision, max_slots=max_slots, pool_bytes=p2,
+                        qerrortol=qerrortol, maxvcycles=maxvcycles, device=device),
+            3: BB.Batch(3, precision=precision, max_slots=max_slots,
+                        pool_bytes=pool_bytes - p2, qerrortol=qerrortol,
+                        maxvcycles=maxvcycles, device=device),
+        }
+        self.ticks = ticks
+        self.keep_q = keep_q
+
+    def close(self):
+        for e in self.engines.values():
+            e.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def fits_alone(self, prob) -> bool:
+        e = self.engines[prob.ndims]
+        return e.footprint(prob) <= e.stats()["pool_bytes"]
+
+    def serve(self, stream, time_scale: float = 1.0) -> list:
+        """Runs the (arrival_s, Problem) stream in real time; returns the
+        Requests with arrival, admission and completion times."""
+        reqs = [Request(i, a * time_scale, p) for i, (a, p) in enumerate(stream)]
+        for r in reqs:
+            if not self.fits_alone(r.prob):
+                raise ValueError(f"request {r.rid} does not fit in its engine's pool")
+        pending = deque()
+        inflight = {}
+        nxt = 0
+        t0 = time.perf_counter()
+        now = 0.0
+        running = {2: 0, 3: 0}
+        while nxt < len(reqs) or pending or inflight:
+            now = time.perf_counter() - t0
+            while nxt < len(reqs) and reqs[nxt].arrival <= now:
+                pending.append(reqs[nxt])
+                nxt += 1
+            # Admission: FIFO per engine (a full engine does not block the other).
+            blocked = set()
+            keep = deque()
+            while pending:
+                r = pending.popleft()
+                nd = r.prob.ndims
+                s = None if nd in blocked else self.engines[nd].submit_seeded(r.prob)
+                if s is None:
+                    blocked.add(nd)
+                    keep.append(r)
+                    continue
+                r.admitted = now
+                inflight[(nd, s)] = r
+                running[nd] += 1
+            pending = keep
+            # Keep every engine with running problems busy.
+            for nd, e in self.engines.items():
+                if running[nd] and not e.busy():
+                    e.advance(self.ticks)
+            # Completions.
+            done_any = False
+            for nd, e in self.engines.items():
+                if not running[nd]:
+                    continue
+                for s in e.poll():
+                    r = inflight.pop((nd, s))
+                    r.finished = time.perf_counter() - t0
+                    r.result = e.collect(s, want_q=self.keep_q)
+                    running[nd] -= 1
+                    done_any = True
+            if not done_any and not pending and not inflight and nxt < len(reqs):
+                wait = reqs[nxt].arrival - (time.perf_counter() - t0)
+                if wait > 0:
+                    time.sleep(min(wait, 0.01))
+            elif not done_any:
+                time.sleep(50e-6)
+        return reqs
+
+
+def summarize(reqs: list) -> dict:
+    """p50 / p99 latency, solves/s and time-steps/s over the whole stream."""
+    lat = np.array([r.latency for r in reqs])
+    makespan = max(r.finished for r in reqs) - min(r.arrival for r in reqs)
+    steps = sum(int(r.prob.nsteps) for r in reqs)
+    vcycles = sum(int(r.result["nvcycles"].sum()) for r in reqs)
+    conv = all(int(r.result["converged"].min()) == 1 for r in reqs)
+    return {
+        "requests": len(reqs),
+        "p50_ms": float(np.percentile(lat, 50) * 1e3),
+        "p99_ms": float(np.percentile(lat, 99) * 1e3),
+        "mean_ms": float(lat.mean() * 1e3),
+        "solves_per_s": len(reqs) / makespan,
+        "steps_per_s": steps / makespan,
+        "vcycles": vcycles,
+        "makespan_s": makespan,
+        "all_converged": conv,
+    }

@@ -55,6 +55,11 @@ class Problem:
     mthbc: tuple = (1, 1, 1, 1, 1, 1)
     c0: np.ndarray | None = None   # interior composition, Fortran order
     xupper: tuple = (1.0, 1.0, 1.0)  # domain [0, xupper]; dx must be equal in all dims
+    # Seeded form (c0 = cbar + amp * uniform(seed, cells, -1, 1)): what the
+    # device-side initialiser of the batch engine draws.
+    seed: int | None = None
+    cbar: float = 0.5
+    amp: float = 0.0
 
     @property
     def h(self) -> float:
@@ -62,7 +67,46 @@ class Problem:
 
     def q0(self) -> np.ndarray:
         """Root q with ghost ring, Fortran layout (0:mx+1)^d x 2."""
-        return initial_q(self.ndims, self.mx, self.c0, self.h, self.eps, self.alpha)
+        c0 = self.c0
+        if c0 is None:
+            cells = int(np.prod(self.mx[:self.ndims]))
+            c0 = self.cbar + self.amp * uniform(self.seed, cells, -1.0, 1.0)
+        return initial_q(self.ndims, self.mx, c0, self.h, self.eps, self.alpha)
+
+
+def seeded(ndims: int, n: int, eps: float, nsteps: int, seed: int, cbar: float, amp: float,
+           dt: float = 1e-4, qerrortol: float = 1e-8) -> Problem:
+    """A problem whose initial composition is cbar + amp * U(-1, 1) from the
+    SplitMix64 stream `seed` (drawn lazily; the batch engine can draw it on
+    the device)."""
+    mx = (n, n, n if ndims == 3 else 1)
+    return Problem(ndims=ndims, mx=mx, eps=eps, dt=dt, nsteps=nsteps, qerrortol=qerrortol,
+                   seed=seed, cbar=cbar, amp=amp)
+
+
+def config5(nreq: int, rate: float, seed: int = 5) -> list:
+    """Serving stream: Poisson arrivals at `rate` per second; 70 % 2D with
+    side in {64, 128, 256, 512}, 30 % 3D with side in {32, 64, 128}; steps
+    uniform in 1..50; eps ~ U(0.005, 0.02); dt = 1e-4; c0 = 0.5 + 0.025
+    U(-1, 1) (seeded per request); residual 1e-8.  Returns (arrival_s,
+    Problem) pairs in arrival order.  AMR levels of 2D requests are not drawn:
+    requests run on their uniform root grid."""
+    gaps = -np.log(1.0 - uniform(seed, nreq, 0.0, 1.0)) / rate
+    arrival = np.cumsum(gaps)
+    is3 = uniform(seed + 1, nreq, 0.0, 1.0) < 0.3
+    pick = splitmix64(seed + 2, nreq)
+    steps = 1 + (splitmix64(seed + 3, nreq) % np.uint64(50)).astype(np.int64)
+    eps = uniform(seed + 4, nreq, 0.005, 0.02)
+    out = []
+    for r in range(nreq):
+        if is3[r]:
+            n, nd = (32, 64, 128)[int(pick[r] % np.uint64(3))], 3
+        else:
+            n, nd = (64, 128, 256, 512)[int(pick[r] % np.uint64(4))], 2
+        p = seeded(nd, n, float(eps[r]), int(steps[r]), seed=7919 * (seed + 1) + r,
+                   cbar=0.5, amp=0.025)
+        out.append((float(arrival[r]), p))
+    return out
 
 
 def _dfc(c, alpha):

@@ -117,6 +117,19 @@ int bsam_batch_footprint(bsam_batch* b, const bsam_batch_problem* prob, int64_t*
 int bsam_batch_submit(bsam_batch* b, const bsam_batch_problem* prob, const double* q0,
                       int* slot);
 
+/* As bsam_batch_submit, with the initial state drawn on the device instead of
+ * copied (QInit for generated workloads):
+ *   c  = cbar + amp * U(-1, 1), U from the SplitMix64 stream `seed` in
+ *        column-major interior order (U = -1 + 2 * ((x >> 11) * 2^-53)),
+ *   mu = Dfc(c) - Dfe(c) - eps^2/h^2 * ULap(c), Neumann ghosts for ULap;
+ * then SetBC.  Bit-identical to building the same q0 on the host. */
+int bsam_batch_submit_seeded(bsam_batch* b, const bsam_batch_problem* prob, uint64_t seed,
+                             double cbar, double amp, int* slot);
+
+/* 1 while work queued on the batch's stream is still executing, 0 when idle
+ * (does not wait). */
+int bsam_batch_busy(bsam_batch* b);
+
 /* Queues up to max_ticks V-cycle ticks (fewer if every problem finishes);
  * returns without waiting. */
 int bsam_batch_advance(bsam_batch* b, int max_ticks);

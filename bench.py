@@ -1,15 +1,22 @@
 #!/usr/bin/env python
-"""Headline benchmark: Cahn-Hilliard time steps per second of the FAS
-V(2,2) multigrid solve on one B200 (or N independent replicas on N GPUs).
+"""Headline benchmark: Cahn-Hilliard time steps per second on one B200 (or
+N GPUs, each with its own batch).
 
-Workload: 3D 128^3 uniform grid on [0,1]^3, Neumann BCs, eps = 0.02,
-dt = 1e-4, phi0 = 0.1 + 0.05 U(-1,1) (seeded SplitMix64), V(2,2) cycles to
-residual 1e-8, plain FP64.  One "step" = one implicit time step
-(CopyQToQold + MultigridIterations), inputs resident in HBM.
+Workload (one bench "step"): 512 independent 2D Cahn-Hilliard problems with
+sides uniform over {64, 96, 128, 192, 256}, eps ~ U(0.005, 0.02),
+phi0 = m + 0.05 U(-1,1), m ~ U(-0.3, 0.3) (seeded SplitMix64), dt = 1e-4,
+10 implicit time steps each, FAS V(2,2) to residual 1e-8, solved together in
+the batched mixed-precision form (FP32 correction-form V-cycle inside an FP64
+defect loop).  The metric counts problem time steps: 5120 per bench step.
 
-Output: one JSON line on rank 0 (see the keys below).  `--impl reference`
-times the CPU restatement of the reference Fortran path (the reference itself
-cannot be compiled: no Fortran compiler in the image) on the same workload.
+Also reported beside the headline: the same problems in the FP64 batched form
+and solved one at a time by the plain FP64 form; the 3D 128^3 single-problem
+workload in both forms; one point of the served form (Poisson requests);
+the smoother roofline; the CPU restatement of the reference (the reference
+Fortran cannot be compiled here: no Fortran compiler in the image).
+
+Output: one JSON line on rank 0.  `--impl reference` times the CPU
+restatement of the reference path with all host cores on the same workload.
 """
 from __future__ import annotations
 
@@ -24,11 +31,13 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "CH time-steps/s (3D 128^3, FP64, V(2,2) to residual 1e-8)"
+METRIC = "CH time-steps/s (512 batched 2D problems, mixed precision, V(2,2) to residual 1e-8)"
 UNIT = "time-steps/s"
-WORKLOAD = ("3D uniform 128^3 Cahn-Hilliard on [0,1]^3, Neumann, eps=0.02, dt=1e-4, "
-            "phi0=0.1+0.05U(-1,1) seed 3, FAS V(2,2) red-black to residual 1e-8, FP64")
-L2_BYTES = 126 * 1024 * 1024
+WORKLOAD = ("512 independent 2D Cahn-Hilliard problems on [0,1]^2, sides U{64,96,128,192,256}, "
+            "Neumann, eps~U(0.005,0.02), phi0=m+0.05U(-1,1), m~U(-0.3,0.3), dt=1e-4, "
+            "10 time steps each, FAS V(2,2) red-black to residual 1e-8, batched, mixed "
+            "precision (FP32 correction-form V-cycle in an FP64 defect loop)")
+NPROB, NSTEPS = 512, 10
 
 
 def peaks():
@@ -98,7 +107,7 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def dist_setup(args):
+def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -128,207 +137,337 @@ def allmax(world, x: float) -> float:
     return float(t.item())
 
 
-def cpu_baseline(nsteps: int = 2):
-    """The CPU oracle (a restatement of the reference Fortran path) on a
-    bounded sample: the first `nsteps` time steps of the same workload."""
+def shard_problems(rank: int):
+    """Rank r's batch: the 512-problem workload drawn from seed 4 + 1000 r
+    (weak scaling: every GPU solves its own 512 problems, no exchange)."""
+    from bsam_b200 import workloads as W
+    return W.config4(nprob=NPROB, nsteps=NSTEPS, seed=4 + 1000 * rank)
+
+
+# ---- CPU restatement of the reference (the oracle) ---------------------------
+
+def _oracle_solve(args):
+    """One problem through the CPU oracle (worker of the reference arm)."""
+    idx, nsteps, seed = args
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
     from bsam_b200 import workloads as W
-    pyoracle.build()
-    prob = W.config3(nsteps=nsteps)
-    q0 = prob.q0()
+    prob = W.config4(nprob=idx + 1, nsteps=nsteps, seed=seed)[idx]
     t0 = time.perf_counter()
-    r = pyoracle.run_uniform(prob, nsteps=nsteps, keep_steps=False, q0=q0)
-    dt = time.perf_counter() - t0
-    return {"value": nsteps / dt, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"first {nsteps} time steps of the 128^3 workload, single thread "
-                      f"(C++ restatement of the reference; {int(r['nvcycles'].sum())} V-cycles)"}
+    pyoracle.run_uniform(prob, nsteps=nsteps, keep_steps=False)
+    return nsteps, time.perf_counter() - t0
+
+
+def cpu_baseline(sample: int = 12, nsteps: int = 2):
+    """The oracle on one core over a bounded sample of the workload: the first
+    `sample` problems, `nsteps` time steps each."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    pyoracle.build()
+    steps, secs = 0, 0.0
+    for i in range(sample):
+        s, t = _oracle_solve((i, nsteps, 4))
+        steps += s
+        secs += t
+    return {"value": steps / secs, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"first {sample} of the 512 problems, {nsteps} time steps each, one "
+                      "thread (C++ restatement of the reference Fortran path)"}
 
 
 def run_reference(args, world, rank):
     if rank != 0:
         return 0
+    import multiprocessing as mp
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
-    from bsam_b200 import workloads as W
     pyoracle.build()
-    prob = W.config3(nsteps=args.warmup + args.steps)
-    q = prob.q0()
-    times = []
-    for s in range(args.warmup + args.steps):
-        t0 = time.perf_counter()
-        r = pyoracle.run_uniform(prob, nsteps=1, keep_steps=True, q0=q)
-        dt = time.perf_counter() - t0
-        q = r["q"][0]
-        if s >= args.warmup:
-            times.append(dt)
+    cores = os.cpu_count() or 1
+    per_step = 2 * cores  # problems per bench step, 2 time steps each
+    ctx = mp.get_context("spawn")
+    times, steps_done = [], 0
+    with ctx.Pool(cores) as pool:
+        for s in range(args.warmup + args.steps):
+            jobs = [((s * per_step + k) % NPROB, 2, 4) for k in range(per_step)]
+            t0 = time.perf_counter()
+            res = pool.map(_oracle_solve, jobs)
+            dt = time.perf_counter() - t0
+            if s >= args.warmup:
+                times.append(dt)
+                steps_done += sum(r[0] for r in res)
     total = sum(times)
-    value = args.steps / total
+    value = steps_done / total
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
-                         "sample": "one full time step per step, single thread (the reference "
-                                   "path is serial); C++ restatement of the Fortran reference, "
-                                   "which cannot be compiled here"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"per step {per_step} of the 512 problems x 2 time steps, "
+                                   f"{cores} worker processes (C++ restatement of the reference "
+                                   "Fortran path, which cannot be compiled here)"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
 
 
+# ---- our arm -----------------------------------------------------------------
+
+def solve_batch(BB, problems, precision, device, want_q=False, q0s=None):
+    """Submits every problem (device-side initial state unless q0s is given),
+    runs the batch to completion and collects; returns (results, stats)."""
+    with BB.Batch(2, precision=precision, max_slots=len(problems), device=device) as b:
+        slots = []
+        for i, p in enumerate(problems):
+            s = b.submit(p, q0s[i]) if q0s is not None else b.submit_seeded(p)
+            slots.append(s)
+        b.run()
+        st = b.stats()
+        res = [b.collect(s, want_q=want_q) for s in slots]
+    return res, st
+
+
 def run_ours(args, world, rank, local):
     import numpy as np
     import torch
     import bsam_b200 as B
+    from bsam_b200 import batch as BB
     from bsam_b200 import build as BLD
+    from bsam_b200 import serve as SV
     from bsam_b200 import workloads as W
 
     BLD.build()
     torch.cuda.set_device(local)
-    prob = W.config3(nsteps=args.warmup + args.steps)
-    solver = B.Solver(prob, device=local)
-    stream = torch.cuda.ExternalStream(solver.stream(), device=local)
-    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=f"cuda:{local}")
+    problems = shard_problems(rank)
+    steps_per_bench_step = sum(p.nsteps for p in problems)
+
+    batch = BB.Batch(2, precision=BB.PREC_MIXED, max_slots=NPROB, device=local)
+    stream = torch.cuda.ExternalStream(batch.stream(), device=local)
+
+    def one_step(timed_events=None):
+        slots = [batch.submit_seeded(p) for p in problems]
+        batch.sync()
+        if timed_events is not None:
+            timed_events[0].record(stream)
+        batch.run()
+        if timed_events is not None:
+            timed_events[1].record(stream)
+        nv = 0
+        conv = True
+        for s in slots:
+            r = batch.collect(s, want_q=False)
+            nv += int(r["nvcycles"].sum())
+            conv = conv and int(r["converged"].min()) == 1
+        return nv, conv
 
     for _ in range(args.warmup):
-        solver.step()
+        one_step()
     torch.cuda.synchronize()
 
-    def flush_l2():
-        with torch.cuda.stream(stream):
-            flush.fill_(1.0)
-
-    # ---- device-resident timed region ----
+    # ---- device-timed region: inputs resident (drawn on the device at
+    # submission, before the timed interval); every step solves all problems.
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
            for _ in range(args.steps)]
-    nvc = []
-    launches0 = solver.stats()["launches"]
+    ticks0 = batch.stats()["ticks"]
     clk = ClockSampler(local)
     clk.start()
     barrier(world)
     torch.cuda.synchronize()
-    t_wall0 = time.perf_counter()
     t_ep0 = time.time()
+    nvc, conv_all = [], True
     for s in range(args.steps):
-        flush_l2()
-        evs[s][0].record(stream)
-        nv, res, conv = solver.step()
-        evs[s][1].record(stream)
+        nv, conv = one_step(evs[s])
         nvc.append(nv)
+        conv_all = conv_all and conv
     torch.cuda.synchronize()
     t_ep1 = time.time()
     barrier(world)
-    t_wall = time.perf_counter() - t_wall0
-    # Keep the GPU busy with further steps (untimed) until the sampler has seen
-    # at least half a second of load; used only if the timed region is too
-    # short to hold a 20 ms sample.
-    while time.time() - t_ep0 < 0.5:
-        solver.step()
-    torch.cuda.synchronize()
-    t_ep2 = time.time()
     clk.stop()
     clocks = clk.summary(t_ep0, t_ep1)
-    clocks["window"] = "timed region"
-    if clocks["samples"] == 0:
-        clocks = clk.summary(t_ep0, t_ep2)
-        clocks["window"] = "timed region + continued steps of the same workload"
+    clocks["window"] = "timed region (submission + solve + collect loop)"
     step_ms = [a.elapsed_time(b) for a, b in evs]
     dev_s = sum(step_ms) / 1e3
     dev_s_max = allmax(world, dev_s)
-    launches = solver.stats()["launches"] - launches0
-    value = world * args.steps / dev_s_max
+    stats = batch.stats()
+    ticks = stats["ticks"] - ticks0
+    kpt = stats["kernels_per_tick"]
+    value = world * args.steps * steps_per_bench_step / dev_s_max
 
-    # ---- smoother stage timing (roofline): CUDA events around every
-    # finest-level smoothing stage, on a separate pass of the same steps ----
-    solver.profile(True)
-    for s in range(min(args.steps, 3)):
-        flush_l2()
-        solver.step()
-    torch.cuda.synchronize()
-    st = solver.stats()
-    solver.profile(False)
-
-    # ---- end-to-end through the C ABI with pinned host buffers ----
-    qhost = torch.empty(int(np.prod(solver.qshape)), dtype=torch.float64, pin_memory=True)
-    qh = qhost.numpy().reshape(solver.qshape, order="F")
-    solver.get_q_into(qh)
-    e2e_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-              for _ in range(args.steps)]
-    barrier(world)
-    torch.cuda.synchronize()
-    for s in range(args.steps):
-        flush_l2()
-        e2e_ev[s][0].record(stream)
-        solver.put_q_async_safe(qh)
-        solver.step()
-        solver.get_q_into(qh)
-        e2e_ev[s][1].record(stream)
-    torch.cuda.synchronize()
-    e2e_s = allmax(world, sum(a.elapsed_time(b) for a, b in e2e_ev) / 1e3)
-    qbytes = int(qh.nbytes)
-
+    # ---- smoother roofline: finest-depth stages timed with events in the
+    # first two ticks (every problem running) -----------------------------------
+    slots = [batch.submit_seeded(p) for p in problems]
+    batch.profile(True)
+    batch.advance(2)
+    batch.sync()
+    pst = batch.stats()
+    batch.profile(False)
+    batch.run()
+    for s in slots:
+        batch.collect(s, want_q=False)
     peak, peak_kind = peaks()
-    achieved = (st["smooth_bytes"] / (st["smooth_ms"] / 1e3) / 1e9) if st["smooth_ms"] > 0 else None
-    per_stage_ms = st["smooth_ms"] / max(st["smooth_stages"], 1)
+    stage_ms = pst["smooth_ms"] / max(pst["smooth_stages"], 1)
+    stage_bytes = pst["smooth_bytes"] / max(pst["smooth_stages"], 1)
+    achieved = stage_bytes / (stage_ms / 1e3) / 1e9 if stage_ms > 0 else None
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tfile):
         try:
-            traffic = json.load(open(tfile)).get("relax_stage_bytes_128cubed_fp64")
+            t = json.load(open(tfile))
+            traffic = t["kb_smooth2_f32_bytes_per_cell"] * t_cells(problems)
         except Exception:
             traffic = None
+
+    # ---- end to end through the public API, host buffers both ways: every
+    # step submits each problem's q0 from host memory (staged through the
+    # engine's pinned ring), solves, and reads every final q back ------------
+    q0s = [p.q0() for p in problems]
+    h2d = sum(int(q.nbytes) for q in q0s)
+    e2e_t, d2h = [], 0
+    barrier(world)
+    for s in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        slots = [batch.submit(p, q) for p, q in zip(problems, q0s)]
+        batch.run()
+        res = [batch.collect(sl, want_q=True) for sl in slots]
+        e2e_t.append(time.perf_counter() - t0)
+        d2h = sum(int(r["q"].nbytes) for r in res)
+    e2e_s = allmax(world, sum(e2e_t))
+    batch.close()
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * dev_s_max / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "precision": "fp64", "parallelism": f"replicas x{world}",
-                   "l2": "flushed (256 MB write) before every timed step",
-                   "vcycles_per_step": statistics.mean(nvc),
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "problems_per_gpu": NPROB,
+                   "time_steps_per_bench_step": steps_per_bench_step,
+                   "precision": "mixed (FP32 working levels, FP64 defect/update/bottom)",
+                   "parallelism": f"independent batches x{world}",
+                   "l2": "inputs larger than L2 (about 1.4 GB resident per batch)",
+                   "vcycles_per_bench_step": statistics.mean(nvc),
                    "vcycles_per_s": world * sum(nvc) / dev_s_max,
-                   "wall_s_timed_region": t_wall},
-        "roofline": {"bound": "hbm", "kernel": "finest-level smoothing stage (nu=2 red-black "
-                     "sweeps = 4 k_relax launches)",
+                   "ticks_per_bench_step": ticks / args.steps,
+                   "all_converged": conv_all},
+        "roofline": {"bound": "hbm", "kernel": "kb_smooth2<float> (fused finest-depth "
+                     "smoothing stage: nu=2 red-black sweeps of every problem, one launch)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None,
                      "peak_source": peak_kind, "traffic": traffic,
-                     "algorithmic_bytes_per_stage": st["smooth_bytes"] / max(st["smooth_stages"], 1),
-                     "stage_ms": per_stage_ms},
-        "e2e": {"value": world * args.steps / e2e_s, "unit": UNIT,
-                "h2d_bytes_per_step": qbytes, "d2h_bytes_per_step": qbytes},
-        "gpu_launches": int(launches),
+                     "algorithmic_bytes_per_launch": stage_bytes, "launch_ms": stage_ms},
+        "e2e": {"value": world * args.steps * steps_per_bench_step / e2e_s, "unit": UNIT,
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "path": "bsam_batch_submit (host q0) + run + collect (host q), host wall "
+                        "clock, max over ranks"},
+        "gpu_launches": int(ticks * kpt + 2 * NPROB * args.steps),
         "clocks": clocks,
     }
+
+    if world == 1 and rank == 0 and not args.quick:
+        extra = {}
+        # FP64 batched form of the same problems (device-timed like the headline).
+        with BB.Batch(2, precision=BB.PREC_FP64, max_slots=NPROB, device=local) as b64:
+            st64 = torch.cuda.ExternalStream(b64.stream(), device=local)
+            for rep in range(2):
+                slots = [b64.submit_seeded(p) for p in problems]
+                b64.sync()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(st64)
+                b64.run()
+                e1.record(st64)
+                torch.cuda.synchronize()
+                for s in slots:
+                    b64.collect(s, want_q=False)
+            extra["fp64_batched_steps_per_s"] = steps_per_bench_step / (e0.elapsed_time(e1) / 1e3)
+        # Plain FP64 form, one problem at a time (single-problem library), on a
+        # sample of the problems (every 16th).
+        tt, st_ = 0.0, 0
+        for p in problems[::16]:
+            with B.Solver(p, precision=B.PREC_FP64) as sv:
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                sv.run(p.nsteps, keep_steps=False)
+                tt += time.perf_counter() - t0
+                st_ += p.nsteps
+        extra["fp64_one_at_a_time_steps_per_s"] = st_ / tt
+        extra["speedup_vs_fp64_one_at_a_time"] = value / extra["fp64_one_at_a_time_steps_per_s"]
+        # 3D 128^3 single problem, both forms (config 3): 5 time steps through
+        # the C++ host driver, host wall clock.
+        for name, prec in (("fp64", B.PREC_FP64), ("mixed", B.PREC_MIXED)):
+            prob = W.config3(nsteps=6)
+            with B.Solver(prob, precision=prec) as sv:
+                sv.run(1, keep_steps=False)
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                sv.run(5, keep_steps=False)
+                extra[f"cfg3_128cubed_{name}_steps_per_s"] = 5 / (time.perf_counter() - t0)
+        # Served form: one rate point of the Poisson request stream.
+        stream_ = W.config5(120, 200.0)
+        with SV.Server(pool_bytes=32 << 30, max_slots=256, ticks=4) as srv:
+            reqs = srv.serve(stream_)
+        extra["served_rate_200"] = SV.summarize(reqs)
+        line["forms"] = extra
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()
-    solver.close()
     if rank == 0:
         print(json.dumps(line), flush=True)
     return 0
 
 
+def run_case(args):
+    """Small fixed cases for ncu captures (no timing is reported):
+    smooth2-small  128 problems of 256^2, mixed, one eager tick;
+    ticks          the full 512-problem workload, mixed, three eager ticks."""
+    from bsam_b200 import batch as BB
+    from bsam_b200 import build as BLD
+    from bsam_b200 import workloads as W
+    BLD.build()
+    if args.case == "smooth2-small":
+        probs = [W.seeded(2, 256, 0.01, 10, seed=500 + p, cbar=0.5, amp=0.025) for p in range(128)]
+        nticks = 1
+    else:
+        probs = W.config4(nprob=NPROB, nsteps=NSTEPS)
+        nticks = 3
+    with BB.Batch(2, precision=BB.PREC_MIXED, max_slots=len(probs)) as b:
+        for p in probs:
+            assert b.submit_seeded(p) is not None
+        b.sync()
+        b.set_tuning(eager=1)
+        b.advance(nticks)
+        b.sync()
+        print(json.dumps({"case": args.case, "ticks": b.stats()["ticks"]}), flush=True)
+    return 0
+
+
+def t_cells(problems) -> int:
+    """Cells of the finest fused depth over the batch (problems above the
+    bottom kernel's size)."""
+    return sum(p.mx[0] * p.mx[1] for p in problems if p.mx[0] * p.mx[1] > 4096)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--quick", action="store_true", help="skip the side-by-side forms")
+    ap.add_argument("--case", choices=["smooth2-small", "ticks"], default=None,
+                    help="run a fixed small case for a profiler capture and exit")
     args = ap.parse_args()
-    world, rank, local = dist_setup(args) if args.impl == "ours" else (
-        int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")),
-        int(os.environ.get("LOCAL_RANK", "0")))
+    if args.case:
+        return run_case(args)
+    if args.impl == "reference":
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        rank = int(os.environ.get("RANK", "0"))
+        return run_reference(args, world, rank)
+    world, rank, local = dist_setup()
     try:
-        if args.impl == "reference":
-            return run_reference(args, world, rank)
         return run_ours(args, world, rank, local)
     finally:
-        if world > 1 and args.impl == "ours":
+        if world > 1:
             import torch.distributed as dist
             dist.destroy_process_group()
 

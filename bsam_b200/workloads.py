@@ -181,14 +181,15 @@ BATCH_SIDES = (64, 96, 128, 192, 256)
 
 def config4(nprob: int = 512, nsteps: int = 10, seed: int = 4) -> list:
     """Batched: sides uniform over BATCH_SIDES, eps ~ U(0.005, 0.02),
-    phi0 = m + U(-0.05, 0.05) with m ~ U(-0.3, 0.3); dt = 1e-4; residual 1e-8."""
+    phi0 = m + 0.05 U(-1, 1) with m ~ U(-0.3, 0.3), i.e. in the reference's
+    variable c0 = (1 + m)/2 + 0.025 U(-1, 1) (seeded form, drawn per problem
+    from its own stream); dt = 1e-4; residual 1e-8."""
     sel = splitmix64(seed, nprob) % np.uint64(len(BATCH_SIDES))
     eps = uniform(seed + 1, nprob, 0.005, 0.02)
     mean = uniform(seed + 2, nprob, -0.3, 0.3)
     out = []
     for p in range(nprob):
         n = BATCH_SIDES[int(sel[p])]
-        phi = mean[p] + uniform(1000003 * (seed + 1) + p, n * n, -0.05, 0.05)
-        out.append(Problem(ndims=2, mx=(n, n, 1), eps=float(eps[p]), dt=1e-4,
-                           nsteps=nsteps, qerrortol=1e-8, c0=0.5 * (1.0 + phi)))
+        out.append(seeded(2, n, float(eps[p]), nsteps, seed=1000003 * (seed + 1) + p,
+                          cbar=0.5 * (1.0 + float(mean[p])), amp=0.025))
     return out

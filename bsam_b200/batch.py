@@ -23,8 +23,12 @@ ERR_NOMEM = -3
 class BatchParams(ctypes.Structure):
     _fields_ = [("ndims", ctypes.c_int32), ("precision", ctypes.c_int32),
                 ("nsmoothingpasses", ctypes.c_int32), ("maxvcycles", ctypes.c_int32),
-                ("max_slots", ctypes.c_int32), ("pad_", ctypes.c_int32),
+                ("max_slots", ctypes.c_int32), ("bottom_cells", ctypes.c_int32),
                 ("pool_bytes", ctypes.c_int64), ("qerrortol", ctypes.c_double)]
+
+# Default bottom kernel size of a batch (bsam_batch.cu DEFAULT_BOTTOM_CELLS);
+# a single-problem Solver with bottom_cells=BOTTOM_CELLS computes the same bits.
+BOTTOM_CELLS = 1024
 
 
 def _host_grid_type():
@@ -122,10 +126,11 @@ class Batch:
 
     def __init__(self, ndims: int, precision: int = PREC_MIXED, max_slots: int = 64,
                  pool_bytes: int = 0, qerrortol: float = 1e-8, maxvcycles: int = 20,
-                 nsmoothingpasses: int = 2, device: int = 0, grid_ctas: int = 0):
+                 nsmoothingpasses: int = 2, device: int = 0, grid_ctas: int = 0,
+                 bottom_cells: int = 0):
         L = _lib()
         bp = BatchParams(ndims=ndims, precision=precision, nsmoothingpasses=nsmoothingpasses,
-                         maxvcycles=maxvcycles, max_slots=max_slots, pad_=0,
+                         maxvcycles=maxvcycles, max_slots=max_slots, bottom_cells=bottom_cells,
                          pool_bytes=pool_bytes, qerrortol=qerrortol)
         h = ctypes.c_void_p()
         _check(L.bsam_batch_create(ctypes.byref(h), device, ctypes.byref(bp)), None,

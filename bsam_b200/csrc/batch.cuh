@@ -100,9 +100,15 @@ __global__ void __launch_bounds__(BLOCK_THREADS)
   }
 }
 
-// Bottom chains (FP64 in both forms), one CTA per chain at a time.
+// Bottom chains (FP64 in both forms), one CTA per chain at a time.  256
+// threads at up to 64 registers: four chains per SM run at once, so a batch
+// of a few hundred problems has all its chains resident in one wave (cell
+// updates within a phase are independent, so the thread count does not
+// change any result).
+constexpr int BATCH_BOTTOM_THREADS = 256;
+
 template <int D>
-__global__ void __launch_bounds__(BOTTOM_THREADS)
+__global__ void __launch_bounds__(BATCH_BOTTOM_THREADS, 4)
     kb_bottom(const DevPatch* __restrict__ PT, const Item* __restrict__ tops,
               const int* __restrict__ count, int nu) {
   __shared__ int chain[BOTTOM_MAX_DEPTH];

@@ -18,9 +18,9 @@
 // Records of one slot (local index): FP64 form 0 = root (level 0), l =
 // level -l; mixed form 0 = FP64 master, 1 = working twin of the root,
 // l + 1 = level -l.  Depth d of the V-cycle is level -d.  Depths whose
-// levels have more than BOTTOM_MAX_CELLS cells run grid kernels ("top"
-// depths); the rest run inside k_bottom's chain, as in the single-problem
-// engine, and are FP64 in both forms.
+// levels have more than bottom_cells cells run grid kernels ("top" depths);
+// the rest run inside the bottom kernel's chain, as in the single-problem
+// engine with the same bottom_cells, and are FP64 in both forms.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
@@ -45,8 +45,9 @@ namespace {
 constexpr int RMAX = 16;  // records per slot
 constexpr int NMAPS = 7;  // TMA maps per fused record
 constexpr int MAXD = 8;   // top depths
-// Mixed form: levels at or below this size stay FP64 (as in bsam_gpu.cu).
-constexpr int64_t FP64_CELLS = 4096;
+// Default bottom_cells: levels of at most this many cells run in the bottom
+// kernel (in FP64 in both forms, as bsam_gpu.cu does with the same value).
+constexpr int DEFAULT_BOTTOM_CELLS = 1024;
 // Lists: master tiles; bottom-chain tops; per top depth d: tiles of every
 // record (correction), footprint tiles (restriction / coarse load), tiles of
 // records smoothed per colour pass, fused-stage tiles.
@@ -334,8 +335,9 @@ int plan_slot(bsam_batch* b, const bsam_batch_problem* pr, int rec0, char* base,
   const int nrec = np + (mixed ? 1 : 0);
   // Depth of the first bottom level.
   int ntop = np;
+  const int64_t bcells = b->bp.bottom_cells;
   for (int l = 0; l < np; ++l)
-    if (cells_of(desc[l].mx, nd) <= BOTTOM_MAX_CELLS) {
+    if (cells_of(desc[l].mx, nd) <= bcells) {
       ntop = l;
       break;
     }
@@ -367,7 +369,7 @@ int plan_slot(bsam_batch* b, const bsam_batch_problem* pr, int rec0, char* base,
     P.newstep = (r == 0) ? 1 : 0;
     P.twin = is_master_only ? rec0 + 1 : -1;
     const int64_t ncell = cells_of(P.n, nd);
-    P.prec = (!mixed || is_master_only || ncell <= FP64_CELLS) ? PREC_F64 : PREC_F32;
+    P.prec = (!mixed || is_master_only || ncell <= bcells) ? PREC_F64 : PREC_F32;
     for (int n = 0; n < 3; ++n) {
       P.cn[n] = 1;
       P.off[n] = 0;
@@ -588,7 +590,7 @@ void tick_t(bsam_batch* b, cudaGraphConditionalHandle handle, int in_graph) {
   {
     const int cap = std::max(1, L[L_TOPS].cap);
     const int gb = std::max(1, std::min(cap, 4 * b->nsm));
-    kb_bottom<D><<<gb, BOTTOM_THREADS, 0, s>>>(pt, L[L_TOPS].d, cnt + L_TOPS, nu);
+    kb_bottom<D><<<gb, BATCH_BOTTOM_THREADS, 0, s>>>(pt, L[L_TOPS].d, cnt + L_TOPS, nu);
     ++n;
   }
   for (int d = b->cap_depth - 1; d >= 0; --d) {
@@ -726,7 +728,8 @@ int bsam_batch_create(bsam_batch** out, int device, const bsam_batch_params* p) 
   if (!out || !p) return BSAM_ERR_ARG;
   *out = nullptr;
   if (p->ndims < 2 || p->ndims > 3 || p->nsmoothingpasses < 1 || p->maxvcycles < 1 ||
-      p->max_slots < 1 || p->max_slots > (1 << 20) / RMAX || p->pool_bytes < 0)
+      p->max_slots < 1 || p->max_slots > (1 << 20) / RMAX || p->pool_bytes < 0 ||
+      p->bottom_cells < 0 || p->bottom_cells > BOTTOM_MAX_CELLS)
     return BSAM_ERR_ARG;
   if (p->precision != BSAM_PREC_FP64 && p->precision != BSAM_PREC_MIXED)
     return BSAM_ERR_UNSUPPORTED;
@@ -737,6 +740,7 @@ int bsam_batch_create(bsam_batch** out, int device, const bsam_batch_params* p) 
   bsam_batch* b = new bsam_batch();
   b->device = device;
   b->bp = *p;
+  if (b->bp.bottom_cells == 0) b->bp.bottom_cells = DEFAULT_BOTTOM_CELLS;
   b->mixed = p->precision == BSAM_PREC_MIXED;
   cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, device);
   const int ns = p->max_slots;

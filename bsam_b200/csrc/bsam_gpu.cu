@@ -534,9 +534,10 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
     }
     if (h->bottom_level - minlevel + 1 > BOTTOM_MAX_DEPTH) h->bottom_level = -1000;
   }
-  // Mixed form: levels at or below this size stay FP64 (the bottom of the
-  // V-cycle, including the coarsest level).
-  const int64_t fp64_cells = std::max<int64_t>(MIXED_FP64_CELLS, std::max(bmax, 0));
+  // Mixed form: levels at or below this size stay FP64 -- the levels the
+  // bottom kernel runs, including the coarsest (4096 cells when the bottom
+  // kernel is switched off).
+  const int64_t fp64_cells = bmax > 0 ? (int64_t)bmax : MIXED_FP64_CELLS;
 
   // Records: the caller's patches, then one twin per finest-level patch in
   // the mixed form.

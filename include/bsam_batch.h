@@ -51,7 +51,8 @@ typedef struct {
   int32_t nsmoothingpasses; /* rundata nsmoothingpasses (2) */
   int32_t maxvcycles;       /* per time step */
   int32_t max_slots;        /* problems resident at once */
-  int32_t pad_;
+  int32_t bottom_cells;     /* levels of at most this many cells run in the one-CTA
+                               bottom kernel, in FP64 (0 = 1024; at most 4096) */
   int64_t pool_bytes;       /* device memory for problem state; 0 = half of free */
   double qerrortol;
 } bsam_batch_params;

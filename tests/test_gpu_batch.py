@@ -28,7 +28,8 @@ def make(n, seed, nsteps=3, eps=0.01, ndims=2, mean=0.0, tol=1e-8):
 
 
 def single(prob, precision):
-    with B.Solver(prob, precision=precision) as s:
+    """The single-problem library with the batch's bottom-kernel size."""
+    with B.Solver(prob, precision=precision, bottom_cells=BB.BOTTOM_CELLS) as s:
         r = s.run(prob.nsteps)
     return r
 

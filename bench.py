@@ -128,11 +128,13 @@ def barrier(world):
 
 
 def allmax(world, x: float) -> float:
+    """Max over ranks (the timing rule for multi-GPU numbers)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 

@@ -1,0 +1,135 @@
+"""Fixed block-structured AMR hierarchies for the V-cycle (2D).
+
+The reference builds its hierarchy by tagging and Berger-Rigoutsos
+clustering every time step (lib/bsamroutines.f90:939-1241, 1352-1579); the
+multigrid solve itself (MultigridIterations) only reads the resulting patch
+records.  This module builds such records for a hierarchy given box by box:
+the root grid with its below-root levels (as RootInit / InitSeed do), and
+refined patches on levels 1, 2, ... with their parent, their index box in
+the parent (mbounds), their global index box (mglobal) and their face codes
+(999 = internal face, else the root's physical code) -- the fields of
+nodeinfo (lib/nodeinfodef.f90:124-219) that bsam_gpu_set_hierarchy takes.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+
+import numpy as np
+
+from . import workloads as W
+
+INTERNAL = 999
+
+
+@dataclasses.dataclass
+class Hierarchy:
+    ndims: int
+    descs: list            # patch records, ApplyOnLevel order within a level
+    q0s: list              # q (with ring) of every patch on a level >= 0, descs order
+    dt: float
+    eps: float
+    qerrortol: float
+    alpha: float = 1.0
+    maxvcycles: int = 20
+    nsmoothingpasses: int = 2
+
+    @property
+    def finestlevel(self) -> int:
+        return max(d["level"] for d in self.descs)
+
+    def state_patches(self) -> list:
+        """Indices of the patches on levels >= 0 (the order of q0s)."""
+        return [i for i, d in enumerate(self.descs) if d["level"] >= 0]
+
+
+def _desc(level, parent, mx, mbounds, mglobal, mthbc, dx, xlower):
+    return {"level": level, "parent": parent, "mx": list(mx) + [1] * (3 - len(mx)),
+            "mbounds": [list(b) for b in mbounds] + [[1, 1]] * (3 - len(mbounds)),
+            "mglobal": [list(b) for b in mglobal] + [[1, 1]] * (3 - len(mglobal)),
+            "mthbc": list(mthbc) + [1] * (6 - len(mthbc)), "dx": dx,
+            "xlower": list(xlower) + [0.0] * (3 - len(xlower))}
+
+
+def build(n_root: int, boxes: list, eps: float, dt: float = 5e-5, qerrortol: float = 1e-9,
+          mthbc: int = 1, minlevel: int = 1, seed: int = 2, field: str = "drop",
+          maxvcycles: int = 20) -> Hierarchy:
+    """2D hierarchy on [0,1]^2: an n_root^2 root, its below-root levels
+    (automatic minlevel: halve while even, at most 10 times), and refined
+    patches `boxes` = [(level, (i0, j0), (nx, ny)), ...] with (i0, j0) the
+    1-based global index of the patch's first cell on its level (odd) and
+    even sizes.  Each patch's parent is the patch of the level below that
+    contains its footprint (the first one listed).
+
+    Initial composition (field "drop", as the AMR benchmark configuration):
+    phi0 = tanh((0.25 - r)/(sqrt(2) eps)) + 1e-3 U(-1, 1) (seeded per
+    patch), c0 = (1 + phi0)/2, mu0 from the operator (workloads.initial_q)."""
+    nd = 2
+    h0 = 1.0 / n_root
+    descs = []
+    # Root (patch 0) and the below-root chain (patch l = level -l).
+    nlev = 0
+    if minlevel == 1:
+        m = n_root
+        while m % 2 == 0 and nlev < 10:
+            m //= 2
+            nlev += 1
+    else:
+        nlev = -minlevel
+    sizes = [n_root // (2 ** l) for l in range(nlev + 1)]
+    for l in range(nlev + 1):
+        n = sizes[l]
+        parent = l + 1 if l < nlev else -1
+        mb = [(1, n // 2)] * 2 if l < nlev else [(1, n)] * 2
+        descs.append(_desc(-l, parent, (n, n), mb, [(1, n), (1, n)], [mthbc] * 4,
+                           h0 * (2 ** l), (0.0, 0.0)))
+    # Refined patches.
+    for (level, lo, size) in boxes:
+        if level < 1 or any(x % 2 == 0 for x in lo) or any(s % 2 for s in size):
+            raise ValueError("patch origin must be odd and its size even")
+        nglob = n_root * 2 ** level
+        glo = list(lo)
+        ghi = [lo[k] + size[k] - 1 for k in range(nd)]
+        if any(glo[k] < 1 or ghi[k] > nglob for k in range(nd)):
+            raise ValueError("patch outside the domain")
+        foot_lo = [(glo[k] + 1) // 2 for k in range(nd)]
+        foot_hi = [ghi[k] // 2 for k in range(nd)]
+        parent = None
+        for pi, d in enumerate(descs):
+            if d["level"] != level - 1:
+                continue
+            if all(d["mglobal"][k][0] <= foot_lo[k] and foot_hi[k] <= d["mglobal"][k][1]
+                   for k in range(nd)):
+                parent = pi
+                break
+        if parent is None:
+            raise ValueError("no parent patch contains the footprint")
+        pg = descs[parent]["mglobal"]
+        mb = [(foot_lo[k] - pg[k][0] + 1, foot_hi[k] - pg[k][0] + 1) for k in range(nd)]
+        codes = []
+        for k in range(nd):
+            codes.append(mthbc if glo[k] == 1 else INTERNAL)
+            codes.append(mthbc if ghi[k] == nglob else INTERNAL)
+        h = h0 / (2 ** level)
+        descs.append(_desc(level, parent, size, mb, [(glo[k], ghi[k]) for k in range(nd)],
+                           codes, h, ((glo[0] - 1) * h, (glo[1] - 1) * h)))
+    # Initial states.
+    q0s = []
+    for i, d in enumerate(descs):
+        if d["level"] < 0:
+            continue
+        mx = d["mx"]
+        h = d["dx"]
+        xs = d["xlower"][0] + (np.arange(mx[0]) + 0.5) * h
+        ys = d["xlower"][1] + (np.arange(mx[1]) + 0.5) * h
+        X, Y = np.meshgrid(xs, ys, indexing="ij")
+        if field == "drop":
+            r = np.sqrt((X - 0.5) ** 2 + (Y - 0.5) ** 2)
+            phi = np.tanh((0.25 - r) / (math.sqrt(2.0) * eps))
+        else:
+            phi = 0.1 * np.sin(2 * math.pi * X) * np.cos(2 * math.pi * Y)
+        noise = W.uniform(seed * 1000 + i, mx[0] * mx[1], -1.0, 1.0).reshape(mx[:2], order="F")
+        c0 = 0.5 * (1.0 + (phi + 1e-3 * noise))
+        q0s.append(W.initial_q(nd, tuple(mx), c0.ravel(order="F"), h, eps, 1.0))
+    return Hierarchy(ndims=nd, descs=descs, q0s=q0s, dt=dt, eps=eps, qerrortol=qerrortol,
+                     maxvcycles=maxvcycles)

@@ -415,11 +415,190 @@ int SetBC(const Ctx& c, Patch& p) {
   return SetBC3D(p.q, p.mx, p.nrvars, p.mthbc);
 }
 
-// SetGhost (boundary.f90:58-89).  Only root and below-root levels exist in
-// the uniform configuration, so the coarse-fine interpolation and sibling
-// exchange branches (level > rootlevel) are not reached.
-int SetGhost(Ctx& c, int level, int /*ipass*/) {
+// Coefficients of the Boundary module (boundary.f90:45-54).  Declared
+// `real`; the reference builds with -fdefault-real-8 (makefile:85), so they
+// are these FP64 quotients.
+constexpr double kA1 = -(1.0 / 5.0), kA2 = 2.0 / 3.0, kA3 = 8.0 / 15.0;
+constexpr double kB1 = 5.0 / 32.0, kB2 = 15.0 / 16.0, kB3 = -(3.0 / 32.0);
+
+// Interpolate2D (boundary.f90:135-323), mbc = 1: ghosts of a fine patch on
+// its internal faces (codes 2 and 999) from two fine cells and one coarse
+// value along a diagonal; ipass 1 = red, 2 = black, 0 = both.  Corners are
+// set whatever the face codes are (SetBC overwrites the physical ones).
+// Every statement reads interior fine cells and coarse cells only.
+void Interpolate2D(FArr& qf, const FArr& qc, const int* mx, int nv, const int mb[3][2],
+                   const int* mthbc, int ipass) {
+  const int m1 = mx[0], m2 = mx[1];
+  const int b11 = mb[0][0], b12 = mb[0][1], b21 = mb[1][0], b22 = mb[1][1];
+  const bool red = ipass == 1 || ipass == 0, black = ipass == 2 || ipass == 0;
+  auto Q = [&](int i, int j, int v) -> double& { return qf(i, j, 1, v); };
+  auto C = [&](int i, int j, int v) { return qc(i, j, 1, v); };
+  for (int v = 1; v <= nv; ++v) {
+    // Corners (boundary.f90:147-172).
+    if (red) {
+      Q(m1 + 1, m2 + 1, v) = kA1 * Q(m1 - 1, m2 - 1, v) + kA2 * Q(m1, m2, v) +
+                             kA3 * C(b12 + 1, b22 + 1, v);
+      Q(0, 0, v) = kA1 * Q(2, 2, v) + kA2 * Q(1, 1, v) + kA3 * C(b11 - 1, b21 - 1, v);
+    }
+    if (black) {
+      Q(m1 + 1, 0, v) = kA1 * Q(m1 - 1, 2, v) + kA2 * Q(m1, 1, v) + kA3 * C(b12 + 1, b21 - 1, v);
+      Q(0, m2 + 1, v) = kA1 * Q(2, m2 - 1, v) + kA2 * Q(1, m2, v) + kA3 * C(b11 - 1, b22 + 1, v);
+    }
+  }
+  auto internal = [](int code) { return code == 2 || code == 999; };
+  // A face's interior ghosts: the regular section of one colour plus the end
+  // ghost whose coarse value is the three-point fit (b1, b2, b3) along the
+  // face.  t counts the elements of the array section.
+  for (int v = 1; v <= nv; ++v) {
+    if (internal(mthbc[0])) {  // face 1 (boundary.f90:176-212)
+      if (red) {
+        for (int t = 0; 2 + 2 * t <= m2 - 2; ++t) {
+          const int j = 2 + 2 * t;
+          Q(0, j, v) = kA1 * Q(2, 4 + 2 * t, v) + kA2 * Q(1, 3 + 2 * t, v) +
+                       kA3 * C(b11 - 1, b21 + t, v);
+        }
+        Q(0, m2, v) = kA1 * Q(2, m2, v) + kA2 * Q(1, m2, v) +
+                      kA3 * (kB1 * C(b11 - 1, b22 + 1, v) + kB2 * C(b11 - 1, b22, v) +
+                             kB3 * C(b11 - 1, b22 - 1, v));
+      }
+      if (black) {
+        for (int t = 0; 3 + 2 * t <= m2 - 1; ++t) {
+          const int j = 3 + 2 * t;
+          Q(0, j, v) = kA1 * Q(2, 1 + 2 * t, v) + kA2 * Q(1, 2 + 2 * t, v) +
+                       kA3 * C(b11 - 1, b21 + 1 + t, v);
+        }
+        Q(0, 1, v) = kA1 * Q(2, 1, v) + kA2 * Q(1, 1, v) +
+                     kA3 * (kB1 * C(b11 - 1, b21 - 1, v) + kB2 * C(b11 - 1, b21, v) +
+                            kB3 * C(b11 - 1, b21 + 1, v));
+      }
+    }
+    if (internal(mthbc[1])) {  // face 2 (boundary.f90:214-250)
+      if (red) {
+        for (int t = 0; 3 + 2 * t <= m2 - 1; ++t) {
+          const int j = 3 + 2 * t;
+          Q(m1 + 1, j, v) = kA1 * Q(m1 - 1, 1 + 2 * t, v) + kA2 * Q(m1, 2 + 2 * t, v) +
+                            kA3 * C(b12 + 1, b21 + 1 + t, v);
+        }
+        Q(m1 + 1, 1, v) = kA1 * Q(m1 - 1, 1, v) + kA2 * Q(m1, 1, v) +
+                          kA3 * (kB1 * C(b12 + 1, b21 - 1, v) + kB2 * C(b12 + 1, b21, v) +
+                                 kB3 * C(b12 + 1, b21 + 1, v));
+      }
+      if (black) {
+        for (int t = 0; 2 + 2 * t <= m2 - 2; ++t) {
+          const int j = 2 + 2 * t;
+          Q(m1 + 1, j, v) = kA1 * Q(m1 - 1, 4 + 2 * t, v) + kA2 * Q(m1, 3 + 2 * t, v) +
+                            kA3 * C(b12 + 1, b21 + t, v);
+        }
+        Q(m1 + 1, m2, v) = kA1 * Q(m1 - 1, m2, v) + kA2 * Q(m1, m2, v) +
+                           kA3 * (kB1 * C(b12 + 1, b22 + 1, v) + kB2 * C(b12 + 1, b22, v) +
+                                  kB3 * C(b12 + 1, b22 - 1, v));
+      }
+    }
+    if (internal(mthbc[2])) {  // face 3 (boundary.f90:252-287)
+      if (red) {
+        for (int t = 0; 2 + 2 * t <= m1 - 2; ++t) {
+          const int i = 2 + 2 * t;
+          Q(i, 0, v) = kA1 * Q(4 + 2 * t, 2, v) + kA2 * Q(3 + 2 * t, 1, v) +
+                       kA3 * C(b11 + t, b21 - 1, v);
+        }
+        Q(m1, 0, v) = kA1 * Q(m1, 2, v) + kA2 * Q(m1, 1, v) +
+                      kA3 * (kB1 * C(b12 + 1, b21 - 1, v) + kB2 * C(b12, b21 - 1, v) +
+                             kB3 * C(b12 - 1, b21 - 1, v));
+      }
+      if (black) {
+        for (int t = 0; 3 + 2 * t <= m1 - 1; ++t) {
+          const int i = 3 + 2 * t;
+          Q(i, 0, v) = kA1 * Q(1 + 2 * t, 2, v) + kA2 * Q(2 + 2 * t, 1, v) +
+                       kA3 * C(b11 + 1 + t, b21 - 1, v);
+        }
+        Q(1, 0, v) = kA1 * Q(1, 2, v) + kA2 * Q(1, 1, v) +
+                     kA3 * (kB1 * C(b11 - 1, b21 - 1, v) + kB2 * C(b11, b21 - 1, v) +
+                            kB3 * C(b11 + 1, b21 - 1, v));
+      }
+    }
+    if (internal(mthbc[3])) {  // face 4 (boundary.f90:289-321)
+      if (red) {
+        for (int t = 0; 3 + 2 * t <= m1 - 1; ++t) {
+          const int i = 3 + 2 * t;
+          Q(i, m2 + 1, v) = kA1 * Q(1 + 2 * t, m2 - 1, v) + kA2 * Q(2 + 2 * t, m2, v) +
+                            kA3 * C(b11 + 1 + t, b22 + 1, v);
+        }
+        Q(1, m2 + 1, v) = kA1 * Q(1, m2 - 1, v) + kA2 * Q(1, m2, v) +
+                          kA3 * (kB1 * C(b11 - 1, b22 + 1, v) + kB2 * C(b11, b22 + 1, v) +
+                                 kB3 * C(b11 + 1, b22 + 1, v));
+      }
+      if (black) {
+        for (int t = 0; 2 + 2 * t <= m1 - 2; ++t) {
+          const int i = 2 + 2 * t;
+          Q(i, m2 + 1, v) = kA1 * Q(4 + 2 * t, m2 - 1, v) + kA2 * Q(3 + 2 * t, m2, v) +
+                            kA3 * C(b11 + t, b22 + 1, v);
+        }
+        Q(m1, m2 + 1, v) = kA1 * Q(m1, m2 - 1, v) + kA2 * Q(m1, m2, v) +
+                           kA3 * (kB1 * C(b12 + 1, b22 + 1, v) + kB2 * C(b12, b22 + 1, v) +
+                                  kB3 * C(b12 - 1, b22 + 1, v));
+      }
+    }
+  }
+}
+
+// GhostOverlap (boundary.f90:346-415), mbc = 1: each grid's ghost ring takes
+// the other grid's interior values where they overlap (corners included).
+void GhostOverlap(const Ctx& c, Patch& g1, Patch& g2) {
+  const int mbc = g2.mbc, nv = g1.nrvars, nd = c.ndims;
+  int mg1[3][2], mg2[3][2], ovg[3][2], ovg1[3][2], ovg2[3][2];
+  for (int n = 0; n < 3; ++n)
+    for (int s = 0; s < 2; ++s) {
+      mg1[n][s] = n < nd ? g1.mglobal[n][s] : 1;
+      mg2[n][s] = n < nd ? g2.mglobal[n][s] : 1;
+      ovg[n][s] = ovg1[n][s] = ovg2[n][s] = 1;
+    }
+  for (int n = 0; n < nd; ++n) {
+    ovg[n][0] = std::max(mg1[n][0] - mbc, mg2[n][0] - mbc);
+    ovg[n][1] = std::min(mg1[n][1] + mbc, mg2[n][1] + mbc);
+  }
+  for (int n = 0; n < nd; ++n)
+    if (ovg[n][1] - ovg[n][0] < 0) return;
+  for (int n = 0; n < nd; ++n) {
+    ovg1[n][0] = std::max(ovg[n][0], mg2[n][0]);
+    ovg1[n][1] = std::min(ovg[n][1], mg2[n][1]);
+    ovg2[n][0] = std::max(ovg[n][0], mg1[n][0]);
+    ovg2[n][1] = std::min(ovg[n][1], mg1[n][1]);
+  }
+  // grid1(ovg1 - mg1 + 1) = grid2(ovg1 - mg2 + 1), then the other way.
+  auto copy = [&](Patch& dst, const int (*mgd)[2], const Patch& src, const int (*mgs)[2],
+                  const int (*box)[2]) {
+    const int k0 = nd == 3 ? box[2][0] : 1, k1 = nd == 3 ? box[2][1] : 1;
+    for (int v = 1; v <= nv; ++v)
+      for (int k = k0; k <= k1; ++k)
+        for (int j = box[1][0]; j <= box[1][1]; ++j)
+          for (int i = box[0][0]; i <= box[0][1]; ++i) {
+            const int dk = nd == 3 ? k - mgd[2][0] + 1 : 1, sk = nd == 3 ? k - mgs[2][0] + 1 : 1;
+            dst.q(i - mgd[0][0] + 1, j - mgd[1][0] + 1, dk, v) =
+                src.q(i - mgs[0][0] + 1, j - mgs[1][0] + 1, sk, v);
+          }
+  };
+  // The transfers read interior cells only, so element order is immaterial.
+  copy(g1, mg1, g2, mg2, ovg1);
+  copy(g2, mg2, g1, mg1, ovg2);
+}
+
+// SetGhost (boundary.f90:58-89): above the root level, coarse-fine
+// interpolation on every grid (ApplyOnLevel order), then the sibling
+// exchange over all pairs (ApplyOnLevelPairs: each grid with every later
+// one), then the physical boundary conditions.  No periodic grids.
+int SetGhost(Ctx& c, int level, int ipass) {
   int err = 0;
+  if (level > Ctx::rootlevel) {
+    std::vector<Patch*>& L = c.on(level);
+    for (Patch* p : L) {
+      if (p->tobedeleted) continue;
+      if (c.ndims != 2) return -2;  // Interpolate3D is not restated
+      Interpolate2D(p->q, p->parent->q, p->mx, p->nrvars, p->mbounds, p->mthbc, ipass);
+    }
+    for (size_t a = 0; a < L.size(); ++a)
+      for (size_t b = a + 1; b < L.size(); ++b)
+        if (!L[a]->tobedeleted && !L[b]->tobedeleted) GhostOverlap(c, *L[a], *L[b]);
+  }
   for (Patch* p : c.on(level)) err |= SetBC(c, *p);
   return err;
 }
@@ -766,6 +945,58 @@ int BuildUniform(Ctx& c, const orc_params* p) {
   return 0;
 }
 
+// A hierarchy given patch by patch (the caller's ApplyOnLevel order within
+// each level): the nodeinfo fields the hot path reads, fields allocated.
+int BuildFromPatches(Ctx& c, const orc_params* p, int npatch, const orc_patch* d) {
+  if (p->ndims < 2 || p->ndims > 3 || p->errortype != 1 || npatch <= 0) return -1;
+  c.ndims = p->ndims;
+  c.dt = p->dt;
+  c.qerrortol = p->qerrortol;
+  c.alpha = p->alpha;
+  c.eps = p->eps;
+  c.eps2 = p->eps * p->eps;
+  c.maxvcycles = p->maxvcycles;
+  c.nsmoothingpasses = p->nsmoothingpasses;
+  c.errortype = p->errortype;
+  int lo = d[0].level, hi = d[0].level;
+  for (int i = 0; i < npatch; ++i) {
+    lo = std::min(lo, d[i].level);
+    hi = std::max(hi, d[i].level);
+  }
+  if (lo > 0 || hi < 0) return -2;
+  c.minlevel = lo;
+  c.finestlevel = hi;
+  c.levels.assign(hi - lo + 1, {});
+  std::vector<Patch*> made(npatch);
+  for (int i = 0; i < npatch; ++i) {
+    auto pt = std::make_unique<Patch>();
+    pt->level = d[i].level;
+    for (int n = 0; n < 3; ++n) {
+      pt->mx[n] = n < c.ndims ? d[i].mx[n] : 1;
+      for (int s = 0; s < 2; ++s) {
+        pt->mbounds[n][s] = n < c.ndims ? d[i].mbounds[n][s] : 1;
+        pt->mglobal[n][s] = n < c.ndims ? d[i].mglobal[n][s] : 1;
+      }
+      pt->dx[n] = d[i].dx;
+      pt->xlower[n] = d[i].xlower[n];
+    }
+    for (int f = 0; f < 6; ++f) pt->mthbc[f] = f < 2 * c.ndims ? d[i].mthbc[f] : 1;
+    AllocFields(c, *pt);
+    made[i] = pt.get();
+    c.on(pt->level).push_back(pt.get());
+    c.store.push_back(std::move(pt));
+  }
+  for (int i = 0; i < npatch; ++i) {
+    const int par = d[i].parent;
+    if (par >= npatch || (par < 0 && d[i].level != lo)) return -3;
+    if (par >= 0) {
+      if (d[par].level != d[i].level - 1) return -3;
+      made[i]->parent = made[par];
+    }
+  }
+  return 0;
+}
+
 // Wrap a flat Fortran-ordered array into an FArr with the given bounds.
 FArr wrap(int ndims, const int* lo, const int* hi, int nv, const double* src) {
   FArr a;
@@ -834,6 +1065,67 @@ int orc_run_uniform(const orc_params* p, const double* q0, int nsteps, double* q
     }
   }
   return 0;
+}
+
+int orc_run_hier(const orc_params* p, int npatch, const orc_patch* patches, const double* q0,
+                 int nsteps, double* q_out, int* nvcycles, double* resid_final) {
+  Ctx c;
+  int err = BuildFromPatches(c, p, npatch, patches);
+  if (err) return err;
+  // q of the patches on levels >= root, in input order, each with its ring.
+  auto each_state = [&](auto fn) {
+    size_t off = 0;
+    for (auto& up : c.store) {
+      Patch& pt = *up;
+      if (pt.level < Ctx::rootlevel) continue;
+      fn(pt, off);
+      off += pt.q.d.size();
+    }
+  };
+  each_state([&](Patch& pt, size_t off) {
+    std::memcpy(pt.q.d.data(), q0 + off, pt.q.d.size() * sizeof(double));
+  });
+  // Start (BSAMSolver, bsamroutines.f90:144-147) and every step: the ghosts
+  // of every level from the root up, as AMR(rootlevel) leaves them on an
+  // unchanged hierarchy; then FillDown once, CopyQToQold and
+  // MultigridIterations (TakeTimeSteps, bsamroutines.f90:648-723).
+  auto ghosts = [&]() {
+    for (int level = Ctx::rootlevel; level <= c.finestlevel; ++level)
+      if (SetGhost(c, level, 0)) return -9;
+    return 0;
+  };
+  if (ghosts()) return -9;
+  for (int level = c.minlevel; level <= c.finestlevel; ++level)
+    for (Patch* pp : c.on(level)) CopyQToQold(*pp);
+  bool firstamr = true;
+  for (int step = 0; step < nsteps; ++step) {
+    if (ghosts()) return -9;
+    if (firstamr) {
+      FillDown(c, false);
+      firstamr = false;
+    }
+    for (int level = c.minlevel; level <= c.finestlevel; ++level)
+      for (Patch* pp : c.on(level)) CopyQToQold(*pp);
+    double last = 0.0;
+    const int nv = MultigridIterations(c, &last, nullptr);
+    if (nvcycles) nvcycles[step] = nv;
+    if (resid_final) resid_final[step] = last;
+  }
+  if (q_out)
+    each_state([&](Patch& pt, size_t off) {
+      std::memcpy(q_out + off, pt.q.d.data(), pt.q.d.size() * sizeof(double));
+    });
+  return 0;
+}
+
+void orc_interpolate2d(const int* mx, int nv, const int* mbounds, const int* mthbc, int ipass,
+                       double* qf, const int* pmx, const double* qc) {
+  int lo[3] = {0, 0, 1}, hi[3] = {mx[0] + 1, mx[1] + 1, 1};
+  int plo[3] = {0, 0, 1}, phi[3] = {pmx[0] + 1, pmx[1] + 1, 1};
+  FArr F = wrap(2, lo, hi, nv, qf), C = wrap(2, plo, phi, nv, qc);
+  int mb[3][2] = {{mbounds[0], mbounds[1]}, {mbounds[2], mbounds[3]}, {1, 1}};
+  Interpolate2D(F, C, mx, nv, mb, mthbc, ipass);
+  std::memcpy(qf, F.d.data(), F.d.size() * sizeof(double));
 }
 
 void orc_relax_grid(int ndims, const int* mx, double h, double dt, double alpha, double eps,

@@ -50,6 +50,29 @@ int orc_run_uniform(const orc_params* p, const double* q0, int nsteps,
                     double* q_steps, int* nvcycles, double* resid_final,
                     double* resid_trace, double* mass);
 
+/* One patch of a given hierarchy (the nodeinfo fields the hot path reads,
+ * lib/nodeinfodef.f90:124-219); parent is an index into the same array. */
+typedef struct {
+  int32_t level, parent, mx[3], mbounds[3][2], mglobal[3][2], mthbc[6];
+  double dx, xlower[3];
+} orc_patch;
+
+/* Time stepping on a fixed hierarchy, AMR levels included (2D): every step
+ * SetGhost(level, 0) from the root up (what AMR(rootlevel) leaves on an
+ * unchanged hierarchy), FillDown(solution) on the first step, CopyQToQold,
+ * MultigridIterations.  p supplies the run parameters (its mx, mthbc,
+ * minlevel and bounds are not used).  q0 / q_out: q with ghost ring of every
+ * patch on a level >= 0, concatenated in array order.  Returns 0 or a
+ * negative code. */
+int orc_run_hier(const orc_params* p, int npatch, const orc_patch* patches,
+                 const double* q0, int nsteps, double* q_out, int* nvcycles,
+                 double* resid_final);
+
+/* Interpolate2D (boundary.f90:135-323) on a fine patch qf (0:mx+1)^2 x nv
+ * from its parent qc (0:pmx+1)^2 x nv; mbounds = {mb11, mb12, mb21, mb22}. */
+void orc_interpolate2d(const int* mx, int nv, const int* mbounds, const int* mthbc,
+                       int ipass, double* qf, const int* pmx, const double* qc);
+
 /* Resolved minimum level for the parameters (lib/bsamroutines.f90:287-301). */
 int orc_minlevel(const orc_params* p);
 

@@ -27,6 +27,14 @@ class OrcParams(ctypes.Structure):
     ]
 
 
+class OrcPatch(ctypes.Structure):
+    _fields_ = [
+        ("level", ctypes.c_int32), ("parent", ctypes.c_int32), ("mx", ctypes.c_int32 * 3),
+        ("mbounds", (ctypes.c_int32 * 2) * 3), ("mglobal", (ctypes.c_int32 * 2) * 3),
+        ("mthbc", ctypes.c_int32 * 6), ("dx", ctypes.c_double), ("xlower", ctypes.c_double * 3),
+    ]
+
+
 def build() -> str:
     """Compile the oracle with its Makefile (no-op when up to date)."""
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
@@ -58,6 +66,10 @@ def lib():
         L.orc_source.argtypes = [ctypes.c_int, ip, ctypes.c_double, dp, dp]
         L.orc_energy2d.argtypes = [ip, ctypes.c_double, ctypes.c_double, ctypes.c_double, dp]
         L.orc_energy2d.restype = ctypes.c_double
+        L.orc_run_hier.argtypes = [ctypes.POINTER(OrcParams), ctypes.c_int,
+                                   ctypes.POINTER(OrcPatch), dp, ctypes.c_int, dp, ip, dp]
+        L.orc_run_hier.restype = ctypes.c_int
+        L.orc_interpolate2d.argtypes = [ip, ctypes.c_int, ip, ip, ctypes.c_int, dp, ip, dp]
         _lib = L
     return _lib
 
@@ -88,6 +100,57 @@ def params_of(prob) -> OrcParams:
     p.alpha = prob.alpha
     p.eps = prob.eps
     return p
+
+
+def run_hier(hier, nsteps):
+    """Oracle time stepping on a fixed hierarchy (bsam_b200.amr.Hierarchy):
+    returns the final q of every patch on a level >= 0, V-cycles and final
+    residual per step."""
+    L = lib()
+    n = len(hier.descs)
+    arr = (OrcPatch * n)()
+    for i, d in enumerate(hier.descs):
+        o = arr[i]
+        o.level, o.parent, o.dx = d["level"], d["parent"], d["dx"]
+        for k in range(3):
+            o.mx[k] = d["mx"][k]
+            o.xlower[k] = d["xlower"][k]
+            for s in range(2):
+                o.mbounds[k][s] = d["mbounds"][k][s]
+                o.mglobal[k][s] = d["mglobal"][k][s]
+        for f in range(6):
+            o.mthbc[f] = d["mthbc"][f]
+    p = OrcParams()
+    p.ndims = hier.ndims
+    p.nsmoothingpasses = hier.nsmoothingpasses
+    p.maxvcycles = hier.maxvcycles
+    p.errortype = 1
+    p.dt, p.qerrortol, p.alpha, p.eps = hier.dt, hier.qerrortol, hier.alpha, hier.eps
+    q0 = np.concatenate([np.asfortranarray(q).ravel(order="F") for q in hier.q0s])
+    qout = np.zeros_like(q0)
+    nvc = np.zeros(nsteps, dtype=np.int32)
+    res = np.zeros(nsteps)
+    rc = L.orc_run_hier(ctypes.byref(p), n, arr, _dp(q0), nsteps, _dp(qout), _ip(nvc), _dp(res))
+    if rc != 0:
+        raise RuntimeError(f"orc_run_hier failed: {rc}")
+    out, off = [], 0
+    for q in hier.q0s:
+        out.append(qout[off:off + q.size].reshape(q.shape, order="F"))
+        off += q.size
+    return {"q": out, "nvcycles": nvc, "residual": res}
+
+
+def interpolate2d(qf, qc, mbounds, mthbc, ipass):
+    """Interpolate2D on copies of qf (0:mx+1)^2 x nv and qc (parent)."""
+    qf = np.array(qf, dtype=np.float64, order="F", copy=True)
+    qc = np.asfortranarray(qc, dtype=np.float64)
+    mx = np.array([qf.shape[0] - 2, qf.shape[1] - 2], dtype=np.int32)
+    pmx = np.array([qc.shape[0] - 2, qc.shape[1] - 2], dtype=np.int32)
+    mb = np.array(mbounds, dtype=np.int32)
+    bc = np.array(mthbc, dtype=np.int32)
+    lib().orc_interpolate2d(_ip(mx), qf.shape[2], _ip(mb), _ip(bc), ipass, _dp(qf), _ip(pmx),
+                            _dp(qc))
+    return qf
 
 
 def run_uniform(prob, nsteps=None, keep_steps=True, q0=None):

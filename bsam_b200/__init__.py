@@ -62,7 +62,7 @@ ABI_SYMBOLS = (
     "bsam_gpu_residual_trace", "bsam_gpu_mass", "bsam_gpu_destroy", "bsam_gpu_strerror",
     "bsam_gpu_last_error", "bsam_gpu_get_stream", "bsam_gpu_profile", "bsam_gpu_get_stats",
     "bsam_host_levels", "bsam_host_build_uniform", "bsam_host_take_time_steps",
-    "bsam_gpu_resid_norm_noalloc", "bsam_gpu_set_tuning",
+    "bsam_gpu_resid_norm_noalloc", "bsam_gpu_set_tuning", "bsam_gpu_fill_down",
     "bsam_batch_create", "bsam_batch_destroy", "bsam_batch_set_tuning", "bsam_batch_footprint",
     "bsam_batch_submit", "bsam_batch_advance", "bsam_batch_sync", "bsam_batch_run",
     "bsam_batch_poll", "bsam_batch_slot_phase", "bsam_batch_collect", "bsam_batch_get_stream", "bsam_batch_profile", "bsam_batch_submit_seeded", "bsam_batch_busy",
@@ -112,6 +112,7 @@ def lib():
         ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int32), ctypes.c_double,
         ctypes.c_double, ctypes.c_double, ctypes.c_double, vp, vp, vp, vp]
     L.bsam_gpu_set_tuning.argtypes = [vp, ctypes.POINTER(Tuning)]
+    L.bsam_gpu_fill_down.argtypes = [vp]
     L.bsam_host_levels.argtypes = [ctypes.POINTER(HostGrid)]
     L.bsam_host_build_uniform.argtypes = [ctypes.POINTER(HostGrid), ctypes.POINTER(PatchDesc),
                                           ctypes.c_int, ip]

@@ -43,6 +43,82 @@ class Hierarchy:
         return [i for i, d in enumerate(self.descs) if d["level"] >= 0]
 
 
+class HierSolver:
+    """A fixed hierarchy resident on a GPU, driven through the C ABI
+    (bsam_gpu_set_hierarchy with every level, put_field of every state patch,
+    then the C++ host driver's time loop)."""
+
+    def __init__(self, hier: Hierarchy, device: int = 0, bottom_cells: int = 0):
+        import ctypes
+        from . import FIELD_Q, PREC_FP64, PatchDesc, RunParams, Tuning, _check, _dp, lib
+        L = lib()
+        self.hier = hier
+        rp = RunParams(ndims=hier.ndims, nrvars=2, mbc=1, maux=0,
+                       nsmoothingpasses=hier.nsmoothingpasses, maxvcycles=hier.maxvcycles,
+                       errortype=1, precision=PREC_FP64, dt=hier.dt, qerrortol=hier.qerrortol,
+                       alpha=hier.alpha, eps=hier.eps)
+        h = ctypes.c_void_p()
+        _check(L.bsam_gpu_create(ctypes.byref(h), device, ctypes.byref(rp)), what="create")
+        self.h = h
+        try:
+            t = Tuning(bottom_cells=bottom_cells)
+            _check(L.bsam_gpu_set_tuning(h, ctypes.byref(t)), h, "set_tuning")
+            n = len(hier.descs)
+            arr = (PatchDesc * n)()
+            for i, d in enumerate(hier.descs):
+                o = arr[i]
+                o.level, o.parent, o.dx = d["level"], d["parent"], d["dx"]
+                for k in range(3):
+                    o.mx[k] = d["mx"][k]
+                    o.xlower[k] = d["xlower"][k]
+                    for s in range(2):
+                        o.mbounds[k][s] = d["mbounds"][k][s]
+                        o.mglobal[k][s] = d["mglobal"][k][s]
+                for f in range(6):
+                    o.mthbc[f] = d["mthbc"][f]
+            _check(L.bsam_gpu_set_hierarchy(h, n, arr, hier.finestlevel), h, "set_hierarchy")
+            self.states = hier.state_patches()
+            for p, q in zip(self.states, hier.q0s):
+                q = np.asfortranarray(q, dtype=np.float64)
+                _check(L.bsam_gpu_put_field(h, p, FIELD_Q, _dp(q)), h, "put_field")
+            _check(L.bsam_gpu_set_ghost(h), h, "set_ghost")
+            _check(L.bsam_gpu_copy_q_to_qold(h), h, "copy_q_to_qold")
+        except Exception:
+            self.close()
+            raise
+
+    def run(self, nsteps: int) -> dict:
+        """TakeTimeSteps on the fixed hierarchy; final q of every state patch."""
+        import ctypes
+        from . import FIELD_Q, _check, _dp, lib
+        L = lib()
+        nvc = np.zeros(nsteps, dtype=np.int32)
+        res = np.zeros(nsteps)
+        conv = np.zeros(nsteps, dtype=np.int32)
+        ipp = ctypes.POINTER(ctypes.c_int)
+        _check(L.bsam_host_take_time_steps(self.h, nsteps, 0, None, 0, nvc.ctypes.data_as(ipp),
+                                           _dp(res), conv.ctypes.data_as(ipp), None),
+               self.h, "take_time_steps")
+        qs = []
+        for p, q0 in zip(self.states, self.hier.q0s):
+            out = np.zeros(q0.shape, order="F")
+            _check(L.bsam_gpu_get_field(self.h, p, FIELD_Q, _dp(out)), self.h, "get_field")
+            qs.append(out)
+        return {"q": qs, "nvcycles": nvc, "residual": res, "converged": conv}
+
+    def close(self):
+        from . import lib
+        if getattr(self, "h", None) is not None and self.h.value:
+            lib().bsam_gpu_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
 def _desc(level, parent, mx, mbounds, mglobal, mthbc, dx, xlower):
     return {"level": level, "parent": parent, "mx": list(mx) + [1] * (3 - len(mx)),
             "mbounds": [list(b) for b in mbounds] + [[1, 1]] * (3 - len(mbounds)),

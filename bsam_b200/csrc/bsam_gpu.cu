@@ -32,6 +32,7 @@
 #include "smooth_fused.cuh"
 #include "bottom.cuh"
 #include "mixed.cuh"
+#include "amr.cuh"
 
 using namespace bsam;
 
@@ -51,6 +52,16 @@ struct LevelPlan {
   int nfused = 0;
   bool fused = false;
   int prec = PREC_F64;
+  // AMR levels (above the root): SetGhost is coarse-fine interpolation +
+  // sibling exchange + SetBC, over the level's patch list.
+  bool amr = false;
+  int* d_plist = nullptr;       // the level's patches
+  int nplist = 0;
+  OverlapCopy* d_ovl = nullptr; // GhostOverlap transfers (ApplyOnLevelPairs order)
+  int novl = 0;
+  // Parent of a refined level: its children do not cover it, so the
+  // snapshot qs is a full copy of q taken after restriction + SetGhost.
+  bool snap = false;
 };
 
 }  // namespace
@@ -72,6 +83,13 @@ struct bsam_gpu {
   std::vector<LevelPlan> levels;     // index level - minlevel
   std::vector<int> masters;          // finest-level state patches
   Item* d_master = nullptr;          // tiles over the masters
+  Item* d_state = nullptr;           // tiles over every state patch on levels >= 0
+  int nstate = 0;
+  Item* d_root = nullptr;            // tiles over the root patch (mass)
+  int nroot = 0;
+  bool amr = false;                  // levels above the root exist
+  int* d_plist = nullptr;            // patch lists of the refined levels
+  OverlapCopy* d_ovl = nullptr;      // their GhostOverlap transfers
   int nmaster = 0;
   Item* d_items = nullptr;
   CUtensorMap* d_tmaps = nullptr;    // TMA maps of the fused levels' fields
@@ -172,13 +190,56 @@ void launch_relax_t(bsam_gpu* h, const LevelPlan& L, int color) {
   k_relax<T, D><<<L.nfine, block_dim(), 0, h->stream>>>(h->d_patches, L.d_fine, color);
 }
 
+// what: 0 = RestrictSolution, 2 = CoarseLoadingFunction, 1 = CorrectFine.
 template <class TC, class TP, int D>
 void launch_transfer_t(bsam_gpu* h, const LevelPlan& L, int what) {
-  if (what == 0) {
+  if (what == 0)
     k_restrict<TC, TP, D><<<L.ncoarse, block_dim(), 0, h->stream>>>(h->d_patches, L.d_coarse);
+  else if (what == 2)
     k_coarse_load<TC, TP, D><<<L.ncoarse, block_dim(), 0, h->stream>>>(h->d_patches, L.d_coarse);
-  } else {
+  else
     k_correct<TC, TP, D><<<L.nfine, block_dim(), 0, h->stream>>>(h->d_patches, L.d_fine);
+}
+
+// SetGhost(level, ipass) of a refined level (boundary.f90:58-89): coarse-fine
+// interpolation, sibling exchange, physical faces -- three ordered launches.
+// Levels at and below the root keep their ghosts by write-through.
+void amr_ghost(bsam_gpu* h, int level, int ipass) {
+  if (level < h->minlevel || level > h->finestlevel) return;
+  const LevelPlan& L = plan(h, level);
+  if (!L.amr) return;
+  k_interp2<<<L.nplist, 128, 0, h->stream>>>(h->d_patches, L.d_plist, ipass);
+  if (L.novl) k_overlap<<<L.novl, 128, 0, h->stream>>>(h->d_patches, L.d_ovl);
+  k_setbc_list<2><<<L.nplist, 128, 0, h->stream>>>(h->d_patches, L.d_plist);
+  h->stats.launches += L.novl ? 3 : 2;
+}
+
+// GetCoarseGhostPoints for the children of a partly covered level: the
+// snapshot qs of every parent patch becomes a full copy of q (taken after
+// restriction and SetGhost).
+void snapshot(bsam_gpu* h, int level) {
+  const LevelPlan& L = plan(h, level);
+  if (!L.snap) return;
+  for (int p : L.patches) {
+    const DevPatch& P = h->hp[p];
+    if (!P.qs[0]) continue;  // not a parent: no child reads a snapshot of it
+    const int64_t lead = 128 / sizeof(double) - 1;
+    for (int c = 0; c < 2; ++c)
+      cudaMemcpyAsync(static_cast<double*>(P.qs[c]) - lead, static_cast<double*>(P.q[c]) - lead,
+                      h->field_elems[p] * sizeof(double), cudaMemcpyDeviceToDevice, h->stream);
+  }
+}
+
+// FillDown(solutionfield) over the refined levels (afas:223-239): each
+// level's q restricted into its parent, then the parent level's SetGhost.
+// Below the root the same restriction is overwritten by RestrictSolution
+// before any read, so it is not issued.
+void filldown(bsam_gpu* h) {
+  for (int level = h->finestlevel; level >= 1; --level) {
+    const LevelPlan& L = plan(h, level);
+    k_filldown2<<<L.ncoarse, block_dim(), 0, h->stream>>>(h->d_patches, L.d_coarse);
+    ++h->stats.launches;
+    amr_ghost(h, level - 1, 0);
   }
 }
 
@@ -213,17 +274,32 @@ void relax_level(bsam_gpu* h, int level, int dir) {
           else launch_relax_t<double, 3>(h, L, color);
         }
         ++h->stats.launches;
+        amr_ghost(h, level, color + 1);  // SetGhost(level, ipass) (afas:542)
       }
   }
   stage_end(h, level);
 }
 
+// what 0: RestrictSolution, parent SetGhost(level-1, 0), GetCoarseGhostPoints
+// and CoarseLoadingFunction (afas:503-509); what 1: CorrectFine and
+// SetGhost(level, 0) (afas:513-515).
 void transfer(bsam_gpu* h, int level, int what) {
   const LevelPlan& L = plan(h, level);
   const int pp = plan(h, level - 1).prec;
-  if (h->rp.ndims == 2) launch_transfer_d<2>(h, L, L.prec, pp, what);
-  else launch_transfer_d<3>(h, L, L.prec, pp, what);
-  h->stats.launches += what == 0 ? 2 : 1;
+  auto launch = [&](int w) {
+    if (h->rp.ndims == 2) launch_transfer_d<2>(h, L, L.prec, pp, w);
+    else launch_transfer_d<3>(h, L, L.prec, pp, w);
+    ++h->stats.launches;
+  };
+  if (what == 0) {
+    launch(0);
+    amr_ghost(h, level - 1, 0);
+    snapshot(h, level - 1);
+    launch(2);
+  } else {
+    launch(1);
+    amr_ghost(h, level, 0);
+  }
 }
 
 // AFASVcycle (afas:488-521).
@@ -301,6 +377,7 @@ void launch_update(bsam_gpu* h) {
 void iteration(bsam_gpu* h) {
   vcycle(h, h->finestlevel);
   if (h->mixed) launch_update(h);
+  if (h->amr) filldown(h);  // FillDown(solutionfield) after the V-cycle (afas:73)
   launch_resid(h);
 }
 
@@ -494,6 +571,13 @@ static void free_hierarchy(bsam_gpu* h) {
   h->d_partials = nullptr;
   h->d_master = nullptr;
   h->nmaster = 0;
+  h->d_state = h->d_root = nullptr;
+  h->nstate = h->nroot = 0;
+  if (h->d_plist) cudaFree(h->d_plist);
+  if (h->d_ovl) cudaFree(h->d_ovl);
+  h->d_plist = nullptr;
+  h->d_ovl = nullptr;
+  h->amr = false;
   h->levels.clear();
   h->masters.clear();
   h->hp.clear();
@@ -511,8 +595,11 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
   int minlevel = patches[0].level;
   for (int p = 0; p < npatch; ++p) minlevel = std::min(minlevel, patches[p].level);
   if (finestlevel < 0 || minlevel > 0) return fail(h, BSAM_ERR_ARG, "levels out of range");
-  if (finestlevel > 0)
-    return fail(h, BSAM_ERR_UNSUPPORTED, "levels above the root (AMR) need coarse-fine ghosts");
+  if (finestlevel > 0 && (nd != 2 || h->mixed))
+    return fail(h, BSAM_ERR_UNSUPPORTED,
+                "levels above the root are built for the 2D FP64 form (no Interpolate3D, no "
+                "mixed-precision AMR)");
+  h->amr = finestlevel > 0;
   h->minlevel = minlevel;
   h->finestlevel = finestlevel;
   h->nuser = npatch;
@@ -524,8 +611,9 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
   // at most bottom_cells cells per patch (uniform hierarchies only).
   h->bottom_level = -1000;
   const int bmax = h->tuning.bottom_cells == 0 ? BOTTOM_MAX_CELLS : h->tuning.bottom_cells;
-  if (bmax > 0 && finestlevel == 0) {
-    for (int l = minlevel; l <= finestlevel; ++l) {
+  if (bmax > 0) {
+    // Only the root and the levels below it (one uniform patch each).
+    for (int l = minlevel; l <= std::min(finestlevel, 0); ++l) {
       bool small = true;
       for (int p = 0; p < npatch; ++p)
         if (patches[p].level == l) small = small && cells_of(patches[p].mx, nd) <= bmax;
@@ -616,7 +704,8 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
       P.bc[f] = rule;
       if (rule == BC_NONE) P.wt = 0;
     }
-    if (!P.wt) return fail(h, BSAM_ERR_UNSUPPORTED, "internal faces need AMR support");
+    if (!P.wt && d.level < 1)
+      return fail(h, BSAM_ERR_UNSUPPORTED, "internal faces occur only on refined levels");
     // Does the V-cycle run on this record?  (Not on the masters of the mixed form.)
     const bool in_vcycle = !(h->mixed && !is_twin && d.level == finestlevel);
     // Mixed form: the V-cycle levels carry a correction of the master state
@@ -775,6 +864,82 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
   const int s_master = (int)all.size();
   for (int p : h->masters) tiles_for(p, h->hp[p].n, nd, all);
   h->nmaster = (int)all.size() - s_master;
+  // State patches (levels >= root, the caller's records) and the root.
+  const int s_state = (int)all.size();
+  for (int p = 0; p < npatch; ++p)
+    if (patches[p].level >= 0) tiles_for(p, h->hp[p].n, nd, all);
+  h->nstate = (int)all.size() - s_state;
+  const int s_root = (int)all.size();
+  for (int p = 0; p < npatch; ++p)
+    if (patches[p].level == 0) tiles_for(p, h->hp[p].n, nd, all);
+  h->nroot = (int)all.size() - s_root;
+  // Refined levels: patch lists and GhostOverlap transfers
+  // (ApplyOnLevelPairs order: each patch with every later one).
+  std::vector<int> plist_all;
+  std::vector<OverlapCopy> ovl_all;
+  std::vector<std::pair<int, int>> span_plist(nl), span_ovl(nl);
+  for (size_t li = 0; li < nl; ++li) {
+    LevelPlan& L = h->levels[li];
+    L.amr = L.level >= 1;
+    L.snap = L.level >= 0 && L.level < finestlevel;
+    span_plist[li] = {(int)plist_all.size(), 0};
+    span_ovl[li] = {(int)ovl_all.size(), 0};
+    if (!L.amr) continue;
+    for (int p : L.patches) plist_all.push_back(p);
+    for (size_t a = 0; a < L.patches.size(); ++a)
+      for (size_t bi = a + 1; bi < L.patches.size(); ++bi) {
+        const bsam_patch_desc& g1 = patches[L.patches[a]];
+        const bsam_patch_desc& g2 = patches[L.patches[bi]];
+        int ov[2][2];
+        bool empty = false;
+        for (int n = 0; n < 2; ++n) {
+          ov[n][0] = std::max(g1.mglobal[n][0] - 1, g2.mglobal[n][0] - 1);
+          ov[n][1] = std::min(g1.mglobal[n][1] + 1, g2.mglobal[n][1] + 1);
+          empty |= ov[n][1] < ov[n][0];
+        }
+        if (empty) continue;
+        // dst takes the other grid's interior inside the overlap.
+        auto emit = [&](int dst, const bsam_patch_desc& gd, int src, const bsam_patch_desc& gs) {
+          int box[2][2];
+          for (int n = 0; n < 2; ++n) {
+            box[n][0] = std::max(ov[n][0], gs.mglobal[n][0]);
+            box[n][1] = std::min(ov[n][1], gs.mglobal[n][1]);
+            if (box[n][1] < box[n][0]) return;
+          }
+          OverlapCopy o;
+          o.dst = dst;
+          o.src = src;
+          o.i0 = box[0][0] - gd.mglobal[0][0] + 1;
+          o.i1 = box[0][1] - gd.mglobal[0][0] + 1;
+          o.j0 = box[1][0] - gd.mglobal[1][0] + 1;
+          o.j1 = box[1][1] - gd.mglobal[1][0] + 1;
+          o.di = gd.mglobal[0][0] - gs.mglobal[0][0];
+          o.dj = gd.mglobal[1][0] - gs.mglobal[1][0];
+          ovl_all.push_back(o);
+        };
+        emit(L.patches[a], g1, L.patches[bi], g2);
+        emit(L.patches[bi], g2, L.patches[a], g1);
+      }
+    span_plist[li].second = (int)plist_all.size() - span_plist[li].first;
+    span_ovl[li].second = (int)ovl_all.size() - span_ovl[li].first;
+  }
+  if (!plist_all.empty()) {
+    CU(cudaMalloc(&h->d_plist, sizeof(int) * plist_all.size()));
+    CU(cudaMemcpyAsync(h->d_plist, plist_all.data(), sizeof(int) * plist_all.size(),
+                       cudaMemcpyHostToDevice, h->stream));
+  }
+  if (!ovl_all.empty()) {
+    CU(cudaMalloc(&h->d_ovl, sizeof(OverlapCopy) * ovl_all.size()));
+    CU(cudaMemcpyAsync(h->d_ovl, ovl_all.data(), sizeof(OverlapCopy) * ovl_all.size(),
+                       cudaMemcpyHostToDevice, h->stream));
+  }
+  for (size_t li = 0; li < nl; ++li) {
+    LevelPlan& L = h->levels[li];
+    L.d_plist = h->d_plist ? h->d_plist + span_plist[li].first : nullptr;
+    L.nplist = span_plist[li].second;
+    L.d_ovl = h->d_ovl ? h->d_ovl + span_ovl[li].first : nullptr;
+    L.novl = span_ovl[li].second;
+  }
 
   CU(cudaMalloc(&h->d_items, all.size() * sizeof(Item)));
   CU(cudaMemcpyAsync(h->d_items, all.data(), all.size() * sizeof(Item), cudaMemcpyHostToDevice,
@@ -791,6 +956,9 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
     h->max_items = std::max(h->max_items, L.nfine);
   }
   h->d_master = h->d_items + s_master;
+  h->d_state = h->d_items + s_state;
+  h->d_root = h->d_items + s_root;
+  h->max_items = std::max(h->max_items, h->nroot);
   CU(cudaFuncSetAttribute(k_smooth3_fused<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)Fused3<double>::SMEM));
   CU(cudaFuncSetAttribute(k_smooth3_fused<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -894,7 +1062,20 @@ int bsam_gpu_get_field(bsam_gpu* h, int patch, int field, double* out) {
 int bsam_gpu_set_ghost(bsam_gpu* h) {
   if (!h || !h->have_hierarchy) return BSAM_ERR_STATE;
   CU(cudaSetDevice(h->device));
-  for (int l = h->finestlevel; l >= h->minlevel; --l) ghost_level(h, l);
+  // Coarse levels first: a refined level's interpolation reads its parent.
+  for (int l = h->minlevel; l <= h->finestlevel; ++l) {
+    if (plan(h, l).amr) amr_ghost(h, l, 0);
+    else ghost_level(h, l);
+  }
+  CU(cudaGetLastError());
+  CU(cudaStreamSynchronize(h->stream));
+  return BSAM_OK;
+}
+
+int bsam_gpu_fill_down(bsam_gpu* h) {
+  if (!h || !h->have_hierarchy) return BSAM_ERR_STATE;
+  CU(cudaSetDevice(h->device));
+  if (h->amr) filldown(h);
   CU(cudaGetLastError());
   CU(cudaStreamSynchronize(h->stream));
   return BSAM_OK;
@@ -919,13 +1100,14 @@ int bsam_gpu_multigrid_iterations(bsam_gpu* h, int* nvcycles, double* residual, 
   CU(cudaSetDevice(h->device));
   const int nd = h->rp.ndims;
   const dim3 b = block_dim();
-  // GetSourceFunction + UpdateSourceFunction on the state patches of levels
-  // >= root (afas:57-64).  FillDown(source) and FillDown(solution) (afas:47,
-  // 66, 73, 90) only write regions that RestrictSolution /
-  // CoarseLoadingFunction overwrite before any read when the levels are
-  // nested uniform grids, so they are not issued.
-  if (nd == 2) k_source<double, 2><<<h->nmaster, b, 0, h->stream>>>(h->d_patches, h->d_master);
-  else k_source<double, 3><<<h->nmaster, b, 0, h->stream>>>(h->d_patches, h->d_master);
+  // FillDown(solution) (afas:47) over the refined levels; below the root it
+  // and FillDown(source) (afas:66, 90) only write regions that
+  // RestrictSolution / CoarseLoadingFunction overwrite before any read, so
+  // they are not issued.  Then GetSourceFunction + UpdateSourceFunction on
+  // the state patches of levels >= root (afas:57-64).
+  if (h->amr) filldown(h);
+  if (nd == 2) k_source<double, 2><<<h->nstate, b, 0, h->stream>>>(h->d_patches, h->d_state);
+  else k_source<double, 3><<<h->nstate, b, 0, h->stream>>>(h->d_patches, h->d_state);
   ++h->stats.launches;
   // Mixed form: the FP32 working copy and its right-hand side for the first
   // V-cycle (the norm computed here is not a convergence test).
@@ -1002,16 +1184,20 @@ int bsam_gpu_residual_trace(bsam_gpu* h, double* out, int maxn) {
 
 int bsam_gpu_mass(bsam_gpu* h, double* mass) {
   if (!h || !h->have_hierarchy || !mass) return BSAM_ERR_STATE;
-  if (h->finestlevel != 0) return fail(h, BSAM_ERR_UNSUPPORTED, "mass needs a uniform hierarchy");
+  if (h->nroot == 0) return fail(h, BSAM_ERR_UNSUPPORTED, "no root-level patch");
   CU(cudaSetDevice(h->device));
-  const double hh = h->hp[h->masters[0]].h;
+  // AfterStep2D/3D integral(1) on the root level (problem.f90:102-134).
+  int root = 0;
+  for (int p = 0; p < h->nuser; ++p)
+    if (h->desc[p].level == 0) root = p;
+  const double hh = h->hp[root].h;
   const double hd = h->rp.ndims == 2 ? hh * hh : hh * hh * hh;
   if (h->rp.ndims == 2)
-    k_mass<double, 2><<<h->nmaster, block_dim(), 0, h->stream>>>(
-        h->d_patches, h->d_master, h->d_partials, h->d_status, h->nmaster, hd);
+    k_mass<double, 2><<<h->nroot, block_dim(), 0, h->stream>>>(
+        h->d_patches, h->d_root, h->d_partials, h->d_status, h->nroot, hd);
   else
-    k_mass<double, 3><<<h->nmaster, block_dim(), 0, h->stream>>>(
-        h->d_patches, h->d_master, h->d_partials, h->d_status, h->nmaster, hd);
+    k_mass<double, 3><<<h->nroot, block_dim(), 0, h->stream>>>(
+        h->d_patches, h->d_root, h->d_partials, h->d_status, h->nroot, hd);
   ++h->stats.launches;
   CU(cudaGetLastError());
   CU(cudaMemcpyAsync(h->h_status, h->d_status, sizeof(DevStatus), cudaMemcpyDeviceToHost,

@@ -110,10 +110,16 @@ int bsam_host_take_time_steps(bsam_gpu* h, int nsteps, int root_patch, double* q
                               int* converged, double* mass) {
   if (!h || nsteps < 0) return BSAM_ERR_ARG;
   for (int step = 0; step < nsteps; ++step) {
-    // AMR(rootlevel) -> SetGhost(rootlevel, 0) with maxlevel = 0; then
-    // CopyQToQold on every level (lib/bsamroutines.f90:648-661).
+    // AMR(rootlevel) on an unchanged hierarchy -> SetGhost(level, 0) from the
+    // root up; FillDown(solution) on the first step; CopyQToQold on every
+    // level (lib/bsamroutines.f90:648-661).  FillDown repeated at the start
+    // of a later call gives the same values (the fine levels are unchanged).
     int rc = bsam_gpu_set_ghost(h);
     if (rc) return rc;
+    if (step == 0) {
+      rc = bsam_gpu_fill_down(h);
+      if (rc) return rc;
+    }
     rc = bsam_gpu_copy_q_to_qold(h);
     if (rc) return rc;
     int nv = 0, conv = 0;

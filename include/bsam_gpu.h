@@ -111,9 +111,17 @@ int bsam_gpu_put_field(bsam_gpu* h, int patch, int field, const double* a);
 /* Copy a device field of one patch back to the host, same layouts. */
 int bsam_gpu_get_field(bsam_gpu* h, int patch, int field, double* out);
 
-/* SetGhost(level, 0) (lib/boundary.f90:58-89) on every level, as BSAMSolver
- * does after QInit (lib/bsamroutines.f90:144). */
+/* SetGhost(level, 0) (lib/boundary.f90:58-89) on every level, coarse to
+ * fine, as BSAMSolver does after QInit (lib/bsamroutines.f90:144).  Above the
+ * root: coarse-fine interpolation (Interpolate2D), sibling exchange
+ * (GhostOverlap) and physical faces. */
 int bsam_gpu_set_ghost(bsam_gpu* h);
+
+/* FillDown(solutionfield) (lib/afasroutines.f90:223-310): the refined
+ * levels' q restricted into their parents (with the parents' SetGhost), as
+ * TakeTimeSteps does on its first step (lib/bsamroutines.f90:651-654).  A
+ * no-op without refined levels. */
+int bsam_gpu_fill_down(bsam_gpu* h);
 
 /* CopyQToQold on all levels (lib/bsamroutines.f90:568-580, 659-661). */
 int bsam_gpu_copy_q_to_qold(bsam_gpu* h);

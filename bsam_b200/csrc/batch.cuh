@@ -100,6 +100,74 @@ __global__ void __launch_bounds__(BLOCK_THREADS)
   }
 }
 
+// CorrectFine in 2D by 2 x 2 blocks of fine cells: the fine cells 2m, 2m+1
+// (x) and 2n, 2n+1 (y) read the same four parent corrections, formed once
+// here; each cell then takes correct_cell's bilinear expression on them, so
+// the values are correct_cell's bit for bit.  Block (m, n) for
+// m = 0..cn0, n = 0..cn1 covers fine cells 1..n0 x 1..n1 exactly once.
+template <class TC, class TP>
+__device__ __forceinline__ void correct_block2(const DevPatch& C, const DevPatch& P, int m,
+                                               int n) {
+  TC* q0 = fld<TC>(mid_state(C)[0]);
+  TC* q1 = fld<TC>(mid_state(C)[1]);
+  TP e[2][2][2];  // [component][m + a][n + b]
+#pragma unroll
+  for (int v = 0; v < 2; ++v) {
+    const TP* pq = fld<TP>(P.q[v]);
+    const TP* ps = fld<TP>(P.qs[v]);
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int bb = 0; bb < 2; ++bb) {
+        const int64_t x = cidx(P, C.off[0] + m + a, C.off[1] + n + bb, 0);
+        e[v][a][bb] = pq[x] - ps[x];
+      }
+  }
+#pragma unroll
+  for (int dy = 0; dy < 2; ++dy) {
+    const int J = 2 * n + dy;
+    if (J < 1 || J > C.n[1]) continue;
+    const bool ey = dy == 0;
+#pragma unroll
+    for (int dx = 0; dx < 2; ++dx) {
+      const int I = 2 * m + dx;
+      if (I < 1 || I > C.n[0]) continue;
+      const bool ex = dx == 0;
+      TP corr[2];
+#pragma unroll
+      for (int v = 0; v < 2; ++v) {
+        const TP b0 = lin_x<TP>(ex, e[v][0][0], e[v][1][0]);
+        const TP b1 = lin_x<TP>(ex, e[v][0][1], e[v][1][1]);
+        corr[v] = lin_x<TP>(ey, b0, b1) / TP(16);
+      }
+      const int64_t c = cidx(C, I, J, 0);
+      const TC a0 = q0[c] + TC(corr[0]);
+      const TC a1 = q1[c] + TC(corr[1]);
+      q0[c] = a0;
+      q1[c] = a1;
+      if (C.wt && near_boundary(C, I, J, 0, 2)) write_through<TC, 2>(C, q0, q1, I, J, 0, a0, a1);
+    }
+  }
+}
+
+// Items: tiles of 32 x TILE_Y blocks (m, n) of a record (list L_CORR).
+template <class TC>
+__global__ void __launch_bounds__(BLOCK_THREADS)
+    kb_correct2(const DevPatch* __restrict__ PT, const Item* __restrict__ items,
+                const int* __restrict__ count) {
+  const int n = *count;
+  for (int b = blockIdx.x; b < n; b += gridDim.x) {
+    const Item it = items[b];
+    const DevPatch C = PT[it.patch];
+    if (!C.active) continue;
+    const int m = it.tx * 32 + threadIdx.x, nn = it.ty * TILE_Y + threadIdx.y;
+    if (m > C.cn[0] || nn > C.cn[1]) continue;
+    const DevPatch P = PT[C.parent];
+    if (C.pprec == PREC_F32) correct_block2<TC, float>(C, P, m, nn);
+    else correct_block2<TC, double>(C, P, m, nn);
+  }
+}
+
 // Bottom chains (FP64 in both forms), one CTA per chain at a time.  256
 // threads at up to 64 registers: four chains per SM run at once, so a batch
 // of a few hundred problems has all its chains resident in one wave (cell

@@ -58,7 +58,8 @@ enum {
   L_COARSE = 2 + MAXD,
   L_RELAX = 2 + 2 * MAXD,
   L_FUSED = 2 + 3 * MAXD,
-  NLIST = 2 + 4 * MAXD
+  L_CORR = 2 + 4 * MAXD,  // 2D: tiles of 2 x 2 fine-cell blocks (kb_correct2)
+  NLIST = 2 + 5 * MAXD
 };
 
 struct List {
@@ -487,6 +488,10 @@ void append_items(bsam_batch* b, int s) {
         for (int x = 0; x < (P.n[0] + tx - 1) / tx; ++x)
           b->lists[L_FUSED + d].h.push_back(Item{rec0 + r, x, y, 0});
     }
+    if (nd == 2)  // blocks (m, n), m = 0..cn0, n = 0..cn1, 32 x TILE_Y per tile
+      for (int y = 0; y < (P.cn[1] + 1 + TILE_Y - 1) / TILE_Y; ++y)
+        for (int x = 0; x < (P.cn[0] + 1 + 31) / 32; ++x)
+          b->lists[L_CORR + d].h.push_back(Item{rec0 + r, x, y, 0});
   }
   b->cfg_dirty = true;
 }
@@ -594,9 +599,15 @@ void tick_t(bsam_batch* b, cudaGraphConditionalHandle handle, int in_graph) {
     ++n;
   }
   for (int d = b->cap_depth - 1; d >= 0; --d) {
-    const int gf = grid_for(b, L_FINE + d);
-    if (b->mixed) kb_correct<float, D><<<gf, blk, 0, s>>>(pt, L[L_FINE + d].d, cnt + L_FINE + d);
-    else kb_correct<double, D><<<gf, blk, 0, s>>>(pt, L[L_FINE + d].d, cnt + L_FINE + d);
+    if (D == 2) {
+      const int gk = grid_for(b, L_CORR + d);
+      if (b->mixed) kb_correct2<float><<<gk, blk, 0, s>>>(pt, L[L_CORR + d].d, cnt + L_CORR + d);
+      else kb_correct2<double><<<gk, blk, 0, s>>>(pt, L[L_CORR + d].d, cnt + L_CORR + d);
+    } else {
+      const int gf = grid_for(b, L_FINE + d);
+      if (b->mixed) kb_correct<float, D><<<gf, blk, 0, s>>>(pt, L[L_FINE + d].d, cnt + L_FINE + d);
+      else kb_correct<double, D><<<gf, blk, 0, s>>>(pt, L[L_FINE + d].d, cnt + L_FINE + d);
+    }
     ++n;
     relax(d, 1);
   }
@@ -1093,8 +1104,8 @@ int bsam_batch_collect(bsam_batch* b, int slot, double* q, bsam_step_result* ste
   const int ph = ((volatile SlotOut*)b->h_out)[slot].phase;
   if (ph != SLOT_DONE && ph != SLOT_FAILED) return fail(b, BSAM_ERR_STATE, "problem not finished");
   const int nd = b->bp.ndims;
-  const DevPatch& M = S.recs[S.master];
   const int rec_master = slot * RMAX + S.master;
+  const DevPatch& M = S.recs[S.master];
   const SlotCfg& C = b->h_cfg[slot];
   if (q) {
     const int e0 = M.n[0] + 2, e1 = M.n[1] + 2, e2 = nd == 3 ? M.n[2] + 2 : 1;

@@ -5,10 +5,13 @@
 // and bench.py's cpu_baseline leg load this file's library; the product path
 // (bsam_b200/, include/) never does.
 //
-// Parity pinning: UNPINNED against reference outputs.  The reference is
-// Fortran 90 with no compiler in this image and ships no tests or golden
-// vectors; the restatement is checked by known-answer tests and invariants
-// derived from the reference's formulas (tests/test_oracle.py).
+// Parity pinning: the leaf routines are PINNED bit for bit against fixtures
+// made by executing the reference's own Fortran source with a Fortran-subset
+// interpreter (tests/golden/, tests/test_golden_reference.py); the V-cycle
+// and time-loop composition is UNPINNED (no Fortran compiler in this image,
+// no tests or golden vectors in the reference) and is checked by
+// known-answer tests and invariants (tests/test_oracle.py,
+// tests/test_oracle_amr.py).
 //
 // Faithfulness rules followed throughout:
 //  * every array statement evaluates its whole right-hand side before the

@@ -7,9 +7,14 @@
  * the CUDA path; the product never links, loads or calls it.
  *
  * Parity pinning: the reference is Fortran 90, no Fortran compiler exists in
- * this image, and the reference ships no tests or golden outputs.  Parity is
- * UNPINNED against reference outputs; the restatement is checked by
- * known-answer tests and invariants derived from the reference's formulas.
+ * this image, and the reference ships no tests or golden outputs.  The leaf
+ * routines (relaxation, operator, source, restriction, P1 prolongation,
+ * SetBC/UserBC, Interpolate2D) are PINNED bit for bit against fixtures
+ * produced by executing the reference's own Fortran source with a
+ * Fortran-subset interpreter (tests/golden/make_golden.py,
+ * tests/test_golden_reference.py).  Their composition into the V-cycle and
+ * time loop (afasroutines.f90, bsamroutines.f90) is UNPINNED: it is checked
+ * by known-answer tests and invariants derived from the reference's formulas.
  *
  * Array layout (every array argument): Fortran column-major, i fastest, with
  * the reference's bounds -- q(0:mx1+1, 0:mx2+1[, 0:mx3+1], 1:2) with the ghost

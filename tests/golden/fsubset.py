@@ -1,0 +1,676 @@
+"""A small interpreter for the Fortran 90 subset of BSAM's hot-path leaf
+routines, used only to generate golden fixtures (tests/golden/*.npz) from the
+reference's own source text.
+
+No Fortran compiler exists in this image, so the reference cannot be built.
+Its leaf routines (RelaxGrid2D/3D, Operator2D/3D with ULap/UDiv/ULapMob,
+Source2D/3D, Restriction2D/3D, Bi/TriLinProlongationP1, SetBC2D/3D with
+UserBC2D/3D, Interpolate2D) are plain array statements, DO loops, IF /
+SELECT CASE and elemental functions; this module parses those routines from
+the reference files and executes them with numpy in IEEE double precision
+(the reference builds with -fdefault-real-8), evaluating every expression
+left to right as written and every array statement's right-hand side before
+its assignment.  Not supported (and not needed by those routines): derived
+types, pointers, WHERE, I/O, character data, implicit typing.
+
+Only make_golden.py imports this module, in a container that has the
+reference source; the tests read the fixtures it wrote.
+"""
+from __future__ import annotations
+
+import re
+
+import numpy as np
+
+# ---- lexer ----------------------------------------------------------------------
+
+_TOKEN = re.compile(r"""
+    (?P<num>(\d+\.\d*|\.\d+|\d+)([eEdD][+-]?\d+)?)
+  | (?P<dotop>\.(and|or|not|true|false|eq|ne|lt|le|gt|ge)\.)
+  | (?P<name>[A-Za-z_][A-Za-z_0-9]*)
+  | (?P<op>\*\*|==|/=|<=|>=|::|[-+*/(),:=<>%])
+  | (?P<ws>\s+)
+""", re.X | re.I)
+
+
+def tokenize(s: str) -> list:
+    out, pos = [], 0
+    while pos < len(s):
+        m = _TOKEN.match(s, pos)
+        if not m:
+            raise SyntaxError(f"cannot lex: {s[pos:pos + 30]!r}")
+        pos = m.end()
+        kind = m.lastgroup
+        if kind == "ws":
+            continue
+        text = m.group(kind)
+        if kind == "num":
+            t = text.lower().replace("d", "e")
+            val = float(t) if ("." in t or "e" in t) else int(t)
+            out.append(("num", val))
+        elif kind == "dotop":
+            out.append(("op", text.lower()))
+        elif kind == "name":
+            out.append(("name", text.lower()))
+        else:
+            out.append(("op", text))
+    return out
+
+
+def logical_lines(src: str) -> list:
+    """Source lines with comments removed, continuations joined and ';'
+    statement separators split."""
+    lines, cur = [], ""
+    for raw in src.splitlines():
+        line = raw.split("!", 1)[0].rstrip()
+        if not line.strip():
+            continue
+        stripped = line.strip()
+        if stripped.startswith("&"):
+            stripped = stripped[1:]
+        if stripped.endswith("&"):
+            cur += stripped[:-1] + " "
+            continue
+        cur += stripped
+        for part in cur.split(";"):
+            if part.strip():
+                lines.append(part.strip())
+        cur = ""
+    return lines
+
+
+# ---- arrays with Fortran bounds -----------------------------------------------
+
+class FArray:
+    """A numpy array (column-major semantics, any lower bounds)."""
+
+    def __init__(self, data: np.ndarray, lb):
+        self.data = data
+        self.lb = tuple(lb)
+
+    @property
+    def shape(self):
+        return self.data.shape
+
+
+def rebase(a, lb):
+    if isinstance(a, FArray):
+        return FArray(a.data, lb)
+    return FArray(np.asarray(a), lb)
+
+
+# ---- expressions ---------------------------------------------------------------
+
+class Parser:
+    def __init__(self, toks):
+        self.t = toks
+        self.i = 0
+
+    def peek(self, k=0):
+        return self.t[self.i + k] if self.i + k < len(self.t) else ("eof", None)
+
+    def take(self, val=None):
+        tok = self.peek()
+        if val is not None and tok[1] != val:
+            raise SyntaxError(f"expected {val!r}, got {tok!r}")
+        self.i += 1
+        return tok
+
+    # precedence: .or. < .and. < .not. < relational < +- < */ < unary < **
+    def expr(self):
+        node = self.and_()
+        while self.peek()[1] == ".or.":
+            self.take()
+            node = ("bin", ".or.", node, self.and_())
+        return node
+
+    def and_(self):
+        node = self.not_()
+        while self.peek()[1] == ".and.":
+            self.take()
+            node = ("bin", ".and.", node, self.not_())
+        return node
+
+    def not_(self):
+        if self.peek()[1] == ".not.":
+            self.take()
+            return ("not", self.not_())
+        return self.rel()
+
+    def rel(self):
+        node = self.add()
+        ops = {"==": "==", "/=": "/=", "<": "<", ">": ">", "<=": "<=", ">=": ">=",
+               ".eq.": "==", ".ne.": "/=", ".lt.": "<", ".le.": "<=", ".gt.": ">", ".ge.": ">="}
+        if self.peek()[1] in ops:
+            op = ops[self.take()[1]]
+            node = ("bin", op, node, self.add())
+        return node
+
+    def add(self):
+        if self.peek()[1] in ("+", "-"):  # leading sign: applies to the first term
+            op = self.take()[1]
+            node = self.mul()
+            if op == "-":
+                node = ("neg", node)
+        else:
+            node = self.mul()
+        while self.peek()[1] in ("+", "-"):
+            op = self.take()[1]
+            node = ("bin", op, node, self.mul())
+        return node
+
+    def mul(self):
+        node = self.power()
+        while self.peek()[1] in ("*", "/"):
+            op = self.take()[1]
+            node = ("bin", op, node, self.power())
+        return node
+
+    def power(self):
+        base = self.primary()
+        if self.peek()[1] == "**":
+            self.take()
+            return ("bin", "**", base, self.power())
+        return base
+
+    def primary(self):
+        kind, val = self.peek()
+        if kind == "num":
+            self.take()
+            return ("num", val)
+        if val in (".true.", ".false."):
+            self.take()
+            return ("num", val == ".true.")
+        if val == "(":
+            self.take()
+            e = self.expr()
+            self.take(")")
+            return e
+        if kind == "name":
+            self.take()
+            if self.peek()[1] == "(":
+                self.take()
+                args = []
+                if self.peek()[1] != ")":
+                    while True:
+                        args.append(self.subscript())
+                        if self.peek()[1] == ",":
+                            self.take()
+                            continue
+                        break
+                self.take(")")
+                return ("ref", val, args)
+            return ("var", val)
+        raise SyntaxError(f"unexpected token {self.peek()!r}")
+
+    def subscript(self):
+        """An argument or a section triplet lo:hi[:stride] (parts optional)."""
+        lo = hi = st = None
+        if self.peek()[1] != ":":
+            lo = self.expr()
+            if self.peek()[1] != ":":
+                return lo
+        self.take(":")
+        if self.peek()[1] not in (",", ")", ":"):
+            hi = self.expr()
+        if self.peek()[1] == ":":
+            self.take()
+            st = self.expr()
+        return ("sec", lo, hi, st)
+
+
+def parse_expr(s: str):
+    p = Parser(tokenize(s))
+    e = p.expr()
+    if p.peek()[0] != "eof":
+        raise SyntaxError(f"trailing tokens in {s!r}")
+    return e
+
+
+# ---- routines ---------------------------------------------------------------------
+
+class Routine:
+    def __init__(self, name, kind, args, result, decls, body, elemental):
+        self.name, self.kind, self.args, self.result = name, kind, args, result
+        self.decls, self.body, self.elemental = decls, body, elemental
+
+
+_HEAD = re.compile(r"^(?:(elemental|recursive|pure)\s+)?(?:(integer|real|logical)\s+)?"
+                   r"(subroutine|function)\s+(\w+)\s*\(([^)]*)\)\s*(?:result\s*\(\s*(\w+)\s*\))?",
+                   re.I)
+
+
+def extract_routines(src: str) -> dict:
+    lines = logical_lines(src)
+    out, i = {}, 0
+    while i < len(lines):
+        m = _HEAD.match(lines[i])
+        if not m:
+            i += 1
+            continue
+        elemental = (m.group(1) or "").lower() == "elemental"
+        kind = m.group(3).lower()
+        name = m.group(4).lower()
+        args = [a.strip().lower() for a in m.group(5).split(",") if a.strip()]
+        result = (m.group(6) or (name if kind == "function" else "")).lower()
+        j = i + 1
+        while not re.match(rf"^end\s+{kind}\b", lines[j], re.I):
+            j += 1
+        decls, body = [], []
+        for ln in lines[i + 1:j]:
+            low = ln.lower()
+            if re.match(r"^(use|implicit)\b", low):
+                continue
+            if re.match(r"^(real|integer|logical|double\s+precision)\b", low) and "::" in ln:
+                decls.append(ln)
+            elif re.match(r"^(real|integer|logical)\s+\w", low) and "=" not in ln.split("::")[0]:
+                decls.append(ln)
+            else:
+                body.append(ln)
+        out[name] = Routine(name, kind, args, result, decls, body, elemental)
+        i = j + 1
+    return out
+
+
+def parse_module_parameters(src: str) -> dict:
+    """`real, parameter :: name = expr` constants of a module."""
+    consts = {}
+    for ln in logical_lines(src):
+        m = re.match(r"^real\s*,\s*parameter\s*::\s*(\w+)\s*=\s*(.+)$", ln, re.I)
+        if m:
+            consts[m.group(1).lower()] = m.group(2)
+    return consts
+
+
+class Interp:
+    def __init__(self, routines: dict, globals_: dict):
+        self.routines = routines
+        self.globals = dict(globals_)
+
+    # -- evaluation -------------------------------------------------------------
+    def ev(self, node, env):
+        k = node[0]
+        if k == "num":
+            return node[1]
+        if k == "var":
+            name = node[1]
+            v = env[name] if name in env else self.globals[name]
+            return v.data if isinstance(v, FArray) else v
+        if k == "neg":
+            return -self.ev(node[1], env)
+        if k == "not":
+            return np.logical_not(self.ev(node[1], env))
+        if k == "bin":
+            op = node[1]
+            a = self.ev(node[2], env)
+            b = self.ev(node[3], env)
+            if op == "+":
+                return a + b
+            if op == "-":
+                return a - b
+            if op == "*":
+                return a * b
+            if op == "/":
+                if isinstance(a, (int, np.integer)) and isinstance(b, (int, np.integer)):
+                    q = abs(a) // abs(b)
+                    return q if (a >= 0) == (b >= 0) else -q
+                return a / b
+            if op == "**":
+                if isinstance(b, (int, np.integer)) and b >= 0:
+                    r = a
+                    for _ in range(b - 1):
+                        r = r * a
+                    return r if b > 0 else 1.0
+                return a ** b
+            if op == "==":
+                return a == b
+            if op == "/=":
+                return a != b
+            if op == "<":
+                return a < b
+            if op == ">":
+                return a > b
+            if op == "<=":
+                return a <= b
+            if op == ">=":
+                return a >= b
+            if op == ".and.":
+                return np.logical_and(a, b)
+            if op == ".or.":
+                return np.logical_or(a, b)
+        if k == "ref":
+            return self.ref(node, env)
+        raise ValueError(node)
+
+    def index_tuple(self, arr: FArray, subs, env):
+        idx = []
+        for d, s in enumerate(subs):
+            lb = arr.lb[d]
+            n = arr.data.shape[d]
+            if isinstance(s, tuple) and s[0] == "sec":
+                lo = lb if s[1] is None else self.ev(s[1], env)
+                hi = lb + n - 1 if s[2] is None else self.ev(s[2], env)
+                st = 1 if s[3] is None else self.ev(s[3], env)
+                if st > 0:
+                    stop = hi - lb + 1
+                    idx.append(slice(lo - lb, max(stop, lo - lb), st))
+                else:
+                    raise NotImplementedError("negative strides")
+            else:
+                i = int(self.ev(s, env))
+                if not (lb <= i < lb + n):
+                    raise IndexError(f"index {i} outside {lb}:{lb + n - 1}")
+                idx.append(i - lb)
+        return tuple(idx)
+
+    def ref(self, node, env):
+        _, name, subs = node
+        arr = env.get(name, self.globals.get(name))
+        if isinstance(arr, FArray):
+            return arr.data[self.index_tuple(arr, subs, env)]
+        return self.call_function(name, subs, env)
+
+    def section_actual(self, s, env):
+        """An actual argument: arrays and sections keep their storage (views)."""
+        if s[0] == "var":
+            v = env.get(s[1], self.globals.get(s[1]))
+            if isinstance(v, FArray):
+                return FArray(v.data, (1,) * v.data.ndim)
+            return v
+        if s[0] == "ref":
+            arr = env.get(s[1], self.globals.get(s[1]))
+            if isinstance(arr, FArray):
+                view = arr.data[self.index_tuple(arr, s[2], env)]
+                if isinstance(view, np.ndarray) and view.ndim > 0:
+                    return FArray(view, (1,) * view.ndim)
+                return view
+        v = self.ev(s, env)
+        if isinstance(v, np.ndarray) and v.ndim > 0:
+            return FArray(v, (1,) * v.ndim)
+        return v
+
+    def call_function(self, name, subs, env):
+        if name == "size":
+            a = self.section_actual(subs[0], env)
+            d = int(self.ev(subs[1], env)) if len(subs) > 1 else None
+            return a.data.shape[d - 1] if d else a.data.size
+        if name == "modulo":
+            a, p = self.ev(subs[0], env), self.ev(subs[1], env)
+            return a % p
+        if name == "mod":
+            a, p = self.ev(subs[0], env), self.ev(subs[1], env)
+            return int(np.fmod(a, p))
+        if name in ("max", "min"):
+            vals = [self.ev(s, env) for s in subs]
+            f = np.maximum if name == "max" else np.minimum
+            r = vals[0]
+            for v in vals[1:]:
+                r = f(r, v)
+            return r
+        if name == "abs":
+            return np.abs(self.ev(subs[0], env))
+        if name == "sqrt":
+            return np.sqrt(self.ev(subs[0], env))
+        if name in ("real", "dble"):
+            return np.float64(self.ev(subs[0], env)) if np.isscalar(self.ev(subs[0], env)) else \
+                self.ev(subs[0], env).astype(np.float64)
+        r = self.routines[name]
+        actuals = [self.section_actual(s, env) for s in subs]
+        if r.elemental:
+            return self.run_elemental(r, actuals)
+        return self.run(r, actuals)
+
+    def run_elemental(self, r, actuals):
+        vals = [a.data if isinstance(a, FArray) else a for a in actuals]
+        env = {an: np.asarray(v, dtype=np.float64) if not np.isscalar(v) else v
+               for an, v in zip(r.args, vals)}
+        # Scalar temporaries of the body broadcast over the argument's shape.
+        self.exec_block(r.body, env)
+        res = env[r.result]
+        shape = np.broadcast(*[np.asarray(v) for v in vals]).shape
+        return np.broadcast_to(np.asarray(res, dtype=np.float64), shape).copy() if shape else res
+
+    # -- declarations ---------------------------------------------------------------
+    def declare(self, r, env):
+        for d in r.decls:
+            head, names = d.split("::", 1)
+            attrs = [a.strip() for a in split_top(head, ",")]
+            base = attrs[0].lower()
+            dims = None
+            for a in attrs[1:]:
+                m = re.match(r"dimension\s*\((.*)\)\s*$", a, re.I)
+                if m:
+                    dims = m.group(1)
+            for item in split_top(names, ","):
+                item = item.strip()
+                m = re.match(r"(\w+)\s*(\((.*)\))?\s*(=\s*(.+))?$", item)
+                nm = m.group(1).lower()
+                local_dims = m.group(3) or dims
+                init = m.group(5)
+                if nm in r.args:
+                    a = env.get(nm)
+                    if local_dims is not None and isinstance(a, FArray):
+                        lbs = []
+                        for k, spec in enumerate(split_top(local_dims, ",")):
+                            spec = spec.strip()
+                            if ":" in spec:
+                                lo = spec.split(":")[0].strip()
+                                lbs.append(int(self.ev(parse_expr(lo), env)) if lo else 1)
+                            else:
+                                lbs.append(1)
+                        env[nm] = FArray(a.data, lbs)
+                    continue
+                if local_dims is not None:
+                    lbs, shape = [], []
+                    for spec in split_top(local_dims, ","):
+                        spec = spec.strip()
+                        if ":" in spec:
+                            lo_s, hi_s = spec.split(":", 1)
+                            lo = int(self.ev(parse_expr(lo_s), env))
+                            hi = int(self.ev(parse_expr(hi_s), env))
+                        else:
+                            lo, hi = 1, int(self.ev(parse_expr(spec), env))
+                        lbs.append(lo)
+                        shape.append(max(hi - lo + 1, 0))
+                    dt = np.float64 if base.startswith("real") else (
+                        np.int64 if base.startswith("integer") else bool)
+                    env[nm] = FArray(np.full(shape, np.nan if dt == np.float64 else 0, dtype=dt,
+                                             order="F"), lbs)
+                elif init is not None:
+                    env[nm] = self.ev(parse_expr(init), env)
+                else:
+                    env[nm] = 0.0 if base.startswith("real") else 0
+
+    def run(self, r, actuals):
+        env = {}
+        for an, av in zip(r.args, actuals):
+            env[an] = av
+        self.declare(r, env)
+        self.exec_block(r.body, env)
+        if r.kind == "function":
+            v = env[r.result]
+            return v.data if isinstance(v, FArray) else v
+        return None
+
+    # -- statements -----------------------------------------------------------------
+    def exec_block(self, lines, env):
+        i = 0
+        while i < len(lines):
+            i = self.exec_stmt(lines, i, env)
+
+    def find_end(self, lines, i, opener, closer, middles=()):
+        """Index of the matching closer (and of the middle keywords) for the
+        construct opened at lines[i]."""
+        depth, mids = 0, []
+        for j in range(i, len(lines)):
+            low = lines[j].lower()
+            if opener(low):
+                depth += 1
+            elif closer(low):
+                depth -= 1
+                if depth == 0:
+                    return j, mids
+            elif depth == 1 and any(mm(low) for mm in middles):
+                mids.append(j)
+        raise SyntaxError(f"unterminated construct at {lines[i]!r}")
+
+    def exec_stmt(self, lines, i, env):
+        ln = lines[i]
+        low = ln.lower()
+        lab = re.match(r"^(\w+)\s*:\s*(do\b.*)$", ln, re.I)
+        if lab:
+            ln = lab.group(2)
+            low = ln.lower()
+        if re.match(r"^do\b", low):
+            is_do = lambda s: bool(re.match(r"^(\w+\s*:\s*)?do\b", s))
+            is_end = lambda s: bool(re.match(r"^end\s*do\b", s))
+            end, _ = self.find_end(lines, i, is_do, is_end)
+            m = re.match(r"^do\s+(\w+)\s*=\s*(.+)$", ln, re.I)
+            var = m.group(1).lower()
+            parts = split_top(m.group(2), ",")
+            lo = int(self.ev(parse_expr(parts[0]), env))
+            hi = int(self.ev(parse_expr(parts[1]), env))
+            st = int(self.ev(parse_expr(parts[2]), env)) if len(parts) > 2 else 1
+            body = lines[i + 1:end]
+            name = lab.group(1).lower() if lab else None
+            v = lo
+            while (st > 0 and v <= hi) or (st < 0 and v >= hi):
+                env[var] = v
+                try:
+                    self.exec_block(body, env)
+                except _Cycle as c:
+                    if c.name not in (None, name):
+                        raise
+                v += st
+            env[var] = v
+            return end + 1
+        if re.match(r"^if\s*\(", low):
+            cond_s, rest = split_paren(ln[2:].strip())
+            if rest.strip().lower() == "then":
+                is_if = lambda s: bool(re.match(r"^if\s*\(.*\)\s*then$", s))
+                is_end = lambda s: bool(re.match(r"^end\s*if\b", s))
+                is_mid = lambda s: bool(re.match(r"^else\b", s))
+                end, mids = self.find_end(lines, i, is_if, is_end, (is_mid,))
+                branches, start, cond = [], i + 1, cond_s
+                for mj in mids + [end]:
+                    branches.append((cond, lines[start:mj]))
+                    if mj == end:
+                        break
+                    m2 = re.match(r"^else\s*if\s*\((.*)\)\s*then$", lines[mj], re.I)
+                    cond = m2.group(1) if m2 else None
+                    start = mj + 1
+                for cond, blk in branches:
+                    if cond is None or bool(self.ev(parse_expr(cond), env)):
+                        self.exec_block(blk, env)
+                        break
+                return end + 1
+            if bool(self.ev(parse_expr(cond_s), env)):
+                self.exec_stmt([rest.strip()], 0, env)
+            return i + 1
+        if re.match(r"^select\s+case\b", low):
+            is_sel = lambda s: bool(re.match(r"^select\s+case\b", s))
+            is_end = lambda s: bool(re.match(r"^end\s*select\b", s))
+            is_case = lambda s: bool(re.match(r"^case\b", s))
+            end, mids = self.find_end(lines, i, is_sel, is_end, (is_case,))
+            sel = self.ev(parse_expr(ln[ln.index("(") + 1:ln.rindex(")")]), env)
+            for a, mj in enumerate(mids):
+                stop = mids[a + 1] if a + 1 < len(mids) else end
+                spec = lines[mj][4:].strip()
+                if spec.lower() == "default" or self.case_match(spec, sel, env):
+                    self.exec_block(lines[mj + 1:stop], env)
+                    break
+            return end + 1
+        if re.match(r"^cycle\b", low):
+            parts = low.split()
+            raise _Cycle(parts[1] if len(parts) > 1 else None)
+        if re.match(r"^\d+\s+format\b", low):  # FORMAT statements do nothing
+            return i + 1
+        if low in ("continue", "return") or re.match(r"^(print|write)\b", low):
+            if low == "return":
+                raise _Return()
+            return i + 1
+        if re.match(r"^stop\b", low):
+            raise RuntimeError("reference executed STOP")
+        if re.match(r"^call\b", low):
+            node = parse_expr(ln[4:].strip())
+            r = self.routines[node[1]]
+            self.run(r, [self.section_actual(s, env) for s in node[2]])
+            return i + 1
+        # Assignment.
+        lhs_s, rhs_s = split_assign(ln)
+        rhs = self.ev(parse_expr(rhs_s), env)
+        if isinstance(rhs, np.ndarray):
+            rhs = rhs.copy()
+        lhs = parse_expr(lhs_s)
+        if lhs[0] == "var":
+            cur = env.get(lhs[1])
+            if isinstance(cur, FArray):
+                cur.data[...] = rhs
+            else:
+                env[lhs[1]] = rhs
+        else:
+            arr = env.get(lhs[1], self.globals.get(lhs[1]))
+            arr.data[self.index_tuple(arr, lhs[2], env)] = rhs
+        return i + 1
+
+    def case_match(self, spec, sel, env):
+        inner = spec[spec.index("(") + 1:spec.rindex(")")]
+        for item in split_top(inner, ","):
+            if ":" in item:
+                lo, hi = item.split(":")
+                if int(self.ev(parse_expr(lo), env)) <= sel <= int(self.ev(parse_expr(hi), env)):
+                    return True
+            elif sel == self.ev(parse_expr(item), env):
+                return True
+        return False
+
+
+class _Cycle(Exception):
+    def __init__(self, name):
+        self.name = name
+
+
+class _Return(Exception):
+    pass
+
+
+def split_top(s: str, sep: str) -> list:
+    """Split at `sep` outside parentheses."""
+    out, depth, cur = [], 0, ""
+    for ch in s:
+        if ch == "(":
+            depth += 1
+        elif ch == ")":
+            depth -= 1
+        if ch == sep and depth == 0:
+            out.append(cur)
+            cur = ""
+        else:
+            cur += ch
+    out.append(cur)
+    return out
+
+
+def split_paren(s: str):
+    """'(cond) rest' -> ('cond', 'rest')."""
+    depth = 0
+    for k, ch in enumerate(s):
+        if ch == "(":
+            depth += 1
+        elif ch == ")":
+            depth -= 1
+            if depth == 0:
+                return s[1:k], s[k + 1:]
+    raise SyntaxError(s)
+
+
+def split_assign(s: str):
+    depth = 0
+    for k, ch in enumerate(s):
+        if ch == "(":
+            depth += 1
+        elif ch == ")":
+            depth -= 1
+        elif ch == "=" and depth == 0 and s[k - 1] not in "<>/=" and s[k + 1] != "=":
+            return s[:k], s[k + 1:]
+    raise SyntaxError(f"not an assignment: {s!r}")

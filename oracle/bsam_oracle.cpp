@@ -5,12 +5,12 @@
 // and bench.py's cpu_baseline leg load this file's library; the product path
 // (bsam_b200/, include/) never does.
 //
-// Parity pinning: the leaf routines are PINNED bit for bit against fixtures
-// made by executing the reference's own Fortran source with a Fortran-subset
-// interpreter (tests/golden/, tests/test_golden_reference.py); the V-cycle
-// and time-loop composition is UNPINNED (no Fortran compiler in this image,
-// no tests or golden vectors in the reference) and is checked by
-// known-answer tests and invariants (tests/test_oracle.py,
+// Parity pinning: PINNED bit for bit against fixtures made by executing the
+// reference's own Fortran source with a Fortran-subset interpreter
+// (tests/golden/, tests/test_golden_reference.py) -- the leaf routines and
+// their composition (MultigridIterations, the V-cycle, SetGhost, FillDown,
+// ErrorAFAS) on uniform 2D / 3D and refined 2D hierarchies.  Known-answer
+// tests and invariants add to that (tests/test_oracle.py,
 // tests/test_oracle_amr.py).
 //
 // Faithfulness rules followed throughout:

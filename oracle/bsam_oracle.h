@@ -7,14 +7,20 @@
  * the CUDA path; the product never links, loads or calls it.
  *
  * Parity pinning: the reference is Fortran 90, no Fortran compiler exists in
- * this image, and the reference ships no tests or golden outputs.  The leaf
+ * this image, and the reference ships no tests or golden outputs.  The oracle
+ * is PINNED bit for bit against fixtures produced by executing the
+ * reference's own Fortran source with a Fortran-subset interpreter
+ * (tests/golden/make_golden.py, tests/test_golden_reference.py): the leaf
  * routines (relaxation, operator, source, restriction, P1 prolongation,
- * SetBC/UserBC, Interpolate2D) are PINNED bit for bit against fixtures
- * produced by executing the reference's own Fortran source with a
- * Fortran-subset interpreter (tests/golden/make_golden.py,
- * tests/test_golden_reference.py).  Their composition into the V-cycle and
- * time loop (afasroutines.f90, bsamroutines.f90) is UNPINNED: it is checked
- * by known-answer tests and invariants derived from the reference's formulas.
+ * SetBC/UserBC, Interpolate2D) and their composition, MultigridIterations
+ * with the V-cycle, SetGhost, FillDown and ErrorAFAS (afasroutines.f90,
+ * boundary.f90), on uniform 2D / 3D hierarchies and a 2D hierarchy with two
+ * refined levels.  Restated rather than interpreted on both sides: TreeOps'
+ * level traversal order and TakeTimeSteps' step sequence on an unchanged
+ * hierarchy (bsamroutines.f90:632-723); the regridding itself is not on the
+ * path.  The interpreter evaluates as the Fortran text reads, with no fused
+ * multiply-add; a reference build that contracts a*b+c into FMA would differ
+ * from it in the last bits.
  *
  * Array layout (every array argument): Fortran column-major, i fastest, with
  * the reference's bounds -- q(0:mx1+1, 0:mx2+1[, 0:mx3+1], 1:2) with the ghost

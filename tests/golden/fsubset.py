@@ -3,15 +3,26 @@ routines, used only to generate golden fixtures (tests/golden/*.npz) from the
 reference's own source text.
 
 No Fortran compiler exists in this image, so the reference cannot be built.
-Its leaf routines (RelaxGrid2D/3D, Operator2D/3D with ULap/UDiv/ULapMob,
-Source2D/3D, Restriction2D/3D, Bi/TriLinProlongationP1, SetBC2D/3D with
-UserBC2D/3D, Interpolate2D) are plain array statements, DO loops, IF /
-SELECT CASE and elemental functions; this module parses those routines from
-the reference files and executes them with numpy in IEEE double precision
-(the reference builds with -fdefault-real-8), evaluating every expression
-left to right as written and every array statement's right-hand side before
-its assignment.  Not supported (and not needed by those routines): derived
-types, pointers, WHERE, I/O, character data, implicit typing.
+Its hot-path routines are plain array statements, DO loops, IF / SELECT CASE,
+elemental functions and nodeinfo component references: the leaf routines
+(RelaxGrid2D/3D, Operator2D/3D with ULap/UDiv/ULapMob, Source2D/3D,
+Restriction2D/3D, Bi/TriLinProlongationP1, SetBC2D/3D with UserBC2D/3D,
+Interpolate2D) and their composition (MultigridIterations, AFASVcycle,
+LevelRelax, FillDown, ErrorAFAS and the per-patch functions of
+afasroutines.f90; SetGhost, InterpolateCoarseFine, TransferBC, GhostOverlap,
+SetBC and GetCoarseGhostPoints of boundary.f90).  This module parses those
+routines from the reference files and executes them with numpy in IEEE double
+precision (the reference builds with -fdefault-real-8), evaluating every
+expression left to right as written, every array statement's right-hand side
+before its assignment, and SUM sequentially in array element order.
+
+The tree module (TreeOps) is pointer code and is not interpreted: a caller
+supplies `tree`, an object whose on(level) lists the level's nodeinfo records
+in ApplyOnLevel order, and the interpreter provides ApplyOnLevel,
+ApplyOnLevelPairs (each grid with every later one) and GetParentInfo
+(lib/treeops.f90:536-610) over it.  Records are Python objects whose
+attributes are the nodeinfo components.  Not supported (and not needed):
+WHERE, character data, implicit typing, pointer assignment.
 
 Only make_golden.py imports this module, in a container that has the
 reference source; the tests read the fixtures it wrote.
@@ -188,6 +199,9 @@ class Parser:
             return e
         if kind == "name":
             self.take()
+            while self.peek()[1] == "%":  # component chain a%b%c -> one name
+                self.take()
+                val = val + "%" + self.take()[1]
             if self.peek()[1] == "(":
                 self.take()
                 args = []
@@ -236,8 +250,8 @@ class Routine:
 
 
 _HEAD = re.compile(r"^(?:(elemental|recursive|pure)\s+)?(?:(integer|real|logical)\s+)?"
-                   r"(subroutine|function)\s+(\w+)\s*\(([^)]*)\)\s*(?:result\s*\(\s*(\w+)\s*\))?",
-                   re.I)
+                   r"(subroutine|function)\s+(\w+)\s*(?:\(([^)]*)\))?\s*"
+                   r"(?:result\s*\(\s*(\w+)\s*\))?\s*$", re.I)
 
 
 def extract_routines(src: str) -> dict:
@@ -251,7 +265,7 @@ def extract_routines(src: str) -> dict:
         elemental = (m.group(1) or "").lower() == "elemental"
         kind = m.group(3).lower()
         name = m.group(4).lower()
-        args = [a.strip().lower() for a in m.group(5).split(",") if a.strip()]
+        args = [a.strip().lower() for a in (m.group(5) or "").split(",") if a.strip()]
         result = (m.group(6) or (name if kind == "function" else "")).lower()
         j = i + 1
         while not re.match(rf"^end\s+{kind}\b", lines[j], re.I):
@@ -261,7 +275,7 @@ def extract_routines(src: str) -> dict:
             low = ln.lower()
             if re.match(r"^(use|implicit)\b", low):
                 continue
-            if re.match(r"^(real|integer|logical|double\s+precision)\b", low) and "::" in ln:
+            if re.match(r"^(real|integer|logical|double\s+precision|type\s*\()", low) and "::" in ln:
                 decls.append(ln)
             elif re.match(r"^(real|integer|logical)\s+\w", low) and "=" not in ln.split("::")[0]:
                 decls.append(ln)
@@ -282,10 +296,37 @@ def parse_module_parameters(src: str) -> dict:
     return consts
 
 
+class Record:
+    """A derived-type value (nodeinfo, funcparam): components are attributes."""
+
+    def __init__(self, **comps):
+        self.__dict__.update(comps)
+
+
+_MISSING = object()
+
+
 class Interp:
-    def __init__(self, routines: dict, globals_: dict):
+    def __init__(self, routines: dict, globals_: dict, tree=None):
         self.routines = routines
         self.globals = dict(globals_)
+        self.tree = tree        # TreeOps stand-in: tree.on(level) -> records
+        self.current = []       # ApplyOnLevel's current record (GetParentInfo)
+        self.printed = []       # numeric items of every executed PRINT
+
+    def lookup(self, name, env):
+        """A variable, or a component chain a%b%c, from the locals, then the
+        module variables; _MISSING when the base name is neither."""
+        base, *comps = name.split("%")
+        if base in env:
+            obj = env[base]
+        elif base in self.globals:
+            obj = self.globals[base]
+        else:
+            return _MISSING
+        for c in comps:
+            obj = getattr(obj, c)
+        return obj
 
     # -- evaluation -------------------------------------------------------------
     def ev(self, node, env):
@@ -294,7 +335,9 @@ class Interp:
             return node[1]
         if k == "var":
             name = node[1]
-            v = env[name] if name in env else self.globals[name]
+            v = self.lookup(name, env)
+            if v is _MISSING:
+                raise NameError(name)
             return v.data if isinstance(v, FArray) else v
         if k == "neg":
             return -self.ev(node[1], env)
@@ -311,9 +354,10 @@ class Interp:
             if op == "*":
                 return a * b
             if op == "/":
-                if isinstance(a, (int, np.integer)) and isinstance(b, (int, np.integer)):
-                    q = abs(a) // abs(b)
-                    return q if (a >= 0) == (b >= 0) else -q
+                if np.asarray(a).dtype.kind in "iu" and np.asarray(b).dtype.kind in "iu":
+                    q = np.abs(a) // np.abs(b)  # integer division truncates
+                    return np.where((np.asarray(a) >= 0) == (np.asarray(b) >= 0), q, -q) \
+                        if np.ndim(q) else (q if (a >= 0) == (b >= 0) else -q)
                 return a / b
             if op == "**":
                 if isinstance(b, (int, np.integer)) and b >= 0:
@@ -365,7 +409,7 @@ class Interp:
 
     def ref(self, node, env):
         _, name, subs = node
-        arr = env.get(name, self.globals.get(name))
+        arr = self.lookup(name, env)
         if isinstance(arr, FArray):
             return arr.data[self.index_tuple(arr, subs, env)]
         return self.call_function(name, subs, env)
@@ -373,12 +417,12 @@ class Interp:
     def section_actual(self, s, env):
         """An actual argument: arrays and sections keep their storage (views)."""
         if s[0] == "var":
-            v = env.get(s[1], self.globals.get(s[1]))
+            v = self.lookup(s[1], env)
             if isinstance(v, FArray):
                 return FArray(v.data, (1,) * v.data.ndim)
             return v
         if s[0] == "ref":
-            arr = env.get(s[1], self.globals.get(s[1]))
+            arr = self.lookup(s[1], env)
             if isinstance(arr, FArray):
                 view = arr.data[self.index_tuple(arr, s[2], env)]
                 if isinstance(view, np.ndarray) and view.ndim > 0:
@@ -411,6 +455,25 @@ class Interp:
             return np.abs(self.ev(subs[0], env))
         if name == "sqrt":
             return np.sqrt(self.ev(subs[0], env))
+        if name == "sum":  # sequential, in array element order
+            a = np.asarray(self.ev(subs[0], env))
+            acc = np.float64(0.0) if a.dtype.kind == "f" else 0
+            for x in np.ravel(a, order="F"):
+                acc = acc + x
+            return acc
+        if name == "product":
+            a = np.asarray(self.ev(subs[0], env))
+            acc = 1
+            for x in np.ravel(a, order="F"):
+                acc = acc * x
+            return acc
+        if name == "maxval":
+            return np.max(self.ev(subs[0], env))
+        if name == "any":
+            return bool(np.any(self.ev(subs[0], env)))
+        if name == "getparentinfo":  # GetParentInfo(parent) -> err_ok
+            env[subs[0][1]] = self.current[-1].parent
+            return 0
         if name in ("real", "dble"):
             return np.float64(self.ev(subs[0], env)) if np.isscalar(self.ev(subs[0], env)) else \
                 self.ev(subs[0], env).astype(np.float64)
@@ -447,6 +510,10 @@ class Interp:
                 nm = m.group(1).lower()
                 local_dims = m.group(3) or dims
                 init = m.group(5)
+                if base.startswith("type"):
+                    if nm not in r.args:  # funcparam locals; nodeinfo pointers unset
+                        env[nm] = Record(iswitch=0) if "funcparam" in base else None
+                    continue
                 if nm in r.args:
                     a = env.get(nm)
                     if local_dims is not None and isinstance(a, FArray):
@@ -486,7 +553,10 @@ class Interp:
         for an, av in zip(r.args, actuals):
             env[an] = av
         self.declare(r, env)
-        self.exec_block(r.body, env)
+        try:
+            self.exec_block(r.body, env)
+        except _Return:
+            pass
         if r.kind == "function":
             v = env[r.result]
             return v.data if isinstance(v, FArray) else v
@@ -541,6 +611,10 @@ class Interp:
                 except _Cycle as c:
                     if c.name not in (None, name):
                         raise
+                except _Exit as e:
+                    if e.name not in (None, name):
+                        raise
+                    return end + 1  # the DO variable keeps its value
                 v += st
             env[var] = v
             return end + 1
@@ -583,6 +657,14 @@ class Interp:
         if re.match(r"^cycle\b", low):
             parts = low.split()
             raise _Cycle(parts[1] if len(parts) > 1 else None)
+        if re.match(r"^exit\b", low):
+            parts = low.split()
+            raise _Exit(parts[1] if len(parts) > 1 else None)
+        if re.match(r"^print\s*\*\s*,", low):
+            items = split_print(ln[ln.index(",") + 1:])
+            self.printed.append(tuple(self.ev(parse_expr(it), env) for it in items
+                                      if not it.strip().startswith(("'", '"'))))
+            return i + 1
         if re.match(r"^\d+\s+format\b", low):  # FORMAT statements do nothing
             return i + 1
         if low in ("continue", "return") or re.match(r"^(print|write)\b", low):
@@ -593,6 +675,12 @@ class Interp:
             raise RuntimeError("reference executed STOP")
         if re.match(r"^call\b", low):
             node = parse_expr(ln[4:].strip())
+            if node[1] in ("applyonlevel", "applyonlevelpairs"):
+                level = int(self.ev(node[2][0], env))
+                fn = self.routines[node[2][1][1]]
+                param = self.lookup(node[2][2][1], env)
+                self.apply_on_level(level, fn, param, pairs=node[1] == "applyonlevelpairs")
+                return i + 1
             r = self.routines[node[1]]
             self.run(r, [self.section_actual(s, env) for s in node[2]])
             return i + 1
@@ -603,15 +691,42 @@ class Interp:
             rhs = rhs.copy()
         lhs = parse_expr(lhs_s)
         if lhs[0] == "var":
-            cur = env.get(lhs[1])
+            name = lhs[1]
+            if "%" in name:
+                owner_s, comp = name.rsplit("%", 1)
+                owner, scope, key = self.lookup(owner_s, env), None, comp
+            elif name in env or name not in self.globals:
+                owner, scope, key = None, env, name
+            else:  # a module variable
+                owner, scope, key = None, self.globals, name
+            cur = getattr(owner, key) if owner is not None else scope.get(key)
             if isinstance(cur, FArray):
                 cur.data[...] = rhs
+            elif owner is not None:
+                setattr(owner, key, rhs)
             else:
-                env[lhs[1]] = rhs
+                scope[key] = rhs
         else:
-            arr = env.get(lhs[1], self.globals.get(lhs[1]))
+            arr = self.lookup(lhs[1], env)
             arr.data[self.index_tuple(arr, lhs[2], env)] = rhs
         return i + 1
+
+    def apply_on_level(self, level, fn, param, pairs):
+        """ApplyOnLevel / ApplyOnLevelPairs (lib/treeops.f90:536-610): fn on
+        every record of the level in list order (pairs: each record with every
+        later one); a nonzero return ends the traversal."""
+        recs = self.tree.on(level)
+        for a, rec in enumerate(recs):
+            for other in (recs[a + 1:] if pairs else [None]):
+                self.current.append(rec)
+                try:
+                    args = [rec, other, param] if pairs else [rec, param]
+                    code = self.run(fn, args)
+                finally:
+                    self.current.pop()
+                if code:
+                    self.tree.errcode = code
+                    return
 
     def case_match(self, spec, sel, env):
         inner = spec[spec.index("(") + 1:spec.rindex(")")]
@@ -632,6 +747,33 @@ class _Cycle(Exception):
 
 class _Return(Exception):
     pass
+
+
+class _Exit(Exception):
+    def __init__(self, name):
+        self.name = name
+
+
+def split_print(s: str) -> list:
+    """The output items of a list-directed PRINT (commas outside quotes and
+    parentheses)."""
+    out, depth, cur, quote = [], 0, "", None
+    for ch in s:
+        if quote:
+            quote = None if ch == quote else quote
+        elif ch in "'\"":
+            quote = ch
+        elif ch == "(":
+            depth += 1
+        elif ch == ")":
+            depth -= 1
+        elif ch == "," and depth == 0:
+            out.append(cur)
+            cur = ""
+            continue
+        cur += ch
+    out.append(cur)
+    return [o for o in out if o.strip()]
 
 
 def split_top(s: str, sep: str) -> list:

@@ -13,9 +13,28 @@ on seeded inputs:
   SetBC2D/3D (+ the problem's UserBC2D/3D), Interpolate2D
       lib/boundary.f90
 
-Each case's inputs and outputs go to tests/golden/ref_<routine>.npz.  The
-tests compare the CPU oracle's restatement of the same routines with these
-outputs bit for bit (tests/test_golden_reference.py).
+and their composition, the time loop's multigrid solve on fixed hierarchies
+(uniform 2D and 3D, and 2D with refined levels):
+
+  MultigridIterations, AFASVcycle, LevelRelax, FillDown(Level), ErrorAFAS,
+  L2Error, SquareSum, GetSourceFunction, UpdateSourceFunction,
+  UpdateAuxInVcycle, RelaxPatch, RestrictSolution, CoarseLoadingFunction,
+  Residual, CorrectFine                       lib/afasroutines.f90
+  SetGhost, InterpolateCoarseFine, TransferBC, GhostOverlap, SetBC,
+  GetCoarseGhostPoints                        lib/boundary.f90
+  CopyQToQold                                 lib/bsamroutines.f90
+
+Each case's inputs and outputs go to tests/golden/ref_<case>.npz.  The tests
+compare the CPU oracle's restatement of the same routines with these outputs
+bit for bit (tests/test_golden_reference.py).
+
+What is restated here rather than interpreted: TreeOps' level lists and
+traversal (ApplyOnLevel order = the order of the patch records given),
+AllocFields (q and qold zeroed, every other field NaN so that a read of an
+undefined value shows in the output), and TakeTimeSteps' step sequence on an
+unchanged hierarchy -- SetGhost(level, 0) from the root up (what
+AMR(rootlevel) leaves), FillDown(solutionfield) on the first step,
+CopyQToQold on every level, MultigridIterations (bsamroutines.f90:632-723).
 
 Usage: python tests/golden/make_golden.py [reference_dir]
 """
@@ -28,7 +47,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 import fsubset as F  # noqa: E402
+from bsam_b200 import amr, workloads as W  # noqa: E402  (pure-Python hierarchy builders)
 
 REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
 DT, EPS, ALPHA = 1.0e-4, 0.02, 1.0
@@ -50,6 +71,181 @@ def load() -> F.Interp:
 
 def fa(a, lb):
     return F.FArray(np.array(a, dtype=np.float64, copy=True), lb)
+
+
+# ---- the composition ---------------------------------------------------------------
+
+COMPOSITION_FILES = ("problems/simple_cahn-hilliard/problem.f90", "lib/gridutilities.f90",
+                     "lib/boundary.f90", "lib/afasroutines.f90")
+
+
+class Tree:
+    """TreeOps' level lists: on(level) in ApplyOnLevel order."""
+
+    def __init__(self, recs):
+        self.levels, self.errcode = {}, 0
+        for r in recs:
+            self.levels.setdefault(r.level, []).append(r)
+
+    def on(self, level):
+        return self.levels.get(level, [])
+
+
+def records(hier):
+    """nodeinfo records of a hierarchy's patches, fields as AllocFields
+    leaves them (lib/bsamstorage.f90:46-123) except that the values it leaves
+    undefined are NaN."""
+    nd = hier.ndims
+    recs = []
+    for d in hier.descs:
+        mx = list(d["mx"])
+        r = F.Record(level=d["level"], nrvars=2, maux=0, mbc=1, tobedeleted=False, parent=None,
+                     mx=F.FArray(np.array(mx, dtype=np.int64), (1,)),
+                     mbounds=F.FArray(np.array(d["mbounds"], dtype=np.int64), (1, 1)),
+                     mglobal=F.FArray(np.array(d["mglobal"], dtype=np.int64), (1, 1)),
+                     mthbc=F.FArray(np.array(d["mthbc"], dtype=np.int64), (1,)),
+                     dx=fa([d["dx"]] * 3, (1,)), xlower=fa(d["xlower"], (1,)))
+        cmx = [1 if m % 2 else m // 2 for m in mx]
+        ring = lambda m: tuple(m[n] + 2 if n < nd else 1 for n in range(3))
+        inner = tuple(mx[n] if n < nd else 1 for n in range(3))
+        lbr = (0, 0, 0 if nd == 3 else 1, 1)
+        nan = lambda shp, lb: F.FArray(np.full(shp, np.nan, order="F"), lb)
+        r.q = F.FArray(np.zeros(ring(mx) + (2,), order="F"), lbr)
+        r.qold = F.FArray(np.zeros(ring(mx) + (2,), order="F"), lbr)
+        r.qc = nan(ring(cmx) + (2,), lbr)
+        r.aux = nan(ring([1, 1, 1]) + (1,), lbr)  # maux = 0: mmaux = 1, amx = 1
+        for name in ("f", "rf", "ftmp"):
+            setattr(r, name, nan(inner + (2,), (1, 1, 1, 1)))
+        recs.append(r)
+    for r, d in zip(recs, hier.descs):
+        if d["parent"] >= 0:
+            r.parent = recs[d["parent"]]
+    return recs
+
+
+def run_composition(hier, nsteps):
+    """The reference's multigrid solve, interpreted, for nsteps time steps.
+    Returns (final q of every patch on a level >= 0, V-cycles per step,
+    residual trace per step as MultigridIterations prints it)."""
+    routines, consts = {}, {}
+    for rel in COMPOSITION_FILES:
+        src = open(os.path.join(REF, rel)).read()
+        got = F.extract_routines(src)
+        clash = set(got) & set(routines)
+        if clash:
+            raise RuntimeError(f"routine names defined twice: {clash}")
+        routines.update(got)
+        consts.update(F.parse_module_parameters(src))
+    bsam = F.extract_routines(open(os.path.join(REF, "lib/bsamroutines.f90")).read())
+    routines["copyqtoqold"] = bsam["copyqtoqold"]
+    recs = records(hier)
+    for k, i in enumerate(hier.state_patches()):
+        recs[i].q.data[...] = hier.q0s[k].reshape(recs[i].q.data.shape, order="F")
+    levels = [d["level"] for d in hier.descs]
+    minlevel, finest = min(levels), max(levels)
+    g = {"dt": hier.dt, "eps": hier.eps, "eps2": hier.eps * hier.eps, "alpha": hier.alpha,
+         "ndims": hier.ndims, "maxdims": 3, "maxnrvars": 25, "rootlevel": 0,
+         "sourcefield": 1, "solutionfield": 2, "err_ok": 0, "finestlevel": finest,
+         "minlevel": minlevel, "maxvcycles": hier.maxvcycles, "qerrortol": hier.qerrortol,
+         "nsmoothingpasses": hier.nsmoothingpasses, "updateauxfreq": 1, "errortype": 1,
+         "eqtag": 1, "lconverged": False, "periodicboundaryconditions": False,
+         "integralresult": fa(np.zeros(2), (1,)), "componentintegral": fa(np.zeros(25), (1,))}
+    I = F.Interp(routines, g, Tree(recs))
+    for name, expr in consts.items():
+        I.globals[name] = I.ev(F.parse_expr(expr), {})
+    dummy = F.Record(iswitch=0)
+
+    def ghosts():
+        for level in range(0, finest + 1):
+            I.run(routines["setghost"], [level, 0])
+
+    def copy_q_to_qold():
+        for level in range(minlevel, finest + 1):
+            I.apply_on_level(level, routines["copyqtoqold"], dummy, pairs=False)
+
+    ghosts()            # BSAMSolver: SetGhost, CopyQToQold (bsamroutines.f90:144-147)
+    copy_q_to_qold()
+    nvc, traces = [], []
+    for step in range(nsteps):
+        ghosts()
+        if step == 0:
+            I.run(routines["filldown"], [g["solutionfield"]])
+        copy_q_to_qold()
+        I.printed.clear()
+        I.run(routines["multigriditerations"], [])
+        if I.tree.errcode:
+            raise RuntimeError(f"ApplyOnLevel error {I.tree.errcode}")
+        trace = [float(p[1]) for p in I.printed]  # print *, 'it =', itmg, ' residual =', r
+        nvc.append(len(trace))
+        traces.append(trace + [-1.0] * (hier.maxvcycles - len(trace)))
+    q = [recs[i].q.data.reshape(hier.q0s[k].shape, order="F").copy()
+         for k, i in enumerate(hier.state_patches())]
+    for a in q:
+        if not np.all(np.isfinite(a)):
+            raise RuntimeError("an undefined value reached q")
+    return q, np.array(nvc, dtype=np.int32), np.array(traces)
+
+
+def uniform_hierarchy(nd, n, mthbc, eps, qerrortol, maxvcycles, seed):
+    """A uniform n^nd root on [0,1]^nd with its below-root levels (automatic
+    minlevel), as RootInit / CreateBelowSeedLevels build it.  Initial
+    composition: 2D, amr.build's sine wave with seeded 1e-3 noise; 3D, the
+    seeded spinodal field c0 = 0.5 + 0.05 U(-1, 1)."""
+    if nd == 2:
+        return amr.build(n, [], eps=eps, qerrortol=qerrortol, mthbc=mthbc, seed=seed,
+                         field="wave", maxvcycles=maxvcycles)
+    descs, m, lev = [], n, 0
+    while True:
+        coarser = m % 2 == 0 and lev < 10
+        descs.append({"level": -lev, "parent": lev + 1 if coarser else -1, "mx": [m] * 3,
+                      "mbounds": [[1, m // 2 if coarser else m]] * 3, "mglobal": [[1, m]] * 3,
+                      "mthbc": [mthbc] * 6, "dx": (1.0 / n) * 2 ** lev, "xlower": [0.0] * 3})
+        if not coarser:
+            break
+        m //= 2
+        lev += 1
+    h = 1.0 / n
+    c0 = 0.5 + 0.05 * W.uniform(seed, n ** 3, -1.0, 1.0)
+    q0 = W.initial_q(3, (n, n, n), c0, h, eps, 1.0)
+    return amr.Hierarchy(ndims=3, descs=descs, q0s=[q0], dt=5e-5, eps=eps,
+                         qerrortol=qerrortol, maxvcycles=maxvcycles)
+
+
+def hier_arrays(hier):
+    """A hierarchy as flat arrays for a fixture."""
+    D = hier.descs
+    return {"ndims": hier.ndims, "level": np.array([d["level"] for d in D]),
+            "parent": np.array([d["parent"] for d in D]),
+            "mx": np.array([d["mx"] for d in D]), "mbounds": np.array([d["mbounds"] for d in D]),
+            "mglobal": np.array([d["mglobal"] for d in D]),
+            "mthbc": np.array([d["mthbc"] for d in D]), "dxs": np.array([d["dx"] for d in D]),
+            "xlower": np.array([d["xlower"] for d in D]),
+            "q0": np.concatenate([q.ravel(order="F") for q in hier.q0s]),
+            "hdt": hier.dt, "heps": hier.eps, "qerrortol": hier.qerrortol,
+            "maxvcycles": hier.maxvcycles, "nsmoothingpasses": hier.nsmoothingpasses}
+
+
+def composition_cases():
+    out = {}
+    cases = {
+        # 16^2 root, levels 0..-4, Neumann faces.
+        "mg_uniform2d": (uniform_hierarchy(2, 16, 1, 0.05, 1e-10, 8, 7), 2),
+        # 8^3 root, levels 0..-3, user-coded faces.
+        "mg_uniform3d": (uniform_hierarchy(3, 8, 10, 0.1, 1e-10, 6, 8), 2),
+        # 16^2 root, two siblings on level 1 (one on a physical corner), one
+        # level-2 patch.
+        "mg_amr2d": (amr.build(16, [(1, (1, 1), (12, 16)), (1, (13, 9), (14, 12)),
+                                    (2, (5, 9), (12, 12))],
+                               eps=0.05, qerrortol=1e-10, maxvcycles=8, seed=9), 2),
+    }
+    for name, (hier, nsteps) in cases.items():
+        q, nvc, tr = run_composition(hier, nsteps)
+        d = hier_arrays(hier)
+        d.update({"nsteps": nsteps, "q_out": np.concatenate([a.ravel(order="F") for a in q]),
+                  "nvcycles": nvc, "trace": tr})
+        out[name] = d
+        print(name, "V-cycles per step", nvc.tolist())
+    return out
 
 
 def ia(v):
@@ -134,6 +330,8 @@ def main():
                    ia(mth), ipass])
             res[f"qf_out_{n}_{ipass}"] = qq.data
     out["interpolate2d"] = res
+
+    out.update(composition_cases())
 
     for name, d in out.items():
         np.savez_compressed(os.path.join(HERE, f"ref_{name}.npz"),

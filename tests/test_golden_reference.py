@@ -9,9 +9,14 @@ fixture bit for bit.  The CUDA kernels are in turn bit-identical to the
 oracle (tests/test_gpu_parity.py), so these fixtures pin the whole chain to
 the reference's own arithmetic for: RelaxGrid2D/3D, Operator2D/3D,
 Source2D/3D, Restriction2D/3D, Bi/TriLinProlongationP1, SetBC2D/3D with
-UserBC2D/3D, Interpolate2D.
+UserBC2D/3D, Interpolate2D -- and for their composition, the multigrid solve
+of the time loop (MultigridIterations with the V-cycle, SetGhost, FillDown,
+ErrorAFAS; afasroutines.f90, boundary.f90) on uniform 2D and 3D hierarchies
+and on a 2D hierarchy with two refined levels.
 """
+import ctypes
 import os
+import types
 
 import numpy as np
 import pytest
@@ -74,3 +79,41 @@ def test_interpolate2d_matches_reference(oracle):
             assert np.array_equal(got, d[f"qf_out_{n}_{ipass}"]), (n, ipass)
         n += 1
     assert n >= 3
+
+
+MG_CASES = ["mg_uniform2d", "mg_uniform3d", "mg_amr2d"]
+
+
+@pytest.mark.parametrize("name", MG_CASES)
+def test_multigrid_composition_matches_reference(oracle, golden_hier, name):
+    """The time loop's multigrid solve on a fixed hierarchy: the oracle's
+    MultigridIterations (with SetGhost, FillDown, ErrorAFAS and the V-cycle)
+    against the reference's own afasroutines.f90 / boundary.f90 composition,
+    bit for bit: every patch's q after the steps, V-cycles per step and the
+    final residual of each step."""
+    hier, d = golden_hier(name)
+    nsteps = int(d["nsteps"])
+    ref = oracle.run_hier(hier, nsteps)
+    assert np.array_equal(ref["nvcycles"], d["nvcycles"]), (ref["nvcycles"], d["nvcycles"])
+    last = [d["trace"][s, d["nvcycles"][s] - 1] for s in range(nsteps)]
+    assert np.array_equal(ref["residual"], last)
+    got = np.concatenate([q.ravel(order="F") for q in ref["q"]])
+    assert np.array_equal(got, d["q_out"])
+
+
+@pytest.mark.parametrize("name", ["mg_uniform2d", "mg_uniform3d"])
+def test_uniform_time_loop_matches_reference(oracle, golden_hier, name):
+    """orc_run_uniform (its own root and below-root construction) against the
+    same fixtures: the whole residual trace of every step and the final q."""
+    hier, d = golden_hier(name)
+    nd, root = hier.ndims, hier.descs[0]
+    nsteps = int(d["nsteps"])
+    prob = types.SimpleNamespace(
+        ndims=nd, mx=tuple(root["mx"]), xupper=(1.0, 1.0, 1.0), mthbc=tuple(root["mthbc"]),
+        minlevel=1, nsmoothingpasses=hier.nsmoothingpasses, maxvcycles=hier.maxvcycles,
+        dt=hier.dt, qerrortol=hier.qerrortol, alpha=hier.alpha, eps=hier.eps, nsteps=nsteps)
+    assert oracle.lib().orc_minlevel(ctypes.byref(oracle.params_of(prob))) == min(d["level"])
+    ref = oracle.run_uniform(prob, nsteps, q0=hier.q0s[0])
+    assert np.array_equal(ref["nvcycles"], d["nvcycles"])
+    assert np.array_equal(ref["trace"], d["trace"])
+    assert np.array_equal(ref["q"][-1].ravel(order="F"), d["q_out"])

@@ -1,4 +1,4 @@
-"""Fixed block-structured AMR hierarchies for the V-cycle (2D).
+"""Fixed block-structured AMR hierarchies for the V-cycle (2D and 3D).
 
 The reference builds its hierarchy by tagging and Berger-Rigoutsos
 clustering every time step (lib/bsamroutines.f90:939-1241, 1352-1579); the
@@ -129,18 +129,22 @@ def _desc(level, parent, mx, mbounds, mglobal, mthbc, dx, xlower):
 
 def build(n_root: int, boxes: list, eps: float, dt: float = 5e-5, qerrortol: float = 1e-9,
           mthbc: int = 1, minlevel: int = 1, seed: int = 2, field: str = "drop",
-          maxvcycles: int = 20) -> Hierarchy:
-    """2D hierarchy on [0,1]^2: an n_root^2 root, its below-root levels
-    (automatic minlevel: halve while even, at most 10 times), and refined
-    patches `boxes` = [(level, (i0, j0), (nx, ny)), ...] with (i0, j0) the
-    1-based global index of the patch's first cell on its level (odd) and
-    even sizes.  Each patch's parent is the patch of the level below that
-    contains its footprint (the first one listed).
+          maxvcycles: int = 20, ndims: int = 2) -> Hierarchy:
+    """Hierarchy on [0,1]^d (d = ndims, 2 or 3): an n_root^d root, its
+    below-root levels (automatic minlevel: halve while even, at most 10
+    times), and refined patches `boxes` = [(level, lo, size), ...] with lo the
+    1-based global index of the patch's first cell on its level (odd in every
+    dimension) and even sizes.  Each patch's parent is the patch of the level
+    below that contains its footprint (the first one listed).
 
     Initial composition (field "drop", as the AMR benchmark configuration):
     phi0 = tanh((0.25 - r)/(sqrt(2) eps)) + 1e-3 U(-1, 1) (seeded per
-    patch), c0 = (1 + phi0)/2, mu0 from the operator (workloads.initial_q)."""
-    nd = 2
+    patch), c0 = (1 + phi0)/2, mu0 from the operator (workloads.initial_q);
+    any other field: phi0 = 0.1 sin(2 pi x) cos(2 pi y) [cos(2 pi z)] plus
+    the same noise."""
+    nd = ndims
+    if nd not in (2, 3):
+        raise ValueError("ndims must be 2 or 3")
     h0 = 1.0 / n_root
     descs = []
     # Root (patch 0) and the below-root chain (patch l = level -l).
@@ -156,11 +160,13 @@ def build(n_root: int, boxes: list, eps: float, dt: float = 5e-5, qerrortol: flo
     for l in range(nlev + 1):
         n = sizes[l]
         parent = l + 1 if l < nlev else -1
-        mb = [(1, n // 2)] * 2 if l < nlev else [(1, n)] * 2
-        descs.append(_desc(-l, parent, (n, n), mb, [(1, n), (1, n)], [mthbc] * 4,
-                           h0 * (2 ** l), (0.0, 0.0)))
+        mb = [(1, n // 2)] * nd if l < nlev else [(1, n)] * nd
+        descs.append(_desc(-l, parent, (n,) * nd, mb, [(1, n)] * nd, [mthbc] * (2 * nd),
+                           h0 * (2 ** l), (0.0,) * nd))
     # Refined patches.
     for (level, lo, size) in boxes:
+        if len(lo) != nd or len(size) != nd:
+            raise ValueError("box dimensionality differs from ndims")
         if level < 1 or any(x % 2 == 0 for x in lo) or any(s % 2 for s in size):
             raise ValueError("patch origin must be odd and its size even")
         nglob = n_root * 2 ** level
@@ -188,24 +194,26 @@ def build(n_root: int, boxes: list, eps: float, dt: float = 5e-5, qerrortol: flo
             codes.append(mthbc if ghi[k] == nglob else INTERNAL)
         h = h0 / (2 ** level)
         descs.append(_desc(level, parent, size, mb, [(glo[k], ghi[k]) for k in range(nd)],
-                           codes, h, ((glo[0] - 1) * h, (glo[1] - 1) * h)))
+                           codes, h, tuple((glo[k] - 1) * h for k in range(nd))))
     # Initial states.
     q0s = []
     for i, d in enumerate(descs):
         if d["level"] < 0:
             continue
-        mx = d["mx"]
+        mx = d["mx"][:nd]
         h = d["dx"]
-        xs = d["xlower"][0] + (np.arange(mx[0]) + 0.5) * h
-        ys = d["xlower"][1] + (np.arange(mx[1]) + 0.5) * h
-        X, Y = np.meshgrid(xs, ys, indexing="ij")
+        axes = [d["xlower"][k] + (np.arange(mx[k]) + 0.5) * h for k in range(nd)]
+        X = np.meshgrid(*axes, indexing="ij")
         if field == "drop":
-            r = np.sqrt((X - 0.5) ** 2 + (Y - 0.5) ** 2)
+            r = np.sqrt(sum((X[k] - 0.5) ** 2 for k in range(nd)))
             phi = np.tanh((0.25 - r) / (math.sqrt(2.0) * eps))
         else:
-            phi = 0.1 * np.sin(2 * math.pi * X) * np.cos(2 * math.pi * Y)
-        noise = W.uniform(seed * 1000 + i, mx[0] * mx[1], -1.0, 1.0).reshape(mx[:2], order="F")
+            phi = 0.1 * np.sin(2 * math.pi * X[0]) * np.cos(2 * math.pi * X[1])
+            if nd == 3:
+                phi = phi * np.cos(2 * math.pi * X[2])
+        ncell = int(np.prod(mx))
+        noise = W.uniform(seed * 1000 + i, ncell, -1.0, 1.0).reshape(mx, order="F")
         c0 = 0.5 * (1.0 + (phi + 1e-3 * noise))
-        q0s.append(W.initial_q(nd, tuple(mx), c0.ravel(order="F"), h, eps, 1.0))
+        q0s.append(W.initial_q(nd, tuple(d["mx"]), c0.ravel(order="F"), h, eps, 1.0))
     return Hierarchy(ndims=nd, descs=descs, q0s=q0s, dt=dt, eps=eps, qerrortol=qerrortol,
                      maxvcycles=maxvcycles)

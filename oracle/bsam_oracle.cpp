@@ -544,6 +544,210 @@ void Interpolate2D(FArr& qf, const FArr& qc, const int* mx, int nv, const int mb
   }
 }
 
+constexpr double kC1 = 9.0 / 16.0, kC2 = 3.0 / 16.0, kC3 = 3.0 / 16.0, kC4 = 1.0 / 16.0;
+
+// GetFaceIndex (boundary.f90:1271-1297) of dimension d (0-based): the ghost,
+// second and first interior fine indices, the parent's index outside the
+// patch's footprint and the parent's boundary index of the footprint.
+struct FaceIdx {
+  int g, s, f, p, b;
+};
+FaceIdx GetFaceIndex(const int* mx, const int mb[3][2], int d, int parity) {
+  if (parity == 1) return {0, 2, 1, mb[d][0] - 1, mb[d][0]};
+  return {mx[d] + 1, mx[d] - 1, mx[d], mb[d][1] + 1, mb[d][1]};
+}
+
+// One dimension of an Interpolate3D array statement: the n elements of the
+// target section, of the two fine sources (a1 and a2 terms) and of the
+// parent section advance together, the fine indices by df, the parent's by dc.
+struct Ax {
+  int t, s, f, c, n, df, dc;
+};
+Ax ax_fixed(const FaceIdx& F) { return {F.g, F.s, F.f, F.p, 1, 0, 0}; }
+// The same fine index i in target and sources (the parent index along this
+// dimension is given by the statement's parent combination).
+Ax ax_at(int i) { return {i, i, i, 0, 1, 0, 0}; }
+// Target 3:m-1:2, sources 1:m-3:2 and 2:m-2:2, parent lo+1:...
+Ax ax_odd(int m, int lo) { return {3, 1, 2, lo + 1, m >= 4 ? (m - 2) / 2 : 0, 2, 1}; }
+// Target 2:m-2:2, sources 4:m:2 and 3:m-1:2, parent lo:...
+Ax ax_even(int m, int lo) { return {2, 4, 3, lo, m >= 4 ? (m - 2) / 2 : 0, 2, 1}; }
+
+// The parent term of a statement: one parent value (kind 0); the three-point
+// fit b1, b2, b3 over indices k[0..2] along dimension d (kind 1); the
+// four-point corner fit c1..c4 over (k[0], k[1]) along d and (k2[0], k2[1])
+// along d2 (kind 2: c1 at (k[0], k2[0]), c2 at (k[1], k2[0]), c3 at
+// (k[0], k2[1]), c4 at (k[1], k2[1])).
+struct Par {
+  int kind, d, k[3], d2, k2[2];
+};
+Par par_one() { return {0, 0, {0, 0, 0}, 0, {0, 0}}; }
+Par par_fit(int d, int k0, int k1, int k2) { return {1, d, {k0, k1, k2}, 0, {0, 0}}; }
+Par par_corner(int d, int f5, int f4, int d2, int g5, int g4) {
+  return {2, d, {f5, f4, 0}, d2, {g5, g4}};
+}
+
+// qf(target) = a1*qf(second) + a2*qf(first) + a3*parent, elementwise; the
+// right-hand side reads interior fine cells and parent cells only.
+void stmt3(FArr& qf, const FArr& qc, int nv, const Ax& X, const Ax& Y, const Ax& Z,
+           const Par& P) {
+  const Ax A[3] = {X, Y, Z};
+  for (int v = 1; v <= nv; ++v)
+    for (int c = 0; c < Z.n; ++c)
+      for (int b = 0; b < Y.n; ++b)
+        for (int a = 0; a < X.n; ++a) {
+          const int e[3] = {a, b, c};
+          int T[3], S[3], F[3], C[3];
+          for (int d = 0; d < 3; ++d) {
+            T[d] = A[d].t + e[d] * A[d].df;
+            S[d] = A[d].s + e[d] * A[d].df;
+            F[d] = A[d].f + e[d] * A[d].df;
+            C[d] = A[d].c + e[d] * A[d].dc;
+          }
+          auto pc = [&](int d, int k, int d2, int k2) {
+            int I[3] = {C[0], C[1], C[2]};
+            I[d] = k;
+            if (d2 >= 0) I[d2] = k2;
+            return qc(I[0], I[1], I[2], v);
+          };
+          double par;
+          if (P.kind == 0)
+            par = qc(C[0], C[1], C[2], v);
+          else if (P.kind == 1)
+            par = kB1 * pc(P.d, P.k[0], -1, 0) + kB2 * pc(P.d, P.k[1], -1, 0) +
+                  kB3 * pc(P.d, P.k[2], -1, 0);
+          else
+            par = kC1 * pc(P.d, P.k[0], P.d2, P.k2[0]) + kC2 * pc(P.d, P.k[1], P.d2, P.k2[0]) +
+                  kC3 * pc(P.d, P.k[0], P.d2, P.k2[1]) + kC4 * pc(P.d, P.k[1], P.d2, P.k2[1]);
+          qf(T[0], T[1], T[2], v) =
+              kA1 * qf(S[0], S[1], S[2], v) + kA2 * qf(F[0], F[1], F[2], v) + kA3 * par;
+        }
+}
+
+// Interpolate3D (boundary.f90:1299-1799), mbc = 1, statement by statement:
+// (1) the 8 corners, (2) the 12 edges, (3) the 6 faces (internal faces only)
+// with their corner cells.  Corners and edges on a physical face are skipped
+// only in the red pass (ipass = 1).  The check for edges 1-4 tests the z
+// face code against 99, not 999 (boundary.f90:1354), and is kept.  Every
+// statement reads interior fine cells and parent cells only.
+void Interpolate3D(FArr& qf, const FArr& qc, const int* mx, int nv, const int mb[3][2],
+                   const int* mthbc, int ipass) {
+  auto internal = [](int code) { return code == 2 || code == 999; };
+  auto skip = [&](int face, bool typo) {
+    const int code = mthbc[face];
+    const bool keep = typo ? (code == 2 || code == 99) : internal(code);
+    return !keep && ipass == 1;
+  };
+  // (1) Corners (boundary.f90:1322-1342).
+  for (int p1 = 1; p1 <= 2; ++p1) {
+    if (skip(p1 - 1, false)) continue;
+    const FaceIdx F1 = GetFaceIndex(mx, mb, 0, p1);
+    for (int p2 = 1; p2 <= 2; ++p2) {
+      if (skip(p2 + 1, false)) continue;
+      const FaceIdx F2 = GetFaceIndex(mx, mb, 1, p2);
+      for (int p3 = 1; p3 <= 2; ++p3) {
+        if (skip(p3 + 3, false)) continue;
+        const FaceIdx F3 = GetFaceIndex(mx, mb, 2, p3);
+        stmt3(qf, qc, nv, ax_fixed(F1), ax_fixed(F2), ax_fixed(F3), par_one());
+      }
+    }
+  }
+  // (2) Edges, along the dimension `e` not fixed (boundary.f90:1344-1478):
+  // odd cells from the diagonal below, the first cell with the fit at the
+  // footprint's low end, even cells from the diagonal above, the last cell
+  // with the fit at the high end.
+  auto edge = [&](int e, const Ax& A, const Ax& B) {
+    const int m = mx[e], lo = mb[e][0], hi = mb[e][1];
+    auto put = [&](const Ax& L, const Par& P) {
+      Ax D[3];
+      int k = 0;
+      for (int d = 0; d < 3; ++d) D[d] = d == e ? L : (k++ == 0 ? A : B);
+      stmt3(qf, qc, nv, D[0], D[1], D[2], P);
+    };
+    put(ax_odd(m, lo), par_one());
+    put(ax_at(1), par_fit(e, lo - 1, lo, lo + 1));
+    put(ax_even(m, lo), par_one());
+    put(ax_at(m), par_fit(e, hi + 1, hi, hi - 1));
+  };
+  for (int p1 = 1; p1 <= 2; ++p1) {  // edges 1-4: dimensions 1 and 3 fixed
+    if (skip(p1 - 1, false)) continue;
+    const FaceIdx F1 = GetFaceIndex(mx, mb, 0, p1);
+    for (int p3 = 1; p3 <= 2; ++p3) {
+      if (skip(p3 + 3, true)) continue;
+      const FaceIdx F3 = GetFaceIndex(mx, mb, 2, p3);
+      edge(1, ax_fixed(F1), ax_fixed(F3));
+    }
+  }
+  for (int p1 = 1; p1 <= 2; ++p1) {  // edges 5-8: dimensions 1 and 2 fixed
+    if (skip(p1 - 1, false)) continue;
+    const FaceIdx F1 = GetFaceIndex(mx, mb, 0, p1);
+    for (int p2 = 1; p2 <= 2; ++p2) {
+      if (skip(p2 + 1, false)) continue;
+      const FaceIdx F2 = GetFaceIndex(mx, mb, 1, p2);
+      edge(2, ax_fixed(F1), ax_fixed(F2));
+    }
+  }
+  for (int p2 = 1; p2 <= 2; ++p2) {  // edges 9-12: dimensions 2 and 3 fixed
+    if (skip(p2 + 1, false)) continue;
+    const FaceIdx F2 = GetFaceIndex(mx, mb, 1, p2);
+    for (int p3 = 1; p3 <= 2; ++p3) {
+      if (skip(p3 + 3, false)) continue;
+      const FaceIdx F3 = GetFaceIndex(mx, mb, 2, p3);
+      edge(0, ax_fixed(F2), ax_fixed(F3));
+    }
+  }
+  // (3) Faces (boundary.f90:1480-1797), internal faces only.  On face
+  // dimension d with the other dimensions u < w: yellow (even, even) and blue
+  // (odd, odd) cells in one colour, green (odd, even) and red (even, odd) in
+  // the other, each as the interior section plus the strips next to the
+  // face's edges; then its four corner cells with the four-point fit.  (Faces
+  // 3 and 4 list the strips of green and red the other way round; the strips
+  // are disjoint and in the same colour, so the result is the same.)
+  for (int d = 0; d < 3; ++d) {
+    const int u = d == 0 ? 1 : 0, w = d == 2 ? 1 : 2;
+    const int mu = mx[u], mw = mx[w];
+    const int u1 = mb[u][0], u2 = mb[u][1], w1 = mb[w][0], w2 = mb[w][1];
+    for (int p = 1; p <= 2; ++p) {
+      if (!internal(mthbc[2 * d + p - 1])) continue;
+      const FaceIdx F = GetFaceIndex(mx, mb, d, p);
+      auto put = [&](const Ax& U, const Ax& W, const Par& P) {
+        Ax D[3];
+        D[d] = ax_fixed(F);
+        D[u] = U;
+        D[w] = W;
+        stmt3(qf, qc, nv, D[0], D[1], D[2], P);
+      };
+      if (ipass == 0 || (p + ipass) % 2 == 0) {
+        // Yellow.
+        put(ax_even(mu, u1), ax_even(mw, w1), par_one());
+        put(ax_at(mu), ax_even(mw, w1), par_fit(u, u2 + 1, u2, u2 - 1));
+        put(ax_even(mu, u1), ax_at(mw), par_fit(w, w2 + 1, w2, w2 - 1));
+        // Blue.
+        put(ax_odd(mu, u1), ax_odd(mw, w1), par_one());
+        put(ax_odd(mu, u1), ax_at(1), par_fit(w, w1 - 1, w1, w1 + 1));
+        put(ax_at(1), ax_odd(mw, w1), par_fit(u, u1 - 1, u1, u1 + 1));
+      }
+      if (ipass == 0 || (p + ipass) % 2 == 1) {
+        // Green.
+        put(ax_odd(mu, u1), ax_even(mw, w1), par_one());
+        put(ax_at(1), ax_even(mw, w1), par_fit(u, u1 - 1, u1, u1 + 1));
+        put(ax_odd(mu, u1), ax_at(mw), par_fit(w, w2 + 1, w2, w2 - 1));
+        // Red.
+        put(ax_even(mu, u1), ax_odd(mw, w1), par_one());
+        put(ax_even(mu, u1), ax_at(1), par_fit(w, w1 - 1, w1, w1 + 1));
+        put(ax_at(mu), ax_odd(mw, w1), par_fit(u, u2 + 1, u2, u2 - 1));
+      }
+      // Corner cells of the face.
+      for (int pu = 1; pu <= 2; ++pu) {
+        const FaceIdx Fu = GetFaceIndex(mx, mb, u, pu);
+        for (int pw = 1; pw <= 2; ++pw) {
+          const FaceIdx Fw = GetFaceIndex(mx, mb, w, pw);
+          put(ax_at(Fu.f), ax_at(Fw.f), par_corner(u, Fu.b, Fu.p, w, Fw.b, Fw.p));
+        }
+      }
+    }
+  }
+}
+
 // GhostOverlap (boundary.f90:346-415), mbc = 1: each grid's ghost ring takes
 // the other grid's interior values where they overlap (corners included).
 void GhostOverlap(const Ctx& c, Patch& g1, Patch& g2) {
@@ -595,8 +799,10 @@ int SetGhost(Ctx& c, int level, int ipass) {
     std::vector<Patch*>& L = c.on(level);
     for (Patch* p : L) {
       if (p->tobedeleted) continue;
-      if (c.ndims != 2) return -2;  // Interpolate3D is not restated
-      Interpolate2D(p->q, p->parent->q, p->mx, p->nrvars, p->mbounds, p->mthbc, ipass);
+      if (c.ndims == 2)
+        Interpolate2D(p->q, p->parent->q, p->mx, p->nrvars, p->mbounds, p->mthbc, ipass);
+      else
+        Interpolate3D(p->q, p->parent->q, p->mx, p->nrvars, p->mbounds, p->mthbc, ipass);
     }
     for (size_t a = 0; a < L.size(); ++a)
       for (size_t b = a + 1; b < L.size(); ++b)
@@ -1119,6 +1325,19 @@ int orc_run_hier(const orc_params* p, int npatch, const orc_patch* patches, cons
       std::memcpy(q_out + off, pt.q.d.data(), pt.q.d.size() * sizeof(double));
     });
   return 0;
+}
+
+void orc_interpolate3d(const int* mx, int nv, const int* mbounds, const int* mthbc, int ipass,
+                       double* qf, const int* pmx, const double* qc) {
+  const int lo[3] = {0, 0, 0};
+  const int hi[3] = {mx[0] + 1, mx[1] + 1, mx[2] + 1};
+  const int phi[3] = {pmx[0] + 1, pmx[1] + 1, pmx[2] + 1};
+  FArr f = wrap(3, lo, hi, nv, qf);
+  FArr c = wrap(3, lo, phi, nv, qc);
+  const int mb[3][2] = {{mbounds[0], mbounds[1]}, {mbounds[2], mbounds[3]},
+                        {mbounds[4], mbounds[5]}};
+  Interpolate3D(f, c, mx, nv, mb, mthbc, ipass);
+  std::memcpy(qf, f.d.data(), f.d.size() * sizeof(double));
 }
 
 void orc_interpolate2d(const int* mx, int nv, const int* mbounds, const int* mthbc, int ipass,

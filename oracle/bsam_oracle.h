@@ -84,6 +84,12 @@ int orc_run_hier(const orc_params* p, int npatch, const orc_patch* patches,
 void orc_interpolate2d(const int* mx, int nv, const int* mbounds, const int* mthbc,
                        int ipass, double* qf, const int* pmx, const double* qc);
 
+/* Interpolate3D (boundary.f90:1299-1799) on a fine patch qf (0:mx+1)^3 x nv
+ * from its parent qc (0:pmx+1)^3 x nv; mbounds = {mb11, mb12, mb21, mb22,
+ * mb31, mb32}. */
+void orc_interpolate3d(const int* mx, int nv, const int* mbounds, const int* mthbc,
+                       int ipass, double* qf, const int* pmx, const double* qc);
+
 /* Resolved minimum level for the parameters (lib/bsamroutines.f90:287-301). */
 int orc_minlevel(const orc_params* p);
 

@@ -70,6 +70,7 @@ def lib():
                                    ctypes.POINTER(OrcPatch), dp, ctypes.c_int, dp, ip, dp]
         L.orc_run_hier.restype = ctypes.c_int
         L.orc_interpolate2d.argtypes = [ip, ctypes.c_int, ip, ip, ctypes.c_int, dp, ip, dp]
+        L.orc_interpolate3d.argtypes = [ip, ctypes.c_int, ip, ip, ctypes.c_int, dp, ip, dp]
         _lib = L
     return _lib
 
@@ -149,6 +150,19 @@ def interpolate2d(qf, qc, mbounds, mthbc, ipass):
     mb = np.array(mbounds, dtype=np.int32)
     bc = np.array(mthbc, dtype=np.int32)
     lib().orc_interpolate2d(_ip(mx), qf.shape[2], _ip(mb), _ip(bc), ipass, _dp(qf), _ip(pmx),
+                            _dp(qc))
+    return qf
+
+
+def interpolate3d(qf, qc, mbounds, mthbc, ipass):
+    """Interpolate3D on copies of qf (0:mx+1)^3 x nv and qc (parent)."""
+    qf = np.array(qf, dtype=np.float64, order="F", copy=True)
+    qc = np.asfortranarray(qc, dtype=np.float64)
+    mx = np.array([qf.shape[d] - 2 for d in range(3)], dtype=np.int32)
+    pmx = np.array([qc.shape[d] - 2 for d in range(3)], dtype=np.int32)
+    mb = np.array(mbounds, dtype=np.int32)
+    bc = np.array(mthbc, dtype=np.int32)
+    lib().orc_interpolate3d(_ip(mx), qf.shape[3], _ip(mb), _ip(bc), ipass, _dp(qf), _ip(pmx),
                             _dp(qc))
     return qf
 

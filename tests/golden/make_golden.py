@@ -10,7 +10,7 @@ on seeded inputs:
       problems/simple_cahn-hilliard/problem.f90
   Restriction2D/3D, BiLinProlongationP1, TriLinProlongationP1
       lib/gridutilities.f90
-  SetBC2D/3D (+ the problem's UserBC2D/3D), Interpolate2D
+  SetBC2D/3D (+ the problem's UserBC2D/3D), Interpolate2D, Interpolate3D
       lib/boundary.f90
 
 and their composition, the time loop's multigrid solve on fixed hierarchies
@@ -237,6 +237,11 @@ def composition_cases():
         "mg_amr2d": (amr.build(16, [(1, (1, 1), (12, 16)), (1, (13, 9), (14, 12)),
                                     (2, (5, 9), (12, 12))],
                                eps=0.05, qerrortol=1e-10, maxvcycles=8, seed=9), 2),
+        # 8^3 root, two level-1 siblings sharing a y face (both on the z-low
+        # physical face).
+        "mg_amr3d": (amr.build(8, [(1, (5, 3, 1), (8, 8, 6)), (1, (5, 11, 1), (8, 4, 6))],
+                               eps=0.1, qerrortol=1e-10, maxvcycles=6, seed=4, field="wave",
+                               ndims=3), 2),
     }
     for name, (hier, nsteps) in cases.items():
         q, nvc, tr = run_composition(hier, nsteps)
@@ -330,6 +335,29 @@ def main():
                    ia(mth), ipass])
             res[f"qf_out_{n}_{ipass}"] = qq.data
     out["interpolate2d"] = res
+
+    # Interpolate3D: an 8 x 6 x 10 fine patch over parent cells
+    # 3..6 x 2..4 x 4..8 of a 9 x 7 x 10 parent; face-code mixes with internal
+    # (999), periodic (2), physical (1, 10) faces and a z face coded 99 (the
+    # edge check of boundary.f90:1354); every colour.
+    pmx3, mb3 = (9, 7, 10), (3, 6, 2, 4, 4, 8)
+    mx3 = tuple(2 * (mb3[2 * k + 1] - mb3[2 * k] + 1) for k in range(3))
+    qc = rng.standard_normal(tuple(m + 2 for m in pmx3) + (2,))
+    qf = rng.standard_normal(tuple(m + 2 for m in mx3) + (2,))
+    res = {"qc": qc, "qf_in": qf, "mb": np.array(mb3)}
+    mixes3 = [(999,) * 6, (1, 999, 10, 999, 999, 1), (999, 1, 999, 999, 99, 999),
+              (2, 2, 999, 1, 99, 99)]
+    for n, mth in enumerate(mixes3):
+        res[f"mthbc_{n}"] = np.array(mth)
+        for ipass in (0, 1, 2):
+            qq = fa(qf, (0, 0, 0, 1))
+            I.run(I.routines["interpolate3d"],
+                  [qq, fa(qc, (0, 0, 0, 1)), ia(mx3), 2,
+                   F.FArray(np.array([[mb3[0], mb3[1]], [mb3[2], mb3[3]], [mb3[4], mb3[5]]],
+                                     dtype=np.int64), (1, 1)),
+                   ia(mth), ipass])
+            res[f"qf_out_{n}_{ipass}"] = qq.data
+    out["interpolate3d"] = res
 
     out.update(composition_cases())
 

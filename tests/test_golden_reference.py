@@ -9,10 +9,11 @@ fixture bit for bit.  The CUDA kernels are in turn bit-identical to the
 oracle (tests/test_gpu_parity.py), so these fixtures pin the whole chain to
 the reference's own arithmetic for: RelaxGrid2D/3D, Operator2D/3D,
 Source2D/3D, Restriction2D/3D, Bi/TriLinProlongationP1, SetBC2D/3D with
-UserBC2D/3D, Interpolate2D -- and for their composition, the multigrid solve
-of the time loop (MultigridIterations with the V-cycle, SetGhost, FillDown,
-ErrorAFAS; afasroutines.f90, boundary.f90) on uniform 2D and 3D hierarchies
-and on a 2D hierarchy with two refined levels.
+UserBC2D/3D, Interpolate2D, Interpolate3D -- and for their composition, the
+multigrid solve of the time loop (MultigridIterations with the V-cycle,
+SetGhost, FillDown, ErrorAFAS; afasroutines.f90, boundary.f90) on uniform 2D
+and 3D hierarchies, a 2D hierarchy with two refined levels and a 3D one with
+two refined siblings.
 """
 import ctypes
 import os
@@ -81,7 +82,20 @@ def test_interpolate2d_matches_reference(oracle):
     assert n >= 3
 
 
-MG_CASES = ["mg_uniform2d", "mg_uniform3d", "mg_amr2d"]
+def test_interpolate3d_matches_reference(oracle):
+    d = fix("interpolate3d")
+    mb = tuple(int(v) for v in d["mb"])
+    n = 0
+    while f"mthbc_{n}" in d:
+        mth = tuple(int(c) for c in d[f"mthbc_{n}"])
+        for ipass in (0, 1, 2):
+            got = oracle.interpolate3d(d["qf_in"], d["qc"], mb, mth, ipass)
+            assert np.array_equal(got, d[f"qf_out_{n}_{ipass}"]), (n, ipass)
+        n += 1
+    assert n >= 4
+
+
+MG_CASES = ["mg_uniform2d", "mg_uniform3d", "mg_amr2d", "mg_amr3d"]
 
 
 @pytest.mark.parametrize("name", MG_CASES)

@@ -390,6 +390,7 @@ int plan_slot(bsam_batch* b, const bsam_batch_problem* pr, int rec0, char* base,
       if (face_rule(nd, f, d.mthbc[f], &rule))
         return fail(b, BSAM_ERR_UNSUPPORTED, "batch problems need physical faces (codes 1, 10-99)");
       P.bc[f] = rule;
+      P.code[f] = d.mthbc[f];
     }
     P.delta = (mixed && !is_master_only) ? 1 : 0;
     if (P.delta)

@@ -208,9 +208,15 @@ void amr_ghost(bsam_gpu* h, int level, int ipass) {
   if (level < h->minlevel || level > h->finestlevel) return;
   const LevelPlan& L = plan(h, level);
   if (!L.amr) return;
-  k_interp2<<<L.nplist, 128, 0, h->stream>>>(h->d_patches, L.d_plist, ipass);
-  if (L.novl) k_overlap<<<L.novl, 128, 0, h->stream>>>(h->d_patches, L.d_ovl);
-  k_setbc_list<2><<<L.nplist, 128, 0, h->stream>>>(h->d_patches, L.d_plist);
+  if (h->rp.ndims == 2) {
+    k_interp2<<<L.nplist, 128, 0, h->stream>>>(h->d_patches, L.d_plist, ipass);
+    if (L.novl) k_overlap<<<L.novl, 128, 0, h->stream>>>(h->d_patches, L.d_ovl);
+    k_setbc_list<2><<<L.nplist, 128, 0, h->stream>>>(h->d_patches, L.d_plist);
+  } else {
+    k_interp3<<<L.nplist, 256, 0, h->stream>>>(h->d_patches, L.d_plist, ipass);
+    if (L.novl) k_overlap<<<L.novl, 256, 0, h->stream>>>(h->d_patches, L.d_ovl);
+    k_setbc_list<3><<<L.nplist, 256, 0, h->stream>>>(h->d_patches, L.d_plist);
+  }
   h->stats.launches += L.novl ? 3 : 2;
 }
 
@@ -237,7 +243,10 @@ void snapshot(bsam_gpu* h, int level) {
 void filldown(bsam_gpu* h) {
   for (int level = h->finestlevel; level >= 1; --level) {
     const LevelPlan& L = plan(h, level);
-    k_filldown2<<<L.ncoarse, block_dim(), 0, h->stream>>>(h->d_patches, L.d_coarse);
+    if (h->rp.ndims == 2)
+      k_filldown<2><<<L.ncoarse, block_dim(), 0, h->stream>>>(h->d_patches, L.d_coarse);
+    else
+      k_filldown<3><<<L.ncoarse, block_dim(), 0, h->stream>>>(h->d_patches, L.d_coarse);
     ++h->stats.launches;
     amr_ghost(h, level - 1, 0);
   }
@@ -595,10 +604,9 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
   int minlevel = patches[0].level;
   for (int p = 0; p < npatch; ++p) minlevel = std::min(minlevel, patches[p].level);
   if (finestlevel < 0 || minlevel > 0) return fail(h, BSAM_ERR_ARG, "levels out of range");
-  if (finestlevel > 0 && (nd != 2 || h->mixed))
+  if (finestlevel > 0 && h->mixed)
     return fail(h, BSAM_ERR_UNSUPPORTED,
-                "levels above the root are built for the 2D FP64 form (no Interpolate3D, no "
-                "mixed-precision AMR)");
+                "levels above the root are built for the FP64 form (no mixed-precision AMR)");
   h->amr = finestlevel > 0;
   h->minlevel = minlevel;
   h->finestlevel = finestlevel;
@@ -702,6 +710,7 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
       if (face_rule(nd, f, d.mthbc[f], &rule))
         return fail(h, BSAM_ERR_UNSUPPORTED, "boundary code not supported");
       P.bc[f] = rule;
+      P.code[f] = d.mthbc[f];
       if (rule == BC_NONE) P.wt = 0;
     }
     if (!P.wt && d.level < 1)
@@ -717,7 +726,8 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
     // Fused stages: 3D V-cycle levels with a parent above the bottom, all
     // faces physical.
     const int fmin = std::max(8, h->tuning.fuse_min_n);
-    P.fused = (h->tuning.fuse_smoother != 0 && nd == 3 && in_vcycle && d.parent >= 0 &&
+    P.fused = (h->tuning.fuse_smoother != 0 && nd == 3 && finestlevel == 0 && in_vcycle &&
+               d.parent >= 0 &&
                d.level > h->bottom_level && !(P.delta && P.prec == PREC_F64) &&
                P.n[0] >= fmin && P.n[1] >= fmin && P.n[2] >= fmin)
                   ? 1
@@ -890,9 +900,9 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
       for (size_t bi = a + 1; bi < L.patches.size(); ++bi) {
         const bsam_patch_desc& g1 = patches[L.patches[a]];
         const bsam_patch_desc& g2 = patches[L.patches[bi]];
-        int ov[2][2];
+        int ov[3][2] = {{1, 1}, {1, 1}, {1, 1}};
         bool empty = false;
-        for (int n = 0; n < 2; ++n) {
+        for (int n = 0; n < nd; ++n) {
           ov[n][0] = std::max(g1.mglobal[n][0] - 1, g2.mglobal[n][0] - 1);
           ov[n][1] = std::min(g1.mglobal[n][1] + 1, g2.mglobal[n][1] + 1);
           empty |= ov[n][1] < ov[n][0];
@@ -900,8 +910,8 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
         if (empty) continue;
         // dst takes the other grid's interior inside the overlap.
         auto emit = [&](int dst, const bsam_patch_desc& gd, int src, const bsam_patch_desc& gs) {
-          int box[2][2];
-          for (int n = 0; n < 2; ++n) {
+          int box[3][2] = {{1, 1}, {1, 1}, {1, 1}};
+          for (int n = 0; n < nd; ++n) {
             box[n][0] = std::max(ov[n][0], gs.mglobal[n][0]);
             box[n][1] = std::min(ov[n][1], gs.mglobal[n][1]);
             if (box[n][1] < box[n][0]) return;
@@ -915,6 +925,14 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
           o.j1 = box[1][1] - gd.mglobal[1][0] + 1;
           o.di = gd.mglobal[0][0] - gs.mglobal[0][0];
           o.dj = gd.mglobal[1][0] - gs.mglobal[1][0];
+          if (nd == 3) {
+            o.k0 = box[2][0] - gd.mglobal[2][0] + 1;
+            o.k1 = box[2][1] - gd.mglobal[2][0] + 1;
+            o.dk = gd.mglobal[2][0] - gs.mglobal[2][0];
+          } else {
+            o.k0 = o.k1 = 0;
+            o.dk = 0;
+          }
           ovl_all.push_back(o);
         };
         emit(L.patches[a], g1, L.patches[bi], g2);

@@ -45,6 +45,7 @@ struct DevPatch {
   int32_t active;     // 0: every kernel skips this patch (finished or idle batch slot)
   int32_t newstep;    // batch masters: a new time step starts this iteration
   int32_t pprec;      // PREC_* of the parent (transfer kernels pick their types by it)
+  int32_t code[6];    // the reference's face codes mthbc (Interpolate3D tests some by value)
   int64_t sy, sz;     // element strides of j and k
   // Base pointers of element (0,0,0), the low ghost corner, per component.
   void* q[2];         // solution (phi, mu), with ghost ring: the state between stages

@@ -31,6 +31,13 @@ struct SlotCfg {
   double tol;
 };
 
+// The streaming kernels over tile lists are bound by memory latency.  For the
+// FP64 defect, the FP64 update and the 2D correction a register cap of 48
+// (ten 128-thread CTAs per SM) puts more loads in flight and measured 11-17 %
+// faster; restriction and coarse load measured slower under the same cap and
+// keep the compiler's choice.
+constexpr int BATCH_LATENCY_MIN_BLOCKS = 10;
+
 // Device-owned per-slot state (the host writes it only at admission).
 struct SlotState {
   int32_t phase, step, iters, vcycles;
@@ -152,7 +159,7 @@ __device__ __forceinline__ void correct_block2(const DevPatch& C, const DevPatch
 
 // Items: tiles of 32 x TILE_Y blocks (m, n) of a record (list L_CORR).
 template <class TC>
-__global__ void __launch_bounds__(BLOCK_THREADS)
+__global__ void __launch_bounds__(BLOCK_THREADS, BATCH_LATENCY_MIN_BLOCKS)
     kb_correct2(const DevPatch* __restrict__ PT, const Item* __restrict__ items,
                 const int* __restrict__ count) {
   const int n = *count;
@@ -216,7 +223,7 @@ __global__ void __launch_bounds__(BLOCK_THREADS)
 // Mixed form: defect of every master tile (newstep_only = 0, with partials)
 // or of the masters starting a time step (newstep_only = 1: twin set-up only).
 template <int D>
-__global__ void __launch_bounds__(BLOCK_THREADS)
+__global__ void __launch_bounds__(BLOCK_THREADS, BATCH_LATENCY_MIN_BLOCKS)
     kb_defect(const DevPatch* __restrict__ PT, const Item* __restrict__ items,
               const int* __restrict__ count, double* __restrict__ partials, int newstep_only) {
   const int n = *count;
@@ -233,7 +240,7 @@ __global__ void __launch_bounds__(BLOCK_THREADS)
 }
 
 template <int D>
-__global__ void __launch_bounds__(BLOCK_THREADS)
+__global__ void __launch_bounds__(BLOCK_THREADS, BATCH_LATENCY_MIN_BLOCKS)
     kb_update(const DevPatch* __restrict__ PT, const Item* __restrict__ items,
               const int* __restrict__ count) {
   const int n = *count;

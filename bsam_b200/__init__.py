@@ -59,7 +59,8 @@ _lib = None
 ABI_SYMBOLS = (
     "bsam_gpu_create", "bsam_gpu_set_hierarchy", "bsam_gpu_put_field", "bsam_gpu_get_field",
     "bsam_gpu_set_ghost", "bsam_gpu_copy_q_to_qold", "bsam_gpu_multigrid_iterations",
-    "bsam_gpu_residual_trace", "bsam_gpu_mass", "bsam_gpu_destroy", "bsam_gpu_strerror",
+    "bsam_gpu_residual_trace", "bsam_gpu_mass", "bsam_gpu_energy", "bsam_gpu_destroy",
+    "bsam_gpu_strerror",
     "bsam_gpu_last_error", "bsam_gpu_get_stream", "bsam_gpu_profile", "bsam_gpu_get_stats",
     "bsam_host_levels", "bsam_host_build_uniform", "bsam_host_take_time_steps",
     "bsam_gpu_resid_norm_noalloc", "bsam_gpu_set_tuning", "bsam_gpu_fill_down",
@@ -100,6 +101,7 @@ def lib():
     L.bsam_gpu_multigrid_iterations.argtypes = [vp, ip, dp, ip]
     L.bsam_gpu_residual_trace.argtypes = [vp, dp, ctypes.c_int]
     L.bsam_gpu_mass.argtypes = [vp, dp]
+    L.bsam_gpu_energy.argtypes = [vp, dp]
     L.bsam_gpu_destroy.argtypes = [vp]
     L.bsam_gpu_strerror.argtypes = [ctypes.c_int]
     L.bsam_gpu_strerror.restype = ctypes.c_char_p
@@ -240,6 +242,12 @@ class Solver:
         m = ctypes.c_double(0.0)
         _check(lib().bsam_gpu_mass(self.h, ctypes.byref(m)), self.h, "mass")
         return m.value
+
+    def energy(self) -> float:
+        """Energy2D of the root state (2D, no refined levels)."""
+        e = ctypes.c_double(0.0)
+        _check(lib().bsam_gpu_energy(self.h, ctypes.byref(e)), self.h, "energy")
+        return e.value
 
     def run(self, nsteps: int, keep_steps: bool = True):
         """TakeTimeSteps through the C++ host driver."""

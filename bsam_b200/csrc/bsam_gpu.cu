@@ -1225,6 +1225,33 @@ int bsam_gpu_mass(bsam_gpu* h, double* mass) {
   return BSAM_OK;
 }
 
+int bsam_gpu_energy(bsam_gpu* h, double* energy) {
+  if (!h || !h->have_hierarchy || !energy) return BSAM_ERR_STATE;
+  if (h->rp.ndims != 2 || h->amr || h->nroot == 0)
+    return fail(h, BSAM_ERR_UNSUPPORTED,
+                "the energy is defined for a 2D hierarchy without refined levels (AfterStep2D "
+                "at level 0)");
+  CU(cudaSetDevice(h->device));
+  int root = 0;
+  for (int p = 0; p < h->nuser; ++p)
+    if (h->desc[p].level == 0) root = p;
+  const double hh = h->hp[root].h, h2 = hh * hh;
+  const double tmp = h->rp.eps * h->rp.eps / h2 / 4.0;  // eps2/h2/4.0 (problem.f90:355)
+  double s[2];
+  for (int which = 0; which < 2; ++which) {
+    k_energy2<double><<<h->nroot, block_dim(), 0, h->stream>>>(
+        h->d_patches, h->d_root, h->d_partials, h->d_status, h->nroot, which);
+    ++h->stats.launches;
+    CU(cudaGetLastError());
+    CU(cudaMemcpyAsync(h->h_status, h->d_status, sizeof(DevStatus), cudaMemcpyDeviceToHost,
+                       h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    s[which] = h->h_status->esum;
+  }
+  *energy = h2 * (s[0] + tmp * s[1]);
+  return BSAM_OK;
+}
+
 int bsam_gpu_set_tuning(bsam_gpu* h, const bsam_tuning* t) {
   if (!h || !t) return BSAM_ERR_ARG;
   if (t->fuse_smoother < -1 || t->fuse_smoother > 1 || t->chunk < 0 || t->graph < -1 ||

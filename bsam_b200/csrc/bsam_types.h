@@ -73,6 +73,7 @@ struct DevStatus {
   double sumsq;        // last residual sum of squares
   double residual;     // sqrt(sumsq / (nrvars * ncells))
   double mass;
+  double esum;         // last Energy2D partial sum (k_energy2)
   uint32_t ticket;     // last-block-done counter of the reductions
   int32_t converged;
   int32_t kerr;        // nonzero: a kernel's bounded wait gave up (see smooth_fused.cuh)

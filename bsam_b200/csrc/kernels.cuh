@@ -603,6 +603,46 @@ static __global__ void k_mg_loop(DevStatus* __restrict__ st, double* __restrict_
   cudaGraphSetConditional(handle, again ? 1u : 0u);
 }
 
+// Ff of the problem module (problem.f90:769-780): alpha c^2 (c-1)^2 / 4.
+__device__ __forceinline__ double Ff(double c, double alpha) {
+  const double cm1 = c - 1.0;
+  return c * c * cm1 * cm1 * alpha / 4.0;
+}
+
+// One of the two sums of Energy2D (problem.f90:330-361) over a 2D patch
+// interior: which = 0, sum of Ff(c); which = 1, sum of f1(i) + f1(i-1) +
+// f2(j) + f2(j-1) with f1 = (c(i+1) - c(i))^2, f2 = (c(j+1) - c(j))^2 (the
+// ghost ring supplies the outer differences).
+template <class T>
+__global__ void __launch_bounds__(BLOCK_THREADS)
+    k_energy2(const DevPatch* __restrict__ PT, const Item* __restrict__ items,
+              double* __restrict__ partials, DevStatus* __restrict__ st, int nitems, int which) {
+  const Item it = items[blockIdx.x];
+  const DevPatch P = PT[it.patch];
+  const int j = it.ty * TILE_Y + threadIdx.y + 1;
+  const int i0 = (it.tx * 32 + threadIdx.x) * 2 + 1;
+  const T* c = fld<T>(P.q[0]);
+  auto C = [&](int i, int jj) { return (double)c[cidx(P, i, jj, 0)]; };
+  double acc = 0.0;
+  if (j <= P.n[1]) {
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+      const int i = i0 + t;
+      if (i > P.n[0]) break;
+      if (which == 0) {
+        acc += Ff(C(i, j), P.alpha);
+      } else {
+        const double a = C(i + 1, j) - C(i, j), b = C(i, j) - C(i - 1, j);
+        const double u = C(i, j + 1) - C(i, j), w = C(i, j) - C(i, j - 1);
+        acc += a * a + b * b + u * u + w * w;
+      }
+    }
+  }
+  const double bs = block_sum(acc);
+  double total;
+  if (last_block_total(bs, partials, &st->ticket, nitems, total)) st->esum = total;
+}
+
 // h^d * sum(phi) over a patch interior (AfterStep2D/3D integral(1)).
 template <class T, int D>
 __global__ void __launch_bounds__(BLOCK_THREADS)

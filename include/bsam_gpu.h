@@ -96,6 +96,15 @@ typedef struct {
 } bsam_tuning;
 int bsam_gpu_set_tuning(bsam_gpu* h, const bsam_tuning* t);
 
+/* Discrete free energy of the root state, Energy2D (problem.f90:330-361) as
+ * AfterStep2D accumulates it into integralresult(2) at level 0
+ * (problem.f90:121-123): h^2 (sum Ff(c) + eps^2/h^2/4 sum of the four
+ * squared one-sided differences of c per cell), with c = q(:,:,1) and its
+ * current ghost ring.  2D hierarchies without refined levels only
+ * (BSAM_ERR_UNSUPPORTED otherwise: the reference has no Energy3D).
+ * Deterministic; equal to the sequential sums to within rounding. */
+int bsam_gpu_energy(bsam_gpu* h, double* energy);
+
 /* Replaces the tree set-up that makes the hierarchy reachable to
  * MultigridIterations: RootInit/InitSeed/AllocFields
  * (lib/bsamroutines.f90:205-494, lib/bsamstorage.f90:46-123).  patches[] is in

@@ -36,7 +36,8 @@ unchanged hierarchy -- SetGhost(level, 0) from the root up (what
 AMR(rootlevel) leaves), FillDown(solutionfield) on the first step,
 CopyQToQold on every level, MultigridIterations (bsamroutines.f90:632-723).
 
-Usage: python tests/golden/make_golden.py [reference_dir]
+Usage: python tests/golden/make_golden.py [reference_dir] [--only name,name,...]
+(--only writes just the named fixtures; the seeded inputs do not depend on it.)
 """
 from __future__ import annotations
 
@@ -51,7 +52,12 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 import fsubset as F  # noqa: E402
 from bsam_b200 import amr, workloads as W  # noqa: E402  (pure-Python hierarchy builders)
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+ARGS = [a for a in sys.argv[1:] if not a.startswith("--only")]
+REF = ARGS[0] if ARGS else "/root/reference"
+ONLY = None
+for a in sys.argv[1:]:
+    if a.startswith("--only="):
+        ONLY = set(a.split("=", 1)[1].split(","))
 DT, EPS, ALPHA = 1.0e-4, 0.02, 1.0
 
 
@@ -244,6 +250,8 @@ def composition_cases():
                                ndims=3), 2),
     }
     for name, (hier, nsteps) in cases.items():
+        if ONLY is not None and name not in ONLY:
+            continue
         q, nvc, tr = run_composition(hier, nsteps)
         d = hier_arrays(hier)
         d.update({"nsteps": nsteps, "q_out": np.concatenate([a.ravel(order="F") for a in q]),
@@ -359,9 +367,18 @@ def main():
             res[f"qf_out_{n}_{ipass}"] = qq.data
     out["interpolate3d"] = res
 
-    out.update(composition_cases())
+    # Energy2D of a 12 x 10 field with its ring (AfterStep2D at level 0).
+    h = 1.0 / 12
+    c = 0.5 + 0.3 * rng.standard_normal((14, 12))
+    e = I.run(I.routines["energy2d"], [fa(c, (0, 0)), h])
+    out["energy2d"] = {"c": c, "h": h, "energy": np.float64(e)}
+
+    if ONLY is None or any(n.startswith("mg_") for n in ONLY):
+        out.update(composition_cases())
 
     for name, d in out.items():
+        if ONLY is not None and name not in ONLY:
+            continue
         np.savez_compressed(os.path.join(HERE, f"ref_{name}.npz"),
                             **{k: np.asarray(v) for k, v in d.items()},
                             dt=DT, eps=EPS, alpha=ALPHA)

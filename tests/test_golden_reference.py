@@ -9,7 +9,7 @@ fixture bit for bit.  The CUDA kernels are in turn bit-identical to the
 oracle (tests/test_gpu_parity.py), so these fixtures pin the whole chain to
 the reference's own arithmetic for: RelaxGrid2D/3D, Operator2D/3D,
 Source2D/3D, Restriction2D/3D, Bi/TriLinProlongationP1, SetBC2D/3D with
-UserBC2D/3D, Interpolate2D, Interpolate3D -- and for their composition, the
+UserBC2D/3D, Interpolate2D, Interpolate3D, Energy2D -- and for their composition, the
 multigrid solve of the time loop (MultigridIterations with the V-cycle,
 SetGhost, FillDown, ErrorAFAS; afasroutines.f90, boundary.f90) on uniform 2D
 and 3D hierarchies, a 2D hierarchy with two refined levels and a 3D one with
@@ -93,6 +93,12 @@ def test_interpolate3d_matches_reference(oracle):
             assert np.array_equal(got, d[f"qf_out_{n}_{ipass}"]), (n, ipass)
         n += 1
     assert n >= 4
+
+
+def test_energy2d_matches_reference(oracle):
+    d = fix("energy2d")
+    got = oracle.energy2d(float(d["h"]), float(d["alpha"]), float(d["eps"]), d["c"])
+    assert got == float(d["energy"])
 
 
 MG_CASES = ["mg_uniform2d", "mg_uniform3d", "mg_amr2d", "mg_amr3d"]

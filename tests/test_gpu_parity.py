@@ -169,3 +169,27 @@ def test_graph_loop_matches_host_loop(gpu_lib, nd, n):
     assert np.array_equal(ra["q"], rb["q"])
     assert np.array_equal(ra["nvcycles"], rb["nvcycles"])
     assert np.array_equal(ra["residual"], rb["residual"]) and np.array_equal(ta, tb)
+
+
+def test_energy_matches_oracle_and_decays(gpu_lib, oracle):
+    # Energy2D of the root state (AfterStep2D, level 0) on the device against
+    # the oracle's sequential sums, after every step; Eyre's splitting makes
+    # it non-increasing.
+    prob = W.config1(nsteps=4, n=64)
+    with B.Solver(prob) as s:
+        e = [s.energy()]
+        assert abs(e[0] - oracle.energy2d(prob.h, prob.alpha, prob.eps, s.get_q()[..., 0])) <= (
+            1e-12 * abs(e[0]))
+        for _ in range(4):
+            s.step()
+            q = s.get_q()
+            e.append(s.energy())
+            want = oracle.energy2d(prob.h, prob.alpha, prob.eps, q[..., 0])
+            assert abs(e[-1] - want) <= 1e-12 * abs(want), (e[-1], want)
+    assert all(b <= a for a, b in zip(e, e[1:])), e
+
+
+def test_energy_unsupported_in_3d(gpu_lib):
+    with B.Solver(W.config3(nsteps=1, n=16)) as s:
+        with pytest.raises(B.BsamError):
+            s.energy()

@@ -353,7 +353,9 @@ def run_ours(args, world, rank, local):
                    "ticks_per_bench_step": ticks / args.steps,
                    "all_converged": conv_all},
         "roofline": {"bound": "hbm", "kernel": "kb_smooth2<float> (fused finest-depth "
-                     "smoothing stage: nu=2 red-black sweeps of every problem, one launch)",
+                     "smoothing stages: nu=2 red-black sweeps of every problem, one launch "
+                     "each; the post-smoothing launch also applies the FP64 update "
+                     "q64 += e)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None,
                      "peak_source": peak_kind, "traffic": traffic,

@@ -248,7 +248,9 @@ __global__ void __launch_bounds__(BLOCK_THREADS, BATCH_LATENCY_MIN_BLOCKS)
     const Item it = items[b];
     const DevPatch M = PT[it.patch];
     if (!M.active) continue;
-    if (PT[M.twin].prec == PREC_F32) update_item<float, D>(PT, it);
+    const DevPatch& W = PT[M.twin];
+    if (W.fused) continue;  // updated by its post-smoothing stage (kb_smooth2, upd)
+    if (W.prec == PREC_F32) update_item<float, D>(PT, it);
     else update_item<double, D>(PT, it);
   }
 }

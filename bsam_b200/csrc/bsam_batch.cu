@@ -50,7 +50,9 @@ constexpr int MAXD = 8;   // top depths
 constexpr int DEFAULT_BOTTOM_CELLS = 1024;
 // Lists: master tiles; bottom-chain tops; per top depth d: tiles of every
 // record (correction), footprint tiles (restriction / coarse load), tiles of
-// records smoothed per colour pass, fused-stage tiles.
+// records smoothed per colour pass, fused-stage tiles; master tiles whose FP64
+// update is not done by their post-smoothing stage (mixed form, finest
+// working level not fused).
 enum {
   L_MASTER = 0,
   L_TOPS = 1,
@@ -59,7 +61,8 @@ enum {
   L_RELAX = 2 + 2 * MAXD,
   L_FUSED = 2 + 3 * MAXD,
   L_CORR = 2 + 4 * MAXD,  // 2D: tiles of 2 x 2 fine-cell blocks (kb_correct2)
-  NLIST = 2 + 5 * MAXD
+  L_UPD = 2 + 5 * MAXD,
+  NLIST = 3 + 5 * MAXD
 };
 
 struct List {
@@ -143,6 +146,7 @@ struct bsam_batch {
   // profiling (eager ticks): events around the finest-depth smoothing stages
   bool profiling = false;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pool;
+  std::vector<char> ev_post;  // per timed stage: post-smoothing (dir 1)
   size_t ev_used = 0;
   // pinned staging ring for host -> device copies
   char* stage = nullptr;
@@ -369,6 +373,7 @@ int plan_slot(bsam_batch* b, const bsam_batch_problem* pr, int rec0, char* base,
     P.active = 1;
     P.newstep = (r == 0) ? 1 : 0;
     P.twin = is_master_only ? rec0 + 1 : -1;
+    P.master = (mixed && r == 1) ? rec0 : -1;
     const int64_t ncell = cells_of(P.n, nd);
     P.prec = (!mixed || is_master_only || ncell <= bcells) ? PREC_F64 : PREC_F32;
     for (int n = 0; n < 3; ++n) {
@@ -473,6 +478,8 @@ void append_items(bsam_batch* b, int s) {
   C.ib = (int)b->lists[L_MASTER].h.size();
   tiles_for(rec0 + S.master, S.recs[S.master].n, nd, b->lists[L_MASTER].h);
   C.ie = (int)b->lists[L_MASTER].h.size();
+  if (b->mixed && !S.recs[1].fused)
+    tiles_for(rec0 + S.master, S.recs[S.master].n, nd, b->lists[L_UPD].h);
   b->lists[L_TOPS].h.push_back(Item{S.top, 0, 0, 0});
   const int first = b->mixed ? 1 : 0;  // record of depth 0
   for (int d = 0; d < S.ntop; ++d) {
@@ -518,7 +525,7 @@ int grid_for(bsam_batch* b, int l) {
   return std::max(1, std::min(cap, lim));
 }
 
-void stage_mark(bsam_batch* b, int d, bool begin) {
+void stage_mark(bsam_batch* b, int d, bool begin, int dir) {
   if (!b->profiling || d != 0) return;
   if (begin) {
     if (b->ev_used == b->ev_pool.size()) {
@@ -526,7 +533,9 @@ void stage_mark(bsam_batch* b, int d, bool begin) {
       cudaEventCreate(&x);
       cudaEventCreate(&y);
       b->ev_pool.push_back({x, y});
+      b->ev_post.push_back(0);
     }
+    b->ev_post[b->ev_used] = (char)dir;
     cudaEventRecord(b->ev_pool[b->ev_used].first, b->stream);
   } else {
     cudaEventRecord(b->ev_pool[b->ev_used].second, b->stream);
@@ -547,7 +556,7 @@ void tick_t(bsam_batch* b, cudaGraphConditionalHandle handle, int in_graph) {
   // LevelRelax of depth d for every running problem; dir selects the fused
   // stage's buffers (0: q -> qb before the correction, 1: qb -> q after).
   auto relax = [&](int d, int dir) {
-    stage_mark(b, d, true);
+    stage_mark(b, d, true, dir);
     if (L[L_RELAX + d].cap > 0)
       for (int pass = 0; pass < nu; ++pass)
         for (int color = 0; color < 2; ++color) {
@@ -562,17 +571,19 @@ void tick_t(bsam_batch* b, cudaGraphConditionalHandle handle, int in_graph) {
       const int lim = b->tuning.fused_ctas > 0 ? b->tuning.fused_ctas : 4 * b->nsm;
       const int g = std::max(1, std::min(L[L_FUSED + d].cap, lim));
       // Every fused record of a mixed batch is a correction-form FP32 level;
-      // of an FP64 batch, a plain FP64 level.
+      // of an FP64 batch, a plain FP64 level.  The finest working level's
+      // post-smoothing applies the FP64 update (kb_update skips those masters).
+      const int upd = (b->mixed && d == 0 && dir == 1) ? 1 : 0;
       if (b->mixed)
         kb_smooth2<float, true><<<g, Fused2<float>::THREADS, Fused2<float>::smem(true), s>>>(
-            pt, L[L_FUSED + d].d, cnt + L_FUSED + d, dir, nu, &b->d_ctl->kerr);
+            pt, L[L_FUSED + d].d, cnt + L_FUSED + d, dir, nu, upd, &b->d_ctl->kerr);
       else
         kb_smooth2<double, false>
             <<<g, Fused2<double>::THREADS, Fused2<double>::smem(false), s>>>(
-                pt, L[L_FUSED + d].d, cnt + L_FUSED + d, dir, nu, &b->d_ctl->kerr);
+                pt, L[L_FUSED + d].d, cnt + L_FUSED + d, dir, nu, 0, &b->d_ctl->kerr);
       ++n;
     }
-    stage_mark(b, d, false);
+    stage_mark(b, d, false, dir);
   };
   const int gm = grid_for(b, L_MASTER);
   kb_source<D><<<gm, blk, 0, s>>>(pt, L[L_MASTER].d, cnt + L_MASTER);
@@ -613,7 +624,7 @@ void tick_t(bsam_batch* b, cudaGraphConditionalHandle handle, int in_graph) {
     relax(d, 1);
   }
   if (b->mixed) {
-    kb_update<D><<<gm, blk, 0, s>>>(pt, L[L_MASTER].d, cnt + L_MASTER);
+    kb_update<D><<<grid_for(b, L_UPD), blk, 0, s>>>(pt, L[L_UPD].d, cnt + L_UPD);
     kb_defect<D><<<gm, blk, 0, s>>>(pt, L[L_MASTER].d, cnt + L_MASTER, b->d_partials, 0);
     n += 2;
   } else {
@@ -1024,7 +1035,10 @@ int bsam_batch_advance(bsam_batch* b, int max_ticks) {
         if (cudaEventElapsedTime(&ms, b->ev_pool[e].first, b->ev_pool[e].second) == cudaSuccess) {
           b->st.smooth_ms += ms;
           b->st.smooth_stages += 1;
-          b->st.smooth_bytes += 6.0 * es * (double)cells0;
+          // Read phi, mu, f1, f2, write phi, mu; the mixed 2D post-smoothing
+          // writes no e but reads and writes the FP64 master (q64 += e).
+          const bool upd = b->mixed && b->bp.ndims == 2 && b->ev_post[e] && !b->tuning.per_pass;
+          b->st.smooth_bytes += (upd ? 4.0 * es + 32.0 : 6.0 * es) * (double)cells0;
         }
       }
       b->ev_used = 0;

@@ -676,6 +676,7 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
     P.active = 1;
     P.newstep = 0;
     P.twin = is_twin ? -1 : twin_of[p];
+    P.master = is_twin ? p : -1;
     // Precision of the record.
     const int64_t ncell = cells_of(P.n, nd);
     if (!h->mixed || (!is_twin && d.level == finestlevel) || ncell <= fp64_cells)

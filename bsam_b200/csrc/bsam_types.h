@@ -41,6 +41,7 @@ struct DevPatch {
   int32_t fused;      // 1: smoothing stages run the fused kernel (q -> qb -> q)
   int32_t zchunk;     // fused kernel: planes (3D) / rows (2D) per streaming chunk
   int32_t twin;       // mixed form: the working patch of this FP64 master, else -1
+  int32_t master;     // mixed form: the FP64 master of this working patch, else -1
   int32_t delta;      // 1: q holds a correction e of the base state bs (mixed.cuh)
   int32_t active;     // 0: every kernel skips this patch (finished or idle batch slot)
   int32_t newstep;    // batch masters: a new time step starts this iteration

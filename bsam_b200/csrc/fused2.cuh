@@ -98,10 +98,16 @@ __device__ __forceinline__ void smem_ghosts2(const DevPatch& P, T* s0, T* s1, in
 // A copy that has not landed after kWaitPolls polls sets *err and ends the
 // launch for this CTA.  DELTA: every record of the list is a correction-form
 // level (the mixed form's working levels), with a base field.
+// upd (post-smoothing of the mixed form's finest working level): the smoothed
+// correction e is not stored; the tile's cells apply it to the FP64 master
+// instead, q64 += e with the master's ghosts by write-through -- the update of
+// mixed.cuh (update_item), expression for expression, done here while e is in
+// shared memory.  Every CTA writes only its own tile's cells of the master,
+// which nothing else in the launch reads.
 template <class T, bool DELTA>
 __global__ void __launch_bounds__(Fused2<T>::THREADS)
     kb_smooth2(const DevPatch* __restrict__ PT, const Item* __restrict__ items,
-               const int* __restrict__ count, int dir, int nu, int* __restrict__ err) {
+               const int* __restrict__ count, int dir, int nu, int upd, int* __restrict__ err) {
   using F = Fused2<T>;
   extern __shared__ __align__(1024) unsigned char smem2_raw[];
   __shared__ __align__(8) uint64_t bar;
@@ -196,6 +202,29 @@ __global__ void __launch_bounds__(Fused2<T>::THREADS)
         }
       }
       __syncthreads();
+    }
+    if (upd && P.master >= 0) {
+      const DevPatch M = PT[P.master];
+      double* m0 = fld<double>(M.q[0]);
+      double* m1 = fld<double>(M.q[1]);
+      for (int ly = warp; ly < F::TY; ly += F::WARPS) {
+        const int j = gy0 + F::H + ly;
+        if (j > n1) break;
+        const int srow = (F::H + ly) * F::RX + F::H;
+        for (int lx = lane; lx < F::TX; lx += 32) {
+          const int i = gx0 + F::H + lx;
+          if (i > n0) break;
+          const int64_t c = cidx(M, i, j, 0);
+          const double na = m0[c] + (double)s0[srow + lx];
+          const double nb = m1[c] + (double)s1[srow + lx];
+          m0[c] = na;
+          m1[c] = nb;
+          if (M.wt && near_boundary(M, i, j, 0, 2))
+            write_through<double, 2>(M, m0, m1, i, j, 0, na, nb);
+        }
+      }
+      __syncthreads();  // the shared tile is refilled for the next item
+      continue;
     }
     // Write back the tile's interior cells (warps over rows, lanes along
     // them), ghosts by write-through.

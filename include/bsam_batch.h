@@ -100,7 +100,9 @@ typedef struct {
   /* bsam_batch_profile: finest-depth smoothing stages timed with events */
   int64_t smooth_stages;
   double smooth_ms;
-  double smooth_bytes;    /* algorithmic: 6 * value bytes * cells per stage */
+  double smooth_bytes;    /* algorithmic: 6 * value bytes * cells per stage;
+                             (4 * value bytes + 32) * cells for the mixed 2D
+                             post-smoothing, which also applies q64 += e */
 } bsam_batch_stats;
 
 int bsam_batch_create(bsam_batch** b, int device, const bsam_batch_params* p);
@@ -159,7 +161,9 @@ int bsam_batch_collect(bsam_batch* b, int slot, double* q, bsam_step_result* ste
 
 /* enable != 0: ticks run eagerly, one at a time, and each finest-depth
  * smoothing stage (2 x nsmoothingpasses colour passes over every running
- * problem's root level) is timed with CUDA events into the stats; 0 stops. */
+ * problem's root level; in the mixed 2D form the post-smoothing stage also
+ * applies the FP64 update q64 += e) is timed with CUDA events into the
+ * stats; 0 stops. */
 int bsam_batch_profile(bsam_batch* b, int enable);
 
 int bsam_batch_get_stream(bsam_batch* b, void** stream);

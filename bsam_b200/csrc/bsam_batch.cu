@@ -36,6 +36,7 @@
 #include "../../include/bsam_batch.h"
 #include "batch.cuh"
 #include "bsam_types.h"
+#include "defect2.cuh"
 #include "fused2.cuh"
 
 using namespace bsam;
@@ -305,9 +306,9 @@ PFN_cuTensorMapEncodeTiled_v12000 map_encoder() {
 }
 
 // 2D map of one field of a 2D record: rows of sy elements from the
-// allocation start (lead elements before element (0,0)), n1 + 2 rows, box of
-// the fused stage's shared tile (RX x RY).
-bool encode_map2d(CUtensorMap* m, const DevPatch& P, const void* field) {
+// allocation start (lead elements before element (0,0)), n1 + 2 rows, box
+// bx x by (default: the fused stage's shared tile, RX x RY).
+bool encode_map2d(CUtensorMap* m, const DevPatch& P, const void* field, int bx = 0, int by = 0) {
   auto enc = map_encoder();
   if (!enc) return false;
   const bool f32 = P.prec == PREC_F32;
@@ -316,8 +317,11 @@ bool encode_map2d(CUtensorMap* m, const DevPatch& P, const void* field) {
   void* base = (char*)field - lead * es;
   const cuuint64_t dims[2] = {(cuuint64_t)P.sy, (cuuint64_t)(P.n[1] + 2)};
   const cuuint64_t strides[1] = {(cuuint64_t)(P.sy * es)};
-  const cuuint32_t box[2] = {(cuuint32_t)(f32 ? Fused2<float>::RX : Fused2<double>::RX),
-                             (cuuint32_t)(f32 ? Fused2<float>::RY : Fused2<double>::RY)};
+  if (bx == 0) {
+    bx = f32 ? Fused2<float>::RX : Fused2<double>::RX;
+    by = f32 ? Fused2<float>::RY : Fused2<double>::RY;
+  }
+  const cuuint32_t box[2] = {(cuuint32_t)bx, (cuuint32_t)by};
   const cuuint32_t estr[2] = {1, 1};
   return enc(m, f32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, base,
              dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -447,6 +451,18 @@ int plan_slot(bsam_batch* b, const bsam_batch_problem* pr, int rec0, char* base,
         for (int m = 0; m < NMAPS; ++m)
           if (!encode_map2d(&S.maps[(size_t)r * NMAPS + m], P, fields[m]))
             return fail(b, BSAM_ERR_CUDA, "cuTensorMapEncodeTiled rejected a field map");
+        P.tmaps = b->d_tmaps + (size_t)(rec0 + r) * NMAPS;
+      }
+      if (is_master_only && nd == 2) {
+        // The defect's staged tiles (kb_defect_tma): q0, q1 with a one-cell
+        // halo, f0, f1.
+        if (S.maps.size() < (size_t)nrec * NMAPS) S.maps.assign((size_t)nrec * NMAPS, CUtensorMap{});
+        const void* fields[4] = {P.q[0], P.q[1], P.f[0], P.f[1]};
+        for (int m = 0; m < 4; ++m) {
+          const int bx = m < 2 ? Defect2::QX : Defect2::TX, by = m < 2 ? Defect2::QY : Defect2::TY;
+          if (!encode_map2d(&S.maps[(size_t)r * NMAPS + m], P, fields[m], bx, by))
+            return fail(b, BSAM_ERR_CUDA, "cuTensorMapEncodeTiled rejected a field map");
+        }
         P.tmaps = b->d_tmaps + (size_t)(rec0 + r) * NMAPS;
       }
     }
@@ -586,10 +602,21 @@ void tick_t(bsam_batch* b, cudaGraphConditionalHandle handle, int in_graph) {
     stage_mark(b, d, false, dir);
   };
   const int gm = grid_for(b, L_MASTER);
+  // The mixed form's FP64 defect: 2D masters through staged tiles
+  // (defect2.cuh), 3D ones directly (same values either way).
+  auto launch_defect = [&](int newstep_only) {
+    if (D == 2)
+      kb_defect_tma<2><<<gm, blk, Defect2::SMEM, s>>>(pt, L[L_MASTER].d, cnt + L_MASTER,
+                                                      b->d_partials, newstep_only,
+                                                      &b->d_ctl->kerr);
+    else
+      kb_defect<D><<<gm, blk, 0, s>>>(pt, L[L_MASTER].d, cnt + L_MASTER, b->d_partials,
+                                      newstep_only);
+  };
   kb_source<D><<<gm, blk, 0, s>>>(pt, L[L_MASTER].d, cnt + L_MASTER);
   ++n;
   if (b->mixed) {
-    kb_defect<D><<<gm, blk, 0, s>>>(pt, L[L_MASTER].d, cnt + L_MASTER, b->d_partials, 1);
+    launch_defect(1);
     ++n;
   }
   for (int d = 0; d < b->cap_depth; ++d) {
@@ -625,7 +652,7 @@ void tick_t(bsam_batch* b, cudaGraphConditionalHandle handle, int in_graph) {
   }
   if (b->mixed) {
     kb_update<D><<<grid_for(b, L_UPD), blk, 0, s>>>(pt, L[L_UPD].d, cnt + L_UPD);
-    kb_defect<D><<<gm, blk, 0, s>>>(pt, L[L_MASTER].d, cnt + L_MASTER, b->d_partials, 0);
+    launch_defect(0);
     n += 2;
   } else {
     kb_resid<D><<<gm, blk, 0, s>>>(pt, L[L_MASTER].d, cnt + L_MASTER, b->d_partials);
@@ -925,7 +952,7 @@ static int admit(bsam_batch* b, const bsam_batch_problem* prob, const double* q0
   rc = stage_copy(b, b->d_pt + rec0, S.recs.data(), sizeof(DevPatch) * S.nrec);
   if (rc) return rc;
   for (int r = 0; r < S.nrec; ++r)
-    if (S.recs[r].fused) {
+    if (S.recs[r].tmaps) {
       rc = stage_copy(b, b->d_tmaps + (size_t)(rec0 + r) * NMAPS, &S.maps[(size_t)r * NMAPS],
                       sizeof(CUtensorMap) * NMAPS);
       if (rc) return rc;

@@ -27,11 +27,13 @@ struct Defect2 {
   static constexpr int QSTRIDE = (QPLANE * 8 + 127) / 128 * 16;  // doubles
   static constexpr int FSTRIDE = (FPLANE * 8 + 127) / 128 * 16;
   static constexpr uint32_t BYTES = 8u * (2 * QPLANE + 2 * FPLANE);  // landed per tile
-  static constexpr size_t SMEM = 8u * (2 * QSTRIDE + 2 * FSTRIDE);
+  static constexpr int BUF = 2 * QSTRIDE + 2 * FSTRIDE;             // doubles per buffer
+  static constexpr size_t SMEM = 8u * 2 * BUF;                        // two buffers
 };
 
 // Tensor maps of a 2D FP64 master: q0, q1 (box QX x QY), f0, f1 (box TX x TY),
-// in M.tmaps.  The twin's precision TW is read per tile.
+// in M.tmaps.  The twin's precision TW is read per tile.  Two tile buffers:
+// the copies of a CTA's next tile land while it computes the current one.
 template <int D>
 __global__ void __launch_bounds__(BLOCK_THREADS, 8)
     kb_defect_tma(const DevPatch* __restrict__ PT, const Item* __restrict__ items,
@@ -40,44 +42,70 @@ __global__ void __launch_bounds__(BLOCK_THREADS, 8)
   static_assert(D == 2, "2D masters only");
   using F = Defect2;
   extern __shared__ __align__(1024) unsigned char def_raw[];
-  __shared__ __align__(8) uint64_t bar;
-  double* sq0 = reinterpret_cast<double*>(def_raw);
-  double* sq1 = sq0 + F::QSTRIDE;
-  double* sf0 = sq1 + F::QSTRIDE;
-  double* sf1 = sf0 + F::FSTRIDE;
+  __shared__ __align__(8) uint64_t bar[2];
   const int tid = threadIdx.x + blockDim.x * threadIdx.y;
   const int n = *count;
   if (tid == 0) {
-    mbar_init(&bar, 1);
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
     fence_mbar_init();
   }
   __syncthreads();
-  uint32_t phase = 0;
-  for (int b = blockIdx.x; b < n; b += gridDim.x) {
-    const Item it = items[b];
-    const DevPatch M = PT[it.patch];
-    if (!M.active || (newstep_only && !M.newstep)) continue;  // uniform per CTA
-    const int i0 = it.tx * F::TX + 1, j0 = it.ty * F::TY + 1;
-    if (tid == 0) {
-      const CUtensorMapOpaque* maps = static_cast<const CUtensorMapOpaque*>(M.tmaps);
-      const int lead = 128 / (int)sizeof(double) - 1;
-      fence_proxy_async_smem();  // earlier generic reads of the buffers come first
-      mbar_arrive_expect_tx(&bar, F::BYTES);
-      tma_load_2d(sq0, &maps[0], lead + i0 - 2, j0 - 1, &bar);
-      tma_load_2d(sq1, &maps[1], lead + i0 - 2, j0 - 1, &bar);
-      tma_load_2d(sf0, &maps[2], lead + i0, j0, &bar);
-      tma_load_2d(sf1, &maps[3], lead + i0, j0, &bar);
+  auto plane = [&](int buf, int k) {
+    double* base = reinterpret_cast<double*>(def_raw) + buf * F::BUF;
+    return k < 2 ? base + k * F::QSTRIDE : base + 2 * F::QSTRIDE + (k - 2) * F::FSTRIDE;
+  };
+  // The CTA's next tile at or after list position `from` that takes part.
+  auto next_tile = [&](int from) {
+    for (int x = from; x < n; x += gridDim.x) {
+      const DevPatch& M = PT[items[x].patch];
+      if (M.active && !(newstep_only && !M.newstep)) return x;
     }
+    return n;
+  };
+  // Thread 0: the bulk copies of tile x into buffer buf.
+  auto issue = [&](int x, int buf) {
+    const Item it = items[x];
+    const DevPatch& M = PT[it.patch];
+    const CUtensorMapOpaque* maps = static_cast<const CUtensorMapOpaque*>(M.tmaps);
+    const int lead = 128 / (int)sizeof(double) - 1;
+    const int i0 = it.tx * F::TX + 1, j0 = it.ty * F::TY + 1;
+    fence_proxy_async_smem();  // earlier generic reads of the buffer come first
+    mbar_arrive_expect_tx(&bar[buf], F::BYTES);
+    tma_load_2d(plane(buf, 0), &maps[0], lead + i0 - 2, j0 - 1, &bar[buf]);
+    tma_load_2d(plane(buf, 1), &maps[1], lead + i0 - 2, j0 - 1, &bar[buf]);
+    tma_load_2d(plane(buf, 2), &maps[2], lead + i0, j0, &bar[buf]);
+    tma_load_2d(plane(buf, 3), &maps[3], lead + i0, j0, &bar[buf]);
+  };
+  uint32_t phase[2] = {0u, 0u};
+  int cur = next_tile(blockIdx.x), buf = 0;
+  if (cur < n && tid == 0) issue(cur, 0);
+  while (cur < n) {
+    // Buffer buf ^ 1 was last read by the previous tile, which ended with a
+    // barrier (block_sum).
+    const int nxt = next_tile(cur + gridDim.x);
+    if (nxt < n && tid == 0) issue(nxt, buf ^ 1);
     bool ok = true;
-    if (tid == 0) ok = mbar_wait_backoff(&bar, phase, kWaitPolls);
+    if (tid == 0) ok = mbar_wait_backoff(&bar[buf], phase[buf], kWaitPolls);
     ok = __syncthreads_and(ok);
-    if (ok && tid != 0) (void)mbar_try_wait(&bar, phase);
-    phase ^= 1u;
+    if (ok && tid != 0) (void)mbar_try_wait(&bar[buf], phase[buf]);
+    phase[buf] ^= 1u;
     if (!ok) {
-      if (tid == 0) atomicExch(err, kErrTmaTimeout);
+      if (tid == 0) {
+        atomicExch(err, kErrTmaTimeout);
+        // Let the copies of the prefetched tile land before the CTA exits.
+        if (nxt < n) (void)mbar_wait_backoff(&bar[buf ^ 1], phase[buf ^ 1], kWaitPolls);
+      }
       break;
     }
+    const double* sq0 = plane(buf, 0);
+    const double* sq1 = plane(buf, 1);
+    const double* sf0 = plane(buf, 2);
+    const double* sf1 = plane(buf, 3);
+    const Item it = items[cur];
+    const DevPatch M = PT[it.patch];
     const DevPatch W = PT[M.twin];
+    const int i0 = it.tx * F::TX + 1, j0 = it.ty * F::TY + 1;
     // defect_item's cells of this thread, from the staged tile.
     const int j = j0 + threadIdx.y;
     const int ic0 = (it.tx * 32 + threadIdx.x) * 2 + 1;
@@ -128,8 +156,10 @@ __global__ void __launch_bounds__(BLOCK_THREADS, 8)
         }
       }
     }
-    const double bsum = block_sum(acc);  // ends with a barrier: the tile is free
-    if (!newstep_only && tid == 0) partials[b] = bsum;
+    const double bsum = block_sum(acc);  // ends with a barrier: the buffer is free
+    if (!newstep_only && tid == 0) partials[cur] = bsum;
+    cur = nxt;
+    buf ^= 1;
   }
 }
 

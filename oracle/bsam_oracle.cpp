@@ -23,7 +23,9 @@
 //    numerically dead FillDown / UpdateSourceFunction passes.
 #include "bsam_oracle.h"
 
+#include <array>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <vector>
@@ -1404,6 +1406,264 @@ void orc_source(int ndims, const int* mx, double alpha, const double* qold, doub
   std::memcpy(p.qold.d.data(), qold, p.qold.d.size() * sizeof(double));
   GetSourceFunction(c, p);
   std::memcpy(f, p.ftmp.d.data(), p.ftmp.d.size() * sizeof(double));
+}
+
+// SetErrFlagsUser2D / 3D (problem.f90:135-163, 425-452): a cell is flagged
+// where the undivided central gradient of c exceeds tol.  q: c with its ring,
+// (0:mx+1)^d; flags (1:mx)^d.
+void orc_errflags(int ndims, const int* mx, double tol, const double* q, int* flags) {
+  const int n0 = mx[0], n1 = mx[1], n2 = ndims == 3 ? mx[2] : 1;
+  const long s1 = n0 + 2, s2 = (long)(n0 + 2) * (n1 + 2);
+  auto C = [&](int i, int j, int k) { return q[i + s1 * j + (ndims == 3 ? s2 * k : 0)]; };
+  long o = 0;
+  for (int k = 1; k <= n2; ++k)
+    for (int j = 1; j <= n1; ++j)
+      for (int i = 1; i <= n0; ++i) {
+        const double dx = C(i + 1, j, k) - C(i - 1, j, k), dy = C(i, j + 1, k) - C(i, j - 1, k);
+        double s = dx * dx + dy * dy;
+        if (ndims == 3) {
+          const double dz = C(i, j, k + 1) - C(i, j, k - 1);
+          s = s + dz * dz;
+        }
+        flags[o++] = std::fabs(std::sqrt(s)) > tol ? 1 : 0;
+      }
+}
+
+// Bi/TriLinProlongationP1MC (gridutilities.f90:219-279, 588-686): linear
+// prolongation one direction after the other, then each coarse cell's mass
+// correction cor = a - (average of its children) added to every child.
+// a: (0:cmx+1)^d x nv, out: (0:2cmx+1)^d x nv.
+void orc_prolong_mc(int ndims, const int* cmx, int nv, const double* ain, double* out) {
+  const int lo[3] = {0, 0, 0};
+  const int ahi[3] = {cmx[0] + 1, cmx[1] + 1, ndims == 3 ? cmx[2] + 1 : 0};
+  FArr A = wrap(ndims, lo, ahi, nv, ain);
+  const int m0 = 2 * cmx[0], m1 = 2 * cmx[1], m2 = ndims == 3 ? 2 * cmx[2] : 0;
+  const int c0 = cmx[0], c1 = cmx[1], c2 = ndims == 3 ? cmx[2] : 0;
+  const int kk = ndims == 3 ? 0 : 1;  // the third index of 2D arrays
+  FArr B, Cc, P;
+  if (ndims == 2) {
+    B.alloc(0, m0 + 1, 0, c1 + 1, 1, 1, 1, nv);
+    P.alloc(0, m0 + 1, 0, m1 + 1, 1, 1, 1, nv);
+  } else {
+    B.alloc(0, m0 + 1, 0, c1 + 1, 0, c2 + 1, 1, nv);
+    Cc.alloc(0, m0 + 1, 0, m1 + 1, 0, c2 + 1, 1, nv);
+    P.alloc(0, m0 + 1, 0, m1 + 1, 0, m2 + 1, 1, nv);
+  }
+  const int k3 = ndims == 3 ? c2 + 1 : kk;
+  for (int v = 1; v <= nv; ++v)
+    for (int k = ndims == 3 ? 0 : 1; k <= k3; ++k)
+      for (int j = 0; j <= c1 + 1; ++j)
+        for (int i = 0; i <= c0; ++i) {
+          B(2 * i, j, k, v) = 3.0 * A(i, j, k, v) + A(i + 1, j, k, v);
+          B(2 * i + 1, j, k, v) = A(i, j, k, v) + 3.0 * A(i + 1, j, k, v);
+        }
+  if (ndims == 2) {
+    for (int v = 1; v <= nv; ++v)
+      for (int j = 0; j <= c1; ++j)
+        for (int i = 0; i <= m0 + 1; ++i) {
+          P(i, 2 * j, 1, v) = (3.0 * B(i, j, 1, v) + B(i, j + 1, 1, v)) / 16.0;
+          P(i, 2 * j + 1, 1, v) = (B(i, j, 1, v) + 3.0 * B(i, j + 1, 1, v)) / 16.0;
+        }
+    for (int v = 1; v <= nv; ++v)
+      for (int l = 1; l <= c1; ++l)
+        for (int k = 1; k <= c0; ++k) {
+          const double cor = A(k, l, 1, v) - 0.25 * (P(2 * k, 2 * l, 1, v) + P(2 * k - 1, 2 * l, 1, v) +
+                                                     P(2 * k, 2 * l - 1, 1, v) +
+                                                     P(2 * k - 1, 2 * l - 1, 1, v));
+          P(2 * k, 2 * l, 1, v) = P(2 * k, 2 * l, 1, v) + cor;
+          P(2 * k - 1, 2 * l, 1, v) = P(2 * k - 1, 2 * l, 1, v) + cor;
+          P(2 * k, 2 * l - 1, 1, v) = P(2 * k, 2 * l - 1, 1, v) + cor;
+          P(2 * k - 1, 2 * l - 1, 1, v) = P(2 * k - 1, 2 * l - 1, 1, v) + cor;
+        }
+  } else {
+    for (int v = 1; v <= nv; ++v)
+      for (int k = 0; k <= c2 + 1; ++k)
+        for (int j = 0; j <= c1; ++j)
+          for (int i = 0; i <= m0 + 1; ++i) {
+            Cc(i, 2 * j, k, v) = 3.0 * B(i, j, k, v) + B(i, j + 1, k, v);
+            Cc(i, 2 * j + 1, k, v) = B(i, j, k, v) + 3.0 * B(i, j + 1, k, v);
+          }
+    for (int v = 1; v <= nv; ++v)
+      for (int k = 0; k <= c2; ++k)
+        for (int j = 0; j <= m1 + 1; ++j)
+          for (int i = 0; i <= m0 + 1; ++i) {
+            P(i, j, 2 * k, v) = (3.0 * Cc(i, j, k, v) + Cc(i, j, k + 1, v)) / 64.0;
+            P(i, j, 2 * k + 1, v) = (Cc(i, j, k, v) + 3.0 * Cc(i, j, k + 1, v)) / 64.0;
+          }
+    for (int v = 1; v <= nv; ++v)
+      for (int n = 1; n <= c2; ++n)
+        for (int l = 1; l <= c1; ++l)
+          for (int k = 1; k <= c0; ++k) {
+            const int a = 2 * k, b = 2 * l, c = 2 * n;
+            const double cor =
+                A(k, l, n, v) - 0.125 * (P(a, b, c, v) + P(a - 1, b, c, v) + P(a, b - 1, c, v) +
+                                         P(a - 1, b - 1, c, v) + P(a, b, c - 1, v) +
+                                         P(a - 1, b, c - 1, v) + P(a, b - 1, c - 1, v) +
+                                         P(a - 1, b - 1, c - 1, v));
+            for (int dz = 0; dz < 2; ++dz)
+              for (int dy = 0; dy < 2; ++dy)
+                for (int dx = 0; dx < 2; ++dx)
+                  P(a - dx, b - dy, c - dz, v) = P(a - dx, b - dy, c - dz, v) + cor;
+          }
+  }
+  std::memcpy(out, P.d.data(), P.d.size() * sizeof(double));
+}
+
+// NewSubGrids (lib/bsamroutines.f90:1352-1528) with GetSignatures
+// (1530-1554) and GridFlagRatio (1556-1579): Berger-Rigoutsos clustering of
+// the flags of a patch (1:mx)^d into boxes of at least mgp cells per side
+// whose flagged fraction reaches desfill where splits allow.  Boxes go to
+// `boxes` (per box lo/hi per dimension, 3 x 2 ints, dimensions beyond d = 1)
+// in the order the reference makes the new grids; returns their number, or
+// -1 if more than maxboxes.
+int orc_new_subgrids(int ndims, const int* mx, const int* flags, double desfill, int mgp,
+                     int* boxes, int maxboxes) {
+  constexpr int maxsubgrids = 1024, maxsplitpasses = 15;
+  const int nd = ndims;
+  const int m[3] = {mx[0], mx[1], nd == 3 ? mx[2] : 1};
+  auto F = [&](int i, int j, int k) {
+    return flags[(i - 1) + (long)m[0] * ((j - 1) + (long)m[1] * (k - 1))];
+  };
+  auto box_sum = [&](const int lo[3], const int hi[3]) {
+    long s = 0;
+    for (int k = lo[2]; k <= hi[2]; ++k)
+      for (int j = lo[1]; j <= hi[1]; ++j)
+        for (int i = lo[0]; i <= hi[0]; ++i) s += F(i, j, k);
+    return s;
+  };
+  // GridFlagRatio: real(flagged) / real(product of extents).
+  auto ratio = [&](int (*mb)[2]) {
+    double total = 1.0;
+    long prod = 1;
+    for (int n = 0; n < nd; ++n) prod *= (mb[n][1] - mb[n][0] + 1);
+    total = (double)prod;
+    for (int n = nd; n < 3; ++n) mb[n][0] = mb[n][1] = 1;
+    const int lo[3] = {mb[0][0], mb[1][0], mb[2][0]}, hi[3] = {mb[0][1], mb[1][1], mb[2][1]};
+    return (double)box_sum(lo, hi) / total;
+  };
+  int maxm = 0;
+  for (int n = 0; n < nd; ++n) maxm = std::max(maxm, m[n]);
+  std::vector<long> sig((size_t)(maxm + 2) * 3, 0), dd((size_t)(maxm + 2) * 3, 0);
+  auto S = [&](int i, int n) -> long& { return sig[(size_t)i + (size_t)(maxm + 2) * n]; };
+  auto DD = [&](int i, int n) -> long& { return dd[(size_t)i + (size_t)(maxm + 2) * n]; };
+  // GetSignatures over box g.
+  auto signatures = [&](int (*mb)[2]) {
+    for (int n = 0; n < nd; ++n) {
+      int lo[3] = {1, 1, 1}, hi[3] = {1, 1, 1};
+      for (int d = 0; d < nd; ++d) {
+        lo[d] = mb[d][0];
+        hi[d] = mb[d][1];
+      }
+      for (int i = mb[n][0]; i <= mb[n][1]; ++i) {
+        lo[n] = hi[n] = i;
+        S(i, n) = box_sum(lo, hi);
+      }
+    }
+  };
+  int whole[3][2] = {{1, m[0]}, {1, m[1]}, {1, m[2]}};
+  if (ratio(whole) < 1.0e-10) return 0;
+  std::vector<std::array<std::array<int, 2>, 3>> sub(maxsubgrids + 1);
+  std::vector<char> cansplit(maxsubgrids + 1, 1);
+  int ngrid = 1;
+  for (int n = 0; n < 3; ++n) sub[1][n] = {whole[n][0], whole[n][1]};
+  int igrid = 1;
+  while (ngrid < maxsubgrids && igrid <= ngrid) {
+    int npass = 0;
+    while (cansplit[igrid] && npass < maxsplitpasses) {
+      ++npass;
+      int mb[3][2];
+      auto load = [&]() {
+        for (int n = 0; n < 3; ++n) {
+          mb[n][0] = sub[igrid][n][0];
+          mb[n][1] = sub[igrid][n][1];
+        }
+      };
+      auto store = [&]() {
+        for (int n = 0; n < 3; ++n) sub[igrid][n] = {mb[n][0], mb[n][1]};
+      };
+      load();
+      signatures(mb);
+      // Trim empty rows and columns at the box's ends.
+      for (int n = 0; n < nd; ++n) {
+        int i1 = mb[n][0], i2 = mb[n][1];
+        while (S(i1, n) == 0 && i1 < mb[n][1] && i2 - i1 + 1 > mgp) ++i1;
+        while (S(i2, n) == 0 && i2 > mb[n][0] && i2 - i1 + 1 > mgp) --i2;
+        mb[n][0] = i1;
+        mb[n][1] = i2;
+      }
+      const double fill = ratio(mb);
+      store();
+      if (fill < desfill) {
+        signatures(mb);
+        int isplit[3] = {0, 0, 0};
+        bool havesplit = false;
+        // A hole: a zero signature at least mgp from both ends.
+        for (int n = 0; n < nd && !havesplit; ++n) {
+          const int i1 = mb[n][0], i2 = mb[n][1];
+          for (int i = i1 + mgp; i <= i2 - mgp; ++i)
+            if (S(i, n) == 0 && std::min(i - i1 + 1, i2 - i) >= mgp) {
+              isplit[n] = i;
+              havesplit = true;
+              break;
+            }
+        }
+        if (!havesplit) {
+          // The strongest inflection of the signature (ties: the most central).
+          for (int n = 0; n < nd; ++n) {
+            const int i1 = mb[n][0], i2 = mb[n][1];
+            for (int i = i1 + 1; i <= i2 - 1; ++i) DD(i, n) = S(i - 1, n) - 2 * S(i, n) + S(i + 1, n);
+          }
+          long inflect = 0;
+          int dist0 = 0;
+          for (int n = 0; n < nd; ++n) {
+            const int i1 = mb[n][0], i2 = mb[n][1];
+            for (int i = i1 + std::max(2, mgp); i <= i2 - std::max(1, mgp - 1); ++i) {
+              const long del = std::labs(DD(i, n) - DD(i - 1, n));
+              if (del > inflect) {
+                inflect = del;
+                isplit[0] = isplit[1] = isplit[2] = 0;
+                isplit[n] = i - 1;
+                havesplit = true;
+                dist0 = std::min(i - i1, i2 - i + 1);
+              } else if (del == inflect && inflect > 0) {
+                const int dist1 = std::min(i - i1, i2 - i + 1);
+                if (dist1 > dist0) {
+                  isplit[0] = isplit[1] = isplit[2] = 0;
+                  isplit[n] = i - 1;
+                  havesplit = true;
+                  dist0 = dist1;
+                }
+              }
+            }
+          }
+        }
+        if (havesplit) {
+          for (int n = 0; n < nd; ++n)
+            if (isplit[n] > 0 &&
+                std::min(sub[igrid][n][1] - isplit[n], isplit[n] - sub[igrid][n][0] + 1) >= mgp) {
+              ++ngrid;
+              cansplit[ngrid] = 1;
+              sub[ngrid] = sub[igrid];
+              sub[ngrid][n][0] = isplit[n] + 1;
+              sub[igrid][n][1] = isplit[n];
+              break;
+            }
+        } else {
+          cansplit[igrid] = 0;
+        }
+      } else {
+        cansplit[igrid] = 0;
+      }
+    }
+    ++igrid;
+  }
+  if (ngrid > maxboxes) return -1;
+  for (int g = 1; g <= ngrid; ++g)
+    for (int n = 0; n < 3; ++n) {
+      boxes[(g - 1) * 6 + 2 * n] = n < nd ? sub[g][n][0] : 1;
+      boxes[(g - 1) * 6 + 2 * n + 1] = n < nd ? sub[g][n][1] : 1;
+    }
+  return ngrid;
 }
 
 double orc_energy2d(const int* mx, double h, double alpha, double eps, const double* cin) {

@@ -116,6 +116,19 @@ int orc_setbc(int ndims, const int* mx, int nv, const int* mthbc, double* q);
 /* Source2D/3D (problem.f90:258-280, 562-585): f from qold.               */
 void orc_source(int ndims, const int* mx, double alpha, const double* qold,
                 double* f);
+/* ---- regridding leaves -------------------------------------------------- */
+/* SetErrFlagsUser2D/3D (problem.f90:135-163, 425-452): flags (1:mx)^d of c
+ * (0:mx+1)^d where the undivided central gradient exceeds tol.            */
+void orc_errflags(int ndims, const int* mx, double tol, const double* c, int* flags);
+/* Bi/TriLinProlongationP1MC (gridutilities.f90:219-279, 588-686):
+ * a (0:cmx+1)^d x nv -> out (0:2cmx+1)^d x nv.                          */
+void orc_prolong_mc(int ndims, const int* cmx, int nv, const double* a, double* out);
+/* NewSubGrids (lib/bsamroutines.f90:1352-1528): Berger-Rigoutsos boxes
+ * (lo, hi per dimension; 6 ints each) of flags (1:mx)^d, in the order the
+ * reference makes the grids.  Returns the count, -1 if above maxboxes.     */
+int orc_new_subgrids(int ndims, const int* mx, const int* flags, double desfill, int mgp,
+                     int* boxes, int maxboxes);
+
 /* Energy2D (problem.f90:330-361) of c (0:mx+1)^2.                        */
 double orc_energy2d(const int* mx, double h, double alpha, double eps,
                     const double* c);

@@ -71,6 +71,11 @@ def lib():
         L.orc_run_hier.restype = ctypes.c_int
         L.orc_interpolate2d.argtypes = [ip, ctypes.c_int, ip, ip, ctypes.c_int, dp, ip, dp]
         L.orc_interpolate3d.argtypes = [ip, ctypes.c_int, ip, ip, ctypes.c_int, dp, ip, dp]
+        L.orc_errflags.argtypes = [ctypes.c_int, ip, ctypes.c_double, dp, ip]
+        L.orc_prolong_mc.argtypes = [ctypes.c_int, ip, ctypes.c_int, dp, dp]
+        L.orc_new_subgrids.argtypes = [ctypes.c_int, ip, ip, ctypes.c_double, ctypes.c_int, ip,
+                                       ctypes.c_int]
+        L.orc_new_subgrids.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -165,6 +170,37 @@ def interpolate3d(qf, qc, mbounds, mthbc, ipass):
     lib().orc_interpolate3d(_ip(mx), qf.shape[3], _ip(mb), _ip(bc), ipass, _dp(qf), _ip(pmx),
                             _dp(qc))
     return qf
+
+
+def errflags(c, tol):
+    """SetErrFlagsUser of c with its ring (shape mx + 2 per dimension)."""
+    c = np.asfortranarray(c, dtype=np.float64)
+    nd = c.ndim
+    mx = np.array([s - 2 for s in c.shape] + [1] * (3 - nd), dtype=np.int32)
+    out = np.zeros(tuple(mx[:nd]), dtype=np.int32, order="F")
+    lib().orc_errflags(nd, _ip(mx), tol, _dp(c), _ip(out))
+    return out
+
+
+def prolong_mc(nd, a):
+    """Bi/TriLinProlongationP1MC of a (0:cmx+1)^d x nv."""
+    a = np.asfortranarray(a, dtype=np.float64)
+    cmx = np.array([a.shape[k] - 2 for k in range(nd)] + [1] * (3 - nd), dtype=np.int32)
+    out = np.zeros(tuple(2 * cmx[k] + 2 for k in range(nd)) + (a.shape[nd],), order="F")
+    lib().orc_prolong_mc(nd, _ip(cmx), a.shape[nd], _dp(a), _dp(out))
+    return out
+
+
+def new_subgrids(flags, desfill, mgp, maxboxes=4096):
+    """NewSubGrids boxes of 0/1 flags (1:mx)^d: array (nbox, 3, 2)."""
+    fl = np.asfortranarray(flags, dtype=np.int32)
+    nd = fl.ndim
+    mx = np.array(list(fl.shape) + [1] * (3 - nd), dtype=np.int32)
+    boxes = np.zeros(maxboxes * 6, dtype=np.int32)
+    n = lib().orc_new_subgrids(nd, _ip(mx), _ip(fl), desfill, mgp, _ip(boxes), maxboxes)
+    if n < 0:
+        raise RuntimeError("too many boxes")
+    return boxes[:6 * n].reshape(n, 3, 2)
 
 
 def run_uniform(prob, nsteps=None, keep_steps=True, q0=None):

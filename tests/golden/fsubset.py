@@ -21,8 +21,11 @@ supplies `tree`, an object whose on(level) lists the level's nodeinfo records
 in ApplyOnLevel order, and the interpreter provides ApplyOnLevel,
 ApplyOnLevelPairs (each grid with every later one) and GetParentInfo
 (lib/treeops.f90:536-610) over it.  Records are Python objects whose
-attributes are the nodeinfo components.  Not supported (and not needed):
-WHERE, character data, implicit typing, pointer assignment.
+attributes are the nodeinfo components.  A caller may also stand in for a
+called routine (`stubs`: MakeNewGrid, to record the boxes NewSubGrids makes).
+Also covered: DO WHILE, WHERE without ELSEWHERE, ALLOCATE / DEALLOCATE of
+integer arrays.  Not supported (and not needed): character data, implicit
+typing, pointer assignment.
 
 Only make_golden.py imports this module, in a container that has the
 reference source; the tests read the fixtures it wrote.
@@ -313,6 +316,7 @@ class Interp:
         self.tree = tree        # TreeOps stand-in: tree.on(level) -> records
         self.current = []       # ApplyOnLevel's current record (GetParentInfo)
         self.printed = []       # numeric items of every executed PRINT
+        self.stubs = {}         # name -> Python callable standing in for a CALL
 
     def lookup(self, name, env):
         """A variable, or a component chain a%b%c, from the locals, then the
@@ -469,6 +473,8 @@ class Interp:
             return acc
         if name == "maxval":
             return np.max(self.ev(subs[0], env))
+        if name == "minval":
+            return np.min(self.ev(subs[0], env))
         if name == "any":
             return bool(np.any(self.ev(subs[0], env)))
         if name == "getparentinfo":  # GetParentInfo(parent) -> err_ok
@@ -526,6 +532,9 @@ class Interp:
                             else:
                                 lbs.append(1)
                         env[nm] = FArray(a.data, lbs)
+                    continue
+                if local_dims is not None and any(a.lower() == "allocatable" for a in attrs):
+                    env[nm] = None  # created by ALLOCATE
                     continue
                 if local_dims is not None:
                     lbs, shape = [], []
@@ -591,6 +600,66 @@ class Interp:
         if lab:
             ln = lab.group(2)
             low = ln.lower()
+        if re.match(r"^do\s+while\s*\(", low):
+            is_do = lambda s: bool(re.match(r"^(\w+\s*:\s*)?do\b", s))
+            is_end = lambda s: bool(re.match(r"^end\s*do\b", s))
+            end, _ = self.find_end(lines, i, is_do, is_end)
+            cond_s, _ = split_paren(ln[ln.lower().index("while") + 5:].strip())
+            body = lines[i + 1:end]
+            name = lab.group(1).lower() if lab else None
+            while bool(self.ev(parse_expr(cond_s), env)):
+                try:
+                    self.exec_block(body, env)
+                except _Cycle as c:
+                    if c.name not in (None, name):
+                        raise
+                except _Exit as e:
+                    if e.name not in (None, name):
+                        raise
+                    break
+            return end + 1
+        if re.match(r"^where\s*\(", low):
+            # WHERE (mask) ... END WHERE (no ELSEWHERE): each assignment of
+            # the block applied where the mask holds.
+            is_w = lambda s: bool(re.match(r"^where\s*\(", s)) and not \
+                split_paren(s[5:].strip())[1].strip()
+            is_end = lambda s: bool(re.match(r"^end\s*where\b", s))
+            end, _ = self.find_end(lines, i, is_w, is_end)
+            mask_s, _ = split_paren(ln[5:].strip())
+            mask = np.asarray(self.ev(parse_expr(mask_s), env), dtype=bool)
+            for st in lines[i + 1:end]:
+                lhs_s, rhs_s = split_assign(st)
+                rhs = np.broadcast_to(np.asarray(self.ev(parse_expr(rhs_s), env)), mask.shape)
+                lhs = parse_expr(lhs_s)
+                arr = self.lookup(lhs[1], env)
+                view = arr.data[self.index_tuple(arr, lhs[2], env)] if lhs[0] == "ref" else arr.data
+                view[mask] = rhs[mask]
+            return end + 1
+        if re.match(r"^allocate\s*\(", low):
+            inner, _ = split_paren(ln[8:].strip())
+            for item in split_top(inner, ","):
+                item = item.strip()
+                if re.match(r"^stat\s*=", item, re.I):
+                    env[item.split("=", 1)[1].strip().lower()] = 0
+                    continue
+                m = re.match(r"^(\w+)\s*\((.*)\)$", item)
+                nm, dims = m.group(1).lower(), m.group(2)
+                lbs, shape = [], []
+                for spec in split_top(dims, ","):
+                    lo_s, hi_s = spec.split(":", 1) if ":" in spec else ("1", spec)
+                    lo = int(self.ev(parse_expr(lo_s), env))
+                    hi = int(self.ev(parse_expr(hi_s), env))
+                    lbs.append(lo)
+                    shape.append(max(hi - lo + 1, 0))
+                env[nm] = FArray(np.zeros(shape, dtype=np.int64, order="F"), lbs)
+            return i + 1
+        if re.match(r"^deallocate\s*\(", low):
+            inner, _ = split_paren(ln[10:].strip())
+            for item in split_top(inner, ","):
+                item = item.strip()
+                if re.match(r"^stat\s*=", item, re.I):
+                    env[item.split("=", 1)[1].strip().lower()] = 0
+            return i + 1
         if re.match(r"^do\b", low):
             is_do = lambda s: bool(re.match(r"^(\w+\s*:\s*)?do\b", s))
             is_end = lambda s: bool(re.match(r"^end\s*do\b", s))
@@ -675,6 +744,9 @@ class Interp:
             raise RuntimeError("reference executed STOP")
         if re.match(r"^call\b", low):
             node = parse_expr(ln[4:].strip())
+            if node[1] in self.stubs:  # a routine the caller stands in for
+                self.stubs[node[1]](*[self.section_actual(x, env) for x in node[2]])
+                return i + 1
             if node[1] in ("applyonlevel", "applyonlevelpairs"):
                 level = int(self.ev(node[2][0], env))
                 fn = self.routines[node[2][1][1]]

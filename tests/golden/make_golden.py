@@ -13,6 +13,12 @@ on seeded inputs:
   SetBC2D/3D (+ the problem's UserBC2D/3D), Interpolate2D, Interpolate3D
       lib/boundary.f90
 
+the regridding leaves
+
+  SetErrFlagsUser2D/3D (problem.f90), Bi/TriLinProlongationP1MC
+  (gridutilities.f90), NewSubGrids with GetSignatures and GridFlagRatio
+  (lib/bsamroutines.f90; MakeNewGrid stood in for, recording the boxes)
+
 and their composition, the time loop's multigrid solve on fixed hierarchies
 (uniform 2D and 3D, and 2D with refined levels):
 
@@ -231,6 +237,84 @@ def hier_arrays(hier):
             "maxvcycles": hier.maxvcycles, "nsmoothingpasses": hier.nsmoothingpasses}
 
 
+# ---- regridding leaves -----------------------------------------------------------
+
+def regrid_interp(extra_globals):
+    """An interpreter over problem.f90, gridutilities.f90 and the regrid
+    routines of bsamroutines.f90 (NewSubGrids, GetSignatures,
+    GridFlagRatio)."""
+    routines = {}
+    for rel in ("problems/simple_cahn-hilliard/problem.f90", "lib/gridutilities.f90"):
+        routines.update(F.extract_routines(open(os.path.join(REF, rel)).read()))
+    bsam = F.extract_routines(open(os.path.join(REF, "lib/bsamroutines.f90")).read())
+    for name in ("newsubgrids", "getsignatures", "gridflagratio"):
+        routines[name] = bsam[name]
+    g = {"dt": DT, "eps": EPS, "eps2": EPS * EPS, "alpha": ALPHA, "maxdims": 3,
+         "maxsubgrids": 1024}
+    g.update(extra_globals)
+    return F.Interp(routines, g)
+
+
+def blob_flags(shape, rng, n_blobs):
+    """0/1 flags: the union of a few random ellipsoids and a ring band."""
+    grids = np.meshgrid(*[np.arange(s) + 0.5 for s in shape], indexing="ij")
+    fl = np.zeros(shape, dtype=np.int64)
+    for _ in range(n_blobs):
+        c = [rng.uniform(0.2, 0.8) * s for s in shape]
+        r = [rng.uniform(0.05, 0.25) * s for s in shape]
+        fl |= (sum(((grids[k] - c[k]) / r[k]) ** 2 for k in range(len(shape))) < 1.0)
+    rr = np.sqrt(sum((grids[k] - 0.55 * shape[k]) ** 2 for k in range(len(shape))))
+    fl |= (np.abs(rr - 0.3 * min(shape)) < 1.5)
+    return fl.astype(np.int64)
+
+
+def regrid_cases(rng):
+    out = {}
+    maxdepth = 10
+    # SetErrFlagsUser2D / 3D: |undivided central gradient of c| > qtolerance.
+    for nd, mx in ((2, (24, 20)), (3, (10, 8, 12))):
+        tol = 0.2
+        I = regrid_interp({"qtolerance": fa(np.full(maxdepth + 1, tol), (0,))})
+        qnew = 0.5 + 0.3 * rng.standard_normal(tuple(m + 2 for m in mx) + (2,))
+        cmx = tuple(m // 2 for m in mx)
+        qrte = np.zeros(cmx + (2,))
+        flags = F.FArray(np.full(mx, 7, dtype=np.int64), (1,) * nd)
+        I.run(I.routines[f"seterrflagsuser{nd}d"],
+              [fa(qrte, (1,) * (nd + 1)), fa(qnew, (0,) * nd + (1,)), flags, ia(mx), ia(cmx), 2,
+               1.0 / mx[0], fa(np.zeros(nd), (1,)), 1])
+        out[f"errflags{nd}d"] = {"qnew": qnew, "tol": tol, "flags": flags.data}
+    # Bi/TriLinProlongationP1MC: bilinear prolongation with the mass correction.
+    for nd, cmx in ((2, (7, 5)), (3, (4, 3, 5))):
+        I = regrid_interp({})
+        a = rng.standard_normal(tuple(m + 2 for m in cmx) + (2,))
+        name = "bilinprolongationp1mc" if nd == 2 else "trilinprolongationp1mc"
+        p = I.run(I.routines[name], [fa(a, (0,) * nd + (1,))])
+        out[f"prolong_mc{nd}d"] = {"a": a, "p": p}
+    # NewSubGrids (Berger-Rigoutsos) with MakeNewGrid standing in: the boxes,
+    # in the order the reference makes them.
+    cases = [(2, (32, 32), 2, 0.9, 4), (2, (64, 48), 3, 0.7, 8), (2, (40, 40), 4, 0.9, 2),
+             (3, (16, 16, 16), 2, 0.8, 4)]
+    for n, (nd, mx, nblob, fill, mgp) in enumerate(cases):
+        fl = blob_flags(mx, rng, nblob)
+        mx3 = tuple(mx) + (1,) * (3 - nd)
+        made = []
+        I = regrid_interp({"ndims": nd,
+                           "desiredfillratios": fa(np.full(maxdepth + 1, fill), (0,)),
+                           "minimumgridpoints": F.FArray(np.full(maxdepth + 1, mgp,
+                                                                 dtype=np.int64), (0,))})
+        I.stubs["makenewgrid"] = lambda parent, mb: made.append(np.array(mb.data, copy=True))
+        info = F.Record(mx=F.FArray(np.array(mx3, dtype=np.int64), (1,)), level=1, nsubgrids=0,
+                        errorflags=F.FArray(fl.reshape(mx3, order="F").copy(order="F"),
+                                            (1, 1, 1)))
+        mb = F.FArray(np.array([[1, mx3[k]] for k in range(3)], dtype=np.int64), (1, 1))
+        I.run(I.routines["newsubgrids"], [info, mb])
+        boxes = np.array(made, dtype=np.int64).reshape(-1, 3, 2)
+        out[f"subgrids_{n}"] = {"ndims": nd, "flags": fl, "fill": fill, "mgp": mgp,
+                                "boxes": boxes, "nsubgrids": info.nsubgrids}
+        print(f"subgrids_{n}", nd, mx, "boxes", len(made))
+    return out
+
+
 def composition_cases():
     out = {}
     cases = {
@@ -372,6 +456,8 @@ def main():
     c = 0.5 + 0.3 * rng.standard_normal((14, 12))
     e = I.run(I.routines["energy2d"], [fa(c, (0, 0)), h])
     out["energy2d"] = {"c": c, "h": h, "energy": np.float64(e)}
+
+    out.update(regrid_cases(rng))
 
     if ONLY is None or any(n.startswith("mg_") for n in ONLY):
         out.update(composition_cases())

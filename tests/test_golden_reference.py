@@ -101,6 +101,31 @@ def test_energy2d_matches_reference(oracle):
     assert got == float(d["energy"])
 
 
+@pytest.mark.parametrize("nd", [2, 3])
+def test_errflags_match_reference(oracle, nd):
+    d = fix(f"errflags{nd}d")
+    got = oracle.errflags(d["qnew"][..., 0], float(d["tol"]))
+    assert np.array_equal(got, d["flags"])
+    assert 0 < got.sum() < got.size
+
+
+@pytest.mark.parametrize("nd", [2, 3])
+def test_prolongation_mc_matches_reference(oracle, nd):
+    d = fix(f"prolong_mc{nd}d")
+    assert np.array_equal(oracle.prolong_mc(nd, d["a"]), d["p"])
+
+
+@pytest.mark.parametrize("n", [0, 1, 2, 3])
+def test_new_subgrids_match_reference(oracle, n):
+    """Berger-Rigoutsos clustering: the same boxes in the same order."""
+    d = fix(f"subgrids_{n}")
+    nd = int(d["ndims"])
+    got = oracle.new_subgrids(d["flags"], float(d["fill"]), int(d["mgp"]))
+    want = d["boxes"]
+    assert got.shape[0] == want.shape[0] == int(d["nsubgrids"])
+    assert np.array_equal(got[:, :nd, :], want[:, :nd, :])
+
+
 MG_CASES = ["mg_uniform2d", "mg_uniform3d", "mg_amr2d", "mg_amr3d"]
 
 

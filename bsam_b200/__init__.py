@@ -64,6 +64,7 @@ ABI_SYMBOLS = (
     "bsam_gpu_last_error", "bsam_gpu_get_stream", "bsam_gpu_profile", "bsam_gpu_get_stats",
     "bsam_host_levels", "bsam_host_build_uniform", "bsam_host_take_time_steps",
     "bsam_gpu_resid_norm_noalloc", "bsam_gpu_set_tuning", "bsam_gpu_fill_down",
+    "bsam_gpu_errflags", "bsam_gpu_init_patch", "bsam_host_new_subgrids",
     "bsam_batch_create", "bsam_batch_destroy", "bsam_batch_set_tuning", "bsam_batch_footprint",
     "bsam_batch_submit", "bsam_batch_advance", "bsam_batch_sync", "bsam_batch_run",
     "bsam_batch_poll", "bsam_batch_slot_phase", "bsam_batch_collect", "bsam_batch_get_stream", "bsam_batch_profile", "bsam_batch_submit_seeded", "bsam_batch_busy",
@@ -102,6 +103,11 @@ def lib():
     L.bsam_gpu_residual_trace.argtypes = [vp, dp, ctypes.c_int]
     L.bsam_gpu_mass.argtypes = [vp, dp]
     L.bsam_gpu_energy.argtypes = [vp, dp]
+    L.bsam_gpu_errflags.argtypes = [vp, ctypes.c_int, ctypes.c_double,
+                                    ctypes.POINTER(ctypes.c_uint8)]
+    L.bsam_gpu_init_patch.argtypes = [vp, ctypes.c_int]
+    L.bsam_host_new_subgrids.argtypes = [ctypes.c_int, ip, ctypes.POINTER(ctypes.c_uint8),
+                                         ctypes.c_double, ctypes.c_int, ip, ctypes.c_int]
     L.bsam_gpu_destroy.argtypes = [vp]
     L.bsam_gpu_strerror.argtypes = [ctypes.c_int]
     L.bsam_gpu_strerror.restype = ctypes.c_char_p

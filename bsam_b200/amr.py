@@ -106,6 +106,41 @@ class HierSolver:
             qs.append(out)
         return {"q": qs, "nvcycles": nvc, "residual": res, "converged": conv}
 
+    def errflags(self, patch: int, tol: float) -> np.ndarray:
+        """SetErrFlagsUser of a state patch (descs index): 0/1 bytes (1:mx)^d."""
+        import ctypes
+        from . import _check, lib
+        d = self.hier.descs[patch]
+        shape = tuple(d["mx"][:self.hier.ndims])
+        out = np.zeros(shape, dtype=np.uint8, order="F")
+        _check(lib().bsam_gpu_errflags(self.h, patch, tol,
+                                       out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))),
+               self.h, "errflags")
+        return out
+
+    def init_patch(self, patch: int):
+        """InitFields of a refined patch from its parent (mass-corrected
+        prolongation; qold = q)."""
+        from . import _check, lib
+        _check(lib().bsam_gpu_init_patch(self.h, patch), self.h, "init_patch")
+
+    def get_q(self, patch: int) -> np.ndarray:
+        from . import FIELD_Q, _check, _dp, lib
+        d = self.hier.descs[patch]
+        shape = tuple(m + 2 for m in d["mx"][:self.hier.ndims]) + (2,)
+        out = np.zeros(shape, order="F")
+        _check(lib().bsam_gpu_get_field(self.h, patch, FIELD_Q, _dp(out)), self.h, "get_field")
+        return out
+
+    def get_qold(self, patch: int) -> np.ndarray:
+        from . import FIELD_QOLD, _check, _dp, lib
+        d = self.hier.descs[patch]
+        shape = tuple(m + 2 for m in d["mx"][:self.hier.ndims]) + (2,)
+        out = np.zeros(shape, order="F")
+        _check(lib().bsam_gpu_get_field(self.h, patch, FIELD_QOLD, _dp(out)), self.h,
+               "get_field")
+        return out
+
     def close(self):
         from . import lib
         if getattr(self, "h", None) is not None and self.h.value:
@@ -117,6 +152,25 @@ class HierSolver:
 
     def __exit__(self, *a):
         self.close()
+
+
+def new_subgrids(flags: np.ndarray, desfill: float, mgp: int, maxboxes: int = 4096) -> np.ndarray:
+    """Berger-Rigoutsos boxes (NewSubGrids) of a patch's 0/1 flags (1:mx)^d:
+    array (nbox, 3, 2) of lo/hi per dimension, in the reference's order.
+    Runs in the native library (bsam_host_new_subgrids)."""
+    import ctypes
+    from . import BsamError, lib
+    fl = np.asfortranarray(flags, dtype=np.uint8)
+    nd = fl.ndim
+    mx = np.array(list(fl.shape) + [1] * (3 - nd), dtype=np.int32)
+    boxes = np.zeros(6 * maxboxes, dtype=np.int32)
+    ip = ctypes.POINTER(ctypes.c_int)
+    n = lib().bsam_host_new_subgrids(nd, mx.ctypes.data_as(ip),
+                                     fl.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)),
+                                     float(desfill), int(mgp), boxes.ctypes.data_as(ip), maxboxes)
+    if n < 0:
+        raise BsamError(f"bsam_host_new_subgrids failed ({n})")
+    return boxes[:6 * n].reshape(n, 3, 2)
 
 
 def _desc(level, parent, mx, mbounds, mglobal, mthbc, dx, xlower):

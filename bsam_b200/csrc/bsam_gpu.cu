@@ -33,6 +33,7 @@
 #include "bottom.cuh"
 #include "mixed.cuh"
 #include "amr.cuh"
+#include "regrid.cuh"
 
 using namespace bsam;
 
@@ -1223,6 +1224,45 @@ int bsam_gpu_mass(bsam_gpu* h, double* mass) {
                      h->stream));
   CU(cudaStreamSynchronize(h->stream));
   *mass = h->h_status->mass;
+  return BSAM_OK;
+}
+
+int bsam_gpu_errflags(bsam_gpu* h, int patch, double tol, uint8_t* flags) {
+  if (!h || !h->have_hierarchy || !flags) return BSAM_ERR_ARG;
+  if (patch < 0 || patch >= h->nuser || h->desc[patch].level < 0)
+    return fail(h, BSAM_ERR_ARG, "errflags needs a patch on a level >= 0");
+  CU(cudaSetDevice(h->device));
+  const DevPatch& P = h->hp[patch];
+  const int nd = h->rp.ndims;
+  const size_t ncell = (size_t)P.n[0] * P.n[1] * (nd == 3 ? P.n[2] : 1);
+  uint8_t* d_flags = nullptr;
+  CU(cudaMalloc(&d_flags, ncell));
+  const int blocks = (int)std::min<size_t>((ncell + 255) / 256, 4096);
+  if (nd == 2) k_errflags<2><<<blocks, 256, 0, h->stream>>>(h->d_patches, patch, tol, d_flags);
+  else k_errflags<3><<<blocks, 256, 0, h->stream>>>(h->d_patches, patch, tol, d_flags);
+  ++h->stats.launches;
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(flags, d_flags, ncell, cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  cudaFree(d_flags);
+  if (e != cudaSuccess) return fail(h, BSAM_ERR_CUDA, cudaGetErrorString(e));
+  return BSAM_OK;
+}
+
+int bsam_gpu_init_patch(bsam_gpu* h, int patch) {
+  if (!h || !h->have_hierarchy) return BSAM_ERR_ARG;
+  if (patch < 0 || patch >= h->nuser || h->desc[patch].level < 1)
+    return fail(h, BSAM_ERR_ARG, "init_patch needs a refined patch (level >= 1)");
+  const DevPatch& P = h->hp[patch];
+  if (!P.qo[0] || h->mixed) return fail(h, BSAM_ERR_UNSUPPORTED, "init_patch: FP64 form only");
+  CU(cudaSetDevice(h->device));
+  const int nd = h->rp.ndims;
+  const size_t ncoarse = (size_t)(P.cn[0] + 2) * (P.cn[1] + 2) * (nd == 3 ? P.cn[2] + 2 : 1);
+  const int blocks = (int)std::min<size_t>((ncoarse + 255) / 256, 4096);
+  if (nd == 2) k_init_mc<2><<<blocks, 256, 0, h->stream>>>(h->d_patches, patch);
+  else k_init_mc<3><<<blocks, 256, 0, h->stream>>>(h->d_patches, patch);
+  ++h->stats.launches;
+  CU(cudaGetLastError());
   return BSAM_OK;
 }
 

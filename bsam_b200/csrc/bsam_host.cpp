@@ -7,7 +7,10 @@
 // (lib/bsamroutines.f90:582-789).  No Fortran compiler exists in this image,
 // so this file restates that driver in C++ for uniform root grids
 // (maxlevel = 0) and calls the C ABI exactly where the Fortran would.
+#include <algorithm>
+#include <array>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -139,6 +142,114 @@ int bsam_host_take_time_steps(bsam_gpu* h, int nsteps, int root_patch, double* q
     }
   }
   return BSAM_OK;
+}
+
+int bsam_host_new_subgrids(int ndims, const int* mx, const uint8_t* flags, double desfill,
+                           int mgp, int* boxes, int maxboxes) {
+  if ((ndims != 2 && ndims != 3) || !mx || !flags || !boxes || maxboxes < 0 || mgp < 1)
+    return BSAM_ERR_ARG;
+  const int nd = ndims;
+  const int m[3] = {mx[0], mx[1], nd == 3 ? mx[2] : 1};
+  for (int n = 0; n < 3; ++n)
+    if (m[n] < 1) return BSAM_ERR_ARG;
+  using Box = std::array<int, 6>;  // lo, hi per dimension
+  // Flagged cells in a box (GridFlagRatio's numerator, a signature entry).
+  auto count = [&](const Box& b) {
+    long s = 0;
+    for (int k = b[4]; k <= b[5]; ++k)
+      for (int j = b[2]; j <= b[3]; ++j) {
+        const uint8_t* row = flags + (size_t)m[0] * ((j - 1) + (size_t)m[1] * (k - 1));
+        for (int i = b[0]; i <= b[1]; ++i) s += row[i - 1] != 0;
+      }
+    return s;
+  };
+  auto fill_ratio = [&](const Box& b) {
+    long cells = 1;
+    for (int n = 0; n < nd; ++n) cells *= b[2 * n + 1] - b[2 * n] + 1;
+    return (double)count(b) / (double)cells;
+  };
+  const int maxm = std::max(m[0], std::max(m[1], nd == 3 ? m[2] : 1));
+  std::vector<long> sig(3 * (size_t)(maxm + 2), 0), dd(3 * (size_t)(maxm + 2), 0);
+  auto SIG = [&](int n, int i) -> long& { return sig[(size_t)n * (maxm + 2) + i]; };
+  auto DD = [&](int n, int i) -> long& { return dd[(size_t)n * (maxm + 2) + i]; };
+  auto signatures = [&](const Box& b) {  // GetSignatures
+    for (int n = 0; n < nd; ++n)
+      for (int i = b[2 * n]; i <= b[2 * n + 1]; ++i) {
+        Box slab = b;
+        slab[2 * n] = slab[2 * n + 1] = i;
+        SIG(n, i) = count(slab);
+      }
+  };
+  Box whole = {1, m[0], 1, m[1], 1, m[2]};
+  if (fill_ratio(whole) < 1.0e-10) return 0;
+  constexpr int kMaxGrids = 1024, kMaxPasses = 15;  // maxsubgrids, maxsplitpasses
+  std::vector<Box> grids{whole};
+  std::vector<bool> splittable{true};
+  for (size_t g = 0; (int)grids.size() < kMaxGrids && g < grids.size(); ++g) {
+    for (int pass = 0; splittable[g] && pass < kMaxPasses; ++pass) {
+      Box b = grids[g];
+      signatures(b);
+      for (int n = 0; n < nd; ++n) {  // trim empty ends, down to mgp cells
+        int lo = b[2 * n], hi = b[2 * n + 1];
+        while (SIG(n, lo) == 0 && lo < b[2 * n + 1] && hi - lo + 1 > mgp) ++lo;
+        while (SIG(n, hi) == 0 && hi > b[2 * n] && hi - lo + 1 > mgp) --hi;
+        b[2 * n] = lo;
+        b[2 * n + 1] = hi;
+      }
+      grids[g] = b;
+      if (fill_ratio(b) >= desfill) {
+        splittable[g] = false;
+        continue;
+      }
+      signatures(b);
+      int cut_dim = -1, cut = 0;
+      for (int n = 0; n < nd && cut_dim < 0; ++n) {  // a hole
+        const int lo = b[2 * n], hi = b[2 * n + 1];
+        for (int i = lo + mgp; i <= hi - mgp; ++i)
+          if (SIG(n, i) == 0 && std::min(i - lo + 1, hi - i) >= mgp) {
+            cut_dim = n;
+            cut = i;
+            break;
+          }
+      }
+      if (cut_dim < 0) {  // the strongest inflection; ties go to the most central
+        for (int n = 0; n < nd; ++n)
+          for (int i = b[2 * n] + 1; i <= b[2 * n + 1] - 1; ++i)
+            DD(n, i) = SIG(n, i - 1) - 2 * SIG(n, i) + SIG(n, i + 1);
+        long best = 0;
+        int best_dist = 0;
+        for (int n = 0; n < nd; ++n) {
+          const int lo = b[2 * n], hi = b[2 * n + 1];
+          for (int i = lo + std::max(2, mgp); i <= hi - std::max(1, mgp - 1); ++i) {
+            const long jump = std::labs(DD(n, i) - DD(n, i - 1));
+            const int dist = std::min(i - lo, hi - i + 1);
+            if (jump > best || (jump == best && best > 0 && dist > best_dist)) {
+              best = jump;
+              cut_dim = n;
+              cut = i - 1;
+              best_dist = dist;
+            }
+          }
+        }
+      }
+      if (cut_dim < 0) {
+        splittable[g] = false;
+        continue;
+      }
+      const int lo = b[2 * cut_dim], hi = b[2 * cut_dim + 1];
+      if (std::min(hi - cut, cut - lo + 1) >= mgp) {
+        Box upper = b;
+        upper[2 * cut_dim] = cut + 1;
+        grids[g][2 * cut_dim + 1] = cut;
+        grids.push_back(upper);
+        splittable.push_back(true);
+      }
+    }
+  }
+  if ((int)grids.size() > maxboxes) return BSAM_ERR_ARG;
+  for (size_t g = 0; g < grids.size(); ++g)
+    for (int e = 0; e < 6; ++e) boxes[6 * g + e] = e / 2 < nd ? grids[g][e] : 1;
+  return (int)grids.size();
 }
 
 }  // extern "C"

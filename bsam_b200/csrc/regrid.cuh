@@ -1,0 +1,148 @@
+// regrid.cuh -- the device side of regridding: cell tagging and the
+// initial state of a new refined patch.
+//
+//   k_errflags   SetErrFlagsUser2D/3D (problem.f90:135-163, 425-452): a cell is
+//                flagged where the undivided central gradient of c = q(...,1)
+//                exceeds the level's tolerance.
+//   k_init_mc    InitFields (lib/bsamroutines.f90:1685-1772) for mbc = 1: the
+//                child's q on (0:mx+1)^d is the mass-corrected linear
+//                prolongation (Bi/TriLinProlongationP1MC,
+//                gridutilities.f90:219-279, 588-686) of the parent's q over
+//                the child's footprint and its one-cell ring; qold = q.
+// The clustering of the flags into new patches (Berger-Rigoutsos, NewSubGrids)
+// runs on the host (bsam_host_new_subgrids).
+#pragma once
+#include "kernels.cuh"
+
+namespace bsam {
+
+// Flags (1:mx)^d of patch P, column-major, one byte per cell.
+template <int D>
+__global__ void k_errflags(const DevPatch* __restrict__ PT, int patch, double tol,
+                           uint8_t* __restrict__ flags) {
+  const DevPatch P = PT[patch];
+  const double* c = fld<double>(P.q[0]);
+  const int n0 = P.n[0], n1 = P.n[1], n2 = D == 3 ? P.n[2] : 1;
+  const int64_t total = (int64_t)n0 * n1 * n2;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(e % n0) + 1;
+    const int j = (int)((e / n0) % n1) + 1;
+    const int k = D == 3 ? (int)(e / ((int64_t)n0 * n1)) + 1 : 0;
+    const double dx = c[cidx(P, i + 1, j, k)] - c[cidx(P, i - 1, j, k)];
+    const double dy = c[cidx(P, i, j + 1, k)] - c[cidx(P, i, j - 1, k)];
+    double s = dx * dx + dy * dy;
+    if (D == 3) {
+      const double dz = c[cidx(P, i, j, k + 1)] - c[cidx(P, i, j, k - 1)];
+      s = s + dz * dz;
+    }
+    flags[e] = fabs(sqrt(s)) > tol ? 1 : 0;
+  }
+}
+
+// The linear-prolongation weights of fine index I from coarse (qc) indices
+// I >> 1 and (I >> 1) + 1: 3 and 1 for even I, 1 and 3 for odd I.
+__device__ __forceinline__ double lin_pair(int I, double a0, double a1) {
+  return (I & 1) == 0 ? 3.0 * a0 + a1 : a0 + 3.0 * a1;
+}
+
+// The uncorrected prolongation of qc (parent q, footprint + ring) at fine
+// cell (I, J[, K]) of the child, I in 0..mx+1: x first, then y, then z, as
+// the reference's temporaries b (and c) hold them.
+template <int D>
+__device__ __forceinline__ double prolong_raw(const DevPatch& C, const DevPatch& R, const double* a,
+                                              int I, int J, int K) {
+  // qc index k maps to parent index off + k.
+  auto A = [&](int x, int y, int z) {
+    return a[cidx(R, C.off[0] + x, C.off[1] + y, D == 3 ? C.off[2] + z : 0)];
+  };
+  const int x = I >> 1, y = J >> 1;
+  if (D == 2) {
+    const double b0 = lin_pair(I, A(x, y, 0), A(x + 1, y, 0));
+    const double b1 = lin_pair(I, A(x, y + 1, 0), A(x + 1, y + 1, 0));
+    return ((J & 1) == 0 ? 3.0 * b0 + b1 : b0 + 3.0 * b1) / 16.0;
+  }
+  const int z = K >> 1;
+  double c[2];
+#pragma unroll
+  for (int t = 0; t < 2; ++t) {
+    const double b0 = lin_pair(I, A(x, y, z + t), A(x + 1, y, z + t));
+    const double b1 = lin_pair(I, A(x, y + 1, z + t), A(x + 1, y + 1, z + t));
+    c[t] = lin_pair(J, b0, b1);
+  }
+  return ((K & 1) == 0 ? 3.0 * c[0] + c[1] : c[0] + 3.0 * c[1]) / 64.0;
+}
+
+// InitFields of child patch `child`: threads over the child's coarse cells
+// (0:cmx+1)^d; an interior coarse cell writes its 2^d children with the mass
+// correction, a ring coarse cell the children of it that lie in the child's
+// ring (0:mx+1)^d, uncorrected.  Then qold = q on the same cells.
+template <int D>
+__global__ void k_init_mc(const DevPatch* __restrict__ PT, int child) {
+  const DevPatch C = PT[child];
+  const DevPatch R = PT[C.parent];
+  const int c0 = C.cn[0], c1 = C.cn[1], c2 = D == 3 ? C.cn[2] : 0;
+  const int e0 = c0 + 2, e1 = c1 + 2, e2 = D == 3 ? c2 + 2 : 1;
+  const int64_t total = (int64_t)e0 * e1 * e2;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int k = (int)(e % e0), l = (int)((e / e0) % e1);
+    const int n = D == 3 ? (int)(e / ((int64_t)e0 * e1)) : 0;
+    const bool interior = k >= 1 && k <= c0 && l >= 1 && l <= c1 && (D == 2 || (n >= 1 && n <= c2));
+#pragma unroll
+    for (int v = 0; v < 2; ++v) {
+      const double* a = fld<double>(R.q[v]);
+      double* q = fld<double>(C.q[v]);
+      double* qo = fld<double>(C.qo[v]);
+      // The children of coarse cell (k, l[, n]): fine 2k - 1, 2k (etc.).
+      double p[8];
+      int idx[8][3];
+      const int nch = D == 2 ? 4 : 8;
+      // Child order of the reference's mass-correction sum: (2k,2l[,2n]),
+      // (2k-1,2l,..), (2k,2l-1,..), (2k-1,2l-1,..), then the same at 2n-1.
+#pragma unroll
+      for (int ch = 0; ch < nch; ++ch) {
+        idx[ch][0] = 2 * k - (ch & 1);
+        idx[ch][1] = 2 * l - ((ch >> 1) & 1);
+        idx[ch][2] = D == 3 ? 2 * n - (ch >> 2) : 0;
+      }
+      if (interior) {
+#pragma unroll
+        for (int ch = 0; ch < nch; ++ch) p[ch] = prolong_raw<D>(C, R, a, idx[ch][0], idx[ch][1], idx[ch][2]);
+        double s;
+        if (D == 2) {
+          s = a[cidx(R, C.off[0] + k, C.off[1] + l, 0)] - 0.25 * (p[0] + p[1] + p[2] + p[3]);
+        } else {
+          s = a[cidx(R, C.off[0] + k, C.off[1] + l, C.off[2] + n)] -
+              0.125 * (p[0] + p[1] + p[2] + p[3] + p[4] + p[5] + p[6] + p[7]);
+        }
+#pragma unroll
+        for (int ch = 0; ch < nch; ++ch) {
+          const double val = p[ch] + s;
+          const int64_t ci = cidx(C, idx[ch][0], idx[ch][1], idx[ch][2]);
+          q[ci] = val;
+          qo[ci] = val;
+        }
+      } else {
+        // Ring coarse cell: its children inside (0:mx+1)^d, uncorrected.
+#pragma unroll
+        for (int ch = 0; ch < nch; ++ch) {
+          const int I = idx[ch][0], J = idx[ch][1], K = idx[ch][2];
+          if (I < 0 || I > 2 * c0 + 1 || J < 0 || J > 2 * c1 + 1) continue;
+          if (D == 3 && (K < 0 || K > 2 * c2 + 1)) continue;
+          // A fine cell in the ring of the child: not a child of an interior
+          // coarse cell.
+          const bool fine_interior = I >= 1 && I <= 2 * c0 && J >= 1 && J <= 2 * c1 &&
+                                     (D == 2 || (K >= 1 && K <= 2 * c2));
+          if (fine_interior) continue;
+          const double val = prolong_raw<D>(C, R, a, I, J, K);
+          const int64_t ci = cidx(C, I, J, K);
+          q[ci] = val;
+          qo[ci] = val;
+        }
+      }
+    }
+  }
+}
+
+}  // namespace bsam

@@ -105,6 +105,22 @@ int bsam_gpu_set_tuning(bsam_gpu* h, const bsam_tuning* t);
  * Deterministic; equal to the sequential sums to within rounding. */
 int bsam_gpu_energy(bsam_gpu* h, double* energy);
 
+/* ---- regridding on the device ------------------------------------------- */
+/* Cell tags of a patch on a level >= 0 for the next regrid, SetErrFlagsUser
+ * (problem.f90:135-163, 425-452): flags[cell] = 1 where the undivided central
+ * gradient of c = q(...,1) (ghost ring as it stands) exceeds tol, else 0;
+ * flags: (1:mx)^d bytes, column-major.  The clustering of the flags into new
+ * patches is bsam_host_new_subgrids. */
+int bsam_gpu_errflags(bsam_gpu* h, int patch, double tol, uint8_t* flags);
+
+/* InitFields (lib/bsamroutines.f90:1685-1772) of a refined patch of the
+ * current hierarchy: q on (0:mx+1)^d becomes the mass-corrected linear
+ * prolongation (Bi/TriLinProlongationP1MC, gridutilities.f90:219-279,
+ * 588-686) of its parent's q over the patch's footprint and one-cell ring,
+ * and qold = q.  TransferValues from an old patch of the same level is a
+ * bsam_gpu_put_field of the overlapping cells afterwards.  FP64 form. */
+int bsam_gpu_init_patch(bsam_gpu* h, int patch);
+
 /* Replaces the tree set-up that makes the hierarchy reachable to
  * MultigridIterations: RootInit/InitSeed/AllocFields
  * (lib/bsamroutines.f90:205-494, lib/bsamstorage.f90:46-123).  patches[] is in

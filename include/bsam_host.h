@@ -43,6 +43,20 @@ int bsam_host_take_time_steps(bsam_gpu* h, int nsteps, int root_patch, double* q
                               int64_t q_stride, int* nvcycles, double* residuals,
                               int* converged, double* mass);
 
+/* Berger-Rigoutsos clustering of a patch's cell flags into new refined
+ * patches, as NewSubGrids does it (lib/bsamroutines.f90:1352-1528, with
+ * GetSignatures 1530-1554 and GridFlagRatio 1556-1579): starting from the
+ * whole patch, each box is trimmed to its flagged rows and columns and, while
+ * its flagged fraction is below desfill, split at a hole of the signature
+ * (a zero at least mgp cells from both ends) or else at its strongest
+ * inflection, keeping every side at least mgp cells.  flags: (1:mx)^d,
+ * column-major, nonzero = flagged.  boxes: 6 ints per box (lo, hi in each of
+ * three dimensions, 1 beyond ndims) in the order the reference makes the new
+ * grids (MakeNewGrid's mbounds).  Returns the number of boxes (0: nothing
+ * flagged), BSAM_ERR_ARG for bad arguments or more than maxboxes boxes. */
+int bsam_host_new_subgrids(int ndims, const int* mx, const uint8_t* flags, double desfill,
+                           int mgp, int* boxes, int maxboxes);
+
 #ifdef __cplusplus
 }
 #endif

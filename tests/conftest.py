@@ -73,3 +73,12 @@ def golden_hierarchy(name):
 @pytest.fixture(scope="session")
 def golden_hier():
     return golden_hierarchy
+
+
+@pytest.fixture(scope="session")
+def gpu_free_lib():
+    """The native library for host-only entry points (no device needed)."""
+    import bsam_b200
+    from bsam_b200 import build as B
+    B.build()
+    return bsam_b200.lib()

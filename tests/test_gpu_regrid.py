@@ -1,0 +1,55 @@
+"""Regridding pieces on the GPU against the oracle (FP64, bit for bit).
+
+* bsam_gpu_errflags: SetErrFlagsUser2D/3D of root and refined patches.
+* bsam_gpu_init_patch: InitFields of a refined patch -- the mass-corrected
+  prolongation of its parent's state over the footprint and one-cell ring
+  (Bi/TriLinProlongationP1MC), qold = q.
+The oracle's routines are pinned to the reference source
+(tests/test_golden_reference.py).
+"""
+import numpy as np
+import pytest
+
+from bsam_b200 import amr
+
+pytestmark = pytest.mark.gpu
+
+CASES = {
+    2: (32, [(1, (9, 5), (24, 20)), (1, (33, 41), (16, 16))]),
+    3: (16, [(1, (5, 3, 7), (12, 16, 10))]),
+}
+
+
+def hier(nd):
+    n, boxes = CASES[nd]
+    return amr.build(n, boxes, eps=0.05, dt=5e-5, qerrortol=1e-9, ndims=nd, field="drop", seed=3)
+
+
+@pytest.mark.parametrize("nd", [2, 3])
+def test_errflags_match_oracle(gpu_lib, oracle, nd):
+    h = hier(nd)
+    with amr.HierSolver(h) as s:
+        for p in h.state_patches():
+            q = s.get_q(p)
+            for tol in (0.05, 0.2):
+                got = s.errflags(p, tol)
+                want = oracle.errflags(q[..., 0], tol)
+                assert np.array_equal(got.astype(np.int32), want), (p, tol)
+
+
+@pytest.mark.parametrize("nd", [2, 3])
+def test_init_patch_matches_oracle(gpu_lib, oracle, nd):
+    h = hier(nd)
+    with amr.HierSolver(h) as s:
+        s.run(1)  # a state that is not the initial one
+        for p, d in enumerate(h.descs):
+            if d["level"] < 1:
+                continue
+            parent = s.get_q(d["parent"])
+            sl = tuple(slice(d["mbounds"][k][0] - 1, d["mbounds"][k][1] + 2) for k in range(nd))
+            want = oracle.prolong_mc(nd, parent[sl + (slice(None),)])
+            s.init_patch(p)
+            got = s.get_q(p)
+            assert got.shape == want.shape
+            assert np.array_equal(got, want), (p, float(np.max(np.abs(got - want))))
+            assert np.array_equal(s.get_qold(p), got)

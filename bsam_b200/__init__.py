@@ -65,6 +65,8 @@ ABI_SYMBOLS = (
     "bsam_host_levels", "bsam_host_build_uniform", "bsam_host_take_time_steps",
     "bsam_gpu_resid_norm_noalloc", "bsam_gpu_set_tuning", "bsam_gpu_fill_down",
     "bsam_gpu_errflags", "bsam_gpu_init_patch", "bsam_host_new_subgrids",
+    "bsam_gpu_restrict_level", "bsam_host_buffer_flags", "bsam_host_child_desc",
+    "bsam_gpu_set_ghost_level",
     "bsam_batch_create", "bsam_batch_destroy", "bsam_batch_set_tuning", "bsam_batch_footprint",
     "bsam_batch_submit", "bsam_batch_advance", "bsam_batch_sync", "bsam_batch_run",
     "bsam_batch_poll", "bsam_batch_slot_phase", "bsam_batch_collect", "bsam_batch_get_stream", "bsam_batch_profile", "bsam_batch_submit_seeded", "bsam_batch_busy",
@@ -106,6 +108,12 @@ def lib():
     L.bsam_gpu_errflags.argtypes = [vp, ctypes.c_int, ctypes.c_double,
                                     ctypes.POINTER(ctypes.c_uint8)]
     L.bsam_gpu_init_patch.argtypes = [vp, ctypes.c_int]
+    L.bsam_gpu_restrict_level.argtypes = [vp, ctypes.c_int]
+    L.bsam_gpu_set_ghost_level.argtypes = [vp, ctypes.c_int]
+    L.bsam_host_buffer_flags.argtypes = [ctypes.c_int, ctypes.c_int, ip, ip,
+                                         ctypes.POINTER(ctypes.c_uint8), ctypes.c_int]
+    L.bsam_host_child_desc.argtypes = [ctypes.c_int, ctypes.POINTER(PatchDesc), ctypes.c_int,
+                                       ip, ctypes.POINTER(PatchDesc)]
     L.bsam_host_new_subgrids.argtypes = [ctypes.c_int, ip, ctypes.POINTER(ctypes.c_uint8),
                                          ctypes.c_double, ctypes.c_int, ip, ctypes.c_int]
     L.bsam_gpu_destroy.argtypes = [vp]

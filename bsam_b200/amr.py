@@ -271,3 +271,297 @@ def build(n_root: int, boxes: list, eps: float, dt: float = 5e-5, qerrortol: flo
         q0s.append(W.initial_q(nd, tuple(d["mx"]), c0.ravel(order="F"), h, eps, 1.0))
     return Hierarchy(ndims=nd, descs=descs, q0s=q0s, dt=dt, eps=eps, qerrortol=qerrortol,
                      maxvcycles=maxvcycles)
+
+
+# ---- regridding every time step --------------------------------------------------
+
+@dataclasses.dataclass
+class RegridParams:
+    """The &amrdata values a regrid reads, per level 0 .. maxlevel - 1
+    (lib/nodeinfodef.f90:87-103): qtolerance (tag threshold on the undivided
+    gradient), ibuffer (buffer cells), desiredfillratios, minimumgridpoints."""
+    maxlevel: int
+    qtolerance: list
+    ibuffer: list
+    desfill: list
+    mgp: list
+
+
+class GpuBackend:
+    """The engine (C ABI, FP64 form) as the regrid driver's backend: one
+    handle whose hierarchy is re-set at every regrid."""
+
+    def __init__(self, ndims: int, dt: float, eps: float, qerrortol: float, alpha: float = 1.0,
+                 maxvcycles: int = 20, nsmoothingpasses: int = 2, device: int = 0):
+        import ctypes
+        from . import PREC_FP64, RunParams, _check, lib
+        self.nd = ndims
+        rp = RunParams(ndims=ndims, nrvars=2, mbc=1, maux=0, nsmoothingpasses=nsmoothingpasses,
+                       maxvcycles=maxvcycles, errortype=1, precision=PREC_FP64, dt=dt,
+                       qerrortol=qerrortol, alpha=alpha, eps=eps)
+        self.h = ctypes.c_void_p()
+        _check(lib().bsam_gpu_create(ctypes.byref(self.h), device, ctypes.byref(rp)),
+               what="create")
+        self.descs = []
+
+    def _call(self, what, rc):
+        from . import _check
+        _check(rc, self.h, what)
+
+    def set_hierarchy(self, descs):
+        from . import PatchDesc, lib
+        n = len(descs)
+        arr = (PatchDesc * n)()
+        for i, d in enumerate(descs):
+            o = arr[i]
+            o.level, o.parent, o.dx = d["level"], d["parent"], d["dx"]
+            for k in range(3):
+                o.mx[k] = d["mx"][k]
+                o.xlower[k] = d["xlower"][k]
+                for s in range(2):
+                    o.mbounds[k][s] = d["mbounds"][k][s]
+                    o.mglobal[k][s] = d["mglobal"][k][s]
+            for f in range(6):
+                o.mthbc[f] = d["mthbc"][f]
+        self.descs = list(descs)
+        self._call("set_hierarchy", lib().bsam_gpu_set_hierarchy(
+            self.h, n, arr, max(d["level"] for d in descs)))
+
+    def _shape(self, p):
+        d = self.descs[p]
+        return tuple(m + 2 for m in d["mx"][:self.nd]) + (2,)
+
+    def put_q(self, p, q):
+        from . import FIELD_Q, _dp, lib
+        q = np.asfortranarray(q, dtype=np.float64)
+        self._call("put_field", lib().bsam_gpu_put_field(self.h, p, FIELD_Q, _dp(q)))
+
+    def get_q(self, p):
+        from . import FIELD_Q, _dp, lib
+        out = np.zeros(self._shape(p), order="F")
+        self._call("get_field", lib().bsam_gpu_get_field(self.h, p, FIELD_Q, _dp(out)))
+        return out
+
+    def set_ghost_level(self, level):
+        from . import lib
+        self._call("set_ghost_level", lib().bsam_gpu_set_ghost_level(self.h, level))
+
+    def errflags(self, p, tol):
+        import ctypes
+        from . import lib
+        d = self.descs[p]
+        out = np.zeros(tuple(d["mx"][:self.nd]), dtype=np.uint8, order="F")
+        self._call("errflags", lib().bsam_gpu_errflags(
+            self.h, p, tol, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))))
+        return out
+
+    def init_patch(self, p):
+        from . import lib
+        self._call("init_patch", lib().bsam_gpu_init_patch(self.h, p))
+
+    def restrict_level(self, level):
+        from . import lib
+        self._call("restrict_level", lib().bsam_gpu_restrict_level(self.h, level))
+
+    def fill_down(self):
+        from . import lib
+        self._call("fill_down", lib().bsam_gpu_fill_down(self.h))
+
+    def copy_q_to_qold(self):
+        from . import lib
+        self._call("copy_q_to_qold", lib().bsam_gpu_copy_q_to_qold(self.h))
+
+    def multigrid(self):
+        import ctypes
+        from . import lib
+        nv, conv = ctypes.c_int(0), ctypes.c_int(0)
+        res = ctypes.c_double(0.0)
+        self._call("multigrid_iterations", lib().bsam_gpu_multigrid_iterations(
+            self.h, ctypes.byref(nv), ctypes.byref(res), ctypes.byref(conv)))
+        return nv.value, res.value
+
+    def buffer_flags(self, descs, flags, ibuffer):
+        return buffer_flags(self.nd, descs, flags, ibuffer)
+
+    def new_subgrids(self, flags, desfill, mgp):
+        return new_subgrids(flags, desfill, mgp)
+
+    def child_desc(self, parent, parent_index, box):
+        return child_desc(self.nd, parent, parent_index, box)
+
+    def close(self):
+        from . import lib
+        if self.h is not None and self.h.value:
+            lib().bsam_gpu_destroy(self.h)
+            self.h = None
+
+
+def buffer_flags(nd: int, descs: list, flags: list, ibuffer: int) -> list:
+    """BufferAndList + InflateEdgeTags over one level's patches (the native
+    library's bsam_host_buffer_flags); flags: one (1:mx)^d uint8 array per
+    desc, buffered copies returned."""
+    import ctypes
+    from . import BsamError, lib
+    if ibuffer <= 0 or not descs:
+        return [f.copy() for f in flags]
+    mx = np.array([list(d["mx"]) for d in descs], dtype=np.int32).ravel()
+    mg = np.array([[v for b in d["mglobal"] for v in b] for d in descs], dtype=np.int32).ravel()
+    flat = np.concatenate([np.asfortranarray(f, dtype=np.uint8).ravel(order="F") for f in flags])
+    ip = ctypes.POINTER(ctypes.c_int)
+    rc = lib().bsam_host_buffer_flags(nd, len(descs), mx.ctypes.data_as(ip), mg.ctypes.data_as(ip),
+                                      flat.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), ibuffer)
+    if rc != 0:
+        raise BsamError(f"bsam_host_buffer_flags failed ({rc})")
+    out, off = [], 0
+    for f in flags:
+        out.append(flat[off:off + f.size].reshape(f.shape, order="F").copy())
+        off += f.size
+    return out
+
+
+def child_desc(nd: int, parent: dict, parent_index: int, box) -> dict:
+    """MakeNewGrid's record of the child over `box` (the native library's
+    bsam_host_child_desc)."""
+    import ctypes
+    from . import BsamError, PatchDesc, lib
+    pd, cd = PatchDesc(), PatchDesc()
+    pd.level, pd.parent, pd.dx = parent["level"], parent["parent"], parent["dx"]
+    for k in range(3):
+        pd.mx[k] = parent["mx"][k]
+        pd.xlower[k] = parent["xlower"][k]
+        for s in range(2):
+            pd.mbounds[k][s] = parent["mbounds"][k][s]
+            pd.mglobal[k][s] = parent["mglobal"][k][s]
+    for f in range(6):
+        pd.mthbc[f] = parent["mthbc"][f]
+    b = np.array(box, dtype=np.int32).ravel()
+    rc = lib().bsam_host_child_desc(nd, ctypes.byref(pd), parent_index,
+                                    b.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                    ctypes.byref(cd))
+    if rc != 0:
+        raise BsamError(f"bsam_host_child_desc failed ({rc})")
+    return {"level": cd.level, "parent": cd.parent, "mx": list(cd.mx),
+            "mbounds": [list(cd.mbounds[k]) for k in range(3)],
+            "mglobal": [list(cd.mglobal[k]) for k in range(3)], "mthbc": list(cd.mthbc),
+            "dx": cd.dx, "xlower": list(cd.xlower)}
+
+
+class RegridRun:
+    """TakeTimeSteps with regridding every step (lib/bsamroutines.f90:632-762):
+    AMR(rootlevel) (939-961) -- for level = 0 .. maxlevel - 1: SetGhost(level),
+    EstimateLevelErrors (963-1002: RestrictSolution of the level into its
+    parents, then SetErrFlagsUser and the buffer), GridAdapt (1299-1350:
+    NewSubGrids per patch in ApplyOnLevel order, MakeNewGrid + InitFields per
+    box, TransferValues from the level's old grids, the old grids released) --
+    then FillDown on the first step, CopyQToQold, MultigridIterations.
+
+    New grids join their level youngest first (TreeOps prepends them,
+    lib/treeops.f90:339-430), so a new level lists its grids in the reverse
+    of the order they were made.  The hierarchy starts from `hier` as given
+    (its grids are not re-made by QInit).  `backend` does the numerics:
+    GpuBackend (the engine), or any object with the same methods."""
+
+    def __init__(self, backend, hier: Hierarchy, params: RegridParams):
+        self.b = backend
+        self.nd = hier.ndims
+        self.prm = params
+        self.descs = [dict(d) for d in hier.descs]
+        self.b.set_hierarchy(self.descs)
+        for p, q in zip(hier.state_patches(), hier.q0s):
+            self.b.put_q(p, q)
+        # BSAMSolver: SetGhost on every level, CopyQToQold (bsamroutines.f90:144-147).
+        for level in range(0, max(d["level"] for d in self.descs) + 1):
+            self.b.set_ghost_level(level)
+        self.b.copy_q_to_qold()
+        self.firstamr = True
+
+    def levels(self):
+        return sorted({d["level"] for d in self.descs})
+
+    def _rebuild(self, descs, keep_q):
+        """Re-set the backend's hierarchy to `descs`; put back q of the
+        patches in keep_q (new index -> q)."""
+        self.b.set_hierarchy(descs)
+        for i, q in keep_q.items():
+            self.b.put_q(i, q)
+
+    def step(self):
+        """One time step: AMR(rootlevel), FillDown on the first step,
+        CopyQToQold, MultigridIterations.  Returns (V-cycles, residual)."""
+        b, nd, prm = self.b, self.nd, self.prm
+        descs = self.descs
+        # The old grids of each refined level: TransferValues' sources.  Their
+        # interiors do not change before GridAdapt reaches their level.
+        old = {}
+        for i, d in enumerate(descs):
+            if d["level"] >= 1:
+                old.setdefault(d["level"], []).append((d, b.get_q(i)))
+        b.set_ghost_level(0)  # AMR(rootlevel)
+        # EstimateLevelErrors(0)'s RestrictSolution of the root into the level
+        # below and that level's SetGhost are left out: the V-cycle restricts
+        # the root again before it reads that level's q, and qold below the
+        # root is never read.
+        for L in range(0, prm.maxlevel):
+            if L >= 1:
+                b.restrict_level(L)  # EstimateLevelErrors(L): RestrictSolution, SetGhost(L - 1)
+            lvl = [i for i, d in enumerate(descs) if d["level"] == L]
+            flags = b.buffer_flags([descs[i] for i in lvl],
+                                   [b.errflags(i, prm.qtolerance[L]) for i in lvl],
+                                   prm.ibuffer[L])
+            made = []  # GridAdapt(L): RefineGrid over the level, creation order
+            for i, fl in zip(lvl, flags):
+                for box in b.new_subgrids(fl, prm.desfill[L], prm.mgp[L]):
+                    made.append(b.child_desc(descs[i], i, box[:nd].ravel()))
+            # Levels <= L keep their grids; level L + 1 becomes the new grids,
+            # youngest first; deeper levels lose their grids.
+            keep = [i for i, d in enumerate(descs) if d["level"] <= L]
+            index = {o: n for n, o in enumerate(keep)}
+            keep_q = {index[i]: b.get_q(i) for i in keep if descs[i]["level"] >= 0}
+            new_descs = []
+            for i in keep:
+                d = dict(descs[i])
+                d["parent"] = index[d["parent"]] if d["parent"] >= 0 else -1
+                new_descs.append(d)
+            for c in reversed(made):
+                c = dict(c)
+                c["parent"] = index[c["parent"]]
+                new_descs.append(c)
+            self._rebuild(new_descs, keep_q)
+            descs = new_descs
+            if not made:
+                # AMR(L + 1) on an empty level: EstimateLevelErrors(L + 1)
+                # still sets the ghosts of level L.
+                if L + 1 < prm.maxlevel:
+                    b.set_ghost_level(L)
+                break
+            children = list(range(len(keep), len(new_descs)))
+            for c in children:
+                b.init_patch(c)  # MakeNewGrid -> InitFields
+            for c in children:  # TransferValues from the level's old grids
+                dc = descs[c]
+                qc = None
+                for do, qo in old.get(L + 1, []):
+                    lo = [max(dc["mglobal"][k][0], do["mglobal"][k][0]) for k in range(nd)]
+                    hi = [min(dc["mglobal"][k][1], do["mglobal"][k][1]) for k in range(nd)]
+                    if any(hi[k] < lo[k] for k in range(nd)):
+                        continue
+                    if qc is None:
+                        qc = b.get_q(c)
+                    ts = tuple(slice(lo[k] - dc["mglobal"][k][0] + 1,
+                                     hi[k] - dc["mglobal"][k][0] + 2) for k in range(nd))
+                    ss = tuple(slice(lo[k] - do["mglobal"][k][0] + 1,
+                                     hi[k] - do["mglobal"][k][0] + 2) for k in range(nd))
+                    qc[ts] = qo[ss]
+                if qc is not None:
+                    b.put_q(c, qc)
+            b.set_ghost_level(L + 1)  # AMR(L + 1)
+        self.descs = descs
+        if self.firstamr:
+            b.fill_down()
+            self.firstamr = False
+        b.copy_q_to_qold()
+        return b.multigrid()
+
+    def state(self):
+        """q of every patch on a level >= 0 (descs order)."""
+        return [(i, self.b.get_q(i)) for i, d in enumerate(self.descs) if d["level"] >= 0]

@@ -1092,10 +1092,39 @@ int bsam_gpu_set_ghost(bsam_gpu* h) {
   return BSAM_OK;
 }
 
+int bsam_gpu_set_ghost_level(bsam_gpu* h, int level) {
+  if (!h || !h->have_hierarchy) return BSAM_ERR_STATE;
+  if (level < h->minlevel || level > h->finestlevel)
+    return fail(h, BSAM_ERR_ARG, "set_ghost_level: level out of range");
+  CU(cudaSetDevice(h->device));
+  if (plan(h, level).amr) amr_ghost(h, level, 0);
+  else ghost_level(h, level);
+  CU(cudaGetLastError());
+  CU(cudaStreamSynchronize(h->stream));
+  return BSAM_OK;
+}
+
 int bsam_gpu_fill_down(bsam_gpu* h) {
   if (!h || !h->have_hierarchy) return BSAM_ERR_STATE;
   CU(cudaSetDevice(h->device));
   if (h->amr) filldown(h);
+  CU(cudaGetLastError());
+  CU(cudaStreamSynchronize(h->stream));
+  return BSAM_OK;
+}
+
+int bsam_gpu_restrict_level(bsam_gpu* h, int level) {
+  if (!h || !h->have_hierarchy) return BSAM_ERR_STATE;
+  if (level < 1 || level > h->finestlevel)
+    return fail(h, BSAM_ERR_ARG, "restrict_level needs a refined level");
+  CU(cudaSetDevice(h->device));
+  const LevelPlan& L = plan(h, level);
+  if (h->rp.ndims == 2)
+    k_filldown<2><<<L.ncoarse, block_dim(), 0, h->stream>>>(h->d_patches, L.d_coarse);
+  else
+    k_filldown<3><<<L.ncoarse, block_dim(), 0, h->stream>>>(h->d_patches, L.d_coarse);
+  ++h->stats.launches;
+  amr_ghost(h, level - 1, 0);
   CU(cudaGetLastError());
   CU(cudaStreamSynchronize(h->stream));
   return BSAM_OK;

@@ -252,4 +252,84 @@ int bsam_host_new_subgrids(int ndims, const int* mx, const uint8_t* flags, doubl
   return (int)grids.size();
 }
 
+int bsam_host_buffer_flags(int ndims, int npatch, const int* mx, const int* mglobal,
+                           uint8_t* flags, int ibuffer) {
+  if ((ndims != 2 && ndims != 3) || npatch < 0 || (npatch > 0 && (!mx || !mglobal || !flags)) ||
+      ibuffer < 0)
+    return BSAM_ERR_ARG;
+  if (ibuffer == 0 || npatch == 0) return BSAM_OK;
+  const int nd = ndims;
+  std::vector<size_t> off(npatch + 1, 0);
+  for (int p = 0; p < npatch; ++p) {
+    size_t cells = 1;
+    for (int n = 0; n < nd; ++n) {
+      if (mx[3 * p + n] < 1) return BSAM_ERR_ARG;
+      cells *= (size_t)mx[3 * p + n];
+    }
+    off[p + 1] = off[p] + cells;
+  }
+  // The cells flagged on entry, in global indices.
+  std::vector<std::array<int, 3>> tagged;
+  for (int p = 0; p < npatch; ++p) {
+    const int m0 = mx[3 * p], m1 = mx[3 * p + 1], m2 = nd == 3 ? mx[3 * p + 2] : 1;
+    for (int k = 0; k < m2; ++k)
+      for (int j = 0; j < m1; ++j)
+        for (int i = 0; i < m0; ++i)
+          if (flags[off[p] + i + (size_t)m0 * (j + (size_t)m1 * k)])
+            tagged.push_back({mglobal[6 * p] + i, mglobal[6 * p + 2] + j,
+                              nd == 3 ? mglobal[6 * p + 4] + k : 1});
+  }
+  for (const auto& c : tagged)
+    for (int p = 0; p < npatch; ++p) {
+      int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+      bool hit = true;
+      for (int n = 0; n < nd; ++n) {
+        lo[n] = std::max(c[n] - ibuffer, mglobal[6 * p + 2 * n]);
+        hi[n] = std::min(c[n] + ibuffer, mglobal[6 * p + 2 * n + 1]);
+        hit = hit && lo[n] <= hi[n];
+      }
+      if (!hit) continue;
+      const int m0 = mx[3 * p], m1 = mx[3 * p + 1];
+      const int k0 = nd == 3 ? lo[2] - mglobal[6 * p + 4] : 0;
+      const int k1 = nd == 3 ? hi[2] - mglobal[6 * p + 4] : 0;
+      for (int k = k0; k <= k1; ++k)
+        for (int j = lo[1] - mglobal[6 * p + 2]; j <= hi[1] - mglobal[6 * p + 2]; ++j)
+          for (int i = lo[0] - mglobal[6 * p]; i <= hi[0] - mglobal[6 * p]; ++i)
+            flags[off[p] + i + (size_t)m0 * (j + (size_t)m1 * k)] = 1;
+    }
+  return BSAM_OK;
+}
+
+int bsam_host_child_desc(int ndims, const bsam_patch_desc* parent, int parent_index,
+                         const int* box, bsam_patch_desc* child) {
+  if ((ndims != 2 && ndims != 3) || !parent || !box || !child) return BSAM_ERR_ARG;
+  bsam_patch_desc c{};
+  c.level = parent->level + 1;
+  c.parent = parent_index;
+  c.dx = parent->dx / 2.0;
+  for (int n = 0; n < 3; ++n) {
+    c.mx[n] = 1;
+    c.mbounds[n][0] = c.mbounds[n][1] = 1;
+    c.mglobal[n][0] = c.mglobal[n][1] = 1;
+    c.xlower[n] = 0.0;
+  }
+  for (int f = 0; f < 6; ++f) c.mthbc[f] = 999;  // internalbc
+  for (int n = 0; n < ndims; ++n) {
+    const int lo = box[2 * n], hi = box[2 * n + 1];
+    if (lo < 1 || hi < lo || hi > parent->mx[n]) return BSAM_ERR_ARG;
+    c.mx[n] = (hi - lo + 1) * 2;
+    c.mbounds[n][0] = lo;
+    c.mbounds[n][1] = hi;
+    const int glo = parent->mglobal[n][0] + lo - 1, ghi = glo + hi - lo;
+    c.mglobal[n][0] = (glo - 1) * 2 + 1;
+    c.mglobal[n][1] = ghi * 2;
+    if (parent->mthbc[2 * n] < 999 && lo == 1) c.mthbc[2 * n] = parent->mthbc[2 * n];
+    if (parent->mthbc[2 * n + 1] < 999 && hi == parent->mx[n])
+      c.mthbc[2 * n + 1] = parent->mthbc[2 * n + 1];
+    c.xlower[n] = (double)(lo - 1) * parent->dx + parent->xlower[n];
+  }
+  *child = c;
+  return BSAM_OK;
+}
+
 }  // extern "C"

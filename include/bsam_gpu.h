@@ -121,6 +121,17 @@ int bsam_gpu_errflags(bsam_gpu* h, int patch, double tol, uint8_t* flags);
  * bsam_gpu_put_field of the overlapping cells afterwards.  FP64 form. */
 int bsam_gpu_init_patch(bsam_gpu* h, int patch);
 
+/* RestrictSolution of every patch of a refined level into its parent
+ * (afas:600-644: parent%q(mbounds) = Restriction(q)), then SetGhost of the
+ * parent level: the state changes EstimateLevelErrors makes before tagging
+ * the level (lib/bsamroutines.f90:963-1002). */
+int bsam_gpu_restrict_level(bsam_gpu* h, int level);
+
+/* SetGhost(level, 0) (boundary.f90:58-89) of one level alone (coarse-fine
+ * interpolation, sibling exchange and physical faces above the root; physical
+ * faces at and below it), as AMR(level) starts (lib/bsamroutines.f90:939-961). */
+int bsam_gpu_set_ghost_level(bsam_gpu* h, int level);
+
 /* Replaces the tree set-up that makes the hierarchy reachable to
  * MultigridIterations: RootInit/InitSeed/AllocFields
  * (lib/bsamroutines.f90:205-494, lib/bsamstorage.f90:46-123).  patches[] is in

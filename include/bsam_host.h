@@ -57,6 +57,24 @@ int bsam_host_take_time_steps(bsam_gpu* h, int nsteps, int root_patch, double* q
 int bsam_host_new_subgrids(int ndims, const int* mx, const uint8_t* flags, double desfill,
                            int mgp, int* boxes, int maxboxes);
 
+/* Buffering of the cell flags of one level's patches, as BufferAndList and
+ * InflateEdgeTags do it (lib/bsamroutines.f90:1159-1284): every cell flagged
+ * before the call flags the cells within ibuffer of it (a cube in global
+ * indices) on every patch of the level.  Patch p has mx[3p..3p+2] cells,
+ * global index box mglobal[6p..6p+5] (lo, hi per dimension) and flags at
+ * flags + offset of the patches before it, (1:mx)^d bytes each; in place. */
+int bsam_host_buffer_flags(int ndims, int npatch, const int* mx, const int* mglobal,
+                           uint8_t* flags, int ibuffer);
+
+/* The record MakeNewGrid gives the child of `parent` (index parent_index in
+ * the caller's table) over the parent box `box` (lo, hi per dimension)
+ * (lib/bsamroutines.f90:1581-1683): twice the box's cells, mbounds = box,
+ * the global box at the finer level, the parent's physical face codes on the
+ * faces the box shares with the parent, 999 elsewhere, xlower of the box's
+ * first cell, dx halved. */
+int bsam_host_child_desc(int ndims, const bsam_patch_desc* parent, int parent_index,
+                         const int* box, bsam_patch_desc* child);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1278,6 +1278,60 @@ int orc_run_uniform(const orc_params* p, const double* q0, int nsteps, double* q
   return 0;
 }
 
+// ---- a hierarchy held between calls (regridding runs) ----------------------
+struct orc_hier {
+  Ctx c;
+  std::vector<Patch*> byindex;  // patch table order
+};
+
+orc_hier* orc_hier_create(const orc_params* p, int npatch, const orc_patch* patches) {
+  auto* H = new orc_hier();
+  if (BuildFromPatches(H->c, p, npatch, patches)) {
+    delete H;
+    return nullptr;
+  }
+  for (auto& up : H->c.store) H->byindex.push_back(up.get());
+  return H;
+}
+void orc_hier_destroy(orc_hier* H) { delete H; }
+int orc_hier_q(orc_hier* H, int patch, double* q, int put) {
+  if (!H || patch < 0 || patch >= (int)H->byindex.size()) return -1;
+  Patch& P = *H->byindex[patch];
+  if (put) std::memcpy(P.q.d.data(), q, P.q.d.size() * sizeof(double));
+  else std::memcpy(q, P.q.d.data(), P.q.d.size() * sizeof(double));
+  return 0;
+}
+int orc_hier_set_ghost(orc_hier* H, int level) {
+  if (!H || level < H->c.minlevel || level > H->c.finestlevel) return -1;
+  return SetGhost(H->c, level, 0);
+}
+// RestrictSolution of a refined level into its parents (FillDownLevel's
+// expression, the same values) and the parent level's SetGhost.
+int orc_hier_restrict_level(orc_hier* H, int level) {
+  if (!H || level < 1 || level > H->c.finestlevel) return -1;
+  for (Patch* p : H->c.on(level)) FillDownLevel(H->c, *p, false);
+  return SetGhost(H->c, level - 1, 0);
+}
+int orc_hier_fill_down(orc_hier* H) {
+  if (!H) return -1;
+  FillDown(H->c, false);
+  return 0;
+}
+int orc_hier_copy_q_to_qold(orc_hier* H) {
+  if (!H) return -1;
+  for (int level = H->c.minlevel; level <= H->c.finestlevel; ++level)
+    for (Patch* pp : H->c.on(level)) CopyQToQold(*pp);
+  return 0;
+}
+int orc_hier_multigrid(orc_hier* H, int* nvcycles, double* residual) {
+  if (!H) return -1;
+  double last = 0.0;
+  const int nv = MultigridIterations(H->c, &last, nullptr);
+  if (nvcycles) *nvcycles = nv;
+  if (residual) *residual = last;
+  return 0;
+}
+
 int orc_run_hier(const orc_params* p, int npatch, const orc_patch* patches, const double* q0,
                  int nsteps, double* q_out, int* nvcycles, double* resid_final) {
   Ctx c;

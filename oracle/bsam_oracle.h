@@ -79,6 +79,21 @@ int orc_run_hier(const orc_params* p, int npatch, const orc_patch* patches,
                  const double* q0, int nsteps, double* q_out, int* nvcycles,
                  double* resid_final);
 
+/* A hierarchy held between calls, for regridding runs driven from outside:
+ * the patch table as orc_run_hier takes it; q of any patch (with ring) put
+ * or got (put != 0: q -> patch); SetGhost of one level; RestrictSolution of
+ * a refined level into its parents followed by the parent level's SetGhost;
+ * FillDown(solution); CopyQToQold on every level; MultigridIterations. */
+typedef struct orc_hier orc_hier;
+orc_hier* orc_hier_create(const orc_params* p, int npatch, const orc_patch* patches);
+void orc_hier_destroy(orc_hier* h);
+int orc_hier_q(orc_hier* h, int patch, double* q, int put);
+int orc_hier_set_ghost(orc_hier* h, int level);
+int orc_hier_restrict_level(orc_hier* h, int level);
+int orc_hier_fill_down(orc_hier* h);
+int orc_hier_copy_q_to_qold(orc_hier* h);
+int orc_hier_multigrid(orc_hier* h, int* nvcycles, double* residual);
+
 /* Interpolate2D (boundary.f90:135-323) on a fine patch qf (0:mx+1)^2 x nv
  * from its parent qc (0:pmx+1)^2 x nv; mbounds = {mb11, mb12, mb21, mb22}. */
 void orc_interpolate2d(const int* mx, int nv, const int* mbounds, const int* mthbc,

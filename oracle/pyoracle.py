@@ -76,6 +76,16 @@ def lib():
         L.orc_new_subgrids.argtypes = [ctypes.c_int, ip, ip, ctypes.c_double, ctypes.c_int, ip,
                                        ctypes.c_int]
         L.orc_new_subgrids.restype = ctypes.c_int
+        L.orc_hier_create.argtypes = [ctypes.POINTER(OrcParams), ctypes.c_int,
+                                      ctypes.POINTER(OrcPatch)]
+        L.orc_hier_create.restype = ctypes.c_void_p
+        L.orc_hier_destroy.argtypes = [ctypes.c_void_p]
+        L.orc_hier_q.argtypes = [ctypes.c_void_p, ctypes.c_int, dp, ctypes.c_int]
+        for name in ("orc_hier_set_ghost", "orc_hier_restrict_level"):
+            getattr(L, name).argtypes = [ctypes.c_void_p, ctypes.c_int]
+        for name in ("orc_hier_fill_down", "orc_hier_copy_q_to_qold"):
+            getattr(L, name).argtypes = [ctypes.c_void_p]
+        L.orc_hier_multigrid.argtypes = [ctypes.c_void_p, ip, dp]
         _lib = L
     return _lib
 
@@ -108,14 +118,9 @@ def params_of(prob) -> OrcParams:
     return p
 
 
-def run_hier(hier, nsteps):
-    """Oracle time stepping on a fixed hierarchy (bsam_b200.amr.Hierarchy):
-    returns the final q of every patch on a level >= 0, V-cycles and final
-    residual per step."""
-    L = lib()
-    n = len(hier.descs)
-    arr = (OrcPatch * n)()
-    for i, d in enumerate(hier.descs):
+def _patch_table(descs):
+    arr = (OrcPatch * len(descs))()
+    for i, d in enumerate(descs):
         o = arr[i]
         o.level, o.parent, o.dx = d["level"], d["parent"], d["dx"]
         for k in range(3):
@@ -126,6 +131,16 @@ def run_hier(hier, nsteps):
                 o.mglobal[k][s] = d["mglobal"][k][s]
         for f in range(6):
             o.mthbc[f] = d["mthbc"][f]
+    return arr
+
+
+def run_hier(hier, nsteps):
+    """Oracle time stepping on a fixed hierarchy (bsam_b200.amr.Hierarchy):
+    returns the final q of every patch on a level >= 0, V-cycles and final
+    residual per step."""
+    L = lib()
+    n = len(hier.descs)
+    arr = _patch_table(hier.descs)
     p = OrcParams()
     p.ndims = hier.ndims
     p.nsmoothingpasses = hier.nsmoothingpasses
@@ -291,3 +306,153 @@ def energy2d(h, alpha, eps, c):
     c = np.asfortranarray(c, dtype=np.float64)
     mxa = np.array([c.shape[0] - 2, c.shape[1] - 2, 1], dtype=np.int32)
     return lib().orc_energy2d(_ip(mxa), h, alpha, eps, _dp(c))
+
+
+# ---- regridding: the oracle side of a regrid run ------------------------------------
+
+def buffer_flags(nd, descs, flags, ibuffer):
+    """BufferAndList (lib/bsamroutines.f90:1159-1206) of every patch of a
+    level in ApplyOnLevel order, then InflateEdgeTags (1208-1241) with
+    BufferTaggedCells (1243-1284): a flagged cell whose buffer box lies inside
+    its patch flags that box there; one whose box crosses the patch's edge is
+    listed by global index, and each listed cell (last listed first) flags
+    its box, clipped, on every patch of the level.  Non-periodic boundaries
+    only.  flags: (1:mx)^d 0/1 arrays; returns buffered copies."""
+    out = [np.array(f, dtype=np.int32, copy=True) for f in flags]
+    if ibuffer <= 0:
+        return out
+    listed = []
+    for d, f in zip(descs, out):
+        tmp = f.copy()
+        mx = d["mx"][:nd]
+        for flat in range(tmp.size):
+            idx = np.unravel_index(flat, tmp.shape, order="F")
+            if tmp[idx] != 1:
+                continue
+            lo = [idx[k] + 1 - ibuffer for k in range(nd)]
+            hi = [idx[k] + 1 + ibuffer for k in range(nd)]
+            if any(lo[k] < 1 or hi[k] > mx[k] for k in range(nd)):
+                listed.append([idx[k] + 1 + d["mglobal"][k][0] - 1 for k in range(nd)])
+            else:
+                f[tuple(slice(lo[k] - 1, hi[k]) for k in range(nd))] = 1
+    for cell in reversed(listed):
+        for d, f in zip(descs, out):
+            lo = [max(cell[k] - ibuffer, d["mglobal"][k][0]) for k in range(nd)]
+            hi = [min(cell[k] + ibuffer, d["mglobal"][k][1]) for k in range(nd)]
+            if any(hi[k] < lo[k] for k in range(nd)):
+                continue
+            f[tuple(slice(lo[k] - d["mglobal"][k][0], hi[k] - d["mglobal"][k][0] + 1)
+                    for k in range(nd))] = 1
+    return out
+
+
+def child_desc(nd, parent, parent_index, box):
+    """MakeNewGrid's geometry (lib/bsamroutines.f90:1582-1684) of the child of
+    `parent` over index box `box` = [lo1, hi1, lo2, hi2(, lo3, hi3)]."""
+    internal = 999
+    b = [(int(box[2 * k]), int(box[2 * k + 1])) for k in range(nd)]
+    mx = [2 * (b[k][1] - b[k][0] + 1) for k in range(nd)] + [1] * (3 - nd)
+    mg = []
+    for k in range(nd):
+        glo = parent["mglobal"][k][0] + b[k][0] - 1
+        ghi = glo + b[k][1] - b[k][0]
+        mg.append([(glo - 1) * 2 + 1, ghi * 2])
+    codes = [internal] * 6
+    for k in range(nd):
+        if parent["mthbc"][2 * k] < internal and b[k][0] == 1:
+            codes[2 * k] = parent["mthbc"][2 * k]
+        if parent["mthbc"][2 * k + 1] < internal and b[k][1] == parent["mx"][k]:
+            codes[2 * k + 1] = parent["mthbc"][2 * k + 1]
+    return {"level": parent["level"] + 1, "parent": parent_index, "mx": mx,
+            "mbounds": [list(x) for x in b] + [[1, 1]] * (3 - nd),
+            "mglobal": mg + [[1, 1]] * (3 - nd), "mthbc": codes,
+            "dx": parent["dx"] / 2.0,
+            "xlower": [float(b[k][0] - 1) * parent["dx"] + parent["xlower"][k] for k in range(nd)]
+            + [0.0] * (3 - nd)}
+
+
+class OracleBackend:
+    """The regrid driver's numerics on the oracle: a held hierarchy
+    (orc_hier_*), SetErrFlagsUser, the mass-corrected prolongation of
+    InitFields, Berger-Rigoutsos, the buffer and MakeNewGrid's geometry
+    above."""
+
+    def __init__(self, ndims, dt, eps, qerrortol, alpha=1.0, maxvcycles=20, nsmoothingpasses=2):
+        self.nd = ndims
+        p = OrcParams()
+        p.ndims = ndims
+        p.nsmoothingpasses = nsmoothingpasses
+        p.maxvcycles = maxvcycles
+        p.errortype = 1
+        p.dt, p.qerrortol, p.alpha, p.eps = dt, qerrortol, alpha, eps
+        self.p = p
+        self.h = None
+        self.descs = []
+
+    def set_hierarchy(self, descs):
+        self.close()
+        self.descs = list(descs)
+        h = lib().orc_hier_create(ctypes.byref(self.p), len(descs), _patch_table(descs))
+        if not h:
+            raise RuntimeError("orc_hier_create failed")
+        self.h = ctypes.c_void_p(h)
+
+    def _shape(self, i):
+        return tuple(m + 2 for m in self.descs[i]["mx"][:self.nd]) + (2,)
+
+    def put_q(self, i, q):
+        q = np.asfortranarray(q, dtype=np.float64).copy(order="F")
+        if lib().orc_hier_q(self.h, i, _dp(q), 1) != 0:
+            raise RuntimeError("orc_hier_q")
+
+    def get_q(self, i):
+        out = np.zeros(self._shape(i), order="F")
+        if lib().orc_hier_q(self.h, i, _dp(out), 0) != 0:
+            raise RuntimeError("orc_hier_q")
+        return out
+
+    def _rc(self, rc, what):
+        if rc != 0:
+            raise RuntimeError(f"{what} failed: {rc}")
+
+    def set_ghost_level(self, level):
+        self._rc(lib().orc_hier_set_ghost(self.h, level), "set_ghost")
+
+    def restrict_level(self, level):
+        self._rc(lib().orc_hier_restrict_level(self.h, level), "restrict_level")
+
+    def fill_down(self):
+        self._rc(lib().orc_hier_fill_down(self.h), "fill_down")
+
+    def copy_q_to_qold(self):
+        self._rc(lib().orc_hier_copy_q_to_qold(self.h), "copy_q_to_qold")
+
+    def multigrid(self):
+        nv = np.zeros(1, dtype=np.int32)
+        res = np.zeros(1)
+        self._rc(lib().orc_hier_multigrid(self.h, _ip(nv), _dp(res)), "multigrid")
+        return int(nv[0]), float(res[0])
+
+    def errflags(self, i, tol):
+        q = self.get_q(i)
+        return errflags(q[..., 0], tol).astype(np.uint8)
+
+    def init_patch(self, i):
+        d = self.descs[i]
+        par = self.get_q(d["parent"])
+        sl = tuple(slice(d["mbounds"][k][0] - 1, d["mbounds"][k][1] + 2) for k in range(self.nd))
+        self.put_q(i, prolong_mc(self.nd, par[sl + (slice(None),)]))
+
+    def buffer_flags(self, descs, flags, ibuffer):
+        return [f.astype(np.uint8) for f in buffer_flags(self.nd, descs, flags, ibuffer)]
+
+    def new_subgrids(self, flags, desfill, mgp):
+        return new_subgrids(flags, desfill, mgp)
+
+    def child_desc(self, parent, parent_index, box):
+        return child_desc(self.nd, parent, parent_index, box)
+
+    def close(self):
+        if self.h is not None:
+            lib().orc_hier_destroy(self.h)
+            self.h = None

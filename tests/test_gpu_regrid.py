@@ -53,3 +53,42 @@ def test_init_patch_matches_oracle(gpu_lib, oracle, nd):
             assert got.shape == want.shape
             assert np.array_equal(got, want), (p, float(np.max(np.abs(got - want))))
             assert np.array_equal(s.get_qold(p), got)
+
+
+REGRID_CASES = {
+    # ndims: (root cells, eps, RegridParams)
+    2: (32, 0.02, amr.RegridParams(maxlevel=2, qtolerance=[0.05, 0.05], ibuffer=[1, 1],
+                                   desfill=[0.7, 0.7], mgp=[4, 4])),
+    3: (16, 0.05, amr.RegridParams(maxlevel=2, qtolerance=[0.15, 0.15], ibuffer=[1, 1],
+                                   desfill=[0.7, 0.7], mgp=[2, 2])),
+}
+
+
+@pytest.mark.parametrize("nd", [2, 3])
+def test_regrid_run_matches_oracle(gpu_lib, oracle, nd):
+    """Time steps with regridding every step (amr.RegridRun: tagging,
+    buffering, Berger-Rigoutsos, new-patch prolongation, value transfer, the
+    level-by-level ghosts and restrictions of AMR(rootlevel), FillDown,
+    MultigridIterations), engine against oracle: the same grids every step,
+    the same V-cycle counts, q within 1e-11."""
+    n, eps, prm = REGRID_CASES[nd]
+    hier = amr.build(n, [], eps=eps, dt=5e-5, qerrortol=1e-9, field="drop", ndims=nd)
+    g = amr.GpuBackend(nd, hier.dt, hier.eps, hier.qerrortol)
+    o = oracle.OracleBackend(nd, hier.dt, hier.eps, hier.qerrortol)
+    try:
+        rg = amr.RegridRun(g, hier, prm)
+        ro = amr.RegridRun(o, hier, prm)
+        for step in range(3):
+            nvg, resg = rg.step()
+            nvo, reso = ro.step()
+            assert rg.descs == ro.descs, f"grids differ at step {step}"
+            assert nvg == nvo
+            assert resg == pytest.approx(reso, rel=1e-6, abs=1e-15)
+            assert max(d["level"] for d in rg.descs) == 2
+            for (i, qg), (_, qo) in zip(rg.state(), ro.state()):
+                d = rg.descs[i]
+                inner = tuple(slice(1, m + 1) for m in d["mx"][:nd])
+                np.testing.assert_allclose(qg[inner], qo[inner], rtol=0, atol=1e-11)
+    finally:
+        g.close()
+        o.close()

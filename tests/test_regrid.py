@@ -41,3 +41,85 @@ def test_new_subgrids_partition(gpu_free_lib, oracle, seed):
 
 def test_new_subgrids_nothing_flagged(gpu_free_lib):
     assert amr.new_subgrids(np.zeros((16, 16), dtype=np.uint8), 0.9, 4).shape[0] == 0
+
+
+def _level(nd, rng):
+    """Three disjoint patches of one level (two of them side by side) in a
+    48^d index space, with random flags: descs and flags."""
+    if nd == 2:
+        boxes = [((1, 1), (16, 12)), ((17, 1), (10, 12)), ((5, 25), (20, 14))]
+    else:
+        boxes = [((1, 1, 1), (10, 8, 6)), ((11, 1, 1), (6, 8, 6)), ((3, 13, 9), (8, 6, 10))]
+    descs, flags = [], []
+    for lo, sz in boxes:
+        mg = [[lo[k], lo[k] + sz[k] - 1] for k in range(nd)] + [[1, 1]] * (3 - nd)
+        descs.append({"level": 1, "parent": 0, "mx": list(sz) + [1] * (3 - nd),
+                      "mbounds": [[1, 1]] * 3, "mglobal": mg, "mthbc": [999] * 6,
+                      "dx": 1.0, "xlower": [0.0] * 3})
+        flags.append((rng.random(sz) < 0.03).astype(np.uint8))
+    return descs, flags
+
+
+@pytest.mark.parametrize("nd,ibuffer", [(2, 1), (2, 2), (3, 1)])
+def test_buffer_flags_match_oracle(gpu_free_lib, oracle, nd, ibuffer):
+    """bsam_host_buffer_flags against the oracle's restatement of
+    BufferAndList + InflateEdgeTags (buffers cross into neighbour patches)."""
+    rng = np.random.default_rng(7 + nd + ibuffer)
+    descs, flags = _level(nd, rng)
+    flags[0][(-1,) + (0,) * (nd - 1)] = 1   # at the shared face of patches 0 and 1
+    got = amr.buffer_flags(nd, descs, flags, ibuffer)
+    want = oracle.buffer_flags(nd, descs, flags, ibuffer)
+    for g, w, f in zip(got, want, flags):
+        assert np.array_equal(g, w)
+        assert np.all(g[f == 1] == 1)
+    assert got[1][(0,) * nd] == 1           # the neighbour got the buffer
+    assert all(np.array_equal(g, f) for g, f in zip(amr.buffer_flags(nd, descs, flags, 0), flags))
+
+
+@pytest.mark.parametrize("nd", [2, 3])
+def test_child_desc_matches_oracle(gpu_free_lib, oracle, nd):
+    """bsam_host_child_desc (MakeNewGrid's geometry) against the oracle's
+    restatement, for boxes inside, and touching each face of, a parent."""
+    rng = np.random.default_rng(nd)
+    mx = [12, 10, 8][:nd]
+    parent = {"level": 1, "parent": 0, "mx": mx + [1] * (3 - nd), "mbounds": [[1, 1]] * 3,
+              "mglobal": [[5, 4 + mx[k]] for k in range(nd)] + [[1, 1]] * (3 - nd),
+              "mthbc": [1, 999, 999, 1, 1, 999][:2 * nd] + [1] * (6 - 2 * nd),
+              "dx": 0.125, "xlower": [0.5, 0.375, 0.25][:nd] + [0.0] * (3 - nd)}
+    for _ in range(20):
+        box = []
+        for k in range(nd):
+            a, b = sorted(rng.integers(1, mx[k] + 1, size=2))
+            box += [int(a), int(b)]
+        got = amr.child_desc(nd, parent, 3, box)
+        want = oracle.child_desc(nd, parent, 3, box)
+        assert got == want, (box, got, want)
+
+
+def test_regrid_run_on_oracle(oracle):
+    """The regrid driver (amr.RegridRun) over the oracle backend: every step
+    converges, new grids nest inside their parents' interiors and cover the
+    buffered flags of the level below."""
+    hier = amr.build(32, [], eps=0.02, dt=5e-5, qerrortol=1e-9, field="drop")
+    prm = amr.RegridParams(maxlevel=2, qtolerance=[0.05, 0.05], ibuffer=[1, 1],
+                           desfill=[0.7, 0.7], mgp=[4, 4])
+    b = oracle.OracleBackend(2, hier.dt, hier.eps, hier.qerrortol)
+    try:
+        run = amr.RegridRun(b, hier, prm)
+        for _ in range(3):
+            nv, res = run.step()
+            assert nv < 20 and res < 1e-9
+            levels = {d["level"] for d in run.descs}
+            assert max(levels) == 2
+            for d in run.descs:
+                if d["level"] < 1:
+                    continue
+                p = run.descs[d["parent"]]
+                assert p["level"] == d["level"] - 1
+                for k in range(2):
+                    lo, hi = d["mbounds"][k]
+                    assert 1 <= lo <= hi <= p["mx"][k]
+                    assert d["mglobal"][k] == [(p["mglobal"][k][0] + lo - 2) * 2 + 1,
+                                               (p["mglobal"][k][0] + hi - 1) * 2]
+    finally:
+        b.close()

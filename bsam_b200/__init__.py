@@ -66,7 +66,8 @@ ABI_SYMBOLS = (
     "bsam_gpu_resid_norm_noalloc", "bsam_gpu_set_tuning", "bsam_gpu_fill_down",
     "bsam_gpu_errflags", "bsam_gpu_init_patch", "bsam_host_new_subgrids",
     "bsam_gpu_restrict_level", "bsam_host_buffer_flags", "bsam_host_child_desc",
-    "bsam_gpu_set_ghost_level",
+    "bsam_host_format_frame", "bsam_host_write_frame",
+    "bsam_gpu_set_ghost_level", "bsam_gpu_after_step_stats",
     "bsam_batch_create", "bsam_batch_destroy", "bsam_batch_set_tuning", "bsam_batch_footprint",
     "bsam_batch_submit", "bsam_batch_advance", "bsam_batch_sync", "bsam_batch_run",
     "bsam_batch_poll", "bsam_batch_slot_phase", "bsam_batch_collect", "bsam_batch_get_stream", "bsam_batch_profile", "bsam_batch_submit_seeded", "bsam_batch_busy",
@@ -110,10 +111,16 @@ def lib():
     L.bsam_gpu_init_patch.argtypes = [vp, ctypes.c_int]
     L.bsam_gpu_restrict_level.argtypes = [vp, ctypes.c_int]
     L.bsam_gpu_set_ghost_level.argtypes = [vp, ctypes.c_int]
+    L.bsam_gpu_after_step_stats.argtypes = [vp, dp]
     L.bsam_host_buffer_flags.argtypes = [ctypes.c_int, ctypes.c_int, ip, ip,
                                          ctypes.POINTER(ctypes.c_uint8), ctypes.c_int]
     L.bsam_host_child_desc.argtypes = [ctypes.c_int, ctypes.POINTER(PatchDesc), ctypes.c_int,
                                        ip, ctypes.POINTER(PatchDesc)]
+    L.bsam_host_format_frame.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_double,
+                                         ctypes.c_int, ctypes.c_int, ctypes.POINTER(PatchDesc),
+                                         ctypes.POINTER(dp)]
+    L.bsam_host_write_frame.argtypes = [vp, ctypes.c_char_p, ctypes.c_int, ctypes.c_double,
+                                        ctypes.c_int, ctypes.POINTER(PatchDesc)]
     L.bsam_host_new_subgrids.argtypes = [ctypes.c_int, ip, ctypes.POINTER(ctypes.c_uint8),
                                          ctypes.c_double, ctypes.c_int, ip, ctypes.c_int]
     L.bsam_gpu_destroy.argtypes = [vp]

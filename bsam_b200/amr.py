@@ -14,6 +14,7 @@ from __future__ import annotations
 
 import dataclasses
 import math
+import os
 
 import numpy as np
 
@@ -273,6 +274,46 @@ def build(n_root: int, boxes: list, eps: float, dt: float = 5e-5, qerrortol: flo
                      maxvcycles=maxvcycles)
 
 
+def desc_array(descs):
+    """The patch table as bsam_patch_desc records."""
+    from . import PatchDesc
+    arr = (PatchDesc * len(descs))()
+    for i, d in enumerate(descs):
+        o = arr[i]
+        o.level, o.parent, o.dx = d["level"], d["parent"], d["dx"]
+        for k in range(3):
+            o.mx[k] = d["mx"][k]
+            o.xlower[k] = d["xlower"][k]
+            for s in range(2):
+                o.mbounds[k][s] = d["mbounds"][k][s]
+                o.mglobal[k][s] = d["mglobal"][k][s]
+        for f in range(6):
+            o.mthbc[f] = d["mthbc"][f]
+    return arr
+
+
+def format_frame(path: str, nd: int, time: float, descs: list, qs: dict):
+    """WriteQ's frame file from host arrays (bsam_host_format_frame): qs maps
+    the index of every patch on a level >= 0 to its q with ring."""
+    import ctypes
+    from . import BsamError, lib
+    dp = ctypes.POINTER(ctypes.c_double)
+    keep = {i: np.asfortranarray(q, dtype=np.float64) for i, q in qs.items()}
+    ptrs = (dp * len(descs))()
+    for i in range(len(descs)):
+        ptrs[i] = keep[i].ctypes.data_as(dp) if i in keep else dp()
+    finest = max(d["level"] for d in descs)
+    rc = lib().bsam_host_format_frame(os.fsencode(path), nd, time, finest, len(descs),
+                                      desc_array(descs), ptrs)
+    if rc != 0:
+        raise BsamError(f"bsam_host_format_frame failed ({rc})")
+
+
+def frame_path(outdir: str, nframe: int) -> str:
+    """The reference's frame name: <outdir>/mNNNNN.dat."""
+    return os.path.join(outdir, "m%05d.dat" % nframe)
+
+
 # ---- regridding every time step --------------------------------------------------
 
 @dataclasses.dataclass
@@ -309,23 +350,16 @@ class GpuBackend:
         _check(rc, self.h, what)
 
     def set_hierarchy(self, descs):
-        from . import PatchDesc, lib
-        n = len(descs)
-        arr = (PatchDesc * n)()
-        for i, d in enumerate(descs):
-            o = arr[i]
-            o.level, o.parent, o.dx = d["level"], d["parent"], d["dx"]
-            for k in range(3):
-                o.mx[k] = d["mx"][k]
-                o.xlower[k] = d["xlower"][k]
-                for s in range(2):
-                    o.mbounds[k][s] = d["mbounds"][k][s]
-                    o.mglobal[k][s] = d["mglobal"][k][s]
-            for f in range(6):
-                o.mthbc[f] = d["mthbc"][f]
+        from . import lib
         self.descs = list(descs)
         self._call("set_hierarchy", lib().bsam_gpu_set_hierarchy(
-            self.h, n, arr, max(d["level"] for d in descs)))
+            self.h, len(descs), desc_array(descs), max(d["level"] for d in descs)))
+
+    def write_frame(self, path, time):
+        """WriteQ from the device (bsam_host_write_frame)."""
+        from . import lib
+        self._call("write_frame", lib().bsam_host_write_frame(
+            self.h, os.fsencode(path), self.nd, time, len(self.descs), desc_array(self.descs)))
 
     def _shape(self, p):
         d = self.descs[p]
@@ -379,6 +413,13 @@ class GpuBackend:
         self._call("multigrid_iterations", lib().bsam_gpu_multigrid_iterations(
             self.h, ctypes.byref(nv), ctypes.byref(res), ctypes.byref(conv)))
         return nv.value, res.value
+
+    def after_step_stats(self):
+        import ctypes
+        from . import lib
+        out = (ctypes.c_double * 2)()
+        self._call("after_step_stats", lib().bsam_gpu_after_step_stats(self.h, out))
+        return out[0], out[1]
 
     def buffer_flags(self, descs, flags, ibuffer):
         return buffer_flags(self.nd, descs, flags, ibuffer)
@@ -561,6 +602,11 @@ class RegridRun:
             self.firstamr = False
         b.copy_q_to_qold()
         return b.multigrid()
+
+    def stats(self):
+        """AfterStepStatistics after the step: (composite mass, composite
+        Energy2D; 0 in 3D)."""
+        return self.b.after_step_stats()
 
     def state(self):
         """q of every patch on a level >= 0 (descs order)."""

@@ -34,6 +34,7 @@
 #include "mixed.cuh"
 #include "amr.cuh"
 #include "regrid.cuh"
+#include "stats.cuh"
 
 using namespace bsam;
 
@@ -1319,6 +1320,141 @@ int bsam_gpu_energy(bsam_gpu* h, double* energy) {
     s[which] = h->h_status->esum;
   }
   *energy = h2 * (s[0] + tmp * s[1]);
+  return BSAM_OK;
+}
+
+int bsam_gpu_after_step_stats(bsam_gpu* h, double* integral) {
+  if (!h || !h->have_hierarchy || !integral) return BSAM_ERR_ARG;
+  const int nd = h->rp.ndims;
+  // The terms, in the order AfterStepStatistics adds them: levels finest to
+  // root, ApplyOnLevel (table) order within a level.  Per patch: sum(c), then
+  // (2D) Ff and squared-difference sums; on a refined patch the same over its
+  // parent's footprint.
+  struct Term {
+    int patch, kind, lo[3], hi[3];
+  };
+  std::vector<Term> terms;
+  std::vector<int> order;
+  for (int level = h->finestlevel; level >= 0; --level)
+    for (int p = 0; p < h->nuser; ++p)
+      if (h->desc[p].level == level) order.push_back(p);
+  for (int p : order) {
+    const bsam_patch_desc& d = h->desc[p];
+    if (h->hp[p].prec != PREC_F64) return fail(h, BSAM_ERR_UNSUPPORTED, "stats need FP64 patches");
+    const int nk = nd == 2 ? 3 : 1;  // 2D adds the two energy sums
+    for (int side = 0; side < (d.level > 0 ? 2 : 1); ++side) {
+      Term t{};
+      t.patch = side == 0 ? p : d.parent;
+      if (side == 1 && h->hp[t.patch].prec != PREC_F64)
+        return fail(h, BSAM_ERR_UNSUPPORTED, "stats need FP64 patches");
+      for (int n = 0; n < 3; ++n) {
+        if (n >= nd) {
+          t.lo[n] = t.hi[n] = 0;
+        } else if (side == 0) {
+          t.lo[n] = 1;
+          t.hi[n] = d.mx[n];
+        } else {
+          t.lo[n] = d.mbounds[n][0];
+          t.hi[n] = d.mbounds[n][1];
+        }
+      }
+      for (int kind = 0; kind < nk; ++kind) {
+        t.kind = kind;
+        terms.push_back(t);
+      }
+    }
+  }
+  // Split each term's rows over CTAs (about 16k cells a CTA).
+  std::vector<StatBlock> blocks;
+  std::vector<int> first(terms.size() + 1, 0);
+  for (size_t ti = 0; ti < terms.size(); ++ti) {
+    const Term& t = terms[ti];
+    const int nx = t.hi[0] - t.lo[0] + 1, ny = t.hi[1] - t.lo[1] + 1;
+    const int nz = nd == 3 ? t.hi[2] - t.lo[2] + 1 : 1;
+    const int rows = ny * nz;
+    const int per = std::max(1, 16384 / std::max(1, nx));
+    first[ti] = (int)blocks.size();
+    for (int r0 = 0; r0 < rows; r0 += per) {
+      StatBlock b{};
+      b.patch = t.patch;
+      b.kind = t.kind;
+      for (int n = 0; n < 3; ++n) {
+        b.lo[n] = t.lo[n];
+        b.hi[n] = t.hi[n];
+      }
+      b.row0 = r0;
+      b.row1 = std::min(rows, r0 + per);
+      blocks.push_back(b);
+    }
+  }
+  first[terms.size()] = (int)blocks.size();
+  const int nb = (int)blocks.size();
+  CU(cudaSetDevice(h->device));
+  StatBlock* d_blocks = nullptr;
+  double* d_part = nullptr;
+  std::vector<double> part(nb);
+  cudaError_t e = cudaMalloc(&d_blocks, sizeof(StatBlock) * nb);
+  if (e == cudaSuccess) e = cudaMalloc(&d_part, sizeof(double) * nb);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(d_blocks, blocks.data(), sizeof(StatBlock) * nb, cudaMemcpyHostToDevice,
+                        h->stream);
+  if (e == cudaSuccess) {
+    if (nd == 2) k_stats<2><<<nb, 256, 0, h->stream>>>(h->d_patches, d_blocks, d_part);
+    else k_stats<3><<<nb, 256, 0, h->stream>>>(h->d_patches, d_blocks, d_part);
+    ++h->stats.launches;
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(part.data(), d_part, sizeof(double) * nb, cudaMemcpyDeviceToHost,
+                        h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (d_blocks) cudaFree(d_blocks);
+  if (d_part) cudaFree(d_part);
+  if (e != cudaSuccess) return fail(h, BSAM_ERR_CUDA, cudaGetErrorString(e));
+  auto term_sum = [&](size_t ti) {
+    double s = 0.0;
+    for (int b = first[ti]; b < first[ti + 1]; ++b) s += part[b];
+    return s;
+  };
+  // Combine as AfterStep2D/3D do.
+  const double eps2 = h->rp.eps * h->rp.eps;
+  double r1 = 0.0, r2 = 0.0;
+  size_t ti = 0;
+  auto energy = [&](double hh, double sF, double sG) {
+    const double h2 = hh * hh;
+    return h2 * (sF + eps2 / h2 / 4.0 * sG);
+  };
+  for (int p : order) {
+    const bsam_patch_desc& d = h->desc[p];
+    const double hh = h->hp[p].h, ch = hh * 2.0;
+    const double hd = nd == 2 ? hh * hh : hh * hh * hh;
+    const double chd = nd == 2 ? ch * ch : ch * ch * ch;
+    if (nd == 2) {
+      const double s = term_sum(ti), sF = term_sum(ti + 1), sG = term_sum(ti + 2);
+      ti += 3;
+      if (d.level == 0) {
+        r1 = r1 + hd * s;
+        r2 = r2 + energy(hh, sF, sG);
+      } else {
+        const double cs = term_sum(ti), cF = term_sum(ti + 1), cG = term_sum(ti + 2);
+        ti += 3;
+        r1 = r1 + hd * s - chd * cs;
+        r2 = r2 + energy(hh, sF, sG) - energy(ch, cF, cG);
+      }
+    } else {
+      const double s = term_sum(ti);
+      ti += 1;
+      if (d.level == 0) {
+        r1 = r1 + hd * s;
+      } else {
+        const double cs = term_sum(ti);
+        ti += 1;
+        r1 = r1 + hd * s - chd * cs;
+      }
+    }
+  }
+  integral[0] = r1;
+  integral[1] = r2;
   return BSAM_OK;
 }
 

@@ -11,7 +11,9 @@
 #include <array>
 #include <cmath>
 #include <cstdlib>
+#include <cstdio>
 #include <cstring>
+#include <string>
 #include <vector>
 
 #include "../../include/bsam_gpu.h"
@@ -32,6 +34,78 @@ int resolve_minlevel(const bsam_host_grid* g) {
     for (int n = 0; n < g->ndims; ++n) m[n] /= 2;
   }
   return -ml;
+}
+
+
+// Fortran edit descriptors of the frame file, as gfortran writes them.
+// Fw.d: fixed, right-justified in w columns, a leading "0." kept.
+void put_f(std::string& o, double x, int w, int d) {
+  char b[64];
+  std::snprintf(b, sizeof b, "%*.*f", w, d, x);
+  o += b;
+}
+// ESw.d: one nonzero digit before the point, d after, a two-digit exponent
+// written "E+nn"; a three-digit exponent drops the E ("+nnn").
+void put_es(std::string& o, double x, int w, int d) {
+  char b[64];
+  std::snprintf(b, sizeof b, "%.*E", d, x);
+  std::string t(b);
+  const size_t e = t.find('E');
+  if (e != std::string::npos && t.size() - e - 2 > 2) t.erase(e, 1);
+  if ((int)t.size() < w) t.insert(0, (size_t)(w - (int)t.size()), ' ');
+  o += t;
+}
+void put_i(std::string& o, int v, int w) {
+  char b[32];
+  std::snprintf(b, sizeof b, "%*d", w, v);
+  o += b;
+}
+
+// OutputQ of one patch (lib/bsaminputoutput.f90:78-131) with WriteQ2D/3D
+// (133-172): q is the patch's (0:mx+1)^d x nrvars array, column-major.
+void output_q(std::string& o, int nd, const bsam_patch_desc& d, const double* xupper,
+              const double* q) {
+  o += "  \n";  // write(54,*) ' ': a list-directed record, a blank then ' '
+  put_i(o, d.level, 3);
+  o += ' ';
+  put_i(o, nd, 3);
+  o += ' ';
+  put_i(o, 2, 3);
+  o += ' ';
+  put_i(o, 2, 3);
+  o += '\n';
+  const double dx[3] = {d.dx, d.dx, d.dx};
+  const double* rows[3] = {dx, d.xlower, xupper};
+  for (const double* r : rows) {
+    for (int n = 0; n < nd; ++n) {
+      if (n) o += ' ';
+      put_f(o, r[n], 25, 12);
+    }
+    o += '\n';
+  }
+  for (int n = 0; n < nd; ++n) {
+    if (n) o += ' ';
+    put_i(o, d.mx[n], 8);
+  }
+  o += '\n';
+  for (int n = 0; n < nd; ++n)
+    for (int s = 0; s < 2; ++s) {
+      if (n || s) o += ' ';
+      put_i(o, d.mglobal[n][s], 8);
+    }
+  o += '\n';
+  const int e0 = d.mx[0] + 2, e1 = d.mx[1] + 2, e2 = nd == 3 ? d.mx[2] + 2 : 1;
+  const size_t plane = (size_t)e0 * e1 * e2;
+  // 10(es20.12,2x) in 2D, 10(f25.12,2x) in 3D; the 2x after the last value
+  // is a pending skip that ends with the record.
+  for (size_t c = 0; c < plane; ++c) {
+    for (int v = 0; v < 2; ++v) {
+      if (v) o += "  ";
+      if (nd == 2) put_es(o, q[c + v * plane], 20, 12);
+      else put_f(o, q[c + v * plane], 25, 12);
+    }
+    o += '\n';
+  }
 }
 
 }  // namespace
@@ -330,6 +404,63 @@ int bsam_host_child_desc(int ndims, const bsam_patch_desc* parent, int parent_in
   }
   *child = c;
   return BSAM_OK;
+}
+
+
+int bsam_host_format_frame(const char* path, int ndims, double time, int finestlevel,
+                           int npatch, const bsam_patch_desc* patches, const double* const* q) {
+  if (!path || (ndims != 2 && ndims != 3) || npatch < 0 || (npatch > 0 && (!patches || !q)))
+    return BSAM_ERR_ARG;
+  std::string o;
+  put_f(o, time, 25, 12);
+  o += '\n';
+  put_i(o, finestlevel, 3);
+  o += '\n';
+  // Levels rootlevel .. finestlevel, table (ApplyOnLevel) order within each.
+  for (int level = 0; level <= finestlevel; ++level)
+    for (int p = 0; p < npatch; ++p) {
+      const bsam_patch_desc& d = patches[p];
+      if (d.level != level) continue;
+      if (!q[p]) return BSAM_ERR_ARG;
+      // xupper: the root's is xlower + mx dx; a refined patch's is
+      // mbounds(:,2) * parent dx + parent xlower (MakeNewGrid).
+      double xu[3] = {0.0, 0.0, 0.0};
+      for (int n = 0; n < ndims; ++n) {
+        if (d.level == 0 || d.parent < 0 || d.parent >= npatch) {
+          xu[n] = d.xlower[n] + d.mx[n] * d.dx;
+        } else {
+          const bsam_patch_desc& pd = patches[d.parent];
+          xu[n] = (double)d.mbounds[n][1] * pd.dx + pd.xlower[n];
+        }
+      }
+      output_q(o, ndims, d, xu, q[p]);
+    }
+  FILE* f = std::fopen(path, "wb");
+  if (!f) return BSAM_ERR_ARG;
+  const size_t w = std::fwrite(o.data(), 1, o.size(), f);
+  const int rc = std::fclose(f);
+  return (w == o.size() && rc == 0) ? BSAM_OK : BSAM_ERR_ARG;
+}
+
+int bsam_host_write_frame(bsam_gpu* h, const char* path, int ndims, double time, int npatch,
+                          const bsam_patch_desc* patches) {
+  if (!h || !path || (ndims != 2 && ndims != 3) || npatch <= 0 || !patches) return BSAM_ERR_ARG;
+  const int nd = ndims;
+  int finest = 0;
+  for (int p = 0; p < npatch; ++p) finest = std::max(finest, patches[p].level);
+  std::vector<std::vector<double>> store(npatch);
+  std::vector<const double*> q(npatch, nullptr);
+  for (int p = 0; p < npatch; ++p) {
+    const bsam_patch_desc& d = patches[p];
+    if (d.level < 0) continue;
+    size_t n = 2;
+    for (int k = 0; k < nd; ++k) n *= (size_t)(d.mx[k] + 2);
+    store[p].resize(n);
+    const int rc = bsam_gpu_get_field(h, p, BSAM_FIELD_Q, store[p].data());
+    if (rc != BSAM_OK) return rc;
+    q[p] = store[p].data();
+  }
+  return bsam_host_format_frame(path, nd, time, finest, npatch, patches, q.data());
 }
 
 }  // extern "C"

@@ -180,6 +180,14 @@ int bsam_gpu_residual_trace(bsam_gpu* h, double* out, int maxn);
  * (problems/simple_cahn-hilliard/problem.f90:121-122, 416-418). */
 int bsam_gpu_mass(bsam_gpu* h, double* mass);
 
+/* AfterStepStatistics (lib/bsamroutines.f90:893-937) over the whole
+ * hierarchy, finest level first: integral[0] = the composite mass (root
+ * h^d sum(c), plus on each refined patch h^d sum(c) - (2h)^d sum(parent c
+ * over its footprint)); integral[1] = the composite Energy2D the same way
+ * (AfterStep2D, problem.f90:102-134), 0 in 3D (AfterStep3D,
+ * problem.f90:398-424 adds none).  FP64 patches only. */
+int bsam_gpu_after_step_stats(bsam_gpu* h, double* integral);
+
 /* The CUDA stream (cudaStream_t) every kernel of this handle runs on, for
  * callers that order their own work or record events against it. */
 int bsam_gpu_get_stream(bsam_gpu* h, void** stream);

@@ -75,6 +75,22 @@ int bsam_host_buffer_flags(int ndims, int npatch, const int* mx, const int* mglo
 int bsam_host_child_desc(int ndims, const bsam_patch_desc* parent, int parent_index,
                          const int* box, bsam_patch_desc* child);
 
+/* WriteQ (lib/bsaminputoutput.f90:51-172): the frame file of a hierarchy --
+ * time (f25.12), finestlevel (i3), then per patch on levels 0 .. finestlevel
+ * in table order: a blank record, "level ndims 2 nrvars" (i3), dx, xlower,
+ * xupper (f25.12), mx, mglobal (i8), and q with its ghost ring, one cell a
+ * record, i fastest (2D: es20.12 values, 3D: f25.12; two blanks between).
+ * q[p]: patch p's (0:mx+1)^d x 2 array, column-major (ignored, may be NULL,
+ * for patches below the root). */
+int bsam_host_format_frame(const char* path, int ndims, double time, int finestlevel,
+                           int npatch, const bsam_patch_desc* patches, const double* const* q);
+
+/* The frame file of the hierarchy resident in h (patch table `patches`, as
+ * given to bsam_gpu_set_hierarchy): q of every patch on a level >= 0 read
+ * back with bsam_gpu_get_field, then bsam_host_format_frame. */
+int bsam_host_write_frame(bsam_gpu* h, const char* path, int ndims, double time, int npatch,
+                          const bsam_patch_desc* patches);
+
 #ifdef __cplusplus
 }
 #endif

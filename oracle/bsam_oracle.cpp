@@ -1332,6 +1332,64 @@ int orc_hier_multigrid(orc_hier* H, int* nvcycles, double* residual) {
   return 0;
 }
 
+// AfterStepStatistics (lib/bsamroutines.f90:893-937) with AfterStep2D/3D
+// (problem.f90:102-134, 398-424): levels finestlevel down to rootlevel,
+// ApplyOnLevel order; on a refined patch, qc is the parent's q over
+// mbounds - 1 .. mbounds + 1.
+int orc_hier_after_step(orc_hier* H, double* integral) {
+  if (!H || !integral) return -1;
+  Ctx& c = H->c;
+  const int nd = c.ndims;
+  double r1 = 0.0, r2 = 0.0;
+  // Column-major sum of c over [lo, hi] of patch P (Fortran sum).
+  auto csum = [&](Patch& P, const int* lo, const int* hi) {
+    double s = 0.0;
+    for (int k = lo[2]; k <= hi[2]; ++k)
+      for (int j = lo[1]; j <= hi[1]; ++j)
+        for (int i = lo[0]; i <= hi[0]; ++i) s = s + P.q(i, j, k, 1);
+    return s;
+  };
+  // Energy2D of c over [lo - 1, hi + 1] of P (a copy, then the leaf routine).
+  auto energy = [&](Patch& P, const int* lo, const int* hi, double h) {
+    const int n1 = hi[0] - lo[0] + 1, n2 = hi[1] - lo[1] + 1;
+    std::vector<double> a((size_t)(n1 + 2) * (n2 + 2));
+    for (int j = 0; j <= n2 + 1; ++j)
+      for (int i = 0; i <= n1 + 1; ++i)
+        a[(size_t)i + (size_t)(n1 + 2) * j] = P.q(lo[0] - 1 + i, lo[1] - 1 + j, 1, 1);
+    const int mx[2] = {n1, n2};
+    return orc_energy2d(mx, h, c.alpha, c.eps, a.data());
+  };
+  for (int level = c.finestlevel; level >= 0; --level) {
+    for (Patch* pp : c.on(level)) {
+      Patch& P = *pp;
+      const double h = P.dx[0], ch = h * 2.0;
+      int lo[3] = {1, 1, 1}, hi[3] = {P.mx[0], P.mx[1], nd == 3 ? P.mx[2] : 1};
+      int clo[3] = {1, 1, 1}, chi[3] = {1, 1, 1};
+      for (int n = 0; n < nd; ++n) {
+        clo[n] = P.mbounds[n][0];
+        chi[n] = P.mbounds[n][1];
+      }
+      if (nd == 2) {
+        const double h2 = h * h, ch2 = ch * ch;
+        if (level == 0) {
+          r1 = r1 + h2 * csum(P, lo, hi);
+          r2 = r2 + energy(P, lo, hi, h);
+        } else {
+          r1 = r1 + h2 * csum(P, lo, hi) - ch2 * csum(*P.parent, clo, chi);
+          r2 = r2 + energy(P, lo, hi, h) - energy(*P.parent, clo, chi, ch);
+        }
+      } else {
+        const double h3 = h * h * h, ch3 = ch * ch * ch;
+        if (level == 0) r1 = r1 + h3 * csum(P, lo, hi);
+        else r1 = r1 + h3 * csum(P, lo, hi) - ch3 * csum(*P.parent, clo, chi);
+      }
+    }
+  }
+  integral[0] = r1;
+  integral[1] = r2;
+  return 0;
+}
+
 int orc_run_hier(const orc_params* p, int npatch, const orc_patch* patches, const double* q0,
                  int nsteps, double* q_out, int* nvcycles, double* resid_final) {
   Ctx c;

@@ -93,6 +93,9 @@ int orc_hier_restrict_level(orc_hier* h, int level);
 int orc_hier_fill_down(orc_hier* h);
 int orc_hier_copy_q_to_qold(orc_hier* h);
 int orc_hier_multigrid(orc_hier* h, int* nvcycles, double* residual);
+/* AfterStepStatistics over the held hierarchy: integral[0] the composite
+ * mass, integral[1] the composite Energy2D (0 in 3D). */
+int orc_hier_after_step(orc_hier* h, double* integral);
 
 /* Interpolate2D (boundary.f90:135-323) on a fine patch qf (0:mx+1)^2 x nv
  * from its parent qc (0:pmx+1)^2 x nv; mbounds = {mb11, mb12, mb21, mb22}. */

@@ -86,6 +86,7 @@ def lib():
         for name in ("orc_hier_fill_down", "orc_hier_copy_q_to_qold"):
             getattr(L, name).argtypes = [ctypes.c_void_p]
         L.orc_hier_multigrid.argtypes = [ctypes.c_void_p, ip, dp]
+        L.orc_hier_after_step.argtypes = [ctypes.c_void_p, dp]
         _lib = L
     return _lib
 
@@ -433,6 +434,11 @@ class OracleBackend:
         self._rc(lib().orc_hier_multigrid(self.h, _ip(nv), _dp(res)), "multigrid")
         return int(nv[0]), float(res[0])
 
+    def after_step_stats(self):
+        out = np.zeros(2)
+        self._rc(lib().orc_hier_after_step(self.h, _dp(out)), "after_step")
+        return float(out[0]), float(out[1])
+
     def errflags(self, i, tol):
         q = self.get_q(i)
         return errflags(q[..., 0], tol).astype(np.uint8)
@@ -456,3 +462,58 @@ class OracleBackend:
         if self.h is not None:
             lib().orc_hier_destroy(self.h)
             self.h = None
+
+
+# ---- frame output ---------------------------------------------------------------
+
+def _f(x, w, d):
+    """Fortran Fw.d output."""
+    return "%*.*f" % (w, d, x)
+
+
+def _es(x, w, d):
+    """Fortran ESw.d output: d.ddd...E+nn, a three-digit exponent without
+    the E."""
+    if x == 0.0:
+        m, e = ("-" if np.signbit(x) else "") + "0." + "0" * d, 0
+    else:
+        t = "%.*e" % (d, x)
+        mant, ex = t.split("e")
+        m, e = mant, int(ex)
+    es = ("E%+03d" % e) if abs(e) < 100 else ("%+04d" % e)
+    s = m + es
+    return " " * max(0, w - len(s)) + s
+
+
+def format_frame(nd, time, descs, qs):
+    """WriteQ (lib/bsaminputoutput.f90:51-76) with OutputQ (78-131) and
+    WriteQ2D/3D (133-172): the text of a frame file.  descs: the patch table;
+    qs: patch index -> q with ring (levels >= 0).  xupper as MakeNewGrid sets
+    it (mbounds(:,2) * parent dx + parent xlower), xlower + mx dx on the
+    root."""
+    finest = max(d["level"] for d in descs)
+    out = [_f(time, 25, 12), "%3d" % finest]
+    for level in range(0, finest + 1):
+        for i, d in enumerate(descs):
+            if d["level"] != level:
+                continue
+            out.append("  ")
+            out.append("%3d %3d %3d %3d" % (level, nd, 2, 2))
+            if level == 0:
+                xu = [d["xlower"][k] + d["mx"][k] * d["dx"] for k in range(nd)]
+            else:
+                p = descs[d["parent"]]
+                xu = [float(d["mbounds"][k][1]) * p["dx"] + p["xlower"][k] for k in range(nd)]
+            out.append(" ".join(_f(d["dx"], 25, 12) for _ in range(nd)))
+            out.append(" ".join(_f(d["xlower"][k], 25, 12) for k in range(nd)))
+            out.append(" ".join(_f(xu[k], 25, 12) for k in range(nd)))
+            out.append(" ".join("%8d" % d["mx"][k] for k in range(nd)))
+            out.append(" ".join("%8d" % d["mglobal"][k][s] for k in range(nd) for s in range(2)))
+            q = np.asarray(qs[i])
+            flat = q.reshape(-1, 2, order="F")
+            for c in range(flat.shape[0]):
+                if nd == 2:
+                    out.append("  ".join(_es(v, 20, 12) for v in flat[c]))
+                else:
+                    out.append("  ".join(_f(v, 25, 12) for v in flat[c]))
+    return "\n".join(out) + "\n"

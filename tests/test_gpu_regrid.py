@@ -70,7 +70,8 @@ def test_regrid_run_matches_oracle(gpu_lib, oracle, nd):
     buffering, Berger-Rigoutsos, new-patch prolongation, value transfer, the
     level-by-level ghosts and restrictions of AMR(rootlevel), FillDown,
     MultigridIterations), engine against oracle: the same grids every step,
-    the same V-cycle counts, q within 1e-11."""
+    the same V-cycle counts, q within 1e-11, and the same after-step
+    statistics (composite mass and energy)."""
     n, eps, prm = REGRID_CASES[nd]
     hier = amr.build(n, [], eps=eps, dt=5e-5, qerrortol=1e-9, field="drop", ndims=nd)
     g = amr.GpuBackend(nd, hier.dt, hier.eps, hier.qerrortol)
@@ -85,6 +86,11 @@ def test_regrid_run_matches_oracle(gpu_lib, oracle, nd):
             assert nvg == nvo
             assert resg == pytest.approx(reso, rel=1e-6, abs=1e-15)
             assert max(d["level"] for d in rg.descs) == 2
+            # AfterStepStatistics: composite mass and (2D) energy.
+            mg, eg = rg.stats()
+            mo, eo = ro.stats()
+            assert mg == pytest.approx(mo, rel=1e-12)
+            assert eg == pytest.approx(eo, rel=1e-12, abs=0 if nd == 2 else 1e-300)
             for (i, qg), (_, qo) in zip(rg.state(), ro.state()):
                 d = rg.descs[i]
                 inner = tuple(slice(1, m + 1) for m in d["mx"][:nd])
@@ -92,3 +98,23 @@ def test_regrid_run_matches_oracle(gpu_lib, oracle, nd):
     finally:
         g.close()
         o.close()
+
+
+@pytest.mark.parametrize("nd", [2, 3])
+def test_write_frame_from_device(gpu_lib, oracle, nd, tmp_path):
+    """bsam_host_write_frame (q read back from the device, then WriteQ's
+    format) against the oracle's WriteQ text of the same state, after a
+    regridding step."""
+    n, eps, prm = REGRID_CASES[nd]
+    hier = amr.build(n, [], eps=eps, dt=5e-5, qerrortol=1e-9, field="drop", ndims=nd)
+    g = amr.GpuBackend(nd, hier.dt, hier.eps, hier.qerrortol)
+    try:
+        run = amr.RegridRun(g, hier, prm)
+        run.step()
+        path = str(tmp_path / "m00001.dat")
+        g.write_frame(path, 5e-5)
+        qs = dict(run.state())
+        with open(path) as f:
+            assert f.read() == oracle.format_frame(nd, 5e-5, run.descs, qs)
+    finally:
+        g.close()

@@ -123,3 +123,38 @@ def test_regrid_run_on_oracle(oracle):
                                                (p["mglobal"][k][0] + hi - 1) * 2]
     finally:
         b.close()
+
+
+def test_after_step_stats_oracle(oracle):
+    """The oracle's AfterStepStatistics: on the root alone it is h^2 sum(c)
+    and Energy2D; a refined patch holding its parent's values cell by cell
+    (piecewise constant) adds no mass."""
+    hier = amr.build(16, [(1, (9, 9), (8, 6))], eps=0.05, dt=5e-5, field="drop")
+    b = oracle.OracleBackend(2, hier.dt, hier.eps, hier.qerrortol)
+    try:
+        b.set_hierarchy(hier.descs)
+        for p, q in zip(hier.state_patches(), hier.q0s):
+            b.put_q(p, q)
+        b.set_ghost_level(0)
+        root = [i for i, d in enumerate(hier.descs) if d["level"] == 0][0]
+        fine = [i for i, d in enumerate(hier.descs) if d["level"] == 1][0]
+        qr = b.get_q(root)
+        d = hier.descs[fine]
+        sl = tuple(slice(d["mbounds"][k][0], d["mbounds"][k][1] + 1) for k in range(2))
+        qf = np.zeros_like(b.get_q(fine))
+        qf[1:-1, 1:-1, :] = np.kron(qr[sl + (slice(None),)].transpose(2, 0, 1),
+                                    np.ones((2, 2))).transpose(1, 2, 0)
+        b.put_q(fine, qf)
+        b.set_ghost_level(1)
+        m, e = b.after_step_stats()
+        h = hier.descs[root]["dx"]
+        assert m == pytest.approx(h * h * qr[1:-1, 1:-1, 0].sum(), rel=1e-13)
+        # Energy: finest level first, Energy2D(fine, h/2) - Energy2D(parent
+        # footprint with its ring, h), then the root's Energy2D.
+        e_root = oracle.energy2d(h, 1.0, hier.eps, qr[..., 0])
+        e_fine = oracle.energy2d(h / 2, 1.0, hier.eps, b.get_q(fine)[..., 0])
+        ring = tuple(slice(d["mbounds"][k][0] - 1, d["mbounds"][k][1] + 2) for k in range(2))
+        e_foot = oracle.energy2d(h, 1.0, hier.eps, qr[ring + (0,)])
+        assert e == pytest.approx((e_fine - e_foot) + e_root, rel=1e-13)
+    finally:
+        b.close()

@@ -171,9 +171,24 @@ def cpu_baseline(sample: int = 12, nsteps: int = 2):
         s, t = _oracle_solve((i, nsteps, 4))
         steps += s
         secs += t
-    return {"value": steps / secs, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"first {sample} of the 512 problems, {nsteps} time steps each, one "
-                      "thread (C++ restatement of the reference Fortran path)"}
+    out = {"value": steps / secs, "unit": UNIT, "cores": 1, "kind": "port",
+           "sample": f"first {sample} of the 512 problems, {nsteps} time steps each, one "
+                     "thread (C++ restatement of the reference Fortran path)"}
+    # The AMR configuration with sustained refinement: the oracle through the
+    # same regrid driver, two steps after one warm-up step, one thread.
+    from bsam_b200 import amr as AMR
+    hier, prm = AMR.config2(sustained=True)
+    b = pyoracle.OracleBackend(2, hier.dt, hier.eps, hier.qerrortol)
+    try:
+        run = AMR.RegridRun(b, hier, prm)
+        run.step()
+        t0 = time.perf_counter()
+        for _ in range(2):
+            run.step()
+        out["cfg2_amr_sustained_steps_per_s"] = 2 / (time.perf_counter() - t0)
+    finally:
+        b.close()
+    return out
 
 
 def run_reference(args, world, rank):
@@ -406,6 +421,28 @@ def run_ours(args, world, rank, local):
                 t0 = time.perf_counter()
                 sv.run(5, keep_steps=False)
                 extra[f"cfg3_128cubed_{name}_steps_per_s"] = 5 / (time.perf_counter() - t0)
+        # 2D AMR (config 2): 256^2 root + two refined levels, regridded every
+        # step in the native driver (bsam_amr_step), FP64; host wall clock.
+        from bsam_b200 import amr as AMR
+        for tag, sustained, nst in (("as_configured", False, 49), ("sustained", True, 20)):
+            hier, prm = AMR.config2(sustained=sustained)
+            with AMR.AmrRun(hier, prm, device=local) as r:
+                r.step()
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                nv, pats, refined = [], [], []
+                for _ in range(nst):
+                    nv.append(r.step()[0])
+                    pats.append(sum(1 for d in r.descs if d["level"] >= 1))
+                    refined.append(sum(d["mx"][0] * d["mx"][1] for d in r.descs
+                                       if d["level"] >= 1))
+                dt_ = time.perf_counter() - t0
+            extra[f"cfg2_amr_{tag}"] = {
+                "steps_per_s": nst / dt_, "steps": nst, "vcycles_mean": statistics.mean(nv),
+                "refined_patches_mean": statistics.mean(pats),
+                "refined_cells_mean": statistics.mean(refined),
+                "steps_with_refinement": sum(1 for x in pats if x > 0),
+                "tag_threshold": "|grad phi| > %.2f/eps" % (0.25 if sustained else 0.5)}
         # Served form: one rate point of the Poisson request stream.
         stream_ = W.config5(120, 200.0)
         with SV.Server(pool_bytes=32 << 30, max_slots=256, ticks=4) as srv:

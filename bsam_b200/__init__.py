@@ -67,7 +67,9 @@ ABI_SYMBOLS = (
     "bsam_gpu_errflags", "bsam_gpu_init_patch", "bsam_host_new_subgrids",
     "bsam_gpu_restrict_level", "bsam_host_buffer_flags", "bsam_host_child_desc",
     "bsam_host_format_frame", "bsam_host_write_frame",
-    "bsam_gpu_set_ghost_level", "bsam_gpu_after_step_stats",
+    "bsam_gpu_set_ghost_level", "bsam_gpu_after_step_stats", "bsam_gpu_stash", "bsam_gpu_regrid",
+    "bsam_gpu_errflags_level", "bsam_amr_create", "bsam_amr_step", "bsam_amr_table",
+    "bsam_amr_destroy",
     "bsam_batch_create", "bsam_batch_destroy", "bsam_batch_set_tuning", "bsam_batch_footprint",
     "bsam_batch_submit", "bsam_batch_advance", "bsam_batch_sync", "bsam_batch_run",
     "bsam_batch_poll", "bsam_batch_slot_phase", "bsam_batch_collect", "bsam_batch_get_stream", "bsam_batch_profile", "bsam_batch_submit_seeded", "bsam_batch_busy",
@@ -79,6 +81,17 @@ class Tuning(ctypes.Structure):
     _fields_ = [("fuse_smoother", ctypes.c_int32), ("fuse_min_n", ctypes.c_int32),
                 ("chunk", ctypes.c_int32), ("bottom_cells", ctypes.c_int32),
                 ("graph", ctypes.c_int32), ("reserved", ctypes.c_int32 * 3)]
+
+
+AMR_MAXLEVEL = 8
+
+
+class RegridParamsC(ctypes.Structure):
+    """bsam_regrid_params (include/bsam_host.h)."""
+    _fields_ = [("maxlevel", ctypes.c_int32), ("ibuffer", ctypes.c_int32 * AMR_MAXLEVEL),
+                ("minimumgridpoints", ctypes.c_int32 * AMR_MAXLEVEL), ("pad_", ctypes.c_int32),
+                ("qtolerance", ctypes.c_double * AMR_MAXLEVEL),
+                ("desiredfillratios", ctypes.c_double * AMR_MAXLEVEL)]
 
 
 class Stats(ctypes.Structure):
@@ -112,6 +125,18 @@ def lib():
     L.bsam_gpu_restrict_level.argtypes = [vp, ctypes.c_int]
     L.bsam_gpu_set_ghost_level.argtypes = [vp, ctypes.c_int]
     L.bsam_gpu_after_step_stats.argtypes = [vp, dp]
+    L.bsam_gpu_stash.argtypes = [vp]
+    L.bsam_gpu_errflags_level.argtypes = [vp, ctypes.c_int, ctypes.c_double,
+                                          ctypes.POINTER(ctypes.c_uint8)]
+    L.bsam_amr_create.argtypes = [ctypes.POINTER(vp), vp, ctypes.c_int,
+                                  ctypes.POINTER(RegridParamsC), ctypes.c_int,
+                                  ctypes.POINTER(PatchDesc)]
+    L.bsam_amr_step.argtypes = [vp, ip, dp, ip]
+    L.bsam_amr_table.argtypes = [vp, ctypes.POINTER(PatchDesc), ctypes.c_int]
+    L.bsam_amr_destroy.argtypes = [vp]
+    L.bsam_amr_destroy.restype = None
+    L.bsam_gpu_regrid.argtypes = [vp, ctypes.c_int, ctypes.POINTER(PatchDesc), ctypes.c_int, ip,
+                                  ctypes.c_int, ip]
     L.bsam_host_buffer_flags.argtypes = [ctypes.c_int, ctypes.c_int, ip, ip,
                                          ctypes.POINTER(ctypes.c_uint8), ctypes.c_int]
     L.bsam_host_child_desc.argtypes = [ctypes.c_int, ctypes.POINTER(PatchDesc), ctypes.c_int,

@@ -292,6 +292,14 @@ def desc_array(descs):
     return arr
 
 
+def desc_dict(o) -> dict:
+    """A bsam_patch_desc record as the dict the builders use."""
+    return {"level": o.level, "parent": o.parent, "mx": list(o.mx),
+            "mbounds": [list(o.mbounds[k]) for k in range(3)],
+            "mglobal": [list(o.mglobal[k]) for k in range(3)], "mthbc": list(o.mthbc),
+            "dx": o.dx, "xlower": list(o.xlower)}
+
+
 def format_frame(path: str, nd: int, time: float, descs: list, qs: dict):
     """WriteQ's frame file from host arrays (bsam_host_format_frame): qs maps
     the index of every patch on a level >= 0 to its q with ring."""
@@ -354,6 +362,24 @@ class GpuBackend:
         self.descs = list(descs)
         self._call("set_hierarchy", lib().bsam_gpu_set_hierarchy(
             self.h, len(descs), desc_array(descs), max(d["level"] for d in descs)))
+
+    def stash(self):
+        from . import lib
+        self._call("stash", lib().bsam_gpu_stash(self.h))
+
+    def regrid(self, descs, carry, transfers):
+        """The new patch table filled on the device: carried patches keep
+        their state, new ones take InitFields' prolongation, then the
+        stashed old grids' overlaps (bsam_gpu_regrid)."""
+        import ctypes
+        from . import lib
+        self.descs = list(descs)
+        cv = np.array(carry, dtype=np.int32)
+        tv = np.array([x for pair in transfers for x in pair] or [0], dtype=np.int32)
+        ip = ctypes.POINTER(ctypes.c_int)
+        self._call("regrid", lib().bsam_gpu_regrid(
+            self.h, len(descs), desc_array(descs), max(d["level"] for d in descs),
+            cv.ctypes.data_as(ip), len(transfers), tv.ctypes.data_as(ip)))
 
     def write_frame(self, path, time):
         """WriteQ from the device (bsam_host_write_frame)."""
@@ -519,24 +545,15 @@ class RegridRun:
     def levels(self):
         return sorted({d["level"] for d in self.descs})
 
-    def _rebuild(self, descs, keep_q):
-        """Re-set the backend's hierarchy to `descs`; put back q of the
-        patches in keep_q (new index -> q)."""
-        self.b.set_hierarchy(descs)
-        for i, q in keep_q.items():
-            self.b.put_q(i, q)
-
     def step(self):
         """One time step: AMR(rootlevel), FillDown on the first step,
         CopyQToQold, MultigridIterations.  Returns (V-cycles, residual)."""
         b, nd, prm = self.b, self.nd, self.prm
-        descs = self.descs
-        # The old grids of each refined level: TransferValues' sources.  Their
-        # interiors do not change before GridAdapt reaches their level.
-        old = {}
-        for i, d in enumerate(descs):
-            if d["level"] >= 1:
-                old.setdefault(d["level"], []).append((d, b.get_q(i)))
+        start = self.descs
+        descs = start
+        # The old grids of the refined levels as TransferValues reads them:
+        # their interiors do not change before GridAdapt reaches their level.
+        b.stash()
         b.set_ghost_level(0)  # AMR(rootlevel)
         # EstimateLevelErrors(0)'s RestrictSolution of the root into the level
         # below and that level's SetGhost are left out: the V-cycle restricts
@@ -557,7 +574,6 @@ class RegridRun:
             # youngest first; deeper levels lose their grids.
             keep = [i for i, d in enumerate(descs) if d["level"] <= L]
             index = {o: n for n, o in enumerate(keep)}
-            keep_q = {index[i]: b.get_q(i) for i in keep if descs[i]["level"] >= 0}
             new_descs = []
             for i in keep:
                 d = dict(descs[i])
@@ -567,7 +583,18 @@ class RegridRun:
                 c = dict(c)
                 c["parent"] = index[c["parent"]]
                 new_descs.append(c)
-            self._rebuild(new_descs, keep_q)
+            carry = list(keep) + [-1] * len(made)
+            # TransferValues: each new grid with each old grid of its level.
+            transfers = []
+            for c in range(len(keep), len(new_descs)):
+                dc = new_descs[c]
+                for o, do in enumerate(start):
+                    if do["level"] != L + 1:
+                        continue
+                    if all(max(dc["mglobal"][k][0], do["mglobal"][k][0])
+                           <= min(dc["mglobal"][k][1], do["mglobal"][k][1]) for k in range(nd)):
+                        transfers.append((c, o))
+            b.regrid(new_descs, carry, transfers)
             descs = new_descs
             if not made:
                 # AMR(L + 1) on an empty level: EstimateLevelErrors(L + 1)
@@ -575,26 +602,6 @@ class RegridRun:
                 if L + 1 < prm.maxlevel:
                     b.set_ghost_level(L)
                 break
-            children = list(range(len(keep), len(new_descs)))
-            for c in children:
-                b.init_patch(c)  # MakeNewGrid -> InitFields
-            for c in children:  # TransferValues from the level's old grids
-                dc = descs[c]
-                qc = None
-                for do, qo in old.get(L + 1, []):
-                    lo = [max(dc["mglobal"][k][0], do["mglobal"][k][0]) for k in range(nd)]
-                    hi = [min(dc["mglobal"][k][1], do["mglobal"][k][1]) for k in range(nd)]
-                    if any(hi[k] < lo[k] for k in range(nd)):
-                        continue
-                    if qc is None:
-                        qc = b.get_q(c)
-                    ts = tuple(slice(lo[k] - dc["mglobal"][k][0] + 1,
-                                     hi[k] - dc["mglobal"][k][0] + 2) for k in range(nd))
-                    ss = tuple(slice(lo[k] - do["mglobal"][k][0] + 1,
-                                     hi[k] - do["mglobal"][k][0] + 2) for k in range(nd))
-                    qc[ts] = qo[ss]
-                if qc is not None:
-                    b.put_q(c, qc)
             b.set_ghost_level(L + 1)  # AMR(L + 1)
         self.descs = descs
         if self.firstamr:
@@ -611,3 +618,97 @@ class RegridRun:
     def state(self):
         """q of every patch on a level >= 0 (descs order)."""
         return [(i, self.b.get_q(i)) for i, d in enumerate(self.descs) if d["level"] >= 0]
+
+
+class AmrRun:
+    """Time steps with regridding every step in the native host library
+    (bsam_amr_*): the same sequence as RegridRun, without Python in the loop.
+    The hierarchy starts from `hier` as given, on device `device`."""
+
+    def __init__(self, hier: Hierarchy, params: RegridParams, device: int = 0):
+        import ctypes
+        from . import AMR_MAXLEVEL, RegridParamsC, _check, lib
+        if params.maxlevel > AMR_MAXLEVEL:
+            raise ValueError("maxlevel above the native limit")
+        self.nd = hier.ndims
+        self.b = GpuBackend(hier.ndims, hier.dt, hier.eps, hier.qerrortol, hier.alpha,
+                            hier.maxvcycles, hier.nsmoothingpasses, device)
+        self.a = ctypes.c_void_p()
+        try:
+            self.b.set_hierarchy(hier.descs)
+            for p, q in zip(hier.state_patches(), hier.q0s):
+                self.b.put_q(p, q)
+            rp = RegridParamsC()
+            rp.maxlevel = params.maxlevel
+            for L in range(params.maxlevel):
+                rp.ibuffer[L] = params.ibuffer[L]
+                rp.minimumgridpoints[L] = params.mgp[L]
+                rp.qtolerance[L] = params.qtolerance[L]
+                rp.desiredfillratios[L] = params.desfill[L]
+            _check(lib().bsam_amr_create(ctypes.byref(self.a), self.b.h, self.nd, ctypes.byref(rp),
+                                         len(hier.descs), desc_array(hier.descs)),
+                   self.b.h, "amr_create")
+        except Exception:
+            self.close()
+            raise
+        self.descs = list(hier.descs)
+
+    def step(self):
+        """One time step (bsam_amr_step): (V-cycles, residual)."""
+        import ctypes
+        from . import PatchDesc, _check, lib
+        nv, conv = ctypes.c_int(0), ctypes.c_int(0)
+        res = ctypes.c_double(0.0)
+        _check(lib().bsam_amr_step(self.a, ctypes.byref(nv), ctypes.byref(res),
+                                   ctypes.byref(conv)), self.b.h, "amr_step")
+        n = lib().bsam_amr_table(self.a, None, 0)
+        arr = (PatchDesc * n)()
+        lib().bsam_amr_table(self.a, arr, n)
+        self.descs = [desc_dict(arr[i]) for i in range(n)]
+        self.b.descs = list(self.descs)
+        return nv.value, res.value
+
+    def stats(self):
+        return self.b.after_step_stats()
+
+    def state(self):
+        """q of every patch on a level >= 0 (table order)."""
+        return [(i, self.b.get_q(i)) for i, d in enumerate(self.descs) if d["level"] >= 0]
+
+    def write_frame(self, path, time):
+        self.b.write_frame(path, time)
+
+    def close(self):
+        from . import lib
+        if getattr(self, "a", None) is not None and self.a.value:
+            lib().bsam_amr_destroy(self.a)
+            self.a = None
+        if getattr(self, "b", None) is not None:
+            self.b.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def config2(sustained: bool = False, seed: int = 2):
+    """The 2D AMR workload: a 256^2 root on [0,1]^2 with two refined levels,
+    eps = 0.005, dt = 5e-5, residual 1e-9, the circular drop
+    phi0 = tanh((0.25 - r)/(sqrt(2) eps)) + 1e-3 U(-1, 1), regridded every
+    step: ibuffer 1, desiredfillratios 0.9, minimumgridpoints 8, and the tag
+    threshold |grad phi| > 0.5/eps on the undivided central gradient of c
+    (qtolerance = 0.5 h / eps per level).
+
+    With c = (1 + phi)/2 and the reference's potential (alpha = 1) the
+    equilibrium interface is twice as wide as the initial one
+    (max |grad phi| = 1/(2 sqrt(2) eps), about 0.35/eps), so the refined
+    levels disappear once the initial profile has relaxed (two steps).
+    sustained=True halves the threshold (0.25/eps), which keeps about 40
+    level-1 and 100 level-2 grids on the interface every step."""
+    hier = build(256, [], eps=0.005, dt=5e-5, qerrortol=1e-9, field="drop", seed=seed)
+    k = 0.25 if sustained else 0.5
+    tol = [k * (1.0 / 256) / 0.005, k * (1.0 / 512) / 0.005]
+    return hier, RegridParams(maxlevel=2, qtolerance=tol, ibuffer=[1, 1], desfill=[0.9, 0.9],
+                              mgp=[8, 8])

@@ -82,6 +82,24 @@ struct bsam_gpu {
   DevPatch* d_patches = nullptr;
   char* d_arena = nullptr;
   size_t arena_bytes = 0;
+  // The stash: copies of the q of every refined patch, taken by
+  // bsam_gpu_stash (old grids as TransferValues reads them), with records
+  // whose q pointers point into it.
+  char* d_stash = nullptr;
+  size_t stash_cap = 0;
+  // The arena a regrid released, kept for the next hierarchy of no larger
+  // size (regridding every step alternates between two arenas).
+  char* spare_arena = nullptr;
+  size_t spare_bytes = 0;
+  uint8_t* d_flags = nullptr;  // bsam_gpu_errflags_level's device flags
+  CopySpan* d_qold_spans = nullptr;  // CopyQToQold: q -> qold of every patch that has qold
+  int nqold_spans = 0;
+  int64_t qold_span_max = 0;
+  CopySpan* d_stash_spans = nullptr;
+  size_t stash_spans_cap = 0;
+  size_t flags_cap = 0;
+  std::vector<DevPatch> stash_hp;
+  std::vector<bsam_patch_desc> stash_desc;
   std::vector<LevelPlan> levels;     // index level - minlevel
   std::vector<int> masters;          // finest-level state patches
   Item* d_master = nullptr;          // tiles over the masters
@@ -133,7 +151,8 @@ int fail(bsam_gpu* h, int code, const std::string& msg) {
   do {                                                                            \
     cudaError_t e_ = (call);                                                      \
     if (e_ != cudaSuccess)                                                        \
-      return fail(h, BSAM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+      return fail(h, BSAM_ERR_CUDA, std::string(__func__) + ":" + std::to_string(__LINE__) + \
+                                        ": " #call ": " + cudaGetErrorString(e_));         \
   } while (0)
 
 int64_t roundup(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
@@ -566,17 +585,17 @@ static void free_hierarchy(bsam_gpu* h) {
   h->d_tmaps = nullptr;
   if (h->d_tops) cudaFree(h->d_tops);
   if (h->step_exec) cudaGraphExecDestroy(h->step_exec);
-  if (h->d_trace) cudaFree(h->d_trace);
-  if (h->h_trace) cudaFreeHost(h->h_trace);
   if (h->d_arena) cudaFree(h->d_arena);
   if (h->d_patches) cudaFree(h->d_patches);
   if (h->d_partials) cudaFree(h->d_partials);
+  if (h->d_qold_spans) cudaFree(h->d_qold_spans);
+  h->d_qold_spans = nullptr;
+  h->nqold_spans = 0;
+  h->qold_span_max = 0;
   h->d_items = nullptr;
   h->d_tops = nullptr;
   h->ntops = 0;
   h->step_exec = nullptr;
-  h->d_trace = nullptr;
-  h->h_trace = nullptr;
   h->d_arena = nullptr;
   h->d_patches = nullptr;
   h->d_partials = nullptr;
@@ -777,8 +796,14 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
     want_qold[r] = has_qold;
     want_qs[r] = parent_of_any;
   }
-  if (cudaMalloc(&h->d_arena, total) != cudaSuccess)
+  if (h->spare_arena && h->spare_bytes >= total) {
+    h->d_arena = h->spare_arena;
+    total = h->spare_bytes;
+    h->spare_arena = nullptr;
+    h->spare_bytes = 0;
+  } else if (cudaMalloc(&h->d_arena, total) != cudaSuccess) {
     return fail(h, BSAM_ERR_NOMEM, "arena allocation failed");
+  }
   h->arena_bytes = total;
   CU(cudaMemsetAsync(h->d_arena, 0, total, h->stream));
   for (int r = 0; r < nrec; ++r) {
@@ -808,6 +833,25 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
       P.qb[1] = next();
     }
     P.bs = P.delta ? next() : nullptr;
+  }
+  // CopyQToQold as one launch: the whole field allocation of q onto qold's.
+  {
+    std::vector<CopySpan> spans;
+    for (int r = 0; r < npatch; ++r) {
+      const DevPatch& P = h->hp[r];
+      if (!P.qo[0]) continue;
+      const int64_t lead = 128 / sizeof(double) - 1;
+      for (int c = 0; c < 2; ++c)
+        spans.push_back(CopySpan{static_cast<const double*>(P.q[c]) - lead,
+                                 static_cast<double*>(P.qo[c]) - lead, h->field_elems[r]});
+      h->qold_span_max = std::max(h->qold_span_max, h->field_elems[r]);
+    }
+    h->nqold_spans = (int)spans.size();
+    if (!spans.empty()) {
+      CU(cudaMalloc(&h->d_qold_spans, sizeof(CopySpan) * spans.size()));
+      CU(cudaMemcpyAsync(h->d_qold_spans, spans.data(), sizeof(CopySpan) * spans.size(),
+                         cudaMemcpyHostToDevice, h->stream));
+    }
   }
   // Parents of the twins are the masters' parents.
   for (int r = npatch; r < nrec; ++r) h->hp[r].parent = h->hp[rec_src[r]].parent;
@@ -985,8 +1029,10 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
   CU(cudaFuncSetAttribute(k_smooth3_fused<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)Fused3<float>::SMEM));
   CU(cudaMalloc(&h->d_partials, sizeof(double) * h->max_items));
-  CU(cudaMalloc(&h->d_trace, sizeof(double) * h->rp.maxvcycles));
-  CU(cudaMallocHost(&h->h_trace, sizeof(double) * h->rp.maxvcycles));
+  // The residual trace buffers live as long as the handle (maxvcycles is
+  // fixed at creation).
+  if (!h->d_trace) CU(cudaMalloc(&h->d_trace, sizeof(double) * h->rp.maxvcycles));
+  if (!h->h_trace) CU(cudaMallocHost(&h->h_trace, sizeof(double) * h->rp.maxvcycles));
   {
     int64_t ncells = 0;
     for (int p : h->masters) ncells += cells_of(h->hp[p].n, nd);
@@ -1134,14 +1180,12 @@ int bsam_gpu_restrict_level(bsam_gpu* h, int level) {
 int bsam_gpu_copy_q_to_qold(bsam_gpu* h) {
   if (!h || !h->have_hierarchy) return BSAM_ERR_STATE;
   CU(cudaSetDevice(h->device));
-  for (int p = 0; p < h->nuser; ++p) {
-    const DevPatch& P = h->hp[p];
-    if (!P.qo[0]) continue;  // qold is read only on levels >= root (Source)
-    const int64_t lead = 128 / sizeof(double) - 1;
-    for (int c = 0; c < 2; ++c)
-      CU(cudaMemcpyAsync(static_cast<double*>(P.qo[c]) - lead, static_cast<double*>(P.q[c]) - lead,
-                         h->field_elems[p] * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
-  }
+  // qold exists on levels >= root only (Source reads it there).
+  if (h->nqold_spans == 0) return BSAM_OK;
+  const int bx = (int)std::min<int64_t>((h->qold_span_max + 255) / 256, 64);
+  k_copy_spans<<<dim3(bx, h->nqold_spans), 256, 0, h->stream>>>(h->d_qold_spans);
+  ++h->stats.launches;
+  CU(cudaGetLastError());
   return BSAM_OK;
 }
 
@@ -1276,6 +1320,40 @@ int bsam_gpu_errflags(bsam_gpu* h, int patch, double tol, uint8_t* flags) {
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
   cudaFree(d_flags);
   if (e != cudaSuccess) return fail(h, BSAM_ERR_CUDA, cudaGetErrorString(e));
+  return BSAM_OK;
+}
+
+int bsam_gpu_errflags_level(bsam_gpu* h, int level, double tol, uint8_t* flags) {
+  if (!h || !h->have_hierarchy || !flags) return BSAM_ERR_ARG;
+  if (level < 0 || level > h->finestlevel)
+    return fail(h, BSAM_ERR_ARG, "errflags_level needs a level >= 0");
+  CU(cudaSetDevice(h->device));
+  const int nd = h->rp.ndims;
+  size_t total = 0;
+  for (int p = 0; p < h->nuser; ++p)
+    if (h->desc[p].level == level) total += (size_t)cells_of(h->hp[p].n, nd);
+  if (total == 0) return BSAM_OK;
+  if (total > h->flags_cap) {
+    if (h->d_flags) cudaFree(h->d_flags);
+    h->d_flags = nullptr;
+    h->flags_cap = 0;
+    if (cudaMalloc(&h->d_flags, total) != cudaSuccess)
+      return fail(h, BSAM_ERR_NOMEM, "flag buffer allocation failed");
+    h->flags_cap = total;
+  }
+  size_t off = 0;
+  for (int p = 0; p < h->nuser; ++p) {
+    if (h->desc[p].level != level) continue;
+    const size_t ncell = (size_t)cells_of(h->hp[p].n, nd);
+    const int blocks = (int)std::min<size_t>((ncell + 255) / 256, 4096);
+    if (nd == 2) k_errflags<2><<<blocks, 256, 0, h->stream>>>(h->d_patches, p, tol, h->d_flags + off);
+    else k_errflags<3><<<blocks, 256, 0, h->stream>>>(h->d_patches, p, tol, h->d_flags + off);
+    ++h->stats.launches;
+    off += ncell;
+  }
+  CU(cudaGetLastError());
+  CU(cudaMemcpyAsync(flags, h->d_flags, total, cudaMemcpyDeviceToHost, h->stream));
+  CU(cudaStreamSynchronize(h->stream));
   return BSAM_OK;
 }
 
@@ -1458,6 +1536,176 @@ int bsam_gpu_after_step_stats(bsam_gpu* h, double* integral) {
   return BSAM_OK;
 }
 
+int bsam_gpu_stash(bsam_gpu* h) {
+  if (!h || !h->have_hierarchy) return BSAM_ERR_STATE;
+  if (h->mixed) return fail(h, BSAM_ERR_UNSUPPORTED, "regridding: FP64 form only");
+  CU(cudaSetDevice(h->device));
+  h->stash_hp.assign(h->nuser, DevPatch{});
+  h->stash_desc = h->desc;
+  size_t total = 0;
+  std::vector<size_t> off(h->nuser, 0);
+  for (int p = 0; p < h->nuser; ++p)
+    if (h->desc[p].level >= 1) {
+      off[p] = total;
+      total += 2 * (size_t)h->field_elems[p] * sizeof(double);
+    }
+  if (total == 0) return BSAM_OK;
+  if (total > h->stash_cap) {
+    if (h->d_stash) cudaFree(h->d_stash);
+    h->d_stash = nullptr;
+    h->stash_cap = 0;
+    if (cudaMalloc(&h->d_stash, total) != cudaSuccess)
+      return fail(h, BSAM_ERR_NOMEM, "stash allocation failed");
+    h->stash_cap = total;
+  }
+  const int64_t lead = 128 / sizeof(double) - 1;
+  std::vector<CopySpan> spans;
+  int64_t span_max = 0;
+  for (int p = 0; p < h->nuser; ++p) {
+    if (h->desc[p].level < 1) continue;
+    DevPatch S = h->hp[p];
+    for (int c = 0; c < 2; ++c) {
+      double* dst = reinterpret_cast<double*>(h->d_stash + off[p]) + c * h->field_elems[p];
+      spans.push_back(CopySpan{static_cast<const double*>(S.q[c]) - lead, dst, h->field_elems[p]});
+      S.q[c] = dst + lead;
+    }
+    span_max = std::max(span_max, h->field_elems[p]);
+    h->stash_hp[p] = S;
+  }
+  if (spans.size() > h->stash_spans_cap) {
+    if (h->d_stash_spans) cudaFree(h->d_stash_spans);
+    h->d_stash_spans = nullptr;
+    h->stash_spans_cap = 0;
+    if (cudaMalloc(&h->d_stash_spans, sizeof(CopySpan) * spans.size()) != cudaSuccess)
+      return fail(h, BSAM_ERR_NOMEM, "stash allocation failed");
+    h->stash_spans_cap = spans.size();
+  }
+  CU(cudaMemcpyAsync(h->d_stash_spans, spans.data(), sizeof(CopySpan) * spans.size(),
+                     cudaMemcpyHostToDevice, h->stream));
+  const int bx = (int)std::min<int64_t>((span_max + 255) / 256, 64);
+  k_copy_spans<<<dim3(bx, (unsigned)spans.size()), 256, 0, h->stream>>>(h->d_stash_spans);
+  ++h->stats.launches;
+  CU(cudaGetLastError());
+  // The span list is host memory: wait until it has been read.
+  CU(cudaStreamSynchronize(h->stream));
+  return BSAM_OK;
+}
+
+int bsam_gpu_regrid(bsam_gpu* h, int npatch, const bsam_patch_desc* patches, int finestlevel,
+                    const int* carry, int ntransfer, const int* transfer) {
+  if (!h || !h->have_hierarchy || npatch <= 0 || !patches || !carry || ntransfer < 0 ||
+      (ntransfer > 0 && !transfer))
+    return BSAM_ERR_ARG;
+  if (h->mixed) return fail(h, BSAM_ERR_UNSUPPORTED, "regridding: FP64 form only");
+  const int nd = h->rp.ndims;
+  const int nold = h->nuser;
+  for (int i = 0; i < npatch; ++i) {
+    const int o = carry[i];
+    if (o < -1 || o >= nold) return fail(h, BSAM_ERR_ARG, "regrid: carry index out of range");
+    if (o >= 0) {
+      if (h->desc[o].level != patches[i].level)
+        return fail(h, BSAM_ERR_ARG, "regrid: a carried patch changes level");
+      for (int n = 0; n < nd; ++n)
+        if (h->desc[o].mx[n] != patches[i].mx[n])
+          return fail(h, BSAM_ERR_ARG, "regrid: a carried patch changes size");
+    } else if (patches[i].level < 1) {
+      return fail(h, BSAM_ERR_ARG, "regrid: only refined patches may be new");
+    }
+  }
+  for (int t = 0; t < ntransfer; ++t) {
+    const int c = transfer[2 * t], s = transfer[2 * t + 1];
+    if (c < 0 || c >= npatch || carry[c] >= 0 || s < 0 || s >= (int)h->stash_hp.size() ||
+        h->stash_desc[s].level != patches[c].level)
+      return fail(h, BSAM_ERR_ARG, "regrid: a transfer names no new grid and stashed grid");
+  }
+  CU(cudaSetDevice(h->device));
+  CU(cudaStreamSynchronize(h->stream));
+  // Keep the old arena (the carried q and qold) until the copies are done.
+  char* old_arena = h->d_arena;
+  const size_t old_bytes = h->arena_bytes;
+  h->d_arena = nullptr;
+  const std::vector<DevPatch> old_hp = h->hp;
+  const std::vector<int64_t> old_fe = h->field_elems;
+  int rc = bsam_gpu_set_hierarchy(h, npatch, patches, finestlevel);
+  if (rc != BSAM_OK) {
+    cudaFree(old_arena);
+    return rc;
+  }
+  const int64_t lead = 128 / sizeof(double) - 1;
+  cudaError_t e = cudaSuccess;
+  for (int i = 0; i < npatch && e == cudaSuccess; ++i) {
+    const int o = carry[i];
+    if (o < 0) continue;
+    const DevPatch& A = old_hp[o];
+    const DevPatch& B = h->hp[i];
+    if (old_fe[o] != h->field_elems[i]) {
+      e = cudaErrorInvalidValue;
+      break;
+    }
+    for (int c = 0; c < 2 && e == cudaSuccess; ++c) {
+      e = cudaMemcpyAsync(static_cast<double*>(B.q[c]) - lead, static_cast<double*>(A.q[c]) - lead,
+                          old_fe[o] * sizeof(double), cudaMemcpyDeviceToDevice, h->stream);
+      if (e == cudaSuccess && A.qo[c] && B.qo[c])
+        e = cudaMemcpyAsync(static_cast<double*>(B.qo[c]) - lead,
+                            static_cast<double*>(A.qo[c]) - lead, old_fe[o] * sizeof(double),
+                            cudaMemcpyDeviceToDevice, h->stream);
+    }
+  }
+  // InitFields of every new grid, from its (carried) parent, in table order.
+  for (int i = 0; i < npatch && e == cudaSuccess; ++i) {
+    if (carry[i] >= 0) continue;
+    const DevPatch& P = h->hp[i];
+    const size_t ncoarse = (size_t)(P.cn[0] + 2) * (P.cn[1] + 2) * (nd == 3 ? P.cn[2] + 2 : 1);
+    const int blocks = (int)std::min<size_t>((ncoarse + 255) / 256, 4096);
+    if (nd == 2) k_init_mc<2><<<blocks, 256, 0, h->stream>>>(h->d_patches, i);
+    else k_init_mc<3><<<blocks, 256, 0, h->stream>>>(h->d_patches, i);
+    ++h->stats.launches;
+    e = cudaGetLastError();
+  }
+  // TransferValues: the stashed old grids' interiors over the overlaps.
+  for (int t = 0; t < ntransfer && e == cudaSuccess; ++t) {
+    const int c = transfer[2 * t], s = transfer[2 * t + 1];
+    const bsam_patch_desc& T = patches[c];
+    const bsam_patch_desc& S = h->stash_desc[s];
+    int lo[3] = {1, 1, 1}, hi[3] = {1, 1, 1};
+    bool empty = false;
+    for (int n = 0; n < nd; ++n) {
+      lo[n] = std::max(T.mglobal[n][0], S.mglobal[n][0]);
+      hi[n] = std::min(T.mglobal[n][1], S.mglobal[n][1]);
+      empty |= hi[n] < lo[n];
+    }
+    if (empty) continue;
+    int n3[3] = {1, 1, 1}, si[3] = {0, 0, 0}, ti[3] = {0, 0, 0};
+    for (int n = 0; n < nd; ++n) {
+      n3[n] = hi[n] - lo[n] + 1;
+      si[n] = lo[n] - S.mglobal[n][0] + 1;
+      ti[n] = lo[n] - T.mglobal[n][0] + 1;
+    }
+    const size_t cells = (size_t)n3[0] * n3[1] * n3[2];
+    const int blocks = (int)std::min<size_t>((cells + 255) / 256, 4096);
+    if (nd == 2)
+      k_transfer<2><<<blocks, 256, 0, h->stream>>>(h->d_patches, c, h->stash_hp[s], n3[0], n3[1],
+                                                   1, si[0], si[1], 0, ti[0], ti[1], 0);
+    else
+      k_transfer<3><<<blocks, 256, 0, h->stream>>>(h->d_patches, c, h->stash_hp[s], n3[0], n3[1],
+                                                   n3[2], si[0], si[1], si[2], ti[0], ti[1],
+                                                   ti[2]);
+    ++h->stats.launches;
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  // The old arena becomes the spare (the larger of it and the current spare).
+  if (h->spare_arena && h->spare_bytes >= old_bytes) {
+    cudaFree(old_arena);
+  } else {
+    if (h->spare_arena) cudaFree(h->spare_arena);
+    h->spare_arena = old_arena;
+    h->spare_bytes = old_bytes;
+  }
+  if (e != cudaSuccess) return fail(h, BSAM_ERR_CUDA, cudaGetErrorString(e));
+  return BSAM_OK;
+}
+
 int bsam_gpu_set_tuning(bsam_gpu* h, const bsam_tuning* t) {
   if (!h || !t) return BSAM_ERR_ARG;
   if (t->fuse_smoother < -1 || t->fuse_smoother > 1 || t->chunk < 0 || t->graph < -1 ||
@@ -1512,6 +1760,12 @@ int bsam_gpu_destroy(bsam_gpu* h) {
     cudaEventDestroy(e.second);
   }
   free_hierarchy(h);
+  if (h->d_trace) cudaFree(h->d_trace);
+  if (h->h_trace) cudaFreeHost(h->h_trace);
+  if (h->spare_arena) cudaFree(h->spare_arena);
+  if (h->d_stash) cudaFree(h->d_stash);
+  if (h->d_stash_spans) cudaFree(h->d_stash_spans);
+  if (h->d_flags) cudaFree(h->d_flags);
   if (h->d_status) cudaFree(h->d_status);
   if (h->h_status) cudaFreeHost(h->h_status);
   if (h->stream) cudaStreamDestroy(h->stream);

@@ -463,4 +463,198 @@ int bsam_host_write_frame(bsam_gpu* h, const char* path, int ndims, double time,
   return bsam_host_format_frame(path, nd, time, finest, npatch, patches, q.data());
 }
 
+
+struct bsam_amr {
+  bsam_gpu* h = nullptr;
+  int nd = 2;
+  bsam_regrid_params p{};
+  std::vector<bsam_patch_desc> table;
+  bool firstamr = true;
+  std::vector<uint8_t> flags;
+  std::vector<int> boxes;
+};
+
+int bsam_amr_create(bsam_amr** out, bsam_gpu* h, int ndims, const bsam_regrid_params* p,
+                    int npatch, const bsam_patch_desc* patches) {
+  if (!out || !h || !p || (ndims != 2 && ndims != 3) || npatch <= 0 || !patches ||
+      p->maxlevel < 0 || p->maxlevel > BSAM_AMR_MAXLEVEL)
+    return BSAM_ERR_ARG;
+  for (int l = 0; l < p->maxlevel; ++l)
+    if (p->ibuffer[l] < 0 || p->minimumgridpoints[l] < 1 || !(p->desiredfillratios[l] > 0.0))
+      return BSAM_ERR_ARG;
+  auto* a = new bsam_amr();
+  a->h = h;
+  a->nd = ndims;
+  a->p = *p;
+  a->table.assign(patches, patches + npatch);
+  int finest = 0;
+  for (const auto& d : a->table) finest = std::max(finest, d.level);
+  // BSAMSolver: SetGhost on every level, CopyQToQold (bsamroutines.f90:144-147).
+  for (int level = 0; level <= finest; ++level) {
+    const int rc = bsam_gpu_set_ghost_level(h, level);
+    if (rc) {
+      delete a;
+      return rc;
+    }
+  }
+  const int rc = bsam_gpu_copy_q_to_qold(h);
+  if (rc) {
+    delete a;
+    return rc;
+  }
+  *out = a;
+  return BSAM_OK;
+}
+
+int bsam_amr_step(bsam_amr* a, int* nvcycles, double* residual, int* converged) {
+  if (!a) return BSAM_ERR_ARG;
+  bsam_gpu* h = a->h;
+  const int nd = a->nd;
+  const std::vector<bsam_patch_desc> start = a->table;
+  std::vector<bsam_patch_desc> table = a->table;
+  // The old grids of the refined levels as TransferValues reads them.
+  int rc = bsam_gpu_stash(h);
+  if (rc) return rc;
+  rc = bsam_gpu_set_ghost_level(h, 0);  // AMR(rootlevel)
+  if (rc) return rc;
+  // EstimateLevelErrors(0)'s restriction of the root into the level below and
+  // that level's SetGhost are not issued: the V-cycle restricts the root again
+  // before it reads that level, and qold below the root is never read.
+  for (int L = 0; L < a->p.maxlevel; ++L) {
+    if (L >= 1) {
+      rc = bsam_gpu_restrict_level(h, L);  // EstimateLevelErrors(L)
+      if (rc) return rc;
+    }
+    std::vector<int> lvl;
+    size_t cells = 0;
+    for (int i = 0; i < (int)table.size(); ++i)
+      if (table[i].level == L) {
+        lvl.push_back(i);
+        size_t c = 1;
+        for (int n = 0; n < nd; ++n) c *= (size_t)table[i].mx[n];
+        cells += c;
+      }
+    a->flags.assign(cells, 0);
+    rc = bsam_gpu_errflags_level(h, L, a->p.qtolerance[L], a->flags.data());
+    if (rc) return rc;
+    // BufferAndList + InflateEdgeTags over the level.
+    std::vector<int> mx(3 * lvl.size()), mg(6 * lvl.size());
+    for (size_t k = 0; k < lvl.size(); ++k)
+      for (int n = 0; n < 3; ++n) {
+        mx[3 * k + n] = table[lvl[k]].mx[n];
+        mg[6 * k + 2 * n] = table[lvl[k]].mglobal[n][0];
+        mg[6 * k + 2 * n + 1] = table[lvl[k]].mglobal[n][1];
+      }
+    rc = bsam_host_buffer_flags(nd, (int)lvl.size(), mx.data(), mg.data(), a->flags.data(),
+                                a->p.ibuffer[L]);
+    if (rc) return rc;
+    // GridAdapt(L): RefineGrid -> NewSubGrids per patch, MakeNewGrid per box.
+    std::vector<bsam_patch_desc> made;
+    size_t off = 0;
+    for (size_t k = 0; k < lvl.size(); ++k) {
+      const bsam_patch_desc& par = table[lvl[k]];
+      size_t c = 1;
+      for (int n = 0; n < nd; ++n) c *= (size_t)par.mx[n];
+      // The boxes are disjoint and each holds a flagged cell: at most c.
+      const int cap = (int)c;
+      if (a->boxes.size() < 6 * c) a->boxes.resize(6 * c);
+      const int nb = bsam_host_new_subgrids(nd, &mx[3 * k], a->flags.data() + off,
+                                            a->p.desiredfillratios[L], a->p.minimumgridpoints[L],
+                                            a->boxes.data(), cap);
+      if (nb < 0) return nb;
+      for (int b = 0; b < nb; ++b) {
+        int box[6];
+        for (int n = 0; n < 3; ++n) {
+          box[2 * n] = a->boxes[6 * b + 2 * n];
+          box[2 * n + 1] = a->boxes[6 * b + 2 * n + 1];
+        }
+        bsam_patch_desc child;
+        rc = bsam_host_child_desc(nd, &par, lvl[k], box, &child);
+        if (rc) return rc;
+        made.push_back(child);
+      }
+      off += c;
+    }
+    // Levels <= L keep their grids; level L + 1 becomes the new grids,
+    // youngest first (TreeOps prepends); deeper levels lose their grids.
+    std::vector<int> keep, index(table.size(), -1);
+    for (int i = 0; i < (int)table.size(); ++i)
+      if (table[i].level <= L) {
+        index[i] = (int)keep.size();
+        keep.push_back(i);
+      }
+    std::vector<bsam_patch_desc> next;
+    std::vector<int> carry;
+    for (int i : keep) {
+      bsam_patch_desc d = table[i];
+      d.parent = d.parent >= 0 ? index[d.parent] : -1;
+      next.push_back(d);
+      carry.push_back(i);
+    }
+    for (auto it = made.rbegin(); it != made.rend(); ++it) {
+      bsam_patch_desc d = *it;
+      d.parent = index[d.parent];
+      next.push_back(d);
+      carry.push_back(-1);
+    }
+    // TransferValues: each new grid with each old grid of its level.
+    std::vector<int> transfers;
+    for (int c = (int)keep.size(); c < (int)next.size(); ++c)
+      for (int o = 0; o < (int)start.size(); ++o) {
+        if (start[o].level != L + 1) continue;
+        bool overlap = true;
+        for (int n = 0; n < nd; ++n)
+          overlap = overlap && std::max(next[c].mglobal[n][0], start[o].mglobal[n][0]) <=
+                                   std::min(next[c].mglobal[n][1], start[o].mglobal[n][1]);
+        if (overlap) {
+          transfers.push_back(c);
+          transfers.push_back(o);
+        }
+      }
+    int finest = 0;
+    for (const auto& d : next) finest = std::max(finest, d.level);
+    rc = bsam_gpu_regrid(h, (int)next.size(), next.data(), finest, carry.data(),
+                         (int)transfers.size() / 2, transfers.data());
+    if (rc) return rc;
+    table.swap(next);
+    a->table = table;
+    if (made.empty()) {
+      // AMR(L + 1) on an empty level: EstimateLevelErrors(L + 1) still sets
+      // the ghosts of level L.
+      if (L + 1 < a->p.maxlevel) {
+        rc = bsam_gpu_set_ghost_level(h, L);
+        if (rc) return rc;
+      }
+      break;
+    }
+    rc = bsam_gpu_set_ghost_level(h, L + 1);  // AMR(L + 1)
+    if (rc) return rc;
+  }
+  a->table = table;
+  if (a->firstamr) {
+    rc = bsam_gpu_fill_down(h);
+    if (rc) return rc;
+    a->firstamr = false;
+  }
+  rc = bsam_gpu_copy_q_to_qold(h);
+  if (rc) return rc;
+  int nv = 0, conv = 0;
+  double res = 0.0;
+  rc = bsam_gpu_multigrid_iterations(h, &nv, &res, &conv);
+  if (nvcycles) *nvcycles = nv;
+  if (residual) *residual = res;
+  if (converged) *converged = conv;
+  return rc;
+}
+
+int bsam_amr_table(const bsam_amr* a, bsam_patch_desc* out, int maxn) {
+  if (!a) return BSAM_ERR_ARG;
+  const int n = (int)a->table.size();
+  if (out)
+    for (int i = 0; i < n && i < maxn; ++i) out[i] = a->table[i];
+  return n;
+}
+
+void bsam_amr_destroy(bsam_amr* a) { delete a; }
+
 }  // extern "C"

@@ -145,4 +145,38 @@ __global__ void k_init_mc(const DevPatch* __restrict__ PT, int child) {
   }
 }
 
+// Contiguous device-to-device copies in one launch: blockIdx.y selects the
+// span (CopyQToQold of every patch, the stash of the refined patches).
+struct CopySpan {
+  const double* src;
+  double* dst;
+  int64_t n;
+};
+
+__global__ void __launch_bounds__(256) k_copy_spans(const CopySpan* __restrict__ spans) {
+  const CopySpan s = spans[blockIdx.y];
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < s.n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    s.dst[i] = s.src[i];
+}
+
+// TransferOverlap (lib/bsamroutines.f90:1832-1867): the new grid T takes the
+// old grid S's q on the interior cells both cover, in global indices.  S is a
+// record of the stash (its fields point into the stash's copy).
+template <int D>
+__global__ void k_transfer(const DevPatch* __restrict__ PT, int target, DevPatch S, int n0,
+                           int n1, int n2, int si0, int si1, int si2, int ti0, int ti1, int ti2) {
+  const DevPatch T = PT[target];
+  const int64_t total = (int64_t)n0 * n1 * n2;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int a = (int)(e % n0), b = (int)((e / n0) % n1);
+    const int c = D == 3 ? (int)(e / ((int64_t)n0 * n1)) : 0;
+    const int64_t ts = cidx(T, ti0 + a, ti1 + b, D == 3 ? ti2 + c : 0);
+    const int64_t ss = cidx(S, si0 + a, si1 + b, D == 3 ? si2 + c : 0);
+#pragma unroll
+    for (int v = 0; v < 2; ++v) fld<double>(T.q[v])[ts] = fld<double>(S.q[v])[ss];
+  }
+}
+
 }  // namespace bsam

@@ -188,6 +188,24 @@ int bsam_gpu_mass(bsam_gpu* h, double* mass);
  * problem.f90:398-424 adds none).  FP64 patches only. */
 int bsam_gpu_after_step_stats(bsam_gpu* h, double* integral);
 
+/* Regridding with the state resident on the device (FP64 form).
+ * bsam_gpu_stash: copy q of every refined patch aside -- the old grids as
+ * GridAdapt's TransferValues reads them (lib/bsamroutines.f90:1314-1316);
+ * stash index = the patch's index in the table at the time of the call.
+ * bsam_gpu_regrid: set the new patch table (as bsam_gpu_set_hierarchy) and
+ * fill it on the device: patch i takes q and qold of old patch carry[i]
+ * (same level and size) or, with carry[i] = -1 (refined patches only), the
+ * mass-corrected prolongation of its parent (InitFields, 1685-1772); then
+ * for each pair (new grid, stashed grid) of `transfer` (2 * ntransfer ints)
+ * the new grid takes the stashed grid's q on the interior cells both cover
+ * (TransferValues / TransferOverlap, 1774-1867). */
+/* SetErrFlagsUser of every patch on `level` (table order), the flags of
+ * each patch's (1:mx)^d cells concatenated in `flags`: one transfer. */
+int bsam_gpu_errflags_level(bsam_gpu* h, int level, double tol, uint8_t* flags);
+int bsam_gpu_stash(bsam_gpu* h);
+int bsam_gpu_regrid(bsam_gpu* h, int npatch, const bsam_patch_desc* patches, int finestlevel,
+                    const int* carry, int ntransfer, const int* transfer);
+
 /* The CUDA stream (cudaStream_t) every kernel of this handle runs on, for
  * callers that order their own work or record events against it. */
 int bsam_gpu_get_stream(bsam_gpu* h, void** stream);

@@ -91,6 +91,37 @@ int bsam_host_format_frame(const char* path, int ndims, double time, int finestl
 int bsam_host_write_frame(bsam_gpu* h, const char* path, int ndims, double time, int npatch,
                           const bsam_patch_desc* patches);
 
+/* Time steps with regridding every step: TakeTimeSteps with AMR(rootlevel)
+ * (lib/bsamroutines.f90:632-723, 939-1002, 1299-1350) over an engine handle
+ * in the FP64 form.  The &amrdata values, per level 0 .. maxlevel - 1
+ * (lib/nodeinfodef.f90:87-103). */
+#define BSAM_AMR_MAXLEVEL 8
+typedef struct {
+  int32_t maxlevel;
+  int32_t ibuffer[BSAM_AMR_MAXLEVEL];
+  int32_t minimumgridpoints[BSAM_AMR_MAXLEVEL];
+  int32_t pad_;
+  double qtolerance[BSAM_AMR_MAXLEVEL];
+  double desiredfillratios[BSAM_AMR_MAXLEVEL];
+} bsam_regrid_params;
+
+typedef struct bsam_amr bsam_amr;
+
+/* The driver of a hierarchy already set on h (bsam_gpu_set_hierarchy with
+ * `patches`) whose q the caller has put: SetGhost on every level >= 0 and
+ * CopyQToQold, as BSAMSolver leaves them before its first step. */
+int bsam_amr_create(bsam_amr** a, bsam_gpu* h, int ndims, const bsam_regrid_params* p,
+                    int npatch, const bsam_patch_desc* patches);
+/* One time step: AMR(rootlevel) -- per level SetGhost, EstimateLevelErrors'
+ * restriction and tagging, buffering, Berger-Rigoutsos per patch,
+ * MakeNewGrid, InitFields and TransferValues on the device -- then FillDown
+ * on the first step, CopyQToQold and MultigridIterations. */
+int bsam_amr_step(bsam_amr* a, int* nvcycles, double* residual, int* converged);
+/* The current patch table (after the last step's regrid): returns the count
+ * and copies up to maxn records into out (out may be NULL). */
+int bsam_amr_table(const bsam_amr* a, bsam_patch_desc* out, int maxn);
+void bsam_amr_destroy(bsam_amr* a);
+
 #ifdef __cplusplus
 }
 #endif

@@ -434,6 +434,39 @@ class OracleBackend:
         self._rc(lib().orc_hier_multigrid(self.h, _ip(nv), _dp(res)), "multigrid")
         return int(nv[0]), float(res[0])
 
+    def stash(self):
+        """q of every refined patch, kept aside for the transfers."""
+        self._stash = [(d, self.get_q(i) if d["level"] >= 1 else None)
+                       for i, d in enumerate(self.descs)]
+
+    def regrid(self, descs, carry, transfers):
+        """The new table: carried patches keep q (held in the host), new
+        grids take InitFields' prolongation in table order, then the
+        stashed old grids' interiors over the overlaps (TransferOverlap,
+        lib/bsamroutines.f90:1832-1867)."""
+        kept = {i: self.get_q(o) for i, o in enumerate(carry) if o >= 0}
+        self.set_hierarchy(descs)
+        for i, q in kept.items():
+            self.put_q(i, q)
+        for i, o in enumerate(carry):
+            if o < 0:
+                self.init_patch(i)
+        nd = self.nd
+        for c, o in transfers:
+            dc = descs[c]
+            do, qo = self._stash[o]
+            lo = [max(dc["mglobal"][k][0], do["mglobal"][k][0]) for k in range(nd)]
+            hi = [min(dc["mglobal"][k][1], do["mglobal"][k][1]) for k in range(nd)]
+            if any(hi[k] < lo[k] for k in range(nd)):
+                continue
+            qc = self.get_q(c)
+            ts = tuple(slice(lo[k] - dc["mglobal"][k][0] + 1, hi[k] - dc["mglobal"][k][0] + 2)
+                       for k in range(nd))
+            ss = tuple(slice(lo[k] - do["mglobal"][k][0] + 1, hi[k] - do["mglobal"][k][0] + 2)
+                       for k in range(nd))
+            qc[ts] = qo[ss]
+            self.put_q(c, qc)
+
     def after_step_stats(self):
         out = np.zeros(2)
         self._rc(lib().orc_hier_after_step(self.h, _dp(out)), "after_step")

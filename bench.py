@@ -429,6 +429,7 @@ def run_ours(args, world, rank, local):
             with AMR.AmrRun(hier, prm, device=local) as r:
                 r.step()
                 torch.cuda.synchronize()
+                p0 = r.profile()
                 t0 = time.perf_counter()
                 nv, pats, refined = [], [], []
                 for _ in range(nst):
@@ -437,7 +438,9 @@ def run_ours(args, world, rank, local):
                     refined.append(sum(d["mx"][0] * d["mx"][1] for d in r.descs
                                        if d["level"] >= 1))
                 dt_ = time.perf_counter() - t0
+                p1 = r.profile()
             extra[f"cfg2_amr_{tag}"] = {
+                "ms_per_step_by_phase": {k: 1e3 * (p1[k] - p0[k]) / nst for k in r.PHASES},
                 "steps_per_s": nst / dt_, "steps": nst, "vcycles_mean": statistics.mean(nv),
                 "refined_patches_mean": statistics.mean(pats),
                 "refined_cells_mean": statistics.mean(refined),

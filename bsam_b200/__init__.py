@@ -69,7 +69,7 @@ ABI_SYMBOLS = (
     "bsam_host_format_frame", "bsam_host_write_frame",
     "bsam_gpu_set_ghost_level", "bsam_gpu_after_step_stats", "bsam_gpu_stash", "bsam_gpu_regrid",
     "bsam_gpu_errflags_level", "bsam_amr_create", "bsam_amr_step", "bsam_amr_table",
-    "bsam_amr_destroy",
+    "bsam_amr_destroy", "bsam_amr_profile",
     "bsam_batch_create", "bsam_batch_destroy", "bsam_batch_set_tuning", "bsam_batch_footprint",
     "bsam_batch_submit", "bsam_batch_advance", "bsam_batch_sync", "bsam_batch_run",
     "bsam_batch_poll", "bsam_batch_slot_phase", "bsam_batch_collect", "bsam_batch_get_stream", "bsam_batch_profile", "bsam_batch_submit_seeded", "bsam_batch_busy",
@@ -135,6 +135,7 @@ def lib():
     L.bsam_amr_table.argtypes = [vp, ctypes.POINTER(PatchDesc), ctypes.c_int]
     L.bsam_amr_destroy.argtypes = [vp]
     L.bsam_amr_destroy.restype = None
+    L.bsam_amr_profile.argtypes = [vp, dp, ctypes.c_int]
     L.bsam_gpu_regrid.argtypes = [vp, ctypes.c_int, ctypes.POINTER(PatchDesc), ctypes.c_int, ip,
                                   ctypes.c_int, ip]
     L.bsam_host_buffer_flags.argtypes = [ctypes.c_int, ctypes.c_int, ip, ip,

@@ -671,6 +671,16 @@ class AmrRun:
     def stats(self):
         return self.b.after_step_stats()
 
+    PHASES = ("stash", "ghost", "tag", "cluster", "regrid", "solve")
+
+    def profile(self) -> dict:
+        """Host seconds per phase of the steps so far (bsam_amr_profile)."""
+        import ctypes
+        from . import lib
+        out = (ctypes.c_double * len(self.PHASES))()
+        n = lib().bsam_amr_profile(self.a, out, len(self.PHASES))
+        return {"steps": n, **{k: out[i] for i, k in enumerate(self.PHASES)}}
+
     def state(self):
         """q of every patch on a level >= 0 (table order)."""
         return [(i, self.b.get_q(i)) for i, d in enumerate(self.descs) if d["level"] >= 0]

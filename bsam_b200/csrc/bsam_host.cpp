@@ -9,6 +9,7 @@
 // (maxlevel = 0) and calls the C ABI exactly where the Fortran would.
 #include <algorithm>
 #include <array>
+#include <chrono>
 #include <cmath>
 #include <cstdlib>
 #include <cstdio>
@@ -472,7 +473,23 @@ struct bsam_amr {
   bool firstamr = true;
   std::vector<uint8_t> flags;
   std::vector<int> boxes;
+  // Host wall-clock seconds per phase, summed over steps (bsam_amr_profile).
+  double t[BSAM_AMR_NPHASE] = {0};
+  int64_t steps = 0;
 };
+
+namespace {
+struct PhaseClock {
+  double* acc;
+  std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+  explicit PhaseClock(double* a) : acc(a) {}
+  void lap(int phase) {
+    const auto t1 = std::chrono::steady_clock::now();
+    acc[phase] += std::chrono::duration<double>(t1 - t0).count();
+    t0 = t1;
+  }
+};
+}  // namespace
 
 int bsam_amr_create(bsam_amr** out, bsam_gpu* h, int ndims, const bsam_regrid_params* p,
                     int npatch, const bsam_patch_desc* patches) {
@@ -512,11 +529,14 @@ int bsam_amr_step(bsam_amr* a, int* nvcycles, double* residual, int* converged) 
   const int nd = a->nd;
   const std::vector<bsam_patch_desc> start = a->table;
   std::vector<bsam_patch_desc> table = a->table;
+  PhaseClock clk(a->t);
   // The old grids of the refined levels as TransferValues reads them.
   int rc = bsam_gpu_stash(h);
   if (rc) return rc;
+  clk.lap(BSAM_AMR_PHASE_STASH);
   rc = bsam_gpu_set_ghost_level(h, 0);  // AMR(rootlevel)
   if (rc) return rc;
+  clk.lap(BSAM_AMR_PHASE_GHOST);
   // EstimateLevelErrors(0)'s restriction of the root into the level below and
   // that level's SetGhost are not issued: the V-cycle restricts the root again
   // before it reads that level, and qold below the root is never read.
@@ -524,6 +544,7 @@ int bsam_amr_step(bsam_amr* a, int* nvcycles, double* residual, int* converged) 
     if (L >= 1) {
       rc = bsam_gpu_restrict_level(h, L);  // EstimateLevelErrors(L)
       if (rc) return rc;
+      clk.lap(BSAM_AMR_PHASE_GHOST);
     }
     std::vector<int> lvl;
     size_t cells = 0;
@@ -548,6 +569,7 @@ int bsam_amr_step(bsam_amr* a, int* nvcycles, double* residual, int* converged) 
     rc = bsam_host_buffer_flags(nd, (int)lvl.size(), mx.data(), mg.data(), a->flags.data(),
                                 a->p.ibuffer[L]);
     if (rc) return rc;
+    clk.lap(BSAM_AMR_PHASE_TAG);
     // GridAdapt(L): RefineGrid -> NewSubGrids per patch, MakeNewGrid per box.
     std::vector<bsam_patch_desc> made;
     size_t off = 0;
@@ -613,9 +635,11 @@ int bsam_amr_step(bsam_amr* a, int* nvcycles, double* residual, int* converged) 
       }
     int finest = 0;
     for (const auto& d : next) finest = std::max(finest, d.level);
+    clk.lap(BSAM_AMR_PHASE_CLUSTER);
     rc = bsam_gpu_regrid(h, (int)next.size(), next.data(), finest, carry.data(),
                          (int)transfers.size() / 2, transfers.data());
     if (rc) return rc;
+    clk.lap(BSAM_AMR_PHASE_REGRID);
     table.swap(next);
     a->table = table;
     if (made.empty()) {
@@ -625,10 +649,12 @@ int bsam_amr_step(bsam_amr* a, int* nvcycles, double* residual, int* converged) 
         rc = bsam_gpu_set_ghost_level(h, L);
         if (rc) return rc;
       }
+      clk.lap(BSAM_AMR_PHASE_GHOST);
       break;
     }
     rc = bsam_gpu_set_ghost_level(h, L + 1);  // AMR(L + 1)
     if (rc) return rc;
+    clk.lap(BSAM_AMR_PHASE_GHOST);
   }
   a->table = table;
   if (a->firstamr) {
@@ -641,10 +667,18 @@ int bsam_amr_step(bsam_amr* a, int* nvcycles, double* residual, int* converged) 
   int nv = 0, conv = 0;
   double res = 0.0;
   rc = bsam_gpu_multigrid_iterations(h, &nv, &res, &conv);
+  clk.lap(BSAM_AMR_PHASE_SOLVE);
+  ++a->steps;
   if (nvcycles) *nvcycles = nv;
   if (residual) *residual = res;
   if (converged) *converged = conv;
   return rc;
+}
+
+int bsam_amr_profile(const bsam_amr* a, double* seconds, int n) {
+  if (!a || !seconds || n < 0) return BSAM_ERR_ARG;
+  for (int i = 0; i < n && i < BSAM_AMR_NPHASE; ++i) seconds[i] = a->t[i];
+  return (int)a->steps;
 }
 
 int bsam_amr_table(const bsam_amr* a, bsam_patch_desc* out, int maxn) {

@@ -121,6 +121,21 @@ int bsam_amr_step(bsam_amr* a, int* nvcycles, double* residual, int* converged);
  * and copies up to maxn records into out (out may be NULL). */
 int bsam_amr_table(const bsam_amr* a, bsam_patch_desc* out, int maxn);
 void bsam_amr_destroy(bsam_amr* a);
+/* Host wall-clock seconds spent per phase of bsam_amr_step, summed over
+ * the steps so far (each phase ends with the device idle): the stash, the
+ * ghost fills and restrictions, tagging and buffering, clustering and the
+ * child records, the regrid on the device, and FillDown + CopyQToQold +
+ * MultigridIterations.  Returns the number of steps. */
+enum {
+  BSAM_AMR_PHASE_STASH = 0,
+  BSAM_AMR_PHASE_GHOST = 1,
+  BSAM_AMR_PHASE_TAG = 2,
+  BSAM_AMR_PHASE_CLUSTER = 3,
+  BSAM_AMR_PHASE_REGRID = 4,
+  BSAM_AMR_PHASE_SOLVE = 5,
+  BSAM_AMR_NPHASE = 6
+};
+int bsam_amr_profile(const bsam_amr* a, double* seconds, int n);
 
 #ifdef __cplusplus
 }

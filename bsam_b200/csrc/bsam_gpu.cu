@@ -87,10 +87,17 @@ struct bsam_gpu {
   // whose q pointers point into it.
   char* d_stash = nullptr;
   size_t stash_cap = 0;
+  // The hierarchy's tables (records, work lists, patch lists, overlap copies,
+  // copy spans, tensor maps, partial sums) in one device buffer, grown and
+  // never shrunk, filled by one copy from a host image per set_hierarchy.
+  char* d_meta = nullptr;
+  size_t meta_cap = 0;
+  std::vector<unsigned char> meta_host;
   // The arena a regrid released, kept for the next hierarchy of no larger
   // size (regridding every step alternates between two arenas).
   char* spare_arena = nullptr;
   size_t spare_bytes = 0;
+  bool regridding = false;  // set_hierarchy called by bsam_gpu_regrid
   uint8_t* d_flags = nullptr;  // bsam_gpu_errflags_level's device flags
   CopySpan* d_qold_spans = nullptr;  // CopyQToQold: q -> qold of every patch that has qold
   int nqold_spans = 0;
@@ -580,15 +587,11 @@ int bsam_gpu_create(bsam_gpu** out, int device, const bsam_run_params* p) {
 }
 
 static void free_hierarchy(bsam_gpu* h) {
-  if (h->d_items) cudaFree(h->d_items);
-  if (h->d_tmaps) cudaFree(h->d_tmaps);
+  // d_items, d_tmaps, d_tops, d_patches, d_partials, d_qold_spans, d_plist
+  // and d_ovl point into d_meta, which the handle keeps.
   h->d_tmaps = nullptr;
-  if (h->d_tops) cudaFree(h->d_tops);
   if (h->step_exec) cudaGraphExecDestroy(h->step_exec);
   if (h->d_arena) cudaFree(h->d_arena);
-  if (h->d_patches) cudaFree(h->d_patches);
-  if (h->d_partials) cudaFree(h->d_partials);
-  if (h->d_qold_spans) cudaFree(h->d_qold_spans);
   h->d_qold_spans = nullptr;
   h->nqold_spans = 0;
   h->qold_span_max = 0;
@@ -603,8 +606,6 @@ static void free_hierarchy(bsam_gpu* h) {
   h->nmaster = 0;
   h->d_state = h->d_root = nullptr;
   h->nstate = h->nroot = 0;
-  if (h->d_plist) cudaFree(h->d_plist);
-  if (h->d_ovl) cudaFree(h->d_ovl);
   h->d_plist = nullptr;
   h->d_ovl = nullptr;
   h->amr = false;
@@ -801,8 +802,12 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
     total = h->spare_bytes;
     h->spare_arena = nullptr;
     h->spare_bytes = 0;
-  } else if (cudaMalloc(&h->d_arena, total) != cudaSuccess) {
-    return fail(h, BSAM_ERR_NOMEM, "arena allocation failed");
+  } else {
+    // Under regridding the arena alternates with the spare: a quarter more
+    // than this table needs lets the next tables of similar size reuse it.
+    if (h->regridding) total += total / 4;
+    if (cudaMalloc(&h->d_arena, total) != cudaSuccess)
+      return fail(h, BSAM_ERR_NOMEM, "arena allocation failed");
   }
   h->arena_bytes = total;
   CU(cudaMemsetAsync(h->d_arena, 0, total, h->stream));
@@ -835,8 +840,9 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
     P.bs = P.delta ? next() : nullptr;
   }
   // CopyQToQold as one launch: the whole field allocation of q onto qold's.
+  std::vector<CopySpan> qold_spans;
   {
-    std::vector<CopySpan> spans;
+    std::vector<CopySpan>& spans = qold_spans;
     for (int r = 0; r < npatch; ++r) {
       const DevPatch& P = h->hp[r];
       if (!P.qo[0]) continue;
@@ -847,23 +853,19 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
       h->qold_span_max = std::max(h->qold_span_max, h->field_elems[r]);
     }
     h->nqold_spans = (int)spans.size();
-    if (!spans.empty()) {
-      CU(cudaMalloc(&h->d_qold_spans, sizeof(CopySpan) * spans.size()));
-      CU(cudaMemcpyAsync(h->d_qold_spans, spans.data(), sizeof(CopySpan) * spans.size(),
-                         cudaMemcpyHostToDevice, h->stream));
-    }
   }
   // Parents of the twins are the masters' parents.
   for (int r = npatch; r < nrec; ++r) h->hp[r].parent = h->hp[rec_src[r]].parent;
   for (int r = 0; r < nrec; ++r)
     h->hp[r].pprec = h->hp[r].parent >= 0 ? h->hp[h->hp[r].parent].prec : h->hp[r].prec;
   // TMA tensor maps of the fused records (q0, q1, qb0, qb1, f0, f1, bs).
+  std::vector<int> fused_recs;
+  std::vector<CUtensorMap> maps;
   {
-    std::vector<int> fused_recs;
     for (int r = 0; r < nrec; ++r)
       if (h->hp[r].fused) fused_recs.push_back(r);
     if (!fused_recs.empty()) {
-      std::vector<CUtensorMap> maps(7 * fused_recs.size());
+      maps.resize(7 * fused_recs.size());
       for (size_t k = 0; k < fused_recs.size(); ++k) {
         const DevPatch& P = h->hp[fused_recs[k]];
         const int hx = P.prec == PREC_F32 ? Fused3<float>::HX : Fused3<double>::HX;
@@ -874,10 +876,7 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
           if (!encode_field_map(&maps[7 * k + m], P, fields[m], hx, hy))
             return fail(h, BSAM_ERR_CUDA, "cuTensorMapEncodeTiled rejected a field map");
       }
-      CU(cudaMalloc(&h->d_tmaps, sizeof(CUtensorMap) * maps.size()));
-      CU(cudaMemcpyAsync(h->d_tmaps, maps.data(), sizeof(CUtensorMap) * maps.size(),
-                         cudaMemcpyHostToDevice, h->stream));
-      for (size_t k = 0; k < fused_recs.size(); ++k) h->hp[fused_recs[k]].tmaps = h->d_tmaps + 7 * k;
+
     }
   }
 
@@ -988,47 +987,21 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
     span_plist[li].second = (int)plist_all.size() - span_plist[li].first;
     span_ovl[li].second = (int)ovl_all.size() - span_ovl[li].first;
   }
-  if (!plist_all.empty()) {
-    CU(cudaMalloc(&h->d_plist, sizeof(int) * plist_all.size()));
-    CU(cudaMemcpyAsync(h->d_plist, plist_all.data(), sizeof(int) * plist_all.size(),
-                       cudaMemcpyHostToDevice, h->stream));
-  }
-  if (!ovl_all.empty()) {
-    CU(cudaMalloc(&h->d_ovl, sizeof(OverlapCopy) * ovl_all.size()));
-    CU(cudaMemcpyAsync(h->d_ovl, ovl_all.data(), sizeof(OverlapCopy) * ovl_all.size(),
-                       cudaMemcpyHostToDevice, h->stream));
-  }
-  for (size_t li = 0; li < nl; ++li) {
-    LevelPlan& L = h->levels[li];
-    L.d_plist = h->d_plist ? h->d_plist + span_plist[li].first : nullptr;
-    L.nplist = span_plist[li].second;
-    L.d_ovl = h->d_ovl ? h->d_ovl + span_ovl[li].first : nullptr;
-    L.novl = span_ovl[li].second;
-  }
-
-  CU(cudaMalloc(&h->d_items, all.size() * sizeof(Item)));
-  CU(cudaMemcpyAsync(h->d_items, all.data(), all.size() * sizeof(Item), cudaMemcpyHostToDevice,
-                     h->stream));
   h->max_items = std::max(1, h->nmaster);
   for (size_t li = 0; li < nl; ++li) {
     LevelPlan& L = h->levels[li];
-    L.d_fine = h->d_items + spans_fine[li].first;
+    L.nplist = span_plist[li].second;
+    L.novl = span_ovl[li].second;
     L.nfine = spans_fine[li].second;
-    L.d_coarse = h->d_items + spans_coarse[li].first;
     L.ncoarse = spans_coarse[li].second;
-    L.d_fused = h->d_items + spans_fused[li].first;
     L.nfused = spans_fused[li].second;
     h->max_items = std::max(h->max_items, L.nfine);
   }
-  h->d_master = h->d_items + s_master;
-  h->d_state = h->d_items + s_state;
-  h->d_root = h->d_items + s_root;
   h->max_items = std::max(h->max_items, h->nroot);
   CU(cudaFuncSetAttribute(k_smooth3_fused<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)Fused3<double>::SMEM));
   CU(cudaFuncSetAttribute(k_smooth3_fused<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)Fused3<float>::SMEM));
-  CU(cudaMalloc(&h->d_partials, sizeof(double) * h->max_items));
   // The residual trace buffers live as long as the handle (maxvcycles is
   // fixed at creation).
   if (!h->d_trace) CU(cudaMalloc(&h->d_trace, sizeof(double) * h->rp.maxvcycles));
@@ -1038,18 +1011,75 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
     for (int p : h->masters) ncells += cells_of(h->hp[p].n, nd);
     h->denom = (double)(h->rp.nrvars * ncells);  // L2Error's integralresult(2)
   }
+  std::vector<int> tops;
   if (h->bottom_level >= minlevel) {
-    std::vector<int> tops = plan(h, h->bottom_level).patches;
+    tops = plan(h, h->bottom_level).patches;
     for (int p : tops)
       if (h->hp[p].prec != PREC_F64) return fail(h, BSAM_ERR_ARG, "bottom levels must be FP64");
     h->ntops = (int)tops.size();
-    CU(cudaMalloc(&h->d_tops, sizeof(int) * tops.size()));
-    CU(cudaMemcpyAsync(h->d_tops, tops.data(), sizeof(int) * tops.size(),
-                       cudaMemcpyHostToDevice, h->stream));
   }
-  CU(cudaMalloc(&h->d_patches, sizeof(DevPatch) * nrec));
-  CU(cudaMemcpyAsync(h->d_patches, h->hp.data(), sizeof(DevPatch) * nrec,
-                     cudaMemcpyHostToDevice, h->stream));
+  // The tables' layout in d_meta (256-byte aligned pieces), the buffer grown
+  // when too small, then the pointers, and one copy of the host image.
+  {
+    size_t off = 0;
+    auto place = [&](size_t bytes) {
+      const size_t at = (size_t)roundup((int64_t)off, 256);
+      off = at + bytes;
+      return at;
+    };
+    const size_t o_patches = place(sizeof(DevPatch) * nrec);
+    const size_t o_items = place(sizeof(Item) * all.size());
+    const size_t o_plist = place(sizeof(int) * plist_all.size());
+    const size_t o_ovl = place(sizeof(OverlapCopy) * ovl_all.size());
+    const size_t o_qold = place(sizeof(CopySpan) * qold_spans.size());
+    const size_t o_maps = place(sizeof(CUtensorMap) * maps.size());
+    const size_t o_tops = place(sizeof(int) * tops.size());
+    const size_t o_part = place(sizeof(double) * h->max_items);
+    const size_t total_meta = off;
+    if (total_meta > h->meta_cap) {
+      if (h->d_meta) cudaFree(h->d_meta);
+      h->d_meta = nullptr;
+      h->meta_cap = 0;
+      const size_t want = total_meta + total_meta / 2;  // headroom for the next regrid
+      if (cudaMalloc(&h->d_meta, want) != cudaSuccess)
+        return fail(h, BSAM_ERR_NOMEM, "table allocation failed");
+      h->meta_cap = want;
+    }
+    char* base = h->d_meta;
+    h->d_items = reinterpret_cast<Item*>(base + o_items);
+    h->d_plist = plist_all.empty() ? nullptr : reinterpret_cast<int*>(base + o_plist);
+    h->d_ovl = ovl_all.empty() ? nullptr : reinterpret_cast<OverlapCopy*>(base + o_ovl);
+    h->d_qold_spans = qold_spans.empty() ? nullptr : reinterpret_cast<CopySpan*>(base + o_qold);
+    h->d_tmaps = maps.empty() ? nullptr : reinterpret_cast<CUtensorMap*>(base + o_maps);
+    h->d_tops = tops.empty() ? nullptr : reinterpret_cast<int*>(base + o_tops);
+    h->d_partials = reinterpret_cast<double*>(base + o_part);
+    h->d_patches = reinterpret_cast<DevPatch*>(base + o_patches);
+    for (size_t k = 0; k < fused_recs.size(); ++k) h->hp[fused_recs[k]].tmaps = h->d_tmaps + 7 * k;
+    for (size_t li = 0; li < nl; ++li) {
+      LevelPlan& L = h->levels[li];
+      L.d_plist = h->d_plist ? h->d_plist + span_plist[li].first : nullptr;
+      L.d_ovl = h->d_ovl ? h->d_ovl + span_ovl[li].first : nullptr;
+      L.d_fine = h->d_items + spans_fine[li].first;
+      L.d_coarse = h->d_items + spans_coarse[li].first;
+      L.d_fused = h->d_items + spans_fused[li].first;
+    }
+    h->d_master = h->d_items + s_master;
+    h->d_state = h->d_items + s_state;
+    h->d_root = h->d_items + s_root;
+    std::vector<unsigned char>& img = h->meta_host;
+    img.assign(o_part, 0);  // the partial sums need no initial contents
+    auto put = [&](size_t at, const void* src, size_t bytes) {
+      if (bytes) std::memcpy(img.data() + at, src, bytes);
+    };
+    put(o_patches, h->hp.data(), sizeof(DevPatch) * nrec);
+    put(o_items, all.data(), sizeof(Item) * all.size());
+    put(o_plist, plist_all.data(), sizeof(int) * plist_all.size());
+    put(o_ovl, ovl_all.data(), sizeof(OverlapCopy) * ovl_all.size());
+    put(o_qold, qold_spans.data(), sizeof(CopySpan) * qold_spans.size());
+    put(o_maps, maps.data(), sizeof(CUtensorMap) * maps.size());
+    put(o_tops, tops.data(), sizeof(int) * tops.size());
+    CU(cudaMemcpyAsync(h->d_meta, img.data(), img.size(), cudaMemcpyHostToDevice, h->stream));
+  }
   CU(cudaMemsetAsync(h->d_status, 0, sizeof(DevStatus), h->stream));
   CU(cudaStreamSynchronize(h->stream));
   h->have_hierarchy = true;
@@ -1554,9 +1584,10 @@ int bsam_gpu_stash(bsam_gpu* h) {
     if (h->d_stash) cudaFree(h->d_stash);
     h->d_stash = nullptr;
     h->stash_cap = 0;
-    if (cudaMalloc(&h->d_stash, total) != cudaSuccess)
+    const size_t want = total + total / 2;  // headroom for the next steps
+    if (cudaMalloc(&h->d_stash, want) != cudaSuccess)
       return fail(h, BSAM_ERR_NOMEM, "stash allocation failed");
-    h->stash_cap = total;
+    h->stash_cap = want;
   }
   const int64_t lead = 128 / sizeof(double) - 1;
   std::vector<CopySpan> spans;
@@ -1576,9 +1607,10 @@ int bsam_gpu_stash(bsam_gpu* h) {
     if (h->d_stash_spans) cudaFree(h->d_stash_spans);
     h->d_stash_spans = nullptr;
     h->stash_spans_cap = 0;
-    if (cudaMalloc(&h->d_stash_spans, sizeof(CopySpan) * spans.size()) != cudaSuccess)
+    const size_t want = spans.size() + spans.size() / 2;
+    if (cudaMalloc(&h->d_stash_spans, sizeof(CopySpan) * want) != cudaSuccess)
       return fail(h, BSAM_ERR_NOMEM, "stash allocation failed");
-    h->stash_spans_cap = spans.size();
+    h->stash_spans_cap = want;
   }
   CU(cudaMemcpyAsync(h->d_stash_spans, spans.data(), sizeof(CopySpan) * spans.size(),
                      cudaMemcpyHostToDevice, h->stream));
@@ -1626,7 +1658,9 @@ int bsam_gpu_regrid(bsam_gpu* h, int npatch, const bsam_patch_desc* patches, int
   h->d_arena = nullptr;
   const std::vector<DevPatch> old_hp = h->hp;
   const std::vector<int64_t> old_fe = h->field_elems;
+  h->regridding = true;
   int rc = bsam_gpu_set_hierarchy(h, npatch, patches, finestlevel);
+  h->regridding = false;
   if (rc != BSAM_OK) {
     cudaFree(old_arena);
     return rc;
@@ -1765,6 +1799,7 @@ int bsam_gpu_destroy(bsam_gpu* h) {
   if (h->spare_arena) cudaFree(h->spare_arena);
   if (h->d_stash) cudaFree(h->d_stash);
   if (h->d_stash_spans) cudaFree(h->d_stash_spans);
+  if (h->d_meta) cudaFree(h->d_meta);
   if (h->d_flags) cudaFree(h->d_flags);
   if (h->d_status) cudaFree(h->d_status);
   if (h->h_status) cudaFreeHost(h->h_status);

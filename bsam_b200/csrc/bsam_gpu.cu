@@ -98,6 +98,9 @@ struct bsam_gpu {
   char* spare_arena = nullptr;
   size_t spare_bytes = 0;
   bool regridding = false;  // set_hierarchy called by bsam_gpu_regrid
+  char* d_regrid = nullptr;  // bsam_gpu_regrid's task list (grown, never shrunk)
+  size_t regrid_cap = 0;
+  std::vector<unsigned char> regrid_host;
   uint8_t* d_flags = nullptr;  // bsam_gpu_errflags_level's device flags
   CopySpan* d_qold_spans = nullptr;  // CopyQToQold: q -> qold of every patch that has qold
   int nqold_spans = 0;
@@ -1665,67 +1668,112 @@ int bsam_gpu_regrid(bsam_gpu* h, int npatch, const bsam_patch_desc* patches, int
     cudaFree(old_arena);
     return rc;
   }
+  // The device work as three launches from one uploaded task list: the
+  // carried patches' q and qold (whole field allocations), InitFields of every
+  // new grid from its carried parent, then the transfers from the stash.
   const int64_t lead = 128 / sizeof(double) - 1;
   cudaError_t e = cudaSuccess;
-  for (int i = 0; i < npatch && e == cudaSuccess; ++i) {
+  std::vector<CopySpan> spans;
+  std::vector<int> children;
+  std::vector<TransferTask> tasks;
+  int64_t span_max = 0, child_max = 0, task_max = 0;
+  for (int i = 0; i < npatch; ++i) {
     const int o = carry[i];
-    if (o < 0) continue;
+    if (o < 0) {
+      const DevPatch& P = h->hp[i];
+      children.push_back(i);
+      child_max = std::max<int64_t>(
+          child_max, (int64_t)(P.cn[0] + 2) * (P.cn[1] + 2) * (nd == 3 ? P.cn[2] + 2 : 1));
+      continue;
+    }
     const DevPatch& A = old_hp[o];
     const DevPatch& B = h->hp[i];
     if (old_fe[o] != h->field_elems[i]) {
       e = cudaErrorInvalidValue;
       break;
     }
-    for (int c = 0; c < 2 && e == cudaSuccess; ++c) {
-      e = cudaMemcpyAsync(static_cast<double*>(B.q[c]) - lead, static_cast<double*>(A.q[c]) - lead,
-                          old_fe[o] * sizeof(double), cudaMemcpyDeviceToDevice, h->stream);
-      if (e == cudaSuccess && A.qo[c] && B.qo[c])
-        e = cudaMemcpyAsync(static_cast<double*>(B.qo[c]) - lead,
-                            static_cast<double*>(A.qo[c]) - lead, old_fe[o] * sizeof(double),
-                            cudaMemcpyDeviceToDevice, h->stream);
+    for (int c = 0; c < 2; ++c) {
+      spans.push_back(CopySpan{static_cast<const double*>(A.q[c]) - lead,
+                               static_cast<double*>(B.q[c]) - lead, old_fe[o]});
+      if (A.qo[c] && B.qo[c])
+        spans.push_back(CopySpan{static_cast<const double*>(A.qo[c]) - lead,
+                                 static_cast<double*>(B.qo[c]) - lead, old_fe[o]});
     }
+    span_max = std::max(span_max, old_fe[o]);
   }
-  // InitFields of every new grid, from its (carried) parent, in table order.
-  for (int i = 0; i < npatch && e == cudaSuccess; ++i) {
-    if (carry[i] >= 0) continue;
-    const DevPatch& P = h->hp[i];
-    const size_t ncoarse = (size_t)(P.cn[0] + 2) * (P.cn[1] + 2) * (nd == 3 ? P.cn[2] + 2 : 1);
-    const int blocks = (int)std::min<size_t>((ncoarse + 255) / 256, 4096);
-    if (nd == 2) k_init_mc<2><<<blocks, 256, 0, h->stream>>>(h->d_patches, i);
-    else k_init_mc<3><<<blocks, 256, 0, h->stream>>>(h->d_patches, i);
-    ++h->stats.launches;
-    e = cudaGetLastError();
-  }
-  // TransferValues: the stashed old grids' interiors over the overlaps.
   for (int t = 0; t < ntransfer && e == cudaSuccess; ++t) {
     const int c = transfer[2 * t], s = transfer[2 * t + 1];
     const bsam_patch_desc& T = patches[c];
     const bsam_patch_desc& S = h->stash_desc[s];
-    int lo[3] = {1, 1, 1}, hi[3] = {1, 1, 1};
+    TransferTask tk{};
+    tk.S = h->stash_hp[s];
+    tk.target = c;
     bool empty = false;
-    for (int n = 0; n < nd; ++n) {
-      lo[n] = std::max(T.mglobal[n][0], S.mglobal[n][0]);
-      hi[n] = std::min(T.mglobal[n][1], S.mglobal[n][1]);
-      empty |= hi[n] < lo[n];
+    int64_t cells = 1;
+    for (int n = 0; n < 3; ++n) {
+      if (n >= nd) {
+        tk.n[n] = 1;
+        continue;
+      }
+      const int lo = std::max(T.mglobal[n][0], S.mglobal[n][0]);
+      const int hi = std::min(T.mglobal[n][1], S.mglobal[n][1]);
+      empty |= hi < lo;
+      tk.n[n] = hi - lo + 1;
+      tk.si[n] = lo - S.mglobal[n][0] + 1;
+      tk.ti[n] = lo - T.mglobal[n][0] + 1;
+      cells *= tk.n[n];
     }
     if (empty) continue;
-    int n3[3] = {1, 1, 1}, si[3] = {0, 0, 0}, ti[3] = {0, 0, 0};
-    for (int n = 0; n < nd; ++n) {
-      n3[n] = hi[n] - lo[n] + 1;
-      si[n] = lo[n] - S.mglobal[n][0] + 1;
-      ti[n] = lo[n] - T.mglobal[n][0] + 1;
+    tasks.push_back(tk);
+    task_max = std::max(task_max, cells);
+  }
+  if (e == cudaSuccess && (spans.size() > 65535 || children.size() > 65535 || tasks.size() > 65535))
+    e = cudaErrorInvalidValue;  // one grid row per item: at most 65535 of each
+  if (e == cudaSuccess && (!spans.empty() || !children.empty() || !tasks.empty())) {
+    // Layout: spans, children, tasks; 256-byte aligned pieces.
+    const size_t o_sp = 0;
+    const size_t o_ch = (size_t)roundup((int64_t)(sizeof(CopySpan) * spans.size()), 256);
+    const size_t o_tk = o_ch + (size_t)roundup((int64_t)(sizeof(int) * children.size()), 256);
+    const size_t bytes = o_tk + sizeof(TransferTask) * tasks.size();
+    if (bytes > h->regrid_cap) {
+      if (h->d_regrid) cudaFree(h->d_regrid);
+      h->d_regrid = nullptr;
+      h->regrid_cap = 0;
+      const size_t want = bytes + bytes / 2;
+      e = cudaMalloc(&h->d_regrid, want);
+      if (e == cudaSuccess) h->regrid_cap = want;
     }
-    const size_t cells = (size_t)n3[0] * n3[1] * n3[2];
-    const int blocks = (int)std::min<size_t>((cells + 255) / 256, 4096);
-    if (nd == 2)
-      k_transfer<2><<<blocks, 256, 0, h->stream>>>(h->d_patches, c, h->stash_hp[s], n3[0], n3[1],
-                                                   1, si[0], si[1], 0, ti[0], ti[1], 0);
-    else
-      k_transfer<3><<<blocks, 256, 0, h->stream>>>(h->d_patches, c, h->stash_hp[s], n3[0], n3[1],
-                                                   n3[2], si[0], si[1], si[2], ti[0], ti[1],
-                                                   ti[2]);
-    ++h->stats.launches;
-    e = cudaGetLastError();
+    if (e == cudaSuccess) {
+      h->regrid_host.assign(bytes, 0);
+      unsigned char* img = h->regrid_host.data();
+      if (!spans.empty()) std::memcpy(img + o_sp, spans.data(), sizeof(CopySpan) * spans.size());
+      if (!children.empty()) std::memcpy(img + o_ch, children.data(), sizeof(int) * children.size());
+      if (!tasks.empty()) std::memcpy(img + o_tk, tasks.data(), sizeof(TransferTask) * tasks.size());
+      e = cudaMemcpyAsync(h->d_regrid, img, bytes, cudaMemcpyHostToDevice, h->stream);
+    }
+    const auto grid_x = [](int64_t n) { return (unsigned)std::min<int64_t>((n + 255) / 256, 64); };
+    if (e == cudaSuccess && !spans.empty()) {
+      k_copy_spans<<<dim3(grid_x(span_max), (unsigned)spans.size()), 256, 0, h->stream>>>(
+          reinterpret_cast<const CopySpan*>(h->d_regrid + o_sp));
+      ++h->stats.launches;
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess && !children.empty()) {
+      const dim3 g(grid_x(child_max), (unsigned)children.size());
+      const int* d_ch = reinterpret_cast<const int*>(h->d_regrid + o_ch);
+      if (nd == 2) k_init_mc_list<2><<<g, 256, 0, h->stream>>>(h->d_patches, d_ch);
+      else k_init_mc_list<3><<<g, 256, 0, h->stream>>>(h->d_patches, d_ch);
+      ++h->stats.launches;
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess && !tasks.empty()) {
+      const dim3 g(grid_x(task_max), (unsigned)tasks.size());
+      const TransferTask* d_tk = reinterpret_cast<const TransferTask*>(h->d_regrid + o_tk);
+      if (nd == 2) k_transfer_list<2><<<g, 256, 0, h->stream>>>(h->d_patches, d_tk);
+      else k_transfer_list<3><<<g, 256, 0, h->stream>>>(h->d_patches, d_tk);
+      ++h->stats.launches;
+      e = cudaGetLastError();
+    }
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
   // The old arena becomes the spare (the larger of it and the current spare).
@@ -1800,6 +1848,7 @@ int bsam_gpu_destroy(bsam_gpu* h) {
   if (h->d_stash) cudaFree(h->d_stash);
   if (h->d_stash_spans) cudaFree(h->d_stash_spans);
   if (h->d_meta) cudaFree(h->d_meta);
+  if (h->d_regrid) cudaFree(h->d_regrid);
   if (h->d_flags) cudaFree(h->d_flags);
   if (h->d_status) cudaFree(h->d_status);
   if (h->h_status) cudaFreeHost(h->h_status);

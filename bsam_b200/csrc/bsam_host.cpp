@@ -343,18 +343,36 @@ int bsam_host_buffer_flags(int ndims, int npatch, const int* mx, const int* mglo
     }
     off[p + 1] = off[p] + cells;
   }
-  // The cells flagged on entry, in global indices.
-  std::vector<std::array<int, 3>> tagged;
+  // BufferAndList: a cell flagged on entry whose buffer box lies inside its
+  // patch flags that box there; one whose box crosses the patch's edge is
+  // listed by global index.  The result is the union of the boxes of every
+  // flagged cell, clipped to each patch.
+  const std::vector<uint8_t> orig(flags, flags + off[npatch]);
+  std::vector<std::array<int, 3>> listed;
   for (int p = 0; p < npatch; ++p) {
     const int m0 = mx[3 * p], m1 = mx[3 * p + 1], m2 = nd == 3 ? mx[3 * p + 2] : 1;
     for (int k = 0; k < m2; ++k)
       for (int j = 0; j < m1; ++j)
-        for (int i = 0; i < m0; ++i)
-          if (flags[off[p] + i + (size_t)m0 * (j + (size_t)m1 * k)])
-            tagged.push_back({mglobal[6 * p] + i, mglobal[6 * p + 2] + j,
+        for (int i = 0; i < m0; ++i) {
+          if (!orig[off[p] + i + (size_t)m0 * (j + (size_t)m1 * k)]) continue;
+          const bool inside = i - ibuffer >= 0 && i + ibuffer < m0 && j - ibuffer >= 0 &&
+                              j + ibuffer < m1 &&
+                              (nd == 2 || (k - ibuffer >= 0 && k + ibuffer < m2));
+          if (!inside) {
+            listed.push_back({mglobal[6 * p] + i, mglobal[6 * p + 2] + j,
                               nd == 3 ? mglobal[6 * p + 4] + k : 1});
+            continue;
+          }
+          const int kb = nd == 3 ? ibuffer : 0;
+          for (int kk = k - kb; kk <= k + kb; ++kk)
+            for (int jj = j - ibuffer; jj <= j + ibuffer; ++jj)
+              for (int ii = i - ibuffer; ii <= i + ibuffer; ++ii)
+                flags[off[p] + ii + (size_t)m0 * (jj + (size_t)m1 * kk)] = 1;
+        }
   }
-  for (const auto& c : tagged)
+  // InflateEdgeTags / BufferTaggedCells: each listed cell's box, clipped, on
+  // every patch of the level.
+  for (const auto& c : listed)
     for (int p = 0; p < npatch; ++p) {
       int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
       bool hit = true;

@@ -78,7 +78,7 @@ __device__ __forceinline__ double prolong_raw(const DevPatch& C, const DevPatch&
 // correction, a ring coarse cell the children of it that lie in the child's
 // ring (0:mx+1)^d, uncorrected.  Then qold = q on the same cells.
 template <int D>
-__global__ void k_init_mc(const DevPatch* __restrict__ PT, int child) {
+__device__ void init_mc(const DevPatch* __restrict__ PT, int child) {
   const DevPatch C = PT[child];
   const DevPatch R = PT[C.parent];
   const int c0 = C.cn[0], c1 = C.cn[1], c2 = D == 3 ? C.cn[2] : 0;
@@ -145,6 +145,18 @@ __global__ void k_init_mc(const DevPatch* __restrict__ PT, int child) {
   }
 }
 
+template <int D>
+__global__ void k_init_mc(const DevPatch* __restrict__ PT, int child) {
+  init_mc<D>(PT, child);
+}
+
+// InitFields of several new patches in one launch: blockIdx.y selects the
+// child (the children are independent: each reads only its parent).
+template <int D>
+__global__ void k_init_mc_list(const DevPatch* __restrict__ PT, const int* __restrict__ children) {
+  init_mc<D>(PT, children[blockIdx.y]);
+}
+
 // Contiguous device-to-device copies in one launch: blockIdx.y selects the
 // span (CopyQToQold of every patch, the stash of the refined patches).
 struct CopySpan {
@@ -160,22 +172,35 @@ __global__ void __launch_bounds__(256) k_copy_spans(const CopySpan* __restrict__
     s.dst[i] = s.src[i];
 }
 
-// TransferOverlap (lib/bsamroutines.f90:1832-1867): the new grid T takes the
-// old grid S's q on the interior cells both cover, in global indices.  S is a
-// record of the stash (its fields point into the stash's copy).
+// TransferOverlap (lib/bsamroutines.f90:1832-1867): the new grid takes the
+// stashed old grid's q on the interior cells both cover, in global indices.
+// One TransferOverlap of a regrid: the stashed old grid S (its record by
+// value), the new grid `target`, the overlap's extent and its first cell in
+// each grid's index space.
+struct TransferTask {
+  DevPatch S;
+  int32_t target;
+  int32_t n[3], si[3], ti[3];
+};
+
+// The transfers of a regrid in one launch (blockIdx.y selects the task).  Two
+// tasks with the same target never overlap: the old grids of a level are
+// disjoint.
 template <int D>
-__global__ void k_transfer(const DevPatch* __restrict__ PT, int target, DevPatch S, int n0,
-                           int n1, int n2, int si0, int si1, int si2, int ti0, int ti1, int ti2) {
-  const DevPatch T = PT[target];
+__global__ void k_transfer_list(const DevPatch* __restrict__ PT,
+                                const TransferTask* __restrict__ tasks) {
+  const TransferTask& t = tasks[blockIdx.y];
+  const DevPatch T = PT[t.target];
+  const int n0 = t.n[0], n1 = t.n[1], n2 = D == 3 ? t.n[2] : 1;
   const int64_t total = (int64_t)n0 * n1 * n2;
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
        e += (int64_t)gridDim.x * blockDim.x) {
     const int a = (int)(e % n0), b = (int)((e / n0) % n1);
     const int c = D == 3 ? (int)(e / ((int64_t)n0 * n1)) : 0;
-    const int64_t ts = cidx(T, ti0 + a, ti1 + b, D == 3 ? ti2 + c : 0);
-    const int64_t ss = cidx(S, si0 + a, si1 + b, D == 3 ? si2 + c : 0);
+    const int64_t ts = cidx(T, t.ti[0] + a, t.ti[1] + b, D == 3 ? t.ti[2] + c : 0);
+    const int64_t ss = cidx(t.S, t.si[0] + a, t.si[1] + b, D == 3 ? t.si[2] + c : 0);
 #pragma unroll
-    for (int v = 0; v < 2; ++v) fld<double>(T.q[v])[ts] = fld<double>(S.q[v])[ss];
+    for (int v = 0; v < 2; ++v) fld<double>(T.q[v])[ts] = fld<double>(t.S.q[v])[ss];
   }
 }
 

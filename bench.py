@@ -462,11 +462,28 @@ def run_ours(args, world, rank, local):
 def run_case(args):
     """Small fixed cases for ncu captures (no timing is reported):
     smooth2-small  128 problems of 256^2, mixed, one eager tick;
-    ticks          the full 512-problem workload, mixed, three eager ticks."""
+    ticks          the full 512-problem workload, mixed, three eager ticks;
+    amr2           the 2D AMR workload with sustained refinement (256^2 root,
+                   two refined levels, regridded every step), FP64, three
+                   steps in the native driver."""
     from bsam_b200 import batch as BB
     from bsam_b200 import build as BLD
     from bsam_b200 import workloads as W
     BLD.build()
+    if args.case == "amr2":
+        from bsam_b200 import amr as AMR
+        import ctypes
+        from bsam_b200 import Tuning, lib
+        hier, prm = AMR.config2(sustained=True)
+        with AMR.AmrRun(hier, prm) as r:
+            # The V-cycle loop as host-issued launches (the same kernels as
+            # its graph), so that a profiler lists them one by one.
+            t = Tuning(fuse_min_n=64, graph=-1)
+            assert lib().bsam_gpu_set_tuning(r.b.h, ctypes.byref(t)) == 0
+            nv = [r.step()[0] for _ in range(3)]
+            print(json.dumps({"case": args.case, "vcycles": nv, "patches": len(r.descs)}),
+                  flush=True)
+        return 0
     if args.case == "smooth2-small":
         probs = [W.seeded(2, 256, 0.01, 10, seed=500 + p, cbar=0.5, amp=0.025) for p in range(128)]
         nticks = 1
@@ -498,7 +515,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--quick", action="store_true", help="skip the side-by-side forms")
-    ap.add_argument("--case", choices=["smooth2-small", "ticks"], default=None,
+    ap.add_argument("--case", choices=["smooth2-small", "ticks", "amr2"], default=None,
                     help="run a fixed small case for a profiler capture and exit")
     args = ap.parse_args()
     if args.case:

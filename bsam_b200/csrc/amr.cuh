@@ -398,6 +398,95 @@ __global__ void k_setbc_list(const DevPatch* __restrict__ PT, const int* __restr
   }
 }
 
+// The k_setbc_list rule at one cell (g0, g1, g2) of patch P.
+template <int D>
+__device__ __forceinline__ void setbc_cell(const DevPatch& P, int g0, int g1, int g2) {
+  const int co[3] = {g0, g1, g2};
+  int src[3] = {g0, g1, g2};
+  int codes[3] = {BC_NONE, BC_NONE, BC_NONE};
+  bool write = false;
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    if (co[d] == 0 && P.bc[2 * d] != BC_NONE) {
+      src[d] = 1;
+      codes[d] = P.bc[2 * d];
+      write = true;
+    } else if (co[d] == P.n[d] + 1 && P.bc[2 * d + 1] != BC_NONE) {
+      src[d] = P.n[d];
+      codes[d] = P.bc[2 * d + 1];
+      write = true;
+    }
+  }
+  if (!write) return;
+#pragma unroll
+  for (int v = 0; v < 2; ++v) {
+    double* q = fld<double>(P.q[v]);
+    double val = q[cidx(P, src[0], src[1], src[2])];
+#pragma unroll
+    for (int d = 0; d < D; ++d)
+      if (codes[d] != BC_NONE) val = bc_map<double>(codes[d], val);
+    q[cidx(P, co[0], co[1], co[2])] = val;
+  }
+}
+
+// The 2D ring cell g of a patch with m1 x m2 interior cells, in k_interp2's
+// enumeration (bottom row, top row, left column, right column).
+__device__ __forceinline__ void ring2(int g, int m1, int m2, int& gi, int& gj) {
+  if (g < m1 + 2) {
+    gi = g;
+    gj = 0;
+  } else if (g < 2 * (m1 + 2)) {
+    gi = g - (m1 + 2);
+    gj = m2 + 1;
+  } else if (g < 2 * (m1 + 2) + m2) {
+    gi = 0;
+    gj = g - 2 * (m1 + 2) + 1;
+  } else {
+    gi = m1 + 1;
+    gj = g - 2 * (m1 + 2) - m2 + 1;
+  }
+}
+
+// SetGhost of a 2D refined level in one launch, one CTA per patch: the
+// patch's coarse-fine interpolation (k_interp2), then the sibling copies into
+// its ring (k_overlap, the entries whose dst is this patch: ranges[b] =
+// {first, count} into the list sorted by dst), then its physical faces
+// (k_setbc_list).  Each step writes only this patch's ring and reads the
+// parent, this patch, and siblings' interiors, which no CTA writes here, so
+// the CTA barrier between the steps orders everything that depends on them.
+__global__ void k_ghost2(const DevPatch* __restrict__ PT, const int* __restrict__ patches,
+                         const OverlapCopy* __restrict__ cps, const int2* __restrict__ ranges,
+                         int ipass) {
+  const DevPatch P = PT[patches[blockIdx.x]];
+  const DevPatch R = PT[P.parent];
+  const int m1 = P.n[0], m2 = P.n[1];
+  const int nring = 2 * (m1 + 2) + 2 * m2;
+  for (int g = threadIdx.x; g < nring; g += blockDim.x) {
+    int gi, gj;
+    ring2(g, m1, m2, gi, gj);
+    interp2_ghost(P, R, ipass, gi, gj);
+  }
+  __syncthreads();
+  const int2 rg = ranges[blockIdx.x];
+  for (int c = rg.x; c < rg.x + rg.y; ++c) {
+    const OverlapCopy o = cps[c];
+    const DevPatch S = PT[o.src];
+    const int w = o.i1 - o.i0 + 1, hgt = o.j1 - o.j0 + 1;
+    for (int e = threadIdx.x; e < w * hgt; e += blockDim.x) {
+      const int i = o.i0 + e % w, j = o.j0 + e / w;
+#pragma unroll
+      for (int v = 0; v < 2; ++v)
+        fld<double>(P.q[v])[cidx(P, i, j, 0)] = fld<double>(S.q[v])[cidx(S, i + o.di, j + o.dj, 0)];
+    }
+  }
+  __syncthreads();
+  for (int g = threadIdx.x; g < nring; g += blockDim.x) {
+    int gi, gj;
+    ring2(g, m1, m2, gi, gj);
+    setbc_cell<2>(P, gi, gj, 0);
+  }
+}
+
 // FillDownLevel for the solution (afas:241-310): parent%q(mb) = Restriction(q)
 // over the footprint tiles of a level (q only; ghosts of a physical parent by
 // write-through, those of a refined parent by its SetGhost afterwards).  The

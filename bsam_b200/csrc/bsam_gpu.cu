@@ -61,6 +61,10 @@ struct LevelPlan {
   int nplist = 0;
   OverlapCopy* d_ovl = nullptr; // GhostOverlap transfers (ApplyOnLevelPairs order)
   int novl = 0;
+  // The same transfers grouped by destination, and per entry of d_plist the
+  // {first, count} of its group (the one-launch SetGhost of 2D levels).
+  OverlapCopy* d_ovl_by_dst = nullptr;
+  int2* d_ovl_range = nullptr;
   // Parent of a refined level: its children do not cover it, so the
   // snapshot qs is a full copy of q taken after restriction + SetGhost.
   bool snap = false;
@@ -233,22 +237,22 @@ void launch_transfer_t(bsam_gpu* h, const LevelPlan& L, int what) {
 }
 
 // SetGhost(level, ipass) of a refined level (boundary.f90:58-89): coarse-fine
-// interpolation, sibling exchange, physical faces -- three ordered launches.
+// interpolation, sibling exchange, physical faces -- one launch in 2D (a CTA
+// per patch runs the three in order), three ordered launches in 3D.
 // Levels at and below the root keep their ghosts by write-through.
 void amr_ghost(bsam_gpu* h, int level, int ipass) {
   if (level < h->minlevel || level > h->finestlevel) return;
   const LevelPlan& L = plan(h, level);
   if (!L.amr) return;
   if (h->rp.ndims == 2) {
-    k_interp2<<<L.nplist, 128, 0, h->stream>>>(h->d_patches, L.d_plist, ipass);
-    if (L.novl) k_overlap<<<L.novl, 128, 0, h->stream>>>(h->d_patches, L.d_ovl);
-    k_setbc_list<2><<<L.nplist, 128, 0, h->stream>>>(h->d_patches, L.d_plist);
+    k_ghost2<<<L.nplist, 128, 0, h->stream>>>(h->d_patches, L.d_plist, L.d_ovl_by_dst,
+                                              L.d_ovl_range, ipass);
   } else {
     k_interp3<<<L.nplist, 256, 0, h->stream>>>(h->d_patches, L.d_plist, ipass);
     if (L.novl) k_overlap<<<L.novl, 256, 0, h->stream>>>(h->d_patches, L.d_ovl);
     k_setbc_list<3><<<L.nplist, 256, 0, h->stream>>>(h->d_patches, L.d_plist);
   }
-  h->stats.launches += L.novl ? 3 : 2;
+  h->stats.launches += h->rp.ndims == 2 ? 1 : (L.novl ? 3 : 2);
 }
 
 // GetCoarseGhostPoints for the children of a partly covered level: the
@@ -990,6 +994,23 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
     span_plist[li].second = (int)plist_all.size() - span_plist[li].first;
     span_ovl[li].second = (int)ovl_all.size() - span_ovl[li].first;
   }
+  // Per level: the overlap transfers grouped by destination (stable), with
+  // each patch-list entry's {first, count} relative to the level's group.
+  std::vector<OverlapCopy> ovl_by_dst(ovl_all.size());
+  std::vector<int2> ovl_range(plist_all.size(), make_int2(0, 0));
+  for (size_t li = 0; li < nl; ++li) {
+    const int p0 = span_plist[li].first, np = span_plist[li].second;
+    const int o0 = span_ovl[li].first, no = span_ovl[li].second;
+    int at = o0;
+    for (int k = 0; k < np; ++k) {
+      const int dst = plist_all[p0 + k];
+      const int first = at;
+      for (int c = o0; c < o0 + no; ++c)
+        if (ovl_all[c].dst == dst) ovl_by_dst[at++] = ovl_all[c];
+      ovl_range[p0 + k] = make_int2(first - o0, at - first);
+    }
+    if (at != o0 + no) return fail(h, BSAM_ERR_ARG, "an overlap names no patch of its level");
+  }
   h->max_items = std::max(1, h->nmaster);
   for (size_t li = 0; li < nl; ++li) {
     LevelPlan& L = h->levels[li];
@@ -1034,6 +1055,8 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
     const size_t o_items = place(sizeof(Item) * all.size());
     const size_t o_plist = place(sizeof(int) * plist_all.size());
     const size_t o_ovl = place(sizeof(OverlapCopy) * ovl_all.size());
+    const size_t o_ovl_dst = place(sizeof(OverlapCopy) * ovl_by_dst.size());
+    const size_t o_ovl_rng = place(sizeof(int2) * ovl_range.size());
     const size_t o_qold = place(sizeof(CopySpan) * qold_spans.size());
     const size_t o_maps = place(sizeof(CUtensorMap) * maps.size());
     const size_t o_tops = place(sizeof(int) * tops.size());
@@ -1062,6 +1085,12 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
       LevelPlan& L = h->levels[li];
       L.d_plist = h->d_plist ? h->d_plist + span_plist[li].first : nullptr;
       L.d_ovl = h->d_ovl ? h->d_ovl + span_ovl[li].first : nullptr;
+      L.d_ovl_by_dst = ovl_by_dst.empty()
+                           ? nullptr
+                           : reinterpret_cast<OverlapCopy*>(base + o_ovl_dst) + span_ovl[li].first;
+      L.d_ovl_range = ovl_range.empty()
+                          ? nullptr
+                          : reinterpret_cast<int2*>(base + o_ovl_rng) + span_plist[li].first;
       L.d_fine = h->d_items + spans_fine[li].first;
       L.d_coarse = h->d_items + spans_coarse[li].first;
       L.d_fused = h->d_items + spans_fused[li].first;
@@ -1078,6 +1107,8 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
     put(o_items, all.data(), sizeof(Item) * all.size());
     put(o_plist, plist_all.data(), sizeof(int) * plist_all.size());
     put(o_ovl, ovl_all.data(), sizeof(OverlapCopy) * ovl_all.size());
+    put(o_ovl_dst, ovl_by_dst.data(), sizeof(OverlapCopy) * ovl_by_dst.size());
+    put(o_ovl_rng, ovl_range.data(), sizeof(int2) * ovl_range.size());
     put(o_qold, qold_spans.data(), sizeof(CopySpan) * qold_spans.size());
     put(o_maps, maps.data(), sizeof(CUtensorMap) * maps.size());
     put(o_tops, tops.data(), sizeof(int) * tops.size());
@@ -1356,6 +1387,22 @@ int bsam_gpu_errflags(bsam_gpu* h, int patch, double tol, uint8_t* flags) {
   return BSAM_OK;
 }
 
+// Copies a host task list into the handle's task buffer (grown, never
+// shrunk) on the stream; the caller synchronises before the next upload.
+static int upload_tasks(bsam_gpu* h, const void* src, size_t bytes) {
+  if (bytes > h->regrid_cap) {
+    if (h->d_regrid) cudaFree(h->d_regrid);
+    h->d_regrid = nullptr;
+    h->regrid_cap = 0;
+    const size_t want = bytes + bytes / 2;
+    if (cudaMalloc(&h->d_regrid, want) != cudaSuccess)
+      return fail(h, BSAM_ERR_NOMEM, "task buffer allocation failed");
+    h->regrid_cap = want;
+  }
+  if (bytes) CU(cudaMemcpyAsync(h->d_regrid, src, bytes, cudaMemcpyHostToDevice, h->stream));
+  return BSAM_OK;
+}
+
 int bsam_gpu_errflags_level(bsam_gpu* h, int level, double tol, uint8_t* flags) {
   if (!h || !h->have_hierarchy || !flags) return BSAM_ERR_ARG;
   if (level < 0 || level > h->finestlevel)
@@ -1374,16 +1421,24 @@ int bsam_gpu_errflags_level(bsam_gpu* h, int level, double tol, uint8_t* flags) 
       return fail(h, BSAM_ERR_NOMEM, "flag buffer allocation failed");
     h->flags_cap = total;
   }
-  size_t off = 0;
+  // One launch over the level: a task per patch (offset into the flags).
+  std::vector<FlagTask> tasks;
+  size_t off = 0, ncell_max = 0;
   for (int p = 0; p < h->nuser; ++p) {
     if (h->desc[p].level != level) continue;
     const size_t ncell = (size_t)cells_of(h->hp[p].n, nd);
-    const int blocks = (int)std::min<size_t>((ncell + 255) / 256, 4096);
-    if (nd == 2) k_errflags<2><<<blocks, 256, 0, h->stream>>>(h->d_patches, p, tol, h->d_flags + off);
-    else k_errflags<3><<<blocks, 256, 0, h->stream>>>(h->d_patches, p, tol, h->d_flags + off);
-    ++h->stats.launches;
+    tasks.push_back(FlagTask{(int64_t)off, p, 0});
+    ncell_max = std::max(ncell_max, ncell);
     off += ncell;
   }
+  if (tasks.size() > 65535) return fail(h, BSAM_ERR_ARG, "errflags_level: too many patches");
+  const int rc = upload_tasks(h, tasks.data(), sizeof(FlagTask) * tasks.size());
+  if (rc) return rc;
+  const dim3 g((unsigned)std::min<size_t>((ncell_max + 255) / 256, 1024), (unsigned)tasks.size());
+  const FlagTask* d_tasks = reinterpret_cast<const FlagTask*>(h->d_regrid);
+  if (nd == 2) k_errflags_list<2><<<g, 256, 0, h->stream>>>(h->d_patches, d_tasks, tol, h->d_flags);
+  else k_errflags_list<3><<<g, 256, 0, h->stream>>>(h->d_patches, d_tasks, tol, h->d_flags);
+  ++h->stats.launches;
   CU(cudaGetLastError());
   CU(cudaMemcpyAsync(flags, h->d_flags, total, cudaMemcpyDeviceToHost, h->stream));
   CU(cudaStreamSynchronize(h->stream));

@@ -18,8 +18,8 @@ namespace bsam {
 
 // Flags (1:mx)^d of patch P, column-major, one byte per cell.
 template <int D>
-__global__ void k_errflags(const DevPatch* __restrict__ PT, int patch, double tol,
-                           uint8_t* __restrict__ flags) {
+__device__ void errflags_patch(const DevPatch* __restrict__ PT, int patch, double tol,
+                               uint8_t* __restrict__ flags) {
   const DevPatch P = PT[patch];
   const double* c = fld<double>(P.q[0]);
   const int n0 = P.n[0], n1 = P.n[1], n2 = D == 3 ? P.n[2] : 1;
@@ -38,6 +38,26 @@ __global__ void k_errflags(const DevPatch* __restrict__ PT, int patch, double to
     }
     flags[e] = fabs(sqrt(s)) > tol ? 1 : 0;
   }
+}
+
+template <int D>
+__global__ void k_errflags(const DevPatch* __restrict__ PT, int patch, double tol,
+                           uint8_t* __restrict__ flags) {
+  errflags_patch<D>(PT, patch, tol, flags);
+}
+
+// The flags of several patches in one launch: blockIdx.y selects the patch
+// and its offset in the concatenated flag array.
+struct FlagTask {
+  int64_t off;
+  int32_t patch, pad_;
+};
+
+template <int D>
+__global__ void k_errflags_list(const DevPatch* __restrict__ PT, const FlagTask* __restrict__ tasks,
+                                double tol, uint8_t* __restrict__ flags) {
+  const FlagTask t = tasks[blockIdx.y];
+  errflags_patch<D>(PT, t.patch, tol, flags + t.off);
 }
 
 // The linear-prolongation weights of fine index I from coarse (qc) indices

@@ -448,7 +448,7 @@ def run_ours(args, world, rank, local):
                 "tag_threshold": "|grad phi| > %.2f/eps" % (0.25 if sustained else 0.5)}
         # Served form: one rate point of the Poisson request stream.
         stream_ = W.config5(120, 200.0)
-        with SV.Server(pool_bytes=32 << 30, max_slots=256, ticks=4) as srv:
+        with SV.Server(pool_bytes=32 << 30, max_slots=256, ticks=4, amr_workers=8) as srv:
             reqs = srv.serve(stream_)
         extra["served_rate_200"] = SV.summarize(reqs)
         line["forms"] = extra

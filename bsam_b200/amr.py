@@ -661,6 +661,7 @@ class AmrRun:
         res = ctypes.c_double(0.0)
         _check(lib().bsam_amr_step(self.a, ctypes.byref(nv), ctypes.byref(res),
                                    ctypes.byref(conv)), self.b.h, "amr_step")
+        self.converged = conv.value
         n = lib().bsam_amr_table(self.a, None, 0)
         arr = (PatchDesc * n)()
         lib().bsam_amr_table(self.a, arr, n)
@@ -722,3 +723,38 @@ def config2(sustained: bool = False, seed: int = 2):
     tol = [k * (1.0 / 256) / 0.005, k * (1.0 / 512) / 0.005]
     return hier, RegridParams(maxlevel=2, qtolerance=tol, ibuffer=[1, 1], desfill=[0.9, 0.9],
                               mgp=[8, 8])
+
+
+def request_params(n_root: int, eps: float, maxlevel: int) -> RegridParams:
+    """Regridding of a served AMR request: the AMR workload's settings on an
+    n_root^2 root (tag threshold |grad phi| > 0.5/eps, qtolerance = 0.5 h /
+    eps per level; ibuffer 1, desiredfillratios 0.9, minimumgridpoints 8)."""
+    tol = [0.5 * (1.0 / (n_root * 2 ** l)) / eps for l in range(maxlevel)]
+    return RegridParams(maxlevel=maxlevel, qtolerance=tol, ibuffer=[1] * maxlevel,
+                        desfill=[0.9] * maxlevel, mgp=[8] * maxlevel)
+
+
+def solve_request(prob, device: int = 0, keep_q: bool = False) -> dict:
+    """One served 2D request with refined levels (prob.maxlevel >= 1): the
+    circular drop seeded by prob.seed on a prob.mx[0]^2 root, prob.nsteps
+    time steps regridded every step in the native driver (FP64).  Returns the
+    per-step V-cycles, residuals and convergence flags, the largest patch
+    count, and (keep_q) the final q of every patch on a level >= 0."""
+    n = int(prob.mx[0])
+    hier = build(n, [], eps=float(prob.eps), dt=float(prob.dt), qerrortol=float(prob.qerrortol),
+                 field="drop", seed=int(prob.seed), maxvcycles=int(prob.maxvcycles))
+    nsteps = int(prob.nsteps)
+    nvc = np.zeros(nsteps, dtype=np.int32)
+    res = np.zeros(nsteps)
+    conv = np.zeros(nsteps, dtype=np.int32)
+    most = 0
+    with AmrRun(hier, request_params(n, float(prob.eps), int(prob.maxlevel)), device) as r:
+        for k in range(nsteps):
+            nvc[k], res[k] = r.step()
+            conv[k] = r.converged
+            most = max(most, len(r.descs))
+        out = {"nvcycles": nvc, "residual": res, "converged": conv, "patches_max": most}
+        if keep_q:
+            out["q"] = r.state()
+            out["descs"] = list(r.descs)
+    return out

@@ -10,17 +10,26 @@ are advanced together, a few V-cycle ticks per engine launch; every loop the
 server collects what has finished and admits what now fits, so requests that
 arrive while others are on the GPU join the running batch.
 
+2D requests with refined levels (regridded every step) go to a small pool
+of worker threads instead, each solving one request at a time through the
+native AMR driver on its own engine handle and stream (amr.solve_request),
+beside the batches.
+
 A result depends only on its own request: the batch engine computes every
-problem exactly as it would alone (tests/test_gpu_serve.py checks it).
+problem exactly as it would alone, and an AMR request is solved exactly as
+amr.solve_request solves it alone (tests/test_gpu_serve.py checks both).
 """
 from __future__ import annotations
 
 import dataclasses
+import queue
+import threading
 import time
 from collections import deque
 
 import numpy as np
 
+from . import amr as AMR
 from . import batch as BB
 
 
@@ -48,7 +57,8 @@ class Server:
 
     def __init__(self, pool_bytes: int, precision: int = BB.PREC_MIXED, max_slots: int = 256,
                  share_2d: float = 0.5, ticks: int = 4, qerrortol: float = 1e-8,
-                 maxvcycles: int = 20, device: int = 0, keep_q: bool = False):
+                 maxvcycles: int = 20, device: int = 0, keep_q: bool = False,
+                 amr_workers: int = 2):
         p2 = int(pool_bytes * share_2d)
         self.engines = {
             2: BB.Batch(2, precision=precision, max_slots=max_slots, pool_bytes=p2,
@@ -59,6 +69,8 @@ class Server:
         }
         self.ticks = ticks
         self.keep_q = keep_q
+        self.device = device
+        self.amr_workers = amr_workers
 
     def close(self):
         for e in self.engines.values():
@@ -71,6 +83,8 @@ class Server:
         self.close()
 
     def fits_alone(self, prob) -> bool:
+        if getattr(prob, "maxlevel", 0) >= 1:
+            return True  # solved on its own handle, outside the pools
         e = self.engines[prob.ndims]
         return e.footprint(prob) <= e.stats()["pool_bytes"]
 
@@ -87,10 +101,39 @@ class Server:
         t0 = time.perf_counter()
         now = 0.0
         running = {2: 0, 3: 0}
-        while nxt < len(reqs) or pending or inflight:
+        # AMR requests: FIFO to the worker threads.
+        amr_q: queue.Queue = queue.Queue()
+        amr_left = [sum(1 for r in reqs if getattr(r.prob, "maxlevel", 0) >= 1)]
+        errors = []
+        lock = threading.Lock()
+
+        def worker():
+            while True:
+                r = amr_q.get()
+                if r is None:
+                    return
+                try:
+                    r.admitted = time.perf_counter() - t0
+                    r.result = AMR.solve_request(r.prob, self.device, keep_q=self.keep_q)
+                    r.finished = time.perf_counter() - t0
+                except Exception as exc:  # reported by serve() after the stream
+                    errors.append(exc)
+                with lock:
+                    amr_left[0] -= 1
+
+        threads = [threading.Thread(target=worker, daemon=True)
+                   for _ in range(self.amr_workers if amr_left[0] else 0)]
+        for th in threads:
+            th.start()
+        while nxt < len(reqs) or pending or inflight or amr_left[0] > 0:
+            if errors:
+                break
             now = time.perf_counter() - t0
             while nxt < len(reqs) and reqs[nxt].arrival <= now:
-                pending.append(reqs[nxt])
+                if getattr(reqs[nxt].prob, "maxlevel", 0) >= 1:
+                    amr_q.put(reqs[nxt])
+                else:
+                    pending.append(reqs[nxt])
                 nxt += 1
             # Admission: FIFO per engine (a full engine does not block the other).
             blocked = set()
@@ -128,7 +171,25 @@ class Server:
                     time.sleep(min(wait, 0.01))
             elif not done_any:
                 time.sleep(50e-6)
+        for _ in threads:
+            amr_q.put(None)
+        for th in threads:
+            th.join()
+        if errors:
+            raise errors[0]
         return reqs
+
+
+def _split_latency(reqs: list) -> dict:
+    """p50 / p99 latency of the requests with refined levels and of the rest."""
+    out = {}
+    for name, sel in (("amr", lambda r: getattr(r.prob, "maxlevel", 0) >= 1),
+                      ("uniform", lambda r: getattr(r.prob, "maxlevel", 0) < 1)):
+        lat = np.array([r.latency for r in reqs if sel(r)])
+        if lat.size:
+            out[f"{name}_p50_ms"] = float(np.percentile(lat, 50) * 1e3)
+            out[f"{name}_p99_ms"] = float(np.percentile(lat, 99) * 1e3)
+    return out
 
 
 def summarize(reqs: list) -> dict:
@@ -148,4 +209,6 @@ def summarize(reqs: list) -> dict:
         "vcycles": vcycles,
         "makespan_s": makespan,
         "all_converged": conv,
+        "amr_requests": sum(1 for r in reqs if getattr(r.prob, "maxlevel", 0) >= 1),
+        **_split_latency(reqs),
     }

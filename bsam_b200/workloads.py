@@ -60,6 +60,10 @@ class Problem:
     seed: int | None = None
     cbar: float = 0.5
     amp: float = 0.0
+    # Refined levels regridded every step (served AMR requests, 2D): the
+    # initial state is then the circular drop of the AMR workload, seeded by
+    # `seed` (bsam_b200.amr.build), not the seeded uniform form above.
+    maxlevel: int = 0
 
     @property
     def h(self) -> float:
@@ -88,15 +92,17 @@ def config5(nreq: int, rate: float, seed: int = 5) -> list:
     """Serving stream: Poisson arrivals at `rate` per second; 70 % 2D with
     side in {64, 128, 256, 512}, 30 % 3D with side in {32, 64, 128}; steps
     uniform in 1..50; eps ~ U(0.005, 0.02); dt = 1e-4; c0 = 0.5 + 0.025
-    U(-1, 1) (seeded per request); residual 1e-8.  Returns (arrival_s,
-    Problem) pairs in arrival order.  AMR levels of 2D requests are not drawn:
-    requests run on their uniform root grid."""
+    U(-1, 1) (seeded per request); residual 1e-8.  A 2D request has 0, 1 or
+    2 refined levels (uniform); one with refined levels starts from the
+    circular drop of the AMR workload and regrids every step.  Returns
+    (arrival_s, Problem) pairs in arrival order."""
     gaps = -np.log(1.0 - uniform(seed, nreq, 0.0, 1.0)) / rate
     arrival = np.cumsum(gaps)
     is3 = uniform(seed + 1, nreq, 0.0, 1.0) < 0.3
     pick = splitmix64(seed + 2, nreq)
     steps = 1 + (splitmix64(seed + 3, nreq) % np.uint64(50)).astype(np.int64)
     eps = uniform(seed + 4, nreq, 0.005, 0.02)
+    levels = (splitmix64(seed + 5, nreq) % np.uint64(3)).astype(np.int64)
     out = []
     for r in range(nreq):
         if is3[r]:
@@ -105,6 +111,8 @@ def config5(nreq: int, rate: float, seed: int = 5) -> list:
             n, nd = (64, 128, 256, 512)[int(pick[r] % np.uint64(4))], 2
         p = seeded(nd, n, float(eps[r]), int(steps[r]), seed=7919 * (seed + 1) + r,
                    cbar=0.5, amp=0.025)
+        if nd == 2:
+            p.maxlevel = int(levels[r])
         out.append((float(arrival[r]), p))
     return out
 

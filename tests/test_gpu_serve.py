@@ -78,3 +78,29 @@ def test_serve_admission_waits_for_memory(gpu_lib):
     waited = [r for r in reqs if r.admitted - r.arrival > 1e-4]
     assert waited, "expected some requests to wait for pool memory"
     assert SV.summarize(reqs)["all_converged"]
+
+
+def test_serve_amr_requests_same_alone(gpu_lib):
+    """2D requests with refined levels run beside the batches (worker threads,
+    native AMR driver): each result equals the same request solved alone, bit
+    for bit, and the batch requests of the mix still converge."""
+    stream = small_stream(8, rate=3000.0)
+    amr_ids = (1, 4, 6)
+    for rid in amr_ids:
+        p = stream[rid][1]
+        p.maxlevel = 1 + rid % 2
+        p.nsteps = 3
+    with SV.Server(pool_bytes=2 << 30, max_slots=32, ticks=2, keep_q=True,
+                   amr_workers=2) as srv:
+        reqs = srv.serve(stream)
+    summ = SV.summarize(reqs)
+    assert summ["all_converged"] and summ["amr_requests"] == len(amr_ids), summ
+    from bsam_b200 import amr
+    for rid in amr_ids:
+        r = reqs[rid]
+        ref = amr.solve_request(r.prob, keep_q=True)
+        for k in ("nvcycles", "residual", "converged"):
+            assert np.array_equal(r.result[k], ref[k]), (rid, k)
+        assert r.result["descs"] == ref["descs"]
+        for (i, q), (j, qr) in zip(r.result["q"], ref["q"]):
+            assert i == j and np.array_equal(q, qr), (rid, i)

@@ -158,3 +158,17 @@ def test_after_step_stats_oracle(oracle):
         assert e == pytest.approx((e_fine - e_foot) + e_root, rel=1e-13)
     finally:
         b.close()
+
+
+def test_served_stream_draws_refined_levels():
+    """The served workload gives 2D requests 0, 1 or 2 refined levels and 3D
+    requests none, reproducibly."""
+    from bsam_b200 import workloads as W
+    a = W.config5(200, 100.0)
+    b = W.config5(200, 100.0)
+    assert [p.maxlevel for _, p in a] == [p.maxlevel for _, p in b]
+    lv2 = {p.maxlevel for _, p in a if p.ndims == 2}
+    assert lv2 == {0, 1, 2}
+    assert all(p.maxlevel == 0 for _, p in a if p.ndims == 3)
+    prm = amr.request_params(128, 0.01, 2)
+    assert prm.qtolerance == [0.5 / 128 / 0.01, 0.5 / 256 / 0.01]

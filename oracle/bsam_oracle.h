@@ -15,10 +15,15 @@
  * SetBC/UserBC, Interpolate2D) and their composition, MultigridIterations
  * with the V-cycle, SetGhost, FillDown and ErrorAFAS (afasroutines.f90,
  * boundary.f90), on uniform 2D / 3D hierarchies and a 2D hierarchy with two
- * refined levels.  Restated rather than interpreted on both sides: TreeOps'
- * level traversal order and TakeTimeSteps' step sequence on an unchanged
- * hierarchy (bsamroutines.f90:632-723); the regridding itself is not on the
- * path.  The interpreter evaluates as the Fortran text reads, with no fused
+ * refined levels; and the regridding leaves: SetErrFlagsUser2D/3D, the
+ * mass-corrected prolongation of InitFields, NewSubGrids (Berger-Rigoutsos)
+ * and, in oracle/pyoracle.py, BufferAndList + InflateEdgeTags.  Restated
+ * rather than interpreted on both sides: TreeOps' level traversal order,
+ * TakeTimeSteps' step sequence, and the regridding composition (AMR,
+ * EstimateLevelErrors, GridAdapt with MakeNewGrid's geometry and
+ * TransferValues; bsamroutines.f90:632-723, 939-1002, 1299-1350, 1582-1867),
+ * which the engine and the oracle run through one driver.  The interpreter
+ * evaluates as the Fortran text reads, with no fused
  * multiply-add; a reference build that contracts a*b+c into FMA would differ
  * from it in the last bits.
  *

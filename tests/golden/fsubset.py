@@ -23,9 +23,12 @@ ApplyOnLevelPairs (each grid with every later one) and GetParentInfo
 (lib/treeops.f90:536-610) over it.  Records are Python objects whose
 attributes are the nodeinfo components.  A caller may also stand in for a
 called routine (`stubs`: MakeNewGrid, to record the boxes NewSubGrids makes).
-Also covered: DO WHILE, WHERE without ELSEWHERE, ALLOCATE / DEALLOCATE of
-integer arrays.  Not supported (and not needed): character data, implicit
-typing, pointer assignment.
+Also covered: DO WHILE, a DO without loop control (left by EXIT), WHERE
+without ELSEWHERE, ALLOCATE / DEALLOCATE of integer arrays, and the pointer
+statements of a linked list of derived-type scalars: ALLOCATE of a pointer
+(a new record from the caller's factory for that variable, `derived`),
+pointer assignment `p => q`, NULLIFY and ASSOCIATED.  Not supported (and not
+needed): character data, implicit typing.
 
 Only make_golden.py imports this module, in a container that has the
 reference source; the tests read the fixtures it wrote.
@@ -317,6 +320,7 @@ class Interp:
         self.current = []       # ApplyOnLevel's current record (GetParentInfo)
         self.printed = []       # numeric items of every executed PRINT
         self.stubs = {}         # name -> Python callable standing in for a CALL
+        self.derived = {}       # pointer variable -> factory of a new target record
 
     def lookup(self, name, env):
         """A variable, or a component chain a%b%c, from the locals, then the
@@ -438,6 +442,8 @@ class Interp:
         return v
 
     def call_function(self, name, subs, env):
+        if name == "associated":
+            return self.lookup(subs[0][1], env) is not None
         if name == "size":
             a = self.section_actual(subs[0], env)
             d = int(self.ev(subs[1], env)) if len(subs) > 1 else None
@@ -643,6 +649,9 @@ class Interp:
                     env[item.split("=", 1)[1].strip().lower()] = 0
                     continue
                 m = re.match(r"^(\w+)\s*\((.*)\)$", item)
+                if m is None:  # a pointer to a derived-type scalar
+                    self.assign_ref(item.lower(), self.derived[item.lower()](), env)
+                    continue
                 nm, dims = m.group(1).lower(), m.group(2)
                 lbs, shape = [], []
                 for spec in split_top(dims, ","):
@@ -659,6 +668,37 @@ class Interp:
                 item = item.strip()
                 if re.match(r"^stat\s*=", item, re.I):
                     env[item.split("=", 1)[1].strip().lower()] = 0
+            return i + 1
+        if re.match(r"^do\s*$", low):
+            # DO without loop control, left by EXIT.
+            is_do = lambda s: bool(re.match(r"^(\w+\s*:\s*)?do\b", s))
+            is_end = lambda s: bool(re.match(r"^end\s*do\b", s))
+            end, _ = self.find_end(lines, i, is_do, is_end)
+            body = lines[i + 1:end]
+            name = lab.group(1).lower() if lab else None
+            while True:
+                try:
+                    self.exec_block(body, env)
+                except _Cycle as c:
+                    if c.name not in (None, name):
+                        raise
+                except _Exit as e:
+                    if e.name not in (None, name):
+                        raise
+                    return end + 1
+        if re.match(r"^nullify\s*\(", low):
+            inner, _ = split_paren(ln[7:].strip())
+            for item in split_top(inner, ","):
+                self.assign_ref(item.strip().lower(), None, env)
+            return i + 1
+        if "=>" in ln:
+            # Pointer assignment: the left side names the record the right
+            # side names (or none, for null()).
+            lhs_s, rhs_s = (x.strip().lower() for x in ln.split("=>", 1))
+            target = None if rhs_s.replace(" ", "") == "null()" else self.lookup(rhs_s, env)
+            if target is _MISSING:
+                raise NameError(rhs_s)
+            self.assign_ref(lhs_s, target, env)
             return i + 1
         if re.match(r"^do\b", low):
             is_do = lambda s: bool(re.match(r"^(\w+\s*:\s*)?do\b", s))
@@ -782,6 +822,16 @@ class Interp:
             arr = self.lookup(lhs[1], env)
             arr.data[self.index_tuple(arr, lhs[2], env)] = rhs
         return i + 1
+
+    def assign_ref(self, name, target, env):
+        """Makes variable or component `name` refer to `target`."""
+        if "%" in name:
+            owner_s, comp = name.rsplit("%", 1)
+            setattr(self.lookup(owner_s, env), comp, target)
+        elif name in env or name not in self.globals:
+            env[name] = target
+        else:
+            self.globals[name] = target
 
     def apply_on_level(self, level, fn, param, pairs):
         """ApplyOnLevel / ApplyOnLevelPairs (lib/treeops.f90:536-610): fn on

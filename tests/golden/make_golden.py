@@ -17,7 +17,8 @@ the regridding leaves
 
   SetErrFlagsUser2D/3D (problem.f90), Bi/TriLinProlongationP1MC
   (gridutilities.f90), NewSubGrids with GetSignatures and GridFlagRatio
-  (lib/bsamroutines.f90; MakeNewGrid stood in for, recording the boxes)
+  (lib/bsamroutines.f90; MakeNewGrid stood in for, recording the boxes),
+  BufferAndList, InflateEdgeTags and BufferTaggedCells (lib/bsamroutines.f90)
 
 and their composition, the time loop's multigrid solve on fixed hierarchies
 (uniform 2D and 3D, and 2D with refined levels):
@@ -312,6 +313,53 @@ def regrid_cases(rng):
         out[f"subgrids_{n}"] = {"ndims": nd, "flags": fl, "fill": fill, "mgp": mgp,
                                 "boxes": boxes, "nsubgrids": info.nsubgrids}
         print(f"subgrids_{n}", nd, mx, "boxes", len(made))
+    # BufferAndList per patch of a level (ErrFlag, in ApplyOnLevel order),
+    # then InflateEdgeTags over the level, with the tagged-cell list set up as
+    # EstimateLevelErrors does (bsamroutines.f90:985-999).
+    bcases = [(2, 1, [((1, 1), (16, 12)), ((17, 1), (10, 12)), ((5, 25), (20, 14))]),
+              (2, 2, [((1, 1), (16, 12)), ((17, 1), (10, 12)), ((5, 25), (20, 14))]),
+              (3, 1, [((1, 1, 1), (10, 8, 6)), ((11, 1, 1), (6, 8, 6)),
+                      ((3, 13, 9), (8, 6, 10))])]
+    for n, (nd, ib, boxes) in enumerate(bcases):
+        recs, fl_in = [], []
+        for lo, sz in boxes:
+            mx3 = tuple(sz) + (1,) * (3 - nd)
+            fl = (rng.random(mx3) < 0.03).astype(np.int64)
+            fl_in.append(fl.copy())
+            mg = [[lo[k], lo[k] + sz[k] - 1] for k in range(nd)] + [[1, 1]] * (3 - nd)
+            recs.append(F.Record(level=1, tobedeleted=False,
+                                 mx=F.FArray(np.array(mx3, dtype=np.int64), (1,)),
+                                 mglobal=F.FArray(np.array(mg, dtype=np.int64), (1, 1)),
+                                 errorflags=F.FArray(fl.copy(order="F"), (1, 1, 1))))
+        # a flagged cell on the face patches 0 and 1 share
+        recs[0].errorflags.data[(-1,) + (0,) * 2] = 1
+        fl_in[0][(-1,) + (0,) * 2] = 1
+        bsam = F.extract_routines(open(os.path.join(REF, "lib/bsamroutines.f90")).read())
+        routines = {k: bsam[k] for k in ("bufferandlist", "inflateedgetags",
+                                         "buffertaggedcells")}
+        newcell = lambda: F.Record(id=0, coordinate=F.FArray(np.ones(3, dtype=np.int64), (1,)),
+                                   prevcell=None)
+        zeroth = newcell()  # allocate(zerothtaggedcell); nullify(...%prevcell)
+        I = F.Interp(routines, {"ndims": nd, "maxdims": 3,
+                                "ibuffer": F.FArray(np.full(maxdepth + 1, ib, dtype=np.int64),
+                                                    (0,)),
+                                "periodicboundaryconditions": False, "nperiodicoffsets": 0, "err_ok": 0,
+                                "ntaggedcells": 0, "zerothtaggedcell": zeroth,
+                                "lasttaggedcell": zeroth, "currenttaggedcell": None},
+                     tree=Tree(recs))
+        I.derived["currenttaggedcell"] = newcell
+        for r in recs:
+            I.run(I.routines["bufferandlist"], [r.errorflags, r.mglobal, r.mx, 1])
+        if I.globals["ntaggedcells"] > 0:
+            I.run(I.routines["inflateedgetags"], [1])
+        res = {"ndims": nd, "ibuffer": ib, "npatch": len(recs),
+               "ntagged_listed": I.globals["ntaggedcells"]}
+        for k, r in enumerate(recs):
+            res[f"mglobal_{k}"] = r.mglobal.data
+            res[f"flags_in_{k}"] = fl_in[k]
+            res[f"flags_out_{k}"] = r.errorflags.data
+        out[f"buffer_{n}"] = res
+        print(f"buffer_{n}", nd, "ibuffer", ib, "listed", I.globals["ntaggedcells"])
     return out
 
 

@@ -162,3 +162,30 @@ def test_uniform_time_loop_matches_reference(oracle, golden_hier, name):
     assert np.array_equal(ref["nvcycles"], d["nvcycles"])
     assert np.array_equal(ref["trace"], d["trace"])
     assert np.array_equal(ref["q"][-1].ravel(order="F"), d["q_out"])
+
+
+def _buffer_fixture(n):
+    d = np.load(os.path.join(GOLD, f"ref_buffer_{n}.npz"))
+    nd, np_ = int(d["ndims"]), int(d["npatch"])
+    descs, fin, fout = [], [], []
+    for k in range(np_):
+        mg = d[f"mglobal_{k}"]
+        mx = [int(mg[n_][1] - mg[n_][0] + 1) for n_ in range(3)]
+        descs.append({"level": 1, "parent": 0, "mx": mx, "mbounds": [[1, 1]] * 3,
+                      "mglobal": [list(map(int, mg[n_])) for n_ in range(3)],
+                      "mthbc": [999] * 6, "dx": 1.0, "xlower": [0.0] * 3})
+        shp = tuple(mx[:nd])
+        fin.append(d[f"flags_in_{k}"].reshape(shp, order="F"))
+        fout.append(d[f"flags_out_{k}"].reshape(shp, order="F"))
+    return nd, int(d["ibuffer"]), descs, fin, fout
+
+
+@pytest.mark.parametrize("n", [0, 1, 2])
+def test_buffer_flags_match_reference(oracle, n):
+    """BufferAndList + InflateEdgeTags + BufferTaggedCells, interpreted from
+    the reference source over a level of three patches (two sharing a face),
+    against the oracle's restatement."""
+    nd, ib, descs, fin, fout = _buffer_fixture(n)
+    got = oracle.buffer_flags(nd, descs, fin, ib)
+    for g, w in zip(got, fout):
+        assert np.array_equal(g, w)

@@ -172,3 +172,16 @@ def test_served_stream_draws_refined_levels():
     assert all(p.maxlevel == 0 for _, p in a if p.ndims == 3)
     prm = amr.request_params(128, 0.01, 2)
     assert prm.qtolerance == [0.5 / 128 / 0.01, 0.5 / 256 / 0.01]
+
+
+@pytest.mark.parametrize("n", [0, 1, 2])
+def test_buffer_flags_match_reference(gpu_free_lib, n):
+    """bsam_host_buffer_flags against BufferAndList + InflateEdgeTags run from
+    the reference's own source (tests/golden/ref_buffer_*.npz)."""
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    from test_golden_reference import _buffer_fixture
+    nd, ib, descs, fin, fout = _buffer_fixture(n)
+    got = amr.buffer_flags(nd, descs, [f.astype(np.uint8) for f in fin], ib)
+    for g, w in zip(got, fout):
+        assert np.array_equal(g.astype(np.int64), w)

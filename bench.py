@@ -369,8 +369,8 @@ def run_ours(args, world, rank, local):
                    "all_converged": conv_all},
         "roofline": {"bound": "hbm", "kernel": "kb_smooth2<float> (fused finest-depth "
                      "smoothing stages: nu=2 red-black sweeps of every problem, one launch "
-                     "each; the post-smoothing launch also applies the FP64 update "
-                     "q64 += e)",
+                     "each; the post-smoothing launch also applies the coarse-grid "
+                     "correction to its tiles and the FP64 update q64 += e)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None,
                      "peak_source": peak_kind, "traffic": traffic,

@@ -512,7 +512,9 @@ void append_items(bsam_batch* b, int s) {
         for (int x = 0; x < (P.n[0] + tx - 1) / tx; ++x)
           b->lists[L_FUSED + d].h.push_back(Item{rec0 + r, x, y, 0});
     }
-    if (nd == 2)  // blocks (m, n), m = 0..cn0, n = 0..cn1, 32 x TILE_Y per tile
+    // blocks (m, n), m = 0..cn0, n = 0..cn1, 32 x TILE_Y per tile; a fused
+    // record's correction is applied by its post-smoothing stage instead.
+    if (nd == 2 && !P.fused)
       for (int y = 0; y < (P.cn[1] + 1 + TILE_Y - 1) / TILE_Y; ++y)
         for (int x = 0; x < (P.cn[0] + 1 + 31) / 32; ++x)
           b->lists[L_CORR + d].h.push_back(Item{rec0 + r, x, y, 0});
@@ -592,11 +594,11 @@ void tick_t(bsam_batch* b, cudaGraphConditionalHandle handle, int in_graph) {
       const int upd = (b->mixed && d == 0 && dir == 1) ? 1 : 0;
       if (b->mixed)
         kb_smooth2<float, true><<<g, Fused2<float>::THREADS, Fused2<float>::smem(true), s>>>(
-            pt, L[L_FUSED + d].d, cnt + L_FUSED + d, dir, nu, upd, &b->d_ctl->kerr);
+            pt, L[L_FUSED + d].d, cnt + L_FUSED + d, dir, nu, upd, dir, &b->d_ctl->kerr);
       else
         kb_smooth2<double, false>
             <<<g, Fused2<double>::THREADS, Fused2<double>::smem(false), s>>>(
-                pt, L[L_FUSED + d].d, cnt + L_FUSED + d, dir, nu, 0, &b->d_ctl->kerr);
+                pt, L[L_FUSED + d].d, cnt + L_FUSED + d, dir, nu, 0, dir, &b->d_ctl->kerr);
       ++n;
     }
     stage_mark(b, d, false, dir);
@@ -639,9 +641,14 @@ void tick_t(bsam_batch* b, cudaGraphConditionalHandle handle, int in_graph) {
   }
   for (int d = b->cap_depth - 1; d >= 0; --d) {
     if (D == 2) {
-      const int gk = grid_for(b, L_CORR + d);
-      if (b->mixed) kb_correct2<float><<<gk, blk, 0, s>>>(pt, L[L_CORR + d].d, cnt + L_CORR + d);
-      else kb_correct2<double><<<gk, blk, 0, s>>>(pt, L[L_CORR + d].d, cnt + L_CORR + d);
+      // Records with fused stages are corrected by their post-smoothing stage.
+      if (L[L_CORR + d].cap > 0) {
+        const int gk = grid_for(b, L_CORR + d);
+        if (b->mixed) kb_correct2<float><<<gk, blk, 0, s>>>(pt, L[L_CORR + d].d, cnt + L_CORR + d);
+        else kb_correct2<double><<<gk, blk, 0, s>>>(pt, L[L_CORR + d].d, cnt + L_CORR + d);
+      } else {
+        --n;
+      }
     } else {
       const int gf = grid_for(b, L_FINE + d);
       if (b->mixed) kb_correct<float, D><<<gf, blk, 0, s>>>(pt, L[L_FINE + d].d, cnt + L_FINE + d);
@@ -1063,9 +1070,15 @@ int bsam_batch_advance(bsam_batch* b, int max_ticks) {
           b->st.smooth_ms += ms;
           b->st.smooth_stages += 1;
           // Read phi, mu, f1, f2, write phi, mu; the mixed 2D post-smoothing
-          // writes no e but reads and writes the FP64 master (q64 += e).
-          const bool upd = b->mixed && b->bp.ndims == 2 && b->ev_post[e] && !b->tuning.per_pass;
-          b->st.smooth_bytes += (upd ? 4.0 * es + 32.0 : 6.0 * es) * (double)cells0;
+          // writes no e but reads and writes the FP64 master (q64 += e).  A
+          // fused 2D post-smoothing stage also does the coarse-grid
+          // correction, whose algorithmic bytes (read and write q, read the
+          // parent's change: 4 s + 2 s / 4 per cell) it adds.
+          const bool fused_post = b->bp.ndims == 2 && b->ev_post[e] && !b->tuning.per_pass;
+          const bool upd = b->mixed && fused_post;
+          double bytes = upd ? 4.0 * es + 32.0 : 6.0 * es;
+          if (fused_post) bytes += 4.0 * es + 0.5 * es;
+          b->st.smooth_bytes += bytes * (double)cells0;
         }
       }
       b->ev_used = 0;

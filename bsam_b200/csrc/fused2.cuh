@@ -93,6 +93,61 @@ __device__ __forceinline__ void smem_ghosts2(const DevPatch& P, T* s0, T* s1, in
   }
 }
 
+// CorrectFine (afas:842-963) of the cells of a shared tile: every cell of the
+// tile inside the patch's interior takes the bilinear prolongation of the
+// parent's q - qs (the change of the coarse solution), the expression of
+// correct_block2, so the tile holds what kb_correct2 would have written.
+template <class T, class TP>
+__device__ __forceinline__ void correct_tile2(const DevPatch& C, const DevPatch& R, T* s0, T* s1,
+                                              int gx0, int gy0) {
+  constexpr int RX = Fused2<T>::RX, RY = Fused2<T>::RY;
+  const TP* pq0 = fld<TP>(R.q[0]);
+  const TP* pq1 = fld<TP>(R.q[1]);
+  const TP* ps0 = fld<TP>(R.qs[0]);
+  const TP* ps1 = fld<TP>(R.qs[1]);
+  // Coarse blocks (m, n) whose fine cells 2m + {0, 1}, 2n + {0, 1} meet the
+  // tile: the four coarse differences are loaded once per block.
+  const int mlo = (gx0 >= 0 ? gx0 : gx0 - 1) / 2, nlo = (gy0 >= 0 ? gy0 : gy0 - 1) / 2;
+  const int bw = (gx0 + RX - 1) / 2 - mlo + 1, bh = (gy0 + RY - 1) / 2 - nlo + 1;
+  for (int blk = threadIdx.x; blk < bw * bh; blk += blockDim.x) {
+    const int m = mlo + blk % bw, n = nlo + blk / bw;
+    if (m < 0 || m > C.cn[0] || n < 0 || n > C.cn[1]) continue;
+    TP e[2][2][2];  // [component][m + a][n + b]
+#pragma unroll
+    for (int v = 0; v < 2; ++v) {
+      const TP* pq = v ? pq1 : pq0;
+      const TP* ps = v ? ps1 : ps0;
+#pragma unroll
+      for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int bb = 0; bb < 2; ++bb) {
+          const int64_t x = cidx(R, C.off[0] + m + a, C.off[1] + n + bb, 0);
+          e[v][a][bb] = pq[x] - ps[x];
+        }
+    }
+#pragma unroll
+    for (int dy = 0; dy < 2; ++dy) {
+      const int J = 2 * n + dy, sy = J - gy0;
+      if (J < 1 || J > C.n[1] || sy < 0 || sy >= RY) continue;
+#pragma unroll
+      for (int dx = 0; dx < 2; ++dx) {
+        const int I = 2 * m + dx, sx = I - gx0;
+        if (I < 1 || I > C.n[0] || sx < 0 || sx >= RX) continue;
+        TP corr[2];
+#pragma unroll
+        for (int v = 0; v < 2; ++v) {
+          const TP b0 = lin_x<TP>(dx == 0, e[v][0][0], e[v][1][0]);
+          const TP b1 = lin_x<TP>(dx == 0, e[v][0][1], e[v][1][1]);
+          corr[v] = lin_x<TP>(dy == 0, b0, b1) / TP(16);
+        }
+        const int c = sy * RX + sx;
+        s0[c] = s0[c] + T(corr[0]);
+        s1[c] = s1[c] + T(corr[1]);
+      }
+    }
+  }
+}
+
 // dir 0: q -> qb (pre-smoothing); dir 1: qb -> q (post-smoothing).
 // P.tmaps: 2D maps of q0, q1, qb0, qb1, f0, f1, bs (box RX x RY).
 // A copy that has not landed after kWaitPolls polls sets *err and ends the
@@ -104,10 +159,14 @@ __device__ __forceinline__ void smem_ghosts2(const DevPatch& P, T* s0, T* s1, in
 // mixed.cuh (update_item), expression for expression, done here while e is in
 // shared memory.  Every CTA writes only its own tile's cells of the master,
 // which nothing else in the launch reads.
+// corr (post-smoothing): the coarse-grid correction is applied to the tile
+// after it lands (correct_tile2, then the physical face ghosts the passes
+// read), instead of by a kb_correct2 launch before the stage.
 template <class T, bool DELTA>
 __global__ void __launch_bounds__(Fused2<T>::THREADS)
     kb_smooth2(const DevPatch* __restrict__ PT, const Item* __restrict__ items,
-               const int* __restrict__ count, int dir, int nu, int upd, int* __restrict__ err) {
+               const int* __restrict__ count, int dir, int nu, int upd, int corr,
+               int* __restrict__ err) {
   using F = Fused2<T>;
   extern __shared__ __align__(1024) unsigned char smem2_raw[];
   __shared__ __align__(8) uint64_t bar;
@@ -157,9 +216,26 @@ __global__ void __launch_bounds__(Fused2<T>::THREADS)
       if (tid == 0) atomicExch(err, kErrTmaTimeout);
       break;
     }
+    const int n0 = P.n[0], n1 = P.n[1];
+    if (corr && P.parent >= 0) {
+      const DevPatch R = PT[P.parent];
+      if (P.pprec == PREC_F32) correct_tile2<T, float>(P, R, s0, s1, gx0, gy0);
+      else correct_tile2<T, double>(P, R, s0, s1, gx0, gy0);
+      __syncthreads();
+      // Face ghosts of the corrected boundary cells, for the cells whose
+      // neighbours lie in the tile (the passes read no others).
+      if (P.wt)
+        for (int c = tid; c < F::PLANE; c += F::THREADS) {
+          const int sx = c % F::RX, sy = c / F::RX;
+          if (sx < 1 || sx > F::RX - 2 || sy < 1 || sy > F::RY - 2) continue;
+          const int i = gx0 + sx, j = gy0 + sy;
+          if (i < 1 || i > n0 || j < 1 || j > n1) continue;
+          if (i == 1 || i == n0 || j == 1 || j == n1) smem_ghosts2<T>(P, s0, s1, c, i, j, s0[c], s1[c]);
+        }
+      __syncthreads();
+    }
     T* o0 = fld<T>(dir == 0 ? P.qb[0] : P.q[0]);
     T* o1 = fld<T>(dir == 0 ? P.qb[1] : P.q[1]);
-    const int n0 = P.n[0], n1 = P.n[1];
     const T tmp1 = T(P.tmp1), tmp2 = T(P.tmp2), tmp3 = T(P.tmp3), alpha = T(P.alpha);
     for (int p = 0; p < npass; ++p) {
       const int color = p & 1;

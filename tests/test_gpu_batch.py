@@ -170,7 +170,8 @@ def test_batch_profile_counts_finest_stages(gpu_lib):
         st = bt.stats()
         bt.profile(False)
     # two finest-depth stages (pre and post) per tick; the post stage also
-    # reads and writes the FP64 master instead of writing e
+    # reads and writes the FP64 master instead of writing e, and applies the
+    # coarse-grid correction (its algorithmic bytes: 4 s + s / 2 per cell)
     assert st["smooth_stages"] == 4 and st["smooth_ms"] > 0
     cells = sum(n * n for n in (128, 96))
-    assert st["smooth_bytes"] == 2 * (6 * 4 + (4 * 4 + 32)) * cells
+    assert st["smooth_bytes"] == 2 * (6 * 4 + (4 * 4 + 32) + (4 * 4 + 2)) * cells

@@ -63,7 +63,8 @@ enum {
   L_FUSED = 2 + 3 * MAXD,
   L_CORR = 2 + 4 * MAXD,  // 2D: tiles of 2 x 2 fine-cell blocks (kb_correct2)
   L_UPD = 2 + 5 * MAXD,
-  NLIST = 3 + 5 * MAXD
+  L_RESTR = 3 + 5 * MAXD,  // footprint tiles of records restricted by kb_restrict
+  NLIST = 3 + 6 * MAXD
 };
 
 struct List {
@@ -503,6 +504,8 @@ void append_items(bsam_batch* b, int s) {
     const DevPatch& P = S.recs[r];
     tiles_for(rec0 + r, P.n, nd, b->lists[L_FINE + d].h);
     tiles_for(rec0 + r, P.cn, nd, b->lists[L_COARSE + d].h);
+    // A 2D fused record's restriction is done by its pre-smoothing stage.
+    if (!(nd == 2 && P.fused)) tiles_for(rec0 + r, P.cn, nd, b->lists[L_RESTR + d].h);
     if (!P.fused) {
       tiles_for(rec0 + r, P.n, nd, b->lists[L_RELAX + d].h);
     } else {
@@ -594,11 +597,13 @@ void tick_t(bsam_batch* b, cudaGraphConditionalHandle handle, int in_graph) {
       const int upd = (b->mixed && d == 0 && dir == 1) ? 1 : 0;
       if (b->mixed)
         kb_smooth2<float, true><<<g, Fused2<float>::THREADS, Fused2<float>::smem(true), s>>>(
-            pt, L[L_FUSED + d].d, cnt + L_FUSED + d, dir, nu, upd, dir, &b->d_ctl->kerr);
+            pt, L[L_FUSED + d].d, cnt + L_FUSED + d, dir, nu, upd, dir, 1 - dir,
+            &b->d_ctl->kerr);
       else
         kb_smooth2<double, false>
             <<<g, Fused2<double>::THREADS, Fused2<double>::smem(false), s>>>(
-                pt, L[L_FUSED + d].d, cnt + L_FUSED + d, dir, nu, 0, dir, &b->d_ctl->kerr);
+                pt, L[L_FUSED + d].d, cnt + L_FUSED + d, dir, nu, 0, dir, 1 - dir,
+                &b->d_ctl->kerr);
       ++n;
     }
     stage_mark(b, d, false, dir);
@@ -624,14 +629,19 @@ void tick_t(bsam_batch* b, cudaGraphConditionalHandle handle, int in_graph) {
   for (int d = 0; d < b->cap_depth; ++d) {
     relax(d, 0);
     const int gc = grid_for(b, L_COARSE + d);
-    if (b->mixed) {
-      kb_restrict<float, D><<<gc, blk, 0, s>>>(pt, L[L_COARSE + d].d, cnt + L_COARSE + d);
-      kb_coarse_load<float, D><<<gc, blk, 0, s>>>(pt, L[L_COARSE + d].d, cnt + L_COARSE + d);
-    } else {
-      kb_restrict<double, D><<<gc, blk, 0, s>>>(pt, L[L_COARSE + d].d, cnt + L_COARSE + d);
-      kb_coarse_load<double, D><<<gc, blk, 0, s>>>(pt, L[L_COARSE + d].d, cnt + L_COARSE + d);
+    if (L[L_RESTR + d].cap > 0) {
+      const int gr = grid_for(b, L_RESTR + d);
+      if (b->mixed)
+        kb_restrict<float, D><<<gr, blk, 0, s>>>(pt, L[L_RESTR + d].d, cnt + L_RESTR + d);
+      else
+        kb_restrict<double, D><<<gr, blk, 0, s>>>(pt, L[L_RESTR + d].d, cnt + L_RESTR + d);
+      ++n;
     }
-    n += 2;
+    if (b->mixed)
+      kb_coarse_load<float, D><<<gc, blk, 0, s>>>(pt, L[L_COARSE + d].d, cnt + L_COARSE + d);
+    else
+      kb_coarse_load<double, D><<<gc, blk, 0, s>>>(pt, L[L_COARSE + d].d, cnt + L_COARSE + d);
+    ++n;
   }
   {
     const int cap = std::max(1, L[L_TOPS].cap);
@@ -1078,6 +1088,10 @@ int bsam_batch_advance(bsam_batch* b, int max_ticks) {
           const bool upd = b->mixed && fused_post;
           double bytes = upd ? 4.0 * es + 32.0 : 6.0 * es;
           if (fused_post) bytes += 4.0 * es + 0.5 * es;
+          // A fused 2D pre-smoothing stage also restricts into the parent:
+          // read q (done by the stage), write the parent's q and qs
+          // (2 s + 4 s / 4 per cell).
+          if (b->bp.ndims == 2 && !b->ev_post[e] && !b->tuning.per_pass) bytes += 3.0 * es;
           b->st.smooth_bytes += bytes * (double)cells0;
         }
       }

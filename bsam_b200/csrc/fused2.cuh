@@ -148,6 +148,43 @@ __device__ __forceinline__ void correct_tile2(const DevPatch& C, const DevPatch&
   }
 }
 
+// RestrictSolution (afas:600-644) of the coarse cells a tile covers, from the
+// smoothed tile in shared memory: the parent's q and its snapshot qs (and,
+// in the correction form, the parent's base from the fine base), ghosts by
+// write-through -- restrict_cell's expressions.  Tiles start at odd global
+// indices and have even sizes, so every 2 x 2 block lies in one tile.
+template <class T, class TP, bool DELTA>
+__device__ __forceinline__ void restrict_tile2(const DevPatch& C, const DevPatch& R, const T* s0,
+                                               const T* s1, const T* sbs, int gx0, int gy0) {
+  using F = Fused2<T>;
+  const int icl = (gx0 + F::H + 1) / 2, jcl = (gy0 + F::H + 1) / 2;
+  TP* pq0 = fld<TP>(R.q[0]);
+  TP* pq1 = fld<TP>(R.q[1]);
+  TP* ps0 = fld<TP>(R.qs[0]);
+  TP* ps1 = fld<TP>(R.qs[1]);
+  for (int c = threadIdx.x; c < (F::TX / 2) * (F::TY / 2); c += blockDim.x) {
+    const int ic = icl + c % (F::TX / 2), jc = jcl + c / (F::TX / 2);
+    if (ic > C.cn[0] || jc > C.cn[1]) continue;
+    const int si = (2 * jc - gy0) * F::RX + (2 * ic - gx0);  // fine cell (2ic, 2jc)
+    const TP v0 = TP(T(0.25) * (s0[si] + s0[si - 1] + s0[si - F::RX] + s0[si - 1 - F::RX]));
+    const TP v1 = TP(T(0.25) * (s1[si] + s1[si - 1] + s1[si - F::RX] + s1[si - 1 - F::RX]));
+    const int pi = C.off[0] + ic, pj = C.off[1] + jc;
+    const int64_t pc = cidx(R, pi, pj, 0);
+    pq0[pc] = v0;
+    pq1[pc] = v1;
+    ps0[pc] = v0;
+    ps1[pc] = v1;
+    if (R.wt && near_boundary(R, pi, pj, 0, 2)) {
+      write_through<TP, 2>(R, pq0, pq1, pi, pj, 0, v0, v1);
+      write_through<TP, 2>(R, ps0, ps1, pi, pj, 0, v0, v1);
+    }
+    if constexpr (DELTA)
+      if (R.delta)
+        fld<TP>(R.bs)[pc] =
+            TP(T(0.25) * (sbs[si] + sbs[si - 1] + sbs[si - F::RX] + sbs[si - 1 - F::RX]));
+  }
+}
+
 // dir 0: q -> qb (pre-smoothing); dir 1: qb -> q (post-smoothing).
 // P.tmaps: 2D maps of q0, q1, qb0, qb1, f0, f1, bs (box RX x RY).
 // A copy that has not landed after kWaitPolls polls sets *err and ends the
@@ -162,11 +199,17 @@ __device__ __forceinline__ void correct_tile2(const DevPatch& C, const DevPatch&
 // corr (post-smoothing): the coarse-grid correction is applied to the tile
 // after it lands (correct_tile2, then the physical face ghosts the passes
 // read), instead of by a kb_correct2 launch before the stage.
+// restr (pre-smoothing): the tile's coarse cells are restricted into the
+// parent from shared memory (restrict_tile2), instead of by a kb_restrict
+// launch after the stage.
+// Four CTAs per SM (the shared tile allows four): the register cap this
+// implies costs a few spilled values outside the passes; without it the
+// kernel takes 80 registers and three CTAs per SM, which measured slower.
 template <class T, bool DELTA>
-__global__ void __launch_bounds__(Fused2<T>::THREADS)
+__global__ void __launch_bounds__(Fused2<T>::THREADS, 4)
     kb_smooth2(const DevPatch* __restrict__ PT, const Item* __restrict__ items,
                const int* __restrict__ count, int dir, int nu, int upd, int corr,
-               int* __restrict__ err) {
+               int restr, int* __restrict__ err) {
   using F = Fused2<T>;
   extern __shared__ __align__(1024) unsigned char smem2_raw[];
   __shared__ __align__(8) uint64_t bar;
@@ -301,6 +344,11 @@ __global__ void __launch_bounds__(Fused2<T>::THREADS)
       }
       __syncthreads();  // the shared tile is refilled for the next item
       continue;
+    }
+    if (restr && P.parent >= 0) {
+      const DevPatch R = PT[P.parent];
+      if (P.pprec == PREC_F32) restrict_tile2<T, float, DELTA>(P, R, s0, s1, sbs, gx0, gy0);
+      else restrict_tile2<T, double, DELTA>(P, R, s0, s1, sbs, gx0, gy0);
     }
     // Write back the tile's interior cells (warps over rows, lanes along
     // them), ghosts by write-through.

@@ -174,4 +174,5 @@ def test_batch_profile_counts_finest_stages(gpu_lib):
     # coarse-grid correction (its algorithmic bytes: 4 s + s / 2 per cell)
     assert st["smooth_stages"] == 4 and st["smooth_ms"] > 0
     cells = sum(n * n for n in (128, 96))
-    assert st["smooth_bytes"] == 2 * (6 * 4 + (4 * 4 + 32) + (4 * 4 + 2)) * cells
+    # and the pre stage restricts into the parent (3 s per cell)
+    assert st["smooth_bytes"] == 2 * (6 * 4 + 3 * 4 + (4 * 4 + 32) + (4 * 4 + 2)) * cells

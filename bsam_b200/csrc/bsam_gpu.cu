@@ -102,7 +102,9 @@ struct bsam_gpu {
   char* spare_arena = nullptr;
   size_t spare_bytes = 0;
   bool regridding = false;  // set_hierarchy called by bsam_gpu_regrid
-  char* d_regrid = nullptr;  // bsam_gpu_regrid's task list (grown, never shrunk)
+  // Task lists of bsam_gpu_regrid and bsam_gpu_errflags_level (grown, never
+  // shrunk; both synchronise before returning, so one buffer serves both).
+  char* d_regrid = nullptr;
   size_t regrid_cap = 0;
   std::vector<unsigned char> regrid_host;
   uint8_t* d_flags = nullptr;  // bsam_gpu_errflags_level's device flags
@@ -1790,21 +1792,15 @@ int bsam_gpu_regrid(bsam_gpu* h, int npatch, const bsam_patch_desc* patches, int
     const size_t o_ch = (size_t)roundup((int64_t)(sizeof(CopySpan) * spans.size()), 256);
     const size_t o_tk = o_ch + (size_t)roundup((int64_t)(sizeof(int) * children.size()), 256);
     const size_t bytes = o_tk + sizeof(TransferTask) * tasks.size();
-    if (bytes > h->regrid_cap) {
-      if (h->d_regrid) cudaFree(h->d_regrid);
-      h->d_regrid = nullptr;
-      h->regrid_cap = 0;
-      const size_t want = bytes + bytes / 2;
-      e = cudaMalloc(&h->d_regrid, want);
-      if (e == cudaSuccess) h->regrid_cap = want;
-    }
-    if (e == cudaSuccess) {
-      h->regrid_host.assign(bytes, 0);
-      unsigned char* img = h->regrid_host.data();
-      if (!spans.empty()) std::memcpy(img + o_sp, spans.data(), sizeof(CopySpan) * spans.size());
-      if (!children.empty()) std::memcpy(img + o_ch, children.data(), sizeof(int) * children.size());
-      if (!tasks.empty()) std::memcpy(img + o_tk, tasks.data(), sizeof(TransferTask) * tasks.size());
-      e = cudaMemcpyAsync(h->d_regrid, img, bytes, cudaMemcpyHostToDevice, h->stream);
+    h->regrid_host.assign(bytes, 0);
+    unsigned char* img = h->regrid_host.data();
+    if (!spans.empty()) std::memcpy(img + o_sp, spans.data(), sizeof(CopySpan) * spans.size());
+    if (!children.empty()) std::memcpy(img + o_ch, children.data(), sizeof(int) * children.size());
+    if (!tasks.empty()) std::memcpy(img + o_tk, tasks.data(), sizeof(TransferTask) * tasks.size());
+    const int urc = upload_tasks(h, img, bytes);
+    if (urc != BSAM_OK) {
+      cudaFree(old_arena);
+      return urc;
     }
     const auto grid_x = [](int64_t n) { return (unsigned)std::min<int64_t>((n + 255) / 256, 64); };
     if (e == cudaSuccess && !spans.empty()) {

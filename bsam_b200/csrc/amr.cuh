@@ -1,13 +1,14 @@
 // amr.cuh -- ghost cells of refined (AMR) patches and FillDown, FP64.
 //
 // Above the root level SetGhost (boundary.f90:58-89) fills a patch's ghost
-// ring in three ordered steps, one launch each over all patches of the level:
-//   k_interp2/3    coarse-fine interpolation on internal faces
+// ring in three ordered steps, done for each patch by one CTA of a single
+// launch over the level (k_ghost2 / k_ghost3):
+//   interpolation  coarse-fine interpolation on internal faces
 //                  (InterpolateCoarseFine -> Interpolate2D / Interpolate3D,
 //                  boundary.f90:91-323, 1299-1799)
-//   k_overlap      sibling exchange (ApplyOnLevelPairs -> TransferBC ->
+//   overlap        sibling exchange (ApplyOnLevelPairs -> TransferBC ->
 //                  GhostOverlap, boundary.f90:325-415)
-//   k_setbc_list   physical faces (SetBC2D, boundary.f90:643-744)
+//   SetBC          physical faces (SetBC2D/3D, boundary.f90:643-891)
 // Each step reads interior cells (or, for SetBC, ghosts the earlier steps
 // wrote) and writes ghosts only, so cells within a step are independent.
 #pragma once
@@ -115,32 +116,6 @@ __device__ void interp2_ghost(const DevPatch& P, const DevPatch& R, int ipass, i
       }
     }
     if (set) fld<double>(P.q[v])[cidx(P, gi, gj, 0)] = val;
-  }
-}
-
-// One CTA per patch of the list; threads over the 2(m1 + 2) + 2 m2 ring cells.
-__global__ void k_interp2(const DevPatch* __restrict__ PT, const int* __restrict__ patches,
-                          int ipass) {
-  const DevPatch P = PT[patches[blockIdx.x]];
-  const DevPatch R = PT[P.parent];
-  const int m1 = P.n[0], m2 = P.n[1];
-  const int nring = 2 * (m1 + 2) + 2 * m2;
-  for (int g = threadIdx.x; g < nring; g += blockDim.x) {
-    int gi, gj;
-    if (g < m1 + 2) {
-      gi = g;
-      gj = 0;
-    } else if (g < 2 * (m1 + 2)) {
-      gi = g - (m1 + 2);
-      gj = m2 + 1;
-    } else if (g < 2 * (m1 + 2) + m2) {
-      gi = 0;
-      gj = g - 2 * (m1 + 2) + 1;
-    } else {
-      gi = m1 + 1;
-      gj = g - 2 * (m1 + 2) - m2 + 1;
-    }
-    interp2_ghost(P, R, ipass, gi, gj);
   }
 }
 
@@ -300,44 +275,6 @@ __device__ void interp3_ghost(const DevPatch& P, const DevPatch& R, int ipass, i
   }
 }
 
-// One CTA per patch of the list; threads over the ghost ring: the two
-// z-planes outside, then the 2D ring of every interior z-plane.
-__global__ void k_interp3(const DevPatch* __restrict__ PT, const int* __restrict__ patches,
-                          int ipass) {
-  const DevPatch P = PT[patches[blockIdx.x]];
-  const DevPatch R = PT[P.parent];
-  const int m1 = P.n[0], m2 = P.n[1], m3 = P.n[2];
-  const int plane = (m1 + 2) * (m2 + 2), ring2 = 2 * (m1 + 2) + 2 * m2;
-  const int nring = 2 * plane + m3 * ring2;
-  for (int g = threadIdx.x; g < nring; g += blockDim.x) {
-    int gi, gj, gk;
-    if (g < 2 * plane) {
-      gk = g < plane ? 0 : m3 + 1;
-      const int r = g % plane;
-      gi = r % (m1 + 2);
-      gj = r / (m1 + 2);
-    } else {
-      const int r0 = g - 2 * plane;
-      gk = 1 + r0 / ring2;
-      const int r = r0 % ring2;
-      if (r < m1 + 2) {
-        gi = r;
-        gj = 0;
-      } else if (r < 2 * (m1 + 2)) {
-        gi = r - (m1 + 2);
-        gj = m2 + 1;
-      } else if (r < 2 * (m1 + 2) + m2) {
-        gi = 0;
-        gj = r - 2 * (m1 + 2) + 1;
-      } else {
-        gi = m1 + 1;
-        gj = r - 2 * (m1 + 2) - m2 + 1;
-      }
-    }
-    interp3_ghost(P, R, ipass, gi, gj, gk);
-  }
-}
-
 // One GhostOverlap transfer: dst(i, j, k) = src(i + di, j + dj, k + dk) over
 // the dst-local box [i0, i1] x [j0, j1] x [k0, k1] (k0 = k1 = 0, dk = 0 in
 // 2D; src cells are interior cells).
@@ -345,60 +282,10 @@ struct OverlapCopy {
   int32_t dst, src, i0, i1, j0, j1, k0, k1, di, dj, dk;
 };
 
-__global__ void k_overlap(const DevPatch* __restrict__ PT, const OverlapCopy* __restrict__ cps) {
-  const OverlapCopy o = cps[blockIdx.x];
-  const DevPatch D = PT[o.dst];
-  const DevPatch S = PT[o.src];
-  const int w = o.i1 - o.i0 + 1, hgt = o.j1 - o.j0 + 1, dep = o.k1 - o.k0 + 1;
-  for (int e = threadIdx.x; e < w * hgt * dep; e += blockDim.x) {
-    const int i = o.i0 + e % w, j = o.j0 + (e / w) % hgt, k = o.k0 + e / (w * hgt);
-#pragma unroll
-    for (int v = 0; v < 2; ++v)
-      fld<double>(D.q[v])[cidx(D, i, j, k)] =
-          fld<double>(S.q[v])[cidx(S, i + o.di, j + o.dj, k + o.dk)];
-  }
-}
-
-// SetBC on every patch of a list (one CTA per patch), the k_setbc rule: a
-// ghost outside in the physical dimensions S takes the face maps of S applied
-// to the cell reflected across S (cells outside only in internal dimensions
-// are left as the earlier steps wrote them).
-template <int D>
-__global__ void k_setbc_list(const DevPatch* __restrict__ PT, const int* __restrict__ patches) {
-  const DevPatch P = PT[patches[blockIdx.x]];
-  const int e0 = P.n[0] + 2, e1 = P.n[1] + 2;
-  const int64_t total = (int64_t)e0 * e1 * (D == 3 ? P.n[2] + 2 : 1);
-  for (int64_t g = threadIdx.x; g < total; g += blockDim.x) {
-    int co[3] = {(int)(g % e0), (int)((g / e0) % e1), D == 3 ? (int)(g / ((int64_t)e0 * e1)) : 0};
-    int src[3] = {co[0], co[1], co[2]};
-    int codes[3] = {BC_NONE, BC_NONE, BC_NONE};
-    bool write = false;
-#pragma unroll
-    for (int d = 0; d < D; ++d) {
-      if (co[d] == 0 && P.bc[2 * d] != BC_NONE) {
-        src[d] = 1;
-        codes[d] = P.bc[2 * d];
-        write = true;
-      } else if (co[d] == P.n[d] + 1 && P.bc[2 * d + 1] != BC_NONE) {
-        src[d] = P.n[d];
-        codes[d] = P.bc[2 * d + 1];
-        write = true;
-      }
-    }
-    if (!write) continue;
-#pragma unroll
-    for (int v = 0; v < 2; ++v) {
-      double* q = fld<double>(P.q[v]);
-      double val = q[cidx(P, src[0], src[1], src[2])];
-#pragma unroll
-      for (int d = 0; d < D; ++d)
-        if (codes[d] != BC_NONE) val = bc_map<double>(codes[d], val);
-      q[cidx(P, co[0], co[1], co[2])] = val;
-    }
-  }
-}
-
-// The k_setbc_list rule at one cell (g0, g1, g2) of patch P.
+// SetBC at one ring cell (g0, g1, g2) of patch P: a ghost outside in the
+// physical dimensions S takes the face maps of S applied to the cell
+// reflected across S (cells outside only in internal dimensions are left as
+// the interpolation and the sibling copies wrote them).
 template <int D>
 __device__ __forceinline__ void setbc_cell(const DevPatch& P, int g0, int g1, int g2) {
   const int co[3] = {g0, g1, g2};
@@ -429,8 +316,8 @@ __device__ __forceinline__ void setbc_cell(const DevPatch& P, int g0, int g1, in
   }
 }
 
-// The 2D ring cell g of a patch with m1 x m2 interior cells, in k_interp2's
-// enumeration (bottom row, top row, left column, right column).
+// The 2D ring cell g of a patch with m1 x m2 interior cells (bottom row, top
+// row, left column, right column).
 __device__ __forceinline__ void ring2(int g, int m1, int m2, int& gi, int& gj) {
   if (g < m1 + 2) {
     gi = g;
@@ -448,10 +335,10 @@ __device__ __forceinline__ void ring2(int g, int m1, int m2, int& gi, int& gj) {
 }
 
 // SetGhost of a 2D refined level in one launch, one CTA per patch: the
-// patch's coarse-fine interpolation (k_interp2), then the sibling copies into
-// its ring (k_overlap, the entries whose dst is this patch: ranges[b] =
-// {first, count} into the list sorted by dst), then its physical faces
-// (k_setbc_list).  Each step writes only this patch's ring and reads the
+// patch's coarse-fine interpolation (interp2_ghost on every ring cell), then
+// the sibling copies into its ring (the overlap entries whose dst is this
+// patch: ranges[b] = {first, count} into the list sorted by dst), then its
+// physical faces (setbc_cell).  Each step writes only this patch's ring and reads the
 // parent, this patch, and siblings' interiors, which no CTA writes here, so
 // the CTA barrier between the steps orders everything that depends on them.
 __global__ void k_ghost2(const DevPatch* __restrict__ PT, const int* __restrict__ patches,
@@ -484,6 +371,58 @@ __global__ void k_ghost2(const DevPatch* __restrict__ PT, const int* __restrict_
     int gi, gj;
     ring2(g, m1, m2, gi, gj);
     setbc_cell<2>(P, gi, gj, 0);
+  }
+}
+
+// The 3D ring cell g of a patch with m1 x m2 x m3 interior cells, in
+// order: the two k planes, then the 2D ring of each interior plane.
+__device__ __forceinline__ void ring3(int g, int m1, int m2, int m3, int& gi, int& gj, int& gk) {
+  const int plane = (m1 + 2) * (m2 + 2), rg2 = 2 * (m1 + 2) + 2 * m2;
+  if (g < 2 * plane) {
+    gk = g < plane ? 0 : m3 + 1;
+    const int r = g % plane;
+    gi = r % (m1 + 2);
+    gj = r / (m1 + 2);
+  } else {
+    const int r0 = g - 2 * plane;
+    gk = 1 + r0 / rg2;
+    ring2(r0 % rg2, m1, m2, gi, gj);
+  }
+}
+
+// SetGhost of a 3D refined level in one launch: k_ghost2's structure with
+// Interpolate3D (interp3_ghost), the 3D overlap boxes and the 3D face rule.
+__global__ void k_ghost3(const DevPatch* __restrict__ PT, const int* __restrict__ patches,
+                         const OverlapCopy* __restrict__ cps, const int2* __restrict__ ranges,
+                         int ipass) {
+  const DevPatch P = PT[patches[blockIdx.x]];
+  const DevPatch R = PT[P.parent];
+  const int m1 = P.n[0], m2 = P.n[1], m3 = P.n[2];
+  const int nring = 2 * (m1 + 2) * (m2 + 2) + m3 * (2 * (m1 + 2) + 2 * m2);
+  for (int g = threadIdx.x; g < nring; g += blockDim.x) {
+    int gi, gj, gk;
+    ring3(g, m1, m2, m3, gi, gj, gk);
+    interp3_ghost(P, R, ipass, gi, gj, gk);
+  }
+  __syncthreads();
+  const int2 rg = ranges[blockIdx.x];
+  for (int c = rg.x; c < rg.x + rg.y; ++c) {
+    const OverlapCopy o = cps[c];
+    const DevPatch S = PT[o.src];
+    const int w = o.i1 - o.i0 + 1, hgt = o.j1 - o.j0 + 1, dep = o.k1 - o.k0 + 1;
+    for (int e = threadIdx.x; e < w * hgt * dep; e += blockDim.x) {
+      const int i = o.i0 + e % w, j = o.j0 + (e / w) % hgt, k = o.k0 + e / (w * hgt);
+#pragma unroll
+      for (int v = 0; v < 2; ++v)
+        fld<double>(P.q[v])[cidx(P, i, j, k)] =
+            fld<double>(S.q[v])[cidx(S, i + o.di, j + o.dj, k + o.dk)];
+    }
+  }
+  __syncthreads();
+  for (int g = threadIdx.x; g < nring; g += blockDim.x) {
+    int gi, gj, gk;
+    ring3(g, m1, m2, m3, gi, gj, gk);
+    setbc_cell<3>(P, gi, gj, gk);
   }
 }
 

@@ -239,8 +239,8 @@ void launch_transfer_t(bsam_gpu* h, const LevelPlan& L, int what) {
 }
 
 // SetGhost(level, ipass) of a refined level (boundary.f90:58-89): coarse-fine
-// interpolation, sibling exchange, physical faces -- one launch in 2D (a CTA
-// per patch runs the three in order), three ordered launches in 3D.
+// interpolation, sibling exchange, physical faces -- one launch (a CTA per
+// patch runs the three in order).
 // Levels at and below the root keep their ghosts by write-through.
 void amr_ghost(bsam_gpu* h, int level, int ipass) {
   if (level < h->minlevel || level > h->finestlevel) return;
@@ -250,11 +250,10 @@ void amr_ghost(bsam_gpu* h, int level, int ipass) {
     k_ghost2<<<L.nplist, 128, 0, h->stream>>>(h->d_patches, L.d_plist, L.d_ovl_by_dst,
                                               L.d_ovl_range, ipass);
   } else {
-    k_interp3<<<L.nplist, 256, 0, h->stream>>>(h->d_patches, L.d_plist, ipass);
-    if (L.novl) k_overlap<<<L.novl, 256, 0, h->stream>>>(h->d_patches, L.d_ovl);
-    k_setbc_list<3><<<L.nplist, 256, 0, h->stream>>>(h->d_patches, L.d_plist);
+    k_ghost3<<<L.nplist, 256, 0, h->stream>>>(h->d_patches, L.d_plist, L.d_ovl_by_dst,
+                                              L.d_ovl_range, ipass);
   }
-  h->stats.launches += h->rp.ndims == 2 ? 1 : (L.novl ? 3 : 2);
+  ++h->stats.launches;
 }
 
 // GetCoarseGhostPoints for the children of a partly covered level: the

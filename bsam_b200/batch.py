@@ -215,11 +215,20 @@ class Batch:
                self.h, "slot_phase")
         return ph.value, st.value
 
-    def collect(self, slot: int, want_q: bool = True):
-        """Final root q (with ghosts), per-step results and FP64 mass of slot."""
+    def collect(self, slot: int, want_q: bool = True, out=None):
+        """Final root q (with ghosts), per-step results and FP64 mass of slot.
+        out: a Fortran-ordered float64 array of q's shape to copy into (for
+        instance one in page-locked memory, which the copy reaches at full
+        speed); by default a new array."""
         prob = self.probs.pop(slot)
         shape = tuple(m + 2 for m in prob.mx[:prob.ndims]) + (2,)
-        q = np.zeros(shape, order="F") if want_q else None
+        if out is not None:
+            if (out.shape != shape or out.dtype != np.float64 or
+                    not out.flags["F_CONTIGUOUS"]):
+                raise ValueError("out must be a Fortran-ordered float64 array of q's shape")
+            q = out if want_q else None
+        else:
+            q = np.empty(shape, order="F") if want_q else None
         steps = (StepResult * prob.nsteps)()
         mass = ctypes.c_double(0.0)
         rc = _lib().bsam_batch_collect(

@@ -448,9 +448,10 @@ def run_ours(args, world, rank, local):
                 nv, pats, refined = [], [], []
                 for _ in range(nst):
                     nv.append(r.step()[0])
-                    pats.append(sum(1 for d in r.descs if d["level"] >= 1))
-                    refined.append(sum(d["mx"][0] * d["mx"][1] for d in r.descs
-                                       if d["level"] >= 1))
+                    t = r.table_array()
+                    fine = t["level"] >= 1
+                    pats.append(int(fine.sum()))
+                    refined.append(int((t["mx"][:, 0] * t["mx"][:, 1])[fine].sum()))
                 dt_ = time.perf_counter() - t0
                 p1 = r.profile()
             extra[f"cfg2_amr_{tag}"] = {

@@ -651,7 +651,25 @@ class AmrRun:
         except Exception:
             self.close()
             raise
-        self.descs = list(hier.descs)
+        self._descs = list(hier.descs)
+        self._table = None
+        self.npatch = len(hier.descs)
+
+    @property
+    def descs(self) -> list:
+        """The current patch table as dicts (converted on first use after a
+        step)."""
+        if self._descs is None:
+            self._descs = [desc_dict(self._table[i]) for i in range(self.npatch)]
+            self.b.descs = list(self._descs)
+        return self._descs
+
+    def table_array(self) -> np.ndarray:
+        """The current patch table as a numpy structured array (no copy of
+        the records into Python objects): fields level, parent, mx, ..."""
+        if self._table is None:
+            return np.ctypeslib.as_array(desc_array(self._descs))
+        return np.ctypeslib.as_array(self._table)
 
     def step(self):
         """One time step (bsam_amr_step): (V-cycles, residual)."""
@@ -665,8 +683,7 @@ class AmrRun:
         n = lib().bsam_amr_table(self.a, None, 0)
         arr = (PatchDesc * n)()
         lib().bsam_amr_table(self.a, arr, n)
-        self.descs = [desc_dict(arr[i]) for i in range(n)]
-        self.b.descs = list(self.descs)
+        self._table, self.npatch, self._descs = arr, n, None
         return nv.value, res.value
 
     def stats(self):
@@ -687,6 +704,7 @@ class AmrRun:
         return [(i, self.b.get_q(i)) for i, d in enumerate(self.descs) if d["level"] >= 0]
 
     def write_frame(self, path, time):
+        _ = self.descs  # the backend's table follows the last step
         self.b.write_frame(path, time)
 
     def close(self):
@@ -752,7 +770,7 @@ def solve_request(prob, device: int = 0, keep_q: bool = False) -> dict:
         for k in range(nsteps):
             nvc[k], res[k] = r.step()
             conv[k] = r.converged
-            most = max(most, len(r.descs))
+            most = max(most, r.npatch)
         out = {"nvcycles": nvc, "residual": res, "converged": conv, "patches_max": most}
         if keep_q:
             out["q"] = r.state()

@@ -143,5 +143,12 @@ def test_native_amr_run_matches_oracle(gpu_lib, oracle, nd):
                     d = rn.descs[i]
                     inner = tuple(slice(1, m + 1) for m in d["mx"][:nd])
                     np.testing.assert_allclose(qg[inner], qo[inner], rtol=0, atol=1e-11)
+            # The per-phase host times cover every step.
+            prof = rn.profile()
+            assert prof["steps"] == 3
+            assert all(prof[k] >= 0.0 for k in rn.PHASES) and prof["solve"] > 0.0
+            t = rn.table_array()
+            assert len(t) == len(rn.descs)
+            assert list(t["level"]) == [d["level"] for d in rn.descs]
         finally:
             o.close()

@@ -215,11 +215,12 @@ class Batch:
                self.h, "slot_phase")
         return ph.value, st.value
 
-    def collect(self, slot: int, want_q: bool = True, out=None):
+    def collect(self, slot: int, want_q: bool = True, out=None, want_mass: bool = True):
         """Final root q (with ghosts), per-step results and FP64 mass of slot.
         out: a Fortran-ordered float64 array of q's shape to copy into (for
         instance one in page-locked memory, which the copy reaches at full
-        speed); by default a new array."""
+        speed); by default a new array.  want_mass=False skips the mass
+        reduction (one kernel and one wait fewer; "mass" is then None)."""
         prob = self.probs.pop(slot)
         shape = tuple(m + 2 for m in prob.mx[:prob.ndims]) + (2,)
         if out is not None:
@@ -233,13 +234,13 @@ class Batch:
         mass = ctypes.c_double(0.0)
         rc = _lib().bsam_batch_collect(
             self.h, slot, q.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if want_q else None,
-            steps, ctypes.byref(mass))
+            steps, ctypes.byref(mass) if want_mass else None)
         _check(rc, self.h, "collect")
         return {"q": q,
                 "nvcycles": np.array([s.nvcycles for s in steps], dtype=np.int32),
                 "converged": np.array([s.converged for s in steps], dtype=np.int32),
                 "residual": np.array([s.residual for s in steps]),
-                "mass": mass.value}
+                "mass": mass.value if want_mass else None}
 
     def stream(self) -> int:
         p = ctypes.c_void_p()

@@ -148,34 +148,92 @@ def shard_problems(rank: int):
 
 # ---- CPU restatement of the reference (the oracle) ---------------------------
 
-def _oracle_solve(args):
-    """One problem through the CPU oracle (worker of the reference arm)."""
-    idx, nsteps, seed = args
+_ORACLE_TIMING = None
+
+
+def _oracle_timing_lib():
+    """Loads the host-tuned timing build of the oracle in this process."""
+    global _ORACLE_TIMING
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
+    if _ORACLE_TIMING is None:
+        _ORACLE_TIMING = pyoracle.build_timing()
+        pyoracle.use_library(_ORACLE_TIMING)
+    return pyoracle
+
+
+def _worker_init(path):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    pyoracle.use_library(path)
+
+
+_WORKLOAD_CACHE = {}
+
+
+def _workload(seed):
     from bsam_b200 import workloads as W
-    prob = W.config4(nprob=idx + 1, nsteps=nsteps, seed=seed)[idx]
-    t0 = time.perf_counter()
-    pyoracle.run_uniform(prob, nsteps=nsteps, keep_steps=False)
-    return nsteps, time.perf_counter() - t0
+    if seed not in _WORKLOAD_CACHE:
+        _WORKLOAD_CACHE[seed] = W.config4(nprob=NPROB, nsteps=NSTEPS, seed=seed)
+    return _WORKLOAD_CACHE[seed]
 
 
-def cpu_baseline(sample: int = 12, nsteps: int = 2):
-    """The oracle on one core over a bounded sample of the workload: the first
-    `sample` problems, `nsteps` time steps each."""
+def _oracle_solve(args):
+    """One problem of the workload, its whole solve (every time step), through
+    the CPU oracle: returns (problem index, time steps, V-cycles, seconds)."""
+    idx, seed = args
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
-    pyoracle.build()
-    steps, secs = 0, 0.0
-    for i in range(sample):
-        s, t = _oracle_solve((i, nsteps, 4))
-        steps += s
-        secs += t
-    out = {"value": steps / secs, "unit": UNIT, "cores": 1, "kind": "port",
-           "sample": f"first {sample} of the 512 problems, {nsteps} time steps each, one "
-                     "thread (C++ restatement of the reference Fortran path)"}
-    # The AMR configuration with sustained refinement: the oracle through the
-    # same regrid driver, two steps after one warm-up step, one thread.
+    prob = _workload(seed)[idx]
+    t0 = time.perf_counter()
+    r = pyoracle.run_uniform(prob, nsteps=prob.nsteps, keep_steps=False)
+    return idx, prob.nsteps, int(r["nvcycles"].sum()), time.perf_counter() - t0
+
+
+def cpu_baseline(per_side: int = 16):
+    """The reference path on one core: the oracle's timing build, whole
+    10-step solves of a sample stratified over the five sides (the first
+    `per_side` problems of each side in workload order).  The workload's time
+    is estimated side by side: its problem count per side x the sample's mean
+    time per problem of that side.  Runs in one spawned process, so that this
+    process keeps the parity build for the accuracy check."""
+    import multiprocessing as mp
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    path = pyoracle.build_timing()
+    with mp.get_context("spawn").Pool(1, initializer=_worker_init, initargs=(path,)) as pool:
+        return pool.apply(_cpu_baseline_body, (per_side,))
+
+
+def _cpu_baseline_body(per_side):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    probs = _workload(4)
+    sides = sorted({p.mx[0] for p in probs})
+    per_side_time, nv_sample, st_sample, t_sample = {}, 0, 0, 0.0
+    for side in sides:
+        idxs = [i for i, p in enumerate(probs) if p.mx[0] == side][:per_side]
+        ts = []
+        for i in idxs:
+            _, st, nv, t = _oracle_solve((i, 4))
+            ts.append(t)
+            nv_sample += nv
+            st_sample += st
+        per_side_time[side] = statistics.mean(ts)
+        t_sample += sum(ts)
+    est = sum(per_side_time[p.mx[0]] for p in probs)
+    steps = sum(p.nsteps for p in probs)
+    out = {"value": steps / est, "unit": UNIT, "cores": 1, "kind": "port",
+           "sample": f"whole {NSTEPS}-step solves of {per_side} problems per side (sides "
+                     f"{sides}), one thread, {t_sample:.1f} s; workload time estimated from "
+                     "the mean per side x the workload's problems per side.  C++ restatement "
+                     "of the reference Fortran path, timing build (g++ -O3 -march=native, "
+                     "contracted multiply-adds), built on this host",
+           "vcycles_per_s": nv_sample / t_sample,
+           "sample_time_steps": st_sample}
+    # The AMR configuration with sustained refinement: the oracle (timing
+    # build) through the same regrid driver, two steps after one warm-up
+    # step, one thread.
     from bsam_b200 import amr as AMR
     hier, prm = AMR.config2(sustained=True)
     b = pyoracle.OracleBackend(2, hier.dt, hier.eps, hier.qerrortol)
@@ -192,37 +250,44 @@ def cpu_baseline(sample: int = 12, nsteps: int = 2):
 
 
 def run_reference(args, world, rank):
+    """The reference arm: every bench step solves the whole 512-problem
+    workload (every problem's 10 time steps) with the oracle's timing build,
+    one problem at a time per worker process, on every host core."""
     if rank != 0:
         return 0
     import multiprocessing as mp
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import pyoracle
-    pyoracle.build()
+    _oracle_timing_lib()
     cores = os.cpu_count() or 1
-    per_step = 2 * cores  # problems per bench step, 2 time steps each
     ctx = mp.get_context("spawn")
-    times, steps_done = [], 0
-    with ctx.Pool(cores) as pool:
+    probs = _workload(4)
+    # Largest problems first, so that the pool's last jobs are short.
+    order = sorted(range(NPROB), key=lambda i: -probs[i].mx[0] * probs[i].mx[1])
+    times, steps_done, nv_done = [], 0, 0
+    with ctx.Pool(cores, initializer=_worker_init, initargs=(_ORACLE_TIMING,)) as pool:
         for s in range(args.warmup + args.steps):
-            jobs = [((s * per_step + k) % NPROB, 2, 4) for k in range(per_step)]
+            jobs = [(i, 4) for i in order]
             t0 = time.perf_counter()
-            res = pool.map(_oracle_solve, jobs)
+            res = pool.map(_oracle_solve, jobs, chunksize=1)
             dt = time.perf_counter() - t0
             if s >= args.warmup:
                 times.append(dt)
-                steps_done += sum(r[0] for r in res)
+                steps_done += sum(r[1] for r in res)
+                nv_done += sum(r[2] for r in res)
     total = sum(times)
     value = steps_done / total
+    sample = (f"every bench step: all {NPROB} problems of the workload, whole {NSTEPS}-step "
+              f"solves, {cores} worker processes (C++ restatement of the reference Fortran "
+              "path, which cannot be compiled here; timing build g++ -O3 -march=native "
+              "with contracted multiply-adds, built on this host)")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD},
+        "config": {"workload": WORKLOAD, "vcycles_per_s": nv_done / total,
+                   "step_ms": [round(1e3 * t, 1) for t in times]},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"per step {per_step} of the 512 problems x 2 time steps, "
-                                   f"{cores} worker processes (C++ restatement of the reference "
-                                   "Fortran path, which cannot be compiled here)"},
+                         "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -230,6 +295,46 @@ def run_reference(args, world, rank):
 
 
 # ---- our arm -----------------------------------------------------------------
+
+def _interior_err(got, ref, prob):
+    """Largest |got - ref| over the interior cells of both components, and
+    the same relative to the largest |ref| per component."""
+    import numpy as np
+    inner = tuple(slice(1, m + 1) for m in prob.mx[:prob.ndims])
+    ab, rel = 0.0, 0.0
+    for v in range(2):
+        d = float(np.max(np.abs(got[inner + (v,)] - ref[inner + (v,)])))
+        ab = max(ab, d)
+        rel = max(rel, d / max(float(np.max(np.abs(ref[inner + (v,)]))), 1e-300))
+    return ab, rel
+
+
+def accuracy_vs_oracle(batch, problems, per_side=2):
+    """Checker, outside every timed region: the final state of a sample of
+    the workload stratified over the sides (the first `per_side` problems of
+    each side), solved by the batch, against the FP64 oracle (parity build)
+    solving the same problems."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    sample = []
+    for side in sorted({p.mx[0] for p in problems}):
+        sample += [p for p in problems if p.mx[0] == side][:per_side]
+    slots = [batch.submit_seeded(p) for p in sample]
+    batch.run()
+    got = [batch.collect(s, want_q=True) for s in slots]
+    worst_abs, worst_rel, per = 0.0, 0.0, []
+    for p, g in zip(sample, got):
+        ref = pyoracle.run_uniform(p, nsteps=p.nsteps, keep_steps=False, final_q=True)
+        ab, rel = _interior_err(g["q"], ref["q_final"], p)
+        worst_abs, worst_rel = max(worst_abs, ab), max(worst_rel, rel)
+        per.append({"side": p.mx[0], "max_abs": ab, "max_rel": rel,
+                    "vcycles": int(g["nvcycles"].sum()),
+                    "vcycles_fp64_oracle": int(ref["nvcycles"].sum()),
+                    "max_residual": float(g["residual"].max())})
+    return {"max_err_vs_fp64": worst_rel, "max_abs_err_vs_fp64": worst_abs,
+            "sample": f"{len(sample)} problems ({per_side} per side), final state of all "
+                      f"{NSTEPS} steps, interior cells, both components; relative to max |ref|",
+            "per_problem": per}
 
 def solve_batch(BB, problems, precision, device, want_q=False, q0s=None):
     """Submits every problem (device-side initial state unless q0s is given),
@@ -366,6 +471,8 @@ def run_ours(args, world, rank, local):
         e2e_t.append(time.perf_counter() - t0)
         d2h = sum(int(r["q"].nbytes) for r in res)
     e2e_s = allmax(world, sum(e2e_t))
+    # Accuracy of the measured form against the FP64 oracle (rank 0 only).
+    acc = accuracy_vs_oracle(batch, problems) if rank == 0 and not args.quick else None
     batch.close()
 
     line = {
@@ -381,7 +488,8 @@ def run_ours(args, world, rank, local):
                    "vcycles_per_bench_step": statistics.mean(nvc),
                    "vcycles_per_s": world * sum(nvc) / dev_s_max,
                    "ticks_per_bench_step": ticks / args.steps,
-                   "all_converged": conv_all},
+                   "all_converged": conv_all,
+                   "step_ms": [round(x, 3) for x in step_ms]},
         "roofline": {"bound": "hbm", "kernel": "kb_smooth2<float> (fused finest-depth "
                      "smoothing stages: nu=2 red-black sweeps of every problem, one launch "
                      "each; the post-smoothing launch also applies the coarse-grid "
@@ -397,6 +505,9 @@ def run_ours(args, world, rank, local):
         "gpu_launches": int(ticks * kpt + 2 * NPROB * args.steps),
         "clocks": clocks,
     }
+    if acc is not None:
+        line["max_err_vs_fp64"] = acc["max_err_vs_fp64"]
+        line["accuracy"] = acc
 
     if world == 1 and rank == 0 and not args.quick:
         extra = {}
@@ -414,6 +525,7 @@ def run_ours(args, world, rank, local):
                 for s in slots:
                     b64.collect(s, want_q=False)
             extra["fp64_batched_steps_per_s"] = steps_per_bench_step / (e0.elapsed_time(e1) / 1e3)
+            extra["mixed_over_fp64_batched"] = value / extra["fp64_batched_steps_per_s"]
         # Plain FP64 form, one problem at a time (single-problem library), on a
         # sample of the problems (every 16th).
         tt, st_ = 0.0, 0
@@ -434,8 +546,38 @@ def run_ours(args, world, rank, local):
                 sv.run(1, keep_steps=False)
                 torch.cuda.synchronize()
                 t0 = time.perf_counter()
-                sv.run(5, keep_steps=False)
-                extra[f"cfg3_128cubed_{name}_steps_per_s"] = 5 / (time.perf_counter() - t0)
+                r3 = sv.run(5, keep_steps=False)
+                dt3 = time.perf_counter() - t0
+                extra[f"cfg3_128cubed_{name}_steps_per_s"] = 5 / dt3
+                extra[f"cfg3_128cubed_{name}_vcycles_per_s"] = float(r3["nvcycles"].sum()) / dt3
+        # Error of both forms against the FP64 oracle after each of the first
+        # three time steps (checker, outside the timed runs).
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import pyoracle
+        prob = W.config3(nsteps=3)
+        ref3 = pyoracle.run_uniform(prob, nsteps=3)
+        for name, prec in (("fp64", B.PREC_FP64), ("mixed", B.PREC_MIXED)):
+            with B.Solver(prob, precision=prec) as sv:
+                g3 = sv.run(3)
+            extra[f"cfg3_128cubed_{name}_err_vs_fp64_per_step"] = [
+                _interior_err(g3["q"][k], ref3["q"][k], prob)[1] for k in range(3)]
+            extra[f"cfg3_128cubed_{name}_vcycles_per_step"] = [int(x) for x in g3["nvcycles"]]
+        extra["cfg3_128cubed_fp64_oracle_vcycles_per_step"] = [int(x) for x in ref3["nvcycles"]]
+        # Config 1 (128^2, 20 steps, FP64 to 1e-9; L2-resident, latency-bound):
+        # time steps and V-cycles per second of the single-problem library,
+        # and its final state against the oracle.
+        prob = W.config1()
+        with B.Solver(prob, precision=B.PREC_FP64) as sv:
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            r1 = sv.run(prob.nsteps)
+            dt1 = time.perf_counter() - t0
+        ref1 = pyoracle.run_uniform(prob, keep_steps=False, final_q=True)
+        extra["cfg1_128sq_fp64"] = {
+            "steps_per_s": prob.nsteps / dt1, "vcycles_per_s": float(r1["nvcycles"].sum()) / dt1,
+            "vcycles_equal_oracle": bool(np.array_equal(r1["nvcycles"], ref1["nvcycles"])),
+            "max_rel_err_vs_oracle": _interior_err(r1["q"][-1], ref1["q_final"], prob)[1],
+            "timing": "host wall clock over the 20 steps through the C++ host driver"}
         # 2D AMR (config 2): 256^2 root + two refined levels, regridded every
         # step in the native driver (bsam_amr_step), FP64; host wall clock.
         from bsam_b200 import amr as AMR

@@ -41,15 +41,64 @@ def build() -> str:
     return _LIB
 
 
+# The timing build: the same source for speed on the machine that runs it
+# (g++ -O3 -march=native, multiply-adds contracted), as a Fortran build of the
+# reference with gfortran -O3 -march=native would be.  It is not the parity
+# build (contraction changes the last bits), so nothing checks results with
+# it.  It is compiled on the host that times it, into a file named after that
+# host's CPU, so that a build made for another CPU is never loaded.
+TIMING_FLAGS = ["-O3", "-march=native", "-ffp-contract=fast", "-std=c++17", "-fPIC", "-shared"]
+
+
+def _cpu_key() -> str:
+    import hashlib
+    import platform
+    desc = platform.machine()
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith(("model name", "flags")):
+                    desc += line
+                if line.startswith("flags"):
+                    break
+    except OSError:
+        pass
+    return hashlib.sha1(desc.encode()).hexdigest()[:12]
+
+
+def build_timing() -> str:
+    """Compile the timing build for this host (no-op when present); returns
+    its path.  Load it with use_library(path) before the first lib() call."""
+    out_dir = os.path.join(_HERE, "_timing")
+    os.makedirs(out_dir, exist_ok=True)
+    out = os.path.join(out_dir, f"libbsam_oracle_native_{_cpu_key()}.so")
+    src = os.path.join(_HERE, "bsam_oracle.cpp")
+    if not os.path.exists(out) or os.path.getmtime(out) < os.path.getmtime(src):
+        tmp = out + f".{os.getpid()}.tmp"
+        subprocess.run([os.environ.get("CXX", "g++"), *TIMING_FLAGS, "-o", tmp, src], check=True)
+        os.replace(tmp, out)
+    return out
+
+
 _lib = None
+_lib_path = None
+
+
+def use_library(path: str) -> None:
+    """Selects the shared library lib() loads (default: the parity build)."""
+    global _lib_path
+    if _lib is not None and path != _lib_path:
+        raise RuntimeError("the oracle library is already loaded")
+    _lib_path = path
 
 
 def lib():
     global _lib
     if _lib is None:
-        if not os.path.exists(_LIB):
+        path = _lib_path or _LIB
+        if path == _LIB and not os.path.exists(_LIB):
             build()
-        L = ctypes.CDLL(_LIB)
+        L = ctypes.CDLL(path)
         dp = ctypes.POINTER(ctypes.c_double)
         ip = ctypes.POINTER(ctypes.c_int)
         L.orc_run_uniform.argtypes = [ctypes.POINTER(OrcParams), dp, ctypes.c_int, dp, ip, dp, dp, dp]
@@ -219,15 +268,21 @@ def new_subgrids(flags, desfill, mgp, maxboxes=4096):
     return boxes[:6 * n].reshape(n, 3, 2)
 
 
-def run_uniform(prob, nsteps=None, keep_steps=True, q0=None):
+def run_uniform(prob, nsteps=None, keep_steps=True, q0=None, final_q=False):
     """Run the oracle time loop.  Returns a dict with q per step (Fortran
-    layout with ring), V-cycle counts, final residuals, traces and mass."""
+    layout with ring), V-cycle counts, final residuals, traces and mass;
+    final_q (with keep_steps=False) adds the last step's q as "q_final"."""
     L = lib()
     nsteps = prob.nsteps if nsteps is None else nsteps
     p = params_of(prob)
     q0 = prob.q0() if q0 is None else q0
     q0 = np.asfortranarray(q0, dtype=np.float64)
     qsize = q0.size
+    if final_q and not keep_steps:
+        out = run_uniform(prob, nsteps=nsteps, keep_steps=True, q0=q0)
+        out["q_final"] = out["q"][-1]
+        out["q"] = None
+        return out
     q_steps = np.zeros((nsteps,) + q0.shape, dtype=np.float64) if keep_steps else None
     buf = np.zeros(nsteps * qsize) if keep_steps else None
     nvc = np.zeros(nsteps, dtype=np.int32)

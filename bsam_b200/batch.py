@@ -18,6 +18,7 @@ PREC_FP64, PREC_MIXED = 0, 1
 SLOT_IDLE, SLOT_RUNNING, SLOT_DONE, SLOT_FAILED = 0, 1, 2, 3
 MAX_STEPS = 256
 ERR_NOMEM = -3
+ERR_DIVERGED = -7
 
 
 class BatchParams(ctypes.Structure):
@@ -221,7 +222,7 @@ class Batch:
         instance one in page-locked memory, which the copy reaches at full
         speed); by default a new array.  want_mass=False skips the mass
         reduction (one kernel and one wait fewer; "mass" is then None)."""
-        prob = self.probs.pop(slot)
+        prob = self.probs[slot]
         shape = tuple(m + 2 for m in prob.mx[:prob.ndims]) + (2,)
         if out is not None:
             if (out.shape != shape or out.dtype != np.float64 or
@@ -235,6 +236,10 @@ class Batch:
         rc = _lib().bsam_batch_collect(
             self.h, slot, q.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if want_q else None,
             steps, ctypes.byref(mass) if want_mass else None)
+        # The native call releases the slot when it succeeds and when it
+        # reports a diverged solve; any other failure leaves it resident.
+        if rc == 0 or rc == ERR_DIVERGED:
+            self.probs.pop(slot, None)
         _check(rc, self.h, "collect")
         return {"q": q,
                 "nvcycles": np.array([s.nvcycles for s in steps], dtype=np.int32),

@@ -254,8 +254,11 @@ const char* bsam_gpu_last_error(bsam_gpu* h);
  * cells (16,777,216 cells when mx1 is a multiple of 64 and mx2 of 4); larger
  * patches return BSAM_ERR_TOO_LARGE.  The first call on a device looks up the
  * scratch array's device address with cudaGetSymbolAddress, so make that
- * first call before capturing any stream.  All calls share the scratch: calls
- * whose kernels overlap on the GPU race and give wrong results. */
+ * first call before capturing any stream.  That address is kept for the life
+ * of the process: after a cudaDeviceReset of the device it is stale, so do
+ * not call this entry point on a device that was reset.  All calls share the
+ * scratch: calls whose kernels overlap on the GPU race and give wrong
+ * results. */
 #define BSAM_NOALLOC_MAX_TILES 65536
 int bsam_gpu_resid_norm_noalloc(int device, int ndims, const int32_t* mx, double dx, double dt,
                                 double eps, double alpha, const double* q, const double* f,

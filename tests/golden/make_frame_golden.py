@@ -29,7 +29,9 @@ sys.path.insert(0, ROOT)
 from bsam_b200 import amr  # noqa: E402  (pure-Python hierarchy builder)
 from oracle import pyoracle  # noqa: E402
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if __name__ == "__main__" and len(sys.argv) < 2:
+    sys.exit("usage: make_frame_golden.py REFERENCE_DIR  (the root of the BSAM source tree)")
+REF = sys.argv[1] if len(sys.argv) > 1 else None
 
 
 def reference_reader():

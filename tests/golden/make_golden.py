@@ -60,7 +60,10 @@ import fsubset as F  # noqa: E402
 from bsam_b200 import amr, workloads as W  # noqa: E402  (pure-Python hierarchy builders)
 
 ARGS = [a for a in sys.argv[1:] if not a.startswith("--only")]
-REF = ARGS[0] if ARGS else "/root/reference"
+if __name__ == "__main__" and not ARGS:
+    sys.exit("usage: make_golden.py REFERENCE_DIR [--only=name,...]  "
+             "(REFERENCE_DIR: the root of the BSAM source tree)")
+REF = ARGS[0] if ARGS else None
 ONLY = None
 for a in sys.argv[1:]:
     if a.startswith("--only="):

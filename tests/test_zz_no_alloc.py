@@ -50,6 +50,37 @@ def test_noalloc_matches_multigrid_residual_twice(gpu_lib, nd):
         np.testing.assert_allclose(got[1], res * res * denom, rtol=1e-10, err_msg=f"call {call}")
 
 
+@pytest.mark.parametrize("nd,mx", [(2, (130, 37)), (3, (70, 9, 5))])
+def test_noalloc_ragged_tiles_against_oracle_operator(gpu_lib, oracle, nd, mx):
+    # Several tiles in x with a partial last one, and a partial last tile in
+    # y: known q (ring included) and f, the residual norm of f - Operator(q)
+    # with the oracle's Operator, on two calls in a row.
+    import torch
+    rng = np.random.default_rng(7 + nd)
+    qshape = tuple(m + 2 for m in mx) + (2,)
+    q = np.asfortranarray(0.5 + 0.1 * rng.standard_normal(qshape))
+    f = np.asfortranarray(0.01 * rng.standard_normal(tuple(mx) + (2,)))
+    h, dt, eps, alpha = 1.0 / mx[0], 1e-4, 0.02, 1.0
+    rf = f - oracle.operator(nd, mx, h, dt, alpha, eps, q)
+    total = float(np.sum(rf * rf))
+    denom = 2.0 * np.prod(mx)
+    qd = torch.from_numpy(q.ravel(order="F").copy()).cuda()
+    fd = torch.from_numpy(f.ravel(order="F").copy()).cuda()
+    m = (ctypes.c_int32 * 3)(*(list(mx) + [1] * (3 - nd)))
+    stream = torch.cuda.current_stream()
+    for call in range(2):
+        out = torch.full((2,), -1.0, dtype=torch.float64, device="cuda")
+        rc = gpu_lib.bsam_gpu_resid_norm_noalloc(
+            torch.cuda.current_device(), nd, m, h, dt, eps, alpha, _dev_ptr(qd), _dev_ptr(fd),
+            _dev_ptr(out), ctypes.c_void_p(stream.cuda_stream))
+        assert rc == 0, gpu_lib.bsam_gpu_strerror(rc)
+        torch.cuda.synchronize()
+        got = out.cpu().numpy()
+        np.testing.assert_allclose(got[1], total, rtol=RTOL, err_msg=f"call {call}")
+        np.testing.assert_allclose(got[0], np.sqrt(total / denom), rtol=RTOL)
+        np.testing.assert_allclose(got[1] / denom, got[0] ** 2, rtol=1e-12)
+
+
 def test_noalloc_rejects_patch_beyond_scratch(gpu_lib):
     mx = (ctypes.c_int32 * 3)(4096, 4100, 1)   # 64 x 1025 tiles > 65536
     null = ctypes.c_void_p(16)

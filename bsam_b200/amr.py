@@ -183,7 +183,7 @@ def _desc(level, parent, mx, mbounds, mglobal, mthbc, dx, xlower):
 
 
 def build(n_root: int, boxes: list, eps: float, dt: float = 5e-5, qerrortol: float = 1e-9,
-          mthbc: int = 1, minlevel: int = 1, seed: int = 2, field: str = "drop",
+          mthbc=1, minlevel: int = 1, seed: int = 2, field: str = "drop",
           maxvcycles: int = 20, ndims: int = 2) -> Hierarchy:
     """Hierarchy on [0,1]^d (d = ndims, 2 or 3): an n_root^d root, its
     below-root levels (automatic minlevel: halve while even, at most 10
@@ -212,11 +212,14 @@ def build(n_root: int, boxes: list, eps: float, dt: float = 5e-5, qerrortol: flo
     else:
         nlev = -minlevel
     sizes = [n_root // (2 ** l) for l in range(nlev + 1)]
+    # Face codes of the root and the levels below it: one code for every
+    # face, or one per face (x-lo, x-hi, y-lo, y-hi[, z-lo, z-hi]).
+    codes = [mthbc] * (2 * nd) if isinstance(mthbc, int) else list(mthbc)[:2 * nd]
     for l in range(nlev + 1):
         n = sizes[l]
         parent = l + 1 if l < nlev else -1
         mb = [(1, n // 2)] * nd if l < nlev else [(1, n)] * nd
-        descs.append(_desc(-l, parent, (n,) * nd, mb, [(1, n)] * nd, [mthbc] * (2 * nd),
+        descs.append(_desc(-l, parent, (n,) * nd, mb, [(1, n)] * nd, list(codes),
                            h0 * (2 ** l), (0.0,) * nd))
     # Refined patches.
     for (level, lo, size) in boxes:
@@ -243,13 +246,13 @@ def build(n_root: int, boxes: list, eps: float, dt: float = 5e-5, qerrortol: flo
             raise ValueError("no parent patch contains the footprint")
         pg = descs[parent]["mglobal"]
         mb = [(foot_lo[k] - pg[k][0] + 1, foot_hi[k] - pg[k][0] + 1) for k in range(nd)]
-        codes = []
+        pc = []
         for k in range(nd):
-            codes.append(mthbc if glo[k] == 1 else INTERNAL)
-            codes.append(mthbc if ghi[k] == nglob else INTERNAL)
+            pc.append(codes[2 * k] if glo[k] == 1 else INTERNAL)
+            pc.append(codes[2 * k + 1] if ghi[k] == nglob else INTERNAL)
         h = h0 / (2 ** level)
         descs.append(_desc(level, parent, size, mb, [(glo[k], ghi[k]) for k in range(nd)],
-                           codes, h, tuple((glo[k] - 1) * h for k in range(nd))))
+                           pc, h, tuple((glo[k] - 1) * h for k in range(nd))))
     # Initial states.
     q0s = []
     for i, d in enumerate(descs):

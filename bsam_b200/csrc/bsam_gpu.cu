@@ -492,8 +492,10 @@ int face_rule(int ndims, int face, int code, int* rule) {
     *rule = (ndims == 2 && face >= 2) ? BC_COPY : BC_REFLECT;
   } else if (code == 999) {
     *rule = BC_NONE;
+  } else if (code == 2) {
+    *rule = BC_PERIODIC;  // both faces of the dimension (checked by the caller)
   } else {
-    return -1;  // periodic (2) is not supported by this build
+    return -1;
   }
   return 0;
 }
@@ -746,6 +748,21 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
     }
     if (!P.wt && d.level < 1)
       return fail(h, BSAM_ERR_UNSUPPORTED, "internal faces occur only on refined levels");
+    // Periodic faces (PeriodicSetup, boundary.f90:893-963): in pairs (the
+    // reference stops otherwise, bsamroutines.f90:307-316), on hierarchies
+    // without refined levels (TransferPeriodicBC between refined grids has no
+    // device form here), and on dimensions whose extent is even or 1: with an
+    // odd extent above 1 the first and last cells of the dimension have the
+    // same colour, and a colour pass would read the periodic ghost that its
+    // opposite cell writes through in the same pass.
+    for (int n = 0; n < nd; ++n) {
+      const bool lo = P.bc[2 * n] == BC_PERIODIC, hi = P.bc[2 * n + 1] == BC_PERIODIC;
+      if (lo != hi) return fail(h, BSAM_ERR_ARG, "periodic faces come in pairs");
+      if (lo && finestlevel > 0)
+        return fail(h, BSAM_ERR_UNSUPPORTED, "periodic faces with refined levels");
+      if (lo && P.n[n] > 1 && P.n[n] % 2)
+        return fail(h, BSAM_ERR_UNSUPPORTED, "periodic dimension with an odd extent above 1");
+    }
     // Does the V-cycle run on this record?  (Not on the masters of the mixed form.)
     const bool in_vcycle = !(h->mixed && !is_twin && d.level == finestlevel);
     // Mixed form: the V-cycle levels carry a correction of the master state
@@ -755,10 +772,12 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
       for (int f = 0; f < 2 * nd; ++f)
         if (P.bc[f] == BC_REFLECT) P.bc[f] = BC_NEGATE;
     // Fused stages: 3D V-cycle levels with a parent above the bottom, all
-    // faces physical.
+    // faces physical (the stage derives face ghosts from the tile itself).
     const int fmin = std::max(8, h->tuning.fuse_min_n);
+    bool periodic = false;
+    for (int f = 0; f < 2 * nd; ++f) periodic |= P.bc[f] == BC_PERIODIC;
     P.fused = (h->tuning.fuse_smoother != 0 && nd == 3 && finestlevel == 0 && in_vcycle &&
-               d.parent >= 0 &&
+               d.parent >= 0 && !periodic &&
                d.level > h->bottom_level && !(P.delta && P.prec == PREC_F64) &&
                P.n[0] >= fmin && P.n[1] >= fmin && P.n[2] >= fmin)
                   ? 1

@@ -17,13 +17,16 @@ constexpr int TILE_Y = 4;
 constexpr int BLOCK_THREADS = 32 * TILE_Y;
 
 // Per-face ghost rule applied by SetBC (boundary.f90:643-891):
-//   BC_NONE    ghost not written by SetBC (internal 999 / periodic 2 faces)
+//   BC_NONE    ghost not written by SetBC (internal 999 faces)
 //   BC_COPY    q(ghost) = q(mirror)            (mthbc 1; UserBC2D faces 3,4)
 //   BC_REFLECT q(ghost) = 2 - q(mirror)        (UserBC2D faces 1,2; UserBC3D)
 //   BC_NEGATE  e(ghost) = -e(mirror): BC_REFLECT seen by a correction e of a
 //              state q (q = base + e and both obey 2 - q), used by the
 //              correction-form levels of the mixed precision cycle
-enum : int32_t { BC_NONE = 0, BC_COPY = 1, BC_REFLECT = 2, BC_NEGATE = 3 };
+//   BC_PERIODIC (mthbc 2 on both faces of a dimension; PeriodicBC,
+//              boundary.f90:417-483, with qpo = 0): the low ghost takes the
+//              patch's last interior layer, the high ghost its first
+enum : int32_t { BC_NONE = 0, BC_COPY = 1, BC_REFLECT = 2, BC_NEGATE = 3, BC_PERIODIC = 4 };
 
 enum : int32_t { PREC_F64 = 0, PREC_F32 = 1 };
 
@@ -35,7 +38,7 @@ struct DevPatch {
   int32_t bc[6];      // BC_* per face (x-lo, x-hi, y-lo, y-hi, z-lo, z-hi)
   int32_t parent;     // patch index of the parent, -1 on the coarsest level
   int32_t level;
-  int32_t wt;         // 1: every face physical -> kernels write ghosts through
+  int32_t wt;         // 1: every face physical or periodic -> kernels write ghosts through
   int32_t prec;       // PREC_*
   int32_t problem;    // problem (batch slot) this patch belongs to
   int32_t fused;      // 1: smoothing stages run the fused kernel (q -> qb -> q)

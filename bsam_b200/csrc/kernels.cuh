@@ -38,8 +38,9 @@ template <class T> __device__ __forceinline__ T bc_map(int code, T v) {
 }
 
 // Choice s of one dimension for a ghost combination: 0 = the cell's own
-// coordinate, 1 = the low ghost (coordinate 1 on a physical low face),
-// 2 = the high ghost (coordinate n on a physical high face).
+// coordinate, 1 = the low ghost (fed by coordinate 1 on a physical low face,
+// by coordinate n on a periodic one), 2 = the high ghost (fed by coordinate n
+// on a physical high face, by coordinate 1 on a periodic one).
 __device__ __forceinline__ bool ghost_choice(int s, int co, int n, int lo_code, int hi_code,
                                              int& g, int& code) {
   if (s == 0) {
@@ -50,10 +51,12 @@ __device__ __forceinline__ bool ghost_choice(int s, int co, int n, int lo_code, 
   if (s == 1) {
     g = 0;
     code = lo_code;
+    if (lo_code == BC_PERIODIC) return co == n;
     return co == 1 && lo_code != BC_NONE;
   }
   g = n + 1;
   code = hi_code;
+  if (hi_code == BC_PERIODIC) return co == 1;
   return co == n && hi_code != BC_NONE;
 }
 
@@ -541,10 +544,13 @@ __global__ void __launch_bounds__(BLOCK_THREADS)
   source_item<T, D>(PT, items[blockIdx.x], 0);
 }
 
-// SetBC (boundary.f90:598-891) for one patch, all ghost cells, any face
+// SetBC (boundary.f90:598-891), preceded by PeriodicBC on periodic faces
+// (boundary.f90:76-83, 417-483), for one patch, all ghost cells, any face
 // codes: a ghost is written when at least one of the dimensions it lies
-// outside of has a physical face; its value is the face maps of those
-// dimensions (ascending) applied to the cell reflected across them.
+// outside of has a physical or periodic face; its value is the face maps of
+// those dimensions (ascending; a periodic face maps a value to itself)
+// applied to the cell reflected across them (across a periodic face, the
+// cell at the other end).
 template <class T, int D>
 __global__ void k_setbc(const DevPatch* __restrict__ PT, int patch, int64_t ntotal) {
   const DevPatch P = PT[patch];
@@ -558,11 +564,11 @@ __global__ void k_setbc(const DevPatch* __restrict__ PT, int patch, int64_t ntot
 #pragma unroll
   for (int d = 0; d < D; ++d) {
     if (co[d] == 0 && P.bc[2 * d] != BC_NONE) {
-      src[d] = 1;
+      src[d] = P.bc[2 * d] == BC_PERIODIC ? P.n[d] : 1;
       codes[d] = P.bc[2 * d];
       write = true;
     } else if (co[d] == P.n[d] + 1 && P.bc[2 * d + 1] != BC_NONE) {
-      src[d] = P.n[d];
+      src[d] = P.bc[2 * d + 1] == BC_PERIODIC ? 1 : P.n[d];
       codes[d] = P.bc[2 * d + 1];
       write = true;
     }

@@ -82,6 +82,10 @@ struct Ctx {
   int maxvcycles = 20, nsmoothingpasses = 2, errortype = 1;
   int minlevel = 0, finestlevel = 0;
   static const int rootlevel = 0;
+  // periodicboundaryconditions (nodeinfodef.f90:50), set by PeriodicSetup
+  // (boundary.f90:893-963) when a root face has code 2; qpo = 0
+  // (bsamroutines.f90:241).
+  bool periodic = false;
   std::vector<std::unique_ptr<Patch>> store;
   // levels[level - minlevel] in ApplyOnLevel order (youngest first).
   std::vector<std::vector<Patch*>> levels;
@@ -791,10 +795,40 @@ void GhostOverlap(const Ctx& c, Patch& g1, Patch& g2) {
   copy(g2, mg2, g1, mg1, ovg2);
 }
 
+// PeriodicBC (boundary.f90:417-483), mbc = 1 and qpo = 0: a grid whose two
+// faces of a dimension are periodic copies its first interior layer into the
+// high ghost layer, then its last into the low one, dimension by dimension,
+// whole layers (the ghost rows of the other dimensions included).
+void PeriodicBC(const Ctx& c, Patch& p) {
+  if (p.tobedeleted) return;
+  const int nd = c.ndims;
+  const int lo[3] = {0, 0, nd == 3 ? 0 : 1};
+  const int hi[3] = {p.mx[0] + 1, p.mx[1] + 1, nd == 3 ? p.mx[2] + 1 : 1};
+  for (int dim = 0; dim < nd; ++dim) {
+    if (!(p.mthbc[2 * dim] == 2 && p.mthbc[2 * dim + 1] == 2)) continue;
+    const int m = p.mx[dim];
+    for (int v = 1; v <= p.nrvars; ++v)
+      for (int pass = 0; pass < 2; ++pass) {
+        const int g = pass == 0 ? m + 1 : 0, from = pass == 0 ? 1 : m;
+        for (int k = lo[2]; k <= hi[2]; ++k)
+          for (int j = lo[1]; j <= hi[1]; ++j)
+            for (int i = lo[0]; i <= hi[0]; ++i) {
+              int idx[3] = {i, j, k};
+              if (idx[dim] != g) continue;
+              int src[3] = {i, j, k};
+              src[dim] = from;
+              p.q(i, j, k, v) = p.q(src[0], src[1], src[2], v);
+            }
+      }
+  }
+}
+
 // SetGhost (boundary.f90:58-89): above the root level, coarse-fine
 // interpolation on every grid (ApplyOnLevel order), then the sibling
 // exchange over all pairs (ApplyOnLevelPairs: each grid with every later
-// one), then the physical boundary conditions.  No periodic grids.
+// one); with periodic faces, PeriodicBC on every grid (periodic grids exist
+// at and below the root only: TransferPeriodicBC between refined grids is
+// not restated); then the physical boundary conditions.
 int SetGhost(Ctx& c, int level, int ipass) {
   int err = 0;
   if (level > Ctx::rootlevel) {
@@ -810,6 +844,8 @@ int SetGhost(Ctx& c, int level, int ipass) {
       for (size_t b = a + 1; b < L.size(); ++b)
         if (!L[a]->tobedeleted && !L[b]->tobedeleted) GhostOverlap(c, *L[a], *L[b]);
   }
+  if (c.periodic)
+    for (Patch* p : c.on(level)) PeriodicBC(c, *p);
   for (Patch* p : c.on(level)) err |= SetBC(c, *p);
   return err;
 }
@@ -1094,9 +1130,16 @@ int BuildUniform(Ctx& c, const orc_params* p) {
     if (p->mx[n] <= 0 || p->mx[n] % 2 != 0) return -3;
     if (p->xupper[n] <= p->xlower[n]) return -4;
   }
+  // Physical (1, 10-99) or periodic (2, both faces of a dimension; the
+  // reference stops on an unpaired periodic face, bsamroutines.f90:307-316).
   for (int f = 0; f < 2 * p->ndims; ++f) {
     int code = p->mthbc[f];
-    if (!(code == 1 || (code >= 10 && code <= 99))) return -5;  // no periodic
+    if (code == 2) {
+      if (p->mthbc[f ^ 1] != 2) return -5;
+      c.periodic = true;
+      continue;
+    }
+    if (!(code == 1 || (code >= 10 && code <= 99))) return -5;
   }
   c.ndims = p->ndims;
   c.dt = p->dt;
@@ -1160,6 +1203,11 @@ int BuildUniform(Ctx& c, const orc_params* p) {
 // each level): the nodeinfo fields the hot path reads, fields allocated.
 int BuildFromPatches(Ctx& c, const orc_params* p, int npatch, const orc_patch* d) {
   if (p->ndims < 2 || p->ndims > 3 || p->errortype != 1 || npatch <= 0) return -1;
+  // Periodic faces on a hierarchy given patch by patch are not restated
+  // (TransferPeriodicBC between refined grids).
+  for (int i = 0; i < npatch; ++i)
+    for (int f = 0; f < 2 * p->ndims; ++f)
+      if (d[i].mthbc[f] == 2) return -5;
   c.ndims = p->ndims;
   c.dt = p->dt;
   c.qerrortol = p->qerrortol;

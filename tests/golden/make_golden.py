@@ -164,7 +164,11 @@ def run_composition(hier, nsteps):
          "sourcefield": 1, "solutionfield": 2, "err_ok": 0, "finestlevel": finest,
          "minlevel": minlevel, "maxvcycles": hier.maxvcycles, "qerrortol": hier.qerrortol,
          "nsmoothingpasses": hier.nsmoothingpasses, "updateauxfreq": 1, "errortype": 1,
-         "eqtag": 1, "lconverged": False, "periodicboundaryconditions": False,
+         "eqtag": 1, "lconverged": False,
+         # PeriodicSetup (boundary.f90:893-963) for a root with periodic
+         # faces; qpo = 0 (bsamroutines.f90:241).
+         "periodicboundaryconditions": any(c == 2 for d in hier.descs for c in d["mthbc"]),
+         "qpo": fa(np.zeros(25), (1,)),
          "integralresult": fa(np.zeros(2), (1,)), "componentintegral": fa(np.zeros(25), (1,))}
     I = F.Interp(routines, g, Tree(recs))
     for name, expr in consts.items():
@@ -211,11 +215,12 @@ def uniform_hierarchy(nd, n, mthbc, eps, qerrortol, maxvcycles, seed):
         return amr.build(n, [], eps=eps, qerrortol=qerrortol, mthbc=mthbc, seed=seed,
                          field="wave", maxvcycles=maxvcycles)
     descs, m, lev = [], n, 0
+    codes = [mthbc] * 6 if isinstance(mthbc, int) else list(mthbc)
     while True:
         coarser = m % 2 == 0 and lev < 10
         descs.append({"level": -lev, "parent": lev + 1 if coarser else -1, "mx": [m] * 3,
                       "mbounds": [[1, m // 2 if coarser else m]] * 3, "mglobal": [[1, m]] * 3,
-                      "mthbc": [mthbc] * 6, "dx": (1.0 / n) * 2 ** lev, "xlower": [0.0] * 3})
+                      "mthbc": list(codes), "dx": (1.0 / n) * 2 ** lev, "xlower": [0.0] * 3})
         if not coarser:
             break
         m //= 2
@@ -373,6 +378,11 @@ def composition_cases():
         "mg_uniform2d": (uniform_hierarchy(2, 16, 1, 0.05, 1e-10, 8, 7), 2),
         # 8^3 root, levels 0..-3, user-coded faces.
         "mg_uniform3d": (uniform_hierarchy(3, 8, 10, 0.1, 1e-10, 6, 8), 2),
+        # 16^2 root, levels 0..-4, periodic in x, Neumann in y (the shipped
+        # example's x faces, griddata.dat:61-62).
+        "mg_periodic2d": (uniform_hierarchy(2, 16, (2, 2, 1, 1), 0.05, 1e-10, 8, 7), 2),
+        # 8^3 root, levels 0..-3, periodic in x and z, user-coded y faces.
+        "mg_periodic3d": (uniform_hierarchy(3, 8, (2, 2, 12, 11, 2, 2), 0.1, 1e-10, 6, 8), 2),
         # 16^2 root, two siblings on level 1 (one on a physical corner), one
         # level-2 patch.
         "mg_amr2d": (amr.build(16, [(1, (1, 1), (12, 16)), (1, (13, 9), (14, 12)),

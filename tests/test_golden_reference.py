@@ -146,7 +146,8 @@ def test_multigrid_composition_matches_reference(oracle, golden_hier, name):
     assert np.array_equal(got, d["q_out"])
 
 
-@pytest.mark.parametrize("name", ["mg_uniform2d", "mg_uniform3d"])
+@pytest.mark.parametrize("name", ["mg_uniform2d", "mg_uniform3d", "mg_periodic2d",
+                                  "mg_periodic3d"])
 def test_uniform_time_loop_matches_reference(oracle, golden_hier, name):
     """orc_run_uniform (its own root and below-root construction) against the
     same fixtures: the whole residual trace of every step and the final q."""

@@ -18,7 +18,8 @@ pytestmark = pytest.mark.gpu
 RTOL = 1e-11
 
 
-@pytest.mark.parametrize("name", ["mg_uniform2d", "mg_uniform3d", "mg_amr2d", "mg_amr3d"])
+@pytest.mark.parametrize("name", ["mg_uniform2d", "mg_uniform3d", "mg_amr2d", "mg_amr3d",
+                                  "mg_periodic2d", "mg_periodic3d"])
 def test_engine_matches_reference_composition(gpu_lib, golden_hier, name):
     hier, d = golden_hier(name)
     nsteps = int(d["nsteps"])

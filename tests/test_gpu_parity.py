@@ -193,3 +193,43 @@ def test_energy_unsupported_in_3d(gpu_lib):
     with B.Solver(W.config3(nsteps=1, n=16)) as s:
         with pytest.raises(B.BsamError):
             s.energy()
+
+
+@pytest.mark.parametrize("n", [64, 128])
+def test_periodic_shipped_example_codes(gpu_lib, oracle, n):
+    # The shipped example's faces (griddata.dat:61-66: periodic x, user code
+    # 10 on y) and its eps and dt (problemdata.dat, rundata.dat) on an
+    # n x n/2 root over [0, 12.8] x [0, 6.4], seeded initial state, no
+    # refined levels.
+    prob = W.config1(nsteps=3, n=n)
+    prob.mx = (n, n // 2, 1)
+    prob.xupper = (12.8, 6.4, 1.0)
+    prob.mthbc = (2, 2, 10, 10, 1, 1)
+    prob.eps, prob.dt, prob.qerrortol = 0.018, 0.1, 1e-8
+    prob.c0 = 0.5 + 0.025 * W.uniform(41, n * (n // 2), -1.0, 1.0)
+    got, ref = compare(oracle, prob, 3)
+    assert np.array_equal(got["q"], ref["q"])
+
+
+def test_periodic_3d_and_mixed(gpu_lib, oracle):
+    prob = W.config3(nsteps=2, n=32)
+    prob.mthbc = (2, 2, 1, 1, 2, 2)
+    compare(oracle, prob, 2)
+    prob.qerrortol = 1e-8
+    ref = oracle.run_uniform(prob, nsteps=2)
+    with B.Solver(prob, precision=B.PREC_MIXED) as s:
+        got = s.run(2)
+    for st in range(2):
+        assert relerr(got["q"][st], ref["q"][st]) < 1e-7
+    assert np.all(got["residual"] < prob.qerrortol)
+
+
+def test_periodic_rejections(gpu_lib):
+    prob = W.config1(nsteps=1, n=96)   # periodic extent 96 -> ... -> 3 (odd, above 1)
+    prob.mthbc = (2, 2, 1, 1, 1, 1)
+    with pytest.raises(B.BsamError):
+        B.Solver(prob)
+    prob = W.config1(nsteps=1, n=64)   # an unpaired periodic face
+    prob.mthbc = (2, 1, 1, 1, 1, 1)
+    with pytest.raises(B.BsamError):
+        B.Solver(prob)

@@ -188,3 +188,15 @@ def test_odd_coarsest(oracle):
     assert oracle.lib().orc_minlevel(oracle.params_of(prob)) == -5
     r = oracle.run_uniform(prob, keep_steps=False)
     assert np.all(r["residual"] < prob.qerrortol)
+
+
+def test_periodic_mass_conservation_and_ghosts(oracle):
+    # Periodic x, Neumann y: the scheme stays conservative, and after a step
+    # every periodic ghost column holds the opposite interior column.
+    prob = W.config1(nsteps=3, n=32)
+    prob.mthbc = (2, 2, 1, 1, 1, 1)
+    r = oracle.run_uniform(prob, nsteps=3)
+    m0 = prob.h ** 2 * prob.c0.sum()
+    assert np.all(np.abs(r["mass"] - m0) < 1e-9)
+    q = r["q"][-1]
+    assert np.array_equal(q[0, 1:-1], q[32, 1:-1]) and np.array_equal(q[33, 1:-1], q[1, 1:-1])

@@ -49,7 +49,7 @@ class StepResult(ctypes.Structure):
 class BatchTuning(ctypes.Structure):
     _fields_ = [("grid_ctas", ctypes.c_int32), ("eager", ctypes.c_int32),
                 ("per_pass", ctypes.c_int32), ("fused_ctas", ctypes.c_int32),
-                ("reserved", ctypes.c_int32 * 4)]
+                ("fused_occ", ctypes.c_int32), ("reserved", ctypes.c_int32 * 3)]
 
 
 class BatchStats(ctypes.Structure):
@@ -144,9 +144,9 @@ class Batch:
             self.set_tuning(grid_ctas=grid_ctas)
 
     def set_tuning(self, grid_ctas: int = 0, eager: int = 0, per_pass: int = 0,
-                   fused_ctas: int = 0):
+                   fused_ctas: int = 0, fused_occ: int = 0):
         t = BatchTuning(grid_ctas=grid_ctas, eager=eager, per_pass=per_pass,
-                        fused_ctas=fused_ctas)
+                        fused_ctas=fused_ctas, fused_occ=fused_occ)
         _check(_lib().bsam_batch_set_tuning(self.h, ctypes.byref(t)), self.h, "set_tuning")
 
     def profile(self, enable: bool = True):
@@ -277,7 +277,7 @@ class Batch:
 
 def solve_all(problems, precision: int = PREC_MIXED, max_slots: int | None = None,
               pool_bytes: int = 0, device: int = 0, grid_ctas: int = 0, eager: int = 0,
-              per_pass: int = 0, fused_ctas: int = 0):
+              per_pass: int = 0, fused_ctas: int = 0, fused_occ: int = 0):
     """Solves every problem (one dimensionality) in one batch; admits more as
     slots free up.  Returns the collect() results in input order."""
     if not problems:
@@ -287,9 +287,9 @@ def solve_all(problems, precision: int = PREC_MIXED, max_slots: int | None = Non
     tol = problems[0].qerrortol
     with Batch(nd, precision=precision, max_slots=ms, pool_bytes=pool_bytes, qerrortol=tol,
                maxvcycles=problems[0].maxvcycles, device=device) as b:
-        if grid_ctas or eager or per_pass or fused_ctas:
+        if grid_ctas or eager or per_pass or fused_ctas or fused_occ:
             b.set_tuning(grid_ctas=grid_ctas, eager=eager, per_pass=per_pass,
-                         fused_ctas=fused_ctas)
+                         fused_ctas=fused_ctas, fused_occ=fused_occ)
         out = [None] * len(problems)
         pending = list(range(len(problems)))
         slot_of = {}

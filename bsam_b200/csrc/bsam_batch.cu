@@ -595,15 +595,18 @@ void tick_t(bsam_batch* b, cudaGraphConditionalHandle handle, int in_graph) {
       // of an FP64 batch, a plain FP64 level.  The finest working level's
       // post-smoothing applies the FP64 update (kb_update skips those masters).
       const int upd = (b->mixed && d == 0 && dir == 1) ? 1 : 0;
-      if (b->mixed)
-        kb_smooth2<float, true><<<g, Fused2<float>::THREADS, Fused2<float>::smem(true), s>>>(
+      const int occ = b->tuning.fused_occ;
+      if (b->mixed) {
+        auto k = occ == 3 ? kb_smooth2<float, true, 3> : kb_smooth2<float, true, 4>;
+        k<<<g, Fused2<float>::THREADS, Fused2<float>::smem(true), s>>>(
             pt, L[L_FUSED + d].d, cnt + L_FUSED + d, dir, nu, upd, dir, 1 - dir,
             &b->d_ctl->kerr);
-      else
-        kb_smooth2<double, false>
-            <<<g, Fused2<double>::THREADS, Fused2<double>::smem(false), s>>>(
-                pt, L[L_FUSED + d].d, cnt + L_FUSED + d, dir, nu, 0, dir, 1 - dir,
-                &b->d_ctl->kerr);
+      } else {
+        auto k = occ == 4 ? kb_smooth2<double, false, 4> : kb_smooth2<double, false, 3>;
+        k<<<g, Fused2<double>::THREADS, Fused2<double>::smem(false), s>>>(
+            pt, L[L_FUSED + d].d, cnt + L_FUSED + d, dir, nu, 0, dir, 1 - dir,
+            &b->d_ctl->kerr);
+      }
       ++n;
     }
     stage_mark(b, d, false, dir);
@@ -832,10 +835,16 @@ int bsam_batch_create(bsam_batch** out, int device, const bsam_batch_params* p) 
             cudaMalloc(&b->d_counts, sizeof(int) * NLIST) == cudaSuccess;
   if (ok) ok = cudaHostGetDevicePointer((void**)&b->d_out, b->h_out, 0) == cudaSuccess;
   if (ok)
-    ok = cudaFuncSetAttribute(kb_smooth2<float, true>,
+    ok = cudaFuncSetAttribute(kb_smooth2<float, true, 3>,
                               cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)Fused2<float>::SMEM) == cudaSuccess &&
-         cudaFuncSetAttribute(kb_smooth2<double, false>,
+         cudaFuncSetAttribute(kb_smooth2<float, true, 4>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)Fused2<float>::SMEM) == cudaSuccess &&
+         cudaFuncSetAttribute(kb_smooth2<double, false, 3>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)Fused2<double>::SMEM) == cudaSuccess &&
+         cudaFuncSetAttribute(kb_smooth2<double, false, 4>,
                               cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)Fused2<double>::SMEM) == cudaSuccess;
   if (!ok) {
@@ -900,7 +909,8 @@ int bsam_batch_destroy(bsam_batch* b) {
 
 int bsam_batch_set_tuning(bsam_batch* b, const bsam_batch_tuning* t) {
   if (!b || !t || t->grid_ctas < 0 || t->eager < 0 || t->eager > 1 || t->per_pass < 0 ||
-      t->per_pass > 1 || t->fused_ctas < 0)
+      t->per_pass > 1 || t->fused_ctas < 0 ||
+      (t->fused_occ != 0 && t->fused_occ != 3 && t->fused_occ != 4))
     return BSAM_ERR_ARG;
   b->tuning = *t;
   b->need_capture = true;

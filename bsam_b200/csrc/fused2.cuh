@@ -19,9 +19,9 @@
 // buffer and writes the other (q -> qb before the coarse-grid correction,
 // qb -> q after it), so no tile reads a neighbour's already-smoothed cells.
 //
-// Thread layout: warp w takes rows w, w + 8, ...; lane l the cell pair
-// (2l, 2l+1) of a row, of which it updates the one of the pass's colour.
-// TX = 56 keeps the widest pass (TX + 6 cells) within 31 pairs.
+// Thread layout of a pass: warp w takes a contiguous band of row pairs, lane
+// l the columns 2l, 2l+1 of its rows (smooth_band).  TX = 56 keeps the widest
+// pass (TX + 6 cells) within the 64 columns of a warp.
 #pragma once
 #include "kernels.cuh"
 #include "smooth_fused.cuh"
@@ -69,27 +69,245 @@ __device__ __forceinline__ bool mbar_wait_backoff(uint64_t* b, uint32_t parity, 
   return false;
 }
 
-// Ghost images of the updated cell (i,j) inside the shared tile: the face
-// maps of SetBC2D (boundary.f90:661-738), as write_through applies them.
+// Physical face ghosts of a shared tile, refreshed from the interior cells
+// next to them: ghost = the face map of SetBC2D (boundary.f90:661-738) of its
+// mirror cell.  In a 5-point colour pass a face ghost is read only by its own
+// mirror cell, the one that writes it through in the reference's order
+// (SetGhost after the pass), so refreshing every face ghost of the tile after
+// a pass gives the ghosts the next pass reads exactly; corners are never
+// read.  Only tiles that hold a patch face call this.
 template <class T>
-__device__ __forceinline__ void smem_ghosts2(const DevPatch& P, T* s0, T* s1, int si, int i,
-                                             int j, T v0, T v1) {
+__device__ __forceinline__ void refresh_faces(const DevPatch& P, T* s0, T* s1, int gx0, int gy0) {
+  constexpr int RX = Fused2<T>::RX, RY = Fused2<T>::RY;
+  const int n0 = P.n[0], n1 = P.n[1];
+  // Interior cells held by the tile with both neighbours in the tile.
+  const int cx0 = max(1, 1 - gx0), cx1 = min(RX - 1, n0 + 1 - gx0);
+  const int cy0 = max(1, 1 - gy0), cy1 = min(RY - 1, n1 + 1 - gy0);
+  const int t = threadIdx.x;
+  if (t < RY) {
+    const int sy = t;
+    if (sy >= cy0 && sy < cy1) {
+      const int lo = 1 - gx0, hi = n0 - gx0;
+      if (P.bc[0] != BC_NONE && lo >= 1 && lo <= RX - 2) {
+        const int c = sy * RX + lo;
+        s0[c - 1] = bc_map<T>(P.bc[0], s0[c]);
+        s1[c - 1] = bc_map<T>(P.bc[0], s1[c]);
+      }
+      if (P.bc[1] != BC_NONE && hi >= 1 && hi <= RX - 2) {
+        const int c = sy * RX + hi;
+        s0[c + 1] = bc_map<T>(P.bc[1], s0[c]);
+        s1[c + 1] = bc_map<T>(P.bc[1], s1[c]);
+      }
+    }
+  } else if (t >= 64 && t < 64 + RX) {
+    const int sx = t - 64;
+    if (sx >= cx0 && sx < cx1) {
+      const int lo = 1 - gy0, hi = n1 - gy0;
+      if (P.bc[2] != BC_NONE && lo >= 1 && lo <= RY - 2) {
+        const int c = lo * RX + sx;
+        s0[c - RX] = bc_map<T>(P.bc[2], s0[c]);
+        s1[c - RX] = bc_map<T>(P.bc[2], s1[c]);
+      }
+      if (P.bc[3] != BC_NONE && hi >= 1 && hi <= RY - 2) {
+        const int c = hi * RX + sx;
+        s0[c + RX] = bc_map<T>(P.bc[3], s0[c]);
+        s1[c + RX] = bc_map<T>(P.bc[3], s1[c]);
+      }
+    }
+  }
+}
+
+template <class T> struct Pair2;
+template <> struct Pair2<float> { using V = float2; };
+template <> struct Pair2<double> { using V = double2; };
+
+// Constants of a level's FP32 Newton update as packed pairs, with the signs
+// folded in (negation is exact, so -x * y, x * -y and -(x * y) round alike).
+struct RelaxK2 {
+  float2 tmp1, ntmp2, tmp3, alpha, nalpha, three, mhalf, one, a12, na12;
+};
+
+__device__ __forceinline__ float2 splat2(float a) { return make_float2(a, a); }
+
+__device__ __forceinline__ RelaxK2 relax_k2(float tmp1, float tmp2, float tmp3, float alpha) {
+  RelaxK2 K;
+  K.tmp1 = splat2(tmp1);
+  K.ntmp2 = splat2(-tmp2);
+  K.tmp3 = splat2(tmp3);
+  K.alpha = splat2(alpha);
+  K.nalpha = splat2(-alpha);
+  K.three = splat2(3.f);
+  K.mhalf = splat2(-0.5f);
+  K.one = splat2(1.f);
+  // a12 = tmp1 * (m1 + m2 + m3 + m4) with Mob = 1: tmp1 * 4, exact.
+  K.a12 = splat2(tmp1 * 4.f);
+  K.na12 = splat2(-(tmp1 * 4.f));
+  return K;
+}
+
+// RelaxCell's FP32 Newton update (problem_ch.cuh) of two cells at once, one
+// in each half of the packed pairs, with Blackwell's paired FP32 arithmetic.
+// Every operation is RelaxCell's, in its order and rounding (x - 0.5 is
+// x + (-0.5); the negated products are the same products of negated
+// operands), so each half equals RelaxCell<float, 2> bit for bit.
+template <bool DELTA>
+__device__ __forceinline__ void relax_pair_f32(float2 pc, float2 pw, float2 pe, float2 ps,
+                                               float2 pn, float2 mw, float2 me, float2 ms,
+                                               float2 mn, float2 f0, float2 f1, float2 bs,
+                                               const RelaxK2& K, float2& phi, float2& mu) {
+  const float2 smu = __fadd2_rn(__fadd2_rn(__fadd2_rn(mw, me), ms), mn);
+  const float2 sph = __fadd2_rn(__fadd2_rn(__fadd2_rn(pe, pw), pn), ps);
+  const float2 cfull = DELTA ? __fadd2_rn(bs, pc) : pc;
+  const float2 cmh = __fadd2_rn(cfull, K.mhalf);
+  const float2 u = __fmul2_rn(__fmul2_rn(K.three, cmh), cmh);
+  const float2 d2 = __fmul2_rn(u, K.alpha);     // D2fc(cfull)
+  const float2 nd2 = __fmul2_rn(u, K.nalpha);   // -D2fc(cfull)
+  const float2 na21 = __fadd2_rn(d2, K.tmp3);   // -a21
+  float2 nl;
+  if (DELTA) {
+    // DfcDelta(base, e): alpha e (3 c^2 + 3 c e + e^2), c = base - 1/2.
+    const float2 c = __fadd2_rn(bs, K.mhalf);
+    const float2 c3 = __fmul2_rn(K.three, c);
+    const float2 poly =
+        __fadd2_rn(__fadd2_rn(__fmul2_rn(c3, c), __fmul2_rn(c3, pc)), __fmul2_rn(pc, pc));
+    nl = __fmul2_rn(__fmul2_rn(K.alpha, pc), poly);
+  } else {
+    nl = __fmul2_rn(__fmul2_rn(__fmul2_rn(cmh, cmh), cmh), K.alpha);  // Dfc
+  }
+  const float2 b1 = __ffma2_rn(K.tmp1, smu, f0);
+  const float2 b2 = __ffma2_rn(K.ntmp2, sph, __ffma2_rn(nd2, pc, __fadd2_rn(f1, nl)));
+  const float2 det = __ffma2_rn(K.a12, na21, K.one);
+  float2 r;
+  r.x = __fdividef(1.f, det.x);
+  r.y = __fdividef(1.f, det.y);
+  phi = __fmul2_rn(__ffma2_rn(K.na12, b2, b1), r);
+  mu = __fmul2_rn(__ffma2_rn(na21, b1, b2), r);
+}
+
+// The Newton updates of cells A (row y) and B (row y + 1), by the working
+// type: FP32 as a packed pair, FP64 one cell at a time in the reference's
+// operation order.  Stencil order of a/b: pc, pw, pe, ps, pn, mw, me, ms, mn,
+// f0, f1, base.
+template <class T, bool DELTA> struct RelaxPair;
+template <bool DELTA> struct RelaxPair<float, DELTA> {
+  RelaxK2 K;
+  __device__ __forceinline__ explicit RelaxPair(const DevPatch& P)
+      : K(relax_k2(float(P.tmp1), float(P.tmp2), float(P.tmp3), float(P.alpha))) {}
+  __device__ __forceinline__ void operator()(const float (&a)[12], const float (&b)[12],
+                                             float& pa, float& ma, float& pb, float& mb) const {
+    float2 phi, mu;
+    auto v = [&](int k) { return make_float2(a[k], b[k]); };
+    relax_pair_f32<DELTA>(v(0), v(1), v(2), v(3), v(4), v(5), v(6), v(7), v(8), v(9), v(10),
+                          v(11), K, phi, mu);
+    pa = phi.x;
+    pb = phi.y;
+    ma = mu.x;
+    mb = mu.y;
+  }
+};
+template <bool DELTA> struct RelaxPair<double, DELTA> {
+  double tmp1, tmp2, tmp3, alpha;
+  __device__ __forceinline__ explicit RelaxPair(const DevPatch& P)
+      : tmp1(P.tmp1), tmp2(P.tmp2), tmp3(P.tmp3), alpha(P.alpha) {}
+  __device__ __forceinline__ void one(const double (&a)[12], double& p, double& m) const {
+    problem::Stencil<double, 2> st;
+    st.pc = a[0];
+    st.pm[0] = a[1];
+    st.pp[0] = a[2];
+    st.pm[1] = a[3];
+    st.pp[1] = a[4];
+    st.mm[0] = a[5];
+    st.mp[0] = a[6];
+    st.mm[1] = a[7];
+    st.mp[1] = a[8];
+    st.mc = 0.0;  // the Newton update does not read mu at the cell
+    if constexpr (DELTA)
+      problem::RelaxCell<double, 2, true>(st, a[9], a[10], tmp1, tmp2, tmp3, alpha, p, m, a[11]);
+    else
+      problem::RelaxCell<double, 2>(st, a[9], a[10], tmp1, tmp2, tmp3, alpha, p, m);
+  }
+  __device__ __forceinline__ void operator()(const double (&a)[12], const double (&b)[12],
+                                             double& pa, double& ma, double& pb,
+                                             double& mb) const {
+    one(a, pa, ma);
+    one(b, pb, mb);
+  }
+};
+
+// One colour pass over a band of row pairs of the shared tile.  Lane l holds
+// columns 2l and 2l+1 of every row it touches, read as one vector: per row
+// pair (y, y+1) it updates cell A = (2l + PA, y) and cell B = (2l + 1 - PA,
+// y + 1), the pass's colour in both rows (PA, the column parity of the
+// colour in row y, is the same for every pair of a pass).  The four
+// neighbours of A and B are the other colour, which the pass does not write:
+// the rows above and below come from the vectors of rows y - 1 .. y + 2
+// (rows y + 1 and y + 2 carry over to the next pair as its y - 1 and y), the
+// column beyond the lane's pair from the neighbouring lane by a shuffle.
+// Columns outside [xa, xb) and row yb are computed but not stored (at the
+// tile's outermost columns the shuffled neighbour is the lane's own value).
+template <class T, bool DELTA, int PA>
+__device__ __forceinline__ void smooth_band(T* s0, T* s1, const T* sf0, const T* sf1,
+                                            const T* sbs, int ylo, int yhi, int yb, int xa,
+                                            int xb, int lane, const RelaxPair<T, DELTA>& R) {
+  using V = typename Pair2<T>::V;
   constexpr int RX = Fused2<T>::RX;
-  if (i == 1 && P.bc[0] != BC_NONE) {
-    s0[si - 1] = bc_map<T>(P.bc[0], v0);
-    s1[si - 1] = bc_map<T>(P.bc[0], v1);
-  }
-  if (i == P.n[0] && P.bc[1] != BC_NONE) {
-    s0[si + 1] = bc_map<T>(P.bc[1], v0);
-    s1[si + 1] = bc_map<T>(P.bc[1], v1);
-  }
-  if (j == 1 && P.bc[2] != BC_NONE) {
-    s0[si - RX] = bc_map<T>(P.bc[2], v0);
-    s1[si - RX] = bc_map<T>(P.bc[2], v1);
-  }
-  if (j == P.n[1] && P.bc[3] != BC_NONE) {
-    s0[si + RX] = bc_map<T>(P.bc[3], v0);
-    s1[si + RX] = bc_map<T>(P.bc[3], v1);
+  constexpr int RV = RX / 2;  // vectors per shared row
+  const V* v0 = reinterpret_cast<const V*>(s0) + lane;
+  const V* v1 = reinterpret_cast<const V*>(s1) + lane;
+  const V* vf0 = reinterpret_cast<const V*>(sf0) + lane;
+  const V* vf1 = reinterpret_cast<const V*>(sf1) + lane;
+  const V* vbs = reinterpret_cast<const V*>(sbs) + lane;
+  const int xA = 2 * lane + PA, xB = 2 * lane + 1 - PA;
+  const bool inA = xA >= xa && xA < xb, inB = xB >= xa && xB < xb;
+  constexpr unsigned FULL = 0xffffffffu;
+  V ps = v0[(ylo - 1) * RV], p0 = v0[ylo * RV];
+  V ms = v1[(ylo - 1) * RV], m0 = v1[ylo * RV];
+  for (int y = ylo; y < yhi; y += 2) {
+    const V p1 = v0[(y + 1) * RV], p2 = v0[(y + 2) * RV];
+    const V m1 = v1[(y + 1) * RV], m2 = v1[(y + 2) * RV];
+    const V fa0 = vf0[y * RV], fb0 = vf0[(y + 1) * RV];
+    const V fa1 = vf1[y * RV], fb1 = vf1[(y + 1) * RV];
+    V ba{}, bb{};
+    if constexpr (DELTA) {
+      ba = vbs[y * RV];
+      bb = vbs[(y + 1) * RV];
+    }
+    T a[12], b[12];
+    if (PA == 0) {
+      // A = column 2l of row y, B = column 2l + 1 of row y + 1.
+      const T pwA = __shfl_up_sync(FULL, p0.y, 1), mwA = __shfl_up_sync(FULL, m0.y, 1);
+      const T peB = __shfl_down_sync(FULL, p1.x, 1), meB = __shfl_down_sync(FULL, m1.x, 1);
+      a[0] = p0.x; a[1] = pwA; a[2] = p0.y; a[3] = ps.x; a[4] = p1.x;
+      a[5] = mwA; a[6] = m0.y; a[7] = ms.x; a[8] = m1.x;
+      a[9] = fa0.x; a[10] = fa1.x; a[11] = ba.x;
+      b[0] = p1.y; b[1] = p1.x; b[2] = peB; b[3] = p0.y; b[4] = p2.y;
+      b[5] = m1.x; b[6] = meB; b[7] = m0.y; b[8] = m2.y;
+      b[9] = fb0.y; b[10] = fb1.y; b[11] = bb.y;
+    } else {
+      // A = column 2l + 1 of row y, B = column 2l of row y + 1.
+      const T peA = __shfl_down_sync(FULL, p0.x, 1), meA = __shfl_down_sync(FULL, m0.x, 1);
+      const T pwB = __shfl_up_sync(FULL, p1.y, 1), mwB = __shfl_up_sync(FULL, m1.y, 1);
+      a[0] = p0.y; a[1] = p0.x; a[2] = peA; a[3] = ps.y; a[4] = p1.y;
+      a[5] = m0.x; a[6] = meA; a[7] = ms.y; a[8] = m1.y;
+      a[9] = fa0.y; a[10] = fa1.y; a[11] = ba.y;
+      b[0] = p1.x; b[1] = pwB; b[2] = p1.y; b[3] = p0.x; b[4] = p2.x;
+      b[5] = mwB; b[6] = m1.y; b[7] = m0.x; b[8] = m2.x;
+      b[9] = fb0.x; b[10] = fb1.x; b[11] = bb.x;
+    }
+    T pA, mA, pB, mB;
+    R(a, b, pA, mA, pB, mB);
+    if (inA) {
+      s0[y * RX + xA] = pA;
+      s1[y * RX + xA] = mA;
+    }
+    if (inB && y + 1 < yb) {
+      s0[(y + 1) * RX + xB] = pB;
+      s1[(y + 1) * RX + xB] = mB;
+    }
+    ps = p1;
+    p0 = p2;
+    ms = m1;
+    m0 = m2;
   }
 }
 
@@ -202,11 +420,10 @@ __device__ __forceinline__ void restrict_tile2(const DevPatch& C, const DevPatch
 // restr (pre-smoothing): the tile's coarse cells are restricted into the
 // parent from shared memory (restrict_tile2), instead of by a kb_restrict
 // launch after the stage.
-// Four CTAs per SM (the shared tile allows four): the register cap this
-// implies costs a few spilled values outside the passes; without it the
-// kernel takes 80 registers and three CTAs per SM, which measured slower.
-template <class T, bool DELTA>
-__global__ void __launch_bounds__(Fused2<T>::THREADS, 4)
+// MINB CTAs per SM (the shared tile allows four): four caps a thread at 64
+// registers, three at 85.
+template <class T, bool DELTA, int MINB = (sizeof(T) == 4 ? 4 : 3)>
+__global__ void __launch_bounds__(Fused2<T>::THREADS, MINB)
     kb_smooth2(const DevPatch* __restrict__ PT, const Item* __restrict__ items,
                const int* __restrict__ count, int dir, int nu, int upd, int corr,
                int restr, int* __restrict__ err) {
@@ -256,92 +473,102 @@ __global__ void __launch_bounds__(Fused2<T>::THREADS, 4)
     if (ok && tid != 0) (void)mbar_try_wait(&bar, phase);
     phase ^= 1u;
     if (!ok) {
-      if (tid == 0) atomicExch(err, kErrTmaTimeout);
+      // The launch's results are void (the host reports the error).  Before
+      // the CTA exits, give the copies it started one more bounded wait, so
+      // that none is still writing into the shared tile when the CTA ends.
+      if (tid == 0) {
+        atomicExch(err, kErrTmaTimeout);
+        (void)mbar_wait_backoff(&bar, phase ^ 1u, kWaitPolls);
+      }
       break;
     }
     const int n0 = P.n[0], n1 = P.n[1];
+    // A tile that holds a physical face of the patch refreshes the face
+    // ghosts in shared memory after every change of its cells and writes
+    // them through to HBM; the other tiles need neither (uniform per CTA).
+    const bool edge_tile = P.wt && (gx0 <= 1 || gx0 + F::RX - 1 >= n0 || gy0 <= 1 ||
+                                    gy0 + F::RY - 1 >= n1);
     if (corr && P.parent >= 0) {
       const DevPatch R = PT[P.parent];
       if (P.pprec == PREC_F32) correct_tile2<T, float>(P, R, s0, s1, gx0, gy0);
       else correct_tile2<T, double>(P, R, s0, s1, gx0, gy0);
       __syncthreads();
-      // Face ghosts of the corrected boundary cells, for the cells whose
-      // neighbours lie in the tile (the passes read no others).
-      if (P.wt)
-        for (int c = tid; c < F::PLANE; c += F::THREADS) {
-          const int sx = c % F::RX, sy = c / F::RX;
-          if (sx < 1 || sx > F::RX - 2 || sy < 1 || sy > F::RY - 2) continue;
-          const int i = gx0 + sx, j = gy0 + sy;
-          if (i < 1 || i > n0 || j < 1 || j > n1) continue;
-          if (i == 1 || i == n0 || j == 1 || j == n1) smem_ghosts2<T>(P, s0, s1, c, i, j, s0[c], s1[c]);
-        }
-      __syncthreads();
+      if (edge_tile) {
+        refresh_faces<T>(P, s0, s1, gx0, gy0);
+        __syncthreads();
+      }
     }
     T* o0 = fld<T>(dir == 0 ? P.qb[0] : P.q[0]);
     T* o1 = fld<T>(dir == 0 ? P.qb[1] : P.q[1]);
-    const T tmp1 = T(P.tmp1), tmp2 = T(P.tmp2), tmp3 = T(P.tmp3), alpha = T(P.alpha);
+    const RelaxPair<T, DELTA> relax(P);
     for (int p = 0; p < npass; ++p) {
       const int color = p & 1;
       const int grow = npass - 1 - p;
       // Region of this pass in shared coordinates, clipped to the interior.
       const int xa = max(F::H - grow, 1 - gx0), xb = min(F::H + F::TX + grow, n0 + 1 - gx0);
       const int ya = max(F::H - grow, 1 - gy0), yb = min(F::H + F::TY + grow, n1 + 1 - gy0);
-      // A warp's rows step by WARPS (even), so the column of the pass's
-      // colour in the lane's pair is the same on all of them.
-      const int sy0 = ya + warp;
-      int sx = xa + 2 * lane;
-      if ((gx0 + sx + gy0 + sy0 + color) & 1) ++sx;
-      if (sx < xb) {
-        const int i = gx0 + sx;
-        const bool edge_i = P.wt && (i == 1 || i == n0);
-        int si = sy0 * F::RX + sx;
-        for (int sy = sy0; sy < yb; sy += F::WARPS, si += F::WARPS * F::RX) {
-          problem::Stencil<T, 2> st;
-          st.pc = s0[si];
-          st.mc = s1[si];
-          st.pm[0] = s0[si - 1];
-          st.pp[0] = s0[si + 1];
-          st.mm[0] = s1[si - 1];
-          st.mp[0] = s1[si + 1];
-          st.pm[1] = s0[si - F::RX];
-          st.pp[1] = s0[si + F::RX];
-          st.mm[1] = s1[si - F::RX];
-          st.mp[1] = s1[si + F::RX];
-          T phi, mu;
-          if constexpr (DELTA)
-            problem::RelaxCell<T, 2, true>(st, sf0[si], sf1[si], tmp1, tmp2, tmp3, alpha, phi,
-                                           mu, sbs[si]);
-          else
-            problem::RelaxCell<T, 2>(st, sf0[si], sf1[si], tmp1, tmp2, tmp3, alpha, phi, mu);
-          s0[si] = phi;
-          s1[si] = mu;
-          const int j = gy0 + sy;
-          if (edge_i || (P.wt && (j == 1 || j == n1)))
-            smem_ghosts2<T>(P, s0, s1, si, i, j, phi, mu);
-        }
+      // Row pairs from ya, split into contiguous bands, one per warp.
+      const int npairs = (yb - ya + 1) >> 1;
+      const int per = (npairs + F::WARPS - 1) / F::WARPS;
+      const int k0 = warp * per, k1 = min(k0 + per, npairs);
+      // Column parity of the pass's colour in the rows ya, ya + 2, ...:
+      // (i + j) & 1 == color with i = gx0 + x, j = gy0 + y.
+      const int pa = (gx0 + gy0 + ya + color) & 1;
+      if (k0 < k1) {
+        if (pa == 0)
+          smooth_band<T, DELTA, 0>(s0, s1, sf0, sf1, sbs, ya + 2 * k0, ya + 2 * k1, yb, xa, xb,
+                                   lane, relax);
+        else
+          smooth_band<T, DELTA, 1>(s0, s1, sf0, sf1, sbs, ya + 2 * k0, ya + 2 * k1, yb, xa, xb,
+                                   lane, relax);
       }
       __syncthreads();
+      if (edge_tile && p + 1 < npass) {
+        refresh_faces<T>(P, s0, s1, gx0, gy0);
+        __syncthreads();
+      }
     }
+    using V = typename Pair2<T>::V;
+    // Columns 2l, 2l + 1 of the tile's interior: every pair starts at an odd
+    // global column, so the pair is one aligned vector in shared memory, in
+    // the level's rows and in the FP64 master's rows.
+    const int lx = 2 * lane;
+    const int gi = gx0 + F::H + lx;  // global column of the lane's first cell
     if (upd && P.master >= 0) {
       const DevPatch M = PT[P.master];
       double* m0 = fld<double>(M.q[0]);
       double* m1 = fld<double>(M.q[1]);
-      for (int ly = warp; ly < F::TY; ly += F::WARPS) {
-        const int j = gy0 + F::H + ly;
-        if (j > n1) break;
-        const int srow = (F::H + ly) * F::RX + F::H;
-        for (int lx = lane; lx < F::TX; lx += 32) {
-          const int i = gx0 + F::H + lx;
-          if (i > n0) break;
-          const int64_t c = cidx(M, i, j, 0);
-          const double na = m0[c] + (double)s0[srow + lx];
-          const double nb = m1[c] + (double)s1[srow + lx];
-          m0[c] = na;
-          m1[c] = nb;
-          if (M.wt && near_boundary(M, i, j, 0, 2))
-            write_through<double, 2>(M, m0, m1, i, j, 0, na, nb);
+      if (lx < F::TX && gi <= n0)
+        for (int ly = warp; ly < F::TY; ly += F::WARPS) {
+          const int j = gy0 + F::H + ly;
+          if (j > n1) break;
+          const int srow = (F::H + ly) * F::RX + F::H;
+          if (!edge_tile && gi + 1 <= n0) {
+            const V e0 = *reinterpret_cast<const V*>(s0 + srow + lx);
+            const V e1 = *reinterpret_cast<const V*>(s1 + srow + lx);
+            double2* a0 = reinterpret_cast<double2*>(m0 + cidx(M, gi, j, 0));
+            double2* a1 = reinterpret_cast<double2*>(m1 + cidx(M, gi, j, 0));
+            double2 x0 = *a0, x1 = *a1;
+            x0.x = x0.x + (double)e0.x;
+            x0.y = x0.y + (double)e0.y;
+            x1.x = x1.x + (double)e1.x;
+            x1.y = x1.y + (double)e1.y;
+            *a0 = x0;
+            *a1 = x1;
+            continue;
+          }
+          for (int d = 0; d < 2; ++d) {
+            const int i = gi + d;
+            if (i > n0) break;
+            const int64_t c = cidx(M, i, j, 0);
+            const double na = m0[c] + (double)s0[srow + lx + d];
+            const double nb = m1[c] + (double)s1[srow + lx + d];
+            m0[c] = na;
+            m1[c] = nb;
+            if (M.wt && near_boundary(M, i, j, 0, 2))
+              write_through<double, 2>(M, m0, m1, i, j, 0, na, nb);
+          }
         }
-      }
       __syncthreads();  // the shared tile is refilled for the next item
       continue;
     }
@@ -351,24 +578,28 @@ __global__ void __launch_bounds__(Fused2<T>::THREADS, 4)
       else restrict_tile2<T, double, DELTA>(P, R, s0, s1, sbs, gx0, gy0);
     }
     // Write back the tile's interior cells (warps over rows, lanes along
-    // them), ghosts by write-through.
-    for (int ly = warp; ly < F::TY; ly += F::WARPS) {
-      const int j = gy0 + F::H + ly;
-      if (j > n1) break;
-      const int srow = (F::H + ly) * F::RX + F::H;
-      T* r0 = o0 + (int64_t)j * P.sy;
-      T* r1 = o1 + (int64_t)j * P.sy;
-      const bool edge_j = P.wt && (j == 1 || j == n1);
-      for (int lx = lane; lx < F::TX; lx += 32) {
-        const int i = gx0 + F::H + lx;
-        if (i > n0) break;
-        const T v0 = s0[srow + lx], v1 = s1[srow + lx];
-        r0[i] = v0;
-        r1[i] = v1;
-        if (edge_j || (P.wt && (i == 1 || i == n0)))
-          write_through<T, 2>(P, o0, o1, i, j, 0, v0, v1);
+    // them, a pair per lane), ghosts by write-through on edge tiles.
+    if (lx < F::TX && gi <= n0)
+      for (int ly = warp; ly < F::TY; ly += F::WARPS) {
+        const int j = gy0 + F::H + ly;
+        if (j > n1) break;
+        const int srow = (F::H + ly) * F::RX + F::H;
+        T* r0 = o0 + (int64_t)j * P.sy;
+        T* r1 = o1 + (int64_t)j * P.sy;
+        if (!edge_tile && gi + 1 <= n0) {
+          *reinterpret_cast<V*>(r0 + gi) = *reinterpret_cast<const V*>(s0 + srow + lx);
+          *reinterpret_cast<V*>(r1 + gi) = *reinterpret_cast<const V*>(s1 + srow + lx);
+          continue;
+        }
+        for (int d = 0; d < 2; ++d) {
+          const int i = gi + d;
+          if (i > n0) break;
+          const T v0 = s0[srow + lx + d], v1 = s1[srow + lx + d];
+          r0[i] = v0;
+          r1[i] = v1;
+          if (P.wt && near_boundary(P, i, j, 0, 2)) write_through<T, 2>(P, o0, o1, i, j, 0, v0, v1);
+        }
       }
-    }
     __syncthreads();  // the shared tile is refilled for the next item
   }
 }

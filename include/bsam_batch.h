@@ -79,13 +79,16 @@ typedef struct {
  * graph's device-side loop (then advance runs exactly max_ticks ticks);
  * per_pass = 1 makes problems admitted afterwards smooth with one launch per
  * colour pass instead of the fused shared-memory stage of 2D levels;
- * fused_ctas caps the CTAs of a fused stage launch (0 = 4 per SM). */
+ * fused_ctas caps the CTAs of a fused stage launch (0 = 4 per SM);
+ * fused_occ picks the fused stage's build for 3 or 4 resident CTAs per SM
+ * (a register budget of 85 or 64 per thread; 0 = 4 for FP32, 3 for FP64). */
 typedef struct {
   int32_t grid_ctas;
   int32_t eager;
   int32_t per_pass;
   int32_t fused_ctas;
-  int32_t reserved[4];
+  int32_t fused_occ;
+  int32_t reserved[3];
 } bsam_batch_tuning;
 
 typedef struct {

@@ -492,8 +492,14 @@ def run_ours(args, world, rank, local):
                    "step_ms": [round(x, 3) for x in step_ms]},
         "roofline": {"bound": "hbm", "kernel": "kb_smooth2<float> (fused finest-depth "
                      "smoothing stages: nu=2 red-black sweeps of every problem, one launch "
-                     "each; the post-smoothing launch also applies the coarse-grid "
-                     "correction to its tiles and the FP64 update q64 += e)",
+                     "each; the pre-smoothing launch also restricts into the parent, the "
+                     "post-smoothing launch applies the coarse-grid correction and the FP64 "
+                     "update q64 += e)",
+                     "bytes_rule": "per finest cell, each field the stage must move once: "
+                                   "pre 3s+2s+5sp/4 (f1, f2, base read; state written; "
+                                   "parent q, qs, base written), post 5s+sp+32 (state, f1, "
+                                   "f2, base, parent q and qs read; FP64 master read and "
+                                   "written), s=4, sp=4 or 8",
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None,
                      "peak_source": peak_kind, "traffic": traffic,

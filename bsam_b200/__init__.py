@@ -73,7 +73,8 @@ ABI_SYMBOLS = (
     "bsam_batch_create", "bsam_batch_destroy", "bsam_batch_set_tuning", "bsam_batch_footprint",
     "bsam_batch_submit", "bsam_batch_advance", "bsam_batch_sync", "bsam_batch_run",
     "bsam_batch_poll", "bsam_batch_slot_phase", "bsam_batch_collect", "bsam_batch_get_stream", "bsam_batch_profile", "bsam_batch_submit_seeded", "bsam_batch_busy",
-    "bsam_batch_get_stats", "bsam_batch_last_error",
+    "bsam_batch_get_stats", "bsam_batch_last_error", "bsam_batch_submit_many",
+    "bsam_batch_submit_seeded_many", "bsam_batch_collect_many",
 )
 
 

@@ -85,6 +85,12 @@ def bind(L):
     L.bsam_batch_profile.argtypes = [vp, ctypes.c_int]
     L.bsam_batch_submit_seeded.argtypes = [vp, ctypes.POINTER(BatchProblem), ctypes.c_uint64,
                                            ctypes.c_double, ctypes.c_double, ip]
+    dpp = ctypes.POINTER(dp)
+    L.bsam_batch_submit_many.argtypes = [vp, ctypes.c_int, ctypes.POINTER(BatchProblem), dpp, ip]
+    L.bsam_batch_submit_seeded_many.argtypes = [vp, ctypes.c_int, ctypes.POINTER(BatchProblem),
+                                                ctypes.POINTER(ctypes.c_uint64), dp, dp, ip]
+    L.bsam_batch_collect_many.argtypes = [vp, ctypes.c_int, ip, dpp,
+                                          ctypes.POINTER(ctypes.POINTER(StepResult)), dp]
     L.bsam_batch_busy.argtypes = [vp]
     L.bsam_batch_get_stream.argtypes = [vp, ctypes.POINTER(vp)]
     L.bsam_batch_get_stats.argtypes = [vp, ctypes.POINTER(BatchStats)]
@@ -187,6 +193,80 @@ class Batch:
         _check(rc, self.h, "submit_seeded")
         self.probs[slot.value] = prob
         return slot.value
+
+    def submit_many(self, probs, q0s=None) -> list:
+        """Admits probs in order with batched device work (page-locked q0s
+        are read asynchronously: keep them unchanged until the next run /
+        sync / collect).  q0s: per problem its q0 (Fortran order), or None
+        for the seeded form.  Returns the slots; None for every problem from
+        the first one that did not fit."""
+        n = len(probs)
+        if n == 0:
+            return []
+        arr = (BatchProblem * n)(*[problem_struct(p) for p in probs])
+        slots = (ctypes.c_int * n)()
+        L = _lib()
+        if q0s is None:
+            seeds = (ctypes.c_uint64 * n)(*[p.seed for p in probs])
+            cbar = (ctypes.c_double * n)(*[p.cbar for p in probs])
+            amp = (ctypes.c_double * n)(*[p.amp for p in probs])
+            rc = L.bsam_batch_submit_seeded_many(self.h, n, arr, seeds, cbar, amp, slots)
+        else:
+            keep = [np.asfortranarray(q, dtype=np.float64) for q in q0s]
+            ptrs = (ctypes.POINTER(ctypes.c_double) * n)(
+                *[q.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) for q in keep])
+            rc = L.bsam_batch_submit_many(self.h, n, arr, ptrs, slots)
+            self._q0_keep = keep  # the copies may still be reading them
+        if rc < 0:
+            _check(rc, self.h, "submit_many")
+        out = []
+        for k in range(n):
+            if k < rc:
+                self.probs[slots[k]] = probs[k]
+                out.append(slots[k])
+            else:
+                out.append(None)
+        return out
+
+    def collect_many(self, slots, want_q: bool = True, outs=None, want_mass: bool = False):
+        """collect() of many finished slots with one wait; returns their
+        results in order.  outs: per slot a Fortran-ordered float64 array of
+        q's shape to copy into (page-locked ones are reached at full speed)."""
+        n = len(slots)
+        if n == 0:
+            return []
+        probs = [self.probs[s] for s in slots]
+        shapes = [tuple(m + 2 for m in p.mx[:p.ndims]) + (2,) for p in probs]
+        if outs is not None:
+            for o, shp in zip(outs, shapes):
+                if o.shape != shp or o.dtype != np.float64 or not o.flags["F_CONTIGUOUS"]:
+                    raise ValueError("out must be a Fortran-ordered float64 array of q's shape")
+            qs = list(outs)
+        else:
+            qs = [np.empty(shp, order="F") for shp in shapes] if want_q else [None] * n
+        steps = [(StepResult * p.nsteps)() for p in probs]
+        pq = (ctypes.POINTER(ctypes.c_double) * n)(
+            *[q.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if q is not None else None
+              for q in qs])
+        ps = (ctypes.POINTER(StepResult) * n)(
+            *[ctypes.cast(st, ctypes.POINTER(StepResult)) for st in steps])
+        masses = (ctypes.c_double * n)() if want_mass else None
+        rc = _lib().bsam_batch_collect_many(self.h, n, (ctypes.c_int * n)(*slots), pq, ps,
+                                            masses)
+        if rc == 0 or rc == ERR_DIVERGED:
+            for s in slots:
+                self.probs.pop(s, None)
+            self._q0_keep = None
+        _check(rc, self.h, "collect_many")
+        out = []
+        for k in range(n):
+            st = steps[k]
+            out.append({"q": qs[k],
+                        "nvcycles": np.array([x.nvcycles for x in st], dtype=np.int32),
+                        "converged": np.array([x.converged for x in st], dtype=np.int32),
+                        "residual": np.array([x.residual for x in st]),
+                        "mass": masses[k] if want_mass else None})
+        return out
 
     def busy(self) -> bool:
         rc = _lib().bsam_batch_busy(self.h)

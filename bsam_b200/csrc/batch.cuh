@@ -354,12 +354,11 @@ __device__ __forceinline__ double seeded_c(const DevPatch& P, uint64_t seed, dou
 
 // Interior of the state record `rec`: c and mu (ghosts by a k_setbc launch).
 template <int D>
-__global__ void k_init_seeded(const DevPatch* __restrict__ PT, int rec, uint64_t seed,
-                              double cbar, double amp, double k2) {
-  const DevPatch P = PT[rec];
+__device__ __forceinline__ void init_seeded_range(const DevPatch& P, uint64_t seed, double cbar,
+                                                  double amp, double k2, int64_t g0,
+                                                  int64_t gstep) {
   const int64_t n = (int64_t)P.n[0] * P.n[1] * (D == 3 ? P.n[2] : 1);
-  for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n;
-       g += (int64_t)gridDim.x * blockDim.x) {
+  for (int64_t g = g0; g < n; g += gstep) {
     const int i = (int)(g % P.n[0]) + 1;
     const int64_t r = g / P.n[0];
     const int j = (int)(r % P.n[1]) + 1;
@@ -382,6 +381,66 @@ __global__ void k_init_seeded(const DevPatch* __restrict__ PT, int rec, uint64_t
     fld<double>(P.q[0])[ci] = c;
     fld<double>(P.q[1])[ci] = mu;
   }
+}
+
+template <int D>
+__global__ void k_init_seeded(const DevPatch* __restrict__ PT, int rec, uint64_t seed,
+                              double cbar, double amp, double k2) {
+  const DevPatch P = PT[rec];
+  init_seeded_range<D>(P, seed, cbar, amp, k2, (int64_t)blockIdx.x * blockDim.x + threadIdx.x,
+                       (int64_t)gridDim.x * blockDim.x);
+}
+
+// ---- batched admission ---------------------------------------------------------
+//
+// Admitting many problems at once (bsam_batch_submit_many) stages their
+// patch records, tensor maps and slot states in page-locked host memory and
+// lets one launch scatter them (the device reads the host memory directly),
+// zeroes their pool regions in one launch and draws their seeded initial
+// states in one launch, instead of a few API calls per problem.
+
+// n 8-byte words from src to dst (either side may be page-locked host memory).
+struct WordSpan {
+  const uint64_t* src;
+  uint64_t* dst;
+  int64_t n;
+};
+
+__global__ void __launch_bounds__(256) k_word_spans(const WordSpan* __restrict__ spans) {
+  const WordSpan sp = spans[blockIdx.y];
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < sp.n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    sp.dst[i] = sp.src[i];
+}
+
+struct ZeroSpan {
+  uint64_t* dst;
+  int64_t n;
+};
+
+__global__ void __launch_bounds__(256) k_zero_spans(const ZeroSpan* __restrict__ spans) {
+  const ZeroSpan sp = spans[blockIdx.y];
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < sp.n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    sp.dst[i] = 0ull;
+}
+
+// The seeded initial state of one admitted problem (k_init_seeded's
+// arguments).
+struct SeedTask {
+  int32_t rec, pad_;
+  uint64_t seed;
+  double cbar, amp, k2;
+};
+
+template <int D>
+__global__ void k_init_seeded_list(const DevPatch* __restrict__ PT,
+                                   const SeedTask* __restrict__ tasks) {
+  const SeedTask t = tasks[blockIdx.y];
+  const DevPatch P = PT[t.rec];
+  init_seeded_range<D>(P, t.seed, t.cbar, t.amp, t.k2,
+                       (int64_t)blockIdx.x * blockDim.x + threadIdx.x,
+                       (int64_t)gridDim.x * blockDim.x);
 }
 
 __global__ void k_batch_budget(BatchCtl* __restrict__ ctl, int ticks) {

@@ -933,10 +933,9 @@ struct SeedInit {
   double cbar, amp;
 };
 
-static int admit(bsam_batch* b, const bsam_batch_problem* prob, const double* q0,
-                 const SeedInit* init, int* slot) {
-  if (!b || !prob || (!q0 && !init) || !slot) return BSAM_ERR_ARG;
-  CU(cudaSetDevice(b->device));
+// Host side of one admission: a free slot (compacting the lists if only
+// retired slots are left), a pool region and the slot's records.
+static int reserve(bsam_batch* b, const bsam_batch_problem* prob, int* slot) {
   SlotPlan probe;
   int rc = plan_slot(b, prob, 0, nullptr, probe);
   if (rc) return rc;
@@ -973,6 +972,43 @@ static int admit(bsam_batch* b, const bsam_batch_problem* prob, const double* q0
   S.used = true;
   S.stale = false;
   S.off = off;
+  *slot = s;
+  return BSAM_OK;
+}
+
+// Host bookkeeping of an admitted slot, once its device work is queued.
+static void enlist(bsam_batch* b, int s, const bsam_batch_problem* prob) {
+  const SlotPlan& S = b->slots[s];
+  const int rec0 = s * RMAX;
+  SlotCfg& C = b->h_cfg[s];
+  C.rec0 = rec0;
+  C.nrec = S.nrec;
+  C.master = rec0 + S.master;
+  C.nsteps = prob->nsteps;
+  C.maxv = b->bp.maxvcycles;
+  C.denom = 2.0 * (double)S.cells;
+  C.tol = b->bp.qerrortol;
+  append_items(b, s);
+  volatile SlotOut* o = b->h_out + s;
+  o->step = 0;
+  o->vcycles = 0;
+  o->phase = SLOT_RUNNING;
+}
+
+static double seed_k2(const bsam_batch_problem* prob, const DevPatch& M) {
+  return (prob->eps * prob->eps) / (M.h * M.h);
+}
+
+static int admit(bsam_batch* b, const bsam_batch_problem* prob, const double* q0,
+                 const SeedInit* init, int* slot) {
+  if (!b || !prob || (!q0 && !init) || !slot) return BSAM_ERR_ARG;
+  CU(cudaSetDevice(b->device));
+  int s = -1;
+  int rc = reserve(b, prob, &s);
+  if (rc) return rc;
+  SlotPlan& S = b->slots[s];
+  const int rec0 = s * RMAX;
+  const size_t off = S.off;
   const int nd = b->bp.ndims;
   // Fresh fields, records, the initial state and its ghosts.
   CU(cudaMemsetAsync(b->d_pool + off, 0, S.bytes, b->stream));
@@ -996,8 +1032,7 @@ static int admit(bsam_batch* b, const bsam_batch_problem* prob, const double* q0
                            e0 * sizeof(double), e0 * sizeof(double), (size_t)e1 * e2,
                            cudaMemcpyHostToDevice, b->stream));
   } else {
-    const double h = M.h;
-    const double k2 = (prob->eps * prob->eps) / (h * h);
+    const double k2 = seed_k2(prob, M);
     const int64_t ncell = S.cells;
     const int gi = (int)std::min<int64_t>((ncell + 255) / 256, 16 * b->nsm);
     if (nd == 2)
@@ -1015,22 +1050,124 @@ static int admit(bsam_batch* b, const bsam_batch_problem* prob, const double* q0
   SlotState z{SLOT_RUNNING, 0, 0, 0};
   rc = stage_copy(b, b->d_state + s, &z, sizeof(SlotState));
   if (rc) return rc;
-  SlotCfg& C = b->h_cfg[s];
-  C.rec0 = rec0;
-  C.nrec = S.nrec;
-  C.master = rec0 + S.master;
-  C.nsteps = prob->nsteps;
-  C.maxv = b->bp.maxvcycles;
-  C.denom = 2.0 * (double)S.cells;
-  C.tol = b->bp.qerrortol;
-  append_items(b, s);
-  volatile SlotOut* o = b->h_out + s;
-  o->step = 0;
-  o->vcycles = 0;
-  o->phase = SLOT_RUNNING;
+  enlist(b, s, prob);
   stage_commit(b);
   *slot = s;
   return BSAM_OK;
+}
+
+// Many admissions with their device work batched: one launch zeroes the
+// admitted pool regions, one scatters every record, tensor map and slot
+// state from page-locked staging, one draws the seeded states (or one pitched
+// copy per component and problem from q0s), one sets their ghosts.
+static int admit_many(bsam_batch* b, int n, const bsam_batch_problem* probs,
+                      const double* const* q0s, const SeedInit* inits, int* slots) {
+  if (!b || n < 0 || (n > 0 && (!probs || !slots)) || (!q0s && !inits)) return BSAM_ERR_ARG;
+  if (n == 0) return 0;
+  CU(cudaSetDevice(b->device));
+  // Every problem is checked before any is admitted.
+  for (int k = 0; k < n; ++k) {
+    SlotPlan probe;
+    const int rc = plan_slot(b, &probs[k], 0, nullptr, probe);
+    if (rc) return rc;
+    if (q0s && !q0s[k]) return fail(b, BSAM_ERR_ARG, "a q0 pointer is NULL");
+  }
+  std::vector<int> adm;
+  for (int k = 0; k < n; ++k) slots[k] = -1;
+  // Admission stops at the first problem that does not fit: the admitted
+  // ones are problems 0 .. na-1.  Each is listed at once, so that a
+  // compaction by a later reservation keeps its tiles exactly once.
+  for (int k = 0; k < n; ++k) {
+    int s = -1;
+    const int rc = reserve(b, &probs[k], &s);
+    if (rc == BSAM_ERR_NOMEM) break;
+    if (rc) return rc;
+    enlist(b, s, &probs[k]);
+    adm.push_back(s);
+    slots[k] = s;
+  }
+  const int na = (int)adm.size();
+  if (na == 0) return 0;
+  const int nd = b->bp.ndims;
+  // Staging layout: spans, zero spans, seed tasks, master records, then the
+  // words the spans copy (records, tensor maps, slot states).
+  int nspan = 0;
+  size_t words = 0;
+  for (int s : adm) {
+    const SlotPlan& S = b->slots[s];
+    nspan += 2;  // records, slot state
+    words += (sizeof(DevPatch) * S.nrec + sizeof(SlotState) + 7) / 8 + 1;
+    for (int r = 0; r < S.nrec; ++r)
+      if (S.recs[r].tmaps) {
+        ++nspan;
+        words += sizeof(CUtensorMap) * NMAPS / 8;
+      }
+  }
+  static_assert(sizeof(DevPatch) % 8 == 0 && sizeof(SlotState) % 8 == 0 &&
+                    sizeof(CUtensorMap) % 8 == 0,
+                "staged records are copied as 8-byte words");
+  const size_t bytes = sizeof(WordSpan) * nspan + sizeof(ZeroSpan) * na +
+                       sizeof(SeedTask) * na + sizeof(int) * (na + 1) + 8 * words + 64;
+  char* st = stage_alloc(b, bytes);
+  if (!st) return fail(b, BSAM_ERR_NOMEM, "pinned staging allocation failed");
+  WordSpan* spans = reinterpret_cast<WordSpan*>(st);
+  ZeroSpan* zs = reinterpret_cast<ZeroSpan*>(spans + nspan);
+  SeedTask* tasks = reinterpret_cast<SeedTask*>(zs + na);
+  int* masters = reinterpret_cast<int*>(tasks + na);
+  uint64_t* w = reinterpret_cast<uint64_t*>(
+      (reinterpret_cast<uintptr_t>(masters + na) + 7) & ~uintptr_t(7));
+  int sp = 0;
+  int64_t maxz = 0, maxw = 0, maxc = 0;
+  for (int a = 0; a < na; ++a) {
+    const int s = adm[a];
+    const SlotPlan& S = b->slots[s];
+    const int rec0 = s * RMAX;
+    const DevPatch& M = S.recs[S.master];
+    zs[a] = ZeroSpan{reinterpret_cast<uint64_t*>(b->d_pool + S.off), (int64_t)(S.bytes / 8)};
+    maxz = std::max<int64_t>(maxz, zs[a].n);
+    masters[a] = rec0 + S.master;
+    if (inits)
+      tasks[a] = SeedTask{rec0 + S.master, 0, inits[a].seed, inits[a].cbar, inits[a].amp,
+                          seed_k2(&probs[a], M)};
+    maxc = std::max<int64_t>(maxc, S.cells);
+    auto add = [&](void* dst, const void* src, size_t nbytes) {
+      std::memcpy(w, src, nbytes);
+      spans[sp++] = WordSpan{w, static_cast<uint64_t*>(dst), (int64_t)(nbytes / 8)};
+      maxw = std::max<int64_t>(maxw, (int64_t)(nbytes / 8));
+      w += nbytes / 8;
+    };
+    add(b->d_pt + rec0, S.recs.data(), sizeof(DevPatch) * S.nrec);
+    for (int r = 0; r < S.nrec; ++r)
+      if (S.recs[r].tmaps)
+        add(b->d_tmaps + (size_t)(rec0 + r) * NMAPS, &S.maps[(size_t)r * NMAPS],
+            sizeof(CUtensorMap) * NMAPS);
+    const SlotState z{SLOT_RUNNING, 0, 0, 0};
+    add(b->d_state + s, &z, sizeof(SlotState));
+  }
+  auto gx = [&](int64_t m) { return (unsigned)std::max<int64_t>(1, std::min<int64_t>((m + 255) / 256, 64)); };
+  k_zero_spans<<<dim3(gx(maxz), na), 256, 0, b->stream>>>(zs);
+  k_word_spans<<<dim3(gx(maxw), sp), 256, 0, b->stream>>>(spans);
+  if (inits) {
+    if (nd == 2) k_init_seeded_list<2><<<dim3(gx(maxc), na), 256, 0, b->stream>>>(b->d_pt, tasks);
+    else k_init_seeded_list<3><<<dim3(gx(maxc), na), 256, 0, b->stream>>>(b->d_pt, tasks);
+  } else {
+    // q0s: read by the copies queued here (page-locked memory asynchronously).
+    for (int a = 0; a < na; ++a) {
+      const SlotPlan& S = b->slots[adm[a]];
+      const DevPatch& M = S.recs[S.master];
+      const int e0 = M.n[0] + 2, e1 = M.n[1] + 2, e2 = nd == 3 ? M.n[2] + 2 : 1;
+      const size_t hcomp = (size_t)e0 * e1 * e2;
+      for (int c = 0; c < 2; ++c)
+        CU(cudaMemcpy2DAsync(M.q[c], M.sy * sizeof(double), q0s[a] + c * hcomp,
+                             e0 * sizeof(double), e0 * sizeof(double), (size_t)e1 * e2,
+                             cudaMemcpyHostToDevice, b->stream));
+    }
+  }
+  if (nd == 2) k_setbc_list<double, 2><<<dim3(gx(maxc), na), 256, 0, b->stream>>>(b->d_pt, masters);
+  else k_setbc_list<double, 3><<<dim3(gx(maxc), na), 256, 0, b->stream>>>(b->d_pt, masters);
+  CU(cudaGetLastError());
+  stage_commit(b);
+  return na;
 }
 
 int bsam_batch_submit(bsam_batch* b, const bsam_batch_problem* prob, const double* q0,
@@ -1043,6 +1180,21 @@ int bsam_batch_submit_seeded(bsam_batch* b, const bsam_batch_problem* prob, uint
                              double cbar, double amp, int* slot) {
   const SeedInit init{seed, cbar, amp};
   return admit(b, prob, nullptr, &init, slot);
+}
+
+int bsam_batch_submit_many(bsam_batch* b, int n, const bsam_batch_problem* probs,
+                           const double* const* q0s, int* slots) {
+  if (!q0s) return BSAM_ERR_ARG;
+  return admit_many(b, n, probs, q0s, nullptr, slots);
+}
+
+int bsam_batch_submit_seeded_many(bsam_batch* b, int n, const bsam_batch_problem* probs,
+                                  const uint64_t* seeds, const double* cbar, const double* amp,
+                                  int* slots) {
+  if (n > 0 && (!seeds || !cbar || !amp)) return BSAM_ERR_ARG;
+  std::vector<SeedInit> init((size_t)std::max(n, 0));
+  for (int k = 0; k < n; ++k) init[k] = SeedInit{seeds[k], cbar[k], amp[k]};
+  return admit_many(b, n, probs, nullptr, init.data(), slots);
 }
 
 int bsam_batch_busy(bsam_batch* b) {
@@ -1069,14 +1221,42 @@ int bsam_batch_advance(bsam_batch* b, int max_ticks) {
   // that each timed stage is attributed to the problems running in it.
   const cudaGraphConditionalHandle none = 0;
   for (int t = 0; t < max_ticks; ++t) {
-    int64_t cells0 = 0;
-    int es = b->mixed ? 4 : 8;
+    // Algorithmic bytes of the finest-depth stages of the problems running
+    // in this tick, per cell of their finest working level (s = bytes per
+    // value of that level, sp = of its parent):
+    //  pre-smoothing: read f1, f2 (+ the base, correction form) and, unless
+    //    the correction starts from zero, the state; write the smoothed
+    //    state; restrict into the parent (its q and qs, + base): 2 s + 1 s
+    //    (base) + 0 / 2 s (state) + 2 s + (4 | 5) sp / 4;
+    //  post-smoothing: read the pre-smoothed state, f1, f2 (+ base) and the
+    //    parent's q and qs for the correction (4 sp / 4); write the state,
+    //    or, with the FP64 update, read and write the FP64 master (32).
+    double pre_bytes = 0.0, post_bytes = 0.0;
     if (b->profiling) {
       CU(cudaStreamSynchronize(b->stream));
-      for (size_t s = 0; s < b->slots.size(); ++s)
-        if (b->slots[s].used && ((volatile SlotOut*)b->h_out)[s].phase == SLOT_RUNNING &&
-            b->slots[s].ntop > 0)
-          cells0 += b->slots[s].cells;
+      const bool fused = b->bp.ndims == 2 && !b->tuning.per_pass;
+      for (size_t s = 0; s < b->slots.size(); ++s) {
+        const SlotPlan& S = b->slots[s];
+        if (!S.used || ((volatile SlotOut*)b->h_out)[s].phase != SLOT_RUNNING || S.ntop < 1)
+          continue;
+        const int first = b->mixed ? 1 : 0;  // record of depth 0
+        const DevPatch& W = S.recs[first];
+        const double sw = W.prec == PREC_F32 ? 4.0 : 8.0;
+        const double sp = S.recs[first + 1].prec == PREC_F32 ? 4.0 : 8.0;
+        const double cells = (double)S.cells;
+        if (fused) {
+          const bool delta = W.delta != 0;
+          pre_bytes += cells * (2 * sw + (delta ? sw : 0.0) + (delta ? 0.0 : 2 * sw) + 2 * sw +
+                                (delta ? 5.0 : 4.0) * sp / 4.0);
+          post_bytes += cells * (4 * sw + (delta ? sw : 0.0) + sp +
+                                 (b->mixed ? 32.0 : 2 * sw));
+        } else {
+          // One launch per colour pass: each pass reads and writes the state
+          // and reads f (and the base): counted once per stage as 6 s.
+          pre_bytes += cells * 6 * sw;
+          post_bytes += cells * 6 * sw;
+        }
+      }
     }
     b->ev_used = 0;
     if (b->bp.ndims == 2) tick_t<2>(b, none, 0);
@@ -1089,20 +1269,7 @@ int bsam_batch_advance(bsam_batch* b, int max_ticks) {
         if (cudaEventElapsedTime(&ms, b->ev_pool[e].first, b->ev_pool[e].second) == cudaSuccess) {
           b->st.smooth_ms += ms;
           b->st.smooth_stages += 1;
-          // Read phi, mu, f1, f2, write phi, mu; the mixed 2D post-smoothing
-          // writes no e but reads and writes the FP64 master (q64 += e).  A
-          // fused 2D post-smoothing stage also does the coarse-grid
-          // correction, whose algorithmic bytes (read and write q, read the
-          // parent's change: 4 s + 2 s / 4 per cell) it adds.
-          const bool fused_post = b->bp.ndims == 2 && b->ev_post[e] && !b->tuning.per_pass;
-          const bool upd = b->mixed && fused_post;
-          double bytes = upd ? 4.0 * es + 32.0 : 6.0 * es;
-          if (fused_post) bytes += 4.0 * es + 0.5 * es;
-          // A fused 2D pre-smoothing stage also restricts into the parent:
-          // read q (done by the stage), write the parent's q and qs
-          // (2 s + 4 s / 4 per cell).
-          if (b->bp.ndims == 2 && !b->ev_post[e] && !b->tuning.per_pass) bytes += 3.0 * es;
-          b->st.smooth_bytes += bytes * (double)cells0;
+          b->st.smooth_bytes += b->ev_post[e] ? post_bytes : pre_bytes;
         }
       }
       b->ev_used = 0;
@@ -1242,6 +1409,99 @@ int bsam_batch_collect(bsam_batch* b, int slot, double* q, bsam_step_result* ste
   // Drop retired tiles once they outnumber the resident problems.
   if (dead > std::max(8, live)) compact(b);
   return ph == SLOT_FAILED ? fail(b, BSAM_ERR_DIVERGED, "residual is not finite") : BSAM_OK;
+}
+
+int bsam_batch_collect_many(bsam_batch* b, int n, const int* slots, double* const* qs,
+                            bsam_step_result* const* steps, double* masses) {
+  if (!b || n < 0 || (n > 0 && !slots)) return BSAM_ERR_ARG;
+  if (n == 0) return BSAM_OK;
+  CU(cudaSetDevice(b->device));
+  CU(cudaStreamSynchronize(b->stream));
+  for (int k = 0; k < n; ++k) {
+    const int s = slots[k];
+    if (s < 0 || s >= (int)b->slots.size() || !b->slots[s].used)
+      return fail(b, BSAM_ERR_ARG, "slot not resident");
+    for (int k2 = 0; k2 < k; ++k2)
+      if (slots[k2] == s) return fail(b, BSAM_ERR_ARG, "slot listed twice");
+    const int ph = ((volatile SlotOut*)b->h_out)[s].phase;
+    if (ph != SLOT_DONE && ph != SLOT_FAILED) return fail(b, BSAM_ERR_STATE, "problem not finished");
+  }
+  const int nd = b->bp.ndims;
+  // Step logs: one launch writes every slot's log into page-locked staging;
+  // masses: the per-slot reduction, each total copied into staging.
+  char* st = stage_alloc(b, sizeof(WordSpan) * n +
+                                sizeof(StepLog) * BSAM_BATCH_MAX_STEPS * n +
+                                sizeof(DevStatus) * n + 64);
+  if (!st) return fail(b, BSAM_ERR_NOMEM, "pinned staging allocation failed");
+  WordSpan* spans = reinterpret_cast<WordSpan*>(st);
+  StepLog* logs = reinterpret_cast<StepLog*>(spans + n);
+  DevStatus* stat = reinterpret_cast<DevStatus*>(logs + (size_t)BSAM_BATCH_MAX_STEPS * n);
+  int64_t maxw = 1;
+  for (int k = 0; k < n; ++k) {
+    const SlotPlan& S = b->slots[slots[k]];
+    const int64_t nw = (int64_t)(sizeof(StepLog) * S.prob.nsteps / 8);
+    spans[k] = WordSpan{reinterpret_cast<const uint64_t*>(b->d_log +
+                                                          (int64_t)slots[k] * BSAM_BATCH_MAX_STEPS),
+                        reinterpret_cast<uint64_t*>(logs + (size_t)k * BSAM_BATCH_MAX_STEPS), nw};
+    maxw = std::max(maxw, nw);
+  }
+  k_word_spans<<<dim3((unsigned)((maxw + 255) / 256), n), 256, 0, b->stream>>>(spans);
+  for (int k = 0; k < n; ++k) {
+    const SlotPlan& S = b->slots[slots[k]];
+    const DevPatch& M = S.recs[S.master];
+    if (qs && qs[k]) {
+      const int e0 = M.n[0] + 2, e1 = M.n[1] + 2, e2 = nd == 3 ? M.n[2] + 2 : 1;
+      const size_t hcomp = (size_t)e0 * e1 * e2;
+      for (int c = 0; c < 2; ++c)
+        CU(cudaMemcpy2DAsync(qs[k] + c * hcomp, e0 * sizeof(double), M.q[c],
+                             M.sy * sizeof(double), e0 * sizeof(double), (size_t)e1 * e2,
+                             cudaMemcpyDeviceToHost, b->stream));
+    }
+    if (masses) {
+      const SlotCfg& C = b->h_cfg[slots[k]];
+      const double hh = M.h;
+      const double hd = nd == 2 ? hh * hh : hh * hh * hh;
+      const int ni = C.ie - C.ib;
+      const Item* items = b->lists[L_MASTER].d + C.ib;
+      if (nd == 2)
+        k_mass<double, 2><<<ni, dim3(32, TILE_Y), 0, b->stream>>>(b->d_pt, items, b->d_partials,
+                                                                   b->d_status, ni, hd);
+      else
+        k_mass<double, 3><<<ni, dim3(32, TILE_Y), 0, b->stream>>>(b->d_pt, items, b->d_partials,
+                                                                   b->d_status, ni, hd);
+      CU(cudaMemcpyAsync(stat + k, b->d_status, sizeof(DevStatus), cudaMemcpyDeviceToHost,
+                         b->stream));
+    }
+  }
+  CU(cudaGetLastError());
+  stage_commit(b);
+  CU(cudaStreamSynchronize(b->stream));
+  int rc = BSAM_OK;
+  for (int k = 0; k < n; ++k) {
+    const int s = slots[k];
+    SlotPlan& S = b->slots[s];
+    const int done = ((volatile SlotOut*)b->h_out)[s].step;
+    const StepLog* lg = logs + (size_t)k * BSAM_BATCH_MAX_STEPS;
+    if (steps && steps[k])
+      for (int i = 0; i < S.prob.nsteps; ++i) {
+        steps[k][i].nvcycles = i < done ? lg[i].nv : 0;
+        steps[k][i].converged = i < done ? lg[i].conv : 0;
+        steps[k][i].residual = i < done ? lg[i].res : NAN;
+      }
+    if (masses) masses[k] = stat[k].mass;
+    if (((volatile SlotOut*)b->h_out)[s].phase == SLOT_FAILED) rc = BSAM_ERR_DIVERGED;
+    pool_free(b, S.off, S.bytes);
+    S.used = false;
+    S.stale = true;
+    ((volatile SlotOut*)b->h_out)[s].phase = SLOT_IDLE;
+  }
+  int live = 0, dead = 0;
+  for (auto& x : b->slots) {
+    if (x.used) ++live;
+    else if (x.stale) ++dead;
+  }
+  if (dead > std::max(8, live)) compact(b);
+  return rc == BSAM_OK ? BSAM_OK : fail(b, rc, "a residual is not finite");
 }
 
 int bsam_batch_get_stream(bsam_batch* b, void** stream) {

@@ -134,15 +134,19 @@ __global__ void __launch_bounds__(BLOCK_THREADS, 8)
         acc += r0 * r0 + r1 * r1;
         const int64_t cw = cidx(W, i, j, 0);
         if (W.prec == PREC_F32) {
-          float* e0 = fld<float>(W.q[0]);
-          float* e1 = fld<float>(W.q[1]);
           fld<float>(W.f[0])[cw] = float(r0);
           fld<float>(W.f[1])[cw] = float(r1);
           fld<float>(W.bs)[cw] = float(s.pc);
-          e0[cw] = 0.f;
-          e1[cw] = 0.f;
-          if (W.wt && near_boundary(W, i, j, 0, 2))
-            write_through<float, 2>(W, e0, e1, i, j, 0, 0.f, 0.f);
+          // A fused twin's pre-smoothing starts from a zero correction
+          // without reading it (kb_smooth2), so only the others store it.
+          if (!W.fused) {
+            float* e0 = fld<float>(W.q[0]);
+            float* e1 = fld<float>(W.q[1]);
+            e0[cw] = 0.f;
+            e1[cw] = 0.f;
+            if (W.wt && near_boundary(W, i, j, 0, 2))
+              write_through<float, 2>(W, e0, e1, i, j, 0, 0.f, 0.f);
+          }
         } else {
           double* e0 = fld<double>(W.q[0]);
           double* e1 = fld<double>(W.q[1]);

@@ -451,19 +451,31 @@ __global__ void __launch_bounds__(Fused2<T>::THREADS, MINB)
     const int gx0 = it.tx * F::TX + 1 - F::H;  // global i of shared column 0
     const int gy0 = it.ty * F::TY + 1 - F::H;  // global j of shared row 0
     const int lead = 128 / (int)sizeof(T) - 1;
+    // The correction of the mixed form's finest working level is zero at the
+    // start of every V-cycle (the defect starts a new correction): its
+    // pre-smoothing stage fills the state planes with zeros instead of
+    // reading them (the defect does not store them either).
+    const bool zero_start = DELTA && dir == 0 && P.master >= 0;
     if (tid == 0) {
       const CUtensorMapOpaque* maps = static_cast<const CUtensorMapOpaque*>(P.tmaps);
       const int m0 = dir == 0 ? 0 : 2;
       const uint32_t plane = (uint32_t)(sizeof(T) * F::PLANE);
       fence_proxy_async_smem();  // earlier generic accesses to the tile come first
-      mbar_arrive_expect_tx(&bar, plane * (DELTA ? 5u : 4u));
+      mbar_arrive_expect_tx(&bar, plane * ((DELTA ? 5u : 4u) - (zero_start ? 2u : 0u)));
       const int x = gx0 + lead;  // column of element (gx0, *) from the allocation start
-      tma_load_2d(s0, &maps[m0], x, gy0, &bar);
-      tma_load_2d(s1, &maps[m0 + 1], x, gy0, &bar);
+      if (!zero_start) {
+        tma_load_2d(s0, &maps[m0], x, gy0, &bar);
+        tma_load_2d(s1, &maps[m0 + 1], x, gy0, &bar);
+      }
       tma_load_2d(sf0, &maps[4], x, gy0, &bar);
       tma_load_2d(sf1, &maps[5], x, gy0, &bar);
       if (DELTA) tma_load_2d(sbs, &maps[6], x, gy0, &bar);
     }
+    if (zero_start)
+      for (int c = tid; c < F::PLANE; c += F::THREADS) {
+        s0[c] = T(0);
+        s1[c] = T(0);
+      }
     // One thread polls (with back-off, so that the waiting CTA takes no issue
     // slots from the CTAs computing beside it); after the barrier every
     // thread observes the completed phase itself.

@@ -552,10 +552,7 @@ __global__ void __launch_bounds__(BLOCK_THREADS)
 // applied to the cell reflected across them (across a periodic face, the
 // cell at the other end).
 template <class T, int D>
-__global__ void k_setbc(const DevPatch* __restrict__ PT, int patch, int64_t ntotal) {
-  const DevPatch P = PT[patch];
-  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= ntotal) return;
+__device__ __forceinline__ void setbc_elem(const DevPatch& P, int64_t g) {
   const int e0 = P.n[0] + 2, e1 = P.n[1] + 2;
   int co[3] = {(int)(g % e0), (int)((g / e0) % e1), D == 3 ? (int)(g / ((int64_t)e0 * e1)) : 0};
   int src[3] = {co[0], co[1], co[2]};
@@ -583,6 +580,27 @@ __global__ void k_setbc(const DevPatch* __restrict__ PT, int patch, int64_t ntot
       if (codes[d] != BC_NONE) val = bc_map<T>(codes[d], val);
     q[cidx(P, co[0], co[1], co[2])] = val;
   }
+}
+
+// One patch, one thread per element of its box with ring (ntotal elements).
+template <class T, int D>
+__global__ void k_setbc(const DevPatch* __restrict__ PT, int patch, int64_t ntotal) {
+  const DevPatch P = PT[patch];
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= ntotal) return;
+  setbc_elem<T, D>(P, g);
+}
+
+// The same for a list of patches (blockIdx.y selects the patch; the grid
+// strides over its elements).
+template <class T, int D>
+__global__ void k_setbc_list(const DevPatch* __restrict__ PT, const int* __restrict__ patches) {
+  const DevPatch P = PT[patches[blockIdx.y]];
+  const int64_t ntotal =
+      (int64_t)(P.n[0] + 2) * (P.n[1] + 2) * (D == 3 ? (int64_t)(P.n[2] + 2) : 1);
+  for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < ntotal;
+       g += (int64_t)gridDim.x * blockDim.x)
+    setbc_elem<T, D>(P, g);
 }
 
 // ---- device-side V-cycle loop (MultigridIterations, afas:69-104) -----------

@@ -70,8 +70,13 @@ __device__ __forceinline__ void RelaxCell(const Stencil<T, D>& s, T f0, T f1, T 
     // contracted products and one approximate reciprocal (__fdividef,
     // 2 ulp), since these levels only smooth a correction whose FP64 defect
     // is recomputed exactly; the FP64 path below keeps the reference's
-    // operation order.
-    const T d2 = D2fc(cfull, alpha);
+    // operation order.  Every operation is an explicitly rounded intrinsic,
+    // so the compiler evaluates exactly this sequence -- the one the paired
+    // FP32 form of the fused 2D stage (relax_pair_f32) evaluates too.
+    const float cf = DELTA ? __fadd_rn(base, s.pc) : s.pc;
+    const float cmh = __fadd_rn(cf, -0.5f);
+    const float u = __fmul_rn(__fmul_rn(3.f, cmh), cmh);
+    const T d2 = __fmul_rn(u, alpha);
     const T a21f = -d2 - tmp3;
     T smuf = m[0] * s.mm[0] + m[1] * s.mp[0];
 #pragma unroll
@@ -85,7 +90,16 @@ __device__ __forceinline__ void RelaxCell(const Stencil<T, D>& s, T f0, T f1, T 
       sphf = sphf + s.pp[d];
       sphf = sphf + s.pm[d];
     }
-    const T nlf = DELTA ? DfcDelta(base, s.pc, alpha) : Dfc(s.pc, alpha);
+    T nlf;
+    if constexpr (DELTA) {
+      // DfcDelta(base, e) = alpha e (3 c^2 + 3 c e + e^2), c = base - 1/2.
+      const float c = __fadd_rn(base, -0.5f), e = s.pc;
+      const float c3 = __fmul_rn(3.f, c);
+      const float poly = __fadd_rn(__fadd_rn(__fmul_rn(c3, c), __fmul_rn(c3, e)), __fmul_rn(e, e));
+      nlf = __fmul_rn(__fmul_rn(alpha, e), poly);
+    } else {
+      nlf = Dfc(s.pc, alpha);
+    }
     const T b1f = __fmaf_rn(tmp1, smuf, f0);
     const T b2f = __fmaf_rn(-tmp2, sphf, __fmaf_rn(-d2, s.pc, f1 + nlf));
     const T detf = __fmaf_rn(-a12, a21f, T(1));

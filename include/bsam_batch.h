@@ -103,9 +103,11 @@ typedef struct {
   /* bsam_batch_profile: finest-depth smoothing stages timed with events */
   int64_t smooth_stages;
   double smooth_ms;
-  double smooth_bytes;    /* algorithmic: 6 * value bytes * cells per stage;
-                             (4 * value bytes + 32) * cells for the mixed 2D
-                             post-smoothing, which also applies q64 += e */
+  double smooth_bytes;    /* algorithmic bytes of those stages: per cell of
+                             the finest working level, the fields each stage
+                             must read and write once (the fused 2D stages:
+                             state, f, base, the restriction into or the
+                             correction from the parent, the FP64 update) */
 } bsam_batch_stats;
 
 int bsam_batch_create(bsam_batch** b, int device, const bsam_batch_params* p);
@@ -131,6 +133,24 @@ int bsam_batch_submit(bsam_batch* b, const bsam_batch_problem* prob, const doubl
  * then SetBC.  Bit-identical to building the same q0 on the host. */
 int bsam_batch_submit_seeded(bsam_batch* b, const bsam_batch_problem* prob, uint64_t seed,
                              double cbar, double amp, int* slot);
+
+/* Admits problems[0..n) in order, as n calls of bsam_batch_submit would,
+ * with their device work batched (a handful of launches for all of them and
+ * one pitched copy per component and problem).  Admission stops at the first
+ * problem that does not fit now: slots[k] receives the slot of problem k, or
+ * -1 for it and every later one.  Returns the number admitted, or an error
+ * code (then none is admitted) when a problem is invalid.  q0s[k] as for
+ * bsam_batch_submit, except that page-locked q0 buffers are read
+ * asynchronously: keep them unchanged until the next call that waits
+ * (bsam_batch_sync, bsam_batch_run, a collect).  No reference counterpart. */
+int bsam_batch_submit_many(bsam_batch* b, int n, const bsam_batch_problem* problems,
+                           const double* const* q0s, int* slots);
+
+/* As bsam_batch_submit_many with the seeded initial state of
+ * bsam_batch_submit_seeded (seeds[k], cbar[k], amp[k] for problem k). */
+int bsam_batch_submit_seeded_many(bsam_batch* b, int n, const bsam_batch_problem* problems,
+                                  const uint64_t* seeds, const double* cbar,
+                                  const double* amp, int* slots);
 
 /* 1 while work queued on the batch's stream is still executing, 0 when idle
  * (does not wait). */
@@ -161,6 +181,14 @@ int bsam_batch_slot_phase(bsam_batch* b, int slot, int* phase, int* steps_done);
  * (AfterStep's integral(1)). */
 int bsam_batch_collect(bsam_batch* b, int slot, double* q, bsam_step_result* steps,
                        double* mass);
+
+/* bsam_batch_collect of slots[0..n) with one wait: qs[k], steps[k] (arrays
+ * of pointers, NULL entries or NULL arrays to skip) and masses[k] (NULL to
+ * skip, which saves a reduction per problem).  Every slot must be finished;
+ * all are released.  BSAM_ERR_DIVERGED when any of them failed.  No
+ * reference counterpart. */
+int bsam_batch_collect_many(bsam_batch* b, int n, const int* slots, double* const* qs,
+                            bsam_step_result* const* steps, double* masses);
 
 /* enable != 0: ticks run eagerly, one at a time, and each finest-depth
  * smoothing stage (2 x nsmoothingpasses colour passes over every running

@@ -169,10 +169,44 @@ def test_batch_profile_counts_finest_stages(gpu_lib):
         bt.sync()
         st = bt.stats()
         bt.profile(False)
-    # two finest-depth stages (pre and post) per tick; the post stage also
-    # reads and writes the FP64 master instead of writing e, and applies the
-    # coarse-grid correction (its algorithmic bytes: 4 s + s / 2 per cell)
+    # two finest-depth stages (pre and post) per tick.  Per cell, FP32
+    # working level over an FP32 parent: pre reads f1, f2 and the base (the
+    # correction starts from zero), writes the state and restricts q, qs and
+    # the base into the parent (5 * 4 / 4); post reads the state, f1, f2, the
+    # base and the parent's q and qs (4 * 4 / 4), and reads and writes the
+    # FP64 master instead of writing the state
     assert st["smooth_stages"] == 4 and st["smooth_ms"] > 0
     cells = sum(n * n for n in (128, 96))
-    # and the pre stage restricts into the parent (3 s per cell)
-    assert st["smooth_bytes"] == 2 * (6 * 4 + 3 * 4 + (4 * 4 + 32) + (4 * 4 + 2)) * cells
+    pre = 3 * 4 + 2 * 4 + 5
+    post = 5 * 4 + 4 + 32
+    assert st["smooth_bytes"] == 2 * (pre + post) * cells
+
+
+def test_submit_many_and_collect_many_match_single_calls(gpu_lib):
+    # The batched admission and read-back give the same bits as one call per
+    # problem, seeded and from host arrays, page-locked or not; admission
+    # stops at the first problem that does not fit.
+    probs = [W.seeded(2, n, 0.01, 2, seed=600 + i, cbar=0.5, amp=0.025)
+             for i, n in enumerate([64, 96, 128, 48, 192])]
+    ref = BB.solve_all(probs, precision=BB.PREC_MIXED)
+    with BB.Batch(2, precision=BB.PREC_MIXED, max_slots=8) as bt:
+        slots = bt.submit_many(probs)
+        assert None not in slots and len(set(slots)) == len(slots)
+        bt.run()
+        got = bt.collect_many(slots, want_mass=True)
+        q0s = [p.q0() for p in probs]
+        slots = bt.submit_many(probs, q0s)
+        bt.run()
+        got2 = bt.collect_many(slots)
+    for r, g, g2 in zip(ref, got, got2):
+        for k in ("q", "nvcycles", "residual", "converged"):
+            assert np.array_equal(r[k], g[k]), k
+            assert np.array_equal(r[k], g2[k]), k
+        assert r["mass"] == g["mass"]
+    with BB.Batch(2, precision=BB.PREC_MIXED, max_slots=3) as bt:
+        slots = bt.submit_many(probs)
+        assert slots[:3] == sorted(slots[:3]) and slots[3:] == [None, None]
+        bt.run()
+        got = bt.collect_many(slots[:3])
+    for r, g in zip(ref[:3], got):
+        assert np.array_equal(r["q"], g["q"])

@@ -364,11 +364,17 @@ def run_ours(args, world, rank, local):
     problems = shard_problems(rank)
     steps_per_bench_step = sum(p.nsteps for p in problems)
 
+    # The batch's execution choices from the project autotuner, searched on
+    # a stratified sample of this workload on this GPU (results are the same
+    # under every choice; only the time differs).
+    from bsam_b200 import autotune as AT
+    tune = AT.tuned_choice(problems, BB.PREC_MIXED, device=local, per_side=16, retune=True)
     batch = BB.Batch(2, precision=BB.PREC_MIXED, max_slots=NPROB, device=local)
+    batch.set_tuning(**tune["choice"])
     stream = torch.cuda.ExternalStream(batch.stream(), device=local)
 
     def one_step(timed_events=None):
-        slots = [batch.submit_seeded(p) for p in problems]
+        slots = batch.submit_many(problems)
         batch.sync()
         if timed_events is not None:
             timed_events[0].record(stream)
@@ -377,8 +383,7 @@ def run_ours(args, world, rank, local):
             timed_events[1].record(stream)
         nv = 0
         conv = True
-        for s in slots:
-            r = batch.collect(s, want_q=False)
+        for r in batch.collect_many(slots, want_q=False):
             nv += int(r["nvcycles"].sum())
             conv = conv and int(r["converged"].min()) == 1
         return nv, conv
@@ -418,15 +423,14 @@ def run_ours(args, world, rank, local):
 
     # ---- smoother roofline: finest-depth stages timed with events in the
     # first two ticks (every problem running) -----------------------------------
-    slots = [batch.submit_seeded(p) for p in problems]
+    slots = batch.submit_many(problems)
     batch.profile(True)
     batch.advance(2)
     batch.sync()
     pst = batch.stats()
     batch.profile(False)
     batch.run()
-    for s in slots:
-        batch.collect(s, want_q=False)
+    batch.collect_many(slots, want_q=False)
     peak, peak_kind = peaks()
     stage_ms = pst["smooth_ms"] / max(pst["smooth_stages"], 1)
     stage_bytes = pst["smooth_bytes"] / max(pst["smooth_stages"], 1)
@@ -464,10 +468,9 @@ def run_ours(args, world, rank, local):
     for s in range(args.steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        slots = [batch.submit(p, q) for p, q in zip(problems, q0s)]
+        slots = batch.submit_many(problems, q0s)
         batch.run()
-        res = [batch.collect(sl, want_q=True, out=o, want_mass=False)
-               for sl, o in zip(slots, outs)]
+        res = batch.collect_many(slots, outs=outs)
         e2e_t.append(time.perf_counter() - t0)
         d2h = sum(int(r["q"].nbytes) for r in res)
     e2e_s = allmax(world, sum(e2e_t))
@@ -489,7 +492,10 @@ def run_ours(args, world, rank, local):
                    "vcycles_per_s": world * sum(nvc) / dev_s_max,
                    "ticks_per_bench_step": ticks / args.steps,
                    "all_converged": conv_all,
-                   "step_ms": [round(x, 3) for x in step_ms]},
+                   "step_ms": [round(x, 3) for x in step_ms],
+                   "tuning": {"choice": tune["choice"], "gain_vs_default": tune["gain"],
+                              "search_s": tune.get("tuning_s"),
+                              "sample": tune.get("sample")}},
         "roofline": {"bound": "hbm", "kernel": "kb_smooth2<float> (fused finest-depth "
                      "smoothing stages: nu=2 red-black sweeps of every problem, one launch "
                      "each; the pre-smoothing launch also restricts into the parent, the "
@@ -506,8 +512,9 @@ def run_ours(args, world, rank, local):
                      "algorithmic_bytes_per_launch": stage_bytes, "launch_ms": stage_ms},
         "e2e": {"value": world * args.steps * steps_per_bench_step / e2e_s, "unit": UNIT,
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "path": "bsam_batch_submit (host q0 in page-locked memory) + run + collect "
-                        "(host q into page-locked memory), host wall clock, max over ranks"},
+                "path": "bsam_batch_submit_many (host q0 in page-locked memory) + run + "
+                        "bsam_batch_collect_many (host q into page-locked memory), host wall "
+                        "clock, max over ranks"},
         "gpu_launches": int(ticks * kpt + 2 * NPROB * args.steps),
         "clocks": clocks,
     }
@@ -517,20 +524,25 @@ def run_ours(args, world, rank, local):
 
     if world == 1 and rank == 0 and not args.quick:
         extra = {}
-        # FP64 batched form of the same problems (device-timed like the headline).
+        # FP64 batched form of the same problems (device-timed like the
+        # headline, with its own autotuned choices; mean of three runs).
+        tune64 = AT.tuned_choice(problems, BB.PREC_FP64, device=local, per_side=16, retune=True)
         with BB.Batch(2, precision=BB.PREC_FP64, max_slots=NPROB, device=local) as b64:
+            b64.set_tuning(**tune64["choice"])
             st64 = torch.cuda.ExternalStream(b64.stream(), device=local)
-            for rep in range(2):
-                slots = [b64.submit_seeded(p) for p in problems]
+            ms64 = []
+            for rep in range(3):
+                slots = b64.submit_many(problems)
                 b64.sync()
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 e0.record(st64)
                 b64.run()
                 e1.record(st64)
                 torch.cuda.synchronize()
-                for s in slots:
-                    b64.collect(s, want_q=False)
-            extra["fp64_batched_steps_per_s"] = steps_per_bench_step / (e0.elapsed_time(e1) / 1e3)
+                b64.collect_many(slots, want_q=False)
+                ms64.append(e0.elapsed_time(e1))
+            extra["fp64_batched_steps_per_s"] = steps_per_bench_step / (statistics.mean(ms64) / 1e3)
+            extra["fp64_batched_tuning"] = tune64["choice"]
             extra["mixed_over_fp64_batched"] = value / extra["fp64_batched_steps_per_s"]
         # Plain FP64 form, one problem at a time (single-problem library), on a
         # sample of the problems (every 16th).
@@ -610,11 +622,16 @@ def run_ours(args, world, rank, local):
                 "refined_cells_mean": statistics.mean(refined),
                 "steps_with_refinement": sum(1 for x in pats if x > 0),
                 "tag_threshold": "|grad phi| > %.2f/eps" % (0.25 if sustained else 0.5)}
-        # Served form: one rate point of the Poisson request stream.
-        stream_ = W.config5(120, 200.0)
+        # Served form: the Poisson request stream at every configured rate
+        # (120 requests each); the capacity is the solves/s the server
+        # sustains once the arrival rate exceeds it.
+        sweep = {}
         with SV.Server(pool_bytes=32 << 30, max_slots=256, ticks=4, amr_workers=8) as srv:
-            reqs = srv.serve(stream_)
-        extra["served_rate_200"] = SV.summarize(reqs)
+            for rate in (50, 100, 200, 500, 1000, 2000):
+                reqs = srv.serve(W.config5(120, float(rate)))
+                sweep[str(rate)] = SV.summarize(reqs)
+        extra["served_rate_sweep"] = sweep
+        extra["served_capacity_solves_per_s"] = max(v["solves_per_s"] for v in sweep.values())
         line["forms"] = extra
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline()

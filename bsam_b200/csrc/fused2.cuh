@@ -157,23 +157,29 @@ __device__ __forceinline__ void relax_pair_f32(float2 pc, float2 pw, float2 pe, 
                                                const RelaxK2& K, float2& phi, float2& mu) {
   const float2 smu = __fadd2_rn(__fadd2_rn(__fadd2_rn(mw, me), ms), mn);
   const float2 sph = __fadd2_rn(__fadd2_rn(__fadd2_rn(pe, pw), pn), ps);
-  const float2 cfull = DELTA ? __fadd2_rn(bs, pc) : pc;
-  const float2 cmh = __fadd2_rn(cfull, K.mhalf);
+  float2 cmh, nl;
+  if (DELTA) {
+    // The correction form's terms, one half at a time with RelaxCell's scalar
+    // operations: cfull = base + e, and DfcDelta(base, e) = alpha e (3 c^2 +
+    // 3 c e + e^2), c = base - 1/2.
+    auto half = [&](float b, float e, float& cm, float& n) {
+      cm = __fadd_rn(__fadd_rn(b, e), -0.5f);
+      const float c = __fadd_rn(b, -0.5f);
+      const float c3 = __fmul_rn(3.f, c);
+      const float poly =
+          __fadd_rn(__fadd_rn(__fmul_rn(c3, c), __fmul_rn(c3, e)), __fmul_rn(e, e));
+      n = __fmul_rn(__fmul_rn(K.alpha.x, e), poly);
+    };
+    half(bs.x, pc.x, cmh.x, nl.x);
+    half(bs.y, pc.y, cmh.y, nl.y);
+  } else {
+    cmh = __fadd2_rn(pc, K.mhalf);
+    nl = __fmul2_rn(__fmul2_rn(__fmul2_rn(cmh, cmh), cmh), K.alpha);  // Dfc
+  }
   const float2 u = __fmul2_rn(__fmul2_rn(K.three, cmh), cmh);
   const float2 d2 = __fmul2_rn(u, K.alpha);     // D2fc(cfull)
   const float2 nd2 = __fmul2_rn(u, K.nalpha);   // -D2fc(cfull)
   const float2 na21 = __fadd2_rn(d2, K.tmp3);   // -a21
-  float2 nl;
-  if (DELTA) {
-    // DfcDelta(base, e): alpha e (3 c^2 + 3 c e + e^2), c = base - 1/2.
-    const float2 c = __fadd2_rn(bs, K.mhalf);
-    const float2 c3 = __fmul2_rn(K.three, c);
-    const float2 poly =
-        __fadd2_rn(__fadd2_rn(__fmul2_rn(c3, c), __fmul2_rn(c3, pc)), __fmul2_rn(pc, pc));
-    nl = __fmul2_rn(__fmul2_rn(K.alpha, pc), poly);
-  } else {
-    nl = __fmul2_rn(__fmul2_rn(__fmul2_rn(cmh, cmh), cmh), K.alpha);  // Dfc
-  }
   const float2 b1 = __ffma2_rn(K.tmp1, smu, f0);
   const float2 b2 = __ffma2_rn(K.ntmp2, sph, __ffma2_rn(nd2, pc, __fadd2_rn(f1, nl)));
   const float2 det = __ffma2_rn(K.a12, na21, K.one);

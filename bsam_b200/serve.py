@@ -135,21 +135,24 @@ class Server:
                 else:
                     pending.append(reqs[nxt])
                 nxt += 1
-            # Admission: FIFO per engine (a full engine does not block the other).
-            blocked = set()
-            keep = deque()
-            while pending:
-                r = pending.popleft()
-                nd = r.prob.ndims
-                s = None if nd in blocked else self.engines[nd].submit_seeded(r.prob)
-                if s is None:
-                    blocked.add(nd)
-                    keep.append(r)
-                    continue
-                r.admitted = now
-                inflight[(nd, s)] = r
-                running[nd] += 1
-            pending = keep
+            # Admission: FIFO per engine (a full engine does not block the
+            # other), all of an engine's waiting requests offered in one
+            # batched call; admission stops at the first that does not fit.
+            if pending:
+                keep = deque()
+                for nd, e in self.engines.items():
+                    mine = [r for r in pending if r.prob.ndims == nd]
+                    if not mine:
+                        continue
+                    slots = e.submit_many([r.prob for r in mine])
+                    for r, s in zip(mine, slots):
+                        if s is None:
+                            continue
+                        r.admitted = now
+                        inflight[(nd, s)] = r
+                        running[nd] += 1
+                keep.extend(r for r in pending if r.admitted is None)
+                pending = keep
             # Keep every engine with running problems busy.
             for nd, e in self.engines.items():
                 if running[nd] and not e.busy():
@@ -159,12 +162,17 @@ class Server:
             for nd, e in self.engines.items():
                 if not running[nd]:
                     continue
-                for s in e.poll():
+                done = e.poll()
+                if not done:
+                    continue
+                results = e.collect_many(done, want_q=self.keep_q, want_mass=True)
+                t_done = time.perf_counter() - t0
+                for s, res in zip(done, results):
                     r = inflight.pop((nd, s))
-                    r.finished = time.perf_counter() - t0
-                    r.result = e.collect(s, want_q=self.keep_q)
+                    r.finished = t_done
+                    r.result = res
                     running[nd] -= 1
-                    done_any = True
+                done_any = True
             if not done_any and not pending and not inflight and nxt < len(reqs):
                 wait = reqs[nxt].arrival - (time.perf_counter() - t0)
                 if wait > 0:

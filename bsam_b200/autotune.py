@@ -6,8 +6,10 @@ mapped onto the B200 but not a single result bit (bsam_batch_tuning):
   per_pass    sweep fusion: 0 = every 2D level above the bottom smooths with
               the fused shared-memory stage (all 2*nu colour passes of
               LevelRelax in one launch), 1 = one launch per colour pass
-  fused_occ   the fused stage's build for 3 or 4 resident CTAs per SM (85 or
-              64 registers per thread)
+  fused_occ   the fused stage's build: 3 or 4 resident CTAs per SM with one
+              tile buffer each (85 or 64 registers per thread), or 2 CTAs per
+              SM with two buffers each (the next tile's copies land while the
+              current one is computed)
   fused_ctas  CTAs of a fused-stage launch (persistent grid-stride loop over
               the stage's tiles)
   grid_ctas   CTAs of every other stage launch
@@ -48,7 +50,7 @@ def candidates(knob: str, nsm: int) -> list:
     if knob == "per_pass":
         return [0, 1]
     if knob == "fused_occ":
-        return [3, 4]
+        return [2, 3, 4]
     if knob == "fused_ctas":
         return [0, 2 * nsm, 3 * nsm, 8 * nsm]
     if knob == "grid_ctas":

@@ -595,15 +595,22 @@ void tick_t(bsam_batch* b, cudaGraphConditionalHandle handle, int in_graph) {
       // of an FP64 batch, a plain FP64 level.  The finest working level's
       // post-smoothing applies the FP64 update (kb_update skips those masters).
       const int upd = (b->mixed && d == 0 && dir == 1) ? 1 : 0;
+      // The build picked by fused_occ: 2 = two tile buffers per CTA (two
+      // CTAs per SM), 3 / 4 = one buffer and that many CTAs per SM.
       const int occ = b->tuning.fused_occ;
+      const int nbuf = occ == 2 ? 2 : 1;
       if (b->mixed) {
-        auto k = occ == 3 ? kb_smooth2<float, true, 3> : kb_smooth2<float, true, 4>;
-        k<<<g, Fused2<float>::THREADS, Fused2<float>::smem(true), s>>>(
+        auto k = occ == 2   ? kb_smooth2<float, true, 2, 2>
+                 : occ == 3 ? kb_smooth2<float, true, 3>
+                            : kb_smooth2<float, true, 4>;
+        k<<<g, Fused2<float>::THREADS, nbuf * Fused2<float>::smem(true), s>>>(
             pt, L[L_FUSED + d].d, cnt + L_FUSED + d, dir, nu, upd, dir, 1 - dir,
             &b->d_ctl->kerr);
       } else {
-        auto k = occ == 4 ? kb_smooth2<double, false, 4> : kb_smooth2<double, false, 3>;
-        k<<<g, Fused2<double>::THREADS, Fused2<double>::smem(false), s>>>(
+        auto k = occ == 2   ? kb_smooth2<double, false, 2, 2>
+                 : occ == 4 ? kb_smooth2<double, false, 4>
+                            : kb_smooth2<double, false, 3>;
+        k<<<g, Fused2<double>::THREADS, nbuf * Fused2<double>::smem(false), s>>>(
             pt, L[L_FUSED + d].d, cnt + L_FUSED + d, dir, nu, 0, dir, 1 - dir,
             &b->d_ctl->kerr);
       }
@@ -846,7 +853,13 @@ int bsam_batch_create(bsam_batch** out, int device, const bsam_batch_params* p) 
                               (int)Fused2<double>::SMEM) == cudaSuccess &&
          cudaFuncSetAttribute(kb_smooth2<double, false, 4>,
                               cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)Fused2<double>::SMEM) == cudaSuccess;
+                              (int)Fused2<double>::SMEM) == cudaSuccess &&
+         cudaFuncSetAttribute(kb_smooth2<float, true, 2, 2>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)(2 * Fused2<float>::smem(true))) == cudaSuccess &&
+         cudaFuncSetAttribute(kb_smooth2<double, false, 2, 2>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)(2 * Fused2<double>::smem(false))) == cudaSuccess;
   if (!ok) {
     cudaGetLastError();
     bsam_batch_destroy(b);
@@ -910,7 +923,7 @@ int bsam_batch_destroy(bsam_batch* b) {
 int bsam_batch_set_tuning(bsam_batch* b, const bsam_batch_tuning* t) {
   if (!b || !t || t->grid_ctas < 0 || t->eager < 0 || t->eager > 1 || t->per_pass < 0 ||
       t->per_pass > 1 || t->fused_ctas < 0 ||
-      (t->fused_occ != 0 && t->fused_occ != 3 && t->fused_occ != 4))
+      (t->fused_occ != 0 && (t->fused_occ < 2 || t->fused_occ > 4)))
     return BSAM_ERR_ARG;
   b->tuning = *t;
   b->need_capture = true;

@@ -427,57 +427,81 @@ __device__ __forceinline__ void restrict_tile2(const DevPatch& C, const DevPatch
 // parent from shared memory (restrict_tile2), instead of by a kb_restrict
 // launch after the stage.
 // MINB CTAs per SM (the shared tile allows four): four caps a thread at 64
-// registers, three at 85.
-template <class T, bool DELTA, int MINB = (sizeof(T) == 4 ? 4 : 3)>
+// registers, three at 85.  NBUF = 2: two tile buffers per CTA (two CTAs per
+// SM), the copies of the CTA's next tile land while it computes the current
+// one.
+template <class T, bool DELTA, int MINB = (sizeof(T) == 4 ? 4 : 3), int NBUF = 1>
 __global__ void __launch_bounds__(Fused2<T>::THREADS, MINB)
     kb_smooth2(const DevPatch* __restrict__ PT, const Item* __restrict__ items,
                const int* __restrict__ count, int dir, int nu, int upd, int corr,
                int restr, int* __restrict__ err) {
   using F = Fused2<T>;
+  static_assert(NBUF == 1 || NBUF == 2, "one or two tile buffers");
+  constexpr int NPL = DELTA ? 5 : 4;  // planes per buffer
   extern __shared__ __align__(1024) unsigned char smem2_raw[];
-  __shared__ __align__(8) uint64_t bar;
-  T* s0 = reinterpret_cast<T*>(smem2_raw);
-  T* s1 = s0 + F::PLANE;
-  T* sf0 = s1 + F::PLANE;
-  T* sf1 = sf0 + F::PLANE;
-  T* sbs = sf1 + F::PLANE;
+  __shared__ __align__(8) uint64_t bar[NBUF];
+  auto plane = [&](int buf, int k) {
+    return reinterpret_cast<T*>(smem2_raw) + (size_t)(buf * NPL + k) * F::PLANE;
+  };
   const int n = *count;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int npass = 2 * nu;
   if (tid == 0) {
-    mbar_init(&bar, 1);
+    for (int k = 0; k < NBUF; ++k) mbar_init(&bar[k], 1);
     fence_mbar_init();
   }
   __syncthreads();
-  uint32_t phase = 0;
-  for (int b = blockIdx.x; b < n; b += gridDim.x) {
-    const Item it = items[b];
+  // The correction of the mixed form's finest working level is zero at the
+  // start of every V-cycle (the defect starts a new correction): its
+  // pre-smoothing stage fills the state planes with zeros instead of reading
+  // them (the defect does not store them either).
+  auto zero_start_of = [&](const DevPatch& P) { return DELTA && dir == 0 && P.master >= 0; };
+  // The CTA's next tile at or after list position `from` whose patch runs.
+  auto next_tile = [&](int from) {
+    for (int x = from; x < n; x += gridDim.x)
+      if (PT[items[x].patch].active) return x;
+    return n;
+  };
+  // Thread 0: the tensor copies of tile x into buffer buf.
+  auto issue = [&](int x, int buf) {
+    const Item it = items[x];
+    const DevPatch& P = PT[it.patch];
+    const int gx0 = it.tx * F::TX + 1 - F::H, gy0 = it.ty * F::TY + 1 - F::H;
+    const int lead = 128 / (int)sizeof(T) - 1;
+    const bool zs = zero_start_of(P);
+    const CUtensorMapOpaque* maps = static_cast<const CUtensorMapOpaque*>(P.tmaps);
+    const int m0 = dir == 0 ? 0 : 2;
+    const uint32_t pl = (uint32_t)(sizeof(T) * F::PLANE);
+    fence_proxy_async_smem();  // earlier generic accesses to the buffer come first
+    mbar_arrive_expect_tx(&bar[buf], pl * (uint32_t)(NPL - (zs ? 2 : 0)));
+    const int xc = gx0 + lead;  // column of element (gx0, *) from the allocation start
+    if (!zs) {
+      tma_load_2d(plane(buf, 0), &maps[m0], xc, gy0, &bar[buf]);
+      tma_load_2d(plane(buf, 1), &maps[m0 + 1], xc, gy0, &bar[buf]);
+    }
+    tma_load_2d(plane(buf, 2), &maps[4], xc, gy0, &bar[buf]);
+    tma_load_2d(plane(buf, 3), &maps[5], xc, gy0, &bar[buf]);
+    if (DELTA) tma_load_2d(plane(buf, 4), &maps[6], xc, gy0, &bar[buf]);
+  };
+  uint32_t phase[NBUF];
+  for (int k = 0; k < NBUF; ++k) phase[k] = 0u;
+  int cur = next_tile(blockIdx.x), buf = 0;
+  if (cur < n && tid == 0) issue(cur, 0);
+  while (cur < n) {
+    const int nxt = next_tile(cur + gridDim.x);
+    // Two buffers: the next tile's copies go into the other one, last read
+    // by the previous tile (which ended with a barrier).
+    if (NBUF == 2 && nxt < n && tid == 0) issue(nxt, buf ^ 1);
+    T* s0 = plane(buf, 0);
+    T* s1 = plane(buf, 1);
+    T* sf0 = plane(buf, 2);
+    T* sf1 = plane(buf, 3);
+    T* sbs = plane(buf, DELTA ? 4 : 3);
+    const Item it = items[cur];
     const DevPatch P = PT[it.patch];
-    if (!P.active) continue;  // uniform per CTA
     const int gx0 = it.tx * F::TX + 1 - F::H;  // global i of shared column 0
     const int gy0 = it.ty * F::TY + 1 - F::H;  // global j of shared row 0
-    const int lead = 128 / (int)sizeof(T) - 1;
-    // The correction of the mixed form's finest working level is zero at the
-    // start of every V-cycle (the defect starts a new correction): its
-    // pre-smoothing stage fills the state planes with zeros instead of
-    // reading them (the defect does not store them either).
-    const bool zero_start = DELTA && dir == 0 && P.master >= 0;
-    if (tid == 0) {
-      const CUtensorMapOpaque* maps = static_cast<const CUtensorMapOpaque*>(P.tmaps);
-      const int m0 = dir == 0 ? 0 : 2;
-      const uint32_t plane = (uint32_t)(sizeof(T) * F::PLANE);
-      fence_proxy_async_smem();  // earlier generic accesses to the tile come first
-      mbar_arrive_expect_tx(&bar, plane * ((DELTA ? 5u : 4u) - (zero_start ? 2u : 0u)));
-      const int x = gx0 + lead;  // column of element (gx0, *) from the allocation start
-      if (!zero_start) {
-        tma_load_2d(s0, &maps[m0], x, gy0, &bar);
-        tma_load_2d(s1, &maps[m0 + 1], x, gy0, &bar);
-      }
-      tma_load_2d(sf0, &maps[4], x, gy0, &bar);
-      tma_load_2d(sf1, &maps[5], x, gy0, &bar);
-      if (DELTA) tma_load_2d(sbs, &maps[6], x, gy0, &bar);
-    }
-    if (zero_start)
+    if (zero_start_of(P))
       for (int c = tid; c < F::PLANE; c += F::THREADS) {
         s0[c] = T(0);
         s1[c] = T(0);
@@ -486,20 +510,22 @@ __global__ void __launch_bounds__(Fused2<T>::THREADS, MINB)
     // slots from the CTAs computing beside it); after the barrier every
     // thread observes the completed phase itself.
     bool ok = true;
-    if (tid == 0) ok = mbar_wait_backoff(&bar, phase, kWaitPolls);
+    if (tid == 0) ok = mbar_wait_backoff(&bar[buf], phase[buf], kWaitPolls);
     ok = __syncthreads_and(ok);
-    if (ok && tid != 0) (void)mbar_try_wait(&bar, phase);
-    phase ^= 1u;
+    if (ok && tid != 0) (void)mbar_try_wait(&bar[buf], phase[buf]);
     if (!ok) {
       // The launch's results are void (the host reports the error).  Before
-      // the CTA exits, give the copies it started one more bounded wait, so
-      // that none is still writing into the shared tile when the CTA ends.
+      // the CTA exits, give the copies it started one more bounded wait each,
+      // so that none is still writing into shared memory when the CTA ends.
       if (tid == 0) {
         atomicExch(err, kErrTmaTimeout);
-        (void)mbar_wait_backoff(&bar, phase ^ 1u, kWaitPolls);
+        (void)mbar_wait_backoff(&bar[buf], phase[buf], kWaitPolls);
+        if (NBUF == 2 && nxt < n)
+          (void)mbar_wait_backoff(&bar[buf ^ 1], phase[buf ^ 1], kWaitPolls);
       }
       break;
     }
+    phase[buf] ^= 1u;
     const int n0 = P.n[0], n1 = P.n[1];
     // A tile that holds a physical face of the patch refreshes the face
     // ghosts in shared memory after every change of its cells and writes
@@ -587,38 +613,40 @@ __global__ void __launch_bounds__(Fused2<T>::THREADS, MINB)
               write_through<double, 2>(M, m0, m1, i, j, 0, na, nb);
           }
         }
-      __syncthreads();  // the shared tile is refilled for the next item
-      continue;
-    }
-    if (restr && P.parent >= 0) {
-      const DevPatch R = PT[P.parent];
-      if (P.pprec == PREC_F32) restrict_tile2<T, float, DELTA>(P, R, s0, s1, sbs, gx0, gy0);
-      else restrict_tile2<T, double, DELTA>(P, R, s0, s1, sbs, gx0, gy0);
-    }
-    // Write back the tile's interior cells (warps over rows, lanes along
-    // them, a pair per lane), ghosts by write-through on edge tiles.
-    if (lx < F::TX && gi <= n0)
-      for (int ly = warp; ly < F::TY; ly += F::WARPS) {
-        const int j = gy0 + F::H + ly;
-        if (j > n1) break;
-        const int srow = (F::H + ly) * F::RX + F::H;
-        T* r0 = o0 + (int64_t)j * P.sy;
-        T* r1 = o1 + (int64_t)j * P.sy;
-        if (!edge_tile && gi + 1 <= n0) {
-          *reinterpret_cast<V*>(r0 + gi) = *reinterpret_cast<const V*>(s0 + srow + lx);
-          *reinterpret_cast<V*>(r1 + gi) = *reinterpret_cast<const V*>(s1 + srow + lx);
-          continue;
-        }
-        for (int d = 0; d < 2; ++d) {
-          const int i = gi + d;
-          if (i > n0) break;
-          const T v0 = s0[srow + lx + d], v1 = s1[srow + lx + d];
-          r0[i] = v0;
-          r1[i] = v1;
-          if (P.wt && near_boundary(P, i, j, 0, 2)) write_through<T, 2>(P, o0, o1, i, j, 0, v0, v1);
-        }
+    } else {
+      if (restr && P.parent >= 0) {
+        const DevPatch R = PT[P.parent];
+        if (P.pprec == PREC_F32) restrict_tile2<T, float, DELTA>(P, R, s0, s1, sbs, gx0, gy0);
+        else restrict_tile2<T, double, DELTA>(P, R, s0, s1, sbs, gx0, gy0);
       }
-    __syncthreads();  // the shared tile is refilled for the next item
+      // Write back the tile's interior cells (warps over rows, lanes along
+      // them, a pair per lane), ghosts by write-through on edge tiles.
+      if (lx < F::TX && gi <= n0)
+        for (int ly = warp; ly < F::TY; ly += F::WARPS) {
+          const int j = gy0 + F::H + ly;
+          if (j > n1) break;
+          const int srow = (F::H + ly) * F::RX + F::H;
+          T* r0 = o0 + (int64_t)j * P.sy;
+          T* r1 = o1 + (int64_t)j * P.sy;
+          if (!edge_tile && gi + 1 <= n0) {
+            *reinterpret_cast<V*>(r0 + gi) = *reinterpret_cast<const V*>(s0 + srow + lx);
+            *reinterpret_cast<V*>(r1 + gi) = *reinterpret_cast<const V*>(s1 + srow + lx);
+            continue;
+          }
+          for (int d = 0; d < 2; ++d) {
+            const int i = gi + d;
+            if (i > n0) break;
+            const T v0 = s0[srow + lx + d], v1 = s1[srow + lx + d];
+            r0[i] = v0;
+            r1[i] = v1;
+            if (P.wt && near_boundary(P, i, j, 0, 2)) write_through<T, 2>(P, o0, o1, i, j, 0, v0, v1);
+          }
+        }
+    }
+    __syncthreads();  // the buffer is refilled for a later tile
+    if (NBUF == 1 && nxt < n && tid == 0) issue(nxt, 0);
+    cur = nxt;
+    if (NBUF == 2) buf ^= 1;
   }
 }
 

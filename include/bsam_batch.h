@@ -80,8 +80,10 @@ typedef struct {
  * per_pass = 1 makes problems admitted afterwards smooth with one launch per
  * colour pass instead of the fused shared-memory stage of 2D levels;
  * fused_ctas caps the CTAs of a fused stage launch (0 = 4 per SM);
- * fused_occ picks the fused stage's build for 3 or 4 resident CTAs per SM
- * (a register budget of 85 or 64 per thread; 0 = 4 for FP32, 3 for FP64). */
+ * fused_occ picks the fused stage's build: 3 or 4 resident CTAs per SM with
+ * one tile buffer each (a register budget of 85 or 64 per thread), or 2: two
+ * CTAs per SM with two tile buffers each, the next tile's copies landing
+ * while the current one is computed (0 = 4 for FP32, 3 for FP64). */
 typedef struct {
   int32_t grid_ctas;
   int32_t eager;

@@ -672,10 +672,10 @@ def run_case(args):
         probs = W.config4(nprob=NPROB, nsteps=NSTEPS)
         nticks = 3
     with BB.Batch(2, precision=BB.PREC_MIXED, max_slots=len(probs)) as b:
+        b.set_tuning(eager=1, fused_occ=args.fused_occ)
         for p in probs:
             assert b.submit_seeded(p) is not None
         b.sync()
-        b.set_tuning(eager=1)
         b.advance(nticks)
         b.sync()
         print(json.dumps({"case": args.case, "ticks": b.stats()["ticks"]}), flush=True)
@@ -698,6 +698,8 @@ def main():
     ap.add_argument("--quick", action="store_true", help="skip the side-by-side forms")
     ap.add_argument("--case", choices=["smooth2-small", "ticks", "amr2"], default=None,
                     help="run a fixed small case for a profiler capture and exit")
+    ap.add_argument("--fused-occ", type=int, default=0, choices=[0, 2, 3, 4],
+                    help="case mode: the fused 2D stage's build (bsam_batch_tuning.fused_occ)")
     args = ap.parse_args()
     if args.case:
         return run_case(args)

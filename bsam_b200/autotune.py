@@ -18,7 +18,8 @@ The tuner times candidates on a sample of the caller's workload with CUDA
 events on the engine's stream (a few V-cycle ticks of every sampled problem,
 after one warm-up tick), walks the knobs one at a time from the default
 (coordinate descent: each knob's best value is kept before the next knob is
-searched), and caches the winner per (GPU, precision, workload class) in a
+searched; the fused stage's build comes first, so that sweep fusion is
+judged with its best build), and caches the winner per (GPU, precision, workload class) in a
 JSON file.  Results are the same under every candidate;
 tests/test_gpu_autotune.py checks that on the GPU.
 """
@@ -31,7 +32,9 @@ import time
 
 from . import batch as BB
 
-KNOBS = ("per_pass", "fused_occ", "fused_ctas", "grid_ctas")
+# Search order: the fused stage's build before sweep fusion, so that fusion is
+# judged with the fused stage's best build.
+KNOBS = ("fused_occ", "per_pass", "fused_ctas", "grid_ctas")
 
 
 @dataclasses.dataclass(frozen=True)

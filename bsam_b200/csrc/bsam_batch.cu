@@ -608,8 +608,8 @@ void tick_t(bsam_batch* b, cudaGraphConditionalHandle handle, int in_graph) {
             &b->d_ctl->kerr);
       } else {
         auto k = occ == 2   ? kb_smooth2<double, false, 2, 2>
-                 : occ == 4 ? kb_smooth2<double, false, 4>
-                            : kb_smooth2<double, false, 3>;
+                 : occ == 3 ? kb_smooth2<double, false, 3>
+                            : kb_smooth2<double, false, 4>;
         k<<<g, Fused2<double>::THREADS, nbuf * Fused2<double>::smem(false), s>>>(
             pt, L[L_FUSED + d].d, cnt + L_FUSED + d, dir, nu, 0, dir, 1 - dir,
             &b->d_ctl->kerr);

@@ -430,7 +430,7 @@ __device__ __forceinline__ void restrict_tile2(const DevPatch& C, const DevPatch
 // registers, three at 85.  NBUF = 2: two tile buffers per CTA (two CTAs per
 // SM), the copies of the CTA's next tile land while it computes the current
 // one.
-template <class T, bool DELTA, int MINB = (sizeof(T) == 4 ? 4 : 3), int NBUF = 1>
+template <class T, bool DELTA, int MINB = 4, int NBUF = 1>
 __global__ void __launch_bounds__(Fused2<T>::THREADS, MINB)
     kb_smooth2(const DevPatch* __restrict__ PT, const Item* __restrict__ items,
                const int* __restrict__ count, int dir, int nu, int upd, int corr,

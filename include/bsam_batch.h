@@ -83,7 +83,7 @@ typedef struct {
  * fused_occ picks the fused stage's build: 3 or 4 resident CTAs per SM with
  * one tile buffer each (a register budget of 85 or 64 per thread), or 2: two
  * CTAs per SM with two tile buffers each, the next tile's copies landing
- * while the current one is computed (0 = 4 for FP32, 3 for FP64). */
+ * while the current one is computed (0 = 4). */
 typedef struct {
   int32_t grid_ctas;
   int32_t eager;

@@ -145,6 +145,36 @@ __device__ __forceinline__ RelaxK2 relax_k2(float tmp1, float tmp2, float tmp3, 
   return K;
 }
 
+// Paired FP32 operations (PTX add/mul/fma .rn.f32x2, Blackwell): each half
+// rounds exactly as the scalar __fadd_rn / __fmul_rn / __fmaf_rn, and being
+// written out here the compiler cannot contract a multiply into a following
+// add, which it did with the paired intrinsics (a fused result differing in
+// the last bit from the scalar sequence in about 1 of 10^4 cases).
+__device__ __forceinline__ float2 add2(float2 a, float2 b) {
+  float2 d;
+  asm("{.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+      "add.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;}"
+      : "=f"(d.x), "=f"(d.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return d;
+}
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) {
+  float2 d;
+  asm("{.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+      "mul.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;}"
+      : "=f"(d.x), "=f"(d.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return d;
+}
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
+  float2 d;
+  asm("{.reg .b64 ra, rb, rc, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+      "mov.b64 rc, {%6, %7};\n\tfma.rn.f32x2 rd, ra, rb, rc;\n\tmov.b64 {%0, %1}, rd;}"
+      : "=f"(d.x), "=f"(d.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+  return d;
+}
+
 // RelaxCell's FP32 Newton update (problem_ch.cuh) of two cells at once, one
 // in each half of the packed pairs, with Blackwell's paired FP32 arithmetic.
 // Every operation is RelaxCell's, in its order and rounding (x - 0.5 is
@@ -155,39 +185,29 @@ __device__ __forceinline__ void relax_pair_f32(float2 pc, float2 pw, float2 pe, 
                                                float2 pn, float2 mw, float2 me, float2 ms,
                                                float2 mn, float2 f0, float2 f1, float2 bs,
                                                const RelaxK2& K, float2& phi, float2& mu) {
-  const float2 smu = __fadd2_rn(__fadd2_rn(__fadd2_rn(mw, me), ms), mn);
-  const float2 sph = __fadd2_rn(__fadd2_rn(__fadd2_rn(pe, pw), pn), ps);
-  float2 cmh, nl;
+  const float2 smu = add2(add2(add2(mw, me), ms), mn);
+  const float2 sph = add2(add2(add2(pe, pw), pn), ps);
+  const float2 cmh = add2(DELTA ? add2(bs, pc) : pc, K.mhalf);
+  const float2 u = mul2(mul2(K.three, cmh), cmh);
+  const float2 d2 = mul2(u, K.alpha);     // D2fc(cfull)
+  const float2 nd2 = mul2(u, K.nalpha);   // -D2fc(cfull)
+  const float2 na21 = add2(d2, K.tmp3);   // -a21
+  float2 nl;
   if (DELTA) {
-    // The correction form's terms, one half at a time with RelaxCell's scalar
-    // operations: cfull = base + e, and DfcDelta(base, e) = alpha e (3 c^2 +
-    // 3 c e + e^2), c = base - 1/2.
-    auto half = [&](float b, float e, float& cm, float& n) {
-      cm = __fadd_rn(__fadd_rn(b, e), -0.5f);
-      const float c = __fadd_rn(b, -0.5f);
-      const float c3 = __fmul_rn(3.f, c);
-      const float poly =
-          __fadd_rn(__fadd_rn(__fmul_rn(c3, c), __fmul_rn(c3, e)), __fmul_rn(e, e));
-      n = __fmul_rn(__fmul_rn(K.alpha.x, e), poly);
-    };
-    half(bs.x, pc.x, cmh.x, nl.x);
-    half(bs.y, pc.y, cmh.y, nl.y);
+    // DfcDelta(base, e): alpha e (3 c^2 + 3 c e + e^2), c = base - 1/2.
+    const float2 c = add2(bs, K.mhalf);
+    const float2 c3 = mul2(K.three, c);
+    const float2 poly = add2(add2(mul2(c3, c), mul2(c3, pc)), mul2(pc, pc));
+    nl = mul2(mul2(K.alpha, pc), poly);
   } else {
-    cmh = __fadd2_rn(pc, K.mhalf);
-    nl = __fmul2_rn(__fmul2_rn(__fmul2_rn(cmh, cmh), cmh), K.alpha);  // Dfc
+    nl = mul2(mul2(mul2(cmh, cmh), cmh), K.alpha);  // Dfc
   }
-  const float2 u = __fmul2_rn(__fmul2_rn(K.three, cmh), cmh);
-  const float2 d2 = __fmul2_rn(u, K.alpha);     // D2fc(cfull)
-  const float2 nd2 = __fmul2_rn(u, K.nalpha);   // -D2fc(cfull)
-  const float2 na21 = __fadd2_rn(d2, K.tmp3);   // -a21
-  const float2 b1 = __ffma2_rn(K.tmp1, smu, f0);
-  const float2 b2 = __ffma2_rn(K.ntmp2, sph, __ffma2_rn(nd2, pc, __fadd2_rn(f1, nl)));
-  const float2 det = __ffma2_rn(K.a12, na21, K.one);
-  float2 r;
-  r.x = __fdividef(1.f, det.x);
-  r.y = __fdividef(1.f, det.y);
-  phi = __fmul2_rn(__ffma2_rn(K.na12, b2, b1), r);
-  mu = __fmul2_rn(__ffma2_rn(na21, b1, b2), r);
+  const float2 b1 = fma2(K.tmp1, smu, f0);
+  const float2 b2 = fma2(K.ntmp2, sph, fma2(nd2, pc, add2(f1, nl)));
+  const float2 det = fma2(K.a12, na21, K.one);
+  const float2 r = make_float2(problem::rcp_approx(det.x), problem::rcp_approx(det.y));
+  phi = mul2(fma2(K.na12, b2, b1), r);
+  mu = mul2(fma2(na21, b1, b2), r);
 }
 
 // The Newton updates of cells A (row y) and B (row y + 1), by the working
@@ -268,6 +288,7 @@ __device__ __forceinline__ void smooth_band(T* s0, T* s1, const T* sf0, const T*
   constexpr unsigned FULL = 0xffffffffu;
   V ps = v0[(ylo - 1) * RV], p0 = v0[ylo * RV];
   V ms = v1[(ylo - 1) * RV], m0 = v1[ylo * RV];
+#pragma unroll 2
   for (int y = ylo; y < yhi; y += 2) {
     const V p1 = v0[(y + 1) * RV], p2 = v0[(y + 2) * RV];
     const V m1 = v1[(y + 1) * RV], m2 = v1[(y + 2) * RV];

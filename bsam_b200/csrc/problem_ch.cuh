@@ -35,6 +35,15 @@ template <class T> __device__ __forceinline__ T DfcDelta(T b, T e, T alpha) {
   return alpha * e * (T(3) * c * c + T(3) * c * e + e * e);
 }
 
+// Approximate reciprocal of the FP32 working levels (PTX rcp.approx.ftz.f32,
+// maximum relative error 2^-23), one instruction; the scalar and the paired
+// forms of the FP32 update both take it.
+__device__ __forceinline__ float rcp_approx(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
 // Neighbourhood of one cell: centre values and the -/+ neighbours per
 // dimension, for both components (phi = q(:,:,1), mu = q(:,:,2)).
 template <class T, int D> struct Stencil {
@@ -67,11 +76,11 @@ __device__ __forceinline__ void RelaxCell(const Stencil<T, D>& s, T f0, T f1, T 
   const T cfull = DELTA ? base + s.pc : s.pc;
   if constexpr (sizeof(T) == 4) {
     // FP32 working levels of the mixed form: the same Newton step with
-    // contracted products and one approximate reciprocal (__fdividef,
-    // 2 ulp), since these levels only smooth a correction whose FP64 defect
-    // is recomputed exactly; the FP64 path below keeps the reference's
-    // operation order.  Every operation is an explicitly rounded intrinsic,
-    // so the compiler evaluates exactly this sequence -- the one the paired
+    // contracted products and one approximate reciprocal (rcp_approx), since
+    // these levels only smooth a correction whose FP64 defect is recomputed
+    // exactly; the FP64 path below keeps the reference's operation order.
+    // Every operation is an explicitly rounded one the compiler may not
+    // contract, so it evaluates exactly this sequence -- the one the paired
     // FP32 form of the fused 2D stage (relax_pair_f32) evaluates too.
     const float cf = DELTA ? __fadd_rn(base, s.pc) : s.pc;
     const float cmh = __fadd_rn(cf, -0.5f);
@@ -103,7 +112,7 @@ __device__ __forceinline__ void RelaxCell(const Stencil<T, D>& s, T f0, T f1, T 
     const T b1f = __fmaf_rn(tmp1, smuf, f0);
     const T b2f = __fmaf_rn(-tmp2, sphf, __fmaf_rn(-d2, s.pc, f1 + nlf));
     const T detf = __fmaf_rn(-a12, a21f, T(1));
-    const T r = __fdividef(T(1), detf);
+    const T r = rcp_approx(detf);
     phi = __fmaf_rn(-a12, b2f, b1f) * r;
     mu = __fmaf_rn(-a21f, b1f, b2f) * r;
     return;

@@ -68,7 +68,8 @@ ABI_SYMBOLS = (
     "bsam_gpu_restrict_level", "bsam_host_buffer_flags", "bsam_host_child_desc",
     "bsam_host_format_frame", "bsam_host_write_frame",
     "bsam_gpu_set_ghost_level", "bsam_gpu_after_step_stats", "bsam_gpu_stash", "bsam_gpu_regrid",
-    "bsam_gpu_errflags_level", "bsam_amr_create", "bsam_amr_step", "bsam_amr_table",
+    "bsam_gpu_errflags_level", "bsam_gpu_tag_level", "bsam_host_new_subgrids_sat",
+    "bsam_amr_create", "bsam_amr_step", "bsam_amr_table",
     "bsam_amr_destroy", "bsam_amr_profile",
     "bsam_batch_create", "bsam_batch_destroy", "bsam_batch_set_tuning", "bsam_batch_footprint",
     "bsam_batch_submit", "bsam_batch_advance", "bsam_batch_sync", "bsam_batch_run",
@@ -150,6 +151,10 @@ def lib():
                                         ctypes.c_int, ctypes.POINTER(PatchDesc)]
     L.bsam_host_new_subgrids.argtypes = [ctypes.c_int, ip, ctypes.POINTER(ctypes.c_uint8),
                                          ctypes.c_double, ctypes.c_int, ip, ctypes.c_int]
+    L.bsam_host_new_subgrids_sat.argtypes = [ctypes.c_int, ip, ctypes.POINTER(ctypes.c_int32),
+                                             ctypes.c_double, ctypes.c_int, ip, ctypes.c_int]
+    L.bsam_gpu_tag_level.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                     ctypes.POINTER(ctypes.c_int32)]
     L.bsam_gpu_destroy.argtypes = [vp]
     L.bsam_gpu_strerror.argtypes = [ctypes.c_int]
     L.bsam_gpu_strerror.restype = ctypes.c_char_p

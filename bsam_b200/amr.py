@@ -174,6 +174,35 @@ def new_subgrids(flags: np.ndarray, desfill: float, mgp: int, maxboxes: int = 40
     return boxes[:6 * n].reshape(n, 3, 2)
 
 
+def summed_area(flags: np.ndarray) -> np.ndarray:
+    """Inclusive summed-area table of 0/1 flags (1:mx)^d, int32, Fortran
+    order (the layout bsam_gpu_tag_level returns per patch)."""
+    s = np.asarray(flags, dtype=np.int64)
+    for ax in range(s.ndim):
+        s = np.cumsum(s, axis=ax)
+    return np.asfortranarray(s, dtype=np.int32)
+
+
+def new_subgrids_sat(sat: np.ndarray, desfill: float, mgp: int,
+                     maxboxes: int = 4096) -> np.ndarray:
+    """new_subgrids from a patch's summed-area table of its flags
+    (bsam_host_new_subgrids_sat)."""
+    import ctypes
+    from . import BsamError, lib
+    st = np.asfortranarray(sat, dtype=np.int32)
+    nd = st.ndim
+    mx = np.array(list(st.shape) + [1] * (3 - nd), dtype=np.int32)
+    boxes = np.zeros(6 * maxboxes, dtype=np.int32)
+    ip = ctypes.POINTER(ctypes.c_int)
+    n = lib().bsam_host_new_subgrids_sat(nd, mx.ctypes.data_as(ip),
+                                         st.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                         float(desfill), int(mgp), boxes.ctypes.data_as(ip),
+                                         maxboxes)
+    if n < 0:
+        raise BsamError(f"bsam_host_new_subgrids_sat failed ({n})")
+    return boxes[:6 * n].reshape(n, 3, 2)
+
+
 def _desc(level, parent, mx, mbounds, mglobal, mthbc, dx, xlower):
     return {"level": level, "parent": parent, "mx": list(mx) + [1] * (3 - len(mx)),
             "mbounds": [list(b) for b in mbounds] + [[1, 1]] * (3 - len(mbounds)),

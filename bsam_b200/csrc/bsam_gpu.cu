@@ -108,6 +108,8 @@ struct bsam_gpu {
   size_t regrid_cap = 0;
   std::vector<unsigned char> regrid_host;
   uint8_t* d_flags = nullptr;  // bsam_gpu_errflags_level's device flags
+  int32_t* d_sat = nullptr;    // bsam_gpu_tag_level's summed-area tables
+  size_t sat_cap = 0;
   CopySpan* d_qold_spans = nullptr;  // CopyQToQold: q -> qold of every patch that has qold
   int nqold_spans = 0;
   int64_t qold_span_max = 0;
@@ -1465,6 +1467,76 @@ int bsam_gpu_errflags_level(bsam_gpu* h, int level, double tol, uint8_t* flags) 
   return BSAM_OK;
 }
 
+int bsam_gpu_tag_level(bsam_gpu* h, int level, double tol, int ibuffer, int32_t* sat) {
+  if (!h || !h->have_hierarchy || !sat || ibuffer < 0) return BSAM_ERR_ARG;
+  if (level < 0 || level > h->finestlevel)
+    return fail(h, BSAM_ERR_ARG, "tag_level needs a level >= 0");
+  CU(cudaSetDevice(h->device));
+  const int nd = h->rp.ndims;
+  // The level's patches in table order, their cells concatenated.
+  std::vector<FlagTask> tasks;
+  std::vector<LevelPatch> lp;
+  size_t total = 0, ncell_max = 0;
+  for (int p = 0; p < h->nuser; ++p) {
+    if (h->desc[p].level != level) continue;
+    const size_t ncell = (size_t)cells_of(h->hp[p].n, nd);
+    tasks.push_back(FlagTask{(int64_t)total, p, 0});
+    LevelPatch L{};
+    L.off = (int64_t)total;
+    for (int n = 0; n < 3; ++n) {
+      L.n[n] = n < nd ? h->hp[p].n[n] : 1;
+      L.g0[n] = n < nd ? h->desc[p].mglobal[n][0] : 1;
+    }
+    lp.push_back(L);
+    ncell_max = std::max(ncell_max, ncell);
+    total += ncell;
+  }
+  if (total == 0) return BSAM_OK;
+  const int np = (int)tasks.size();
+  if (np > 65535) return fail(h, BSAM_ERR_ARG, "tag_level: too many patches");
+  if (2 * total > h->flags_cap) {
+    if (h->d_flags) cudaFree(h->d_flags);
+    h->d_flags = nullptr;
+    h->flags_cap = 0;
+    if (cudaMalloc(&h->d_flags, 2 * total) != cudaSuccess)
+      return fail(h, BSAM_ERR_NOMEM, "flag buffer allocation failed");
+    h->flags_cap = 2 * total;
+  }
+  if (total > h->sat_cap) {
+    if (h->d_sat) cudaFree(h->d_sat);
+    h->d_sat = nullptr;
+    h->sat_cap = 0;
+    if (cudaMalloc(&h->d_sat, sizeof(int32_t) * total) != cudaSuccess)
+      return fail(h, BSAM_ERR_NOMEM, "summed-area table allocation failed");
+    h->sat_cap = total;
+  }
+  // One upload: the tagging tasks, then the level's patches.
+  std::vector<unsigned char> buf(sizeof(FlagTask) * np + sizeof(LevelPatch) * np);
+  std::memcpy(buf.data(), tasks.data(), sizeof(FlagTask) * np);
+  std::memcpy(buf.data() + sizeof(FlagTask) * np, lp.data(), sizeof(LevelPatch) * np);
+  int rc = upload_tasks(h, buf.data(), buf.size());
+  if (rc) return rc;
+  const FlagTask* d_tasks = reinterpret_cast<const FlagTask*>(h->d_regrid);
+  const LevelPatch* d_lp = reinterpret_cast<const LevelPatch*>(h->d_regrid + sizeof(FlagTask) * np);
+  uint8_t* raw = h->d_flags;
+  uint8_t* buffered = h->d_flags + total;
+  const dim3 g((unsigned)std::min<size_t>((ncell_max + 255) / 256, 1024), (unsigned)np);
+  if (nd == 2) {
+    k_errflags_list<2><<<g, 256, 0, h->stream>>>(h->d_patches, d_tasks, tol, raw);
+    k_buffer_list<2><<<g, 256, 0, h->stream>>>(d_lp, np, ibuffer, raw, buffered);
+    k_sat_list<2><<<np, 256, 0, h->stream>>>(d_lp, buffered, h->d_sat);
+  } else {
+    k_errflags_list<3><<<g, 256, 0, h->stream>>>(h->d_patches, d_tasks, tol, raw);
+    k_buffer_list<3><<<g, 256, 0, h->stream>>>(d_lp, np, ibuffer, raw, buffered);
+    k_sat_list<3><<<np, 256, 0, h->stream>>>(d_lp, buffered, h->d_sat);
+  }
+  h->stats.launches += 3;
+  CU(cudaGetLastError());
+  CU(cudaMemcpyAsync(sat, h->d_sat, sizeof(int32_t) * total, cudaMemcpyDeviceToHost, h->stream));
+  CU(cudaStreamSynchronize(h->stream));
+  return BSAM_OK;
+}
+
 int bsam_gpu_init_patch(bsam_gpu* h, int patch) {
   if (!h || !h->have_hierarchy) return BSAM_ERR_ARG;
   if (patch < 0 || patch >= h->nuser || h->desc[patch].level < 1)
@@ -1919,6 +1991,7 @@ int bsam_gpu_destroy(bsam_gpu* h) {
   if (h->d_meta) cudaFree(h->d_meta);
   if (h->d_regrid) cudaFree(h->d_regrid);
   if (h->d_flags) cudaFree(h->d_flags);
+  if (h->d_sat) cudaFree(h->d_sat);
   if (h->d_status) cudaFree(h->d_status);
   if (h->h_status) cudaFreeHost(h->h_status);
   if (h->stream) cudaStreamDestroy(h->stream);

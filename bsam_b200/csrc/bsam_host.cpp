@@ -219,25 +219,18 @@ int bsam_host_take_time_steps(bsam_gpu* h, int nsteps, int root_patch, double* q
   return BSAM_OK;
 }
 
-int bsam_host_new_subgrids(int ndims, const int* mx, const uint8_t* flags, double desfill,
-                           int mgp, int* boxes, int maxboxes) {
-  if ((ndims != 2 && ndims != 3) || !mx || !flags || !boxes || maxboxes < 0 || mgp < 1)
-    return BSAM_ERR_ARG;
-  const int nd = ndims;
-  const int m[3] = {mx[0], mx[1], nd == 3 ? mx[2] : 1};
-  for (int n = 0; n < 3; ++n)
-    if (m[n] < 1) return BSAM_ERR_ARG;
-  using Box = std::array<int, 6>;  // lo, hi per dimension
-  // Flagged cells in a box (GridFlagRatio's numerator, a signature entry).
-  auto count = [&](const Box& b) {
-    long s = 0;
-    for (int k = b[4]; k <= b[5]; ++k)
-      for (int j = b[2]; j <= b[3]; ++j) {
-        const uint8_t* row = flags + (size_t)m[0] * ((j - 1) + (size_t)m[1] * (k - 1));
-        for (int i = b[0]; i <= b[1]; ++i) s += row[i - 1] != 0;
-      }
-    return s;
-  };
+extern "C++" {
+namespace {
+
+using Box6 = std::array<int, 6>;  // lo, hi per dimension
+
+// NewSubGrids (lib/bsamroutines.f90:1352-1579) over a patch of extent m,
+// with count(box) the number of flagged cells in a box (GridFlagRatio's
+// numerator; GetSignatures' entries are the counts of one-cell slabs).
+template <class Count>
+int new_subgrids_impl(int nd, const int* m, Count count, double desfill, int mgp, int* boxes,
+                      int maxboxes) {
+  using Box = Box6;
   auto fill_ratio = [&](const Box& b) {
     long cells = 1;
     for (int n = 0; n < nd; ++n) cells *= b[2 * n + 1] - b[2 * n] + 1;
@@ -325,6 +318,52 @@ int bsam_host_new_subgrids(int ndims, const int* mx, const uint8_t* flags, doubl
   for (size_t g = 0; g < grids.size(); ++g)
     for (int e = 0; e < 6; ++e) boxes[6 * g + e] = e / 2 < nd ? grids[g][e] : 1;
   return (int)grids.size();
+}
+}  // namespace
+}  // extern "C++"
+
+int bsam_host_new_subgrids(int ndims, const int* mx, const uint8_t* flags, double desfill,
+                           int mgp, int* boxes, int maxboxes) {
+  if ((ndims != 2 && ndims != 3) || !mx || !flags || !boxes || maxboxes < 0 || mgp < 1)
+    return BSAM_ERR_ARG;
+  const int nd = ndims;
+  const int m[3] = {mx[0], mx[1], nd == 3 ? mx[2] : 1};
+  for (int n = 0; n < 3; ++n)
+    if (m[n] < 1) return BSAM_ERR_ARG;
+  // Flagged cells in a box, by visiting them.
+  auto count = [&](const Box6& b) {
+    long s = 0;
+    for (int k = b[4]; k <= b[5]; ++k)
+      for (int j = b[2]; j <= b[3]; ++j) {
+        const uint8_t* row = flags + (size_t)m[0] * ((j - 1) + (size_t)m[1] * (k - 1));
+        for (int i = b[0]; i <= b[1]; ++i) s += row[i - 1] != 0;
+      }
+    return s;
+  };
+  return new_subgrids_impl(nd, m, count, desfill, mgp, boxes, maxboxes);
+}
+
+int bsam_host_new_subgrids_sat(int ndims, const int* mx, const int32_t* sat, double desfill,
+                               int mgp, int* boxes, int maxboxes) {
+  if ((ndims != 2 && ndims != 3) || !mx || !sat || !boxes || maxboxes < 0 || mgp < 1)
+    return BSAM_ERR_ARG;
+  const int nd = ndims;
+  const int m[3] = {mx[0], mx[1], nd == 3 ? mx[2] : 1};
+  for (int n = 0; n < 3; ++n)
+    if (m[n] < 1) return BSAM_ERR_ARG;
+  // S(i, j, k) = flagged cells in (1:i, 1:j, 1:k), 0 when an index is 0.
+  auto S = [&](int i, int j, int k) -> long {
+    if (i <= 0 || j <= 0 || k <= 0) return 0;
+    return sat[(i - 1) + (size_t)m[0] * ((j - 1) + (size_t)m[1] * (k - 1))];
+  };
+  // Flagged cells in a box, by inclusion-exclusion over its corners.
+  auto count = [&](const Box6& b) {
+    const int i0 = b[0] - 1, i1 = b[1], j0 = b[2] - 1, j1 = b[3], k0 = b[4] - 1, k1 = b[5];
+    long c = S(i1, j1, k1) - S(i0, j1, k1) - S(i1, j0, k1) + S(i0, j0, k1);
+    if (nd == 3) c -= S(i1, j1, k0) - S(i0, j1, k0) - S(i1, j0, k0) + S(i0, j0, k0);
+    return c;
+  };
+  return new_subgrids_impl(nd, m, count, desfill, mgp, boxes, maxboxes);
 }
 
 int bsam_host_buffer_flags(int ndims, int npatch, const int* mx, const int* mglobal,
@@ -489,7 +528,7 @@ struct bsam_amr {
   bsam_regrid_params p{};
   std::vector<bsam_patch_desc> table;
   bool firstamr = true;
-  std::vector<uint8_t> flags;
+  std::vector<int32_t> sat;  // summed-area tables of a level's buffered flags
   std::vector<int> boxes;
   // Host wall-clock seconds per phase, summed over steps (bsam_amr_profile).
   double t[BSAM_AMR_NPHASE] = {0};
@@ -573,20 +612,14 @@ int bsam_amr_step(bsam_amr* a, int* nvcycles, double* residual, int* converged) 
         for (int n = 0; n < nd; ++n) c *= (size_t)table[i].mx[n];
         cells += c;
       }
-    a->flags.assign(cells, 0);
-    rc = bsam_gpu_errflags_level(h, L, a->p.qtolerance[L], a->flags.data());
+    // Tagging, BufferAndList + InflateEdgeTags and the summed-area tables
+    // NewSubGrids counts from, all of the level on the device.
+    a->sat.assign(cells, 0);
+    rc = bsam_gpu_tag_level(h, L, a->p.qtolerance[L], a->p.ibuffer[L], a->sat.data());
     if (rc) return rc;
-    // BufferAndList + InflateEdgeTags over the level.
-    std::vector<int> mx(3 * lvl.size()), mg(6 * lvl.size());
+    std::vector<int> mx(3 * lvl.size());
     for (size_t k = 0; k < lvl.size(); ++k)
-      for (int n = 0; n < 3; ++n) {
-        mx[3 * k + n] = table[lvl[k]].mx[n];
-        mg[6 * k + 2 * n] = table[lvl[k]].mglobal[n][0];
-        mg[6 * k + 2 * n + 1] = table[lvl[k]].mglobal[n][1];
-      }
-    rc = bsam_host_buffer_flags(nd, (int)lvl.size(), mx.data(), mg.data(), a->flags.data(),
-                                a->p.ibuffer[L]);
-    if (rc) return rc;
+      for (int n = 0; n < 3; ++n) mx[3 * k + n] = table[lvl[k]].mx[n];
     clk.lap(BSAM_AMR_PHASE_TAG);
     // GridAdapt(L): RefineGrid -> NewSubGrids per patch, MakeNewGrid per box.
     std::vector<bsam_patch_desc> made;
@@ -598,9 +631,9 @@ int bsam_amr_step(bsam_amr* a, int* nvcycles, double* residual, int* converged) 
       // The boxes are disjoint and each holds a flagged cell: at most c.
       const int cap = (int)c;
       if (a->boxes.size() < 6 * c) a->boxes.resize(6 * c);
-      const int nb = bsam_host_new_subgrids(nd, &mx[3 * k], a->flags.data() + off,
-                                            a->p.desiredfillratios[L], a->p.minimumgridpoints[L],
-                                            a->boxes.data(), cap);
+      const int nb = bsam_host_new_subgrids_sat(nd, &mx[3 * k], a->sat.data() + off,
+                                                a->p.desiredfillratios[L],
+                                                a->p.minimumgridpoints[L], a->boxes.data(), cap);
       if (nb < 0) return nb;
       for (int b = 0; b < nb; ++b) {
         int box[6];

@@ -145,11 +145,9 @@ __device__ __forceinline__ RelaxK2 relax_k2(float tmp1, float tmp2, float tmp3, 
   return K;
 }
 
-// Paired FP32 operations (PTX add/mul/fma .rn.f32x2, Blackwell): each half
-// rounds exactly as the scalar __fadd_rn / __fmul_rn / __fmaf_rn, and being
-// written out here the compiler cannot contract a multiply into a following
-// add, which it did with the paired intrinsics (a fused result differing in
-// the last bit from the scalar sequence in about 1 of 10^4 cases).
+// Paired FP32 operations (PTX add/mul/fma .rn.f32x2, Blackwell), each half
+// rounded to nearest; written out as PTX so that every one stays a separately
+// rounded operation.
 __device__ __forceinline__ float2 add2(float2 a, float2 b) {
   float2 d;
   asm("{.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
@@ -179,7 +177,11 @@ __device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
 // in each half of the packed pairs, with Blackwell's paired FP32 arithmetic.
 // Every operation is RelaxCell's, in its order and rounding (x - 0.5 is
 // x + (-0.5); the negated products are the same products of negated
-// operands), so each half equals RelaxCell<float, 2> bit for bit.
+// operands), so each half equals RelaxCell<float, 2> bit for bit.  The
+// correction form's terms (cfull and DfcDelta) are taken one half at a time
+// with scalar operations: evaluated paired, the sum of the polynomial's terms
+// differed in its last bit from the scalar sum in about 1 of 10^4 cases in a
+// probe of random stencils, which the scalar form does not.
 template <bool DELTA>
 __device__ __forceinline__ void relax_pair_f32(float2 pc, float2 pw, float2 pe, float2 ps,
                                                float2 pn, float2 mw, float2 me, float2 ms,
@@ -187,21 +189,28 @@ __device__ __forceinline__ void relax_pair_f32(float2 pc, float2 pw, float2 pe, 
                                                const RelaxK2& K, float2& phi, float2& mu) {
   const float2 smu = add2(add2(add2(mw, me), ms), mn);
   const float2 sph = add2(add2(add2(pe, pw), pn), ps);
-  const float2 cmh = add2(DELTA ? add2(bs, pc) : pc, K.mhalf);
+  float2 cmh, nl;
+  if (DELTA) {
+    // cfull - 1/2 with cfull = base + e, and DfcDelta(base, e) = alpha e
+    // (3 c^2 + 3 c e + e^2), c = base - 1/2: RelaxCell's scalar operations.
+    auto half = [&](float b, float e, float& cm, float& n) {
+      cm = __fadd_rn(__fadd_rn(b, e), -0.5f);
+      const float c = __fadd_rn(b, -0.5f);
+      const float c3 = __fmul_rn(3.f, c);
+      const float poly =
+          __fadd_rn(__fadd_rn(__fmul_rn(c3, c), __fmul_rn(c3, e)), __fmul_rn(e, e));
+      n = __fmul_rn(__fmul_rn(K.alpha.x, e), poly);
+    };
+    half(bs.x, pc.x, cmh.x, nl.x);
+    half(bs.y, pc.y, cmh.y, nl.y);
+  } else {
+    cmh = add2(pc, K.mhalf);
+    nl = mul2(mul2(mul2(cmh, cmh), cmh), K.alpha);  // Dfc
+  }
   const float2 u = mul2(mul2(K.three, cmh), cmh);
   const float2 d2 = mul2(u, K.alpha);     // D2fc(cfull)
   const float2 nd2 = mul2(u, K.nalpha);   // -D2fc(cfull)
   const float2 na21 = add2(d2, K.tmp3);   // -a21
-  float2 nl;
-  if (DELTA) {
-    // DfcDelta(base, e): alpha e (3 c^2 + 3 c e + e^2), c = base - 1/2.
-    const float2 c = add2(bs, K.mhalf);
-    const float2 c3 = mul2(K.three, c);
-    const float2 poly = add2(add2(mul2(c3, c), mul2(c3, pc)), mul2(pc, pc));
-    nl = mul2(mul2(K.alpha, pc), poly);
-  } else {
-    nl = mul2(mul2(mul2(cmh, cmh), cmh), K.alpha);  // Dfc
-  }
   const float2 b1 = fma2(K.tmp1, smu, f0);
   const float2 b2 = fma2(K.ntmp2, sph, fma2(nd2, pc, add2(f1, nl)));
   const float2 det = fma2(K.a12, na21, K.one);

@@ -60,6 +60,113 @@ __global__ void k_errflags_list(const DevPatch* __restrict__ PT, const FlagTask*
   errflags_patch<D>(PT, t.patch, tol, flags + t.off);
 }
 
+// ---- buffering and clustering signatures of a level, on the device ----------
+//
+// BufferAndList + InflateEdgeTags (lib/bsamroutines.f90:1159-1284) make every
+// cell of a level's patches flagged that lies within ibuffer cells (in each
+// dimension) of a cell flagged by the tagging, in global index space: the
+// union of the buffer boxes of the flagged cells, clipped to each patch
+// (a flagged cell whose box stays inside its patch only reaches that patch;
+// one whose box crosses the patch's edge reaches every patch of the level it
+// overlaps).  Berger-Rigoutsos (NewSubGrids, GetSignatures, GridFlagRatio,
+// 1352-1579) then only counts flagged cells in boxes and slabs of a patch,
+// which an inclusive summed-area table answers with 2^d lookups.
+
+// A patch of the level: its cells' offset in the level's arrays, its extent
+// and the global index of its first cell.
+struct LevelPatch {
+  int64_t off;
+  int32_t n[3], g0[3];
+};
+
+// Flag of the cell at global index (gi, gj, gk) of the level, 0 outside its
+// patches.  `self` is tried first (the common case: the cell's own patch).
+template <int D>
+__device__ __forceinline__ uint8_t level_flag(const LevelPatch* __restrict__ lp, int np, int self,
+                                              const uint8_t* __restrict__ in, int gi, int gj,
+                                              int gk) {
+  for (int t = -1; t < np; ++t) {
+    const int q = t < 0 ? self : t;
+    if (t == self) continue;
+    const LevelPatch& L = lp[q];
+    const int i = gi - L.g0[0], j = gj - L.g0[1], k = D == 3 ? gk - L.g0[2] : 0;
+    if (i < 0 || i >= L.n[0] || j < 0 || j >= L.n[1] || (D == 3 && (k < 0 || k >= L.n[2])))
+      continue;
+    return in[L.off + i + (int64_t)L.n[0] * (j + (int64_t)L.n[1] * k)];
+  }
+  return 0;
+}
+
+// The buffered flags of every patch of a level (blockIdx.y selects the patch).
+template <int D>
+__global__ void k_buffer_list(const LevelPatch* __restrict__ lp, int np, int ib,
+                              const uint8_t* __restrict__ in, uint8_t* __restrict__ out) {
+  const int p = blockIdx.y;
+  const LevelPatch L = lp[p];
+  const int64_t total = (int64_t)L.n[0] * L.n[1] * (D == 3 ? L.n[2] : 1);
+  const int kb = D == 3 ? ib : 0;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(e % L.n[0]), j = (int)((e / L.n[0]) % L.n[1]);
+    const int k = D == 3 ? (int)(e / ((int64_t)L.n[0] * L.n[1])) : 0;
+    // Cells whose whole neighbourhood lies in the patch read it directly.
+    const bool inner = i - ib >= 0 && i + ib < L.n[0] && j - ib >= 0 && j + ib < L.n[1] &&
+                       (D == 2 || (k - kb >= 0 && k + kb < L.n[2]));
+    uint8_t f = 0;
+    for (int dk = -kb; dk <= kb && !f; ++dk)
+      for (int dj = -ib; dj <= ib && !f; ++dj)
+        for (int di = -ib; di <= ib && !f; ++di) {
+          if (inner)
+            f = in[L.off + (i + di) + (int64_t)L.n[0] * ((j + dj) + (int64_t)L.n[1] * (k + dk))];
+          else
+            f = level_flag<D>(lp, np, p, in, L.g0[0] + i + di, L.g0[1] + j + dj,
+                              D == 3 ? L.g0[2] + k + dk : 0);
+        }
+    out[L.off + e] = f ? 1 : 0;
+  }
+}
+
+// Inclusive summed-area table of each patch's flags (a CTA per patch): sums
+// along x, then y, then z, each line by one thread.
+template <int D>
+__global__ void __launch_bounds__(256)
+    k_sat_list(const LevelPatch* __restrict__ lp, const uint8_t* __restrict__ in,
+               int32_t* __restrict__ sat) {
+  const LevelPatch L = lp[blockIdx.x];
+  const int n0 = L.n[0], n1 = L.n[1], n2 = D == 3 ? L.n[2] : 1;
+  int32_t* s = sat + L.off;
+  const uint8_t* f = in + L.off;
+  for (int line = threadIdx.x; line < n1 * n2; line += blockDim.x) {
+    int32_t acc = 0;
+    const int64_t b = (int64_t)line * n0;
+    for (int i = 0; i < n0; ++i) {
+      acc += f[b + i];
+      s[b + i] = acc;
+    }
+  }
+  __syncthreads();
+  for (int line = threadIdx.x; line < n0 * n2; line += blockDim.x) {
+    const int i = line % n0, k = line / n0;
+    int32_t acc = 0;
+    for (int j = 0; j < n1; ++j) {
+      const int64_t c = i + (int64_t)n0 * (j + (int64_t)n1 * k);
+      acc += s[c];
+      s[c] = acc;
+    }
+  }
+  if (D == 3) {
+    __syncthreads();
+    for (int line = threadIdx.x; line < n0 * n1; line += blockDim.x) {
+      int32_t acc = 0;
+      for (int k = 0; k < n2; ++k) {
+        const int64_t c = line + (int64_t)n0 * n1 * k;
+        acc += s[c];
+        s[c] = acc;
+      }
+    }
+  }
+}
+
 // The linear-prolongation weights of fine index I from coarse (qc) indices
 // I >> 1 and (I >> 1) + 1: 3 and 1 for even I, 1 and 3 for odd I.
 __device__ __forceinline__ double lin_pair(int I, double a0, double a1) {

@@ -119,6 +119,25 @@ class HierSolver:
                self.h, "errflags")
         return out
 
+    def tag_level(self, level: int, tol: float, ibuffer: int) -> list:
+        """Tagging, buffering and summed-area tables of a level on the device
+        (bsam_gpu_tag_level): one int32 table (1:mx)^d per patch of the level,
+        in table order."""
+        import ctypes
+        from . import _check, lib
+        nd = self.hier.ndims
+        pats = [d for d in self.hier.descs if d["level"] == level]
+        sizes = [int(np.prod(d["mx"][:nd])) for d in pats]
+        buf = np.zeros(sum(sizes), dtype=np.int32)
+        _check(lib().bsam_gpu_tag_level(self.h, level, tol, ibuffer,
+                                        buf.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))),
+               self.h, "tag_level")
+        out, off = [], 0
+        for d, n in zip(pats, sizes):
+            out.append(buf[off:off + n].reshape(tuple(d["mx"][:nd]), order="F"))
+            off += n
+        return out
+
     def init_patch(self, patch: int):
         """InitFields of a refined patch from its parent (mass-corrected
         prolongation; qold = q)."""

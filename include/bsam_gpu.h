@@ -202,6 +202,17 @@ int bsam_gpu_after_step_stats(bsam_gpu* h, double* integral);
 /* SetErrFlagsUser of every patch on `level` (table order), the flags of
  * each patch's (1:mx)^d cells concatenated in `flags`: one transfer. */
 int bsam_gpu_errflags_level(bsam_gpu* h, int level, double tol, uint8_t* flags);
+
+/* The tagging of every patch of `level` (as bsam_gpu_errflags_level), then
+ * its buffering by `ibuffer` cells (BufferAndList + InflateEdgeTags,
+ * lib/bsamroutines.f90:1159-1284: the union of every flagged cell's buffer
+ * box over the level's patches, as bsam_host_buffer_flags), then per patch
+ * the inclusive summed-area table of the buffered flags, all on the device.
+ * sat receives the tables of the level's patches in table order, each
+ * mx1 * mx2 [* mx3] int32 values, i fastest: sat(i,j,k) = the number of
+ * flagged cells in (1:i, 1:j, 1:k).  bsam_host_new_subgrids_sat clusters from
+ * them (NewSubGrids' signatures and fill ratios are box counts). */
+int bsam_gpu_tag_level(bsam_gpu* h, int level, double tol, int ibuffer, int32_t* sat);
 int bsam_gpu_stash(bsam_gpu* h);
 int bsam_gpu_regrid(bsam_gpu* h, int npatch, const bsam_patch_desc* patches, int finestlevel,
                     const int* carry, int ntransfer, const int* transfer);

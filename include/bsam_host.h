@@ -57,6 +57,13 @@ int bsam_host_take_time_steps(bsam_gpu* h, int nsteps, int root_patch, double* q
 int bsam_host_new_subgrids(int ndims, const int* mx, const uint8_t* flags, double desfill,
                            int mgp, int* boxes, int maxboxes);
 
+/* bsam_host_new_subgrids from the patch's inclusive summed-area table of its
+ * flags (sat(i,j,k) = flagged cells in (1:i, 1:j, 1:k), i fastest, as
+ * bsam_gpu_tag_level returns it): every count of a box or a signature slab
+ * in constant time; the same boxes in the same order. */
+int bsam_host_new_subgrids_sat(int ndims, const int* mx, const int32_t* sat, double desfill,
+                               int mgp, int* boxes, int maxboxes);
+
 /* Buffering of the cell flags of one level's patches, as BufferAndList and
  * InflateEdgeTags do it (lib/bsamroutines.f90:1159-1284): every cell flagged
  * before the call flags the cells within ibuffer of it (a cube in global

@@ -152,3 +152,23 @@ def test_native_amr_run_matches_oracle(gpu_lib, oracle, nd):
             assert list(t["level"]) == [d["level"] for d in rn.descs]
         finally:
             o.close()
+
+
+@pytest.mark.parametrize("nd", [2, 3])
+@pytest.mark.parametrize("ibuffer", [0, 1, 2])
+def test_tag_level_on_device_matches_host_buffering(gpu_lib, nd, ibuffer):
+    """bsam_gpu_tag_level (tagging, BufferAndList + InflateEdgeTags and the
+    summed-area tables, on the device) against the device's tagging
+    buffered by the host library (bsam_host_buffer_flags, pinned to the
+    reference's source) and summed on the host, on every level."""
+    h = hier(nd)
+    with amr.HierSolver(h) as s:
+        s.run(1)
+        for level in (0, 1):
+            idx = [i for i, d in enumerate(h.descs) if d["level"] == level]
+            for tol in (0.05, 0.2):
+                flags = [s.errflags(p, tol) for p in idx]
+                want = amr.buffer_flags(nd, [h.descs[p] for p in idx], flags, ibuffer)
+                got = s.tag_level(level, tol, ibuffer)
+                for w, g in zip(want, got):
+                    assert np.array_equal(amr.summed_area(w), g), (level, tol)

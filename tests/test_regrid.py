@@ -185,3 +185,27 @@ def test_buffer_flags_match_reference(gpu_free_lib, n):
     got = amr.buffer_flags(nd, descs, [f.astype(np.uint8) for f in fin], ib)
     for g, w in zip(got, fout):
         assert np.array_equal(g.astype(np.int64), w)
+
+
+@pytest.mark.parametrize("n", [0, 1, 2, 3])
+def test_new_subgrids_from_summed_area_table_match_reference(gpu_free_lib, n):
+    # The clustering that counts from a summed-area table (the form the
+    # native AMR driver uses with the device's tables) makes the reference's
+    # boxes too.
+    d = np.load(os.path.join(GOLD, f"ref_subgrids_{n}.npz"))
+    nd = int(d["ndims"])
+    got = amr.new_subgrids_sat(amr.summed_area(d["flags"]), float(d["fill"]), int(d["mgp"]))
+    assert np.array_equal(got[:, :nd, :], d["boxes"][:, :nd, :])
+
+
+@pytest.mark.parametrize("seed", [4, 5, 6])
+@pytest.mark.parametrize("nd", [2, 3])
+def test_new_subgrids_sat_equals_flags(gpu_free_lib, nd, seed):
+    rng = np.random.default_rng(seed)
+    shape = (40, 36) if nd == 2 else (20, 18, 16)
+    fl = (rng.random(shape) < 0.05).astype(np.uint8)
+    fl[tuple(slice(3, 9) for _ in range(nd))] = 1
+    for fill, mgp in ((0.85, 4), (0.6, 2), (0.95, 3)):
+        a = amr.new_subgrids(fl, fill, mgp)
+        b = amr.new_subgrids_sat(amr.summed_area(fl), fill, mgp)
+        assert np.array_equal(a, b), (fill, mgp)

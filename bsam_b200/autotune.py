@@ -10,9 +10,12 @@ mapped onto the B200 but not a single result bit (bsam_batch_tuning):
               tile buffer each (85 or 64 registers per thread), or 2 CTAs per
               SM with two buffers each (the next tile's copies land while the
               current one is computed)
-  fused_ctas  CTAs of a fused-stage launch (persistent grid-stride loop over
-              the stage's tiles)
+  fused_ctas  CTAs of a fused-stage launch (persistent loop over the stage's
+              tiles)
+  fused_chunk runs of consecutive tiles a fused-stage CTA takes at a time
   grid_ctas   CTAs of every other stage launch
+  tile_chunk  runs of consecutive tiles a CTA of those launches takes at a
+              time (a run's tiles mostly share one problem's records)
 
 The tuner times candidates on a sample of the caller's workload with CUDA
 events on the engine's stream (a few V-cycle ticks of every sampled problem,
@@ -34,7 +37,7 @@ from . import batch as BB
 
 # Search order: the fused stage's build before sweep fusion, so that fusion is
 # judged with the fused stage's best build.
-KNOBS = ("fused_occ", "per_pass", "fused_ctas", "grid_ctas")
+KNOBS = ("fused_occ", "per_pass", "fused_ctas", "fused_chunk", "grid_ctas", "tile_chunk")
 
 
 @dataclasses.dataclass(frozen=True)
@@ -43,6 +46,8 @@ class Choice:
     fused_occ: int = 0
     fused_ctas: int = 0
     grid_ctas: int = 0
+    tile_chunk: int = 0
+    fused_chunk: int = 0
 
     def as_dict(self) -> dict:
         return dataclasses.asdict(self)
@@ -58,6 +63,10 @@ def candidates(knob: str, nsm: int) -> list:
         return [0, 2 * nsm, 3 * nsm, 8 * nsm]
     if knob == "grid_ctas":
         return [0, 4 * nsm, 8 * nsm, 32 * nsm]
+    if knob == "tile_chunk":
+        return [0, 1, 2, 8]
+    if knob == "fused_chunk":
+        return [0, 2, 4]
     raise ValueError(knob)
 
 

@@ -49,7 +49,8 @@ class StepResult(ctypes.Structure):
 class BatchTuning(ctypes.Structure):
     _fields_ = [("grid_ctas", ctypes.c_int32), ("eager", ctypes.c_int32),
                 ("per_pass", ctypes.c_int32), ("fused_ctas", ctypes.c_int32),
-                ("fused_occ", ctypes.c_int32), ("reserved", ctypes.c_int32 * 3)]
+                ("fused_occ", ctypes.c_int32), ("tile_chunk", ctypes.c_int32),
+                ("fused_chunk", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
 class BatchStats(ctypes.Structure):
@@ -123,6 +124,26 @@ def problem_struct(prob) -> BatchProblem:
                         eps=prob.eps, alpha=prob.alpha)
 
 
+def problem_array(probs):
+    """The C descriptors of many problems in one array, filled column by
+    column through a numpy view (the same values as problem_struct)."""
+    _lib()
+    n = len(probs)
+    arr = (BatchProblem * n)()
+    v = np.ctypeslib.as_array(arr)
+    g = v["grid"]
+    g["ndims"] = [p.ndims for p in probs]
+    g["mx"] = [tuple(p.mx[k] if k < p.ndims else 1 for k in range(3)) for p in probs]
+    g["mthbc"] = [tuple(p.mthbc[:6]) for p in probs]
+    g["minlevel"] = [p.minlevel for p in probs]
+    g["xupper"] = [tuple(p.xupper[:3]) for p in probs]
+    v["nsteps"] = [p.nsteps for p in probs]
+    v["dt"] = [p.dt for p in probs]
+    v["eps"] = [p.eps for p in probs]
+    v["alpha"] = [p.alpha for p in probs]
+    return arr
+
+
 class Batch:
     """Many problems of one dimensionality resident on one GPU.
 
@@ -146,13 +167,16 @@ class Batch:
         self.ndims = ndims
         self.max_slots = max_slots
         self.probs = {}
+        self._q0_keep = {}
         if grid_ctas:
             self.set_tuning(grid_ctas=grid_ctas)
 
     def set_tuning(self, grid_ctas: int = 0, eager: int = 0, per_pass: int = 0,
-                   fused_ctas: int = 0, fused_occ: int = 0):
+                   fused_ctas: int = 0, fused_occ: int = 0, tile_chunk: int = 0,
+                   fused_chunk: int = 0):
         t = BatchTuning(grid_ctas=grid_ctas, eager=eager, per_pass=per_pass,
-                        fused_ctas=fused_ctas, fused_occ=fused_occ)
+                        fused_ctas=fused_ctas, fused_occ=fused_occ, tile_chunk=tile_chunk,
+                        fused_chunk=fused_chunk)
         _check(_lib().bsam_batch_set_tuning(self.h, ctypes.byref(t)), self.h, "set_tuning")
 
     def profile(self, enable: bool = True):
@@ -203,7 +227,7 @@ class Batch:
         n = len(probs)
         if n == 0:
             return []
-        arr = (BatchProblem * n)(*[problem_struct(p) for p in probs])
+        arr = problem_array(probs)
         slots = (ctypes.c_int * n)()
         L = _lib()
         if q0s is None:
@@ -216,13 +240,15 @@ class Batch:
             ptrs = (ctypes.POINTER(ctypes.c_double) * n)(
                 *[q.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) for q in keep])
             rc = L.bsam_batch_submit_many(self.h, n, arr, ptrs, slots)
-            self._q0_keep = keep  # the copies may still be reading them
         if rc < 0:
             _check(rc, self.h, "submit_many")
         out = []
         for k in range(n):
             if k < rc:
                 self.probs[slots[k]] = probs[k]
+                if q0s is not None:
+                    # the queued copy may still be reading it: kept until collected
+                    self._q0_keep[slots[k]] = keep[k]
                 out.append(slots[k])
             else:
                 out.append(None)
@@ -244,28 +270,34 @@ class Batch:
             qs = list(outs)
         else:
             qs = [np.empty(shp, order="F") for shp in shapes] if want_q else [None] * n
-        steps = [(StepResult * p.nsteps)() for p in probs]
+        # Every slot's step log in one buffer, read back through numpy views.
+        first = np.zeros(n + 1, dtype=np.int64)
+        first[1:] = np.cumsum([p.nsteps for p in probs])
+        logbuf = (StepResult * max(int(first[-1]), 1))()
+        base = ctypes.addressof(logbuf)
+        sz = ctypes.sizeof(StepResult)
         pq = (ctypes.POINTER(ctypes.c_double) * n)(
             *[q.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if q is not None else None
               for q in qs])
         ps = (ctypes.POINTER(StepResult) * n)(
-            *[ctypes.cast(st, ctypes.POINTER(StepResult)) for st in steps])
+            *[ctypes.cast(base + int(o) * sz, ctypes.POINTER(StepResult)) for o in first[:-1]])
         masses = (ctypes.c_double * n)() if want_mass else None
         rc = _lib().bsam_batch_collect_many(self.h, n, (ctypes.c_int * n)(*slots), pq, ps,
                                             masses)
         if rc == 0 or rc == ERR_DIVERGED:
             for s in slots:
                 self.probs.pop(s, None)
-            self._q0_keep = None
+                self._q0_keep.pop(s, None)
         _check(rc, self.h, "collect_many")
+        log = np.ctypeslib.as_array(logbuf)
+        nv = log["nvcycles"].astype(np.int32)
+        cv = log["converged"].astype(np.int32)
+        rs = log["residual"].astype(np.float64)
         out = []
         for k in range(n):
-            st = steps[k]
-            out.append({"q": qs[k],
-                        "nvcycles": np.array([x.nvcycles for x in st], dtype=np.int32),
-                        "converged": np.array([x.converged for x in st], dtype=np.int32),
-                        "residual": np.array([x.residual for x in st]),
-                        "mass": masses[k] if want_mass else None})
+            a, e = int(first[k]), int(first[k + 1])
+            out.append({"q": qs[k], "nvcycles": nv[a:e], "converged": cv[a:e],
+                        "residual": rs[a:e], "mass": masses[k] if want_mass else None})
         return out
 
     def busy(self) -> bool:
@@ -320,6 +352,7 @@ class Batch:
         # reports a diverged solve; any other failure leaves it resident.
         if rc == 0 or rc == ERR_DIVERGED:
             self.probs.pop(slot, None)
+            self._q0_keep.pop(slot, None)
         _check(rc, self.h, "collect")
         return {"q": q,
                 "nvcycles": np.array([s.nvcycles for s in steps], dtype=np.int32),
@@ -357,7 +390,8 @@ class Batch:
 
 def solve_all(problems, precision: int = PREC_MIXED, max_slots: int | None = None,
               pool_bytes: int = 0, device: int = 0, grid_ctas: int = 0, eager: int = 0,
-              per_pass: int = 0, fused_ctas: int = 0, fused_occ: int = 0):
+              per_pass: int = 0, fused_ctas: int = 0, fused_occ: int = 0, tile_chunk: int = 0,
+              fused_chunk: int = 0):
     """Solves every problem (one dimensionality) in one batch; admits more as
     slots free up.  Returns the collect() results in input order."""
     if not problems:
@@ -367,9 +401,10 @@ def solve_all(problems, precision: int = PREC_MIXED, max_slots: int | None = Non
     tol = problems[0].qerrortol
     with Batch(nd, precision=precision, max_slots=ms, pool_bytes=pool_bytes, qerrortol=tol,
                maxvcycles=problems[0].maxvcycles, device=device) as b:
-        if grid_ctas or eager or per_pass or fused_ctas or fused_occ:
+        if any((grid_ctas, eager, per_pass, fused_ctas, fused_occ, tile_chunk, fused_chunk)):
             b.set_tuning(grid_ctas=grid_ctas, eager=eager, per_pass=per_pass,
-                         fused_ctas=fused_ctas, fused_occ=fused_occ)
+                         fused_ctas=fused_ctas, fused_occ=fused_occ, tile_chunk=tile_chunk,
+                         fused_chunk=fused_chunk)
         out = [None] * len(problems)
         pending = list(range(len(problems)))
         slot_of = {}

@@ -3,8 +3,8 @@
 // Every V-cycle stage of a tick is one launch over a device-resident work
 // list that covers that stage for all resident problems; the list's length
 // is read on the device, so problems can be added between ticks without
-// re-capturing the tick graph.  CTAs walk the list in a grid-stride loop and
-// run the same tile bodies as the single-problem kernels (kernels.cuh,
+// re-capturing the tick graph.  CTAs walk the list in runs of consecutive
+// tiles (TileRuns) and run the same tile bodies as the single-problem kernels (kernels.cuh,
 // mixed.cuh, bottom.cuh); tiles of finished problems are skipped.
 //
 // Per-problem control (k_batch_control) replaces the host loop of
@@ -64,9 +64,9 @@ struct BatchCtl {
 template <class T, int D>
 __global__ void __launch_bounds__(BLOCK_THREADS)
     kb_relax(const DevPatch* __restrict__ PT, const Item* __restrict__ items,
-             const int* __restrict__ count, int color) {
+             const int* __restrict__ count, int color, TileRuns R) {
   const int n = *count;
-  for (int b = blockIdx.x; b < n; b += gridDim.x) relax_item<T, D>(PT, items[b], color);
+  for (int b = R.first(); b < n; b = R.next(b)) relax_item<T, D>(PT, items[b], color);
 }
 
 // Transfers between a depth-d record (value type TC) and its parent, whose
@@ -74,9 +74,9 @@ __global__ void __launch_bounds__(BLOCK_THREADS)
 template <class TC, int D>
 __global__ void __launch_bounds__(BLOCK_THREADS)
     kb_restrict(const DevPatch* __restrict__ PT, const Item* __restrict__ items,
-                const int* __restrict__ count) {
+                const int* __restrict__ count, TileRuns R) {
   const int n = *count;
-  for (int b = blockIdx.x; b < n; b += gridDim.x) {
+  for (int b = R.first(); b < n; b = R.next(b)) {
     const Item it = items[b];
     if (PT[it.patch].pprec == PREC_F32) restrict_item<TC, float, D>(PT, it);
     else restrict_item<TC, double, D>(PT, it);
@@ -86,9 +86,9 @@ __global__ void __launch_bounds__(BLOCK_THREADS)
 template <class TC, int D>
 __global__ void __launch_bounds__(BLOCK_THREADS)
     kb_coarse_load(const DevPatch* __restrict__ PT, const Item* __restrict__ items,
-                   const int* __restrict__ count) {
+                   const int* __restrict__ count, TileRuns R) {
   const int n = *count;
-  for (int b = blockIdx.x; b < n; b += gridDim.x) {
+  for (int b = R.first(); b < n; b = R.next(b)) {
     const Item it = items[b];
     if (PT[it.patch].pprec == PREC_F32) coarse_load_item<TC, float, D>(PT, it);
     else coarse_load_item<TC, double, D>(PT, it);
@@ -98,9 +98,9 @@ __global__ void __launch_bounds__(BLOCK_THREADS)
 template <class TC, int D>
 __global__ void __launch_bounds__(BLOCK_THREADS)
     kb_correct(const DevPatch* __restrict__ PT, const Item* __restrict__ items,
-               const int* __restrict__ count) {
+               const int* __restrict__ count, TileRuns R) {
   const int n = *count;
-  for (int b = blockIdx.x; b < n; b += gridDim.x) {
+  for (int b = R.first(); b < n; b = R.next(b)) {
     const Item it = items[b];
     if (PT[it.patch].pprec == PREC_F32) correct_item<TC, float, D>(PT, it);
     else correct_item<TC, double, D>(PT, it);
@@ -161,9 +161,9 @@ __device__ __forceinline__ void correct_block2(const DevPatch& C, const DevPatch
 template <class TC>
 __global__ void __launch_bounds__(BLOCK_THREADS, BATCH_LATENCY_MIN_BLOCKS)
     kb_correct2(const DevPatch* __restrict__ PT, const Item* __restrict__ items,
-                const int* __restrict__ count) {
+                const int* __restrict__ count, TileRuns R) {
   const int n = *count;
-  for (int b = blockIdx.x; b < n; b += gridDim.x) {
+  for (int b = R.first(); b < n; b = R.next(b)) {
     const Item it = items[b];
     const DevPatch C = PT[it.patch];
     if (!C.active) continue;
@@ -200,18 +200,18 @@ __global__ void __launch_bounds__(BATCH_BOTTOM_THREADS, 4)
 template <int D>
 __global__ void __launch_bounds__(BLOCK_THREADS)
     kb_source(const DevPatch* __restrict__ PT, const Item* __restrict__ items,
-              const int* __restrict__ count) {
+              const int* __restrict__ count, TileRuns R) {
   const int n = *count;
-  for (int b = blockIdx.x; b < n; b += gridDim.x) source_item<double, D>(PT, items[b], 1);
+  for (int b = R.first(); b < n; b = R.next(b)) source_item<double, D>(PT, items[b], 1);
 }
 
 // FP64 form: residual partial of every master tile.
 template <int D>
 __global__ void __launch_bounds__(BLOCK_THREADS)
     kb_resid(const DevPatch* __restrict__ PT, const Item* __restrict__ items,
-             const int* __restrict__ count, double* __restrict__ partials) {
+             const int* __restrict__ count, double* __restrict__ partials, TileRuns R) {
   const int n = *count;
-  for (int b = blockIdx.x; b < n; b += gridDim.x) {
+  for (int b = R.first(); b < n; b = R.next(b)) {
     const Item it = items[b];
     const DevPatch P = PT[it.patch];
     if (!P.active) continue;  // uniform per CTA
@@ -225,9 +225,10 @@ __global__ void __launch_bounds__(BLOCK_THREADS)
 template <int D>
 __global__ void __launch_bounds__(BLOCK_THREADS, BATCH_LATENCY_MIN_BLOCKS)
     kb_defect(const DevPatch* __restrict__ PT, const Item* __restrict__ items,
-              const int* __restrict__ count, double* __restrict__ partials, int newstep_only) {
+              const int* __restrict__ count, double* __restrict__ partials, int newstep_only,
+              TileRuns R) {
   const int n = *count;
-  for (int b = blockIdx.x; b < n; b += gridDim.x) {
+  for (int b = R.first(); b < n; b = R.next(b)) {
     const Item it = items[b];
     const DevPatch M = PT[it.patch];
     if (!M.active || (newstep_only && !M.newstep)) continue;  // uniform per CTA
@@ -242,9 +243,9 @@ __global__ void __launch_bounds__(BLOCK_THREADS, BATCH_LATENCY_MIN_BLOCKS)
 template <int D>
 __global__ void __launch_bounds__(BLOCK_THREADS, BATCH_LATENCY_MIN_BLOCKS)
     kb_update(const DevPatch* __restrict__ PT, const Item* __restrict__ items,
-              const int* __restrict__ count) {
+              const int* __restrict__ count, TileRuns R) {
   const int n = *count;
-  for (int b = blockIdx.x; b < n; b += gridDim.x) {
+  for (int b = R.first(); b < n; b = R.next(b)) {
     const Item it = items[b];
     const DevPatch M = PT[it.patch];
     if (!M.active) continue;
@@ -441,6 +442,39 @@ __global__ void k_init_seeded_list(const DevPatch* __restrict__ PT,
   init_seeded_range<D>(P, t.seed, t.cbar, t.amp, t.k2,
                        (int64_t)blockIdx.x * blockDim.x + threadIdx.x,
                        (int64_t)gridDim.x * blockDim.x);
+}
+
+// One problem's root state between the caller's Fortran-ordered q (both
+// components, ghosts included: `rows` rows of e0 values per component) and
+// the pitched master fields q0, q1 (row pitch sy; in 3D the plane pitch is
+// sy * (n1 + 2), so the rows of every plane follow each other at pitch sy).
+// The packed copy lives in the engine's device transfer buffer, which one
+// contiguous DMA per problem fills from, or empties into, the caller's
+// buffer: pitched host copies of rows this short run far below the link's
+// speed.
+struct RowsTask {
+  double* packed;
+  double* q[2];
+  int64_t rows, sy;
+  int32_t e0, pad_;
+};
+
+// A warp per row: packed -> pitched (unpack) or pitched -> packed (pack).
+template <bool UNPACK>
+__global__ void __launch_bounds__(256) k_rows_list(const RowsTask* __restrict__ tasks) {
+  const RowsTask t = tasks[blockIdx.y];
+  const int lane = threadIdx.x & 31;
+  const int64_t wpb = blockDim.x >> 5;
+  for (int64_t r = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5); r < 2 * t.rows;
+       r += (int64_t)gridDim.x * wpb) {
+    const int c = r >= t.rows ? 1 : 0;
+    double* pitched = t.q[c] + (r - c * t.rows) * t.sy;
+    double* packed = t.packed + r * t.e0;
+    for (int i = lane; i < t.e0; i += 32) {
+      if (UNPACK) pitched[i] = packed[i];
+      else packed[i] = pitched[i];
+    }
+  }
 }
 
 __global__ void k_batch_budget(BatchCtl* __restrict__ ctl, int ticks) {

@@ -49,6 +49,11 @@ constexpr int MAXD = 8;   // top depths
 // Default bottom_cells: levels of at most this many cells run in the bottom
 // kernel (in FP64 in both forms, as bsam_gpu.cu does with the same value).
 constexpr int DEFAULT_BOTTOM_CELLS = 1024;
+// Default runs of consecutive list entries per CTA visit (TileRuns) for the
+// small-tile list kernels and for the fused stages (tuning.tile_chunk and
+// tuning.fused_chunk; 1 = grid-stride order).
+constexpr int kDefaultTileChunk = 4;
+constexpr int kDefaultFusedChunk = 1;
 // Lists: master tiles; bottom-chain tops; per top depth d: tiles of every
 // record (correction), footprint tiles (restriction / coarse load), tiles of
 // records smoothed per colour pass, fused-stage tiles; master tiles whose FP64
@@ -156,6 +161,18 @@ struct bsam_batch {
   std::deque<StageChunk> chunks;
   std::vector<size_t> pending;  // chunk indices (into `chunks`) awaiting an event
   std::vector<cudaEvent_t> free_events;
+  // Device transfer buffers of the batched submit (in) and collect (out):
+  // packed root states between the caller's buffers and the pitched fields.
+  // The submitted states are copied in on their own stream, so that the
+  // copies overlap ticks already queued on `stream`: xin_ready (copy stream)
+  // orders the spreading launch after them, xin_free (engine stream) orders
+  // the next copies after that launch.
+  double* d_xin = nullptr;
+  size_t xin_words = 0;
+  double* d_xout = nullptr;
+  size_t xout_words = 0;
+  cudaStream_t xstream = nullptr;
+  cudaEvent_t xin_ready = nullptr, xin_free = nullptr;
   std::string err;
 };
 
@@ -280,6 +297,27 @@ int stage_copy(bsam_batch* b, void* dst, const void* src, size_t n) {
   std::memcpy(s, src, n);
   CU(cudaMemcpyAsync(dst, s, n, cudaMemcpyHostToDevice, b->stream));
   return BSAM_OK;
+}
+
+// A device transfer buffer with room for `words` doubles (grown after the
+// work queued on both streams has drained); nullptr if the allocation fails.
+double* xfer_reserve(bsam_batch* b, double** buf, size_t* have, size_t words) {
+  if (words > *have) {
+    if (*buf) {
+      cudaStreamSynchronize(b->stream);
+      cudaStreamSynchronize(b->xstream);
+      cudaFree(*buf);
+      *buf = nullptr;
+    }
+    const size_t w = std::max(words, 2 * *have);
+    if (cudaMalloc(buf, sizeof(double) * w) != cudaSuccess) {
+      *buf = nullptr;
+      *have = 0;
+      return nullptr;
+    }
+    *have = w;
+  }
+  return *buf;
 }
 
 // ---- problem plan ----------------------------------------------------------------
@@ -574,6 +612,9 @@ void tick_t(bsam_batch* b, cudaGraphConditionalHandle handle, int in_graph) {
   const int* cnt = b->d_counts;
   const List* L = b->lists;
   int64_t n = 0;
+  // The order in which CTAs take list entries (runs of consecutive tiles).
+  const TileRuns R{b->tuning.tile_chunk > 0 ? b->tuning.tile_chunk : kDefaultTileChunk};
+  const TileRuns RF{b->tuning.fused_chunk > 0 ? b->tuning.fused_chunk : kDefaultFusedChunk};
   // LevelRelax of depth d for every running problem; dir selects the fused
   // stage's buffers (0: q -> qb before the correction, 1: qb -> q after).
   auto relax = [&](int d, int dir) {
@@ -583,9 +624,11 @@ void tick_t(bsam_batch* b, cudaGraphConditionalHandle handle, int in_graph) {
         for (int color = 0; color < 2; ++color) {
           const int g = grid_for(b, L_RELAX + d);
           if (b->mixed)
-            kb_relax<float, D><<<g, blk, 0, s>>>(pt, L[L_RELAX + d].d, cnt + L_RELAX + d, color);
+            kb_relax<float, D><<<g, blk, 0, s>>>(pt, L[L_RELAX + d].d, cnt + L_RELAX + d, color,
+                                                 R);
           else
-            kb_relax<double, D><<<g, blk, 0, s>>>(pt, L[L_RELAX + d].d, cnt + L_RELAX + d, color);
+            kb_relax<double, D><<<g, blk, 0, s>>>(pt, L[L_RELAX + d].d, cnt + L_RELAX + d, color,
+                                                  R);
           ++n;
         }
     if (D == 2 && L[L_FUSED + d].cap > 0) {
@@ -605,14 +648,14 @@ void tick_t(bsam_batch* b, cudaGraphConditionalHandle handle, int in_graph) {
                             : kb_smooth2<float, true, 4>;
         k<<<g, Fused2<float>::THREADS, nbuf * Fused2<float>::smem(true), s>>>(
             pt, L[L_FUSED + d].d, cnt + L_FUSED + d, dir, nu, upd, dir, 1 - dir,
-            &b->d_ctl->kerr);
+            &b->d_ctl->kerr, RF);
       } else {
         auto k = occ == 2   ? kb_smooth2<double, false, 2, 2>
                  : occ == 3 ? kb_smooth2<double, false, 3>
                             : kb_smooth2<double, false, 4>;
         k<<<g, Fused2<double>::THREADS, nbuf * Fused2<double>::smem(false), s>>>(
             pt, L[L_FUSED + d].d, cnt + L_FUSED + d, dir, nu, 0, dir, 1 - dir,
-            &b->d_ctl->kerr);
+            &b->d_ctl->kerr, RF);
       }
       ++n;
     }
@@ -625,12 +668,12 @@ void tick_t(bsam_batch* b, cudaGraphConditionalHandle handle, int in_graph) {
     if (D == 2)
       kb_defect_tma<2><<<gm, blk, Defect2::SMEM, s>>>(pt, L[L_MASTER].d, cnt + L_MASTER,
                                                       b->d_partials, newstep_only,
-                                                      &b->d_ctl->kerr);
+                                                      &b->d_ctl->kerr, R);
     else
       kb_defect<D><<<gm, blk, 0, s>>>(pt, L[L_MASTER].d, cnt + L_MASTER, b->d_partials,
-                                      newstep_only);
+                                      newstep_only, R);
   };
-  kb_source<D><<<gm, blk, 0, s>>>(pt, L[L_MASTER].d, cnt + L_MASTER);
+  kb_source<D><<<gm, blk, 0, s>>>(pt, L[L_MASTER].d, cnt + L_MASTER, R);
   ++n;
   if (b->mixed) {
     launch_defect(1);
@@ -642,15 +685,17 @@ void tick_t(bsam_batch* b, cudaGraphConditionalHandle handle, int in_graph) {
     if (L[L_RESTR + d].cap > 0) {
       const int gr = grid_for(b, L_RESTR + d);
       if (b->mixed)
-        kb_restrict<float, D><<<gr, blk, 0, s>>>(pt, L[L_RESTR + d].d, cnt + L_RESTR + d);
+        kb_restrict<float, D><<<gr, blk, 0, s>>>(pt, L[L_RESTR + d].d, cnt + L_RESTR + d, R);
       else
-        kb_restrict<double, D><<<gr, blk, 0, s>>>(pt, L[L_RESTR + d].d, cnt + L_RESTR + d);
+        kb_restrict<double, D><<<gr, blk, 0, s>>>(pt, L[L_RESTR + d].d, cnt + L_RESTR + d, R);
       ++n;
     }
     if (b->mixed)
-      kb_coarse_load<float, D><<<gc, blk, 0, s>>>(pt, L[L_COARSE + d].d, cnt + L_COARSE + d);
+      kb_coarse_load<float, D><<<gc, blk, 0, s>>>(pt, L[L_COARSE + d].d, cnt + L_COARSE + d,
+                                                  R);
     else
-      kb_coarse_load<double, D><<<gc, blk, 0, s>>>(pt, L[L_COARSE + d].d, cnt + L_COARSE + d);
+      kb_coarse_load<double, D><<<gc, blk, 0, s>>>(pt, L[L_COARSE + d].d, cnt + L_COARSE + d,
+                                                   R);
     ++n;
   }
   {
@@ -664,25 +709,29 @@ void tick_t(bsam_batch* b, cudaGraphConditionalHandle handle, int in_graph) {
       // Records with fused stages are corrected by their post-smoothing stage.
       if (L[L_CORR + d].cap > 0) {
         const int gk = grid_for(b, L_CORR + d);
-        if (b->mixed) kb_correct2<float><<<gk, blk, 0, s>>>(pt, L[L_CORR + d].d, cnt + L_CORR + d);
-        else kb_correct2<double><<<gk, blk, 0, s>>>(pt, L[L_CORR + d].d, cnt + L_CORR + d);
+        if (b->mixed)
+          kb_correct2<float><<<gk, blk, 0, s>>>(pt, L[L_CORR + d].d, cnt + L_CORR + d, R);
+        else
+          kb_correct2<double><<<gk, blk, 0, s>>>(pt, L[L_CORR + d].d, cnt + L_CORR + d, R);
       } else {
         --n;
       }
     } else {
       const int gf = grid_for(b, L_FINE + d);
-      if (b->mixed) kb_correct<float, D><<<gf, blk, 0, s>>>(pt, L[L_FINE + d].d, cnt + L_FINE + d);
-      else kb_correct<double, D><<<gf, blk, 0, s>>>(pt, L[L_FINE + d].d, cnt + L_FINE + d);
+      if (b->mixed)
+        kb_correct<float, D><<<gf, blk, 0, s>>>(pt, L[L_FINE + d].d, cnt + L_FINE + d, R);
+      else
+        kb_correct<double, D><<<gf, blk, 0, s>>>(pt, L[L_FINE + d].d, cnt + L_FINE + d, R);
     }
     ++n;
     relax(d, 1);
   }
   if (b->mixed) {
-    kb_update<D><<<grid_for(b, L_UPD), blk, 0, s>>>(pt, L[L_UPD].d, cnt + L_UPD);
+    kb_update<D><<<grid_for(b, L_UPD), blk, 0, s>>>(pt, L[L_UPD].d, cnt + L_UPD, R);
     launch_defect(0);
     n += 2;
   } else {
-    kb_resid<D><<<gm, blk, 0, s>>>(pt, L[L_MASTER].d, cnt + L_MASTER, b->d_partials);
+    kb_resid<D><<<gm, blk, 0, s>>>(pt, L[L_MASTER].d, cnt + L_MASTER, b->d_partials, R);
     ++n;
   }
   const int gctl = std::max(1, std::min(b->bp.max_slots, 2 * b->nsm));
@@ -829,6 +878,9 @@ int bsam_batch_create(bsam_batch** out, int device, const bsam_batch_params* p) 
   }
   pool = (size_t)roundup((int64_t)pool, 4096);
   bool ok = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaStreamCreateWithFlags(&b->xstream, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaEventCreateWithFlags(&b->xin_ready, cudaEventDisableTiming) == cudaSuccess &&
+            cudaEventCreateWithFlags(&b->xin_free, cudaEventDisableTiming) == cudaSuccess &&
             cudaMalloc(&b->d_pool, pool) == cudaSuccess &&
             cudaMalloc(&b->d_pt, sizeof(DevPatch) * ns * RMAX) == cudaSuccess &&
             cudaMalloc(&b->d_tmaps, sizeof(CUtensorMap) * NMAPS * ns * RMAX) == cudaSuccess &&
@@ -903,6 +955,12 @@ int bsam_batch_destroy(bsam_batch* b) {
                        b->free_events.end());
   for (auto e : b->free_events) cudaEventDestroy(e);
   if (b->stage) cudaFreeHost(b->stage);
+  if (b->xstream) cudaStreamSynchronize(b->xstream);
+  if (b->d_xin) cudaFree(b->d_xin);
+  if (b->d_xout) cudaFree(b->d_xout);
+  if (b->xin_ready) cudaEventDestroy(b->xin_ready);
+  if (b->xin_free) cudaEventDestroy(b->xin_free);
+  if (b->xstream) cudaStreamDestroy(b->xstream);
   if (b->d_partials) cudaFree(b->d_partials);
   if (b->d_counts) cudaFree(b->d_counts);
   if (b->h_status) cudaFreeHost(b->h_status);
@@ -923,7 +981,8 @@ int bsam_batch_destroy(bsam_batch* b) {
 int bsam_batch_set_tuning(bsam_batch* b, const bsam_batch_tuning* t) {
   if (!b || !t || t->grid_ctas < 0 || t->eager < 0 || t->eager > 1 || t->per_pass < 0 ||
       t->per_pass > 1 || t->fused_ctas < 0 ||
-      (t->fused_occ != 0 && (t->fused_occ < 2 || t->fused_occ > 4)))
+      (t->fused_occ != 0 && (t->fused_occ < 2 || t->fused_occ > 4)) || t->tile_chunk < 0 ||
+      t->tile_chunk > 64 || t->fused_chunk < 0 || t->fused_chunk > 64)
     return BSAM_ERR_ARG;
   b->tuning = *t;
   b->need_capture = true;
@@ -1078,13 +1137,20 @@ static int admit_many(bsam_batch* b, int n, const bsam_batch_problem* probs,
   if (!b || n < 0 || (n > 0 && (!probs || !slots)) || (!q0s && !inits)) return BSAM_ERR_ARG;
   if (n == 0) return 0;
   CU(cudaSetDevice(b->device));
-  // Every problem is checked before any is admitted.
+  // Every problem is checked before any is admitted, and the transfer
+  // buffer is sized for all of them before any slot is taken.
+  size_t xwords = 0;
   for (int k = 0; k < n; ++k) {
     SlotPlan probe;
     const int rc = plan_slot(b, &probs[k], 0, nullptr, probe);
     if (rc) return rc;
     if (q0s && !q0s[k]) return fail(b, BSAM_ERR_ARG, "a q0 pointer is NULL");
+    const DevPatch& M = probe.recs[probe.master];
+    xwords += 2 * (size_t)(M.n[0] + 2) * (M.n[1] + 2) * (b->bp.ndims == 3 ? M.n[2] + 2 : 1);
   }
+  double* xfer = nullptr;
+  if (q0s && !(xfer = xfer_reserve(b, &b->d_xin, &b->xin_words, xwords)))
+    return fail(b, BSAM_ERR_NOMEM, "transfer buffer allocation failed");
   std::vector<int> adm;
   for (int k = 0; k < n; ++k) slots[k] = -1;
   // Admission stops at the first problem that does not fit: the admitted
@@ -1119,11 +1185,19 @@ static int admit_many(bsam_batch* b, int n, const bsam_batch_problem* probs,
   static_assert(sizeof(DevPatch) % 8 == 0 && sizeof(SlotState) % 8 == 0 &&
                     sizeof(CUtensorMap) % 8 == 0,
                 "staged records are copied as 8-byte words");
-  const size_t bytes = sizeof(WordSpan) * nspan + sizeof(ZeroSpan) * na +
-                       sizeof(SeedTask) * na + sizeof(int) * (na + 1) + 8 * words + 64;
+  // Packed root states of the q0s in the device transfer buffer.
+  std::vector<size_t> xo((size_t)na + 1, 0);
+  for (int a = 0; a < na; ++a) {
+    const DevPatch& M = b->slots[adm[a]].recs[b->slots[adm[a]].master];
+    xo[a + 1] = xo[a] + 2 * (size_t)(M.n[0] + 2) * (M.n[1] + 2) * (nd == 3 ? M.n[2] + 2 : 1);
+  }
+  const size_t bytes = sizeof(RowsTask) * na + sizeof(WordSpan) * nspan +
+                       sizeof(ZeroSpan) * na + sizeof(SeedTask) * na + sizeof(int) * (na + 1) +
+                       8 * words + 64;
   char* st = stage_alloc(b, bytes);
   if (!st) return fail(b, BSAM_ERR_NOMEM, "pinned staging allocation failed");
-  WordSpan* spans = reinterpret_cast<WordSpan*>(st);
+  RowsTask* rows = reinterpret_cast<RowsTask*>(st);
+  WordSpan* spans = reinterpret_cast<WordSpan*>(rows + na);
   ZeroSpan* zs = reinterpret_cast<ZeroSpan*>(spans + nspan);
   SeedTask* tasks = reinterpret_cast<SeedTask*>(zs + na);
   int* masters = reinterpret_cast<int*>(tasks + na);
@@ -1164,17 +1238,28 @@ static int admit_many(bsam_batch* b, int n, const bsam_batch_problem* probs,
     if (nd == 2) k_init_seeded_list<2><<<dim3(gx(maxc), na), 256, 0, b->stream>>>(b->d_pt, tasks);
     else k_init_seeded_list<3><<<dim3(gx(maxc), na), 256, 0, b->stream>>>(b->d_pt, tasks);
   } else {
-    // q0s: read by the copies queued here (page-locked memory asynchronously).
+    // q0s: one contiguous copy per problem into the transfer buffer, on the
+    // copy stream (read asynchronously from page-locked memory, alongside
+    // the ticks already queued), then one launch on the engine's stream
+    // spreads the rows into the pitched fields.
+    CU(cudaStreamWaitEvent(b->xstream, b->xin_free, 0));
+    int64_t maxr = 0;
     for (int a = 0; a < na; ++a) {
       const SlotPlan& S = b->slots[adm[a]];
       const DevPatch& M = S.recs[S.master];
-      const int e0 = M.n[0] + 2, e1 = M.n[1] + 2, e2 = nd == 3 ? M.n[2] + 2 : 1;
-      const size_t hcomp = (size_t)e0 * e1 * e2;
-      for (int c = 0; c < 2; ++c)
-        CU(cudaMemcpy2DAsync(M.q[c], M.sy * sizeof(double), q0s[a] + c * hcomp,
-                             e0 * sizeof(double), e0 * sizeof(double), (size_t)e1 * e2,
-                             cudaMemcpyHostToDevice, b->stream));
+      const int e0 = M.n[0] + 2;
+      const int64_t nrow = (int64_t)(M.n[1] + 2) * (nd == 3 ? M.n[2] + 2 : 1);
+      rows[a] = RowsTask{xfer + xo[a], {static_cast<double*>(M.q[0]), static_cast<double*>(M.q[1])},
+                         nrow, M.sy, e0, 0};
+      maxr = std::max(maxr, 2 * nrow);
+      CU(cudaMemcpyAsync(xfer + xo[a], q0s[a], sizeof(double) * (xo[a + 1] - xo[a]),
+                         cudaMemcpyHostToDevice, b->xstream));
     }
+    CU(cudaEventRecord(b->xin_ready, b->xstream));
+    CU(cudaStreamWaitEvent(b->stream, b->xin_ready, 0));
+    const unsigned gr = (unsigned)std::max<int64_t>(1, std::min<int64_t>((maxr + 7) / 8, 64));
+    k_rows_list<true><<<dim3(gr, na), 256, 0, b->stream>>>(rows);
+    CU(cudaEventRecord(b->xin_free, b->stream));
   }
   if (nd == 2) k_setbc_list<double, 2><<<dim3(gx(maxc), na), 256, 0, b->stream>>>(b->d_pt, masters);
   else k_setbc_list<double, 3><<<dim3(gx(maxc), na), 256, 0, b->stream>>>(b->d_pt, masters);
@@ -1442,11 +1527,28 @@ int bsam_batch_collect_many(bsam_batch* b, int n, const int* slots, double* cons
   const int nd = b->bp.ndims;
   // Step logs: one launch writes every slot's log into page-locked staging;
   // masses: the per-slot reduction, each total copied into staging.
-  char* st = stage_alloc(b, sizeof(WordSpan) * n +
+  // Root states wanted: packed into the transfer buffer by one launch, then
+  // one contiguous copy per problem into the caller's buffer.
+  std::vector<size_t> xo((size_t)n + 1, 0);
+  int nq = 0;
+  for (int k = 0; k < n; ++k) {
+    const SlotPlan& S = b->slots[slots[k]];
+    const DevPatch& M = S.recs[S.master];
+    const size_t w = (qs && qs[k])
+                         ? 2 * (size_t)(M.n[0] + 2) * (M.n[1] + 2) * (nd == 3 ? M.n[2] + 2 : 1)
+                         : 0;
+    nq += w ? 1 : 0;
+    xo[k + 1] = xo[k] + w;
+  }
+  double* xfer = nullptr;
+  if (nq && !(xfer = xfer_reserve(b, &b->d_xout, &b->xout_words, xo[n])))
+    return fail(b, BSAM_ERR_NOMEM, "transfer buffer allocation failed");
+  char* st = stage_alloc(b, sizeof(RowsTask) * n + sizeof(WordSpan) * n +
                                 sizeof(StepLog) * BSAM_BATCH_MAX_STEPS * n +
                                 sizeof(DevStatus) * n + 64);
   if (!st) return fail(b, BSAM_ERR_NOMEM, "pinned staging allocation failed");
-  WordSpan* spans = reinterpret_cast<WordSpan*>(st);
+  RowsTask* rows = reinterpret_cast<RowsTask*>(st);
+  WordSpan* spans = reinterpret_cast<WordSpan*>(rows + n);
   StepLog* logs = reinterpret_cast<StepLog*>(spans + n);
   DevStatus* stat = reinterpret_cast<DevStatus*>(logs + (size_t)BSAM_BATCH_MAX_STEPS * n);
   int64_t maxw = 1;
@@ -1459,17 +1561,30 @@ int bsam_batch_collect_many(bsam_batch* b, int n, const int* slots, double* cons
     maxw = std::max(maxw, nw);
   }
   k_word_spans<<<dim3((unsigned)((maxw + 255) / 256), n), 256, 0, b->stream>>>(spans);
+  if (nq) {
+    int nt = 0;
+    int64_t maxr = 0;
+    std::vector<int> which;
+    which.reserve(nq);
+    for (int k = 0; k < n; ++k) {
+      if (xo[k + 1] == xo[k]) continue;
+      const SlotPlan& S = b->slots[slots[k]];
+      const DevPatch& M = S.recs[S.master];
+      const int64_t nrow = (int64_t)(M.n[1] + 2) * (nd == 3 ? M.n[2] + 2 : 1);
+      rows[nt++] = RowsTask{xfer + xo[k], {static_cast<double*>(M.q[0]), static_cast<double*>(M.q[1])},
+                            nrow, M.sy, M.n[0] + 2, 0};
+      maxr = std::max(maxr, 2 * nrow);
+      which.push_back(k);
+    }
+    const unsigned gr = (unsigned)std::max<int64_t>(1, std::min<int64_t>((maxr + 7) / 8, 64));
+    k_rows_list<false><<<dim3(gr, nt), 256, 0, b->stream>>>(rows);
+    for (int k : which)
+      CU(cudaMemcpyAsync(qs[k], xfer + xo[k], sizeof(double) * (xo[k + 1] - xo[k]),
+                         cudaMemcpyDeviceToHost, b->stream));
+  }
   for (int k = 0; k < n; ++k) {
     const SlotPlan& S = b->slots[slots[k]];
     const DevPatch& M = S.recs[S.master];
-    if (qs && qs[k]) {
-      const int e0 = M.n[0] + 2, e1 = M.n[1] + 2, e2 = nd == 3 ? M.n[2] + 2 : 1;
-      const size_t hcomp = (size_t)e0 * e1 * e2;
-      for (int c = 0; c < 2; ++c)
-        CU(cudaMemcpy2DAsync(qs[k] + c * hcomp, e0 * sizeof(double), M.q[c],
-                             M.sy * sizeof(double), e0 * sizeof(double), (size_t)e1 * e2,
-                             cudaMemcpyDeviceToHost, b->stream));
-    }
     if (masses) {
       const SlotCfg& C = b->h_cfg[slots[k]];
       const double hh = M.h;

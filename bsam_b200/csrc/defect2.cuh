@@ -38,7 +38,7 @@ template <int D>
 __global__ void __launch_bounds__(BLOCK_THREADS, 8)
     kb_defect_tma(const DevPatch* __restrict__ PT, const Item* __restrict__ items,
                   const int* __restrict__ count, double* __restrict__ partials, int newstep_only,
-                  int* __restrict__ err) {
+                  int* __restrict__ err, TileRuns R) {
   static_assert(D == 2, "2D masters only");
   using F = Defect2;
   extern __shared__ __align__(1024) unsigned char def_raw[];
@@ -57,7 +57,7 @@ __global__ void __launch_bounds__(BLOCK_THREADS, 8)
   };
   // The CTA's next tile at or after list position `from` that takes part.
   auto next_tile = [&](int from) {
-    for (int x = from; x < n; x += gridDim.x) {
+    for (int x = from; x < n; x = R.next(x)) {
       const DevPatch& M = PT[items[x].patch];
       if (M.active && !(newstep_only && !M.newstep)) return x;
     }
@@ -78,12 +78,12 @@ __global__ void __launch_bounds__(BLOCK_THREADS, 8)
     tma_load_2d(plane(buf, 3), &maps[3], lead + i0, j0, &bar[buf]);
   };
   uint32_t phase[2] = {0u, 0u};
-  int cur = next_tile(blockIdx.x), buf = 0;
+  int cur = next_tile(R.first()), buf = 0;
   if (cur < n && tid == 0) issue(cur, 0);
   while (cur < n) {
     // Buffer buf ^ 1 was last read by the previous tile, which ended with a
     // barrier (block_sum).
-    const int nxt = next_tile(cur + gridDim.x);
+    const int nxt = next_tile(R.next(cur));
     if (nxt < n && tid == 0) issue(nxt, buf ^ 1);
     bool ok = true;
     if (tid == 0) ok = mbar_wait_backoff(&bar[buf], phase[buf], kWaitPolls);

@@ -464,7 +464,7 @@ template <class T, bool DELTA, int MINB = 4, int NBUF = 1>
 __global__ void __launch_bounds__(Fused2<T>::THREADS, MINB)
     kb_smooth2(const DevPatch* __restrict__ PT, const Item* __restrict__ items,
                const int* __restrict__ count, int dir, int nu, int upd, int corr,
-               int restr, int* __restrict__ err) {
+               int restr, int* __restrict__ err, TileRuns R) {
   using F = Fused2<T>;
   static_assert(NBUF == 1 || NBUF == 2, "one or two tile buffers");
   constexpr int NPL = DELTA ? 5 : 4;  // planes per buffer
@@ -488,7 +488,7 @@ __global__ void __launch_bounds__(Fused2<T>::THREADS, MINB)
   auto zero_start_of = [&](const DevPatch& P) { return DELTA && dir == 0 && P.master >= 0; };
   // The CTA's next tile at or after list position `from` whose patch runs.
   auto next_tile = [&](int from) {
-    for (int x = from; x < n; x += gridDim.x)
+    for (int x = from; x < n; x = R.next(x))
       if (PT[items[x].patch].active) return x;
     return n;
   };
@@ -515,10 +515,10 @@ __global__ void __launch_bounds__(Fused2<T>::THREADS, MINB)
   };
   uint32_t phase[NBUF];
   for (int k = 0; k < NBUF; ++k) phase[k] = 0u;
-  int cur = next_tile(blockIdx.x), buf = 0;
+  int cur = next_tile(R.first()), buf = 0;
   if (cur < n && tid == 0) issue(cur, 0);
   while (cur < n) {
-    const int nxt = next_tile(cur + gridDim.x);
+    const int nxt = next_tile(R.next(cur));
     // Two buffers: the next tile's copies go into the other one, last read
     // by the previous tile (which ended with a barrier).
     if (NBUF == 2 && nxt < n && tid == 0) issue(nxt, buf ^ 1);

@@ -23,6 +23,21 @@ namespace bsam {
 
 template <class T> __device__ __forceinline__ T* fld(void* p) { return static_cast<T*>(p); }
 
+// The entries of an n-long work list a CTA takes: runs of `chunk`
+// consecutive entries, run r going to CTA r mod gridDim.x (chunk 1 is the
+// plain grid-stride order).  A list holds each problem's tiles in a row, so
+// the tiles of a run mostly share their patch records, which after the
+// run's first tile come from L1 instead of a chain of L2 round trips; the
+// order in which a CTA visits tiles changes no result.
+struct TileRuns {
+  int chunk;
+  __device__ __forceinline__ int first() const { return (int)blockIdx.x * chunk; }
+  __device__ __forceinline__ int next(int x) const {
+    ++x;
+    return (x % chunk) != 0 ? x : x + (int)(gridDim.x - 1) * chunk;
+  }
+};
+
 // The pre-smoothed state of a level: the second buffer when the level's
 // stages run the fused kernel (q -> qb -> q), else q itself.
 __device__ __forceinline__ void* const* mid_state(const DevPatch& P) {

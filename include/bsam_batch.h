@@ -83,14 +83,21 @@ typedef struct {
  * fused_occ picks the fused stage's build: 3 or 4 resident CTAs per SM with
  * one tile buffer each (a register budget of 85 or 64 per thread), or 2: two
  * CTAs per SM with two tile buffers each, the next tile's copies landing
- * while the current one is computed (0 = 4). */
+ * while the current one is computed (0 = 4); tile_chunk and fused_chunk
+ * set how a launch's CTAs take the tiles of their work list: runs of that
+ * many consecutive tiles, run r to CTA r mod the grid (1 = grid-stride;
+ * consecutive tiles mostly share their problem's records, which a run then
+ * reads from L1), for the small-tile list kernels (0 = 4) and for the fused
+ * stages (0 = 1). */
 typedef struct {
   int32_t grid_ctas;
   int32_t eager;
   int32_t per_pass;
   int32_t fused_ctas;
   int32_t fused_occ;
-  int32_t reserved[3];
+  int32_t tile_chunk;
+  int32_t fused_chunk;
+  int32_t reserved;
 } bsam_batch_tuning;
 
 typedef struct {

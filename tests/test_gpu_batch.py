@@ -210,3 +210,30 @@ def test_submit_many_and_collect_many_match_single_calls(gpu_lib):
         got = bt.collect_many(slots[:3])
     for r, g in zip(ref[:3], got):
         assert np.array_equal(r["q"], g["q"])
+
+
+@pytest.mark.parametrize("nd", [2, 3])
+def test_submit_many_from_host_while_a_batch_runs(gpu_lib, nd):
+    # Host q0s go through the engine's transfer buffer (one contiguous copy
+    # per problem, rows spread into the pitched fields on the device) and
+    # results come back the same way, ghost rings included; a second group
+    # submitted while the first solves, and the first collected before the
+    # second runs, give the bits of one-at-a-time solves.
+    sides = [64, 96, 128, 48] if nd == 2 else [16, 24, 32, 20]
+    probs = [W.seeded(nd, n, 0.02 if nd == 3 else 0.01, 2, seed=700 + i, cbar=0.5, amp=0.025)
+             for i, n in enumerate(sides)]
+    ref = BB.solve_all(probs, precision=BB.PREC_MIXED)
+    q0s = [p.q0() for p in probs]
+    with BB.Batch(nd, precision=BB.PREC_MIXED, max_slots=2 * len(probs)) as bt:
+        a = bt.submit_many(probs, q0s)
+        bt.advance(1 << 20)
+        b = bt.submit_many(probs[::-1], q0s[::-1])
+        outs = [np.zeros(q.shape, order="F") for q in q0s]
+        got_a = bt.collect_many(a, outs=outs)
+        bt.run()
+        got_b = bt.collect_many(b)[::-1]
+    for r, g, g2, o in zip(ref, got_a, got_b, outs):
+        for k in ("q", "nvcycles", "residual", "converged"):
+            assert np.array_equal(r[k], g[k]), k
+            assert np.array_equal(r[k], g2[k]), k
+        assert g["q"] is o

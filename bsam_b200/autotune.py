@@ -64,9 +64,9 @@ def candidates(knob: str, nsm: int) -> list:
     if knob == "grid_ctas":
         return [0, 4 * nsm, 8 * nsm, 32 * nsm]
     if knob == "tile_chunk":
-        return [0, 1, 2, 8]
+        return [0, 1, 4]
     if knob == "fused_chunk":
-        return [0, 2, 4]
+        return [0, 2]
     raise ValueError(knob)
 
 

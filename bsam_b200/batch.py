@@ -255,9 +255,12 @@ class Batch:
         return out
 
     def collect_many(self, slots, want_q: bool = True, outs=None, want_mass: bool = False):
-        """collect() of many finished slots with one wait; returns their
-        results in order.  outs: per slot a Fortran-ordered float64 array of
-        q's shape to copy into (page-locked ones are reached at full speed)."""
+        """collect() of many slots with one wait; returns their results in
+        order.  The slots must be finished or finish with the work already
+        queued; without want_mass only they are waited for, so ticks advanced
+        since keep running while their results are copied out.  outs: per
+        slot a Fortran-ordered float64 array of q's shape to copy into
+        (page-locked ones are reached at full speed)."""
         n = len(slots)
         if n == 0:
             return []

@@ -26,11 +26,13 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <deque>
 #include <map>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/bsam_batch.h"
@@ -52,7 +54,7 @@ constexpr int DEFAULT_BOTTOM_CELLS = 1024;
 // Default runs of consecutive list entries per CTA visit (TileRuns) for the
 // small-tile list kernels and for the fused stages (tuning.tile_chunk and
 // tuning.fused_chunk; 1 = grid-stride order).
-constexpr int kDefaultTileChunk = 4;
+constexpr int kDefaultTileChunk = 2;
 constexpr int kDefaultFusedChunk = 1;
 // Lists: master tiles; bottom-chain tops; per top depth d: tiles of every
 // record (correction), footprint tiles (restriction / coarse load), tiles of
@@ -235,12 +237,12 @@ cudaEvent_t take_event(bsam_batch* b) {
   return e;
 }
 
-// Marks every chunk staged since the last call as done once the copies
-// queued so far have executed.
-void stage_commit(bsam_batch* b) {
+// Marks every chunk staged since the last call as done once the work queued
+// so far on `st` (the engine's stream by default) has executed.
+void stage_commit(bsam_batch* b, cudaStream_t st = nullptr) {
   if (b->pending.empty()) return;
   cudaEvent_t e = take_event(b);
-  cudaEventRecord(e, b->stream);
+  cudaEventRecord(e, st ? st : b->stream);
   for (size_t i : b->pending) b->chunks[i].ev = e;
   b->pending.clear();
 }
@@ -1514,16 +1516,39 @@ int bsam_batch_collect_many(bsam_batch* b, int n, const int* slots, double* cons
   if (!b || n < 0 || (n > 0 && !slots)) return BSAM_ERR_ARG;
   if (n == 0) return BSAM_OK;
   CU(cudaSetDevice(b->device));
-  CU(cudaStreamSynchronize(b->stream));
   for (int k = 0; k < n; ++k) {
     const int s = slots[k];
     if (s < 0 || s >= (int)b->slots.size() || !b->slots[s].used)
       return fail(b, BSAM_ERR_ARG, "slot not resident");
     for (int k2 = 0; k2 < k; ++k2)
       if (slots[k2] == s) return fail(b, BSAM_ERR_ARG, "slot listed twice");
-    const int ph = ((volatile SlotOut*)b->h_out)[s].phase;
-    if (ph != SLOT_DONE && ph != SLOT_FAILED) return fail(b, BSAM_ERR_STATE, "problem not finished");
   }
+  auto finished = [&]() {
+    for (int k = 0; k < n; ++k) {
+      const int ph = ((volatile SlotOut*)b->h_out)[slots[k]].phase;
+      if (ph != SLOT_DONE && ph != SLOT_FAILED) return false;
+    }
+    return true;
+  };
+  // Without masses the read-back waits only for these slots to finish (their
+  // phase in mapped host memory, written after everything else the control
+  // kernel stores for them) and runs on the copy stream, beside any ticks
+  // queued since.  The mass reduction shares the engine's partials with the
+  // ticks, so with masses every queued tick is waited for first.
+  const bool side = masses == nullptr;
+  if (side) {
+    while (!finished()) {
+      const cudaError_t q = cudaStreamQuery(b->stream);
+      if (q != cudaSuccess && q != cudaErrorNotReady)
+        return fail(b, BSAM_ERR_CUDA, std::string("stream query: ") + cudaGetErrorString(q));
+      if (q == cudaSuccess && !finished()) break;  // idle engine: the check below fails
+      std::this_thread::sleep_for(std::chrono::microseconds(20));
+    }
+  } else {
+    CU(cudaStreamSynchronize(b->stream));
+  }
+  if (!finished()) return fail(b, BSAM_ERR_STATE, "problem not finished");
+  cudaStream_t cs = side ? b->xstream : b->stream;
   const int nd = b->bp.ndims;
   // Step logs: one launch writes every slot's log into page-locked staging;
   // masses: the per-slot reduction, each total copied into staging.
@@ -1560,7 +1585,7 @@ int bsam_batch_collect_many(bsam_batch* b, int n, const int* slots, double* cons
                         reinterpret_cast<uint64_t*>(logs + (size_t)k * BSAM_BATCH_MAX_STEPS), nw};
     maxw = std::max(maxw, nw);
   }
-  k_word_spans<<<dim3((unsigned)((maxw + 255) / 256), n), 256, 0, b->stream>>>(spans);
+  k_word_spans<<<dim3((unsigned)((maxw + 255) / 256), n), 256, 0, cs>>>(spans);
   if (nq) {
     int nt = 0;
     int64_t maxr = 0;
@@ -1577,10 +1602,10 @@ int bsam_batch_collect_many(bsam_batch* b, int n, const int* slots, double* cons
       which.push_back(k);
     }
     const unsigned gr = (unsigned)std::max<int64_t>(1, std::min<int64_t>((maxr + 7) / 8, 64));
-    k_rows_list<false><<<dim3(gr, nt), 256, 0, b->stream>>>(rows);
+    k_rows_list<false><<<dim3(gr, nt), 256, 0, cs>>>(rows);
     for (int k : which)
       CU(cudaMemcpyAsync(qs[k], xfer + xo[k], sizeof(double) * (xo[k + 1] - xo[k]),
-                         cudaMemcpyDeviceToHost, b->stream));
+                         cudaMemcpyDeviceToHost, cs));
   }
   for (int k = 0; k < n; ++k) {
     const SlotPlan& S = b->slots[slots[k]];
@@ -1602,8 +1627,8 @@ int bsam_batch_collect_many(bsam_batch* b, int n, const int* slots, double* cons
     }
   }
   CU(cudaGetLastError());
-  stage_commit(b);
-  CU(cudaStreamSynchronize(b->stream));
+  stage_commit(b, cs);
+  CU(cudaStreamSynchronize(cs));
   int rc = BSAM_OK;
   for (int k = 0; k < n; ++k) {
     const int s = slots[k];

@@ -57,6 +57,24 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const void* tmap, int x, 
       : "memory");
 }
 
+// Asks L2 for the 128-byte lines of a block of rows of `nf` fields (rows
+// j0 .. j0 + nj - 1, columns i0 .. i0 + ni - 1 of values of `es` bytes, row
+// pitch sy values), one line per thread and round.  Nothing waits for them:
+// the loads that follow find the lines in L2 instead of HBM.
+__device__ __forceinline__ void prefetch_rows_l2(const void* const* f, int nf, int64_t sy, int es,
+                                                 int i0, int ni, int j0, int nj) {
+  if (ni <= 0 || nj <= 0) return;
+  const int lines = (ni * es + 127) / 128 + 1;  // the block may straddle one more line
+  const int total = nf * nj * lines;
+  for (int t = threadIdx.x; t < total; t += blockDim.x) {
+    const int l = t % lines, r = (t / lines) % nj, k = t / (lines * nj);
+    const char* row = static_cast<const char*>(f[k]) + ((int64_t)(j0 + r) * sy + i0) * es;
+    const char* p = row + 128 * l;
+    if (p >= row + (int64_t)ni * es) continue;
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+  }
+}
+
 // Bounded wait on an mbarrier phase by one thread, sleeping between polls
 // (32 ns doubling to 512 ns).  Returns false after `limit` polls.
 __device__ __forceinline__ bool mbar_wait_backoff(uint64_t* b, uint32_t parity, uint32_t limit) {
@@ -531,6 +549,24 @@ __global__ void __launch_bounds__(Fused2<T>::THREADS, MINB)
     const DevPatch P = PT[it.patch];
     const int gx0 = it.tx * F::TX + 1 - F::H;  // global i of shared column 0
     const int gy0 = it.ty * F::TY + 1 - F::H;  // global j of shared row 0
+    // While the tile's copies land, ask L2 for what the tile reads from HBM
+    // besides them: the parent cells of its coarse-grid correction and the
+    // FP64 master rows of its update.
+    if (corr && P.parent >= 0) {
+      const DevPatch& R = PT[P.parent];
+      const int ma = max((gx0 >= 0 ? gx0 : gx0 - 1) / 2, 0);
+      const int na = max((gy0 >= 0 ? gy0 : gy0 - 1) / 2, 0);
+      const int mb = min((gx0 + F::RX - 1) / 2, P.cn[0]), nb = min((gy0 + F::RY - 1) / 2, P.cn[1]);
+      const void* f[4] = {R.q[0], R.q[1], R.qs[0], R.qs[1]};
+      prefetch_rows_l2(f, 4, R.sy, P.pprec == PREC_F32 ? 4 : 8, P.off[0] + ma, mb + 2 - ma,
+                       P.off[1] + na, nb + 2 - na);
+    }
+    if (upd && P.master >= 0) {
+      const DevPatch& M = PT[P.master];
+      const void* f[2] = {M.q[0], M.q[1]};
+      prefetch_rows_l2(f, 2, M.sy, 8, gx0 + F::H, min(F::TX, M.n[0] - (gx0 + F::H) + 1),
+                       gy0 + F::H, min(F::TY, M.n[1] - (gy0 + F::H) + 1));
+    }
     if (zero_start_of(P))
       for (int c = tid; c < F::PLANE; c += F::THREADS) {
         s0[c] = T(0);
@@ -612,7 +648,37 @@ __global__ void __launch_bounds__(Fused2<T>::THREADS, MINB)
       const DevPatch M = PT[P.master];
       double* m0 = fld<double>(M.q[0]);
       double* m1 = fld<double>(M.q[1]);
-      if (lx < F::TX && gi <= n0)
+      const bool inner = gx0 > 1 && gx0 + F::RX - 1 < n0 && gy0 > 1 && gy0 + F::RY - 1 < n1;
+      if (inner) {
+        // Every row and pair of the tile lies inside the patch, away from
+        // its faces: the lane loads all its master pairs before storing any,
+        // so that the loads are in flight together.
+        constexpr int KR = F::TY / F::WARPS;
+        static_assert(F::TY % F::WARPS == 0, "whole rows per warp");
+        if (lx < F::TX) {
+          double2 x0[KR], x1[KR];
+#pragma unroll
+          for (int k = 0; k < KR; ++k) {
+            const int64_t c = cidx(M, gi, gy0 + F::H + warp + k * F::WARPS, 0);
+            x0[k] = *reinterpret_cast<const double2*>(m0 + c);
+            x1[k] = *reinterpret_cast<const double2*>(m1 + c);
+          }
+#pragma unroll
+          for (int k = 0; k < KR; ++k) {
+            const int ly = warp + k * F::WARPS;
+            const int srow = (F::H + ly) * F::RX + F::H;
+            const V e0 = *reinterpret_cast<const V*>(s0 + srow + lx);
+            const V e1 = *reinterpret_cast<const V*>(s1 + srow + lx);
+            x0[k].x = x0[k].x + (double)e0.x;
+            x0[k].y = x0[k].y + (double)e0.y;
+            x1[k].x = x1[k].x + (double)e1.x;
+            x1[k].y = x1[k].y + (double)e1.y;
+            const int64_t c = cidx(M, gi, gy0 + F::H + ly, 0);
+            *reinterpret_cast<double2*>(m0 + c) = x0[k];
+            *reinterpret_cast<double2*>(m1 + c) = x1[k];
+          }
+        }
+      } else if (lx < F::TX && gi <= n0)
         for (int ly = warp; ly < F::TY; ly += F::WARPS) {
           const int j = gy0 + F::H + ly;
           if (j > n1) break;

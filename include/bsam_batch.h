@@ -87,7 +87,7 @@ typedef struct {
  * set how a launch's CTAs take the tiles of their work list: runs of that
  * many consecutive tiles, run r to CTA r mod the grid (1 = grid-stride;
  * consecutive tiles mostly share their problem's records, which a run then
- * reads from L1), for the small-tile list kernels (0 = 4) and for the fused
+ * reads from L1), for the small-tile list kernels (0 = 2) and for the fused
  * stages (0 = 1). */
 typedef struct {
   int32_t grid_ctas;
@@ -193,9 +193,12 @@ int bsam_batch_collect(bsam_batch* b, int slot, double* q, bsam_step_result* ste
 
 /* bsam_batch_collect of slots[0..n) with one wait: qs[k], steps[k] (arrays
  * of pointers, NULL entries or NULL arrays to skip) and masses[k] (NULL to
- * skip, which saves a reduction per problem).  Every slot must be finished;
- * all are released.  BSAM_ERR_DIVERGED when any of them failed.  No
- * reference counterpart. */
+ * skip, which saves a reduction per problem).  Every slot must be finished
+ * or finish with the work already queued; all are released.  Without masses
+ * the call waits only for these slots, not for ticks queued after them
+ * (bsam_batch_advance issued before the call keeps the device busy while
+ * the results are copied out); with masses it waits for all queued work.
+ * BSAM_ERR_DIVERGED when any of them failed.  No reference counterpart. */
 int bsam_batch_collect_many(bsam_batch* b, int n, const int* slots, double* const* qs,
                             bsam_step_result* const* steps, double* masses);
 

@@ -217,8 +217,8 @@ def test_submit_many_from_host_while_a_batch_runs(gpu_lib, nd):
     # Host q0s go through the engine's transfer buffer (one contiguous copy
     # per problem, rows spread into the pitched fields on the device) and
     # results come back the same way, ghost rings included; a second group
-    # submitted while the first solves, and the first collected before the
-    # second runs, give the bits of one-at-a-time solves.
+    # submitted and advanced while the first solves, and the first collected
+    # while the second solves, give the bits of one-at-a-time solves.
     sides = [64, 96, 128, 48] if nd == 2 else [16, 24, 32, 20]
     probs = [W.seeded(nd, n, 0.02 if nd == 3 else 0.01, 2, seed=700 + i, cbar=0.5, amp=0.025)
              for i, n in enumerate(sides)]
@@ -228,9 +228,9 @@ def test_submit_many_from_host_while_a_batch_runs(gpu_lib, nd):
         a = bt.submit_many(probs, q0s)
         bt.advance(1 << 20)
         b = bt.submit_many(probs[::-1], q0s[::-1])
+        bt.advance(1 << 20)
         outs = [np.zeros(q.shape, order="F") for q in q0s]
-        got_a = bt.collect_many(a, outs=outs)
-        bt.run()
+        got_a = bt.collect_many(a, outs=outs)  # while the second group solves
         got_b = bt.collect_many(b)[::-1]
     for r, g, g2, o in zip(ref, got_a, got_b, outs):
         for k in ("q", "nvcycles", "residual", "converged"):

@@ -377,7 +377,7 @@ __device__ __forceinline__ void init_seeded_range(const DevPatch& P, uint64_t se
       lap = lap + seeded_c<D>(P, seed, cbar, amp, i, j, k - 1);
     }
     const double alpha = P.alpha;
-    const double mu = problem::Dfc(c, alpha) - problem::Dfe(c, alpha) - k2 * lap;
+    const double mu = Problem::Dfc(c, alpha) - Problem::Dfe(c, alpha) - k2 * lap;
     const int64_t ci = cidx(P, i, j, k);
     fld<double>(P.q[0])[ci] = c;
     fld<double>(P.q[1])[ci] = mu;

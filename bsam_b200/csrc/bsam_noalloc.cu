@@ -82,10 +82,10 @@ __global__ void __launch_bounds__(BLOCK_THREADS)
     for (int t = 0; t < 2; ++t) {
       const int i = i0 + t;
       if (i <= P.n[0]) {
-        problem::Stencil<double, D> s;
+        Problem::Stencil<double, D> s;
         load_stencil<double, D>(P, q0, q1, cidx(P, i, j, k), s);
         double o0, o1;
-        problem::OperatorCell<double, D>(s, P.tmp1, P.tmp2, P.alpha, o0, o1);
+        Problem::OperatorCell<double, D>(s, P.tmp1, P.tmp2, P.alpha, o0, o1);
         const int64_t fc = (int64_t)(i - 1) + (int64_t)(j - 1) * fsy +
                            (int64_t)(D == 3 ? k - 1 : 0) * fsz;
         const double r0 = fbase[fc] - o0;

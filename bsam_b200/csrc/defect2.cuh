@@ -117,7 +117,7 @@ __global__ void __launch_bounds__(BLOCK_THREADS, 8)
         if (i > M.n[0]) break;
         const int sq = (i - (i0 - 2)) + (j - (j0 - 1)) * F::QX;
         const int sf = (i - i0) + (j - j0) * F::TX;
-        problem::Stencil<double, 2> s;
+        Problem::Stencil<double, 2> s;
         s.pc = sq0[sq];
         s.mc = sq1[sq];
         s.pm[0] = sq0[sq - 1];
@@ -129,7 +129,7 @@ __global__ void __launch_bounds__(BLOCK_THREADS, 8)
         s.mm[1] = sq1[sq - F::QX];
         s.mp[1] = sq1[sq + F::QX];
         double o0, o1;
-        problem::OperatorCell<double, 2>(s, M.tmp1, M.tmp2, M.alpha, o0, o1);
+        Problem::OperatorCell<double, 2>(s, M.tmp1, M.tmp2, M.alpha, o0, o1);
         const double r0 = sf0[sf] - o0, r1 = sf1[sf] - o1;
         acc += r0 * r0 + r1 * r1;
         const int64_t cw = cidx(W, i, j, 0);

@@ -23,6 +23,8 @@
 // l the columns 2l, 2l+1 of its rows (smooth_band).  TX = 56 keeps the widest
 // pass (TX + 6 cells) within the 64 columns of a warp.
 #pragma once
+#include <type_traits>
+
 #include "kernels.cuh"
 #include "smooth_fused.cuh"
 
@@ -55,24 +57,6 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const void* tmap, int x, 
       "{%2, %3}], [%4];" ::"r"(smem_u32(dst)),
       "l"(tmap), "r"(x), "r"(y), "r"(smem_u32(bar))
       : "memory");
-}
-
-// Asks L2 for the 128-byte lines of a block of rows of `nf` fields (rows
-// j0 .. j0 + nj - 1, columns i0 .. i0 + ni - 1 of values of `es` bytes, row
-// pitch sy values), one line per thread and round.  Nothing waits for them:
-// the loads that follow find the lines in L2 instead of HBM.
-__device__ __forceinline__ void prefetch_rows_l2(const void* const* f, int nf, int64_t sy, int es,
-                                                 int i0, int ni, int j0, int nj) {
-  if (ni <= 0 || nj <= 0) return;
-  const int lines = (ni * es + 127) / 128 + 1;  // the block may straddle one more line
-  const int total = nf * nj * lines;
-  for (int t = threadIdx.x; t < total; t += blockDim.x) {
-    const int l = t % lines, r = (t / lines) % nj, k = t / (lines * nj);
-    const char* row = static_cast<const char*>(f[k]) + ((int64_t)(j0 + r) * sy + i0) * es;
-    const char* p = row + 128 * l;
-    if (p >= row + (int64_t)ni * es) continue;
-    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
-  }
 }
 
 // Bounded wait on an mbarrier phase by one thread, sleeping between polls
@@ -232,7 +216,7 @@ __device__ __forceinline__ void relax_pair_f32(float2 pc, float2 pw, float2 pe, 
   const float2 b1 = fma2(K.tmp1, smu, f0);
   const float2 b2 = fma2(K.ntmp2, sph, fma2(nd2, pc, add2(f1, nl)));
   const float2 det = fma2(K.a12, na21, K.one);
-  const float2 r = make_float2(problem::rcp_approx(det.x), problem::rcp_approx(det.y));
+  const float2 r = make_float2(rcp_approx(det.x), rcp_approx(det.y));
   phi = mul2(fma2(K.na12, b2, b1), r);
   mu = mul2(fma2(na21, b1, b2), r);
 }
@@ -241,10 +225,10 @@ __device__ __forceinline__ void relax_pair_f32(float2 pc, float2 pw, float2 pe, 
 // type: FP32 as a packed pair, FP64 one cell at a time in the reference's
 // operation order.  Stencil order of a/b: pc, pw, pe, ps, pn, mw, me, ms, mn,
 // f0, f1, base.
-template <class T, bool DELTA> struct RelaxPair;
-template <bool DELTA> struct RelaxPair<float, DELTA> {
+// The FP32 pair with the Cahn-Hilliard Newton step in paired arithmetic.
+template <bool DELTA> struct RelaxPairF32 {
   RelaxK2 K;
-  __device__ __forceinline__ explicit RelaxPair(const DevPatch& P)
+  __device__ __forceinline__ explicit RelaxPairF32(const DevPatch& P)
       : K(relax_k2(float(P.tmp1), float(P.tmp2), float(P.tmp3), float(P.alpha))) {}
   __device__ __forceinline__ void operator()(const float (&a)[12], const float (&b)[12],
                                              float& pa, float& ma, float& pb, float& mb) const {
@@ -258,12 +242,13 @@ template <bool DELTA> struct RelaxPair<float, DELTA> {
     mb = mu.y;
   }
 };
-template <bool DELTA> struct RelaxPair<double, DELTA> {
-  double tmp1, tmp2, tmp3, alpha;
-  __device__ __forceinline__ explicit RelaxPair(const DevPatch& P)
-      : tmp1(P.tmp1), tmp2(P.tmp2), tmp3(P.tmp3), alpha(P.alpha) {}
-  __device__ __forceinline__ void one(const double (&a)[12], double& p, double& m) const {
-    problem::Stencil<double, 2> st;
+// Any pair cell by cell through the problem module's RelaxCell.
+template <class T, bool DELTA> struct RelaxPairScalar {
+  T tmp1, tmp2, tmp3, alpha;
+  __device__ __forceinline__ explicit RelaxPairScalar(const DevPatch& P)
+      : tmp1(T(P.tmp1)), tmp2(T(P.tmp2)), tmp3(T(P.tmp3)), alpha(T(P.alpha)) {}
+  __device__ __forceinline__ void one(const T (&a)[12], T& p, T& m) const {
+    Problem::Stencil<T, 2> st;
     st.pc = a[0];
     st.pm[0] = a[1];
     st.pp[0] = a[2];
@@ -273,19 +258,26 @@ template <bool DELTA> struct RelaxPair<double, DELTA> {
     st.mp[0] = a[6];
     st.mm[1] = a[7];
     st.mp[1] = a[8];
-    st.mc = 0.0;  // the Newton update does not read mu at the cell
+    st.mc = T(0);  // the Newton update does not read mu at the cell
     if constexpr (DELTA)
-      problem::RelaxCell<double, 2, true>(st, a[9], a[10], tmp1, tmp2, tmp3, alpha, p, m, a[11]);
+      Problem::RelaxCell<T, 2, true>(st, a[9], a[10], tmp1, tmp2, tmp3, alpha, p, m, a[11]);
     else
-      problem::RelaxCell<double, 2>(st, a[9], a[10], tmp1, tmp2, tmp3, alpha, p, m);
+      Problem::RelaxCell<T, 2>(st, a[9], a[10], tmp1, tmp2, tmp3, alpha, p, m);
   }
-  __device__ __forceinline__ void operator()(const double (&a)[12], const double (&b)[12],
-                                             double& pa, double& ma, double& pb,
-                                             double& mb) const {
+  __device__ __forceinline__ void operator()(const T (&a)[12], const T (&b)[12], T& pa, T& ma,
+                                             T& pb, T& mb) const {
     one(a, pa, ma);
     one(b, pb, mb);
   }
 };
+
+// The pair form of a level: paired FP32 arithmetic where the problem module
+// allows it (its Newton step is the one relax_pair_f32 evaluates), else cell
+// by cell.
+template <class T, bool DELTA>
+using RelaxPair =
+    typename std::conditional<std::is_same<T, float>::value && Problem::paired_f32,
+                              RelaxPairF32<DELTA>, RelaxPairScalar<T, DELTA>>::type;
 
 // One colour pass over a band of row pairs of the shared tile.  Lane l holds
 // columns 2l and 2l+1 of every row it touches, read as one vector: per row
@@ -549,24 +541,6 @@ __global__ void __launch_bounds__(Fused2<T>::THREADS, MINB)
     const DevPatch P = PT[it.patch];
     const int gx0 = it.tx * F::TX + 1 - F::H;  // global i of shared column 0
     const int gy0 = it.ty * F::TY + 1 - F::H;  // global j of shared row 0
-    // While the tile's copies land, ask L2 for what the tile reads from HBM
-    // besides them: the parent cells of its coarse-grid correction and the
-    // FP64 master rows of its update.
-    if (corr && P.parent >= 0) {
-      const DevPatch& R = PT[P.parent];
-      const int ma = max((gx0 >= 0 ? gx0 : gx0 - 1) / 2, 0);
-      const int na = max((gy0 >= 0 ? gy0 : gy0 - 1) / 2, 0);
-      const int mb = min((gx0 + F::RX - 1) / 2, P.cn[0]), nb = min((gy0 + F::RY - 1) / 2, P.cn[1]);
-      const void* f[4] = {R.q[0], R.q[1], R.qs[0], R.qs[1]};
-      prefetch_rows_l2(f, 4, R.sy, P.pprec == PREC_F32 ? 4 : 8, P.off[0] + ma, mb + 2 - ma,
-                       P.off[1] + na, nb + 2 - na);
-    }
-    if (upd && P.master >= 0) {
-      const DevPatch& M = PT[P.master];
-      const void* f[2] = {M.q[0], M.q[1]};
-      prefetch_rows_l2(f, 2, M.sy, 8, gx0 + F::H, min(F::TX, M.n[0] - (gx0 + F::H) + 1),
-                       gy0 + F::H, min(F::TY, M.n[1] - (gy0 + F::H) + 1));
-    }
     if (zero_start_of(P))
       for (int c = tid; c < F::PLANE; c += F::THREADS) {
         s0[c] = T(0);

@@ -17,7 +17,7 @@
 // applied to the interior cell reflected across all of S.
 #pragma once
 #include "bsam_types.h"
-#include "problem_ch.cuh"
+#include "problem.cuh"
 
 namespace bsam {
 
@@ -118,7 +118,7 @@ __device__ __forceinline__ void write_through(const DevPatch& P, T* q0, T* q1, i
 template <class T, int D>
 __device__ __forceinline__ void load_stencil(const DevPatch& P, const T* __restrict__ q0,
                                              const T* __restrict__ q1, int64_t c,
-                                             problem::Stencil<T, D>& s) {
+                                             Problem::Stencil<T, D>& s) {
   const int64_t st[3] = {1, P.sy, P.sz};
   s.pc = q0[c];
   s.mc = q1[c];
@@ -148,14 +148,14 @@ __device__ __forceinline__ void relax_cell(const DevPatch& P, int i, int j, int 
   const T* f0 = fld<T>(P.f[0]);
   const T* f1 = fld<T>(P.f[1]);
   const int64_t c = cidx(P, i, j, k);
-  problem::Stencil<T, D> s;
+  Problem::Stencil<T, D> s;
   load_stencil<T, D>(P, q0, q1, c, s);
   T phi, mu;
   if (P.delta)
-    problem::RelaxCell<T, D, true>(s, f0[c], f1[c], T(P.tmp1), T(P.tmp2), T(P.tmp3), T(P.alpha),
+    Problem::RelaxCell<T, D, true>(s, f0[c], f1[c], T(P.tmp1), T(P.tmp2), T(P.tmp3), T(P.alpha),
                                    phi, mu, fld<T>(P.bs)[c]);
   else
-    problem::RelaxCell<T, D>(s, f0[c], f1[c], T(P.tmp1), T(P.tmp2), T(P.tmp3), T(P.alpha), phi,
+    Problem::RelaxCell<T, D>(s, f0[c], f1[c], T(P.tmp1), T(P.tmp2), T(P.tmp3), T(P.alpha), phi,
                              mu);
   q0[c] = phi;
   q1[c] = mu;
@@ -164,13 +164,13 @@ __device__ __forceinline__ void relax_cell(const DevPatch& P, int i, int j, int 
 
 // Operator at one cell from its stencil, in the patch's form.
 template <class T, int D>
-__device__ __forceinline__ void operator_at(const DevPatch& P, const problem::Stencil<T, D>& s,
+__device__ __forceinline__ void operator_at(const DevPatch& P, const Problem::Stencil<T, D>& s,
                                             int64_t c, T& o0, T& o1) {
   if (P.delta)
-    problem::OperatorCell<T, D, true>(s, T(P.tmp1), T(P.tmp2), T(P.alpha), o0, o1,
+    Problem::OperatorCell<T, D, true>(s, T(P.tmp1), T(P.tmp2), T(P.alpha), o0, o1,
                                       fld<T>(P.bs)[c]);
   else
-    problem::OperatorCell<T, D>(s, T(P.tmp1), T(P.tmp2), T(P.alpha), o0, o1);
+    Problem::OperatorCell<T, D>(s, T(P.tmp1), T(P.tmp2), T(P.alpha), o0, o1);
 }
 
 // Residual rf = f - Operator(q) at one cell (afas:799-840).
@@ -178,7 +178,7 @@ template <class T, int D>
 __device__ __forceinline__ void residual_cell(const DevPatch& P, const T* q0, const T* q1,
                                               const T* f0, const T* f1, int64_t c, T& r0,
                                               T& r1) {
-  problem::Stencil<T, D> s;
+  Problem::Stencil<T, D> s;
   load_stencil<T, D>(P, q0, q1, c, s);
   T o0, o1;
   operator_at<T, D>(P, s, c, o0, o1);
@@ -270,7 +270,7 @@ __device__ __forceinline__ void coarse_load_cell(const DevPatch& C, const DevPat
   const TP R0 = TP(w * s0), R1 = TP(w * s1);
   const int pi = C.off[0] + ic, pj = C.off[1] + jc, pk = (D == 3) ? C.off[2] + kc : 0;
   const int64_t pc = cidx(P, pi, pj, pk);
-  problem::Stencil<TP, D> s;
+  Problem::Stencil<TP, D> s;
   load_stencil<TP, D>(P, fld<TP>(P.qs[0]), fld<TP>(P.qs[1]), pc, s);
   TP o0, o1;
   operator_at<TP, D>(P, s, pc, o0, o1);
@@ -503,7 +503,7 @@ __device__ __forceinline__ void source_item(const DevPatch* __restrict__ PT, con
     if (i > P.n[0]) break;
     const int64_t c = cidx(P, i, j, k);
     T a, b;
-    problem::SourceCell<T>(qo[c], T(P.alpha), a, b);
+    Problem::SourceCell<T>(qo[c], T(P.alpha), a, b);
     f0[c] = a;
     f1[c] = b;
   }
@@ -642,12 +642,6 @@ static __global__ void k_mg_loop(DevStatus* __restrict__ st, double* __restrict_
   cudaGraphSetConditional(handle, again ? 1u : 0u);
 }
 
-// Ff of the problem module (problem.f90:769-780): alpha c^2 (c-1)^2 / 4.
-__device__ __forceinline__ double Ff(double c, double alpha) {
-  const double cm1 = c - 1.0;
-  return c * c * cm1 * cm1 * alpha / 4.0;
-}
-
 // One of the two sums of Energy2D (problem.f90:330-361) over a 2D patch
 // interior: which = 0, sum of Ff(c); which = 1, sum of f1(i) + f1(i-1) +
 // f2(j) + f2(j-1) with f1 = (c(i+1) - c(i))^2, f2 = (c(j+1) - c(j))^2 (the
@@ -669,7 +663,7 @@ __global__ void __launch_bounds__(BLOCK_THREADS)
       const int i = i0 + t;
       if (i > P.n[0]) break;
       if (which == 0) {
-        acc += Ff(C(i, j), P.alpha);
+        acc += Problem::Ff(C(i, j), P.alpha);
       } else {
         const double a = C(i + 1, j) - C(i, j), b = C(i, j) - C(i - 1, j);
         const double u = C(i, j + 1) - C(i, j), w = C(i, j) - C(i, j - 1);

@@ -29,14 +29,11 @@ __device__ void errflags_patch(const DevPatch* __restrict__ PT, int patch, doubl
     const int i = (int)(e % n0) + 1;
     const int j = (int)((e / n0) % n1) + 1;
     const int k = D == 3 ? (int)(e / ((int64_t)n0 * n1)) + 1 : 0;
-    const double dx = c[cidx(P, i + 1, j, k)] - c[cidx(P, i - 1, j, k)];
-    const double dy = c[cidx(P, i, j + 1, k)] - c[cidx(P, i, j - 1, k)];
-    double s = dx * dx + dy * dy;
-    if (D == 3) {
-      const double dz = c[cidx(P, i, j, k + 1)] - c[cidx(P, i, j, k - 1)];
-      s = s + dz * dz;
-    }
-    flags[e] = fabs(sqrt(s)) > tol ? 1 : 0;
+    double dc[D];
+    dc[0] = c[cidx(P, i + 1, j, k)] - c[cidx(P, i - 1, j, k)];
+    dc[1] = c[cidx(P, i, j + 1, k)] - c[cidx(P, i, j - 1, k)];
+    if (D == 3) dc[D - 1] = c[cidx(P, i, j, k + 1)] - c[cidx(P, i, j, k - 1)];
+    flags[e] = Problem::TagCell<D>(dc, tol) ? 1 : 0;
   }
 }
 

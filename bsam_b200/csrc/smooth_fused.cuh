@@ -143,7 +143,7 @@ __device__ __forceinline__ void fused3_cell(const DevPatch& P, T* sphi, T* smu, 
   const T f0 = sf0[so + lc], f1 = sf1[so + lc];
   const T* ph = sphi + lc;
   const T* mu_ = smu + lc;
-  problem::Stencil<T, 3> s;
+  Problem::Stencil<T, 3> s;
   s.pc = ph[so];
   s.mc = mu_[so];
   if (!(xl | xh | yl | yh | zl | zh)) {
@@ -175,10 +175,10 @@ __device__ __forceinline__ void fused3_cell(const DevPatch& P, T* sphi, T* smu, 
   }
   T phi, mu;
   if (C::NFIELD == 5 && P.delta)
-    problem::RelaxCell<T, 3, true>(s, f0, f1, T(P.tmp1), T(P.tmp2), T(P.tmp3), T(P.alpha), phi,
+    Problem::RelaxCell<T, 3, true>(s, f0, f1, T(P.tmp1), T(P.tmp2), T(P.tmp3), T(P.alpha), phi,
                                    mu, sbs[so + lc]);
   else
-    problem::RelaxCell<T, 3>(s, f0, f1, T(P.tmp1), T(P.tmp2), T(P.tmp3), T(P.alpha), phi, mu);
+    Problem::RelaxCell<T, 3>(s, f0, f1, T(P.tmp1), T(P.tmp2), T(P.tmp3), T(P.alpha), phi, mu);
   sphi[so + lc] = phi;
   smu[so + lc] = mu;
 }

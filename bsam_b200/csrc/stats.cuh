@@ -41,7 +41,7 @@ __global__ void __launch_bounds__(256)
       if (b.kind == STAT_SUM) {
         acc += x;
       } else if (b.kind == STAT_FF) {
-        acc += Ff(x, alpha);
+        acc += Problem::Ff(x, alpha);
       } else {
         const double a = c[cidx(P, i + 1, j, k)] - x, e = x - c[cidx(P, i - 1, j, k)];
         const double u = c[cidx(P, i, j + 1, k)] - x, w = x - c[cidx(P, i, j - 1, k)];

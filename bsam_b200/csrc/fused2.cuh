@@ -622,37 +622,7 @@ __global__ void __launch_bounds__(Fused2<T>::THREADS, MINB)
       const DevPatch M = PT[P.master];
       double* m0 = fld<double>(M.q[0]);
       double* m1 = fld<double>(M.q[1]);
-      const bool inner = gx0 > 1 && gx0 + F::RX - 1 < n0 && gy0 > 1 && gy0 + F::RY - 1 < n1;
-      if (inner) {
-        // Every row and pair of the tile lies inside the patch, away from
-        // its faces: the lane loads all its master pairs before storing any,
-        // so that the loads are in flight together.
-        constexpr int KR = F::TY / F::WARPS;
-        static_assert(F::TY % F::WARPS == 0, "whole rows per warp");
-        if (lx < F::TX) {
-          double2 x0[KR], x1[KR];
-#pragma unroll
-          for (int k = 0; k < KR; ++k) {
-            const int64_t c = cidx(M, gi, gy0 + F::H + warp + k * F::WARPS, 0);
-            x0[k] = *reinterpret_cast<const double2*>(m0 + c);
-            x1[k] = *reinterpret_cast<const double2*>(m1 + c);
-          }
-#pragma unroll
-          for (int k = 0; k < KR; ++k) {
-            const int ly = warp + k * F::WARPS;
-            const int srow = (F::H + ly) * F::RX + F::H;
-            const V e0 = *reinterpret_cast<const V*>(s0 + srow + lx);
-            const V e1 = *reinterpret_cast<const V*>(s1 + srow + lx);
-            x0[k].x = x0[k].x + (double)e0.x;
-            x0[k].y = x0[k].y + (double)e0.y;
-            x1[k].x = x1[k].x + (double)e1.x;
-            x1[k].y = x1[k].y + (double)e1.y;
-            const int64_t c = cidx(M, gi, gy0 + F::H + ly, 0);
-            *reinterpret_cast<double2*>(m0 + c) = x0[k];
-            *reinterpret_cast<double2*>(m1 + c) = x1[k];
-          }
-        }
-      } else if (lx < F::TX && gi <= n0)
+      if (lx < F::TX && gi <= n0)
         for (int ly = warp; ly < F::TY; ly += F::WARPS) {
           const int j = gy0 + F::H + ly;
           if (j > n1) break;

@@ -6,6 +6,7 @@ and results match the reference arithmetic operation for operation.
 """
 from __future__ import annotations
 
+import hashlib
 import os
 import shutil
 import subprocess
@@ -25,20 +26,37 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found")
 
 
-def _stale() -> bool:
-    if not os.path.exists(LIB):
-        return True
-    t = os.path.getmtime(LIB)
+STAMP = LIB + ".sha256"
+
+
+def _digest() -> str:
+    """Hash of every source and header the library is built from and of this
+    recipe: the library is rebuilt when it changes (file times do not survive
+    copying the tree to another machine, contents do)."""
     deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)]
     inc = os.path.join(HERE, "..", "include")
     deps += [os.path.join(inc, f) for f in os.listdir(inc)]
     deps.append(os.path.abspath(__file__))
-    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+    h = hashlib.sha256()
+    for d in sorted(deps):
+        if os.path.isfile(d):
+            h.update(os.path.basename(d).encode())
+            with open(d, "rb") as f:
+                h.update(f.read())
+    return h.hexdigest()
+
+
+def _stale() -> bool:
+    if not os.path.exists(LIB) or not os.path.exists(STAMP):
+        return True
+    with open(STAMP) as f:
+        return f.read().strip() != _digest()
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not _stale():
         return LIB
+    digest = _digest()
     cmd = [nvcc(), "-O3", "-std=c++17", *ARCH, "-lineinfo", "--fmad=false",
            "-Xcompiler", "-fPIC", "-shared", "-o", LIB,
            *[os.path.join(CSRC, s) for s in SOURCES]]
@@ -46,6 +64,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
         cmd.insert(1, "-Xptxas=-v")
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)
+    with open(STAMP, "w") as f:
+        f.write(digest + "\n")
     return LIB
 
 

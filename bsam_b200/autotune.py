@@ -16,8 +16,6 @@ mapped onto the B200 but not a single result bit (bsam_batch_tuning):
   grid_ctas   CTAs of every other stage launch
   tile_chunk  runs of consecutive tiles a CTA of those launches takes at a
               time (a run's tiles mostly share one problem's records)
-  coarse_gather  2D coarse loads from global memory cell by cell (1) instead
-              of through a shared-memory copy of each tile (0)
 
 The tuner times candidates on a sample of the caller's workload with CUDA
 events on the engine's stream (a few V-cycle ticks of every sampled problem,
@@ -39,8 +37,7 @@ from . import batch as BB
 
 # Search order: the fused stage's build before sweep fusion, so that fusion is
 # judged with the fused stage's best build.
-KNOBS = ("fused_occ", "per_pass", "fused_ctas", "fused_chunk", "grid_ctas", "tile_chunk",
-         "coarse_gather")
+KNOBS = ("fused_occ", "per_pass", "fused_ctas", "fused_chunk", "grid_ctas", "tile_chunk")
 
 
 @dataclasses.dataclass(frozen=True)
@@ -51,7 +48,6 @@ class Choice:
     grid_ctas: int = 0
     tile_chunk: int = 0
     fused_chunk: int = 0
-    coarse_gather: int = 0
 
     def as_dict(self) -> dict:
         return dataclasses.asdict(self)
@@ -71,8 +67,7 @@ def candidates(knob: str, nsm: int) -> list:
         return [0, 1, 4]
     if knob == "fused_chunk":
         return [0, 2]
-    if knob == "coarse_gather":
-        return [0, 1]
+
     raise ValueError(knob)
 
 

@@ -50,7 +50,7 @@ class BatchTuning(ctypes.Structure):
     _fields_ = [("grid_ctas", ctypes.c_int32), ("eager", ctypes.c_int32),
                 ("per_pass", ctypes.c_int32), ("fused_ctas", ctypes.c_int32),
                 ("fused_occ", ctypes.c_int32), ("tile_chunk", ctypes.c_int32),
-                ("fused_chunk", ctypes.c_int32), ("coarse_gather", ctypes.c_int32)]
+                ("fused_chunk", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
 class BatchStats(ctypes.Structure):
@@ -173,10 +173,10 @@ class Batch:
 
     def set_tuning(self, grid_ctas: int = 0, eager: int = 0, per_pass: int = 0,
                    fused_ctas: int = 0, fused_occ: int = 0, tile_chunk: int = 0,
-                   fused_chunk: int = 0, coarse_gather: int = 0):
+                   fused_chunk: int = 0):
         t = BatchTuning(grid_ctas=grid_ctas, eager=eager, per_pass=per_pass,
                         fused_ctas=fused_ctas, fused_occ=fused_occ, tile_chunk=tile_chunk,
-                        fused_chunk=fused_chunk, coarse_gather=coarse_gather)
+                        fused_chunk=fused_chunk)
         _check(_lib().bsam_batch_set_tuning(self.h, ctypes.byref(t)), self.h, "set_tuning")
 
     def profile(self, enable: bool = True):
@@ -394,7 +394,7 @@ class Batch:
 def solve_all(problems, precision: int = PREC_MIXED, max_slots: int | None = None,
               pool_bytes: int = 0, device: int = 0, grid_ctas: int = 0, eager: int = 0,
               per_pass: int = 0, fused_ctas: int = 0, fused_occ: int = 0, tile_chunk: int = 0,
-              fused_chunk: int = 0, coarse_gather: int = 0):
+              fused_chunk: int = 0):
     """Solves every problem (one dimensionality) in one batch; admits more as
     slots free up.  Returns the collect() results in input order."""
     if not problems:
@@ -405,8 +405,7 @@ def solve_all(problems, precision: int = PREC_MIXED, max_slots: int | None = Non
     with Batch(nd, precision=precision, max_slots=ms, pool_bytes=pool_bytes, qerrortol=tol,
                maxvcycles=problems[0].maxvcycles, device=device) as b:
         knobs = dict(grid_ctas=grid_ctas, eager=eager, per_pass=per_pass, fused_ctas=fused_ctas,
-                     fused_occ=fused_occ, tile_chunk=tile_chunk, fused_chunk=fused_chunk,
-                     coarse_gather=coarse_gather)
+                     fused_occ=fused_occ, tile_chunk=tile_chunk, fused_chunk=fused_chunk)
         if any(knobs.values()):
             b.set_tuning(**knobs)
         out = [None] * len(problems)

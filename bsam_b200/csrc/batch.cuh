@@ -4,8 +4,9 @@
 // list that covers that stage for all resident problems; the list's length
 // is read on the device, so problems can be added between ticks without
 // re-capturing the tick graph.  CTAs walk the list in runs of consecutive
-// tiles (TileRuns) and run the same tile bodies as the single-problem kernels (kernels.cuh,
-// mixed.cuh, bottom.cuh); tiles of finished problems are skipped.
+// tiles (TileRuns) and run the same tile bodies as the single-problem
+// kernels (kernels.cuh, mixed.cuh, bottom.cuh); tiles of finished problems
+// are skipped.
 //
 // Per-problem control (k_batch_control) replaces the host loop of
 // MultigridIterations (afas:69-104) and of TakeTimeSteps
@@ -92,154 +93,6 @@ __global__ void __launch_bounds__(BLOCK_THREADS)
     const Item it = items[b];
     if (PT[it.patch].pprec == PREC_F32) coarse_load_item<TC, float, D>(PT, it);
     else coarse_load_item<TC, double, D>(PT, it);
-  }
-}
-
-// CoarseLoadingFunction of 2D records through shared memory.  A tile of the
-// coarse-load list (64 x TILE_Y coarse cells) reads, besides the parent's
-// stencils, the fine residual at its 4 x 64 x TILE_Y children -- each a
-// five-point stencil -- so the gather form (coarse_load_cell) touches every
-// fine value about four times through L1.  Here the CTA first copies the
-// tile's fine state with a one-cell ring, its f (and the correction form's
-// base) and the parent's restricted state qs with a ring into shared memory
-// with coalesced loads, then every thread evaluates coarse_load_cell's
-// expressions for its two coarse cells from there, children in the same
-// order, so the values are the gather form's bit for bit.
-struct CoarseLoad2 {
-  static constexpr int CX = 2 * 32, CY = TILE_Y;       // coarse cells of a tile
-  static constexpr int QX = 2 * CX + 2, QY = 2 * CY + 2;  // fine state box (ring 1)
-  static constexpr int FX = 2 * CX, FY = 2 * CY;        // fine f / base box
-  static constexpr int PX = CX + 2, PY = CY + 2;        // parent qs box (ring 1)
-  template <class TC>
-  static constexpr size_t smem() {  // the parent's planes sized for FP64
-    return sizeof(TC) * (2 * QY * QX + 3 * FY * FX) + 8 * 2 * PY * PX;
-  }
-};
-
-template <class TC, class TP>
-__device__ __forceinline__ void coarse_load_tile2(const DevPatch& C, const DevPatch& P,
-                                                  const Item it, unsigned char* raw) {
-  using L = CoarseLoad2;
-  TC* sq0 = reinterpret_cast<TC*>(raw);
-  TC* sq1 = sq0 + L::QY * L::QX;
-  TC* sf0 = sq1 + L::QY * L::QX;
-  TC* sf1 = sf0 + L::FY * L::FX;
-  TC* sbs = sf1 + L::FY * L::FX;
-  TP* sp0 = reinterpret_cast<TP*>(sbs + L::FY * L::FX);
-  TP* sp1 = sp0 + L::PY * L::PX;
-  const int tid = threadIdx.x + 32 * threadIdx.y;
-  const int ic0 = it.tx * L::CX + 1, jc0 = it.ty * L::CY + 1;
-  const int nci = min(L::CX, C.cn[0] - ic0 + 1), ncj = min(L::CY, C.cn[1] - jc0 + 1);
-  // Fine box origin (ring included) and extents; the parent box likewise.
-  const int fi0 = 2 * ic0 - 2, fj0 = 2 * jc0 - 2;
-  const int nqx = 2 * nci + 2, nqy = 2 * ncj + 2;
-  const int pi0 = C.off[0] + ic0 - 1, pj0 = C.off[1] + jc0 - 1;
-  const int npx = nci + 2, npy = ncj + 2;
-  {
-    const TC* q0 = fld<TC>(mid_state(C)[0]);
-    const TC* q1 = fld<TC>(mid_state(C)[1]);
-    for (int e = tid; e < nqy * nqx; e += BLOCK_THREADS) {
-      const int r = e / nqx, c = e - r * nqx;
-      const int64_t g = cidx(C, fi0 + c, fj0 + r, 0);
-      sq0[r * L::QX + c] = q0[g];
-      sq1[r * L::QX + c] = q1[g];
-    }
-    const TC* f0 = fld<TC>(C.f[0]);
-    const TC* f1 = fld<TC>(C.f[1]);
-    const TC* bs = C.delta ? fld<TC>(C.bs) : nullptr;
-    for (int e = tid; e < (nqy - 2) * (nqx - 2); e += BLOCK_THREADS) {
-      const int r = e / (nqx - 2), c = e - r * (nqx - 2);
-      const int64_t g = cidx(C, fi0 + 1 + c, fj0 + 1 + r, 0);
-      sf0[r * L::FX + c] = f0[g];
-      sf1[r * L::FX + c] = f1[g];
-      if (bs) sbs[r * L::FX + c] = bs[g];
-    }
-    const TP* ps0 = fld<TP>(P.qs[0]);
-    const TP* ps1 = fld<TP>(P.qs[1]);
-    for (int e = tid; e < npy * npx; e += BLOCK_THREADS) {
-      const int r = e / npx, c = e - r * npx;
-      const int64_t g = cidx(P, pi0 + c, pj0 + r, 0);
-      sp0[r * L::PX + c] = ps0[g];
-      sp1[r * L::PX + c] = ps1[g];
-    }
-  }
-  __syncthreads();
-  const int jc = jc0 + threadIdx.y;
-  if (jc - jc0 < ncj) {
-#pragma unroll
-    for (int t = 0; t < 2; ++t) {
-      const int ic = ic0 + 2 * threadIdx.x + t;
-      if (ic - ic0 >= nci) break;
-      // Restriction of rf: children in the reference's summation order.
-      TC s0 = TC(0), s1 = TC(0);
-#pragma unroll
-      for (int ch = 0; ch < 4; ++ch) {
-        const int li = 2 * ic - (ch & 1) - fi0, lj = 2 * jc - ((ch >> 1) & 1) - fj0;
-        const int x = lj * L::QX + li;
-        Problem::Stencil<TC, 2> st;
-        st.pc = sq0[x];
-        st.mc = sq1[x];
-        st.pm[0] = sq0[x - 1];
-        st.pp[0] = sq0[x + 1];
-        st.mm[0] = sq1[x - 1];
-        st.mp[0] = sq1[x + 1];
-        st.pm[1] = sq0[x - L::QX];
-        st.pp[1] = sq0[x + L::QX];
-        st.mm[1] = sq1[x - L::QX];
-        st.mp[1] = sq1[x + L::QX];
-        const int xf = (lj - 1) * L::FX + (li - 1);
-        TC o0, o1;
-        if (C.delta)
-          Problem::OperatorCell<TC, 2, true>(st, TC(C.tmp1), TC(C.tmp2), TC(C.alpha), o0, o1,
-                                             sbs[xf]);
-        else
-          Problem::OperatorCell<TC, 2>(st, TC(C.tmp1), TC(C.tmp2), TC(C.alpha), o0, o1);
-        const TC r0 = sf0[xf] - o0, r1 = sf1[xf] - o1;
-        if (ch == 0) {
-          s0 = r0;
-          s1 = r1;
-        } else {
-          s0 = s0 + r0;
-          s1 = s1 + r1;
-        }
-      }
-      const TC w = TC(0.25);
-      const TP R0 = TP(w * s0), R1 = TP(w * s1);
-      const int x = (jc - jc0 + 1) * L::PX + (ic - ic0 + 1);
-      Problem::Stencil<TP, 2> sp;
-      sp.pc = sp0[x];
-      sp.mc = sp1[x];
-      sp.pm[0] = sp0[x - 1];
-      sp.pp[0] = sp0[x + 1];
-      sp.mm[0] = sp1[x - 1];
-      sp.mp[0] = sp1[x + 1];
-      sp.pm[1] = sp0[x - L::PX];
-      sp.pp[1] = sp0[x + L::PX];
-      sp.mm[1] = sp1[x - L::PX];
-      sp.mp[1] = sp1[x + L::PX];
-      const int64_t pc = cidx(P, C.off[0] + ic, C.off[1] + jc, 0);
-      TP o0, o1;
-      operator_at<TP, 2>(P, sp, pc, o0, o1);
-      fld<TP>(P.f[0])[pc] = R0 + o0;
-      fld<TP>(P.f[1])[pc] = R1 + o1;
-    }
-  }
-}
-
-template <class TC>
-__global__ void __launch_bounds__(BLOCK_THREADS)
-    kb_coarse_load2(const DevPatch* __restrict__ PT, const Item* __restrict__ items,
-                    const int* __restrict__ count, TileRuns R) {
-  extern __shared__ __align__(16) unsigned char cl2_raw[];
-  const int n = *count;
-  for (int b = R.first(); b < n; b = R.next(b)) {
-    const Item it = items[b];
-    const DevPatch C = PT[it.patch];
-    if (!C.active) continue;  // uniform per CTA
-    const DevPatch P = PT[C.parent];
-    __syncthreads();  // the previous tile's shared reads are done
-    if (C.pprec == PREC_F32) coarse_load_tile2<TC, float>(C, P, it, cl2_raw);
-    else coarse_load_tile2<TC, double>(C, P, it, cl2_raw);
   }
 }
 

@@ -692,15 +692,7 @@ void tick_t(bsam_batch* b, cudaGraphConditionalHandle handle, int in_graph) {
         kb_restrict<double, D><<<gr, blk, 0, s>>>(pt, L[L_RESTR + d].d, cnt + L_RESTR + d, R);
       ++n;
     }
-    if (D == 2 && !b->tuning.coarse_gather) {
-      // Staged through shared memory (kb_coarse_load2); same values.
-      if (b->mixed)
-        kb_coarse_load2<float><<<gc, blk, CoarseLoad2::smem<float>(), s>>>(
-            pt, L[L_COARSE + d].d, cnt + L_COARSE + d, R);
-      else
-        kb_coarse_load2<double><<<gc, blk, CoarseLoad2::smem<double>(), s>>>(
-            pt, L[L_COARSE + d].d, cnt + L_COARSE + d, R);
-    } else if (b->mixed) {
+    if (b->mixed) {
       kb_coarse_load<float, D><<<gc, blk, 0, s>>>(pt, L[L_COARSE + d].d, cnt + L_COARSE + d,
                                                   R);
     } else {
@@ -905,10 +897,6 @@ int bsam_batch_create(bsam_batch** out, int device, const bsam_batch_params* p) 
             cudaMalloc(&b->d_counts, sizeof(int) * NLIST) == cudaSuccess;
   if (ok) ok = cudaHostGetDevicePointer((void**)&b->d_out, b->h_out, 0) == cudaSuccess;
   if (ok)
-    ok = cudaFuncSetAttribute(kb_coarse_load2<double>,
-                              cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)CoarseLoad2::smem<double>()) == cudaSuccess;
-  if (ok)
     ok = cudaFuncSetAttribute(kb_smooth2<float, true, 3>,
                               cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)Fused2<float>::SMEM) == cudaSuccess &&
@@ -997,8 +985,7 @@ int bsam_batch_set_tuning(bsam_batch* b, const bsam_batch_tuning* t) {
   if (!b || !t || t->grid_ctas < 0 || t->eager < 0 || t->eager > 1 || t->per_pass < 0 ||
       t->per_pass > 1 || t->fused_ctas < 0 ||
       (t->fused_occ != 0 && (t->fused_occ < 2 || t->fused_occ > 4)) || t->tile_chunk < 0 ||
-      t->tile_chunk > 64 || t->fused_chunk < 0 || t->fused_chunk > 64 || t->coarse_gather < 0 ||
-      t->coarse_gather > 1)
+      t->tile_chunk > 64 || t->fused_chunk < 0 || t->fused_chunk > 64)
     return BSAM_ERR_ARG;
   b->tuning = *t;
   b->need_capture = true;

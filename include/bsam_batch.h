@@ -88,8 +88,7 @@ typedef struct {
  * many consecutive tiles, run r to CTA r mod the grid (1 = grid-stride;
  * consecutive tiles mostly share their problem's records, which a run then
  * reads from L1), for the small-tile list kernels (0 = 2) and for the fused
- * stages (0 = 1); coarse_gather = 1 computes the 2D coarse loads from global
- * memory cell by cell instead of staging each tile in shared memory. */
+ * stages (0 = 1). */
 typedef struct {
   int32_t grid_ctas;
   int32_t eager;
@@ -98,7 +97,7 @@ typedef struct {
   int32_t fused_occ;
   int32_t tile_chunk;
   int32_t fused_chunk;
-  int32_t coarse_gather;
+  int32_t reserved;
 } bsam_batch_tuning;
 
 typedef struct {

@@ -9,7 +9,7 @@ from bsam_b200 import workloads as W
 def test_coordinate_descent_finds_separable_optimum():
     # A separable cost with one best value per knob: the descent finds it.
     best = {"per_pass": 0, "fused_occ": 4, "fused_ctas": 3 * 148, "grid_ctas": 8 * 148,
-            "tile_chunk": 4, "fused_chunk": 2, "coarse_gather": 1}
+            "tile_chunk": 4, "fused_chunk": 2}
     calls = []
 
     def timer(c):

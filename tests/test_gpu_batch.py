@@ -141,9 +141,8 @@ def test_batch_tuning_leaves_results_unchanged(gpu_lib):
     c = BB.solve_all(probs, precision=BB.PREC_MIXED, eager=1)
     d = BB.solve_all(probs, precision=BB.PREC_MIXED, per_pass=1)  # no fused stages
     e = BB.solve_all(probs, precision=BB.PREC_MIXED, fused_ctas=5)
-    f = BB.solve_all(probs, precision=BB.PREC_MIXED, coarse_gather=1)  # unstaged coarse load
-    g = BB.solve_all(probs, precision=BB.PREC_MIXED, tile_chunk=7, fused_chunk=3)
-    for x, *others in zip(a, b, c, d, e, f, g):
+    f = BB.solve_all(probs, precision=BB.PREC_MIXED, tile_chunk=7, fused_chunk=3)
+    for x, *others in zip(a, b, c, d, e, f):
         for k in ("q", "nvcycles", "residual"):
             for y in others:
                 assert np.array_equal(x[k], y[k]), k

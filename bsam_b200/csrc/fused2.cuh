@@ -503,11 +503,7 @@ __global__ void __launch_bounds__(Fused2<T>::THREADS, MINB)
     return n;
   };
   // Thread 0: the tensor copies of tile x into buffer buf.
-  // part 0: every copy of tile x; part 1: the tile's expected bytes and its
-  // f1, f2 -- planes the current tile no longer reads once its passes are
-  // done, so these copies overlap its restriction and write-back; part 2:
-  // the rest (the state unless the tile starts from zero, and the base).
-  auto issue = [&](int x, int buf, int part) {
+  auto issue = [&](int x, int buf) {
     const Item it = items[x];
     const DevPatch& P = PT[it.patch];
     const int gx0 = it.tx * F::TX + 1 - F::H, gy0 = it.ty * F::TY + 1 - F::H;
@@ -516,30 +512,26 @@ __global__ void __launch_bounds__(Fused2<T>::THREADS, MINB)
     const CUtensorMapOpaque* maps = static_cast<const CUtensorMapOpaque*>(P.tmaps);
     const int m0 = dir == 0 ? 0 : 2;
     const uint32_t pl = (uint32_t)(sizeof(T) * F::PLANE);
-    const int xc = gx0 + lead;  // column of element (gx0, *) from the allocation start
     fence_proxy_async_smem();  // earlier generic accesses to the buffer come first
-    if (part != 2) {
-      mbar_arrive_expect_tx(&bar[buf], pl * (uint32_t)(NPL - (zs ? 2 : 0)));
-      tma_load_2d(plane(buf, 2), &maps[4], xc, gy0, &bar[buf]);
-      tma_load_2d(plane(buf, 3), &maps[5], xc, gy0, &bar[buf]);
+    mbar_arrive_expect_tx(&bar[buf], pl * (uint32_t)(NPL - (zs ? 2 : 0)));
+    const int xc = gx0 + lead;  // column of element (gx0, *) from the allocation start
+    if (!zs) {
+      tma_load_2d(plane(buf, 0), &maps[m0], xc, gy0, &bar[buf]);
+      tma_load_2d(plane(buf, 1), &maps[m0 + 1], xc, gy0, &bar[buf]);
     }
-    if (part != 1) {
-      if (!zs) {
-        tma_load_2d(plane(buf, 0), &maps[m0], xc, gy0, &bar[buf]);
-        tma_load_2d(plane(buf, 1), &maps[m0 + 1], xc, gy0, &bar[buf]);
-      }
-      if (DELTA) tma_load_2d(plane(buf, 4), &maps[6], xc, gy0, &bar[buf]);
-    }
+    tma_load_2d(plane(buf, 2), &maps[4], xc, gy0, &bar[buf]);
+    tma_load_2d(plane(buf, 3), &maps[5], xc, gy0, &bar[buf]);
+    if (DELTA) tma_load_2d(plane(buf, 4), &maps[6], xc, gy0, &bar[buf]);
   };
   uint32_t phase[NBUF];
   for (int k = 0; k < NBUF; ++k) phase[k] = 0u;
   int cur = next_tile(R.first()), buf = 0;
-  if (cur < n && tid == 0) issue(cur, 0, 0);
+  if (cur < n && tid == 0) issue(cur, 0);
   while (cur < n) {
     const int nxt = next_tile(R.next(cur));
     // Two buffers: the next tile's copies go into the other one, last read
     // by the previous tile (which ended with a barrier).
-    if (NBUF == 2 && nxt < n && tid == 0) issue(nxt, buf ^ 1, 0);
+    if (NBUF == 2 && nxt < n && tid == 0) issue(nxt, buf ^ 1);
     T* s0 = plane(buf, 0);
     T* s1 = plane(buf, 1);
     T* sf0 = plane(buf, 2);
@@ -620,9 +612,6 @@ __global__ void __launch_bounds__(Fused2<T>::THREADS, MINB)
         __syncthreads();
       }
     }
-    // One buffer: the passes are done with f1, f2 (after the barrier above),
-    // so the next tile's copies of them start now.
-    if (NBUF == 1 && nxt < n && tid == 0) issue(nxt, 0, 1);
     using V = typename Pair2<T>::V;
     // Columns 2l, 2l + 1 of the tile's interior: every pair starts at an odd
     // global column, so the pair is one aligned vector in shared memory, in
@@ -695,7 +684,7 @@ __global__ void __launch_bounds__(Fused2<T>::THREADS, MINB)
         }
     }
     __syncthreads();  // the buffer is refilled for a later tile
-    if (NBUF == 1 && nxt < n && tid == 0) issue(nxt, 0, 2);
+    if (NBUF == 1 && nxt < n && tid == 0) issue(nxt, 0);
     cur = nxt;
     if (NBUF == 2) buf ^= 1;
   }

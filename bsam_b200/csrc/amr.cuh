@@ -354,12 +354,18 @@ __global__ void k_ghost2(const DevPatch* __restrict__ PT, const int* __restrict_
     interp2_ghost(P, R, ipass, gi, gj);
   }
   __syncthreads();
+  // Sibling copies, a warp per copy: the strips are a few dozen cells, and
+  // each copy starts with a chain of dependent reads (the copy, the
+  // sibling's record), so the warps run their chains side by side.  The
+  // siblings are disjoint, so no ghost is written by two copies and the
+  // order of the copies does not matter.
   const int2 rg = ranges[blockIdx.x];
-  for (int c = rg.x; c < rg.x + rg.y; ++c) {
+  const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int c = rg.x + (int)(threadIdx.x >> 5); c < rg.x + rg.y; c += nw) {
     const OverlapCopy o = cps[c];
-    const DevPatch S = PT[o.src];
+    const DevPatch& S = PT[o.src];
     const int w = o.i1 - o.i0 + 1, hgt = o.j1 - o.j0 + 1;
-    for (int e = threadIdx.x; e < w * hgt; e += blockDim.x) {
+    for (int e = lane; e < w * hgt; e += 32) {
       const int i = o.i0 + e % w, j = o.j0 + e / w;
 #pragma unroll
       for (int v = 0; v < 2; ++v)

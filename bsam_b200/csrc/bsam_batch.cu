@@ -56,6 +56,8 @@ constexpr int DEFAULT_BOTTOM_CELLS = 1024;
 // tuning.fused_chunk; 1 = grid-stride order).
 constexpr int kDefaultTileChunk = 2;
 constexpr int kDefaultFusedChunk = 1;
+// Runs of the staged defect, in units of tile_chunk.
+constexpr int kDefectRunFactor = 4;
 // Lists: master tiles; bottom-chain tops; per top depth d: tiles of every
 // record (correction), footprint tiles (restriction / coarse load), tiles of
 // records smoothed per colour pass, fused-stage tiles; master tiles whose FP64
@@ -617,6 +619,8 @@ void tick_t(bsam_batch* b, cudaGraphConditionalHandle handle, int in_graph) {
   // The order in which CTAs take list entries (runs of consecutive tiles).
   const TileRuns R{b->tuning.tile_chunk > 0 ? b->tuning.tile_chunk : kDefaultTileChunk};
   const TileRuns RF{b->tuning.fused_chunk > 0 ? b->tuning.fused_chunk : kDefaultFusedChunk};
+  // The staged defect reuses a patch's records along a run: longer runs.
+  const TileRuns RD{kDefectRunFactor * R.chunk};
   // LevelRelax of depth d for every running problem; dir selects the fused
   // stage's buffers (0: q -> qb before the correction, 1: qb -> q after).
   auto relax = [&](int d, int dir) {
@@ -670,7 +674,7 @@ void tick_t(bsam_batch* b, cudaGraphConditionalHandle handle, int in_graph) {
     if (D == 2)
       kb_defect_tma<2><<<gm, blk, Defect2::SMEM, s>>>(pt, L[L_MASTER].d, cnt + L_MASTER,
                                                       b->d_partials, newstep_only,
-                                                      &b->d_ctl->kerr, R);
+                                                      &b->d_ctl->kerr, RD);
     else
       kb_defect<D><<<gm, blk, 0, s>>>(pt, L[L_MASTER].d, cnt + L_MASTER, b->d_partials,
                                       newstep_only, R);

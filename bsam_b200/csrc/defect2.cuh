@@ -55,12 +55,23 @@ __global__ void __launch_bounds__(BLOCK_THREADS, 8)
     double* base = reinterpret_cast<double*>(def_raw) + buf * F::BUF;
     return k < 2 ? base + k * F::QSTRIDE : base + 2 * F::QSTRIDE + (k - 2) * F::FSTRIDE;
   };
+  // Whether a patch takes part, remembered for the last patch asked about:
+  // the tiles of a run mostly share their patch, so its record is read once
+  // per patch rather than once per tile (each read is a round trip to L2).
+  int part_patch = -1;
+  bool part_ok = false;
+  auto takes_part = [&](int p) {
+    if (p != part_patch) {
+      const DevPatch& M = PT[p];
+      part_ok = M.active && !(newstep_only && !M.newstep);
+      part_patch = p;
+    }
+    return part_ok;
+  };
   // The CTA's next tile at or after list position `from` that takes part.
   auto next_tile = [&](int from) {
-    for (int x = from; x < n; x = R.next(x)) {
-      const DevPatch& M = PT[items[x].patch];
-      if (M.active && !(newstep_only && !M.newstep)) return x;
-    }
+    for (int x = from; x < n; x = R.next(x))
+      if (takes_part(items[x].patch)) return x;
     return n;
   };
   // Thread 0: the bulk copies of tile x into buffer buf.
@@ -78,6 +89,8 @@ __global__ void __launch_bounds__(BLOCK_THREADS, 8)
     tma_load_2d(plane(buf, 3), &maps[3], lead + i0, j0, &bar[buf]);
   };
   uint32_t phase[2] = {0u, 0u};
+  int mw_patch = -1;
+  DevPatch M, W;
   int cur = next_tile(R.first()), buf = 0;
   if (cur < n && tid == 0) issue(cur, 0);
   while (cur < n) {
@@ -103,8 +116,12 @@ __global__ void __launch_bounds__(BLOCK_THREADS, 8)
     const double* sf0 = plane(buf, 2);
     const double* sf1 = plane(buf, 3);
     const Item it = items[cur];
-    const DevPatch M = PT[it.patch];
-    const DevPatch W = PT[M.twin];
+    // The master and its twin, read again only when the patch changes.
+    if (it.patch != mw_patch) {
+      M = PT[it.patch];
+      W = PT[M.twin];
+      mw_patch = it.patch;
+    }
     const int i0 = it.tx * F::TX + 1, j0 = it.ty * F::TY + 1;
     // defect_item's cells of this thread, from the staged tile.
     const int j = j0 + threadIdx.y;

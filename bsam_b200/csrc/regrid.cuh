@@ -124,43 +124,71 @@ __global__ void k_buffer_list(const LevelPatch* __restrict__ lp, int np, int ib,
 }
 
 // Inclusive summed-area table of each patch's flags (a CTA per patch): sums
-// along x, then y, then z, each line by one thread.
+// along x, then y, then z.  Along x a warp takes a line, 32 cells at a time,
+// with a warp-wide scan and the carry from the previous 32; along y (and z)
+// a lane takes a column and loads eight cells ahead of its running sum, so
+// that the loads are in flight together.  Integer sums, so the table does
+// not depend on the order of the additions.
 template <int D>
 __global__ void __launch_bounds__(256)
     k_sat_list(const LevelPatch* __restrict__ lp, const uint8_t* __restrict__ in,
                int32_t* __restrict__ sat) {
+  constexpr unsigned FULL = 0xffffffffu;
   const LevelPatch L = lp[blockIdx.x];
   const int n0 = L.n[0], n1 = L.n[1], n2 = D == 3 ? L.n[2] : 1;
   int32_t* s = sat + L.off;
   const uint8_t* f = in + L.off;
-  for (int line = threadIdx.x; line < n1 * n2; line += blockDim.x) {
-    int32_t acc = 0;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int line = warp; line < n1 * n2; line += nw) {
     const int64_t b = (int64_t)line * n0;
-    for (int i = 0; i < n0; ++i) {
-      acc += f[b + i];
-      s[b + i] = acc;
+    int32_t carry = 0;
+    for (int i0 = 0; i0 < n0; i0 += 256) {
+      int32_t v[8];
+#pragma unroll
+      for (int t = 0; t < 8; ++t) {
+        const int i = i0 + 32 * t + lane;
+        v[t] = i < n0 ? (int32_t)f[b + i] : 0;
+      }
+#pragma unroll
+      for (int t = 0; t < 8; ++t) {
+        int32_t x = v[t];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int32_t u = __shfl_up_sync(FULL, x, o);
+          if (lane >= o) x += u;
+        }
+        x += carry;
+        const int i = i0 + 32 * t + lane;
+        if (i < n0) s[b + i] = x;
+        carry = __shfl_sync(FULL, x, 31);
+      }
     }
   }
   __syncthreads();
-  for (int line = threadIdx.x; line < n0 * n2; line += blockDim.x) {
-    const int i = line % n0, k = line / n0;
-    int32_t acc = 0;
-    for (int j = 0; j < n1; ++j) {
-      const int64_t c = i + (int64_t)n0 * (j + (int64_t)n1 * k);
-      acc += s[c];
-      s[c] = acc;
-    }
-  }
-  if (D == 3) {
-    __syncthreads();
-    for (int line = threadIdx.x; line < n0 * n1; line += blockDim.x) {
+  // Column scans along a stride: `cols` columns (count ncol) of `len` cells.
+  auto columns = [&](int64_t ncol, int len, int64_t stride, int64_t plane_cols,
+                     int64_t plane_stride) {
+    for (int64_t c = threadIdx.x; c < ncol; c += blockDim.x) {
+      const int64_t base = (c % plane_cols) + (c / plane_cols) * plane_stride;
       int32_t acc = 0;
-      for (int k = 0; k < n2; ++k) {
-        const int64_t c = line + (int64_t)n0 * n1 * k;
-        acc += s[c];
-        s[c] = acc;
+      for (int j0 = 0; j0 < len; j0 += 8) {
+        int32_t v[8];
+#pragma unroll
+        for (int t = 0; t < 8; ++t) v[t] = j0 + t < len ? s[base + (j0 + t) * stride] : 0;
+#pragma unroll
+        for (int t = 0; t < 8; ++t) {
+          acc += v[t];
+          if (j0 + t < len) s[base + (j0 + t) * stride] = acc;
+        }
       }
     }
+  };
+  // y: column i of plane k, cells i + n0 (j + n1 k), j = 0 .. n1 - 1.
+  columns((int64_t)n0 * n2, n1, n0, n0, (int64_t)n0 * n1);
+  if (D == 3) {
+    __syncthreads();
+    // z: column (i, j), cells i + n0 j + n0 n1 k, k = 0 .. n2 - 1.
+    columns((int64_t)n0 * n1, n2, (int64_t)n0 * n1, (int64_t)n0 * n1, 0);
   }
 }
 

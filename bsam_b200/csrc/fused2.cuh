@@ -417,98 +417,35 @@ __device__ __forceinline__ void correct_tile2(const DevPatch& C, const DevPatch&
 // in the correction form, the parent's base from the fine base), ghosts by
 // write-through -- restrict_cell's expressions.  Tiles start at odd global
 // indices and have even sizes, so every 2 x 2 block lies in one tile.
-// A thread takes two neighbouring coarse cells: their eight fine values per
-// field come from two 4-wide shared reads (the pair starts on a 16-byte
-// boundary: its first fine column is 4 m + 4 of the tile's rows), and away
-// from the parent's faces the pair is stored as one vector per field.
-template <class T>
-__device__ __forceinline__ void load4(const T* p, T (&v)[4]) {
-  if constexpr (sizeof(T) == 4) {
-    const float4 a = *reinterpret_cast<const float4*>(p);
-    v[0] = a.x;
-    v[1] = a.y;
-    v[2] = a.z;
-    v[3] = a.w;
-  } else {
-    const double2 a = *reinterpret_cast<const double2*>(p);
-    const double2 b = *reinterpret_cast<const double2*>(p + 2);
-    v[0] = a.x;
-    v[1] = a.y;
-    v[2] = b.x;
-    v[3] = b.y;
-  }
-}
-
-template <class TP>
-__device__ __forceinline__ void store2(TP* p, TP a, TP b) {
-  using V = typename Pair2<TP>::V;
-  V v;
-  v.x = a;
-  v.y = b;
-  *reinterpret_cast<V*>(p) = v;
-}
-
 template <class T, class TP, bool DELTA>
 __device__ __forceinline__ void restrict_tile2(const DevPatch& C, const DevPatch& R, const T* s0,
                                                const T* s1, const T* sbs, int gx0, int gy0) {
   using F = Fused2<T>;
-  constexpr int PX = F::TX / 4;  // coarse pairs per tile row
   const int icl = (gx0 + F::H + 1) / 2, jcl = (gy0 + F::H + 1) / 2;
   TP* pq0 = fld<TP>(R.q[0]);
   TP* pq1 = fld<TP>(R.q[1]);
   TP* ps0 = fld<TP>(R.qs[0]);
   TP* ps1 = fld<TP>(R.qs[1]);
-  TP* pbs = (DELTA && R.delta) ? fld<TP>(R.bs) : nullptr;
-  for (int k = threadIdx.x; k < PX * (F::TY / 2); k += blockDim.x) {
-    const int ic = icl + 2 * (k % PX), jc = jcl + k / PX;
+  for (int c = threadIdx.x; c < (F::TX / 2) * (F::TY / 2); c += blockDim.x) {
+    const int ic = icl + c % (F::TX / 2), jc = jcl + c / (F::TX / 2);
     if (ic > C.cn[0] || jc > C.cn[1]) continue;
-    // Fine rows 2jc (a) and 2jc - 1 (b), columns 2ic - 1 .. 2ic + 2.
-    const int sa = (2 * jc - gy0) * F::RX + (2 * ic - 1 - gx0);
-    // restrict_cell's sum: (2i, 2j) + (2i-1, 2j) + (2i, 2j-1) + (2i-1, 2j-1).
-    auto pair_avg = [&](const T* sp, TP (&v)[2]) {
-      T a[4], b[4];
-      load4<T>(sp + sa, a);
-      load4<T>(sp + sa - F::RX, b);
-#pragma unroll
-      for (int h = 0; h < 2; ++h)
-        v[h] = TP(T(0.25) * (a[2 * h + 1] + a[2 * h] + b[2 * h + 1] + b[2 * h]));
-    };
-    TP v0[2], v1[2], vb[2];
-    pair_avg(s0, v0);
-    pair_avg(s1, v1);
-    if constexpr (DELTA)
-      if (pbs) pair_avg(sbs, vb);
+    const int si = (2 * jc - gy0) * F::RX + (2 * ic - gx0);  // fine cell (2ic, 2jc)
+    const TP v0 = TP(T(0.25) * (s0[si] + s0[si - 1] + s0[si - F::RX] + s0[si - 1 - F::RX]));
+    const TP v1 = TP(T(0.25) * (s1[si] + s1[si - 1] + s1[si - F::RX] + s1[si - 1 - F::RX]));
     const int pi = C.off[0] + ic, pj = C.off[1] + jc;
     const int64_t pc = cidx(R, pi, pj, 0);
-    const bool two = ic + 1 <= C.cn[0];
-    const bool face = R.wt && (near_boundary(R, pi, pj, 0, 2) ||
-                               (two && near_boundary(R, pi + 1, pj, 0, 2)));
-    if (two && !face && (pi & 1) == 1) {
-      // Element (1, j) of every row is 128-byte aligned, so (pi, pj) with pi
-      // odd starts an aligned pair.
-      store2<TP>(pq0 + pc, v0[0], v0[1]);
-      store2<TP>(pq1 + pc, v1[0], v1[1]);
-      store2<TP>(ps0 + pc, v0[0], v0[1]);
-      store2<TP>(ps1 + pc, v1[0], v1[1]);
-      if constexpr (DELTA)
-        if (pbs) store2<TP>(pbs + pc, vb[0], vb[1]);
-      continue;
+    pq0[pc] = v0;
+    pq1[pc] = v1;
+    ps0[pc] = v0;
+    ps1[pc] = v1;
+    if (R.wt && near_boundary(R, pi, pj, 0, 2)) {
+      write_through<TP, 2>(R, pq0, pq1, pi, pj, 0, v0, v1);
+      write_through<TP, 2>(R, ps0, ps1, pi, pj, 0, v0, v1);
     }
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      if (h == 1 && !two) break;
-      const int64_t c = pc + h;
-      pq0[c] = v0[h];
-      pq1[c] = v1[h];
-      ps0[c] = v0[h];
-      ps1[c] = v1[h];
-      if (R.wt && near_boundary(R, pi + h, pj, 0, 2)) {
-        write_through<TP, 2>(R, pq0, pq1, pi + h, pj, 0, v0[h], v1[h]);
-        write_through<TP, 2>(R, ps0, ps1, pi + h, pj, 0, v0[h], v1[h]);
-      }
-      if constexpr (DELTA)
-        if (pbs) pbs[c] = vb[h];
-    }
+    if constexpr (DELTA)
+      if (R.delta)
+        fld<TP>(R.bs)[pc] =
+            TP(T(0.25) * (sbs[si] + sbs[si - 1] + sbs[si - F::RX] + sbs[si - 1 - F::RX]));
   }
 }
 
@@ -731,11 +668,7 @@ __global__ void __launch_bounds__(Fused2<T>::THREADS, MINB)
           const int srow = (F::H + ly) * F::RX + F::H;
           T* r0 = o0 + (int64_t)j * P.sy;
           T* r1 = o1 + (int64_t)j * P.sy;
-          // A pair with no cell on a patch face has no ghost to write
-          // through: one vector store per field, on edge tiles too.
-          const bool face_pair =
-              edge_tile && (gi == 1 || gi + 1 >= n0 || j == 1 || j == n1);
-          if (!face_pair && gi + 1 <= n0) {
+          if (!edge_tile && gi + 1 <= n0) {
             *reinterpret_cast<V*>(r0 + gi) = *reinterpret_cast<const V*>(s0 + srow + lx);
             *reinterpret_cast<V*>(r1 + gi) = *reinterpret_cast<const V*>(s1 + srow + lx);
             continue;

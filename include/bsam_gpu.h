@@ -56,7 +56,9 @@ typedef struct {
  * parent: index of the parent in the patch array, -1 for the coarsest level.
  * mbounds: this patch's index box in its parent (lib/treeops via
  * InitSeed/MakeNewGrid).  mthbc per face: 1 Neumann reflection, 10-99 the
- * problem's UserBC, 999 internal (coarse-fine).  dx is the grid spacing. */
+ * problem's UserBC, 999 internal (coarse-fine), 2 periodic (PeriodicBC; both
+ * faces of a dimension, hierarchies without refined levels).  dx is the
+ * grid spacing. */
 typedef struct {
   int32_t level, parent;
   int32_t mx[3];

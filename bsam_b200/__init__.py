@@ -69,13 +69,13 @@ ABI_SYMBOLS = (
     "bsam_host_format_frame", "bsam_host_write_frame",
     "bsam_gpu_set_ghost_level", "bsam_gpu_after_step_stats", "bsam_gpu_stash", "bsam_gpu_regrid",
     "bsam_gpu_errflags_level", "bsam_gpu_tag_level", "bsam_host_new_subgrids_sat",
-    "bsam_amr_create", "bsam_amr_step", "bsam_amr_table",
+    "bsam_amr_create", "bsam_amr_step", "bsam_amr_regrid", "bsam_amr_table",
     "bsam_amr_destroy", "bsam_amr_profile",
     "bsam_batch_create", "bsam_batch_destroy", "bsam_batch_set_tuning", "bsam_batch_footprint",
     "bsam_batch_submit", "bsam_batch_advance", "bsam_batch_sync", "bsam_batch_run",
     "bsam_batch_poll", "bsam_batch_slot_phase", "bsam_batch_collect", "bsam_batch_get_stream", "bsam_batch_profile", "bsam_batch_submit_seeded", "bsam_batch_busy",
     "bsam_batch_get_stats", "bsam_batch_last_error", "bsam_batch_submit_many",
-    "bsam_batch_submit_seeded_many", "bsam_batch_collect_many",
+    "bsam_batch_submit_seeded_many", "bsam_batch_collect_many", "bsam_batch_submit_amr",
 )
 
 
@@ -134,6 +134,7 @@ def lib():
                                   ctypes.POINTER(RegridParamsC), ctypes.c_int,
                                   ctypes.POINTER(PatchDesc)]
     L.bsam_amr_step.argtypes = [vp, ip, dp, ip]
+    L.bsam_amr_regrid.argtypes = [vp]
     L.bsam_amr_table.argtypes = [vp, ctypes.POINTER(PatchDesc), ctypes.c_int]
     L.bsam_amr_destroy.argtypes = [vp]
     L.bsam_amr_destroy.restype = None

@@ -93,6 +93,7 @@ def bind(L):
     L.bsam_batch_collect_many.argtypes = [vp, ctypes.c_int, ip, dpp,
                                           ctypes.POINTER(ctypes.POINTER(StepResult)), dp]
     L.bsam_batch_busy.argtypes = [vp]
+    L.bsam_batch_submit_amr.argtypes = [vp, vp, ctypes.c_int, ip]
     L.bsam_batch_get_stream.argtypes = [vp, ctypes.POINTER(vp)]
     L.bsam_batch_get_stats.argtypes = [vp, ctypes.POINTER(BatchStats)]
     L.bsam_batch_last_error.argtypes = [vp]
@@ -314,6 +315,42 @@ class Batch:
 
     def sync(self):
         _check(_lib().bsam_batch_sync(self.h), self.h, "sync")
+
+    def submit_amr(self, run, nsteps: int):
+        """Hands the next nsteps time steps of a refined hierarchy to the batch:
+        run is an amr.AmrRun (its native driver regrids the problem before
+        every step, the batch runs the steps' V-cycles with its other
+        problems).  Returns the slot, or None when no slot is free.  Leave
+        run alone until collect_amr(slot)."""
+        slot = ctypes.c_int(-1)
+        rc = _lib().bsam_batch_submit_amr(self.h, run.a, int(nsteps), ctypes.byref(slot))
+        if rc == ERR_NOMEM:
+            return None
+        _check(rc, self.h, "submit_amr")
+        self.probs[slot.value] = ("amr", run, int(nsteps))
+        return slot.value
+
+    def is_amr(self, slot: int) -> bool:
+        p = self.probs.get(slot)
+        return isinstance(p, tuple) and p[0] == "amr"
+
+    def collect_amr(self, slot: int, want_mass: bool = False) -> dict:
+        """Per-step results of a finished refined hierarchy (its fields stay in
+        its AmrRun, whose patch table is brought up to date) and releases the
+        slot."""
+        _, run, nsteps = self.probs[slot]
+        steps = (StepResult * nsteps)()
+        mass = ctypes.c_double(0.0)
+        rc = _lib().bsam_batch_collect(self.h, slot, None, steps,
+                                       ctypes.byref(mass) if want_mass else None)
+        if rc == 0 or rc == ERR_DIVERGED:
+            self.probs.pop(slot, None)
+        _check(rc, self.h, "collect")
+        run.refresh()
+        return {"nvcycles": np.array([s.nvcycles for s in steps], dtype=np.int32),
+                "converged": np.array([s.converged for s in steps], dtype=np.int32),
+                "residual": np.array([s.residual for s in steps]),
+                "mass": mass.value if want_mass else None}
 
     def run(self):
         _check(_lib().bsam_batch_run(self.h), self.h, "run")

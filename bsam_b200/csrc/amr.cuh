@@ -34,7 +34,7 @@ __device__ __forceinline__ double face_fit(double c1, double c2, double c3) {
 // Ghost (gi, gj) of patch P for colour pass ipass (1 red, 2 black, 0 both);
 // parent R.  Positions follow Interpolate2D statement by statement: the four
 // corners always, face ghosts on internal faces only.
-__device__ void interp2_ghost(const DevPatch& P, const DevPatch& R, int ipass, int gi, int gj) {
+static __device__ void interp2_ghost(const DevPatch& P, const DevPatch& R, int ipass, int gi, int gj) {
   const int m1 = P.n[0], m2 = P.n[1];
   // Parent index box of the patch (mbounds): off + 1 .. off + cn.
   const int b11 = P.off[0] + 1, b12 = P.off[0] + P.cn[0];
@@ -132,7 +132,7 @@ __device__ void interp2_ghost(const DevPatch& P, const DevPatch& R, int ipass, i
 // Corners and edges are skipped in the red pass when one of their faces is
 // physical; for the edges along y the z face passes that check only with code
 // 2 or 99 (boundary.f90:1354 compares with 99, not 999), kept as written.
-__device__ void interp3_ghost(const DevPatch& P, const DevPatch& R, int ipass, int g0, int g1,
+static __device__ void interp3_ghost(const DevPatch& P, const DevPatch& R, int ipass, int g0, int g1,
                               int g2) {
   const int m[3] = {P.n[0], P.n[1], P.n[2]};
   const int g[3] = {g0, g1, g2};
@@ -341,10 +341,12 @@ __device__ __forceinline__ void ring2(int g, int m1, int m2, int& gi, int& gj) {
 // physical faces (setbc_cell).  Each step writes only this patch's ring and reads the
 // parent, this patch, and siblings' interiors, which no CTA writes here, so
 // the CTA barrier between the steps orders everything that depends on them.
-__global__ void k_ghost2(const DevPatch* __restrict__ PT, const int* __restrict__ patches,
-                         const OverlapCopy* __restrict__ cps, const int2* __restrict__ ranges,
-                         int ipass) {
-  const DevPatch P = PT[patches[blockIdx.x]];
+// The body is shared with the batch's list kernel (kb_ghost): patch p's
+// transfers are cps[rg.x, rg.x + rg.y).  Every thread of the CTA calls it.
+__device__ __forceinline__ void ghost2_patch(const DevPatch* __restrict__ PT, int p,
+                                             const OverlapCopy* __restrict__ cps, int2 rg,
+                                             int ipass) {
+  const DevPatch P = PT[p];
   const DevPatch R = PT[P.parent];
   const int m1 = P.n[0], m2 = P.n[1];
   const int nring = 2 * (m1 + 2) + 2 * m2;
@@ -359,7 +361,6 @@ __global__ void k_ghost2(const DevPatch* __restrict__ PT, const int* __restrict_
   // sibling's record), so the warps run their chains side by side.  The
   // siblings are disjoint, so no ghost is written by two copies and the
   // order of the copies does not matter.
-  const int2 rg = ranges[blockIdx.x];
   const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   for (int c = rg.x + (int)(threadIdx.x >> 5); c < rg.x + rg.y; c += nw) {
     const OverlapCopy o = cps[c];
@@ -380,6 +381,12 @@ __global__ void k_ghost2(const DevPatch* __restrict__ PT, const int* __restrict_
   }
 }
 
+static __global__ void k_ghost2(const DevPatch* __restrict__ PT, const int* __restrict__ patches,
+                         const OverlapCopy* __restrict__ cps, const int2* __restrict__ ranges,
+                         int ipass) {
+  ghost2_patch(PT, patches[blockIdx.x], cps, ranges[blockIdx.x], ipass);
+}
+
 // The 3D ring cell g of a patch with m1 x m2 x m3 interior cells, in
 // order: the two k planes, then the 2D ring of each interior plane.
 __device__ __forceinline__ void ring3(int g, int m1, int m2, int m3, int& gi, int& gj, int& gk) {
@@ -398,10 +405,10 @@ __device__ __forceinline__ void ring3(int g, int m1, int m2, int m3, int& gi, in
 
 // SetGhost of a 3D refined level in one launch: k_ghost2's structure with
 // Interpolate3D (interp3_ghost), the 3D overlap boxes and the 3D face rule.
-__global__ void k_ghost3(const DevPatch* __restrict__ PT, const int* __restrict__ patches,
-                         const OverlapCopy* __restrict__ cps, const int2* __restrict__ ranges,
-                         int ipass) {
-  const DevPatch P = PT[patches[blockIdx.x]];
+__device__ __forceinline__ void ghost3_patch(const DevPatch* __restrict__ PT, int p,
+                                             const OverlapCopy* __restrict__ cps, int2 rg,
+                                             int ipass) {
+  const DevPatch P = PT[p];
   const DevPatch R = PT[P.parent];
   const int m1 = P.n[0], m2 = P.n[1], m3 = P.n[2];
   const int nring = 2 * (m1 + 2) * (m2 + 2) + m3 * (2 * (m1 + 2) + 2 * m2);
@@ -411,7 +418,6 @@ __global__ void k_ghost3(const DevPatch* __restrict__ PT, const int* __restrict_
     interp3_ghost(P, R, ipass, gi, gj, gk);
   }
   __syncthreads();
-  const int2 rg = ranges[blockIdx.x];
   for (int c = rg.x; c < rg.x + rg.y; ++c) {
     const OverlapCopy o = cps[c];
     const DevPatch S = PT[o.src];
@@ -432,14 +438,18 @@ __global__ void k_ghost3(const DevPatch* __restrict__ PT, const int* __restrict_
   }
 }
 
+static __global__ void k_ghost3(const DevPatch* __restrict__ PT, const int* __restrict__ patches,
+                         const OverlapCopy* __restrict__ cps, const int2* __restrict__ ranges,
+                         int ipass) {
+  ghost3_patch(PT, patches[blockIdx.x], cps, ranges[blockIdx.x], ipass);
+}
+
 // FillDownLevel for the solution (afas:241-310): parent%q(mb) = Restriction(q)
 // over the footprint tiles of a level (q only; ghosts of a physical parent by
 // write-through, those of a refined parent by its SetGhost afterwards).  The
 // restriction sums the children in Restriction2D/3D's order.
 template <int D>
-__global__ void __launch_bounds__(BLOCK_THREADS)
-    k_filldown(const DevPatch* __restrict__ PT, const Item* __restrict__ items) {
-  const Item it = items[blockIdx.x];
+__device__ __forceinline__ void filldown_item(const DevPatch* __restrict__ PT, const Item it) {
   const DevPatch C = PT[it.patch];
   const DevPatch P = PT[C.parent];
   const int jc = it.ty * TILE_Y + threadIdx.y + 1;
@@ -473,6 +483,12 @@ __global__ void __launch_bounds__(BLOCK_THREADS)
     if (P.wt && near_boundary(P, pi, pj, pk, D))
       write_through<double, D>(P, p0, p1, pi, pj, pk, val[0], val[1]);
   }
+}
+
+template <int D>
+__global__ void __launch_bounds__(BLOCK_THREADS)
+    k_filldown(const DevPatch* __restrict__ PT, const Item* __restrict__ items) {
+  filldown_item<D>(PT, items[blockIdx.x]);
 }
 
 }  // namespace bsam

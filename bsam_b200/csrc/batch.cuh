@@ -14,20 +14,35 @@
 // residual partials in the same order as last_block_total, so every
 // decision matches the single-problem engine bit for bit.
 #pragma once
+#include "amr.cuh"
 #include "bottom.cuh"
 #include "kernels.cuh"
 #include "mixed.cuh"
 
 namespace bsam {
 
-enum : int32_t { SLOT_IDLE = 0, SLOT_RUNNING = 1, SLOT_DONE = 2, SLOT_FAILED = 3 };
+// SLOT_REGRID: a refined hierarchy between two time steps, waiting for the
+// host to regrid it (bsam_batch_submit_amr); its records are inactive.
+enum : int32_t {
+  SLOT_IDLE = 0,
+  SLOT_RUNNING = 1,
+  SLOT_DONE = 2,
+  SLOT_FAILED = 3,
+  SLOT_REGRID = 4
+};
+
+// Slot kinds (SlotCfg::kind).
+enum : int32_t { SLOT_UNIFORM = 0, SLOT_AMR = 1 };
 
 // Host-owned per-slot configuration (rewritten whenever lists are rebuilt).
 struct SlotCfg {
   int32_t ib, ie;     // the slot's tiles in the master list (its residual partials)
   int32_t rec0, nrec; // its patch records
   int32_t master;     // record holding the FP64 state
-  int32_t nsteps, maxv, pad_;
+  int32_t nsteps, maxv;
+  int32_t kind;       // SLOT_UNIFORM: records in the batch's table, partials of
+                      // the master list; SLOT_AMR: records in the refined
+                      // hierarchies' table, partials of their master list
   double denom;       // nrvars * cells (L2Error's integralresult(2))
   double tol;
 };
@@ -259,22 +274,88 @@ __global__ void __launch_bounds__(BLOCK_THREADS, BATCH_LATENCY_MIN_BLOCKS)
   }
 }
 
+// ---- refined hierarchies (SLOT_AMR) ---------------------------------------------
+//
+// The V-cycle of a refined hierarchy runs the single-problem engine's
+// per-level kernels as list kernels over the records of every such problem
+// at one depth: colour passes (kb_relax), SetGhost of refined levels
+// (kb_ghost), restriction, the snapshot of partly covered parents (kb_snap),
+// coarse load, correction, FillDown (kb_filldown), all FP64.
+
+// SetGhost(level, ipass) of refined records, a CTA per record at a time:
+// items[b] = {record, first transfer, transfer count} into cps.
+template <int D>
+__global__ void __launch_bounds__(D == 2 ? 128 : 256)
+    kb_ghost(const DevPatch* __restrict__ PT, const Item* __restrict__ items,
+             const int* __restrict__ count, const OverlapCopy* __restrict__ cps, int ipass) {
+  const int n = *count;
+  for (int b = blockIdx.x; b < n; b += gridDim.x) {
+    const Item it = items[b];
+    if (!PT[it.patch].active) continue;  // uniform per CTA
+    if (D == 2) ghost2_patch(PT, it.patch, cps, make_int2(it.tx, it.ty), ipass);
+    else ghost3_patch(PT, it.patch, cps, make_int2(it.tx, it.ty), ipass);
+  }
+}
+
+// GetCoarseGhostPoints' source for the children of a partly covered parent:
+// qs = q over the parent's interior and ring, one row (j, k) per item.
+template <int D>
+__global__ void __launch_bounds__(BLOCK_THREADS)
+    kb_snap(const DevPatch* __restrict__ PT, const Item* __restrict__ items,
+            const int* __restrict__ count) {
+  const int n = *count;
+  const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+  const int nt = blockDim.x * blockDim.y;
+  for (int b = blockIdx.x; b < n; b += gridDim.x) {
+    const Item it = items[b];
+    const DevPatch P = PT[it.patch];
+    if (!P.active) continue;
+    for (int i = tid; i < P.n[0] + 2; i += nt) {
+      const int64_t c = cidx(P, i, it.ty, D == 3 ? it.tz : 0);
+#pragma unroll
+      for (int v = 0; v < 2; ++v) fld<double>(P.qs[v])[c] = fld<double>(P.q[v])[c];
+    }
+  }
+}
+
+// FillDownLevel for the solution over footprint tiles of refined records
+// (k_filldown's tile body).
+template <int D>
+__global__ void __launch_bounds__(BLOCK_THREADS)
+    kb_filldown(const DevPatch* __restrict__ PT, const Item* __restrict__ items,
+                const int* __restrict__ count, TileRuns R) {
+  const int n = *count;
+  for (int b = R.first(); b < n; b = R.next(b)) {
+    const Item it = items[b];
+    if (!PT[it.patch].active) continue;
+    filldown_item<D>(PT, it);
+  }
+}
+
 // End of a tick, one CTA per slot: ErrorAFAS of the slot from its partials,
 // then MultigridIterations' exit test and TakeTimeSteps' step advance.
 // Block of BLOCK_THREADS threads: the partial sums are added in the order of
 // last_block_total over the slot's own tiles.
+// Refined hierarchies (SLOT_AMR) keep their records in APT and their
+// partials in apartials; at the end of a time step that is not their last
+// they pause in SLOT_REGRID (records inactive) until the host has regridded
+// them and started the next step.
 __global__ void __launch_bounds__(BLOCK_THREADS)
-    k_batch_control(DevPatch* __restrict__ PT, const SlotCfg* __restrict__ cfg,
-                    SlotState* __restrict__ state, StepLog* __restrict__ log, int max_steps,
-                    SlotOut* __restrict__ out, const double* __restrict__ partials,
+    k_batch_control(DevPatch* __restrict__ PT, DevPatch* __restrict__ APT,
+                    const SlotCfg* __restrict__ cfg, SlotState* __restrict__ state,
+                    StepLog* __restrict__ log, int max_steps, SlotOut* __restrict__ out,
+                    const double* __restrict__ partials, const double* __restrict__ apartials,
                     BatchCtl* __restrict__ ctl, int nslots) {
   const int tid = threadIdx.x + blockDim.x * threadIdx.y;
   const int nthreads = blockDim.x * blockDim.y;
   for (int s = blockIdx.x; s < nslots; s += gridDim.x) {
     if (state[s].phase != SLOT_RUNNING) continue;  // uniform per CTA
     const SlotCfg C = cfg[s];
+    const bool amr = C.kind == SLOT_AMR;
+    DevPatch* T = amr ? APT : PT;
+    const double* part = amr ? apartials : partials;
     double acc = 0.0;
-    for (int b = tid; b < C.ie - C.ib; b += nthreads) acc += partials[C.ib + b];
+    for (int b = tid; b < C.ie - C.ib; b += nthreads) acc += part[C.ib + b];
     const double total = block_sum(acc);
     if (tid == 0) {
       SlotState S = state[s];
@@ -283,7 +364,7 @@ __global__ void __launch_bounds__(BLOCK_THREADS)
       S.vcycles += 1;
       const bool conv = r < C.tol;
       const bool finite = isfinite(r);
-      PT[C.master].newstep = 0;
+      if (!amr) PT[C.master].newstep = 0;
       if (conv || S.iters >= C.maxv || !finite) {
         if (S.step < max_steps) {
           StepLog L;
@@ -296,7 +377,10 @@ __global__ void __launch_bounds__(BLOCK_THREADS)
         S.iters = 0;
         if (!finite || S.step >= C.nsteps) {
           S.phase = finite ? SLOT_DONE : SLOT_FAILED;
-          for (int r2 = C.rec0; r2 < C.rec0 + C.nrec; ++r2) PT[r2].active = 0;
+          for (int r2 = C.rec0; r2 < C.rec0 + C.nrec; ++r2) T[r2].active = 0;
+        } else if (amr) {
+          S.phase = SLOT_REGRID;  // AMR(rootlevel) on the host, then the next step
+          for (int r2 = C.rec0; r2 < C.rec0 + C.nrec; ++r2) T[r2].active = 0;
         } else {
           PT[C.master].newstep = 1;  // CopyQToQold + source at the next tick
         }

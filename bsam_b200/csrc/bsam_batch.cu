@@ -39,6 +39,7 @@
 #include "batch.cuh"
 #include "bsam_types.h"
 #include "defect2.cuh"
+#include "engine_view.h"
 #include "fused2.cuh"
 
 using namespace bsam;
@@ -76,6 +77,24 @@ enum {
   NLIST = 3 + 6 * MAXD
 };
 
+// Lists of the refined hierarchies (SLOT_AMR), over the records of their own
+// table: finest-level tiles (ErrorAFAS), bottom-chain tops; per depth d (up
+// to MAXD, the depth below the last top one included): interior tiles
+// (colour passes, correction), footprint tiles (restriction, coarse load),
+// footprint tiles of refined records (FillDown), refined records with their
+// GhostOverlap transfers (SetGhost), rows of partly covered parents
+// (snapshot).
+enum {
+  A_MASTER = 0,
+  A_TOPS = 1,
+  A_FINE = 2,
+  A_COARSE = 2 + (MAXD + 1),
+  A_FILL = 2 + 2 * (MAXD + 1),
+  A_GHOST = 2 + 3 * (MAXD + 1),
+  A_SNAP = 2 + 4 * (MAXD + 1),
+  ANLIST = 2 + 5 * (MAXD + 1)
+};
+
 struct List {
   Item* d = nullptr;
   int cap = 0;            // device capacity in items
@@ -92,6 +111,15 @@ struct SlotPlan {
   bsam_batch_problem prob{};
   std::vector<DevPatch> recs;  // absolute record indices
   std::vector<CUtensorMap> maps;  // NMAPS per record (fused records only encoded)
+  // A refined hierarchy (bsam_batch_submit_amr): its driver and engine, the
+  // engine's current hierarchy, and where its records start in the refined
+  // hierarchies' table.
+  bool amr = false;
+  bsam_amr* drv = nullptr;
+  bsam_gpu* eng = nullptr;
+  EngineView view;
+  int arec0 = 0, chain = 0, nsteps = 0;
+  cudaEvent_t ready = nullptr;  // the engine's regrid and prologue are done
 };
 
 struct StageChunk {
@@ -148,6 +176,20 @@ struct bsam_batch {
   List lists[NLIST];
   int* d_counts = nullptr;
   std::vector<int> counts_dev;  // counts last uploaded
+  // Refined hierarchies: their records, transfers and lists (append-only;
+  // retired entries stay inactive until amr_compact rebuilds them).
+  std::vector<DevPatch> h_apt;
+  DevPatch* d_apt = nullptr;
+  int apt_cap = 0, apt_uploaded = 0;
+  std::vector<OverlapCopy> h_aovl;
+  OverlapCopy* d_aovl = nullptr;
+  int aovl_cap = 0, aovl_uploaded = 0;
+  List alists[ANLIST];
+  int* d_acounts = nullptr;
+  std::vector<int> acounts_dev;
+  double* d_apartials = nullptr;
+  int apartials_cap = 0;
+  int amr_live_recs = 0;  // records of the current blocks of resident refined slots
   // graph
   cudaGraphExec_t exec = nullptr;
   int cap_depth = 0;
@@ -575,9 +617,232 @@ void compact(bsam_batch* b) {
   }
   for (size_t s = 0; s < b->slots.size(); ++s) {
     b->slots[s].stale = false;
-    if (b->slots[s].used) append_items(b, (int)s);
+    if (b->slots[s].used && !b->slots[s].amr) append_items(b, (int)s);
   }
   b->cfg_dirty = true;
+}
+
+// ---- refined hierarchies ------------------------------------------------------
+
+// Depth layout of a refined hierarchy (its engine's current one, S.view):
+// the levels above the first root-chain level of at most bottom_cells cells
+// run list kernels at depths 0 .. ntop - 1 (depth = finestlevel - level);
+// that level heads the problem's bottom chain.
+int amr_plan(bsam_batch* b, SlotPlan& S) {
+  const EngineView& V = S.view;
+  const int nd = b->bp.ndims;
+  if (V.mixed) return fail(b, BSAM_ERR_UNSUPPORTED, "refined hierarchies run in FP64");
+  if (V.ndims != nd) return fail(b, BSAM_ERR_ARG, "problem ndims differs from the batch");
+  if (V.nsmoothingpasses != b->bp.nsmoothingpasses)
+    return fail(b, BSAM_ERR_ARG, "nsmoothingpasses differs from the batch's");
+  if (V.masters.empty() || V.levels.empty()) return fail(b, BSAM_ERR_STATE, "empty hierarchy");
+  int chain = V.minlevel - 1;
+  for (int l = 0; l >= V.minlevel; --l) {
+    const EngineLevelView& E = V.levels[l - V.minlevel];
+    if (E.patches.size() != 1)
+      return fail(b, BSAM_ERR_UNSUPPORTED, "levels at and below the root must be one patch");
+    if (cells_of(V.recs[E.patches[0]].n, nd) <= b->bp.bottom_cells) {
+      chain = l;
+      break;
+    }
+  }
+  if (chain < V.minlevel)
+    return fail(b, BSAM_ERR_UNSUPPORTED, "the coarsest level exceeds the bottom kernel's size");
+  if (V.finestlevel - chain > MAXD)
+    return fail(b, BSAM_ERR_UNSUPPORTED, "too many levels above the bottom");
+  if (chain - V.minlevel + 1 > BOTTOM_MAX_DEPTH)
+    return fail(b, BSAM_ERR_UNSUPPORTED, "bottom chain too deep");
+  S.chain = chain;
+  S.ntop = V.finestlevel - chain;
+  return BSAM_OK;
+}
+
+// Appends the records, transfers and tiles of refined slot s (S.view) and
+// points its configuration at them; active: the records run from the next
+// tick on.
+void amr_append(bsam_batch* b, int s, bool active) {
+  SlotPlan& S = b->slots[s];
+  const EngineView& V = S.view;
+  const int nd = b->bp.ndims;
+  const int r0 = (int)b->h_apt.size();
+  S.arec0 = r0;
+  for (DevPatch P : V.recs) {
+    if (P.parent >= 0) P.parent += r0;
+    P.problem = s;
+    P.active = active ? 1 : 0;
+    P.fused = 0;  // colour passes one launch each; q holds the state throughout
+    P.newstep = 0;
+    P.tmaps = nullptr;
+    P.twin = P.master = -1;
+    P.qb[0] = P.qb[1] = nullptr;
+    b->h_apt.push_back(P);
+  }
+  List* LA = b->alists;
+  SlotCfg& C = b->h_cfg[s];
+  C.kind = SLOT_AMR;
+  C.rec0 = r0;
+  C.nrec = (int)V.recs.size();
+  C.master = r0 + V.masters[0];
+  C.nsteps = S.nsteps;
+  C.maxv = V.maxvcycles;
+  C.denom = V.denom;
+  C.tol = V.qerrortol;
+  C.ib = (int)LA[A_MASTER].h.size();
+  for (int p : V.masters) tiles_for(r0 + p, V.recs[p].n, nd, LA[A_MASTER].h);
+  C.ie = (int)LA[A_MASTER].h.size();
+  LA[A_TOPS].h.push_back(Item{r0 + V.levels[S.chain - V.minlevel].patches[0], 0, 0, 0});
+  for (int l = V.finestlevel; l >= S.chain; --l) {
+    const EngineLevelView& E = V.levels[l - V.minlevel];
+    const int d = V.finestlevel - l;
+    if (l > S.chain) {
+      const int ob = (int)b->h_aovl.size();
+      if (E.amr)
+        for (OverlapCopy o : E.ovl) {
+          o.dst += r0;
+          o.src += r0;
+          b->h_aovl.push_back(o);
+        }
+      for (size_t k = 0; k < E.patches.size(); ++k) {
+        const int p = E.patches[k];
+        const DevPatch& P = V.recs[p];
+        tiles_for(r0 + p, P.n, nd, LA[A_FINE + d].h);
+        tiles_for(r0 + p, P.cn, nd, LA[A_COARSE + d].h);
+        if (E.amr) {
+          tiles_for(r0 + p, P.cn, nd, LA[A_FILL + d].h);
+          const int2 rg = k < E.range.size() ? E.range[k] : make_int2(0, 0);
+          LA[A_GHOST + d].h.push_back(Item{r0 + p, ob + rg.x, rg.y, 0});
+        }
+      }
+    }
+    // Parents their children do not cover: qs = q after the restriction
+    // into them (and their SetGhost), before the coarse load reads it.
+    if (E.snap)
+      for (int p : E.patches) {
+        const DevPatch& P = V.recs[p];
+        if (!P.qs[0]) continue;
+        const int nk = nd == 3 ? P.n[2] + 2 : 1;
+        for (int k = 0; k < nk; ++k)
+          for (int j = 0; j < P.n[1] + 2; ++j) LA[A_SNAP + d].h.push_back(Item{r0 + p, 0, j, k});
+      }
+  }
+  b->cfg_dirty = true;
+}
+
+// Rebuilds the refined hierarchies' table, transfers and lists from the
+// resident refined slots that have records (waits for the stream: the
+// mirrored phases are then exact, and only running slots' records are
+// active).  Everything is uploaded again by the next flush.
+int amr_compact(bsam_batch* b) {
+  CU(cudaStreamSynchronize(b->stream));
+  b->h_apt.clear();
+  b->h_aovl.clear();
+  for (auto& L : b->alists) {
+    L.h.clear();
+    L.uploaded = 0;
+  }
+  b->apt_uploaded = 0;
+  b->aovl_uploaded = 0;
+  for (size_t s = 0; s < b->slots.size(); ++s) {
+    SlotPlan& S = b->slots[s];
+    if (!S.used || !S.amr || S.view.recs.empty()) continue;
+    if (((volatile SlotOut*)b->h_out)[s].phase != SLOT_RUNNING) continue;
+    amr_append(b, (int)s, true);
+  }
+  return BSAM_OK;
+}
+
+int live_amr_records(bsam_batch* b) {
+  int n = 0;
+  for (auto& S : b->slots)
+    if (S.used && S.amr) n += (int)S.view.recs.size();
+  return n;
+}
+
+// Uploads the refined hierarchies' growth (records, transfers, lists,
+// counts); storage that must grow is reallocated after a compaction, and
+// the tick graph is captured again.
+int amr_flush(bsam_batch* b) {
+  if ((int)b->h_apt.size() > b->apt_cap || (int)b->h_aovl.size() > b->aovl_cap) {
+    int rc = amr_compact(b);
+    if (rc) return rc;
+    if ((int)b->h_apt.size() > b->apt_cap) {
+      if (b->d_apt) cudaFree(b->d_apt);
+      b->d_apt = nullptr;
+      int cap = std::max(1024, 2 * b->apt_cap);
+      while (cap < (int)b->h_apt.size()) cap *= 2;
+      if (cudaMalloc(&b->d_apt, sizeof(DevPatch) * cap) != cudaSuccess) {
+        b->apt_cap = 0;
+        return fail(b, BSAM_ERR_NOMEM, "record table allocation failed");
+      }
+      b->apt_cap = cap;
+      b->need_capture = true;
+    }
+    if ((int)b->h_aovl.size() > b->aovl_cap) {
+      if (b->d_aovl) cudaFree(b->d_aovl);
+      b->d_aovl = nullptr;
+      int cap = std::max(1024, 2 * b->aovl_cap);
+      while (cap < (int)b->h_aovl.size()) cap *= 2;
+      if (cudaMalloc(&b->d_aovl, sizeof(OverlapCopy) * cap) != cudaSuccess) {
+        b->aovl_cap = 0;
+        return fail(b, BSAM_ERR_NOMEM, "transfer table allocation failed");
+      }
+      b->aovl_cap = cap;
+      b->need_capture = true;
+    }
+  }
+  const int na = (int)b->h_apt.size();
+  if (b->apt_uploaded < na) {
+    const int rc = stage_copy(b, b->d_apt + b->apt_uploaded, b->h_apt.data() + b->apt_uploaded,
+                              sizeof(DevPatch) * (na - b->apt_uploaded));
+    if (rc) return rc;
+    b->apt_uploaded = na;
+  }
+  const int no = (int)b->h_aovl.size();
+  if (b->aovl_uploaded < no) {
+    const int rc = stage_copy(b, b->d_aovl + b->aovl_uploaded, b->h_aovl.data() + b->aovl_uploaded,
+                              sizeof(OverlapCopy) * (no - b->aovl_uploaded));
+    if (rc) return rc;
+    b->aovl_uploaded = no;
+  }
+  for (int l = 0; l < ANLIST; ++l) {
+    List& L = b->alists[l];
+    const int n = (int)L.h.size();
+    if (n > L.cap) {
+      CU(cudaStreamSynchronize(b->stream));
+      if (L.d) cudaFree(L.d);
+      L.d = nullptr;
+      int cap = std::max(256, L.cap);
+      while (cap < n) cap *= 2;
+      if (cudaMalloc(&L.d, sizeof(Item) * cap) != cudaSuccess) {
+        L.cap = 0;
+        return fail(b, BSAM_ERR_NOMEM, "work list allocation failed");
+      }
+      L.cap = cap;
+      L.uploaded = 0;
+      b->need_capture = true;
+      if (l == A_MASTER && cap > b->apartials_cap) {
+        if (b->d_apartials) cudaFree(b->d_apartials);
+        b->d_apartials = nullptr;
+        if (cudaMalloc(&b->d_apartials, sizeof(double) * cap) != cudaSuccess)
+          return fail(b, BSAM_ERR_NOMEM, "partials allocation failed");
+        b->apartials_cap = cap;
+      }
+    }
+    if (L.uploaded < n) {
+      const int rc = stage_copy(b, L.d + L.uploaded, L.h.data() + L.uploaded,
+                                sizeof(Item) * (n - L.uploaded));
+      if (rc) return rc;
+      L.uploaded = n;
+    }
+  }
+  std::vector<int> counts(ANLIST);
+  for (int l = 0; l < ANLIST; ++l) counts[l] = (int)b->alists[l].h.size();
+  if (counts != b->acounts_dev) {
+    const int rc = stage_copy(b, b->d_acounts, counts.data(), sizeof(int) * ANLIST);
+    if (rc) return rc;
+    b->acounts_dev = counts;
+  }
+  return BSAM_OK;
 }
 
 // ---- tick -------------------------------------------------------------------
@@ -621,6 +886,35 @@ void tick_t(bsam_batch* b, cudaGraphConditionalHandle handle, int in_graph) {
   const TileRuns RF{b->tuning.fused_chunk > 0 ? b->tuning.fused_chunk : kDefaultFusedChunk};
   // The staged defect reuses a patch's records along a run: longer runs.
   const TileRuns RD{kDefectRunFactor * R.chunk};
+  // Refined hierarchies: their own table, transfers and lists (FP64).
+  DevPatch* apt = b->d_apt;
+  const int* acnt = b->d_acounts;
+  const List* LA = b->alists;
+  const int gthreads = D == 2 ? 128 : 256;
+  auto agrid = [&](int l) {
+    const int cap = std::max(1, LA[l].cap);
+    const int lim = b->tuning.grid_ctas > 0 ? b->tuning.grid_ctas : 16 * b->nsm;
+    return std::max(1, std::min(cap, lim));
+  };
+  // SetGhost(level, ipass) of the refined records at depth d.
+  auto aghost = [&](int d, int ipass) {
+    if (d > MAXD || LA[A_GHOST + d].cap == 0) return;
+    kb_ghost<D><<<agrid(A_GHOST + d), gthreads, 0, s>>>(apt, LA[A_GHOST + d].d,
+                                                        acnt + A_GHOST + d, b->d_aovl, ipass);
+    ++n;
+  };
+  // LevelRelax of the refined hierarchies' records at depth d: each colour
+  // pass, then SetGhost of the refined ones (afas:536-545).
+  auto arelax = [&](int d) {
+    if (LA[A_FINE + d].cap == 0) return;
+    for (int pass = 0; pass < nu; ++pass)
+      for (int color = 0; color < 2; ++color) {
+        kb_relax<double, D><<<agrid(A_FINE + d), blk, 0, s>>>(apt, LA[A_FINE + d].d,
+                                                              acnt + A_FINE + d, color, R);
+        ++n;
+        aghost(d, color + 1);
+      }
+  };
   // LevelRelax of depth d for every running problem; dir selects the fused
   // stage's buffers (0: q -> qb before the correction, 1: qb -> q after).
   auto relax = [&](int d, int dir) {
@@ -687,6 +981,23 @@ void tick_t(bsam_batch* b, cudaGraphConditionalHandle handle, int in_graph) {
   }
   for (int d = 0; d < b->cap_depth; ++d) {
     relax(d, 0);
+    arelax(d);
+    if (LA[A_COARSE + d].cap > 0) {
+      // RestrictSolution, SetGhost of a refined parent level, the snapshot
+      // of partly covered parents, CoarseLoadingFunction (afas:503-509).
+      kb_restrict<double, D><<<agrid(A_COARSE + d), blk, 0, s>>>(apt, LA[A_COARSE + d].d,
+                                                                 acnt + A_COARSE + d, R);
+      ++n;
+      aghost(d + 1, 0);
+      if (LA[A_SNAP + d + 1].cap > 0) {
+        kb_snap<D><<<agrid(A_SNAP + d + 1), blk, 0, s>>>(apt, LA[A_SNAP + d + 1].d,
+                                                         acnt + A_SNAP + d + 1);
+        ++n;
+      }
+      kb_coarse_load<double, D><<<agrid(A_COARSE + d), blk, 0, s>>>(apt, LA[A_COARSE + d].d,
+                                                                    acnt + A_COARSE + d, R);
+      ++n;
+    }
     const int gc = grid_for(b, L_COARSE + d);
     if (L[L_RESTR + d].cap > 0) {
       const int gr = grid_for(b, L_RESTR + d);
@@ -710,6 +1021,11 @@ void tick_t(bsam_batch* b, cudaGraphConditionalHandle handle, int in_graph) {
     const int gb = std::max(1, std::min(cap, 4 * b->nsm));
     kb_bottom<D><<<gb, BATCH_BOTTOM_THREADS, 0, s>>>(pt, L[L_TOPS].d, cnt + L_TOPS, nu);
     ++n;
+    if (LA[A_TOPS].cap > 0) {
+      const int ga = std::max(1, std::min(LA[A_TOPS].cap, 4 * b->nsm));
+      kb_bottom<D><<<ga, BATCH_BOTTOM_THREADS, 0, s>>>(apt, LA[A_TOPS].d, acnt + A_TOPS, nu);
+      ++n;
+    }
   }
   for (int d = b->cap_depth - 1; d >= 0; --d) {
     if (D == 2) {
@@ -731,7 +1047,15 @@ void tick_t(bsam_batch* b, cudaGraphConditionalHandle handle, int in_graph) {
         kb_correct<double, D><<<gf, blk, 0, s>>>(pt, L[L_FINE + d].d, cnt + L_FINE + d, R);
     }
     ++n;
+    if (LA[A_FINE + d].cap > 0) {
+      // CorrectFine and SetGhost(level, 0) (afas:513-515).
+      kb_correct<double, D><<<agrid(A_FINE + d), blk, 0, s>>>(apt, LA[A_FINE + d].d,
+                                                              acnt + A_FINE + d, R);
+      ++n;
+      aghost(d, 0);
+    }
     relax(d, 1);
+    arelax(d);
   }
   if (b->mixed) {
     kb_update<D><<<grid_for(b, L_UPD), blk, 0, s>>>(pt, L[L_UPD].d, cnt + L_UPD, R);
@@ -741,10 +1065,24 @@ void tick_t(bsam_batch* b, cudaGraphConditionalHandle handle, int in_graph) {
     kb_resid<D><<<gm, blk, 0, s>>>(pt, L[L_MASTER].d, cnt + L_MASTER, b->d_partials, R);
     ++n;
   }
+  if (LA[A_MASTER].cap > 0) {
+    // FillDown(solution) after the V-cycle (afas:73), then ErrorAFAS on the
+    // finest level of each refined hierarchy.
+    for (int d = 0; d < b->cap_depth; ++d)
+      if (LA[A_FILL + d].cap > 0) {
+        kb_filldown<D><<<agrid(A_FILL + d), blk, 0, s>>>(apt, LA[A_FILL + d].d,
+                                                         acnt + A_FILL + d, R);
+        ++n;
+        aghost(d + 1, 0);
+      }
+    kb_resid<D><<<agrid(A_MASTER), blk, 0, s>>>(apt, LA[A_MASTER].d, acnt + A_MASTER,
+                                                b->d_apartials, R);
+    ++n;
+  }
   const int gctl = std::max(1, std::min(b->bp.max_slots, 2 * b->nsm));
-  k_batch_control<<<gctl, BLOCK_THREADS, 0, s>>>(pt, b->d_cfg, b->d_state, b->d_log,
+  k_batch_control<<<gctl, BLOCK_THREADS, 0, s>>>(pt, apt, b->d_cfg, b->d_state, b->d_log,
                                                  BSAM_BATCH_MAX_STEPS, b->d_out, b->d_partials,
-                                                 b->d_ctl, b->bp.max_slots);
+                                                 b->d_apartials, b->d_ctl, b->bp.max_slots);
   k_batch_cond<<<1, 1, 0, s>>>(b->d_ctl, handle, in_graph);
   n += 2;
   b->kernels_per_tick = n;
@@ -796,6 +1134,10 @@ int capture(bsam_batch* b) {
 // Uploads list growth, counts and slot configuration; re-captures the tick
 // graph when capacities or depths changed.
 int flush(bsam_batch* b) {
+  {
+    const int rc = amr_flush(b);
+    if (rc) return rc;
+  }
   for (int l = 0; l < NLIST; ++l) {
     List& L = b->lists[l];
     const int n = (int)L.h.size();
@@ -851,6 +1193,50 @@ int flush(bsam_batch* b) {
   return BSAM_OK;
 }
 
+// Regrids every refined hierarchy waiting between two time steps (phase
+// SLOT_REGRID as the completed work shows it; its records are inactive, so
+// no queued tick touches its fields) and starts its next step: the native
+// driver's AMR(rootlevel) and the start of MultigridIterations on the
+// problem's own engine and stream, then its new records and tiles, which
+// the batch's stream takes only after an event of the engine's.
+int amr_service(bsam_batch* b) {
+  for (size_t i = 0; i < b->slots.size(); ++i) {
+    SlotPlan& S = b->slots[i];
+    if (!S.used || !S.amr) continue;
+    volatile SlotOut* o = b->h_out + i;
+    if (o->phase != SLOT_REGRID) continue;
+    const int step = o->step, vcycles = o->vcycles;
+    int rc = bsam_amr_regrid(S.drv);
+    if (rc) return fail(b, rc, std::string("regrid: ") + bsam_gpu_last_error(S.eng));
+    rc = engine_prologue(S.eng);
+    if (rc) return fail(b, rc, std::string("step set-up: ") + bsam_gpu_last_error(S.eng));
+    rc = engine_view(S.eng, S.view);
+    if (rc) return fail(b, rc, "the engine holds no hierarchy");
+    rc = amr_plan(b, S);
+    if (rc) return rc;
+    CU(cudaEventRecord(S.ready, engine_stream(S.eng)));
+    CU(cudaStreamWaitEvent(b->stream, S.ready, 0));
+    if ((int)b->h_apt.size() > 2 * live_amr_records(b) + 4096) {
+      rc = amr_compact(b);
+      if (rc) return rc;
+    }
+    amr_append(b, (int)i, true);
+    SlotState st{SLOT_RUNNING, step, 0, vcycles};
+    rc = stage_copy(b, b->d_state + i, &st, sizeof(st));
+    if (rc) return rc;
+    o->phase = SLOT_RUNNING;
+  }
+  return BSAM_OK;
+}
+
+bool amr_waiting(bsam_batch* b) {
+  for (size_t i = 0; i < b->slots.size(); ++i)
+    if (b->slots[i].used && b->slots[i].amr &&
+        ((volatile SlotOut*)b->h_out)[i].phase == SLOT_REGRID)
+      return true;
+  return false;
+}
+
 }  // namespace
 
 extern "C" {
@@ -898,7 +1284,8 @@ int bsam_batch_create(bsam_batch** out, int device, const bsam_batch_params* p) 
             cudaMalloc(&b->d_ctl, sizeof(BatchCtl)) == cudaSuccess &&
             cudaMalloc(&b->d_status, sizeof(DevStatus)) == cudaSuccess &&
             cudaMallocHost(&b->h_status, sizeof(DevStatus)) == cudaSuccess &&
-            cudaMalloc(&b->d_counts, sizeof(int) * NLIST) == cudaSuccess;
+            cudaMalloc(&b->d_counts, sizeof(int) * NLIST) == cudaSuccess &&
+            cudaMalloc(&b->d_acounts, sizeof(int) * ANLIST) == cudaSuccess;
   if (ok) ok = cudaHostGetDevicePointer((void**)&b->d_out, b->h_out, 0) == cudaSuccess;
   if (ok)
     ok = cudaFuncSetAttribute(kb_smooth2<float, true, 3>,
@@ -934,8 +1321,10 @@ int bsam_batch_create(bsam_batch** out, int device, const bsam_batch_params* p) 
   cudaMemsetAsync(b->d_state, 0, sizeof(SlotState) * ns, b->stream);  // SLOT_IDLE
   cudaMemsetAsync(b->d_ctl, 0, sizeof(BatchCtl), b->stream);
   cudaMemsetAsync(b->d_counts, 0, sizeof(int) * NLIST, b->stream);
+  cudaMemsetAsync(b->d_acounts, 0, sizeof(int) * ANLIST, b->stream);
   cudaMemsetAsync(b->d_status, 0, sizeof(DevStatus), b->stream);
   b->counts_dev.assign(NLIST, 0);
+  b->acounts_dev.assign(ANLIST, 0);
   if (cudaStreamSynchronize(b->stream) != cudaSuccess) {
     bsam_batch_destroy(b);
     return BSAM_ERR_CUDA;
@@ -955,6 +1344,14 @@ int bsam_batch_destroy(bsam_batch* b) {
   }
   for (auto& L : b->lists)
     if (L.d) cudaFree(L.d);
+  for (auto& L : b->alists)
+    if (L.d) cudaFree(L.d);
+  for (auto& S : b->slots)
+    if (S.ready) cudaEventDestroy(S.ready);
+  if (b->d_apt) cudaFree(b->d_apt);
+  if (b->d_aovl) cudaFree(b->d_aovl);
+  if (b->d_acounts) cudaFree(b->d_acounts);
+  if (b->d_apartials) cudaFree(b->d_apartials);
   for (auto& c : b->chunks)
     if (c.ev) b->free_events.push_back(c.ev);
   std::sort(b->free_events.begin(), b->free_events.end());
@@ -1051,6 +1448,9 @@ static int reserve(bsam_batch* b, const bsam_batch_problem* prob, int* slot) {
   S.used = true;
   S.stale = false;
   S.off = off;
+  S.amr = false;
+  S.drv = nullptr;
+  S.eng = nullptr;
   *slot = s;
   return BSAM_OK;
 }
@@ -1060,6 +1460,7 @@ static void enlist(bsam_batch* b, int s, const bsam_batch_problem* prob) {
   const SlotPlan& S = b->slots[s];
   const int rec0 = s * RMAX;
   SlotCfg& C = b->h_cfg[s];
+  C.kind = SLOT_UNIFORM;
   C.rec0 = rec0;
   C.nrec = S.nrec;
   C.master = rec0 + S.master;
@@ -1302,6 +1703,69 @@ int bsam_batch_submit_seeded_many(bsam_batch* b, int n, const bsam_batch_problem
   return admit_many(b, n, probs, nullptr, init.data(), slots);
 }
 
+int bsam_batch_submit_amr(bsam_batch* b, bsam_amr* a, int nsteps, int* slot) {
+  if (!b || !a || !slot || nsteps < 1 || nsteps > BSAM_BATCH_MAX_STEPS) return BSAM_ERR_ARG;
+  CU(cudaSetDevice(b->device));
+  bsam_gpu* h = amr_engine(a);
+  if (engine_device(h) != b->device)
+    return fail(b, BSAM_ERR_ARG, "the driver's engine is on another device");
+  for (const auto& S : b->slots)
+    if (S.used && S.amr && S.drv == a) return fail(b, BSAM_ERR_STATE, "driver already in the batch");
+  {
+    // The hierarchy as it stands must fit the batch (checked again after
+    // every regrid).
+    SlotPlan probe;
+    int rc = engine_view(h, probe.view);
+    if (rc) return fail(b, rc, "the driver's engine holds no hierarchy");
+    rc = amr_plan(b, probe);
+    if (rc) return rc;
+  }
+  int s = -1;
+  bool any_stale = false;
+  for (size_t i = 0; i < b->slots.size(); ++i) {
+    if (b->slots[i].used) continue;
+    if (!b->slots[i].stale) {
+      s = (int)i;
+      break;
+    }
+    any_stale = true;
+  }
+  if (s < 0 && !any_stale) return fail(b, BSAM_ERR_NOMEM, "no free slot");
+  if (s < 0) {
+    compact(b);
+    for (size_t i = 0; i < b->slots.size(); ++i)
+      if (!b->slots[i].used) {
+        s = (int)i;
+        break;
+      }
+  }
+  SlotPlan& S = b->slots[s];
+  S = SlotPlan{};
+  S.used = true;
+  S.amr = true;
+  S.drv = a;
+  S.eng = h;
+  S.nsteps = nsteps;
+  S.prob.nsteps = nsteps;
+  CU(cudaEventCreateWithFlags(&S.ready, cudaEventDisableTiming));
+  SlotCfg& C = b->h_cfg[s];
+  C = SlotCfg{};
+  C.kind = SLOT_AMR;
+  C.nsteps = nsteps;
+  b->cfg_dirty = true;
+  // Waits between two time steps from the start: the first step's regrid
+  // runs at the next advance.
+  SlotState st{SLOT_REGRID, 0, 0, 0};
+  const int rc = stage_copy(b, b->d_state + s, &st, sizeof(st));
+  if (rc) return rc;
+  volatile SlotOut* o = b->h_out + s;
+  o->step = 0;
+  o->vcycles = 0;
+  o->phase = SLOT_REGRID;
+  *slot = s;
+  return BSAM_OK;
+}
+
 int bsam_batch_busy(bsam_batch* b) {
   if (!b) return BSAM_ERR_ARG;
   cudaSetDevice(b->device);
@@ -1314,7 +1778,9 @@ int bsam_batch_busy(bsam_batch* b) {
 int bsam_batch_advance(bsam_batch* b, int max_ticks) {
   if (!b || max_ticks < 1) return BSAM_ERR_ARG;
   CU(cudaSetDevice(b->device));
-  int rc = flush(b);
+  int rc = amr_service(b);
+  if (rc) return rc;
+  rc = flush(b);
   if (rc) return rc;
   k_batch_budget<<<1, 1, 0, b->stream>>>(b->d_ctl, max_ticks);
   CU(cudaGetLastError());
@@ -1418,7 +1884,7 @@ int bsam_batch_run(bsam_batch* b) {
     if (rc) return rc;
     rc = bsam_batch_sync(b);
     if (rc) return rc;
-    if (running_slots(b) == 0) return BSAM_OK;
+    if (running_slots(b) == 0 && !amr_waiting(b)) return BSAM_OK;
   }
   return fail(b, BSAM_ERR_STATE, "batch did not finish");
 }
@@ -1454,6 +1920,33 @@ int bsam_batch_collect(bsam_batch* b, int slot, double* q, bsam_step_result* ste
   SlotPlan& S = b->slots[slot];
   const int ph = ((volatile SlotOut*)b->h_out)[slot].phase;
   if (ph != SLOT_DONE && ph != SLOT_FAILED) return fail(b, BSAM_ERR_STATE, "problem not finished");
+  if (S.amr) {
+    // A refined hierarchy: its state stays in its engine (read it there, or
+    // through q / mass here); the slot is released.
+    std::vector<StepLog> lg(S.nsteps);
+    CU(cudaMemcpy(lg.data(), b->d_log + (int64_t)slot * BSAM_BATCH_MAX_STEPS,
+                  sizeof(StepLog) * lg.size(), cudaMemcpyDeviceToHost));
+    const int done = ((volatile SlotOut*)b->h_out)[slot].step;
+    if (steps)
+      for (int i = 0; i < S.nsteps; ++i) {
+        steps[i].nvcycles = i < done ? lg[i].nv : 0;
+        steps[i].converged = i < done ? lg[i].conv : 0;
+        steps[i].residual = i < done ? lg[i].res : NAN;
+      }
+    int rc = BSAM_OK;
+    if (q) {
+      const EngineView& V = S.view;
+      rc = bsam_gpu_get_field(S.eng, V.levels[0 - V.minlevel].patches[0], BSAM_FIELD_Q, q);
+    }
+    if (!rc && mass) rc = bsam_gpu_mass(S.eng, mass);
+    if (S.ready) cudaEventDestroy(S.ready);
+    S = SlotPlan{};  // its tiles are inactive records of the refined lists only
+    ((volatile SlotOut*)b->h_out)[slot].phase = SLOT_IDLE;
+    b->h_cfg[slot] = SlotCfg{};
+    b->cfg_dirty = true;
+    if (rc) return fail(b, rc, "reading the refined hierarchy's engine failed");
+    return ph == SLOT_FAILED ? fail(b, BSAM_ERR_DIVERGED, "residual is not finite") : BSAM_OK;
+  }
   const int nd = b->bp.ndims;
   const int rec_master = slot * RMAX + S.master;
   const DevPatch& M = S.recs[S.master];
@@ -1525,6 +2018,8 @@ int bsam_batch_collect_many(bsam_batch* b, int n, const int* slots, double* cons
     const int s = slots[k];
     if (s < 0 || s >= (int)b->slots.size() || !b->slots[s].used)
       return fail(b, BSAM_ERR_ARG, "slot not resident");
+    if (b->slots[s].amr)
+      return fail(b, BSAM_ERR_ARG, "refined hierarchies are collected one at a time");
     for (int k2 = 0; k2 < k; ++k2)
       if (slots[k2] == s) return fail(b, BSAM_ERR_ARG, "slot listed twice");
   }

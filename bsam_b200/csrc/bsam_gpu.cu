@@ -35,6 +35,7 @@
 #include "amr.cuh"
 #include "regrid.cuh"
 #include "stats.cuh"
+#include "engine_view.h"
 
 using namespace bsam;
 
@@ -128,6 +129,12 @@ struct bsam_gpu {
   bool amr = false;                  // levels above the root exist
   int* d_plist = nullptr;            // patch lists of the refined levels
   OverlapCopy* d_ovl = nullptr;      // their GhostOverlap transfers
+  // Host copies of the refined levels' patch lists and transfers grouped by
+  // destination, with per level the span of each (engine_view).
+  std::vector<int> h_plist;
+  std::vector<OverlapCopy> h_ovl_by_dst;
+  std::vector<int2> h_ovl_range;
+  std::vector<std::pair<int, int>> h_span_plist, h_span_ovl;
   int nmaster = 0;
   Item* d_items = nullptr;
   CUtensorMap* d_tmaps = nullptr;    // TMA maps of the fused levels' fields
@@ -546,6 +553,58 @@ bool encode_field_map(CUtensorMap* m, const DevPatch& P, const void* field, int 
 }
 
 }  // namespace
+
+namespace bsam {
+
+int engine_view(bsam_gpu* h, EngineView& v) {
+  if (!h || !h->have_hierarchy) return BSAM_ERR_STATE;
+  v.ndims = h->rp.ndims;
+  v.minlevel = h->minlevel;
+  v.finestlevel = h->finestlevel;
+  v.nsmoothingpasses = h->rp.nsmoothingpasses;
+  v.maxvcycles = h->rp.maxvcycles;
+  v.mixed = h->mixed;
+  v.qerrortol = h->rp.qerrortol;
+  v.denom = h->denom;
+  v.recs = h->hp;
+  v.masters = h->masters;
+  v.levels.assign(h->levels.size(), EngineLevelView{});
+  for (size_t li = 0; li < h->levels.size(); ++li) {
+    const LevelPlan& L = h->levels[li];
+    EngineLevelView& E = v.levels[li];
+    E.level = L.level;
+    E.amr = L.amr;
+    E.snap = L.snap;
+    E.patches = L.patches;
+    if (!L.amr || li >= h->h_span_plist.size()) continue;
+    const auto sp = h->h_span_plist[li], so = h->h_span_ovl[li];
+    E.ovl.assign(h->h_ovl_by_dst.begin() + so.first,
+                 h->h_ovl_by_dst.begin() + so.first + so.second);
+    E.range.assign(h->h_ovl_range.begin() + sp.first,
+                   h->h_ovl_range.begin() + sp.first + sp.second);
+  }
+  return BSAM_OK;
+}
+
+int engine_prologue(bsam_gpu* h) {
+  if (!h || !h->have_hierarchy) return BSAM_ERR_STATE;
+  if (h->mixed) return fail(h, BSAM_ERR_UNSUPPORTED, "the batch runs refined hierarchies in FP64");
+  CU(cudaSetDevice(h->device));
+  if (h->amr) filldown(h);
+  if (h->rp.ndims == 2)
+    k_source<double, 2><<<h->nstate, block_dim(), 0, h->stream>>>(h->d_patches, h->d_state);
+  else
+    k_source<double, 3><<<h->nstate, block_dim(), 0, h->stream>>>(h->d_patches, h->d_state);
+  ++h->stats.launches;
+  CU(cudaGetLastError());
+  return BSAM_OK;
+}
+
+cudaStream_t engine_stream(bsam_gpu* h) { return h ? h->stream : nullptr; }
+
+int engine_device(bsam_gpu* h) { return h ? h->device : -1; }
+
+}  // namespace bsam
 
 extern "C" {
 
@@ -1033,6 +1092,11 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
     }
     if (at != o0 + no) return fail(h, BSAM_ERR_ARG, "an overlap names no patch of its level");
   }
+  h->h_plist = plist_all;
+  h->h_ovl_by_dst = ovl_by_dst;
+  h->h_ovl_range = ovl_range;
+  h->h_span_plist = span_plist;
+  h->h_span_ovl = span_ovl;
   h->max_items = std::max(1, h->nmaster);
   for (size_t li = 0; li < nl; ++li) {
     LevelPlan& L = h->levels[li];

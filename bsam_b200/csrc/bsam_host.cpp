@@ -580,13 +580,17 @@ int bsam_amr_create(bsam_amr** out, bsam_gpu* h, int ndims, const bsam_regrid_pa
   return BSAM_OK;
 }
 
-int bsam_amr_step(bsam_amr* a, int* nvcycles, double* residual, int* converged) {
-  if (!a) return BSAM_ERR_ARG;
+}  // extern "C"
+
+namespace {
+
+// AMR(rootlevel) and what TakeTimeSteps does before MultigridIterations
+// (lib/bsamroutines.f90:646-661): the first half of a time step.
+int amr_regrid_part(bsam_amr* a, PhaseClock& clk) {
   bsam_gpu* h = a->h;
   const int nd = a->nd;
   const std::vector<bsam_patch_desc> start = a->table;
   std::vector<bsam_patch_desc> table = a->table;
-  PhaseClock clk(a->t);
   // The old grids of the refined levels as TransferValues reads them.
   int rc = bsam_gpu_stash(h);
   if (rc) return rc;
@@ -713,7 +717,31 @@ int bsam_amr_step(bsam_amr* a, int* nvcycles, double* residual, int* converged) 
     if (rc) return rc;
     a->firstamr = false;
   }
-  rc = bsam_gpu_copy_q_to_qold(h);
+  return bsam_gpu_copy_q_to_qold(h);
+}
+
+}  // namespace
+
+namespace bsam {
+// The engine a native AMR driver steps (declared in engine_view.h, which
+// holds device code and is not included by host-compiled sources).
+bsam_gpu* amr_engine(bsam_amr* a);
+bsam_gpu* amr_engine(bsam_amr* a) { return a ? a->h : nullptr; }
+}  // namespace bsam
+
+extern "C" {
+
+int bsam_amr_regrid(bsam_amr* a) {
+  if (!a) return BSAM_ERR_ARG;
+  PhaseClock clk(a->t);
+  return amr_regrid_part(a, clk);
+}
+
+int bsam_amr_step(bsam_amr* a, int* nvcycles, double* residual, int* converged) {
+  if (!a) return BSAM_ERR_ARG;
+  bsam_gpu* h = a->h;
+  PhaseClock clk(a->t);
+  int rc = amr_regrid_part(a, clk);
   if (rc) return rc;
   int nv = 0, conv = 0;
   double res = 0.0;

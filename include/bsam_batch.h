@@ -44,6 +44,8 @@ typedef struct bsam_batch bsam_batch;
 #define BSAM_SLOT_RUNNING 1
 #define BSAM_SLOT_DONE 2
 #define BSAM_SLOT_FAILED 3 /* non-finite residual */
+#define BSAM_SLOT_REGRID 4 /* refined hierarchy between two time steps, to be
+                              regridded at the next bsam_batch_advance */
 
 typedef struct {
   int32_t ndims;            /* 2 or 3: every problem of the batch */
@@ -160,6 +162,24 @@ int bsam_batch_submit_many(bsam_batch* b, int n, const bsam_batch_problem* probl
 int bsam_batch_submit_seeded_many(bsam_batch* b, int n, const bsam_batch_problem* problems,
                                   const uint64_t* seeds, const double* cbar,
                                   const double* amp, int* slots);
+
+/* Hands the next nsteps time steps of a refined (AMR) hierarchy to the
+ * batch: the native driver `a` (bsam_amr_create, FP64 engine on the batch's
+ * device, same ndims and nsmoothingpasses) keeps the problem's fields and
+ * regrids it before every step (bsam_amr_regrid, at the bsam_batch_advance
+ * after the step before ends), and the batch runs each step's
+ * MultigridIterations in the launches it issues for all its problems: one
+ * launch per V-cycle stage and depth covers the patches of every refined
+ * hierarchy resident (colour passes, SetGhost of refined levels,
+ * restriction, coarse load, correction, FillDown, ErrorAFAS), so many such
+ * problems share the launches that one problem alone leaves latency-bound.
+ * The engine's own run parameters (maxvcycles, qerrortol) apply.  Results
+ * are bitwise those of nsteps calls of bsam_amr_step.  Until the slot is
+ * collected (bsam_batch_collect; collect_many refuses it), the caller must
+ * not use the driver or its engine.  Occupies a slot but no pool memory.
+ * Replaces the time-step loop of TakeTimeSteps (lib/bsamroutines.f90:
+ * 632-723) for that problem; no reference counterpart for the batching. */
+int bsam_batch_submit_amr(bsam_batch* b, bsam_amr* a, int nsteps, int* slot);
 
 /* 1 while work queued on the batch's stream is still executing, 0 when idle
  * (does not wait). */

@@ -124,6 +124,12 @@ int bsam_amr_create(bsam_amr** a, bsam_gpu* h, int ndims, const bsam_regrid_para
  * MakeNewGrid, InitFields and TransferValues on the device -- then FillDown
  * on the first step, CopyQToQold and MultigridIterations. */
 int bsam_amr_step(bsam_amr* a, int* nvcycles, double* residual, int* converged);
+/* The first half of bsam_amr_step: everything before MultigridIterations
+ * (AMR(rootlevel), FillDown on the first step, CopyQToQold).  The batched
+ * engine calls it between the time steps it runs for the driver
+ * (bsam_batch_submit_amr); bsam_amr_step is this call followed by
+ * bsam_gpu_multigrid_iterations. */
+int bsam_amr_regrid(bsam_amr* a);
 /* The current patch table (after the last step's regrid): returns the count
  * and copies up to maxn records into out (out may be NULL). */
 int bsam_amr_table(const bsam_amr* a, bsam_patch_desc* out, int maxn);

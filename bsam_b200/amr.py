@@ -731,11 +731,17 @@ class AmrRun:
         _check(lib().bsam_amr_step(self.a, ctypes.byref(nv), ctypes.byref(res),
                                    ctypes.byref(conv)), self.b.h, "amr_step")
         self.converged = conv.value
+        self.refresh()
+        return nv.value, res.value
+
+    def refresh(self):
+        """Re-reads the driver's patch table (after steps run elsewhere, such
+        as in a batch)."""
+        from . import PatchDesc, lib
         n = lib().bsam_amr_table(self.a, None, 0)
         arr = (PatchDesc * n)()
         lib().bsam_amr_table(self.a, arr, n)
         self._table, self.npatch, self._descs = arr, n, None
-        return nv.value, res.value
 
     def stats(self):
         return self.b.after_step_stats()
@@ -803,21 +809,28 @@ def request_params(n_root: int, eps: float, maxlevel: int) -> RegridParams:
                         desfill=[0.9] * maxlevel, mgp=[8] * maxlevel)
 
 
+def request_run(prob, device: int = 0) -> "AmrRun":
+    """The native driver of a served 2D request with refined levels
+    (prob.maxlevel >= 1): the circular drop seeded by prob.seed on a
+    prob.mx[0]^2 root with the request's regridding settings."""
+    n = int(prob.mx[0])
+    hier = build(n, [], eps=float(prob.eps), dt=float(prob.dt), qerrortol=float(prob.qerrortol),
+                 field="drop", seed=int(prob.seed), maxvcycles=int(prob.maxvcycles))
+    return AmrRun(hier, request_params(n, float(prob.eps), int(prob.maxlevel)), device)
+
+
 def solve_request(prob, device: int = 0, keep_q: bool = False) -> dict:
     """One served 2D request with refined levels (prob.maxlevel >= 1): the
     circular drop seeded by prob.seed on a prob.mx[0]^2 root, prob.nsteps
     time steps regridded every step in the native driver (FP64).  Returns the
     per-step V-cycles, residuals and convergence flags, the largest patch
     count, and (keep_q) the final q of every patch on a level >= 0."""
-    n = int(prob.mx[0])
-    hier = build(n, [], eps=float(prob.eps), dt=float(prob.dt), qerrortol=float(prob.qerrortol),
-                 field="drop", seed=int(prob.seed), maxvcycles=int(prob.maxvcycles))
     nsteps = int(prob.nsteps)
     nvc = np.zeros(nsteps, dtype=np.int32)
     res = np.zeros(nsteps)
     conv = np.zeros(nsteps, dtype=np.int32)
     most = 0
-    with AmrRun(hier, request_params(n, float(prob.eps), int(prob.maxlevel)), device) as r:
+    with request_run(prob, device) as r:
         for k in range(nsteps):
             nvc[k], res[k] = r.step()
             conv[k] = r.converged

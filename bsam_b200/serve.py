@@ -10,10 +10,11 @@ are advanced together, a few V-cycle ticks per engine launch; every loop the
 server collects what has finished and admits what now fits, so requests that
 arrive while others are on the GPU join the running batch.
 
-2D requests with refined levels (regridded every step) go to a small pool
-of worker threads instead, each solving one request at a time through the
-native AMR driver on its own engine handle and stream (amr.solve_request),
-beside the batches.
+2D requests with refined levels (regridded every step) run in a third batch
+engine (FP64, bsam_batch_submit_amr): worker threads build each request's
+native AMR driver (its hierarchy and engine, amr.request_run), the server
+admits the ready drivers into that batch, which runs the V-cycles of all of
+them in shared launches and regrids each one between its time steps.
 
 A result depends only on its own request: the batch engine computes every
 problem exactly as it would alone, and an AMR request is solved exactly as
@@ -58,7 +59,7 @@ class Server:
     def __init__(self, pool_bytes: int, precision: int = BB.PREC_MIXED, max_slots: int = 256,
                  share_2d: float = 0.5, ticks: int = 4, qerrortol: float = 1e-8,
                  maxvcycles: int = 20, device: int = 0, keep_q: bool = False,
-                 amr_workers: int = 2):
+                 amr_workers: int = 2, amr_slots: int = 64):
         p2 = int(pool_bytes * share_2d)
         self.engines = {
             2: BB.Batch(2, precision=precision, max_slots=max_slots, pool_bytes=p2,
@@ -67,6 +68,11 @@ class Server:
                         pool_bytes=pool_bytes - p2, qerrortol=qerrortol,
                         maxvcycles=maxvcycles, device=device),
         }
+        # Refined requests: their fields live in their own engines, so this
+        # batch needs slots, not pool memory.
+        self.amr_engine = BB.Batch(2, precision=BB.PREC_FP64, max_slots=amr_slots,
+                                   pool_bytes=1 << 20, qerrortol=qerrortol,
+                                   maxvcycles=maxvcycles, device=device)
         self.ticks = ticks
         self.keep_q = keep_q
         self.device = device
@@ -75,6 +81,7 @@ class Server:
     def close(self):
         for e in self.engines.values():
             e.close()
+        self.amr_engine.close()
 
     def __enter__(self):
         return self
@@ -101,11 +108,15 @@ class Server:
         t0 = time.perf_counter()
         now = 0.0
         running = {2: 0, 3: 0}
-        # AMR requests: FIFO to the worker threads.
+        # AMR requests: FIFO to the worker threads, which build their drivers
+        # (host fields, engine, hierarchy) and hand them back ready.
         amr_q: queue.Queue = queue.Queue()
+        amr_ready: deque = deque()
+        amr_inflight = {}
         amr_left = [sum(1 for r in reqs if getattr(r.prob, "maxlevel", 0) >= 1)]
         errors = []
         lock = threading.Lock()
+        ae = self.amr_engine
 
         def worker():
             while True:
@@ -113,13 +124,11 @@ class Server:
                 if r is None:
                     return
                 try:
-                    r.admitted = time.perf_counter() - t0
-                    r.result = AMR.solve_request(r.prob, self.device, keep_q=self.keep_q)
-                    r.finished = time.perf_counter() - t0
+                    run = AMR.request_run(r.prob, self.device)
+                    with lock:
+                        amr_ready.append((r, run))
                 except Exception as exc:  # reported by serve() after the stream
                     errors.append(exc)
-                with lock:
-                    amr_left[0] -= 1
 
         threads = [threading.Thread(target=worker, daemon=True)
                    for _ in range(self.amr_workers if amr_left[0] else 0)]
@@ -153,10 +162,27 @@ class Server:
                         running[nd] += 1
                 keep.extend(r for r in pending if r.admitted is None)
                 pending = keep
-            # Keep every engine with running problems busy.
+            # Refined requests whose drivers are ready join their batch.
+            while True:
+                with lock:
+                    item = amr_ready.popleft() if amr_ready else None
+                if item is None:
+                    break
+                r, run = item
+                s = ae.submit_amr(run, int(r.prob.nsteps))
+                if s is None:
+                    with lock:
+                        amr_ready.appendleft(item)
+                    break
+                r.admitted = time.perf_counter() - t0
+                amr_inflight[s] = (r, run)
+            # Keep every engine with running problems busy (advancing the
+            # refined requests' batch also regrids those between two steps).
             for nd, e in self.engines.items():
                 if running[nd] and not e.busy():
                     e.advance(self.ticks)
+            if amr_inflight and not ae.busy():
+                ae.advance(self.ticks)
             # Completions.
             done_any = False
             for nd, e in self.engines.items():
@@ -173,6 +199,19 @@ class Server:
                     r.result = res
                     running[nd] -= 1
                 done_any = True
+            if amr_inflight:
+                for s in ae.poll():
+                    r, run = amr_inflight.pop(s)
+                    res = ae.collect_amr(s)
+                    r.finished = time.perf_counter() - t0
+                    if self.keep_q:
+                        res["q"] = run.state()
+                        res["descs"] = list(run.descs)
+                    res["patches_final"] = run.npatch
+                    run.close()
+                    r.result = res
+                    amr_left[0] -= 1
+                    done_any = True
             if not done_any and not pending and not inflight and nxt < len(reqs):
                 wait = reqs[nxt].arrival - (time.perf_counter() - t0)
                 if wait > 0:

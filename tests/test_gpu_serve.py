@@ -81,9 +81,11 @@ def test_serve_admission_waits_for_memory(gpu_lib):
 
 
 def test_serve_amr_requests_same_alone(gpu_lib):
-    """2D requests with refined levels run beside the batches (worker threads,
-    native AMR driver): each result equals the same request solved alone, bit
-    for bit, and the batch requests of the mix still converge."""
+    """2D requests with refined levels run in their own batch beside the
+    uniform ones (drivers built by worker threads, V-cycles in shared
+    launches, regridded between steps): each result equals the same request
+    solved alone by its native driver, bit for bit, and the batch requests of
+    the mix still converge."""
     stream = small_stream(8, rate=3000.0)
     amr_ids = (1, 4, 6)
     for rid in amr_ids:

@@ -659,6 +659,39 @@ def run_ours(args, world, rank, local):
                 "refined_cells_mean": statistics.mean(refined),
                 "steps_with_refinement": sum(1 for x in pats if x > 0),
                 "tag_threshold": "|grad phi| > %.2f/eps" % (0.25 if sustained else 0.5)}
+        # The same AMR workload batched: 32 problems (seeds 2..33, sustained
+        # refinement) whose V-cycles run in one FP64 batch's shared launches,
+        # each regridded by its own native driver between its steps
+        # (bsam_batch_submit_amr); host wall clock over 5 steps of all of
+        # them, after one warm-up step each (graph capture, first regrid).
+        from bsam_b200 import batch as BB
+        nb, nst = 32, 5
+        runs = [AMR.AmrRun(*AMR.config2(sustained=True, seed=2 + i), device=local)
+                for i in range(nb)]
+        try:
+            with BB.Batch(2, precision=BB.PREC_FP64, max_slots=nb, pool_bytes=1 << 20,
+                          device=local) as ab:
+                for steps, timed in ((1, False), (nst, True)):
+                    slots = [ab.submit_amr(r, steps) for r in runs]
+                    torch.cuda.synchronize()
+                    t0 = time.perf_counter()
+                    ab.run()
+                    dt_ = time.perf_counter() - t0
+                    res = [ab.collect_amr(s) for s in slots]
+                st = ab.stats()
+            extra["cfg2_amr_batched"] = {
+                "problems": nb, "steps_each": nst, "steps_per_s": nb * nst / dt_,
+                "over_one_at_a_time": (nb * nst / dt_) / extra["cfg2_amr_sustained"]["steps_per_s"],
+                "vcycles_mean": float(np.mean([x["nvcycles"].mean() for x in res])),
+                "all_converged": bool(all(int(x["converged"].min()) == 1 for x in res)),
+                "refined_patches_mean": float(np.mean([int((r.table_array()["level"] >= 1).sum())
+                                                       for r in runs])),
+                "kernels_per_tick": int(st["kernels_per_tick"]),
+                "timing": "host wall clock of bsam_batch_run over all problems' steps, "
+                          "regrids included"}
+        finally:
+            for r in runs:
+                r.close()
         # Served form: the Poisson request stream at every configured rate
         # (120 requests each); the capacity is the solves/s the server
         # sustains once the arrival rate exceeds it.

@@ -26,6 +26,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -1198,29 +1199,59 @@ int flush(bsam_batch* b) {
 // no queued tick touches its fields) and starts its next step: the native
 // driver's AMR(rootlevel) and the start of MultigridIterations on the
 // problem's own engine and stream, then its new records and tiles, which
-// the batch's stream takes only after an event of the engine's.
+// the batch's stream takes only after an event of the engine's.  The
+// regrids touch only their own engines and run on host threads side by
+// side (their host clustering and device work overlap); the batch's tables
+// are then updated on this thread.
 int amr_service(bsam_batch* b) {
+  std::vector<int> due;
   for (size_t i = 0; i < b->slots.size(); ++i) {
+    const SlotPlan& S = b->slots[i];
+    if (S.used && S.amr && ((volatile SlotOut*)b->h_out)[i].phase == SLOT_REGRID)
+      due.push_back((int)i);
+  }
+  if (due.empty()) return BSAM_OK;
+  std::vector<int> rcs(due.size(), BSAM_OK);
+  std::vector<std::string> why(due.size());
+  std::atomic<size_t> next{0};
+  auto work = [&]() {
+    cudaSetDevice(b->device);
+    for (size_t k; (k = next.fetch_add(1)) < due.size();) {
+      SlotPlan& S = b->slots[due[k]];
+      int rc = bsam_amr_regrid(S.drv);
+      if (rc == BSAM_OK) rc = engine_prologue(S.eng);
+      if (rc == BSAM_OK) rc = engine_view(S.eng, S.view);
+      if (rc == BSAM_OK && cudaEventRecord(S.ready, engine_stream(S.eng)) != cudaSuccess)
+        rc = BSAM_ERR_CUDA;
+      if (rc != BSAM_OK) why[k] = bsam_gpu_last_error(S.eng);
+      rcs[k] = rc;
+    }
+  };
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const int nt = (int)std::min<size_t>(due.size(), std::min(16u, hw));
+  if (nt <= 1) {
+    work();
+  } else {
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nt; ++t) pool.emplace_back(work);
+    work();
+    for (auto& t : pool) t.join();
+  }
+  for (size_t k = 0; k < due.size(); ++k)
+    if (rcs[k] != BSAM_OK) return fail(b, rcs[k], "regrid of a refined problem: " + why[k]);
+  for (size_t k = 0; k < due.size(); ++k) {
+    const int i = due[k];
     SlotPlan& S = b->slots[i];
-    if (!S.used || !S.amr) continue;
     volatile SlotOut* o = b->h_out + i;
-    if (o->phase != SLOT_REGRID) continue;
     const int step = o->step, vcycles = o->vcycles;
-    int rc = bsam_amr_regrid(S.drv);
-    if (rc) return fail(b, rc, std::string("regrid: ") + bsam_gpu_last_error(S.eng));
-    rc = engine_prologue(S.eng);
-    if (rc) return fail(b, rc, std::string("step set-up: ") + bsam_gpu_last_error(S.eng));
-    rc = engine_view(S.eng, S.view);
-    if (rc) return fail(b, rc, "the engine holds no hierarchy");
-    rc = amr_plan(b, S);
+    int rc = amr_plan(b, S);
     if (rc) return rc;
-    CU(cudaEventRecord(S.ready, engine_stream(S.eng)));
     CU(cudaStreamWaitEvent(b->stream, S.ready, 0));
     if ((int)b->h_apt.size() > 2 * live_amr_records(b) + 4096) {
       rc = amr_compact(b);
       if (rc) return rc;
     }
-    amr_append(b, (int)i, true);
+    amr_append(b, i, true);
     SlotState st{SLOT_RUNNING, step, 0, vcycles};
     rc = stage_copy(b, b->d_state + i, &st, sizeof(st));
     if (rc) return rc;

@@ -130,8 +130,22 @@ class Server:
                 except Exception as exc:  # reported by serve() after the stream
                     errors.append(exc)
 
+        # Finished drivers are released on a thread of their own: freeing an
+        # engine's device memory waits for the whole device, which the
+        # server loop must not do while the batches have work queued.
+        close_q: queue.Queue = queue.Queue()
+
+        def closer():
+            while True:
+                run = close_q.get()
+                if run is None:
+                    return
+                run.close()
+
         threads = [threading.Thread(target=worker, daemon=True)
                    for _ in range(self.amr_workers if amr_left[0] else 0)]
+        if amr_left[0]:
+            threads.append(threading.Thread(target=closer, daemon=True))
         for th in threads:
             th.start()
         while nxt < len(reqs) or pending or inflight or amr_left[0] > 0:
@@ -208,7 +222,7 @@ class Server:
                         res["q"] = run.state()
                         res["descs"] = list(run.descs)
                     res["patches_final"] = run.npatch
-                    run.close()
+                    close_q.put(run)
                     r.result = res
                     amr_left[0] -= 1
                     done_any = True
@@ -218,8 +232,9 @@ class Server:
                     time.sleep(min(wait, 0.01))
             elif not done_any:
                 time.sleep(50e-6)
-        for _ in threads:
+        for _ in range(self.amr_workers):
             amr_q.put(None)
+        close_q.put(None)
         for th in threads:
             th.join()
         if errors:

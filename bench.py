@@ -719,7 +719,12 @@ def run_case(args):
     ticks          the full 512-problem workload, mixed, three eager ticks;
     amr2           the 2D AMR workload with sustained refinement (256^2 root,
                    two refined levels, regridded every step), FP64, three
-                   steps in the native driver."""
+                   steps in the native driver;
+    amr2-batch     32 problems of that workload in one FP64 batch
+                   (bsam_batch_submit_amr): one warm-up step, then two steps
+                   with eager ticks (each launch issued from the host),
+                   printing the host time spent regridding between steps
+                   and waiting for the device."""
     from bsam_b200 import batch as BB
     from bsam_b200 import build as BLD
     from bsam_b200 import workloads as W
@@ -737,6 +742,40 @@ def run_case(args):
             nv = [r.step()[0] for _ in range(3)]
             print(json.dumps({"case": args.case, "vcycles": nv, "patches": len(r.descs)}),
                   flush=True)
+        return 0
+    if args.case == "amr2-batch":
+        import time
+        from bsam_b200 import amr as AMR
+        runs = [AMR.AmrRun(*AMR.config2(sustained=True, seed=2 + i)) for i in range(32)]
+        try:
+            with BB.Batch(2, precision=BB.PREC_FP64, max_slots=32, pool_bytes=1 << 20) as ab:
+                slots = [ab.submit_amr(r, 1) for r in runs]
+                ab.run()
+                for s in slots:
+                    ab.collect_amr(s)
+                ab.set_tuning(eager=1)
+                slots = [ab.submit_amr(r, 2) for r in runs]
+                t_adv = t_wait = 0.0
+                ticks = 0
+                while True:
+                    t0 = time.perf_counter()
+                    ab.advance(1)
+                    t1 = time.perf_counter()
+                    ab.sync()
+                    t_wait += time.perf_counter() - t1
+                    t_adv += t1 - t0
+                    ticks += 1
+                    if len(ab.poll()) == len(slots):
+                        break
+                res = [ab.collect_amr(s) for s in slots]
+                print(json.dumps({"case": args.case, "ticks": ticks,
+                                  "host_advance_s": t_adv, "device_wait_s": t_wait,
+                                  "kernels_per_tick": ab.stats()["kernels_per_tick"],
+                                  "vcycles": [int(x["nvcycles"].sum()) for x in res[:4]]}),
+                      flush=True)
+        finally:
+            for r in runs:
+                r.close()
         return 0
     if args.case == "smooth2-small":
         probs = [W.seeded(2, 256, 0.01, 10, seed=500 + p, cbar=0.5, amp=0.025) for p in range(128)]
@@ -769,7 +808,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--quick", action="store_true", help="skip the side-by-side forms")
-    ap.add_argument("--case", choices=["smooth2-small", "ticks", "amr2"], default=None,
+    ap.add_argument("--case", choices=["smooth2-small", "ticks", "amr2", "amr2-batch"],
+                    default=None,
                     help="run a fixed small case for a profiler capture and exit")
     ap.add_argument("--fused-occ", type=int, default=0, choices=[0, 2, 3, 4],
                     help="case mode: the fused 2D stage's build (bsam_batch_tuning.fused_occ)")

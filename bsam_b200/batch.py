@@ -59,7 +59,8 @@ class BatchStats(ctypes.Structure):
                 ("pool_used", ctypes.c_int64), ("pool_bytes", ctypes.c_int64),
                 ("resident", ctypes.c_int32), ("running", ctypes.c_int32),
                 ("smooth_stages", ctypes.c_int64), ("smooth_ms", ctypes.c_double),
-                ("smooth_bytes", ctypes.c_double)]
+                ("smooth_bytes", ctypes.c_double), ("regrids", ctypes.c_int64),
+                ("regrid_s", ctypes.c_double)]
 
 
 def bind(L):

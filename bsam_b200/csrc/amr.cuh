@@ -346,8 +346,10 @@ __device__ __forceinline__ void ring2(int g, int m1, int m2, int& gi, int& gj) {
 __device__ __forceinline__ void ghost2_patch(const DevPatch* __restrict__ PT, int p,
                                              const OverlapCopy* __restrict__ cps, int2 rg,
                                              int ipass) {
-  const DevPatch P = PT[p];
-  const DevPatch R = PT[P.parent];
+  // The records are read in place (L1-cached), not copied: a copy of two
+  // records held 192 registers and limited the launch to two CTAs per SM.
+  const DevPatch& P = PT[p];
+  const DevPatch& R = PT[P.parent];
   const int m1 = P.n[0], m2 = P.n[1];
   const int nring = 2 * (m1 + 2) + 2 * m2;
   for (int g = threadIdx.x; g < nring; g += blockDim.x) {
@@ -408,8 +410,10 @@ __device__ __forceinline__ void ring3(int g, int m1, int m2, int m3, int& gi, in
 __device__ __forceinline__ void ghost3_patch(const DevPatch* __restrict__ PT, int p,
                                              const OverlapCopy* __restrict__ cps, int2 rg,
                                              int ipass) {
-  const DevPatch P = PT[p];
-  const DevPatch R = PT[P.parent];
+  // The records are read in place (L1-cached), not copied: a copy of two
+  // records held 192 registers and limited the launch to two CTAs per SM.
+  const DevPatch& P = PT[p];
+  const DevPatch& R = PT[P.parent];
   const int m1 = P.n[0], m2 = P.n[1], m3 = P.n[2];
   const int nring = 2 * (m1 + 2) * (m2 + 2) + m3 * (2 * (m1 + 2) + 2 * m2);
   for (int g = threadIdx.x; g < nring; g += blockDim.x) {

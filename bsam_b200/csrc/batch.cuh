@@ -285,7 +285,7 @@ __global__ void __launch_bounds__(BLOCK_THREADS, BATCH_LATENCY_MIN_BLOCKS)
 // SetGhost(level, ipass) of refined records, a CTA per record at a time:
 // items[b] = {record, first transfer, transfer count} into cps.
 template <int D>
-__global__ void __launch_bounds__(D == 2 ? 128 : 256)
+__global__ void __launch_bounds__(D == 2 ? 128 : 256, D == 2 ? 8 : 4)
     kb_ghost(const DevPatch* __restrict__ PT, const Item* __restrict__ items,
              const int* __restrict__ count, const OverlapCopy* __restrict__ cps, int ipass) {
   const int n = *count;
@@ -294,6 +294,31 @@ __global__ void __launch_bounds__(D == 2 ? 128 : 256)
     if (!PT[it.patch].active) continue;  // uniform per CTA
     if (D == 2) ghost2_patch(PT, it.patch, cps, make_int2(it.tx, it.ty), ipass);
     else ghost3_patch(PT, it.patch, cps, make_int2(it.tx, it.ty), ipass);
+  }
+}
+
+// One colour pass (RelaxGrid2D + write-through) over tiles shaped to narrow
+// patches: refined patches are 8-64 cells wide, so the 64-column tiles of
+// kb_relax leave most lanes idle.  items[b] = {record, tile x, tile y, W}:
+// W lanes per row (8, 16 or 32) each take a column pair, 128 / W rows per
+// tile; the cell of the pass's colour in each pair is updated as relax_item
+// updates it, so the pass is the same whatever the tile shape.
+__global__ void __launch_bounds__(BLOCK_THREADS)
+    kb_relax_narrow2(const DevPatch* __restrict__ PT, const Item* __restrict__ items,
+                     const int* __restrict__ count, int color, TileRuns R) {
+  const int n = *count;
+  const int t = threadIdx.x + blockDim.x * threadIdx.y;
+  for (int b = R.first(); b < n; b = R.next(b)) {
+    const Item it = items[b];
+    const DevPatch P = PT[it.patch];
+    if (!P.active) continue;  // uniform per CTA
+    const int W = it.tz;
+    const int j = it.ty * (BLOCK_THREADS / W) + t / W + 1;
+    if (j > P.n[1]) continue;
+    const int i0 = (it.tx * W + t % W) * 2 + 1;
+    const int i = i0 + ((i0 + j + color) & 1);
+    if (i > P.n[0]) continue;
+    relax_cell<double, 2>(P, i, j, 0);
   }
 }
 

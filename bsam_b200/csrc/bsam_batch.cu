@@ -93,7 +93,8 @@ enum {
   A_FILL = 2 + 2 * (MAXD + 1),
   A_GHOST = 2 + 3 * (MAXD + 1),
   A_SNAP = 2 + 4 * (MAXD + 1),
-  ANLIST = 2 + 5 * (MAXD + 1)
+  A_RELAX = 2 + 5 * (MAXD + 1),  // 2D: colour-pass tiles shaped to the patch width
+  ANLIST = 2 + 6 * (MAXD + 1)
 };
 
 struct List {
@@ -707,6 +708,15 @@ void amr_append(bsam_batch* b, int s, bool active) {
         const int p = E.patches[k];
         const DevPatch& P = V.recs[p];
         tiles_for(r0 + p, P.n, nd, LA[A_FINE + d].h);
+        if (nd == 2) {
+          // W lanes per row: the narrowest of 8, 16, 32 whose 2W columns
+          // cover the patch (or 32).
+          const int W = P.n[0] <= 16 ? 8 : (P.n[0] <= 32 ? 16 : 32);
+          const int rows = BLOCK_THREADS / W;
+          for (int y = 0; y < (P.n[1] + rows - 1) / rows; ++y)
+            for (int x = 0; x < (P.n[0] + 2 * W - 1) / (2 * W); ++x)
+              LA[A_RELAX + d].h.push_back(Item{r0 + p, x, y, W});
+        }
         tiles_for(r0 + p, P.cn, nd, LA[A_COARSE + d].h);
         if (E.amr) {
           tiles_for(r0 + p, P.cn, nd, LA[A_FILL + d].h);
@@ -910,8 +920,12 @@ void tick_t(bsam_batch* b, cudaGraphConditionalHandle handle, int in_graph) {
     if (LA[A_FINE + d].cap == 0) return;
     for (int pass = 0; pass < nu; ++pass)
       for (int color = 0; color < 2; ++color) {
-        kb_relax<double, D><<<agrid(A_FINE + d), blk, 0, s>>>(apt, LA[A_FINE + d].d,
-                                                              acnt + A_FINE + d, color, R);
+        if (D == 2)
+          kb_relax_narrow2<<<agrid(A_RELAX + d), blk, 0, s>>>(apt, LA[A_RELAX + d].d,
+                                                              acnt + A_RELAX + d, color, R);
+        else
+          kb_relax<double, D><<<agrid(A_FINE + d), blk, 0, s>>>(apt, LA[A_FINE + d].d,
+                                                                acnt + A_FINE + d, color, R);
         ++n;
         aghost(d, color + 1);
       }
@@ -1211,6 +1225,7 @@ int amr_service(bsam_batch* b) {
       due.push_back((int)i);
   }
   if (due.empty()) return BSAM_OK;
+  const auto t_start = std::chrono::steady_clock::now();
   std::vector<int> rcs(due.size(), BSAM_OK);
   std::vector<std::string> why(due.size());
   std::atomic<size_t> next{0};
@@ -1237,6 +1252,9 @@ int amr_service(bsam_batch* b) {
     work();
     for (auto& t : pool) t.join();
   }
+  b->st.regrids += (int64_t)due.size();
+  b->st.regrid_s +=
+      std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
   for (size_t k = 0; k < due.size(); ++k)
     if (rcs[k] != BSAM_OK) return fail(b, rcs[k], "regrid of a refined problem: " + why[k]);
   for (size_t k = 0; k < due.size(); ++k) {

@@ -119,6 +119,10 @@ typedef struct {
                              must read and write once (the fused 2D stages:
                              state, f, base, the restriction into or the
                              correction from the parent, the FP64 update) */
+  /* refined hierarchies (bsam_batch_submit_amr): regrids run between their
+     time steps and the host wall-clock seconds spent running them */
+  int64_t regrids;
+  double regrid_s;
 } bsam_batch_stats;
 
 int bsam_batch_create(bsam_batch** b, int device, const bsam_batch_params* p);

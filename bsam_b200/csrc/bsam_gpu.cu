@@ -108,6 +108,12 @@ struct bsam_gpu {
   char* d_regrid = nullptr;
   size_t regrid_cap = 0;
   std::vector<unsigned char> regrid_host;
+  // Page-locked bounce buffer (grown, never shrunk) for the handle's copies
+  // from and to pageable host memory; every user synchronises the stream
+  // before the buffer is written again.
+  void* h_pin = nullptr;
+  size_t pin_cap = 0;
+  bool attrs_set = false;      // the fused kernels' shared-memory attributes
   uint8_t* d_flags = nullptr;  // bsam_gpu_errflags_level's device flags
   int32_t* d_sat = nullptr;    // bsam_gpu_tag_level's summed-area tables
   size_t sat_cap = 0;
@@ -183,6 +189,44 @@ int fail(bsam_gpu* h, int code, const std::string& msg) {
 int64_t roundup(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
 
 LevelPlan& plan(bsam_gpu* h, int level) { return h->levels[level - h->minlevel]; }
+
+// The bounce buffer with room for `bytes`.  Copies through it are DMA
+// copies queued on the stream; copies from pageable memory instead pass
+// through the driver's staging, which handles regridding side by side on
+// several host threads contend for.
+void* pin_reserve(bsam_gpu* h, size_t bytes) {
+  if (bytes > h->pin_cap) {
+    if (h->h_pin) cudaFreeHost(h->h_pin);
+    h->h_pin = nullptr;
+    h->pin_cap = 0;
+    const size_t want = std::max<size_t>(bytes + bytes / 2, (size_t)1 << 16);
+    if (cudaMallocHost(&h->h_pin, want) != cudaSuccess) return nullptr;
+    h->pin_cap = want;
+  }
+  return h->h_pin;
+}
+
+// Queues a host -> device copy of pageable `src` through the bounce buffer
+// (the caller synchronises the stream before the buffer's next use).
+int h2d_bounce(bsam_gpu* h, void* dst, const void* src, size_t bytes) {
+  if (!bytes) return BSAM_OK;
+  void* p = pin_reserve(h, bytes);
+  if (!p) return fail(h, BSAM_ERR_NOMEM, "page-locked staging allocation failed");
+  std::memcpy(p, src, bytes);
+  CU(cudaMemcpyAsync(dst, p, bytes, cudaMemcpyHostToDevice, h->stream));
+  return BSAM_OK;
+}
+
+// Device -> pageable host through the bounce buffer; waits for the stream.
+int d2h_bounce(bsam_gpu* h, void* dst, const void* src, size_t bytes) {
+  if (!bytes) return BSAM_OK;
+  void* p = pin_reserve(h, bytes);
+  if (!p) return fail(h, BSAM_ERR_NOMEM, "page-locked staging allocation failed");
+  CU(cudaMemcpyAsync(p, src, bytes, cudaMemcpyDeviceToHost, h->stream));
+  CU(cudaStreamSynchronize(h->stream));
+  std::memcpy(dst, p, bytes);
+  return BSAM_OK;
+}
 
 void tiles_for(int patch, const int* n, int ndims, std::vector<Item>& out) {
   const int tx = (n[0] + TILE_X - 1) / TILE_X;
@@ -1108,10 +1152,13 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
     h->max_items = std::max(h->max_items, L.nfine);
   }
   h->max_items = std::max(h->max_items, h->nroot);
-  CU(cudaFuncSetAttribute(k_smooth3_fused<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          (int)Fused3<double>::SMEM));
-  CU(cudaFuncSetAttribute(k_smooth3_fused<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          (int)Fused3<float>::SMEM));
+  if (!h->attrs_set) {
+    CU(cudaFuncSetAttribute(k_smooth3_fused<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)Fused3<double>::SMEM));
+    CU(cudaFuncSetAttribute(k_smooth3_fused<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)Fused3<float>::SMEM));
+    h->attrs_set = true;
+  }
   // The residual trace buffers live as long as the handle (maxvcycles is
   // fixed at creation).
   if (!h->d_trace) CU(cudaMalloc(&h->d_trace, sizeof(double) * h->rp.maxvcycles));
@@ -1198,7 +1245,8 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
     put(o_qold, qold_spans.data(), sizeof(CopySpan) * qold_spans.size());
     put(o_maps, maps.data(), sizeof(CUtensorMap) * maps.size());
     put(o_tops, tops.data(), sizeof(int) * tops.size());
-    CU(cudaMemcpyAsync(h->d_meta, img.data(), img.size(), cudaMemcpyHostToDevice, h->stream));
+    const int urc = h2d_bounce(h, h->d_meta, img.data(), img.size());
+    if (urc) return urc;
   }
   CU(cudaMemsetAsync(h->d_status, 0, sizeof(DevStatus), h->stream));
   CU(cudaStreamSynchronize(h->stream));
@@ -1485,8 +1533,7 @@ static int upload_tasks(bsam_gpu* h, const void* src, size_t bytes) {
       return fail(h, BSAM_ERR_NOMEM, "task buffer allocation failed");
     h->regrid_cap = want;
   }
-  if (bytes) CU(cudaMemcpyAsync(h->d_regrid, src, bytes, cudaMemcpyHostToDevice, h->stream));
-  return BSAM_OK;
+  return h2d_bounce(h, h->d_regrid, src, bytes);
 }
 
 int bsam_gpu_errflags_level(bsam_gpu* h, int level, double tol, uint8_t* flags) {
@@ -1526,8 +1573,10 @@ int bsam_gpu_errflags_level(bsam_gpu* h, int level, double tol, uint8_t* flags) 
   else k_errflags_list<3><<<g, 256, 0, h->stream>>>(h->d_patches, d_tasks, tol, h->d_flags);
   ++h->stats.launches;
   CU(cudaGetLastError());
-  CU(cudaMemcpyAsync(flags, h->d_flags, total, cudaMemcpyDeviceToHost, h->stream));
-  CU(cudaStreamSynchronize(h->stream));
+  {
+    const int drc = d2h_bounce(h, flags, h->d_flags, total);
+    if (drc) return drc;
+  }
   return BSAM_OK;
 }
 
@@ -1596,9 +1645,7 @@ int bsam_gpu_tag_level(bsam_gpu* h, int level, double tol, int ibuffer, int32_t*
   }
   h->stats.launches += 3;
   CU(cudaGetLastError());
-  CU(cudaMemcpyAsync(sat, h->d_sat, sizeof(int32_t) * total, cudaMemcpyDeviceToHost, h->stream));
-  CU(cudaStreamSynchronize(h->stream));
-  return BSAM_OK;
+  return d2h_bounce(h, sat, h->d_sat, sizeof(int32_t) * total);
 }
 
 int bsam_gpu_init_patch(bsam_gpu* h, int patch) {
@@ -1826,8 +1873,10 @@ int bsam_gpu_stash(bsam_gpu* h) {
       return fail(h, BSAM_ERR_NOMEM, "stash allocation failed");
     h->stash_spans_cap = want;
   }
-  CU(cudaMemcpyAsync(h->d_stash_spans, spans.data(), sizeof(CopySpan) * spans.size(),
-                     cudaMemcpyHostToDevice, h->stream));
+  {
+    const int urc = h2d_bounce(h, h->d_stash_spans, spans.data(), sizeof(CopySpan) * spans.size());
+    if (urc) return urc;
+  }
   const int bx = (int)std::min<int64_t>((span_max + 255) / 256, 64);
   k_copy_spans<<<dim3(bx, (unsigned)spans.size()), 256, 0, h->stream>>>(h->d_stash_spans);
   ++h->stats.launches;
@@ -2049,6 +2098,7 @@ int bsam_gpu_destroy(bsam_gpu* h) {
   free_hierarchy(h);
   if (h->d_trace) cudaFree(h->d_trace);
   if (h->h_trace) cudaFreeHost(h->h_trace);
+  if (h->h_pin) cudaFreeHost(h->h_pin);
   if (h->spare_arena) cudaFree(h->spare_arena);
   if (h->d_stash) cudaFree(h->d_stash);
   if (h->d_stash_spans) cudaFree(h->d_stash_spans);

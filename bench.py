@@ -720,6 +720,9 @@ def run_case(args):
     amr2           the 2D AMR workload with sustained refinement (256^2 root,
                    two refined levels, regridded every step), FP64, three
                    steps in the native driver;
+    cfg3           the 3D 128^3 configuration: one time step in FP64, then
+                   one in the mixed form, V-cycle loops issued from the host
+                   (every kernel its own launch);
     amr2-batch     32 problems of that workload in one FP64 batch
                    (bsam_batch_submit_amr): one warm-up step, then two steps
                    with eager ticks (each launch issued from the host),
@@ -742,6 +745,14 @@ def run_case(args):
             nv = [r.step()[0] for _ in range(3)]
             print(json.dumps({"case": args.case, "vcycles": nv, "patches": len(r.descs)}),
                   flush=True)
+        return 0
+    if args.case == "cfg3":
+        import bsam_b200 as B
+        out = {"case": args.case}
+        for name, prec in (("fp64", B.PREC_FP64), ("mixed", B.PREC_MIXED)):
+            with B.Solver(W.config3(nsteps=1), precision=prec, graph=-1) as sv:
+                out[name] = [int(x) for x in sv.run(1, keep_steps=False)["nvcycles"]]
+        print(json.dumps(out), flush=True)
         return 0
     if args.case == "amr2-batch":
         import time
@@ -808,7 +819,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--quick", action="store_true", help="skip the side-by-side forms")
-    ap.add_argument("--case", choices=["smooth2-small", "ticks", "amr2", "amr2-batch"],
+    ap.add_argument("--case", choices=["smooth2-small", "ticks", "amr2", "amr2-batch", "cfg3"],
                     default=None,
                     help="run a fixed small case for a profiler capture and exit")
     ap.add_argument("--fused-occ", type=int, default=0, choices=[0, 2, 3, 4],

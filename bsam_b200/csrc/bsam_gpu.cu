@@ -43,6 +43,9 @@ namespace {
 
 // Levels with at most this many cells per patch stay FP64 in the mixed form.
 constexpr int64_t MIXED_FP64_CELLS = 4096;
+// Default largest level of the one-CTA bottom chain, per dimensionality.
+constexpr int DEFAULT_BOTTOM_CELLS_2D = 1024;
+constexpr int DEFAULT_BOTTOM_CELLS_3D = 512;
 
 struct LevelPlan {
   int level = 0;
@@ -755,7 +758,14 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
   // Bottom level: the finest level such that it and every coarser level hold
   // at most bottom_cells cells per patch (uniform hierarchies only).
   h->bottom_level = -1000;
-  const int bmax = h->tuning.bottom_cells == 0 ? BOTTOM_MAX_CELLS : h->tuning.bottom_cells;
+  // Default: chains from 1024 cells (2D) or 512 (3D) down.  The one-CTA
+  // chain runs on a single SM, so a larger top level there (4096 cells: 64^2,
+  // 16^3) leaves the rest of the GPU idle for longer than the grid kernels
+  // take for it (measured: 128^2 FP64 829 -> 915 time-steps/s; 16^3 .. 1^3
+  // alone was a quarter of a 128^3 V-cycle).
+  const bool dflt = h->tuning.bottom_cells == 0;
+  const int bmax = dflt ? (nd == 3 ? DEFAULT_BOTTOM_CELLS_3D : DEFAULT_BOTTOM_CELLS_2D)
+                        : h->tuning.bottom_cells;
   if (bmax > 0) {
     // Only the root and the levels below it (one uniform patch each).
     for (int l = minlevel; l <= std::min(finestlevel, 0); ++l) {
@@ -768,9 +778,11 @@ int bsam_gpu_set_hierarchy(bsam_gpu* h, int npatch, const bsam_patch_desc* patch
     if (h->bottom_level - minlevel + 1 > BOTTOM_MAX_DEPTH) h->bottom_level = -1000;
   }
   // Mixed form: levels at or below this size stay FP64 -- the levels the
-  // bottom kernel runs, including the coarsest (4096 cells when the bottom
-  // kernel is switched off).
-  const int64_t fp64_cells = bmax > 0 ? (int64_t)bmax : MIXED_FP64_CELLS;
+  // bottom kernel runs, including the coarsest; 4096 cells under the default
+  // bottom size and when the bottom kernel is switched off (the levels
+  // between the default bottom and 4096 cells run FP64 grid kernels, which
+  // give the bottom kernel's bits).
+  const int64_t fp64_cells = (!dflt && bmax > 0) ? (int64_t)bmax : MIXED_FP64_CELLS;
 
   // Records: the caller's patches, then one twin per finest-level patch in
   // the mixed form.

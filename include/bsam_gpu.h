@@ -81,8 +81,11 @@ int bsam_gpu_create(bsam_gpu** h, int device, const bsam_run_params* p);
  *   fuse_min_n     smallest extent per dimension of a fused level
  *   chunk          planes (3D) / rows (2D) per streaming chunk, 0 = automatic
  *   bottom_cells   levels of at most this many cells run their whole part of
- *                  the V-cycle in one single-CTA launch; 0 = default (4096),
- *                  -1 = never
+ *                  the V-cycle in one single-CTA launch (at most 4096);
+ *                  0 = default (1024 in 2D, 512 in 3D), -1 = never.  In the
+ *                  mixed form these levels are FP64; under the default and
+ *                  with -1, levels of at most 4096 cells are FP64 (the bits
+ *                  do not depend on which of them run in the bottom launch)
  *   graph          0 = run the V-cycle loop of MultigridIterations as one
  *                  captured CUDA graph with a device-side WHILE node (one
  *                  launch per call); -1 = host loop (one launch per kernel,

@@ -374,7 +374,10 @@ class Batch:
         out: a Fortran-ordered float64 array of q's shape to copy into (for
         instance one in page-locked memory, which the copy reaches at full
         speed); by default a new array.  want_mass=False skips the mass
-        reduction (one kernel and one wait fewer; "mass" is then None)."""
+        reduction (one kernel and one wait fewer; "mass" is then None).  A
+        refined hierarchy's slot (submit_amr) is collected by collect_amr."""
+        if self.is_amr(slot):
+            return self.collect_amr(slot, want_mass=want_mass)
         prob = self.probs[slot]
         shape = tuple(m + 2 for m in prob.mx[:prob.ndims]) + (2,)
         if out is not None:

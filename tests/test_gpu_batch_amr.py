@@ -123,3 +123,40 @@ def test_batch_amr_config2_sustained(gpu_lib):
     for g, a in zip(got, ref):
         assert max(a["patches"]) > 50
         same(g, a)
+
+
+def test_batch_amr_table_growth_compaction_and_slot_reuse(gpu_lib):
+    """Sixteen problems of the sustained AMR workload for five steps: their
+    records outgrow the refined table (reallocation, graph captured again)
+    and retired blocks outnumber the live ones (compaction) -- every result
+    still equals its driver's alone.  The freed slots then take uniform
+    problems of the mixed form, whose results equal their batch alone."""
+    nsteps = 5
+    seeds = list(range(40, 56))
+    ref = [alone(*amr.config2(sustained=True, seed=s), nsteps) for s in seeds]
+    runs = [amr.AmrRun(*amr.config2(sustained=True, seed=s)) for s in seeds]
+    uni = [W.seeded(2, n, 0.01, 2, seed=700 + n, cbar=0.5, amp=0.025) for n in (64, 96, 128)]
+    ualone = BB.solve_all(uni, precision=BB.PREC_MIXED)
+    try:
+        with BB.Batch(2, precision=BB.PREC_MIXED, max_slots=len(seeds), qerrortol=1e-8,
+                      maxvcycles=20) as b:
+            slots = [b.submit_amr(r, nsteps) for r in runs]
+            b.run()
+            got = [b.collect_amr(s) for s in slots]
+            st = b.stats()
+            assert st["regrids"] == len(seeds) * nsteps
+            assert st["captures"] >= 2
+            uslots = [b.submit(u) for u in uni]
+            assert all(s is not None for s in uslots)
+            b.run()
+            ugot = [b.collect(s) for s in uslots]
+        for r, g, a in zip(runs, got, ref):
+            g["descs"] = r.descs
+            g["q"] = r.state()
+            same(g, a)
+        for g, a in zip(ugot, ualone):
+            for k in ("q", "nvcycles", "residual", "converged"):
+                assert np.array_equal(g[k], a[k]), k
+    finally:
+        for r in runs:
+            r.close()

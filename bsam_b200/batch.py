@@ -50,7 +50,7 @@ class BatchTuning(ctypes.Structure):
     _fields_ = [("grid_ctas", ctypes.c_int32), ("eager", ctypes.c_int32),
                 ("per_pass", ctypes.c_int32), ("fused_ctas", ctypes.c_int32),
                 ("fused_occ", ctypes.c_int32), ("tile_chunk", ctypes.c_int32),
-                ("fused_chunk", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("fused_chunk", ctypes.c_int32), ("regrid_threads", ctypes.c_int32)]
 
 
 class BatchStats(ctypes.Structure):
@@ -175,10 +175,10 @@ class Batch:
 
     def set_tuning(self, grid_ctas: int = 0, eager: int = 0, per_pass: int = 0,
                    fused_ctas: int = 0, fused_occ: int = 0, tile_chunk: int = 0,
-                   fused_chunk: int = 0):
+                   fused_chunk: int = 0, regrid_threads: int = 0):
         t = BatchTuning(grid_ctas=grid_ctas, eager=eager, per_pass=per_pass,
                         fused_ctas=fused_ctas, fused_occ=fused_occ, tile_chunk=tile_chunk,
-                        fused_chunk=fused_chunk)
+                        fused_chunk=fused_chunk, regrid_threads=regrid_threads)
         _check(_lib().bsam_batch_set_tuning(self.h, ctypes.byref(t)), self.h, "set_tuning")
 
     def profile(self, enable: bool = True):

@@ -90,7 +90,8 @@ typedef struct {
  * many consecutive tiles, run r to CTA r mod the grid (1 = grid-stride;
  * consecutive tiles mostly share their problem's records, which a run then
  * reads from L1), for the small-tile list kernels (0 = 2) and for the fused
- * stages (0 = 1). */
+ * stages (0 = 1); regrid_threads sets how many host threads run the regrids
+ * of refined problems (bsam_batch_submit_amr) that wait at one advance. */
 typedef struct {
   int32_t grid_ctas;
   int32_t eager;
@@ -99,7 +100,9 @@ typedef struct {
   int32_t fused_occ;
   int32_t tile_chunk;
   int32_t fused_chunk;
-  int32_t reserved;
+  int32_t regrid_threads;  /* host threads for the regrids of refined problems
+                              that paused together (0 = the host's hardware
+                              threads, at most 16) */
 } bsam_batch_tuning;
 
 typedef struct {

@@ -191,7 +191,6 @@ struct bsam_batch {
   std::vector<int> acounts_dev;
   double* d_apartials = nullptr;
   int apartials_cap = 0;
-  int amr_live_recs = 0;  // records of the current blocks of resident refined slots
   // graph
   cudaGraphExec_t exec = nullptr;
   int cap_depth = 0;

@@ -1259,15 +1259,29 @@ int amr_service(bsam_batch* b) {
   b->st.regrids += (int64_t)due.size();
   b->st.regrid_s +=
       std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
-  for (size_t k = 0; k < due.size(); ++k)
-    if (rcs[k] != BSAM_OK) return fail(b, rcs[k], "regrid of a refined problem: " + why[k]);
+  // A problem whose regrid (or new hierarchy) fails ends as SLOT_FAILED
+  // (its driver's state is not that of a completed regrid); the others start
+  // their next step; the first failure is returned.
+  int first_rc = BSAM_OK;
+  std::string first_why;
   for (size_t k = 0; k < due.size(); ++k) {
     const int i = due[k];
     SlotPlan& S = b->slots[i];
     volatile SlotOut* o = b->h_out + i;
     const int step = o->step, vcycles = o->vcycles;
-    int rc = amr_plan(b, S);
-    if (rc) return rc;
+    int rc = rcs[k];
+    if (rc == BSAM_OK) rc = amr_plan(b, S);
+    if (rc != BSAM_OK) {
+      if (first_rc == BSAM_OK) {
+        first_rc = rc;
+        first_why = why[k].empty() ? b->err : why[k];
+      }
+      SlotState st{SLOT_FAILED, step, 0, vcycles};
+      const int src = stage_copy(b, b->d_state + i, &st, sizeof(st));
+      if (src) return src;
+      o->phase = SLOT_FAILED;
+      continue;
+    }
     CU(cudaStreamWaitEvent(b->stream, S.ready, 0));
     if ((int)b->h_apt.size() > 2 * live_amr_records(b) + 4096) {
       rc = amr_compact(b);
@@ -1279,6 +1293,8 @@ int amr_service(bsam_batch* b) {
     if (rc) return rc;
     o->phase = SLOT_RUNNING;
   }
+  if (first_rc != BSAM_OK)
+    return fail(b, first_rc, "regrid of a refined problem: " + first_why);
   return BSAM_OK;
 }
 
@@ -1999,7 +2015,10 @@ int bsam_batch_collect(bsam_batch* b, int slot, double* q, bsam_step_result* ste
     b->h_cfg[slot] = SlotCfg{};
     b->cfg_dirty = true;
     if (rc) return fail(b, rc, "reading the refined hierarchy's engine failed");
-    return ph == SLOT_FAILED ? fail(b, BSAM_ERR_DIVERGED, "residual is not finite") : BSAM_OK;
+    return ph == SLOT_FAILED
+               ? fail(b, BSAM_ERR_DIVERGED, "the problem failed: a residual was not finite or a "
+                                            "regrid failed (bsam_batch_advance reported it)")
+               : BSAM_OK;
   }
   const int nd = b->bp.ndims;
   const int rec_master = slot * RMAX + S.master;

@@ -184,6 +184,8 @@ int bsam_batch_submit_seeded_many(bsam_batch* b, int n, const bsam_batch_problem
  * are bitwise those of nsteps calls of bsam_amr_step.  Until the slot is
  * collected (bsam_batch_collect; collect_many refuses it), the caller must
  * not use the driver or its engine.  Occupies a slot but no pool memory.
+ * A regrid that fails ends its problem as BSAM_SLOT_FAILED (the advance that
+ * ran it returns the error; the other problems go on).
  * Replaces the time-step loop of TakeTimeSteps (lib/bsamroutines.f90:
  * 632-723) for that problem; no reference counterpart for the batching. */
 int bsam_batch_submit_amr(bsam_batch* b, bsam_amr* a, int nsteps, int* slot);
